@@ -1,0 +1,81 @@
+"""Oracle: CCD detector (test infrastructure only).
+
+Restates specula/processing_objects/ccd.py:198-287 (integration, binning,
+QE, background/dark, Poisson photon noise, Gaussian readout noise, ADU
+quantisation).  Excess (EMCCD), CIC and CTE noise are not on the SCAO SH
+step and are not restated.
+
+Noise draws use the same NumPy generators as the reference CPU path
+(``default_rng(photon_seed)``, ``default_rng(readout_seed)``), so with equal
+seeds this oracle reproduces the reference CPU CCD bit for bit.
+"""
+import numpy as np
+
+
+class CCDOracle:
+    def __init__(self, size, dt_s, loop_dt_s, bandw, binning=1, photon_noise=False,
+                 readout_noise=False, background_noise=False, darkcurrent_noise=False,
+                 readout_level=0.0, background_level=0.0, darkcurrent_level=0.0,
+                 quantum_eff=1.0, photon_seed=1, readout_seed=2, ADU_gain=8, ADU_bias=400,
+                 precision=1):
+        self.dtype = np.float32 if precision == 1 else np.float64
+        self.size = (size[0] // binning, size[1] // binning)
+        self.binning = binning
+        self.integrated = np.zeros((self.size[0] * binning, self.size[1] * binning), dtype=self.dtype)
+        self.dt_ratio = loop_dt_s * bandw
+        self.frames_per_read = int(round(dt_s / loop_dt_s))
+        self.count = 0
+        self.photon_noise = photon_noise
+        self.readout_noise = readout_noise
+        self.background_noise = background_noise
+        self.darkcurrent_noise = darkcurrent_noise
+        self.readout_level = readout_level
+        self.background_level = background_level
+        self.darkcurrent_level = darkcurrent_level
+        self.qe = quantum_eff
+        self.gain = ADU_gain
+        self.bias = ADU_bias
+        self.photon_rng = np.random.default_rng(photon_seed)
+        self.readout_rng = np.random.default_rng(readout_seed)
+
+    def step(self, intensity):
+        """One loop step; returns the frame when a read-out happens, else None
+        (ccd.py:198-216 with start_time 0)."""
+        self.integrated += intensity * self.dt_ratio
+        self.count += 1
+        if self.count % self.frames_per_read:
+            return None
+        frame = self._binning()
+        if self.qe != 1:
+            frame = frame * self.qe
+        frame = self._noise(frame)
+        self.integrated *= 0.0
+        return frame
+
+    def _binning(self):
+        # ccd.py:264-280
+        f = self.integrated.copy()
+        if self.binning > 1:
+            tot = np.sum(f)
+            b = self.binning
+            f = f.reshape(self.size[0], b, self.size[1], b).sum(axis=(1, 3))
+            f = f * b ** 2 * (tot / np.sum(f))
+        return f
+
+    def _noise(self, f):
+        # ccd.py:218-262
+        if self.background_noise or self.darkcurrent_noise:
+            f += (self.background_level + self.darkcurrent_level)
+        if self.photon_noise:
+            f = self.photon_rng.poisson(f)                      # int64 from here on
+        if self.readout_noise:
+            ron = self.readout_rng.standard_normal(size=f.size)
+            f += (ron.reshape(f.shape) * self.readout_level).astype(f.dtype)
+        if self.photon_noise:
+            f = np.round(f * self.gain) + self.bias
+            f = np.where(f < 0, 0, f)
+            f -= self.bias
+            f = (f / self.gain).astype(f.dtype)
+            if self.darkcurrent_noise:
+                f -= self.darkcurrent_level
+        return f
