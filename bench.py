@@ -1,0 +1,321 @@
+"""Benchmark: closed-loop SCAO Shack-Hartmann steps per second on B200.
+
+Workload (one step = one pass of the whole loop over one frame): 39 m pupil
+on 640 px, 80x80 sub-apertures of 8x8 phase px, 16x16 FFT (cut 4) onto 6x6
+detector px, complex64 field, 7-layer atmosphere (Cn2 0.5/0.15/0.1/0.1/
+0.05/0.05/0.05, 0-16 km, winds 5-30 m/s in random directions), r0 0.15 m,
+L0 25 m, photon noise (1e3 ph / sub-aperture / frame) and 3 e- read-out,
+500-mode DM, modal reconstructor, integrator gain 0.5 with 2-frame delay.
+Synthetic seeded inputs (screens from the von Karman synthesis, random
+influence functions and reconstructor of the right shapes).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One JSON line on rank 0.  ``value``: whole-job steps/s of the captured
+CUDA-graph step with everything resident in HBM; ``e2e``: steps/s through
+the public object API (LoopControl.iter) with the per-step inputs copied
+host->device and the slopes + DM commands read back device->host.
+``--impl reference`` times the CPU oracle (NumPy restatement of the
+reference's CPU path) on the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = 'SH loop steps/s at 80x80 subaps'
+UNIT = 'steps/s'
+WORKLOAD = 'elt_80x80_fft16_7layers_500modes'
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument('--gpus', type=int, default=1)
+    p.add_argument('--steps', type=int, default=200)
+    p.add_argument('--warmup', type=int, default=5)
+    p.add_argument('--impl', default='b200', choices=['b200', 'reference'])
+    p.add_argument('--cpu-baseline-seconds', type=float, default=20.0)
+    p.add_argument('--no-cpu-baseline', action='store_true')
+    return p.parse_args()
+
+
+def config_dict(cfg, n_gpus):
+    return {'workload': WORKLOAD, 'pupil_px': cfg.pixel_pupil, 'diameter_m': cfg.diameter_m,
+            'subaps': f'{cfg.n_lenses}x{cfg.n_lenses}', 'phase_px_per_subap': cfg.pixel_pupil // cfg.n_lenses,
+            'fft': 16, 'detector_px_per_subap': cfg.subap_npx, 'layers': len(cfg.heights), 'modes': cfg.n_modes,
+            'parallelism': f'replicas{n_gpus}',
+            'l2': 'inputs larger than L2 (influence functions 631 MB streamed every step)'}
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms in the background."""
+    FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+              'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+              'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, gpu_index):
+        self.gpu = str(gpu_index)
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', self.gpu, f'--query-gpu={self.FIELDS}',
+                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for l in self.lines:
+            f = [x.strip() for x in l.split(',')]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() in ('active', '1', 'yes'):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {'sm_mhz': statistics.median(sm), 'sm_max_mhz': mx, 'reasons': sorted(reasons), 'samples': len(sm)}
+
+
+def measured_peak_hbm():
+    try:
+        with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as f:
+            return float(json.load(f)['hbm_gbs']), 'measured'
+    except (OSError, KeyError, ValueError):
+        return 6650.0, 'fallback'
+
+
+def cpu_oracle_loop(cfg, loop=None):
+    """Oracle chain on the bench workload; uses the GPU loop's IF / R / tables
+    when given so both arms run the same system."""
+    from oracle.loop import OracleScaoLoop
+    from specula_b200.scao import ScaoLoop, valid_subaps
+    from specula_b200.lib.make_mask import make_mask
+    import math
+    pupil = make_mask(cfg.pixel_pupil, cfg.obsratio, 1.0)
+    idxs, _ = valid_subaps(pupil, cfg.n_lenses, cfg.subap_npx)
+    nv = int(pupil.sum())
+    rng = np.random.default_rng(cfg.seed)
+    if loop is not None:
+        ifunc = loop.dm._ifunc.influence_function.cpu().numpy()
+        recmat = loop.rec.recmat.recmat.cpu().numpy()
+        S0 = loop.prop.outputs['out_on_axis_source_ef'].S0
+    else:
+        ifunc = rng.standard_normal((cfg.n_modes, nv), dtype=np.float32) * 10.0
+        recmat = rng.standard_normal((cfg.n_modes, 2 * len(idxs)), dtype=np.float32) / math.sqrt(2 * len(idxs))
+        n_valid_est = max(1, int(round(pupil.sum() / (cfg.pixel_pupil / cfg.n_lenses) ** 2)))
+        S0 = cfg.photons_per_subap * n_valid_est / (pupil.sum() * cfg.pitch ** 2 * cfg.time_step)
+    return OracleScaoLoop(cfg, ifunc, recmat, idxs, pupil, S0)
+
+
+def blas_threads():
+    try:
+        from threadpoolctl import threadpool_info
+        n = [i.get('num_threads', 1) for i in threadpool_info() if i.get('user_api') == 'blas']
+        return max(n) if n else 1
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def time_cpu_oracle(cfg, budget_s, max_steps, loop=None):
+    """Steps/s of the CPU oracle: one untimed step, then steps until the
+    budget is spent (at most max_steps)."""
+    ol = cpu_oracle_loop(cfg, loop)
+    ol.step()
+    n = 0
+    t0 = time.perf_counter()
+    while n < max_steps and (time.perf_counter() - t0) < budget_s:
+        ol.step()
+        n += 1
+    dt = time.perf_counter() - t0
+    return n / dt, n, dt
+
+
+def run_reference(args):
+    from specula_b200.scao import elt_config
+    rank = int(os.environ.get('RANK', '0'))
+    if rank != 0:
+        return
+    cfg = elt_config()
+    steps = max(1, min(args.steps, 50))
+    value, n, dt = time_cpu_oracle(cfg, budget_s=120.0, max_steps=steps)
+    cores = blas_threads()
+    sample = f'{n} oracle loop steps of the workload after 1 untimed step ({dt:.1f} s)'
+    line = {'metric': METRIC, 'value': value, 'unit': UNIT, 'impl': 'reference', 'n_gpus': args.gpus,
+            'steps': n, 'warmup': 1, 'ms_per_step': 1e3 / value, 'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic', 'config': config_dict(cfg, 1),
+            'cpu_baseline': {'value': value, 'unit': UNIT, 'cores': cores, 'kind': 'port', 'sample': sample},
+            'e2e': {'value': value, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+    from specula_b200.scao import ScaoLoop, elt_config
+    from specula_b200 import _lib
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    torch.cuda.set_device(local)
+    dev = torch.device('cuda', local)
+    if world > 1:
+        import datetime
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    cfg = elt_config()
+    loop = ScaoLoop(cfg, device_idx=local)
+    loop.start()
+    loop.step_eager()                     # t = 0 (no screen motion yet)
+    loop.capture()
+    for _ in range(max(3, args.warmup)):
+        loop.replay()
+    torch.cuda.synchronize(dev)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    st = torch.cuda.current_stream(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(args.steps):
+        loop.replay()
+    e1.record(st)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * args.steps / (ms_max / 1e3)
+
+    # dominant kernel: DM influence-function projection, timed alone on the
+    # launching stream (IF = 631 MB > L2, so no launch reuses cached lines)
+    dm = loop.dm
+    n_rep = max(20, min(args.steps, 200))
+    dm.trigger_code()
+    torch.cuda.synchronize(dev)
+    d0 = torch.cuda.Event(enable_timing=True)
+    d1 = torch.cuda.Event(enable_timing=True)
+    d0.record(st)
+    for _ in range(n_rep):
+        dm.trigger_code()
+    d1.record(st)
+    torch.cuda.synchronize(dev)
+    dm_ms = d0.elapsed_time(d1) / n_rep
+    nm, nv = dm._IF.shape[0], loop.n_valid_pixels
+    dm_bytes = nm * nv * 4 + nm * 4 + nv * 4 + nv * 4   # IF + commands + index table + phase writes
+    peak, peak_kind = measured_peak_hbm()
+    achieved = dm_bytes / (dm_ms / 1e3) / 1e9
+
+    # algorithmic bytes of one whole step (screens, pupil, IF, R, DM phase,
+    # detector frame, slopes, modes): the step's own roofline position
+    L = cfg.pixel_pupil
+    nsl = 2 * loop.n_valid_subaps
+    step_bytes = (len(cfg.heights) * L * (L + 1) * 4 + L * L * 4 + nm * nv * 4 + nm * nsl * 4 + L * L * 4 +
+                  (cfg.n_lenses * cfg.subap_npx) ** 2 * 4 + nsl * 4 + nm * 4)
+
+    # end to end through the public API: LoopControl.iter object by object,
+    # per-step host->device input copy and device->host read of the results
+    e2e_steps = max(10, min(args.steps, 100))
+    h_in = torch.empty(1 + 2 * len(cfg.heights), dtype=torch.float64).pin_memory()
+    h_in[0] = cfg.seeing
+    h_in[1:1 + len(cfg.heights)] = torch.tensor(cfg.wind_speed)
+    h_in[1 + len(cfg.heights):] = torch.tensor(cfg.wind_direction)
+    d_in = torch.empty_like(h_in, device=dev)
+    h_out = torch.empty(nsl + nm, dtype=torch.float32).pin_memory()
+    nl = len(cfg.heights)
+    for _ in range(3):
+        loop.step_eager()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        d_in.copy_(h_in, non_blocking=True)
+        loop.seeing.value = d_in[0:1]
+        loop.wind_speed.value = d_in[1:1 + nl]
+        loop.wind_direction.value = d_in[1 + nl:]
+        loop.step_eager()
+        h_out[:nsl].copy_(loop.slopec.slopes.slopes, non_blocking=True)
+        h_out[nsl:].copy_(loop.integ.out_comm.value, non_blocking=True)
+        torch.cuda.synchronize(dev)
+    e2e_dt = time.perf_counter() - t0
+    e2e = torch.tensor([e2e_dt], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(e2e, op=dist.ReduceOp.MAX)
+    e2e_value = world * e2e_steps / float(e2e.item())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, n, dt = time_cpu_oracle(cfg, budget_s=args.cpu_baseline_seconds, max_steps=200, loop=loop)
+        cpu = {'value': v, 'unit': UNIT, 'cores': blas_threads(), 'kind': 'port',
+               'sample': f'{n} CPU-oracle loop steps of the same system after 1 untimed step ({dt:.1f} s)'}
+
+    if rank == 0:
+        line = {'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
+                'warmup': max(3, args.warmup), 'ms_per_step': ms_max / args.steps, 'higher_is_better': True,
+                'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+                'config': config_dict(cfg, world),
+                'e2e': {'value': e2e_value, 'unit': UNIT, 'h2d_bytes_per_step': int(h_in.numel() * 8),
+                        'd2h_bytes_per_step': int(h_out.numel() * 4)},
+                'gpu_launches': ScaoLoop.KERNELS_PER_STEP * args.steps,
+                'roofline': {'bound': 'hbm', 'kernel': 'dm_project_kernel', 'achieved': achieved, 'peak': peak,
+                             'peak_kind': peak_kind, 'unit': 'GB/s', 'frac': achieved / peak, 'traffic': None,
+                             'algorithmic_bytes_per_launch': dm_bytes, 'avg_launch_us': dm_ms * 1e3},
+                'step_roofline': {'algorithmic_bytes': step_bytes,
+                                  'achieved_gbs': step_bytes / (ms_max / args.steps / 1e3) / 1e9,
+                                  'frac': step_bytes / (ms_max / args.steps / 1e3) / 1e9 / peak},
+                'clocks': clk, 'cpu_baseline': cpu}
+        print(json.dumps(line), flush=True)
+    del loop
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == 'reference':
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == '__main__':
+    main()

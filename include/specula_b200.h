@@ -1,0 +1,242 @@
+/*
+ * specula_b200.h — C ABI of the B200 closed-loop Shack-Hartmann step.
+ *
+ * Every entry point takes plain device pointers, sizes and a cudaStream_t
+ * (passed as void*), launches its kernels on that stream and returns an int
+ * status (SB_OK == 0, negative on error; sb_last_error() describes the last
+ * failure of the calling thread).  No entry point allocates device memory or
+ * synchronises the host, so a sequence of calls can be captured in a CUDA
+ * graph.  Work buffers ("scratch") are passed in by the caller; their size is
+ * given by the matching *_scratch_bytes() query.
+ *
+ * Each function cites the reference (SPECULA) code it replaces; paths are
+ * relative to the SPECULA project root.  The Python processing objects of
+ * the package (specula_b200.processing_objects.*) call these through ctypes
+ * from their trigger_code().
+ */
+#ifndef SPECULA_B200_H
+#define SPECULA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SB_OK 0
+#define SB_EINVAL (-1)        /* bad pointer or parameter value            */
+#define SB_ESHAPE (-2)        /* sizes outside what the kernels support     */
+#define SB_ECUDA (-3)         /* a CUDA launch or query failed              */
+#define SB_ESCRATCH (-4)      /* scratch buffer missing or too small        */
+#define SB_ETIMEOUT (-5)      /* a bounded device-side wait gave up         */
+#define SB_EUNSUPPORTED (-6)  /* option not implemented on this path        */
+
+/* ABI version (major*100 + minor). */
+int sb_version(void);
+/* Message of the last failing call on this host thread ("" if none). */
+const char *sb_last_error(void);
+
+/* ------------------------------------------------------------------------
+ * SH sensor forward model
+ * replaces specula/processing_objects/sh.py:348-420 (trigger_code: field
+ * build, zero-padded FFT, |E|^2, fftshift, field-stop mask, FoV cut, mosaic)
+ * + specula/lib/toccd.py:33-113 (LCM area rebin)
+ * + specula/processing_objects/sh.py:422-428 (post_trigger photon
+ * normalisation i *= S0*masked_area/sum(i)).
+ *
+ * Geometry integers come from the host-side solve that restates
+ * sh.py:112-323.  The DFT is evaluated only on the cut window and only from
+ * the np x np non-zero samples of each zero-padded sub-aperture.
+ * ---------------------------------------------------------------------- */
+typedef struct sb_sh_plan {
+    int n_lenses;        /* sub-apertures per side (Lenslet.dimx == dimy)      */
+    int np_sub;          /* field samples per sub-aperture side (ovs_np_sub)   */
+    int cutsize;         /* focal-plane samples kept per side (fft - cut)      */
+    int subap_npx;       /* detector pixels per sub-aperture side              */
+    int field_ld;        /* row stride (elements) of A and phase               */
+    float phase_to_rad;  /* float32(2*pi/lambda_nm)                            */
+    /* device tables, all float32, prepared once at setup */
+    const float *twiddle;  /* [cutsize][np_sub][2]: exp(-2*pi*i*k_b*c/fft)    */
+    const float *tilt;     /* [np_sub][np_sub][2]: half-pixel tilt (sh.py:469) */
+    const float *fp_mask;  /* [cutsize][cutsize]: field stop on the cut window */
+    const float *rebin;    /* [subap_npx][cutsize]: LCM overlap / dx_out       */
+} sb_sh_plan;
+
+size_t sb_sh_scratch_bytes(const sb_sh_plan *plan);
+
+/*
+ * A, phase_nm: the sampled field, (n_lenses*np_sub) rows of field_ld floats.
+ * A_norm: amplitude of the field the SH object received (n_norm floats; the
+ *   same pointer as A unless the field was resampled).
+ * photon_scale: S0 * pixel_pitch^2 of that field.
+ * intensity: (n_lenses*subap_npx)^2 float32, row-major, scaled so that its
+ *   sum equals photon_scale * sum(A_norm) (sh.py:425-427).
+ */
+int sb_sh_forward(const sb_sh_plan *plan, const float *A, const float *phase_nm,
+                  const float *A_norm, int n_norm, float photon_scale, float *intensity,
+                  void *scratch, size_t scratch_bytes, void *stream);
+
+/* replaces specula/lib/extrapolate_edge_pixel.py:4-28.
+ * out[p] = phase[p] if src1[p] < 0; phase[src1[p]] if src2[p] < 0;
+ * else 2*phase[src1[p]] - phase[src2[p]].  Tables from the host restatement
+ * of specula/lib/extrapolate_edge_pixel_mat_define.py:5-143. */
+int sb_edge_extrapolate(const float *phase, const int32_t *src1, const int32_t *src2,
+                        int n_pixels, float *out, void *stream);
+
+/* replaces specula/lib/interp2d.py:95-122 for the SH oversampling
+ * (sh.py:353-357): bilinear resampling of A and phase at precomputed,
+ * clamped coordinates yy/xx (float32, n_out entries) of an in_rows x in_cols
+ * input; the last input row is handled like the reference kernel
+ * (interp2d.py:31-38). */
+int sb_interp2d_field(const float *A_in, const float *phase_in, int in_rows, int in_cols,
+                      const float *yy, const float *xx, int n_out,
+                      float *A_out, float *phase_out, void *stream);
+
+/* ------------------------------------------------------------------------
+ * CCD — replaces specula/processing_objects/ccd.py:198-287 (integration,
+ * binning 1, QE, background/dark, Poisson photon noise, Gaussian readout,
+ * ADU quantisation).  Noise is drawn from a counter-based Philox4x32-10
+ * stream keyed by (seed, frame, pixel): deterministic and reproducible.
+ * ---------------------------------------------------------------------- */
+typedef struct sb_ccd_state {   /* device-resident, zero-initialised      */
+    uint64_t frame_index;   /* frames read so far: the RNG counter            */
+    int n_integrated;       /* loop steps integrated into the open frame      */
+    unsigned int blocks_done;  /* internal: completion count of the last launch */
+} sb_ccd_state;
+
+typedef struct sb_ccd_params {
+    int n_pixels;
+    int frames_per_read;    /* detector dt / loop dt (ccd.py:59-63,207)       */
+    float rate;             /* loop_dt_s * bandw (ccd.py:205)                 */
+    float qe;
+    float bg_plus_dark;     /* added when background or dark noise is on      */
+    int photon_noise;
+    int readout_noise;
+    float readout_level;
+    float adu_gain;
+    float adu_bias;
+    float dark_level;       /* subtracted after ADU when dark noise is on     */
+    int dark_noise;
+    uint64_t photon_seed;
+    uint64_t readout_seed;
+    sb_ccd_state *state;    /* device pointer; advanced by the kernel itself  */
+} sb_ccd_params;
+
+/* One loop step: integrate; when the frame closes, read it out into
+ * `pixels` (otherwise `pixels` is left untouched).  The frame counter and
+ * the integration count live in *state, so repeated calls (or replays of a
+ * captured graph) draw fresh noise every frame. */
+int sb_ccd_step(const sb_ccd_params *p, const float *intensity, float *integrated,
+                float *pixels, void *stream);
+
+/* Raw Philox4x32-10 stream, for determinism tests: out[4*i..4*i+3] is the
+ * block for counter (i, c1, c2, c3) under key (key0, key1). */
+int sb_philox_raw(uint32_t key0, uint32_t key1, uint32_t c1, uint32_t c2, uint32_t c3,
+                  int n_blocks, uint32_t *out, void *stream);
+
+/* ------------------------------------------------------------------------
+ * ShSlopec — replaces specula/processing_objects/sh_slopec.py:308-438
+ * (calc_slopes_nofor: gather, threshold, clamp, CoG with the
+ * 1e-3*mean(flux) cut-off) with weights from sh_slopec.py:86-132.
+ * slopes = [sx(0..n-1), sy(0..n-1)] (slopes.py:26-33).
+ * ---------------------------------------------------------------------- */
+typedef struct sb_slopec_plan {
+    int n_subaps;
+    int npx2;               /* pixels per sub-aperture (np_sub^2)             */
+    float thr;              /* subtracted then clamped at 0 (0: no threshold) */
+    const int32_t *idxs;    /* [n_subaps][npx2] flat indices into the frame   */
+    const float *xw;        /* [npx2] x weights                               */
+    const float *yw;        /* [npx2] y weights                               */
+    const float *mw;        /* [npx2] mask weights                            */
+} sb_slopec_plan;
+
+size_t sb_slopec_scratch_bytes(const sb_slopec_plan *plan);
+int sb_slopec(const sb_slopec_plan *plan, const float *pixels, float *slopes, float *flux,
+              void *scratch, size_t scratch_bytes, void *stream);
+
+/* ------------------------------------------------------------------------
+ * Modalrec — replaces specula/processing_objects/modalrec.py:159
+ * (modes = R @ slopes), R row-major (n_modes x n_slopes).
+ * ---------------------------------------------------------------------- */
+int sb_modalrec(const float *R, int n_modes, int n_slopes, int ldr, const float *slopes,
+                float *modes, void *stream);
+
+/* ------------------------------------------------------------------------
+ * Integrator — replaces specula/processing_objects/iir_filter.py:100-211
+ * for the 2-tap filters built by iir_filter_data.py:264-292 (num=[0,g],
+ * den=[-ff,1]); state is (n x total) with total = ceil(delay)+1, ist/ost are
+ * (n x 2).  Output = state[:, delay] (integer delay) or the fractional mix.
+ * ---------------------------------------------------------------------- */
+typedef struct sb_iir_plan {
+    int n;
+    int total;              /* state columns (ceil(delay) + 1)                */
+    int shift;              /* delay > 0: shift the state buffer first        */
+    int k_out;              /* state column read (int(delay) or ceil(delay))  */
+    float rem;              /* delay % 1 (0: integer delay)                   */
+    float one_minus_rem;    /* 1 - (delay % 1), rounded once on the host      */
+    const float *num;       /* [n][2] */
+    const float *den;       /* [n][2] */
+    float *ist;             /* [n][2] */
+    float *ost;             /* [n][2] */
+    float *state;           /* [n][total] */
+} sb_iir_plan;
+
+int sb_integrator(const sb_iir_plan *plan, const float *delta, float *out, void *stream);
+
+/* ------------------------------------------------------------------------
+ * DM — replaces specula/processing_objects/dm.py:72-86:
+ * phase[mask_idx[p]] = sum_m (sign * cmd[m]) * IF[m][p]; IF row-major
+ * (n_modes x n_valid) with row stride ld_if >= n_valid.  Pixels outside the
+ * mask are not written.
+ * ---------------------------------------------------------------------- */
+int sb_dm_project(const float *ifunc, int n_modes, int n_valid, int ld_if,
+                  const float *cmd, int n_cmd, float sign, const int32_t *mask_idx,
+                  float *phase, void *stream);
+
+/* ------------------------------------------------------------------------
+ * AtmoEvolution — replaces specula/processing_objects/atmo_evolution.py:
+ * 286-294: per layer, (1-f)*P[:, q:q+L] + f*P[:, q+1:q+1+L], rot90 by k,
+ * order-1 rotation by the fractional part of the wind direction in degrees
+ * (scipy.ndimage.rotate(reshape=False, order=1, mode='constant')), times
+ * the r0 scale.  One launch updates every layer.
+ * ---------------------------------------------------------------------- */
+#define SB_MAX_LAYERS 16
+typedef struct sb_atmo_layer {
+    const float *screen;    /* strip, rows = L, row stride screen_ld          */
+    int screen_ld;
+    int screen_cols;        /* strip width: positions cycle to 0 beyond it    */
+    double delta;           /* wind_speed * delta_time / pixel_pitch (float64) */
+    int rot90;              /* k in 0..3                                      */
+    int rotate;             /* nonzero: apply the fractional-degree rotation  */
+    double m00, m01, m10, m11, off0, off1;  /* scipy affine map (output->input) */
+    float scale;            /* (pitch / r0_lambda)^(5/6)                      */
+    float *out;             /* L x L, row-major                               */
+} sb_atmo_layer;
+
+/* positions: device float64[n_layers], the layers' last positions (pixels);
+ * the call advances them by `delta` (cycling to 0 when pos + L reaches the
+ * strip width, atmo_evolution.py:269-279) and then writes every layer. */
+int sb_atmo_evolve(const sb_atmo_layer *layers, int n_layers, int L, double *positions,
+                   void *stream);
+
+/* ------------------------------------------------------------------------
+ * AtmoPropagation, on-axis branch — replaces
+ * specula/processing_objects/atmo_propagation.py:105-125 with
+ * electric_field.py:35-43,77-82: reset, then A *= layer.A[crop],
+ * phase += layer.phase[crop] for each layer in order.
+ * ---------------------------------------------------------------------- */
+typedef struct sb_prop_layer {
+    const float *A;         /* NULL: all ones                                 */
+    const float *phase;     /* NULL: all zeros                                */
+    int ld;
+    int top, left;          /* crop offsets                                   */
+} sb_prop_layer;
+
+int sb_propagate_on_axis(const sb_prop_layer *layers, int n_layers, int pupil,
+                         float *A_out, float *phase_out, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPECULA_B200_H */

@@ -1,0 +1,110 @@
+"""ctypes binding of libspecula_b200.so (the C ABI in include/specula_b200.h).
+
+The library is built in-tree by ``specula_b200/csrc/build.py``.  There is no
+CPU fallback: if the library is missing or cannot be loaded, every GPU entry
+point raises ``RuntimeError`` naming the file it looked for.
+"""
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, 'libspecula_b200.so')
+
+SB_OK = 0
+STATUS_NAMES = {0: 'SB_OK', -1: 'SB_EINVAL', -2: 'SB_ESHAPE', -3: 'SB_ECUDA', -4: 'SB_ESCRATCH',
+                -5: 'SB_ETIMEOUT', -6: 'SB_EUNSUPPORTED'}
+SB_MAX_LAYERS = 16
+
+vp = C.c_void_p
+fp = C.c_void_p   # device float*
+ip = C.c_void_p   # device int32*
+
+
+class ShPlan(C.Structure):
+    _fields_ = [('n_lenses', C.c_int), ('np_sub', C.c_int), ('cutsize', C.c_int), ('subap_npx', C.c_int),
+                ('field_ld', C.c_int), ('phase_to_rad', C.c_float),
+                ('twiddle', fp), ('tilt', fp), ('fp_mask', fp), ('rebin', fp)]
+
+
+class CcdParams(C.Structure):
+    _fields_ = [('n_pixels', C.c_int), ('frames_per_read', C.c_int), ('rate', C.c_float), ('qe', C.c_float),
+                ('bg_plus_dark', C.c_float), ('photon_noise', C.c_int), ('readout_noise', C.c_int),
+                ('readout_level', C.c_float), ('adu_gain', C.c_float), ('adu_bias', C.c_float),
+                ('dark_level', C.c_float), ('dark_noise', C.c_int), ('photon_seed', C.c_uint64),
+                ('readout_seed', C.c_uint64), ('state', vp)]
+
+
+class SlopecPlan(C.Structure):
+    _fields_ = [('n_subaps', C.c_int), ('npx2', C.c_int), ('thr', C.c_float),
+                ('idxs', ip), ('xw', fp), ('yw', fp), ('mw', fp)]
+
+
+class IirPlan(C.Structure):
+    _fields_ = [('n', C.c_int), ('total', C.c_int), ('shift', C.c_int), ('k_out', C.c_int),
+                ('rem', C.c_float), ('one_minus_rem', C.c_float),
+                ('num', fp), ('den', fp), ('ist', fp), ('ost', fp), ('state', fp)]
+
+
+class AtmoLayer(C.Structure):
+    _fields_ = [('screen', fp), ('screen_ld', C.c_int), ('screen_cols', C.c_int), ('delta', C.c_double),
+                ('rot90', C.c_int), ('rotate', C.c_int),
+                ('m00', C.c_double), ('m01', C.c_double), ('m10', C.c_double), ('m11', C.c_double),
+                ('off0', C.c_double), ('off1', C.c_double), ('scale', C.c_float), ('out', fp)]
+
+
+class PropLayer(C.Structure):
+    _fields_ = [('A', fp), ('phase', fp), ('ld', C.c_int), ('top', C.c_int), ('left', C.c_int)]
+
+
+# name -> (restype, argtypes); every function of include/specula_b200.h
+SIGNATURES = {
+    'sb_version': (C.c_int, []),
+    'sb_last_error': (C.c_char_p, []),
+    'sb_sh_scratch_bytes': (C.c_size_t, [C.POINTER(ShPlan)]),
+    'sb_sh_forward': (C.c_int, [C.POINTER(ShPlan), fp, fp, fp, C.c_int, C.c_float, fp, vp, C.c_size_t, vp]),
+    'sb_edge_extrapolate': (C.c_int, [fp, ip, ip, C.c_int, fp, vp]),
+    'sb_interp2d_field': (C.c_int, [fp, fp, C.c_int, C.c_int, fp, fp, C.c_int, fp, fp, vp]),
+    'sb_ccd_step': (C.c_int, [C.POINTER(CcdParams), fp, fp, fp, vp]),
+    'sb_philox_raw': (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, vp, vp]),
+    'sb_slopec_scratch_bytes': (C.c_size_t, [C.POINTER(SlopecPlan)]),
+    'sb_slopec': (C.c_int, [C.POINTER(SlopecPlan), fp, fp, fp, vp, C.c_size_t, vp]),
+    'sb_modalrec': (C.c_int, [fp, C.c_int, C.c_int, C.c_int, fp, fp, vp]),
+    'sb_integrator': (C.c_int, [C.POINTER(IirPlan), fp, fp, vp]),
+    'sb_dm_project': (C.c_int, [fp, C.c_int, C.c_int, C.c_int, fp, C.c_int, C.c_float, ip, fp, vp]),
+    'sb_atmo_evolve': (C.c_int, [C.POINTER(AtmoLayer), C.c_int, C.c_int, vp, vp]),
+    'sb_propagate_on_axis': (C.c_int, [C.POINTER(PropLayer), C.c_int, C.c_int, fp, fp, vp]),
+}
+
+_lib = None
+
+
+def load():
+    """Load the library (once) and bind every exported symbol."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f'specula_b200 CUDA library not found at {LIB_PATH}; '
+                           'build it with `python specula_b200/csrc/build.py` (there is no CPU fallback)')
+    lib = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def call(name, *args):
+    """Call an entry point; raise RuntimeError with the library's message on failure."""
+    lib = load()
+    rc = getattr(lib, name)(*args)
+    if rc != SB_OK:
+        msg = lib.sb_last_error().decode(errors='replace')
+        raise RuntimeError(f'{name} failed with {STATUS_NAMES.get(rc, rc)}: {msg}')
+    return rc
+
+
+def ptr(t):
+    """Device address of a torch tensor (None -> NULL)."""
+    return None if t is None else t.data_ptr()

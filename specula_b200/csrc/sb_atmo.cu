@@ -1,0 +1,159 @@
+// Turbulence layer update and on-axis propagation on the B200.
+//
+// sb_atmo_evolve: one launch updates every layer; blockIdx.z selects the
+// layer.  Each output pixel is evaluated straight from the screen strip:
+// the column lerp (atmo_evolution.py:290), the rot90 index map (:291), the
+// order-1 fractional-degree rotation with scipy's 'constant' boundary (:293;
+// a sample outside [0, L-1] on either axis gives 0, otherwise bilinear from
+// the four neighbours, neighbours off the grid counting 0) and the r0 scale
+// (:294).  Float32 operations keep NumPy's order (no FMA contraction) and the
+// rotation coordinates and weights are computed in double like SciPy, so
+// results track the reference to the last bits.
+#include "sb_common.cuh"
+
+namespace {
+
+struct EvolveArgs {
+    sb_atmo_layer layer[SB_MAX_LAYERS];
+    int n, L;
+    double *pos;
+};
+
+// new = last + delta; cycle to 0 when new + L reaches the strip width;
+// float64 like the reference's NumPy arithmetic (atmo_evolution.py:269-277)
+__global__ void atmo_advance_kernel(EvolveArgs a) {
+    const int k = threadIdx.x;
+    if (k >= a.n) return;
+    double np = __dadd_rn(a.pos[k], a.layer[k].delta);
+    if (__dadd_rn(np, (double)a.L) >= (double)a.layer[k].screen_cols) np = 0.0;
+    a.pos[k] = np;
+}
+
+struct Window {
+    const float *row0;
+    int ld;
+    float frac;
+};
+
+// lerped strip value at (r, c) of the un-rotated layer (atmo_evolution.py:290)
+__device__ __forceinline__ float lerp_at(const Window &w, int r, int c) {
+    const float *row = w.row0 + (size_t)r * w.ld + c;
+    const float w0 = __fsub_rn(1.0f, w.frac);
+    return __fadd_rn(__fmul_rn(w0, row[0]), __fmul_rn(w.frac, row[1]));
+}
+
+// value of rot90(lerped, k) at (y, x)
+__device__ __forceinline__ float rot90_at(const Window &w, int k, int L, int y, int x) {
+    switch (k) {
+        case 1: return lerp_at(w, x, L - 1 - y);
+        case 2: return lerp_at(w, L - 1 - y, L - 1 - x);
+        case 3: return lerp_at(w, L - 1 - x, y);
+        default: return lerp_at(w, y, x);
+    }
+}
+
+__global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgs a) {
+    const sb_atmo_layer &ly = a.layer[blockIdx.z];
+    const int L = a.L;
+    // integer position and float32 remainder (atmo_evolution.py:278-279)
+    const double np = a.pos[blockIdx.z];
+    const double q = floor(np);
+    Window w;
+    w.row0 = ly.screen + (long long)q;
+    w.ld = ly.screen_ld;
+    w.frac = (float)(np - q);
+    const int k = ly.rot90;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= L || y >= L) return;
+    float v;
+    if (!ly.rotate) {
+        v = rot90_at(w, k, L, y, x);
+    } else {
+        const double ir = __dadd_rn(__dadd_rn(__dmul_rn(ly.m00, (double)y), __dmul_rn(ly.m01, (double)x)), ly.off0);
+        const double ic = __dadd_rn(__dadd_rn(__dmul_rn(ly.m10, (double)y), __dmul_rn(ly.m11, (double)x)), ly.off1);
+        if (!(ir >= 0.0 && ir <= (double)(L - 1) && ic >= 0.0 && ic <= (double)(L - 1))) {
+            v = 0.0f;
+        } else {
+            const int r0 = (int)floor(ir), c0 = (int)floor(ic);
+            const double fr = ir - r0, fc = ic - c0;
+            const int r1 = r0 + 1, c1 = c0 + 1;
+            const double q00 = rot90_at(w, k, L, r0, c0);
+            const double q01 = c1 < L ? (double)rot90_at(w, k, L, r0, c1) : 0.0;
+            const double q10 = r1 < L ? (double)rot90_at(w, k, L, r1, c0) : 0.0;
+            const double q11 = (r1 < L && c1 < L) ? (double)rot90_at(w, k, L, r1, c1) : 0.0;
+            v = (float)(q00 * (1 - fr) * (1 - fc) + q01 * (1 - fr) * fc + q10 * fr * (1 - fc) + q11 * fr * fc);
+        }
+    }
+    ly.out[(size_t)y * L + x] = __fmul_rn(v, ly.scale);
+}
+
+struct PropArgs {
+    sb_prop_layer layer[SB_MAX_LAYERS];
+    int n, pupil;
+};
+
+__global__ void __launch_bounds__(256) propagate_kernel(PropArgs a, float *__restrict__ A, float *__restrict__ P) {
+    const int n = a.pupil * a.pupil;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const int r = e / a.pupil, c = e - r * a.pupil;
+        float amp = 1.0f, ph = 0.0f;                       // ElectricField.reset()
+        for (int k = 0; k < a.n; ++k) {
+            const sb_prop_layer &l = a.layer[k];
+            const size_t g = (size_t)(r + l.top) * l.ld + (c + l.left);
+            if (l.A) amp = __fmul_rn(amp, l.A[g]);
+            if (l.phase) ph = __fadd_rn(ph, l.phase[g]);
+        }
+        A[e] = amp;
+        P[e] = ph;
+    }
+}
+
+}  // namespace
+
+extern "C" int sb_atmo_evolve(const sb_atmo_layer *layers, int n_layers, int L, double *positions, void *stream) {
+    sb::clear_error();
+    if (!layers || !positions || n_layers < 0 || L < 1) return sb::fail(SB_EINVAL, "sb_atmo_evolve: bad args");
+    if (n_layers > SB_MAX_LAYERS) return sb::fail(SB_ESHAPE, "sb_atmo_evolve: at most %d layers", SB_MAX_LAYERS);
+    if (n_layers == 0) return SB_OK;
+    EvolveArgs a;
+    for (int k = 0; k < n_layers; ++k) {
+        const sb_atmo_layer &l = layers[k];
+        // the window [pos, pos + L] must stay inside the strip for every
+        // position the cycling rule allows: pos + L < screen_cols
+        if (!l.screen || !l.out || l.screen_cols < L + 1 || l.screen_ld < l.screen_cols || l.rot90 < 0 ||
+            l.rot90 > 3 || !(l.delta >= 0.0))
+            return sb::fail(SB_EINVAL, "sb_atmo_evolve: layer %d: bad screen window", k);
+        a.layer[k] = l;
+    }
+    a.n = n_layers;
+    a.L = L;
+    a.pos = positions;
+    cudaStream_t st = sb::as_stream(stream);
+    atmo_advance_kernel<<<1, 32, 0, st>>>(a);
+    int rc = sb::check_launch("atmo_advance_kernel");
+    if (rc) return rc;
+    dim3 block(32, 8), grid((L + 31) / 32, (L + 7) / 8, n_layers);
+    atmo_evolve_kernel<<<grid, block, 0, st>>>(a);
+    return sb::check_launch("atmo_evolve_kernel");
+}
+
+extern "C" int sb_propagate_on_axis(const sb_prop_layer *layers, int n_layers, int pupil, float *A_out,
+                                    float *phase_out, void *stream) {
+    sb::clear_error();
+    if (!layers || !A_out || !phase_out || n_layers < 0 || pupil < 1)
+        return sb::fail(SB_EINVAL, "sb_propagate_on_axis: bad args");
+    if (n_layers > SB_MAX_LAYERS) return sb::fail(SB_ESHAPE, "sb_propagate_on_axis: at most %d layers", SB_MAX_LAYERS);
+    PropArgs a;
+    for (int k = 0; k < n_layers; ++k) {
+        if (layers[k].top < 0 || layers[k].left < 0 || layers[k].ld < pupil + layers[k].left)
+            return sb::fail(SB_EINVAL, "sb_propagate_on_axis: layer %d: bad crop", k);
+        a.layer[k] = layers[k];
+    }
+    a.n = n_layers;
+    a.pupil = pupil;
+    int nblk = (pupil * pupil + 255) / 256;
+    nblk = nblk > 1184 ? 1184 : nblk;
+    propagate_kernel<<<nblk, 256, 0, sb::as_stream(stream)>>>(a, A_out, phase_out);
+    return sb::check_launch("propagate_kernel");
+}

@@ -1,0 +1,189 @@
+// Reconstructor, integrator and DM projection on the B200.
+//
+// All three are HBM-streaming: the reconstructor reads R once per step
+// (n_modes x n_slopes), the DM projection reads the influence functions once
+// per step (n_modes x n_valid, the largest array of the loop).  Both kernels
+// issue 16-byte loads with several in flight per thread and reduce in a
+// fixed order, so results are bit-reproducible run to run.
+#include "sb_common.cuh"
+
+namespace {
+
+// modes[m] = sum_j R[m][j] * s[j]: one CTA per row (modalrec.py:159)
+template <bool VEC>
+__global__ void __launch_bounds__(256) gemv_rows_kernel(const float *__restrict__ R, int ncols, int ldr,
+                                                        const float *__restrict__ s, float *__restrict__ y) {
+    __shared__ float red[33];
+    const int m = blockIdx.x;
+    const float *row = R + (size_t)m * ldr;
+    float acc = 0.f;
+    if (VEC) {
+        const int n4 = ncols >> 2;
+        const float4 *r4 = reinterpret_cast<const float4 *>(row);
+        const float4 *s4 = reinterpret_cast<const float4 *>(s);
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+        for (int j = threadIdx.x; j < n4; j += blockDim.x) {
+            const float4 r = __ldg(r4 + j), v = __ldg(s4 + j);
+            a0 = fmaf(r.x, v.x, a0);
+            a1 = fmaf(r.y, v.y, a1);
+            a2 = fmaf(r.z, v.z, a2);
+            a3 = fmaf(r.w, v.w, a3);
+        }
+        acc = (a0 + a1) + (a2 + a3);
+        for (int j = (n4 << 2) + threadIdx.x; j < ncols; j += blockDim.x) acc = fmaf(row[j], s[j], acc);
+    } else {
+        for (int j = threadIdx.x; j < ncols; j += blockDim.x) acc = fmaf(row[j], s[j], acc);
+    }
+    acc = sb::block_sum(acc, red);
+    if (threadIdx.x == 0) y[m] = acc;
+}
+
+// 2-tap IIR per mode, operation order of iir_filter.py:100-211 (no FMA
+// contraction, so float32 results match the reference bit for bit)
+__global__ void integrator_kernel(sb_iir_plan p, const float *__restrict__ delta, float *__restrict__ out) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= p.n) return;
+    float *st = p.state + (size_t)e * p.total;
+    if (p.shift)
+        for (int k = p.total - 1; k >= 1; --k) st[k] = st[k - 1];
+    float *ist = p.ist + 2 * e, *ost = p.ost + 2 * e;
+    const float *num = p.num + 2 * e, *den = p.den + 2 * e;
+    ost[0] = ost[1];
+    ost[1] = 0.f;
+    ist[0] = ist[1];
+    ist[1] = 0.f;
+    ist[1] = delta[e];
+    const float factor = __fdiv_rn(1.0f, den[1]);
+    const float num_c = __fadd_rn(__fmul_rn(num[0], ist[0]), __fmul_rn(num[1], ist[1]));
+    const float den_c = __fmul_rn(den[0], ost[0]);
+    const float y = __fmul_rn(factor, __fsub_rn(num_c, den_c));
+    ost[1] = y;
+    st[0] = y;
+    float o;
+    if (p.rem == 0.f) {
+        o = st[p.k_out];
+    } else {
+        o = __fadd_rn(__fmul_rn(p.rem, st[p.k_out]), __fmul_rn(p.one_minus_rem, st[p.k_out - 1]));
+    }
+    out[e] = o;
+}
+
+// phase[idx[p]] = sum_m c[m] * IF[m][p]; CTA = 8 warps sharing a strip of
+// 32*W columns, warp w takes modes w, w+8, ...; partial strips are reduced
+// across warps in shared memory (fixed order).  W = 4 (float4) when the rows
+// are 16-byte aligned, else 1.
+template <int W>
+__global__ void __launch_bounds__(256) dm_project_kernel(const float *__restrict__ IF, int nmodes, int nvalid,
+                                                         int ld, const float *__restrict__ cmd, int ncmd, float sign,
+                                                         const int32_t *__restrict__ idx,
+                                                         float *__restrict__ phase) {
+    extern __shared__ float sm[];
+    float *c = sm;                     // nmodes
+    float *part = sm + nmodes;         // 8 warps x 32*W
+    for (int m = threadIdx.x; m < nmodes; m += blockDim.x) c[m] = m < ncmd ? sign * cmd[m] : 0.f;
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int col0 = blockIdx.x * 32 * W + lane * W;
+    float acc[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k) acc[k] = 0.f;
+    if (col0 < nvalid) {
+        if (W == 4 && col0 + 3 < nvalid) {
+            const float *base = IF + col0;
+            int m = warp;
+            for (; m + 24 < nmodes; m += 32) {
+                const float4 v0 = __ldg(reinterpret_cast<const float4 *>(base + (size_t)m * ld));
+                const float4 v1 = __ldg(reinterpret_cast<const float4 *>(base + (size_t)(m + 8) * ld));
+                const float4 v2 = __ldg(reinterpret_cast<const float4 *>(base + (size_t)(m + 16) * ld));
+                const float4 v3 = __ldg(reinterpret_cast<const float4 *>(base + (size_t)(m + 24) * ld));
+                const float c0 = c[m], c1 = c[m + 8], c2 = c[m + 16], c3 = c[m + 24];
+                acc[0] = fmaf(c0, v0.x, acc[0]); acc[1] = fmaf(c0, v0.y, acc[1]);
+                acc[2] = fmaf(c0, v0.z, acc[2]); acc[3] = fmaf(c0, v0.w, acc[3]);
+                acc[0] = fmaf(c1, v1.x, acc[0]); acc[1] = fmaf(c1, v1.y, acc[1]);
+                acc[2] = fmaf(c1, v1.z, acc[2]); acc[3] = fmaf(c1, v1.w, acc[3]);
+                acc[0] = fmaf(c2, v2.x, acc[0]); acc[1] = fmaf(c2, v2.y, acc[1]);
+                acc[2] = fmaf(c2, v2.z, acc[2]); acc[3] = fmaf(c2, v2.w, acc[3]);
+                acc[0] = fmaf(c3, v3.x, acc[0]); acc[1] = fmaf(c3, v3.y, acc[1]);
+                acc[2] = fmaf(c3, v3.z, acc[2]); acc[3] = fmaf(c3, v3.w, acc[3]);
+            }
+            for (; m < nmodes; m += 8) {
+                const float4 v = __ldg(reinterpret_cast<const float4 *>(base + (size_t)m * ld));
+                const float cm = c[m];
+                acc[0] = fmaf(cm, v.x, acc[0]); acc[1] = fmaf(cm, v.y, acc[1]);
+                acc[2] = fmaf(cm, v.z, acc[2]); acc[3] = fmaf(cm, v.w, acc[3]);
+            }
+        } else {
+            for (int m = warp; m < nmodes; m += 8) {
+                const float cm = c[m];
+#pragma unroll
+                for (int k = 0; k < W; ++k)
+                    if (col0 + k < nvalid) acc[k] = fmaf(cm, __ldg(IF + (size_t)m * ld + col0 + k), acc[k]);
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < W; ++k) part[warp * 32 * W + lane * W + k] = acc[k];
+    __syncthreads();
+    for (int t = threadIdx.x; t < 32 * W; t += blockDim.x) {
+        const int col = blockIdx.x * 32 * W + t;
+        if (col < nvalid) {
+            float s = 0.f;
+#pragma unroll
+            for (int w = 0; w < 8; ++w) s += part[w * 32 * W + t];
+            phase[idx[col]] = s;
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" int sb_modalrec(const float *R, int n_modes, int n_slopes, int ldr, const float *slopes, float *modes,
+                           void *stream) {
+    sb::clear_error();
+    if (!R || !slopes || !modes || n_modes < 0 || n_slopes < 0 || ldr < n_slopes)
+        return sb::fail(SB_EINVAL, "sb_modalrec: bad args");
+    if (n_modes == 0) return SB_OK;
+    cudaStream_t st = sb::as_stream(stream);
+    const bool vec = (ldr % 4 == 0) && ((uintptr_t)R % 16 == 0) && ((uintptr_t)slopes % 16 == 0);
+    if (vec)
+        gemv_rows_kernel<true><<<n_modes, 256, 0, st>>>(R, n_slopes, ldr, slopes, modes);
+    else
+        gemv_rows_kernel<false><<<n_modes, 256, 0, st>>>(R, n_slopes, ldr, slopes, modes);
+    return sb::check_launch("gemv_rows_kernel");
+}
+
+extern "C" int sb_integrator(const sb_iir_plan *p, const float *delta, float *out, void *stream) {
+    sb::clear_error();
+    if (!p || !delta || !out || !p->num || !p->den || !p->ist || !p->ost || !p->state)
+        return sb::fail(SB_EINVAL, "sb_integrator: null pointer");
+    if (p->n < 0 || p->total < 1 || p->k_out < 0 || p->k_out >= p->total || (p->rem != 0.f && p->k_out < 1))
+        return sb::fail(SB_EINVAL, "sb_integrator: bad state layout");
+    if (p->n == 0) return SB_OK;
+    integrator_kernel<<<(p->n + 127) / 128, 128, 0, sb::as_stream(stream)>>>(*p, delta, out);
+    return sb::check_launch("integrator_kernel");
+}
+
+extern "C" int sb_dm_project(const float *ifunc, int n_modes, int n_valid, int ld_if, const float *cmd, int n_cmd,
+                             float sign, const int32_t *mask_idx, float *phase, void *stream) {
+    sb::clear_error();
+    if (!ifunc || !cmd || !mask_idx || !phase || n_modes < 1 || n_valid < 0 || ld_if < n_valid || n_cmd < 0)
+        return sb::fail(SB_EINVAL, "sb_dm_project: bad args");
+    if (n_cmd > n_modes) return sb::fail(SB_ESHAPE, "sb_dm_project: %d commands for %d modes", n_cmd, n_modes);
+    if (n_valid == 0) return SB_OK;
+    cudaStream_t st = sb::as_stream(stream);
+    const bool vec = (ld_if % 4 == 0) && ((uintptr_t)ifunc % 16 == 0);
+    const int W = vec ? 4 : 1;
+    const size_t smem = (size_t)(n_modes + 8 * 32 * W) * sizeof(float);
+    if (smem > 200 * 1024) return sb::fail(SB_ESHAPE, "sb_dm_project: too many modes (%d)", n_modes);
+    const int nblk = (n_valid + 32 * W - 1) / (32 * W);
+    if (vec) {
+        if (smem > 48 * 1024)
+            cudaFuncSetAttribute(dm_project_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        dm_project_kernel<4><<<nblk, 256, smem, st>>>(ifunc, n_modes, n_valid, ld_if, cmd, n_cmd, sign, mask_idx, phase);
+    } else {
+        if (smem > 48 * 1024)
+            cudaFuncSetAttribute(dm_project_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        dm_project_kernel<1><<<nblk, 256, smem, st>>>(ifunc, n_modes, n_valid, ld_if, cmd, n_cmd, sign, mask_idx, phase);
+    }
+    return sb::check_launch("dm_project_kernel");
+}

@@ -1,0 +1,267 @@
+// CCD detector and Shack-Hartmann slope computer on the B200.
+//
+// CCD (ccd.py:198-287): one thread per pixel integrates the intensity and,
+// on read-out steps, applies QE, background/dark, Poisson photon noise,
+// Gaussian read-out noise and the ADU quantisation.  Random numbers come
+// from Philox4x32-10 (Salmon, Moraes, Dror & Shaw, SC'11), a counter-based
+// generator: the draw of pixel e in frame f is a pure function of
+// (seed, f, e, draw), so results do not depend on the launch shape.
+// Poisson sampling: sequential-search inversion below mean 10, Hormann's
+// PTRS transformed rejection (1993) above.
+//
+// ShSlopec (sh_slopec.py:308-438): one warp per valid sub-aperture gathers
+// its pixels through the index table and reduces flux, denominator and the
+// two weighted sums; a second kernel applies the 1e-3*mean cut-off that
+// needs the mean over all sub-apertures, in a fixed order.
+#include "sb_common.cuh"
+
+namespace {
+
+struct u4 {
+    uint32_t x, y, z, w;
+};
+
+__host__ __device__ __forceinline__ void mulhilo(uint32_t a, uint32_t b, uint32_t &hi, uint32_t &lo) {
+    const uint64_t p = (uint64_t)a * (uint64_t)b;
+    hi = (uint32_t)(p >> 32);
+    lo = (uint32_t)p;
+}
+
+// Philox4x32 with 10 rounds; multipliers and Weyl key increments as published.
+__host__ __device__ __forceinline__ u4 philox4x32_10(u4 c, uint32_t k0, uint32_t k1) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        uint32_t hi0, lo0, hi1, lo1;
+        mulhilo(M0, c.x, hi0, lo0);
+        mulhilo(M1, c.z, hi1, lo1);
+        u4 n;
+        n.x = hi1 ^ c.y ^ k0;
+        n.y = lo1;
+        n.z = hi0 ^ c.w ^ k1;
+        n.w = lo0;
+        c = n;
+        k0 += W0;
+        k1 += W1;
+    }
+    return c;
+}
+
+// uniform in (0,1) with 53 random bits from two words
+__device__ __forceinline__ double u01(uint32_t a, uint32_t b) {
+    const uint64_t m = ((uint64_t)(a >> 5) << 26) | (uint64_t)(b >> 6);  // 27 + 26 bits
+    return ((double)m + 0.5) * (1.0 / 9007199254740992.0);
+}
+
+constexpr uint32_t kPhotonTag = 0x50484f54u;   // "PHOT"
+constexpr uint32_t kReadoutTag = 0x52454144u;  // "READ"
+
+__device__ double poisson_sample(double lam, uint32_t e, uint64_t frame, uint64_t seed) {
+    if (!(lam > 0.0)) return 0.0;
+    const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32) ^ kPhotonTag;
+    if (lam < 10.0) {
+        // inversion by sequential search: smallest k with CDF(k) >= u
+        const u4 r = philox4x32_10({e, (uint32_t)frame, (uint32_t)(frame >> 32), 0u}, k0, k1);
+        const double u = u01(r.x, r.y);
+        double pk = exp(-lam), cdf = pk;
+        int k = 0;
+        while (u > cdf && k < 200) {
+            ++k;
+            pk *= lam / k;
+            cdf += pk;
+        }
+        return (double)k;
+    }
+    // PTRS (Hormann 1993): transformed rejection with squeeze
+    const double slam = sqrt(lam), loglam = log(lam);
+    const double b = 0.931 + 2.53 * slam;
+    const double a = -0.059 + 0.02483 * b;
+    const double inv_alpha = 1.1239 + 1.1328 / (b - 3.4);
+    const double vr = 0.9277 - 3.6224 / (b - 2.0);
+    for (uint32_t it = 0; it < 64; ++it) {
+        const u4 r = philox4x32_10({e, (uint32_t)frame, (uint32_t)(frame >> 32), 1u + it}, k0, k1);
+        const double U = u01(r.x, r.y) - 0.5;
+        const double V = u01(r.z, r.w);
+        const double us = 0.5 - fabs(U);
+        const double k = floor((2.0 * a / us + b) * U + lam + 0.43);
+        if (us >= 0.07 && V <= vr) return k;
+        if (k < 0.0 || (us < 0.013 && V > us)) continue;
+        if (log(V) + log(inv_alpha) - log(a / (us * us) + b) <= -lam + k * loglam - lgamma(k + 1.0)) return k;
+    }
+    return floor(lam + 0.5);  // unreachable in practice (acceptance > 0.9 per try)
+}
+
+__device__ __forceinline__ double std_normal(uint32_t e, uint64_t frame, uint64_t seed) {
+    const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32) ^ kReadoutTag;
+    const u4 r = philox4x32_10({e, (uint32_t)frame, (uint32_t)(frame >> 32), 0u}, k0, k1);
+    const double u1 = u01(r.x, r.y), u2 = u01(r.z, r.w);
+    return sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);   // Box-Muller
+}
+
+__global__ void __launch_bounds__(256) ccd_kernel(sb_ccd_params p, const float *__restrict__ in,
+                                                  float *__restrict__ integ, float *__restrict__ pix) {
+    // frame bookkeeping lives on the device; every block reads it before the
+    // last block to finish advances it (see the end of the kernel)
+    volatile sb_ccd_state *vs = p.state;
+    const uint64_t frame = vs->frame_index;
+    const int nint = vs->n_integrated + 1;
+    const bool readout = nint >= p.frames_per_read;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < p.n_pixels; e += gridDim.x * blockDim.x) {
+        // integrated_i += i * (loop_dt * bandw)   (ccd.py:205)
+        float acc = __fadd_rn(integ[e], __fmul_rn(in[e], p.rate));
+        if (!readout) {
+            integ[e] = acc;
+            continue;
+        }
+        float f = acc;
+        if (p.qe != 1.0f) f = __fmul_rn(f, p.qe);                  // ccd.py:282-287
+        f = __fadd_rn(f, p.bg_plus_dark);                           // ccd.py:220-221
+        float outv;
+        if (p.photon_noise) {
+            double v = poisson_sample((double)f, (uint32_t)e, frame, p.photon_seed);
+            if (p.readout_noise) v += trunc(std_normal((uint32_t)e, frame, p.readout_seed) * p.readout_level);
+            // ADU: round(x*g)+bias, clamp at 0, -bias, /g, back to the
+            // integer dtype of the Poisson draw (ccd.py:247-258)
+            double x = rint(v * (double)p.adu_gain) + (double)p.adu_bias;
+            x = x < 0.0 ? 0.0 : x;
+            x -= (double)p.adu_bias;
+            x = trunc(x / (double)p.adu_gain);
+            if (p.dark_noise) x -= (double)p.dark_level;
+            outv = (float)x;
+        } else {
+            if (p.readout_noise)
+                f = __fadd_rn(f, (float)(std_normal((uint32_t)e, frame, p.readout_seed) * p.readout_level));
+            outv = f;
+        }
+        pix[e] = outv;
+        integ[e] = 0.0f;                                            // ccd.py:216
+    }
+    // the last block to finish advances the frame state
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned int prev = atomicAdd(&p.state->blocks_done, 1u);
+        last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        vs->n_integrated = readout ? 0 : nint;
+        if (readout) vs->frame_index = frame + 1;
+        vs->blocks_done = 0u;
+        __threadfence();
+    }
+}
+
+__global__ void philox_raw_kernel(uint32_t k0, uint32_t k1, uint32_t c1, uint32_t c2, uint32_t c3, int n,
+                                  uint32_t *out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const u4 r = philox4x32_10({(uint32_t)i, c1, c2, c3}, k0, k1);
+        out[4 * i + 0] = r.x;
+        out[4 * i + 1] = r.y;
+        out[4 * i + 2] = r.z;
+        out[4 * i + 3] = r.w;
+    }
+}
+
+__global__ void __launch_bounds__(256) slopec_sums_kernel(sb_slopec_plan pl, const float *__restrict__ pix,
+                                                          float *__restrict__ flux, float *__restrict__ tot,
+                                                          float *__restrict__ sxn, float *__restrict__ syn) {
+    const int lane = threadIdx.x & 31;
+    const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (s >= pl.n_subaps) return;
+    const int32_t *ix = pl.idxs + (size_t)s * pl.npx2;
+    float f = 0.f, t = 0.f, x = 0.f, y = 0.f;
+    for (int e = lane; e < pl.npx2; e += 32) {
+        const float v = pix[ix[e]];
+        f += v;
+        float w = v - pl.thr;                 // pixels -= thr; clamp < 0 -> 0
+        w = w < 0.f ? 0.f : w;
+        t = fmaf(w, pl.mw[e], t);
+        x = fmaf(w, pl.xw[e], x);
+        y = fmaf(w, pl.yw[e], y);
+    }
+    f = sb::warp_sum(f);
+    t = sb::warp_sum(t);
+    x = sb::warp_sum(x);
+    y = sb::warp_sum(y);
+    if (lane == 0) {
+        flux[s] = f;
+        tot[s] = t;
+        sxn[s] = x;
+        syn[s] = y;
+    }
+}
+
+__global__ void __launch_bounds__(256) slopec_finish_kernel(int n, const float *__restrict__ tot,
+                                                            const float *__restrict__ sxn,
+                                                            const float *__restrict__ syn,
+                                                            float *__restrict__ slopes) {
+    __shared__ double red[33];
+    double acc = 0.0;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) acc += tot[e];
+    acc = sb::block_sum_all_d(acc, red);
+    const float mean = (float)(acc / n);
+    const float cut = 1.0f / (mean * 1e-3f);   // sh_slopec.py:393-400
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        float fac = 1.0f / tot[s];
+        fac = fac > cut ? 0.0f : fac;
+        slopes[s] = sxn[s] * fac;
+        slopes[n + s] = syn[s] * fac;
+    }
+}
+
+}  // namespace
+
+extern "C" int sb_ccd_step(const sb_ccd_params *p, const float *intensity, float *integrated, float *pixels,
+                           void *stream) {
+    sb::clear_error();
+    if (!p || !intensity || !integrated || !pixels || !p->state)
+        return sb::fail(SB_EINVAL, "sb_ccd_step: null pointer");
+    if (p->n_pixels < 0 || p->frames_per_read < 1) return sb::fail(SB_EINVAL, "sb_ccd_step: bad sizes");
+    if (p->photon_noise && !(p->adu_gain > 0.f)) return sb::fail(SB_EINVAL, "sb_ccd_step: ADU gain must be > 0");
+    int nblk = (p->n_pixels + 255) / 256;
+    nblk = nblk < 1 ? 1 : (nblk > 1184 ? 1184 : nblk);
+    ccd_kernel<<<nblk, 256, 0, sb::as_stream(stream)>>>(*p, intensity, integrated, pixels);
+    return sb::check_launch("ccd_kernel");
+}
+
+extern "C" int sb_philox_raw(uint32_t key0, uint32_t key1, uint32_t c1, uint32_t c2, uint32_t c3, int n_blocks,
+                             uint32_t *out, void *stream) {
+    sb::clear_error();
+    if (!out || n_blocks < 0) return sb::fail(SB_EINVAL, "sb_philox_raw: bad args");
+    if (n_blocks == 0) return SB_OK;
+    int nblk = (n_blocks + 255) / 256;
+    nblk = nblk > 1184 ? 1184 : nblk;
+    philox_raw_kernel<<<nblk, 256, 0, sb::as_stream(stream)>>>(key0, key1, c1, c2, c3, n_blocks, out);
+    return sb::check_launch("philox_raw_kernel");
+}
+
+extern "C" size_t sb_slopec_scratch_bytes(const sb_slopec_plan *pl) {
+    if (!pl || pl->n_subaps < 0) return 0;
+    return ((size_t)3 * pl->n_subaps * sizeof(float) + 255) & ~(size_t)255;
+}
+
+extern "C" int sb_slopec(const sb_slopec_plan *pl, const float *pixels, float *slopes, float *flux, void *scratch,
+                         size_t scratch_bytes, void *stream) {
+    sb::clear_error();
+    if (!pl || !pixels || !slopes || !flux || !pl->idxs || !pl->xw || !pl->yw || !pl->mw)
+        return sb::fail(SB_EINVAL, "sb_slopec: null pointer");
+    if (pl->n_subaps < 1 || pl->npx2 < 1) return sb::fail(SB_EINVAL, "sb_slopec: empty sub-aperture set");
+    const size_t need = sb_slopec_scratch_bytes(pl);
+    if (!scratch || scratch_bytes < need)
+        return sb::fail(SB_ESCRATCH, "sb_slopec: scratch needs %zu bytes, got %zu", need, scratch_bytes);
+    float *tot = static_cast<float *>(scratch);
+    float *sxn = tot + pl->n_subaps;
+    float *syn = sxn + pl->n_subaps;
+    cudaStream_t st = sb::as_stream(stream);
+    const int warps_per_block = 8;
+    const int nblk = (pl->n_subaps + warps_per_block - 1) / warps_per_block;
+    slopec_sums_kernel<<<nblk, 32 * warps_per_block, 0, st>>>(*pl, pixels, flux, tot, sxn, syn);
+    int rc = sb::check_launch("slopec_sums_kernel");
+    if (rc) return rc;
+    int nb2 = (pl->n_subaps + 255) / 256;
+    nb2 = nb2 > 148 ? 148 : nb2;
+    slopec_finish_kernel<<<nb2, 256, 0, st>>>(pl->n_subaps, tot, sxn, syn, slopes);
+    return sb::check_launch("slopec_finish_kernel");
+}

@@ -1,0 +1,310 @@
+// Shack-Hartmann forward model on the B200.
+//
+// One warp owns one sub-aperture; a CTA holds the sub-apertures of one chunk
+// of a lenslet row.  Per sub-aperture (all in shared memory):
+//   E[r][c]  = A * exp(i * k * phase) * tilt          (np x np, complex)
+//   G[r][b]  = sum_c E[r][c] * W[b][c]                 (np x cutsize)
+//   F[a][b]  = sum_r W[a][r] * G[r][b]                 (cutsize x cutsize)
+//   I[a][b]  = |F|^2 * field_stop[a][b]
+//   D[p][q]  = sum_ab R[p][a] R[q][b] I[a][b]           (subap_npx^2, LCM rebin)
+// W holds only the DFT rows that survive the fftshift + FoV cut, so the
+// zero-padded FFT of the reference (sh.py:376-405) is evaluated on exactly
+// the samples that reach the detector.  Row/column sums of D and of the
+// input amplitude go to per-CTA partials; a second kernel turns them into
+// the photon normalisation of sh.py:425-427 in a fixed (deterministic) order.
+#include "sb_common.cuh"
+
+namespace {
+
+struct ShArgs {
+    int n, p, cs, npx, ld, spc;
+    float k;
+    const float2 *tw;
+    const float2 *tilt;
+    const float *mask;
+    const float *rebin;
+    const float *A;
+    const float *ph;
+    const float *A_norm;
+    int n_norm;
+    float *out;
+    float *part_I;
+    float *part_A;
+};
+
+struct ShSmem {
+    int tw, tilt, mask, rebin, per_warp_E, per_warp_G, per_warp_I, per_warp_H, tables, per_warp;
+};
+
+__host__ __device__ inline ShSmem sh_smem_layout(int p, int cs, int npx) {
+    ShSmem s;
+    // float2 arrays first (8-byte aligned), then floats; offsets in bytes
+    s.tw = 0;
+    s.tilt = s.tw + cs * p * 8;
+    s.mask = s.tilt + p * p * 8;
+    s.rebin = s.mask + cs * cs * 4;
+    s.tables = ((s.rebin + npx * cs * 4) + 15) & ~15;
+    s.per_warp_E = 0;
+    s.per_warp_G = s.per_warp_E + p * p * 8;
+    s.per_warp_I = s.per_warp_G + p * cs * 8;
+    s.per_warp_H = s.per_warp_I + cs * cs * 4;
+    s.per_warp = ((s.per_warp_H + cs * npx * 4) + 15) & ~15;
+    return s;
+}
+
+__global__ void __launch_bounds__(256) sh_forward_kernel(ShArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const ShSmem L = sh_smem_layout(a.p, a.cs, a.npx);
+    float2 *tw = reinterpret_cast<float2 *>(smem + L.tw);
+    float2 *tilt = reinterpret_cast<float2 *>(smem + L.tilt);
+    float *mask = reinterpret_cast<float *>(smem + L.mask);
+    float *R = reinterpret_cast<float *>(smem + L.rebin);
+    __shared__ float red[33];
+
+    const int p = a.p, cs = a.cs, npx = a.npx;
+    for (int e = threadIdx.x; e < cs * p; e += blockDim.x) tw[e] = a.tw[e];
+    for (int e = threadIdx.x; e < p * p; e += blockDim.x) tilt[e] = a.tilt[e];
+    for (int e = threadIdx.x; e < cs * cs; e += blockDim.x) mask[e] = a.mask[e];
+    for (int e = threadIdx.x; e < npx * cs; e += blockDim.x) R[e] = a.rebin[e];
+    __syncthreads();
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.y;                       // lenslet row
+    const int j = blockIdx.x * a.spc + warp;        // lenslet column
+    unsigned char *wbase = smem + L.tables + warp * L.per_warp;
+    float2 *E = reinterpret_cast<float2 *>(wbase + L.per_warp_E);
+    float2 *G = reinterpret_cast<float2 *>(wbase + L.per_warp_G);
+    float *I = reinterpret_cast<float *>(wbase + L.per_warp_I);
+    float *H = reinterpret_cast<float *>(wbase + L.per_warp_H);
+
+    float local = 0.f;
+    if (j < a.n) {
+        // field build (electric_field.py:60-75 and sh.py:376)
+        const size_t row0 = (size_t)i * p;
+        const size_t col0 = (size_t)j * p;
+        for (int e = lane; e < p * p; e += 32) {
+            const int r = e / p, c = e - r * p;
+            const size_t g = (row0 + r) * (size_t)a.ld + col0 + c;
+            const float amp = a.A[g];
+            const float phi = a.ph[g] * a.k;
+            float s, co;
+            sincosf(phi, &s, &co);
+            const float re = co * amp, im = s * amp;
+            const float2 t = tilt[e];
+            E[e] = make_float2(re * t.x - im * t.y, re * t.y + im * t.x);
+        }
+        __syncwarp();
+        // DFT along columns, kept frequencies only
+        for (int e = lane; e < p * cs; e += 32) {
+            const int r = e / cs, b = e - r * cs;
+            float xr = 0.f, xi = 0.f;
+            const float2 *er = E + r * p;
+            const float2 *wb = tw + b * p;
+            for (int c = 0; c < p; ++c) {
+                const float2 u = er[c], w = wb[c];
+                xr = fmaf(u.x, w.x, fmaf(-u.y, w.y, xr));
+                xi = fmaf(u.x, w.y, fmaf(u.y, w.x, xi));
+            }
+            G[e] = make_float2(xr, xi);
+        }
+        __syncwarp();
+        // DFT along rows, |F|^2 and field stop (sh.py:378-399)
+        for (int e = lane; e < cs * cs; e += 32) {
+            const int aa = e / cs, b = e - aa * cs;
+            float xr = 0.f, xi = 0.f;
+            const float2 *wa = tw + aa * p;
+            for (int r = 0; r < p; ++r) {
+                const float2 u = G[r * cs + b], w = wa[r];
+                xr = fmaf(u.x, w.x, fmaf(-u.y, w.y, xr));
+                xi = fmaf(u.x, w.y, fmaf(u.y, w.x, xi));
+            }
+            I[e] = (xr * xr + xi * xi) * mask[e];
+        }
+        __syncwarp();
+        // LCM area rebin, separable (toccd.py:55-61)
+        for (int e = lane; e < cs * npx; e += 32) {
+            const int aa = e / npx, q = e - aa * npx;
+            float acc = 0.f;
+            const float *ia = I + aa * cs;
+            const float *rq = R + q * cs;
+            for (int b = 0; b < cs; ++b) acc = fmaf(ia[b], rq[b], acc);
+            H[e] = acc;
+        }
+        __syncwarp();
+        const int out_ld = a.n * npx;
+        for (int e = lane; e < npx * npx; e += 32) {
+            const int pp = e / npx, q = e - pp * npx;
+            float acc = 0.f;
+            const float *rp = R + pp * cs;
+            for (int aa = 0; aa < cs; ++aa) acc = fmaf(rp[aa], H[aa * npx + q], acc);
+            a.out[((size_t)i * npx + pp) * out_ld + (size_t)j * npx + q] = acc;
+            local += acc;
+        }
+    }
+    const int bid = blockIdx.y * gridDim.x + blockIdx.x;
+    const float tot = sb::block_sum(local, red);
+    // partial sum of the normalising amplitude: disjoint contiguous chunks
+    const int nblk = gridDim.x * gridDim.y;
+    const int chunk = (a.n_norm + nblk - 1) / nblk;
+    const int lo = bid * chunk;
+    const int hi = min(a.n_norm, lo + chunk);
+    float sa = 0.f;
+    for (int e = lo + threadIdx.x; e < hi; e += blockDim.x) sa += a.A_norm[e];
+    const float tota = sb::block_sum(sa, red);
+    if (threadIdx.x == 0) {
+        a.part_I[bid] = tot;
+        a.part_A[bid] = tota;
+    }
+}
+
+__global__ void __launch_bounds__(256) sh_normalize_kernel(const float *part_I, const float *part_A, int nparts,
+                                                           float photon_scale, float *out, int n_out) {
+    __shared__ double red[33];
+    double si = 0.0, sa = 0.0;
+    for (int e = threadIdx.x; e < nparts; e += blockDim.x) {
+        si += part_I[e];
+        sa += part_A[e];
+    }
+    si = sb::block_sum_all_d(si, red);
+    sa = sb::block_sum_all_d(sa, red);
+    // phot = S0 * pitch^2 * sum(A); i *= phot / sum(i)  (sh.py:426-427)
+    const float phot = (float)(photon_scale * sa);
+    const float scale = phot / (float)si;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_out; e += gridDim.x * blockDim.x) out[e] *= scale;
+}
+
+__global__ void edge_extrapolate_kernel(const float *ph, const int32_t *s1, const int32_t *s2, int n, float *out) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const int a1 = s1[e];
+        float v;
+        if (a1 < 0) {
+            v = ph[e];
+        } else {
+            const int a2 = s2[e];
+            v = a2 < 0 ? ph[a1] : 2.0f * ph[a1] - ph[a2];
+        }
+        out[e] = v;
+    }
+}
+
+__global__ void interp2d_field_kernel(const float *A, const float *P, int rows, int cols, const float *yy,
+                                      const float *xx, int n_out, float *Ao, float *Po) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_out; e += gridDim.x * blockDim.x) {
+        // bilinear on the integer grid in double precision, like SciPy's
+        // RegularGridInterpolator on the reference CPU path (interp2d.py:117-122)
+        const double y = yy[e], x = xx[e];
+        int y0 = (int)floor(y), x0 = (int)floor(x);
+        y0 = max(0, min(y0, rows - 2));
+        x0 = max(0, min(x0, cols - 2));
+        const double fy = y - y0, fx = x - x0;
+        const size_t i00 = (size_t)y0 * cols + x0;
+        const double w00 = (1 - fy) * (1 - fx), w01 = (1 - fy) * fx, w10 = fy * (1 - fx), w11 = fy * fx;
+        Ao[e] = (float)(A[i00] * w00 + A[i00 + 1] * w01 + A[i00 + cols] * w10 + A[i00 + cols + 1] * w11);
+        Po[e] = (float)(P[i00] * w00 + P[i00 + 1] * w01 + P[i00 + cols] * w10 + P[i00 + cols + 1] * w11);
+    }
+}
+
+int sh_grid(const sb_sh_plan *pl, int *spc, dim3 *grid, size_t *smem) {
+    const ShSmem L = sh_smem_layout(pl->np_sub, pl->cutsize, pl->subap_npx);
+    const int budget = 200 * 1024;
+    if (L.tables + L.per_warp > budget) return -1;
+    int s = (budget - L.tables) / L.per_warp;
+    s = s > 8 ? 8 : s;
+    if (s > pl->n_lenses) s = pl->n_lenses;
+    *spc = s;
+    *grid = dim3((pl->n_lenses + s - 1) / s, pl->n_lenses, 1);
+    *smem = (size_t)L.tables + (size_t)s * L.per_warp;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" size_t sb_sh_scratch_bytes(const sb_sh_plan *pl) {
+    if (!pl) return 0;
+    int spc;
+    dim3 grid;
+    size_t smem;
+    if (sh_grid(pl, &spc, &grid, &smem)) return 0;
+    const size_t nb = (size_t)grid.x * grid.y;
+    return ((2 * nb * sizeof(float)) + 255) & ~(size_t)255;
+}
+
+extern "C" int sb_sh_forward(const sb_sh_plan *pl, const float *A, const float *phase_nm, const float *A_norm,
+                             int n_norm, float photon_scale, float *intensity, void *scratch,
+                             size_t scratch_bytes, void *stream) {
+    sb::clear_error();
+    if (!pl || !A || !phase_nm || !A_norm || !intensity || !pl->twiddle || !pl->tilt || !pl->fp_mask ||
+        !pl->rebin)
+        return sb::fail(SB_EINVAL, "sb_sh_forward: null pointer");
+    if (pl->n_lenses < 1 || pl->np_sub < 1 || pl->cutsize < 1 || pl->subap_npx < 1 || n_norm < 0 ||
+        pl->field_ld < pl->n_lenses * pl->np_sub)
+        return sb::fail(SB_EINVAL, "sb_sh_forward: bad geometry");
+    int spc;
+    dim3 grid;
+    size_t smem;
+    if (sh_grid(pl, &spc, &grid, &smem))
+        return sb::fail(SB_ESHAPE, "sb_sh_forward: sub-aperture (np=%d, cut=%d, npx=%d) does not fit in shared memory",
+                        pl->np_sub, pl->cutsize, pl->subap_npx);
+    const size_t need = sb_sh_scratch_bytes(pl);
+    if (!scratch || scratch_bytes < need)
+        return sb::fail(SB_ESCRATCH, "sb_sh_forward: scratch needs %zu bytes, got %zu", need, scratch_bytes);
+    const int nb = grid.x * grid.y;
+    ShArgs a;
+    a.n = pl->n_lenses;
+    a.p = pl->np_sub;
+    a.cs = pl->cutsize;
+    a.npx = pl->subap_npx;
+    a.ld = pl->field_ld;
+    a.spc = spc;
+    a.k = pl->phase_to_rad;
+    a.tw = reinterpret_cast<const float2 *>(pl->twiddle);
+    a.tilt = reinterpret_cast<const float2 *>(pl->tilt);
+    a.mask = pl->fp_mask;
+    a.rebin = pl->rebin;
+    a.A = A;
+    a.ph = phase_nm;
+    a.A_norm = A_norm;
+    a.n_norm = n_norm;
+    a.out = intensity;
+    a.part_I = static_cast<float *>(scratch);
+    a.part_A = static_cast<float *>(scratch) + nb;
+    cudaStream_t st = sb::as_stream(stream);
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(sh_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return sb::fail(SB_ECUDA, "sb_sh_forward: smem attribute: %s", cudaGetErrorString(e));
+    }
+    sh_forward_kernel<<<grid, 32 * spc, smem, st>>>(a);
+    int rc = sb::check_launch("sh_forward_kernel");
+    if (rc) return rc;
+    const int n_out = pl->n_lenses * pl->subap_npx * pl->n_lenses * pl->subap_npx;
+    int nblk = (n_out + 255) / 256;
+    nblk = nblk > 592 ? 592 : nblk;
+    sh_normalize_kernel<<<nblk, 256, 0, st>>>(a.part_I, a.part_A, nb, photon_scale, intensity, n_out);
+    return sb::check_launch("sh_normalize_kernel");
+}
+
+extern "C" int sb_edge_extrapolate(const float *phase, const int32_t *src1, const int32_t *src2, int n_pixels,
+                                   float *out, void *stream) {
+    sb::clear_error();
+    if (!phase || !src1 || !src2 || !out || n_pixels < 0) return sb::fail(SB_EINVAL, "sb_edge_extrapolate: bad args");
+    if (n_pixels == 0) return SB_OK;
+    int nblk = (n_pixels + 255) / 256;
+    nblk = nblk > 1184 ? 1184 : nblk;
+    edge_extrapolate_kernel<<<nblk, 256, 0, sb::as_stream(stream)>>>(phase, src1, src2, n_pixels, out);
+    return sb::check_launch("edge_extrapolate_kernel");
+}
+
+extern "C" int sb_interp2d_field(const float *A_in, const float *phase_in, int in_rows, int in_cols,
+                                 const float *yy, const float *xx, int n_out, float *A_out, float *phase_out,
+                                 void *stream) {
+    sb::clear_error();
+    if (!A_in || !phase_in || !yy || !xx || !A_out || !phase_out || n_out < 0)
+        return sb::fail(SB_EINVAL, "sb_interp2d_field: bad args");
+    if (in_rows < 2 || in_cols < 2) return sb::fail(SB_ESHAPE, "sb_interp2d_field: input must be at least 2x2");
+    if (n_out == 0) return SB_OK;
+    int nblk = (n_out + 255) / 256;
+    nblk = nblk > 1184 ? 1184 : nblk;
+    interp2d_field_kernel<<<nblk, 256, 0, sb::as_stream(stream)>>>(A_in, phase_in, in_rows, in_cols, yy, xx, n_out,
+                                                                    A_out, phase_out);
+    return sb::check_launch("interp2d_field_kernel");
+}

@@ -1,0 +1,190 @@
+"""Turbulence evolution on the B200 (mirrors
+specula/processing_objects/atmo_evolution.py:14-323).
+
+Screens are synthesised once at construction (float64 on the device,
+specula_b200.lib.phasescreen) and cut into per-layer strips exactly as
+atmo_evolution.py:164-226 does (sqrt(Cn2), de-mean, nm, odd layers
+flipped), then stored in float32.  Each step is one sb_atmo_evolve call:
+the layer positions live on the device in float64 and are advanced by
+wind_speed * dt / pitch with the reference's cycling rule, then every layer
+gets the column lerp, rot90, fractional-degree rotation and r0 scaling.
+"""
+import math
+
+import numpy as np
+import torch
+
+from specula_b200 import ASEC2RAD, _lib, cpuArray
+from specula_b200.base_processing_obj import BaseProcessingObj
+from specula_b200.base_value import BaseValue
+from specula_b200.connections import InputValue
+from specula_b200.data_objects.layer import Layer
+from specula_b200.lib.phasescreen import calc_phasescreen
+
+
+def _cosdg_sindg(angle):
+    """cos/sin of an angle in degrees, exact at multiples of 90 (scipy.special.cosdg/sindg)."""
+    from scipy.special import cosdg, sindg
+    return float(cosdg(angle)), float(sindg(angle))
+
+
+class AtmoEvolution(BaseProcessingObj):
+    def __init__(self, simul_params, L0: list, heights: list, Cn2: list, data_dir: str,
+                 wavelengthInNm: float = 500.0, fov: float = 0.0, pixel_phasescreens: int = 8192, seed: int = 1,
+                 verbose: bool = False, user_defined_phasescreen: str = '', make_cycle: bool = False,
+                 fov_in_m: float = None, pupil_position: list = (0, 0), target_device_idx: int = None,
+                 precision: int = None):
+        super().__init__(target_device_idx=target_device_idx, precision=precision)
+        if make_cycle:
+            raise NotImplementedError('make_cycle is not implemented')
+        if user_defined_phasescreen:
+            raise NotImplementedError('AtmoEvolution: user-defined screen files are not read by specula_b200; '
+                                      'assign .phasescreens instead')
+        npdt = np.float32 if self.precision == 1 else np.float64
+        self.simul_params = simul_params
+        self.pixel_pupil = simul_params.pixel_pupil
+        self.pixel_pitch = simul_params.pixel_pitch
+        self.zenithAngleInDeg = simul_params.zenithAngleInDeg
+        self.n_phasescreens = len(heights)
+        self.airmass = 1.0 / np.cos(np.radians(self.zenithAngleInDeg or 0.0), dtype=npdt)
+        heights = np.array(heights, dtype=npdt)
+        fov_rad = fov * ASEC2RAD
+        self.pixel_layer = np.ceil((self.pixel_pupil + 2 * np.sqrt(np.sum(np.array(pupil_position, dtype=npdt) * 2))
+                                    / self.pixel_pitch + abs(heights) / self.pixel_pitch * fov_rad) / 2.0) * 2.0
+        if fov_in_m is not None:
+            self.pixel_layer = np.full_like(heights, int(fov_in_m / self.pixel_pitch / 2.0) * 2)
+        self.L0 = L0
+        self.heights = heights
+        self.Cn2 = np.array(Cn2, dtype=npdt)
+        self.data_dir = data_dir
+        self.wavelengthInNm = wavelengthInNm
+        self.pixel_square_phasescreens = pixel_phasescreens
+        if self.pixel_square_phasescreens < max(self.pixel_layer):
+            raise ValueError('Error: phase-screens dimension must be greater than layer dimension!')
+        if len(set(int(x) for x in self.pixel_layer)) != 1:
+            raise NotImplementedError('AtmoEvolution: layers of different sizes are not on the specula_b200 path')
+        if not np.isclose(np.sum(self.Cn2), 1.0, atol=1e-6):
+            raise ValueError(f' Cn2 total must be 1. Instead is: {np.sum(self.Cn2)}.')
+        if seed <= 0:
+            raise ValueError('seed must be >0')
+        self.verbose = verbose
+        L = int(self.pixel_layer[0])
+        self.layer_list = [Layer(L, L, self.pixel_pitch, float(h), precision=self.precision,
+                                 target_device_idx=self.target_device_idx) for h in heights]
+        for layer in self.layer_list:
+            layer._unit_amplitude = True      # amplitude stays 1 (atmo_evolution.py never changes it)
+        self.outputs['layer_list'] = self.layer_list
+        self.inputs['seeing'] = InputValue(type=BaseValue)
+        self.inputs['wind_speed'] = InputValue(type=BaseValue)
+        self.inputs['wind_direction'] = InputValue(type=BaseValue)
+        self.last_t = 0
+        self.extra_delta_time = 0
+        self.delta_time = 1
+        self._seed = seed
+        self.compute()
+
+    @property
+    def seed(self):
+        return self._seed
+
+    @seed.setter
+    def seed(self, value):
+        self._seed = value
+        self.compute()
+
+    def compute(self):
+        """Square screens -> per-layer strips (atmo_evolution.py:142-252)."""
+        L = int(self.pixel_layer[0])
+        if len(np.unique(np.atleast_1d(self.L0))) != 1:
+            raise NotImplementedError('AtmoEvolution: per-layer L0 is not on the specula_b200 path')
+        L0 = float(np.atleast_1d(self.L0)[0])
+        per_square = self.pixel_square_phasescreens // L
+        n_sq = int(math.ceil(self.n_phasescreens / per_square))
+        squares = [calc_phasescreen(L0, self.pixel_square_phasescreens, self.pixel_pitch, seed=self._seed + k,
+                                    device=self.device) for k in range(n_sq)]
+        strips = []
+        for i in range(self.n_phasescreens):
+            sq, k = divmod(i, per_square)
+            s = squares[sq][L * k:L * (k + 1), :].clone()
+            s *= float(np.sqrt(self.Cn2[i]))
+            s -= torch.mean(s)
+            s *= self.wavelengthInNm / (2 * np.pi)
+            if i % 2 != 0:
+                s = torch.flip(s, dims=(1,))
+            strips.append(s.to(self.dtype).contiguous())
+        del squares
+        self.phasescreens = strips
+        self.phasescreens_sizes = [s.shape[1] for s in strips]
+        self._positions = torch.zeros(self.n_phasescreens, dtype=torch.float64, device=self.device)
+
+    def set_last_position(self, last_position):
+        lp = np.broadcast_to(np.asarray(last_position, dtype=np.float64), (self.n_phasescreens,))
+        L = int(self.pixel_layer[0])
+        for p, s in zip(lp, self.phasescreens_sizes):
+            # the kernel reads columns [pos, pos + L]; keep the window inside the strip
+            if not (0 <= p < s - L):
+                raise ValueError(f'AtmoEvolution: position {p} outside [0, {s - L}) for a {s}-column strip')
+        self._positions.copy_(torch.as_tensor(np.array(lp)))
+
+    @property
+    def last_position(self):
+        return self._positions.detach().cpu().numpy()
+
+    def set_last_t(self, last_t):
+        self.last_t = last_t
+
+    def setup(self):
+        super().setup()
+        self._require_gpu_fp32()
+        for s in self.phasescreens:
+            if s.dtype != torch.float32 or s.device != self.device or not s.is_contiguous():
+                raise ValueError('AtmoEvolution: phase screens must be contiguous float32 on the device')
+
+    def prepare_trigger(self, t):
+        super().prepare_trigger(t)
+        self.delta_time = self.t_to_seconds(self.current_time - self.last_t) + self.extra_delta_time
+
+    def layer_params(self, delta_time):
+        """Per-layer kernel descriptors for this step (atmo_evolution.py:262-294)."""
+        seeing = float(cpuArray(self.local_inputs['seeing'].value))
+        ws = np.broadcast_to(np.asarray(cpuArray(self.local_inputs['wind_speed'].value), dtype=np.float64),
+                             (self.n_phasescreens,))
+        wd = np.broadcast_to(np.asarray(cpuArray(self.local_inputs['wind_direction'].value), dtype=np.float64),
+                             (self.n_phasescreens,))
+        r0 = 0.9759 * 0.5 / (seeing * 4.848) * self.airmass ** (-3. / 5.)
+        r0l = r0 * (self.wavelengthInNm / 500.0) ** (6. / 5.)
+        scale = (self.pixel_pitch / r0l) ** (5. / 6.)
+        delta = ws * delta_time / self.pixel_pitch
+        _, wdi = np.modf(wd / 90.0)
+        wdf_full, _ = np.modf(wd)
+        L = int(self.pixel_layer[0])
+        arr = (_lib.AtmoLayer * len(self.phasescreens))()
+        for k, (p, out) in enumerate(zip(self.phasescreens, self.layer_list)):
+            d = arr[k]
+            d.screen = p.data_ptr()
+            d.screen_ld = p.stride(0)
+            d.screen_cols = p.shape[1]
+            d.delta = float(delta[k])
+            d.rot90 = int(wdi[k]) % 4
+            d.rotate = int(wdf_full[k] != 0)
+            if d.rotate:
+                # scipy.ndimage.rotate(reshape=False): input = M @ output + offset
+                c, s = _cosdg_sindg(wdf_full[k])
+                ctr = (L - 1) / 2.0
+                d.m00, d.m01, d.m10, d.m11 = c, s, -s, c
+                d.off0 = ctr - (c * ctr + s * ctr)
+                d.off1 = ctr - (-s * ctr + c * ctr)
+            d.scale = float(scale)
+            d.out = out.phaseInNm.data_ptr()
+        return arr
+
+    def trigger_code(self):
+        arr = self.layer_params(self.delta_time)
+        L = int(self.pixel_layer[0])
+        _lib.call('sb_atmo_evolve', arr, len(self.phasescreens), L, self._positions.data_ptr(),
+                  self.stream_handle())
+
+    def post_trigger(self):
+        for layer in self.layer_list:
+            layer.generation_time = self.current_time
+        self.last_t = self.current_time

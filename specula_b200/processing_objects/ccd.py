@@ -1,0 +1,142 @@
+"""CCD detector on the B200 (mirrors specula/processing_objects/ccd.py:22-305).
+
+Same constructor, inputs (``in_i``) and outputs (``out_pixels``,
+``integrated_i``).  ``trigger_code()`` is one sb_ccd_step call: integrate the
+intensity, and on the steps that close a frame apply QE, background/dark,
+Poisson and read-out noise and the ADU quantisation (ccd.py:198-262).
+
+Noise uses Philox4x32-10 keyed by (photon_seed | readout_seed, frame,
+pixel) instead of NumPy's PCG64 / CuPy's XORWOW, so draws are deterministic
+and independent of launch shape; the reference's own CPU and GPU streams
+already differ from each other, so only the distributions are shared.  The
+frame counter lives on the device, so the object can be replayed from a CUDA
+graph.  Not on this path (raise NotImplementedError): excess (EMCCD), CIC and
+CTE noise, binning > 1, pixel gains, start_time > 0, 'auto' noise levels.
+"""
+import torch
+
+from specula_b200 import _lib
+from specula_b200.base_processing_obj import BaseProcessingObj
+from specula_b200.connections import InputValue
+from specula_b200.data_objects.intensity import Intensity
+from specula_b200.data_objects.pixels import Pixels
+
+
+class CCD(BaseProcessingObj):
+    def __init__(self,
+                 simul_params,
+                 size,
+                 dt: float,
+                 bandw: float,
+                 name: str = '',
+                 binning: int = 1,
+                 photon_noise: bool = False,
+                 readout_noise: bool = False,
+                 excess_noise: bool = False,
+                 darkcurrent_noise: bool = False,
+                 background_noise: bool = False,
+                 cic_noise: bool = False,
+                 cte_noise: bool = False,
+                 readout_level='',
+                 darkcurrent_level='',
+                 background_level='',
+                 cic_level: float = 0,
+                 cte_mat=None,
+                 quantum_eff: float = 1.0,
+                 pixelGains=None,
+                 photon_seed: int = 1,
+                 readout_seed: int = 2,
+                 excess_seed: int = 3,
+                 excess_delta: float = 1.0,
+                 start_time: int = 0,
+                 ADU_gain: int = 8,
+                 ADU_bias: int = 400,
+                 emccd_gain: int = 1,
+                 target_device_idx: int = None,
+                 precision: int = None):
+        super().__init__(target_device_idx=target_device_idx, precision=precision)
+        if dt <= 0:
+            raise ValueError(f'dt (integration time) is {dt} and must be greater than zero')
+        self.loop_dt = self.seconds_to_t(simul_params.time_step)
+        self._dt = self.seconds_to_t(dt)
+        if self._dt % self.loop_dt != 0:
+            raise ValueError(f'integration time dt={dt} must be a multiple of the basic simulation '
+                             f'time_step={simul_params.time_step}')
+        for flag, what in ((excess_noise, 'excess (EMCCD) noise'), (cic_noise, 'CIC noise'),
+                           (cte_noise, 'CTE noise'), (binning != 1, 'binning > 1'),
+                           (pixelGains is not None, 'pixel gains'), (start_time != 0, 'start_time > 0'),
+                           ('auto' in (readout_level, darkcurrent_level, background_level), "'auto' levels")):
+            if flag:
+                raise NotImplementedError(f'CCD: {what} is not on the specula_b200 path')
+        self._photon_noise = bool(photon_noise)
+        self._readout_noise = bool(readout_noise)
+        self._darkcurrent_noise = bool(darkcurrent_noise)
+        self._background_noise = bool(background_noise)
+        self._readout_level = float(readout_level) if readout_level != '' else 0.0
+        self._darkcurrent_level = float(darkcurrent_level) if darkcurrent_level != '' else 0.0
+        self._background_level = float(background_level) if background_level != '' else 0.0
+        self._qe = quantum_eff
+        self._binning = binning
+        self._bandw = bandw
+        self._ADU_gain = ADU_gain
+        self._ADU_bias = ADU_bias
+        self._photon_seed = int(photon_seed)
+        self._readout_seed = int(readout_seed)
+        self._pixels = Pixels(size[0] // binning, size[1] // binning, target_device_idx=target_device_idx,
+                              precision=precision)
+        self._integrated_i = Intensity(size[0], size[1], target_device_idx=target_device_idx, precision=precision)
+        self._frames_per_read = self._dt // self.loop_dt
+        self._n_integrated = 0
+        self.inputs['in_i'] = InputValue(type=Intensity)
+        self.outputs['out_pixels'] = self._pixels
+        self.outputs['integrated_i'] = self._integrated_i
+
+    @property
+    def dt(self):
+        return self._dt
+
+    @property
+    def size(self):
+        return self._pixels.size
+
+    @property
+    def bandw(self):
+        return self._bandw
+
+    def setup(self):
+        super().setup()
+        self._require_gpu_fp32()
+        in_i = self.inputs['in_i'].get(self.target_device_idx)
+        if in_i is None:
+            raise ValueError('Input intensity object has not been set')
+        if in_i.size != self._integrated_i.size:
+            raise ValueError(f'CCD: intensity {in_i.size} does not match detector {self._integrated_i.size}')
+        # sb_ccd_state: uint64 frame_index, int n_integrated, uint blocks_done
+        self._state = torch.zeros(2, dtype=torch.int64, device=self.device)
+        bg = self._background_level + self._darkcurrent_level \
+            if (self._background_noise or self._darkcurrent_noise) else 0.0
+        self._params = _lib.CcdParams(
+            n_pixels=self._integrated_i.i.numel(), frames_per_read=int(self._frames_per_read),
+            rate=float(self.t_to_seconds(self.loop_dt) * self._bandw), qe=float(self._qe), bg_plus_dark=float(bg),
+            photon_noise=int(self._photon_noise), readout_noise=int(self._readout_noise),
+            readout_level=self._readout_level, adu_gain=float(self._ADU_gain), adu_bias=float(self._ADU_bias),
+            dark_level=self._darkcurrent_level, dark_noise=int(self._darkcurrent_noise),
+            photon_seed=self._photon_seed, readout_seed=self._readout_seed, state=self._state.data_ptr())
+        self._in_i = in_i
+
+    def trigger_code(self):
+        _lib.call('sb_ccd_step', _byref(self._params), self._in_i.i.data_ptr(), self._integrated_i.i.data_ptr(),
+                  self._pixels.pixels.data_ptr(), self.stream_handle())
+
+    def post_trigger(self):
+        # host mirror of the device frame counter, for the time stamps
+        self._n_integrated += 1
+        if self._n_integrated >= self._frames_per_read:
+            self._n_integrated = 0
+            self._pixels.generation_time = self.current_time
+        self._integrated_i.generation_time = self.current_time
+
+
+def _byref(s):
+    import ctypes
+    return ctypes.byref(s)

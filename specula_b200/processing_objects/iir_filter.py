@@ -1,0 +1,72 @@
+"""IIR temporal filter on the B200 (mirrors specula/processing_objects/iir_filter.py:9-211)
+for 2-tap filters (integrators with forgetting factor).  One sb_integrator
+call per step performs the state shift of prepare_trigger, the filter update
+of trigger_code and the delayed output of post_trigger, with the reference's
+float32 operation order (bit-exact)."""
+import math
+
+import numpy as np
+import torch
+
+from specula_b200 import _lib
+from specula_b200.base_processing_obj import BaseProcessingObj
+from specula_b200.base_value import BaseValue
+from specula_b200.connections import InputValue
+
+
+class IirFilter(BaseProcessingObj):
+    def __init__(self, simul_params, iir_filter_data, delay: float = 0, integration: bool = True,
+                 offset: float = None, og_shaper: float = None, target_device_idx=None, precision=None):
+        if integration is False:
+            raise NotImplementedError('IirFilter: integration=False is not implemented yet')
+        if og_shaper is not None:
+            raise NotImplementedError('OG Shaper not implementd yet')
+        if offset is not None:
+            raise NotImplementedError('Offset not implemented yet')
+        super().__init__(target_device_idx=target_device_idx, precision=precision)
+        self.simul_params = simul_params
+        self.time_step = simul_params.time_step
+        self.iir_filter_data = iir_filter_data
+        if iir_filter_data.num_np.shape[1] != 2 or iir_filter_data.den_np.shape[1] != 2:
+            raise NotImplementedError('IirFilter: only 2-tap filters (integrators) are on the specula_b200 path')
+        self.delay = delay if delay is not None else 0
+        self._n = iir_filter_data.nfilter
+        self._total_length = int(np.ceil(self.delay)) + 1
+        self.state = torch.zeros((self._n, self._total_length), dtype=self.dtype, device=self.device)
+        self._ist = torch.zeros((self._n, 2), dtype=self.dtype, device=self.device)
+        self._ost = torch.zeros((self._n, 2), dtype=self.dtype, device=self.device)
+        self.out_comm = BaseValue(value=torch.zeros(self._n, dtype=self.dtype, device=self.device),
+                                  target_device_idx=target_device_idx)
+        self.inputs['delta_comm'] = InputValue(type=BaseValue)
+        self.outputs['out_comm'] = self.out_comm
+
+    @property
+    def last_state(self):
+        return self.state[:, 0]
+
+    def setup(self):
+        super().setup()
+        self._require_gpu_fp32()
+        rem = self.delay % 1
+        k_out = int(self.delay) if rem == 0 else int(math.ceil(self.delay))
+        self._num = self.iir_filter_data.num.to(self.device, torch.float32).contiguous()
+        self._den = self.iir_filter_data.den.to(self.device, torch.float32).contiguous()
+        self._plan = _lib.IirPlan(n=self._n, total=self._total_length, shift=int(self.delay > 0), k_out=k_out,
+                                  rem=float(np.float32(rem)), one_minus_rem=float(np.float32(1 - rem)),
+                                  num=self._num.data_ptr(), den=self._den.data_ptr(), ist=self._ist.data_ptr(),
+                                  ost=self._ost.data_ptr(), state=self.state.data_ptr())
+
+    def trigger_code(self):
+        d = self.local_inputs['delta_comm'].value
+        if not isinstance(d, torch.Tensor) or d.device != self.device or d.dtype != torch.float32:
+            d = torch.as_tensor(d, dtype=torch.float32, device=self.device)
+        _lib.call('sb_integrator', _byref(self._plan), d.contiguous().data_ptr(),
+                  self.out_comm.value.data_ptr(), self.stream_handle())
+
+    def post_trigger(self):
+        self.out_comm.generation_time = self.current_time
+
+
+def _byref(s):
+    import ctypes
+    return ctypes.byref(s)

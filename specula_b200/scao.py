@@ -1,0 +1,213 @@
+"""Assemble and run the single-conjugate Shack-Hartmann closed loop.
+
+``build_scao(cfg)`` wires the processing objects exactly as the reference's
+SCAO SH configuration does (main/scao/params_scao_sh.yml; trigger order of
+simul.py:109-135): AtmoEvolution -> AtmoPropagation (atmosphere + pupil stop
++ the DM layer of the previous step) -> SH -> CCD -> ShSlopec -> Modalrec ->
+Integrator -> DM.  ``ScaoLoop`` runs it either object by object through
+``LoopControl`` (the reference's scheduling) or as one CUDA graph holding
+every object's ``trigger_code`` for a step; all loop state (layer positions,
+CCD frame counter, integrator state, DM shape) lives on the device, so each
+graph replay is a full new step.
+"""
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from specula_b200.base_value import BaseValue
+from specula_b200.data_objects.ifunc import IFunc
+from specula_b200.data_objects.pupilstop import Pupilstop
+from specula_b200.data_objects.recmat import Recmat
+from specula_b200.data_objects.simul_params import SimulParams
+from specula_b200.data_objects.source import Source
+from specula_b200.data_objects.subap_data import SubapData
+from specula_b200.lib.make_mask import make_mask
+from specula_b200.loop_control import LoopControl
+from specula_b200.processing_objects.atmo_evolution import AtmoEvolution
+from specula_b200.processing_objects.atmo_propagation import AtmoPropagation
+from specula_b200.processing_objects.ccd import CCD
+from specula_b200.processing_objects.dm import DM
+from specula_b200.processing_objects.integrator import Integrator
+from specula_b200.processing_objects.modalrec import Modalrec
+from specula_b200.processing_objects.sh import SH
+from specula_b200.processing_objects.sh_slopec import ShSlopec
+
+RAD2ASEC = 180 * 3600 / math.pi
+
+
+@dataclass
+class ScaoConfig:
+    """Synthetic SCAO SH system; defaults are the 8 m / 20x20 system."""
+    pixel_pupil: int = 160
+    diameter_m: float = 8.0
+    obsratio: float = 0.14
+    n_lenses: int = 20
+    subap_npx: int = 8
+    wavelength_nm: float = 750.0
+    pxscale_over_lamd: float = 0.875       # detector pixel in lambda/d_sub
+    fov_ovs_coeff: float = 1.0
+    heights: list = field(default_factory=lambda: [0.0])
+    cn2: list = field(default_factory=lambda: [1.0])
+    wind_speed: list = field(default_factory=lambda: [10.0])
+    wind_direction: list = field(default_factory=lambda: [0.0])
+    r0: float = 0.15
+    L0: float = 25.0
+    pixel_phasescreens: int = 1024
+    screen_seed: int = 1
+    n_modes: int = 54
+    gain: float = 0.5
+    delay: float = 2
+    photons_per_subap: float = 1e3
+    readout_noise: float = 3.0
+    photon_noise: bool = True
+    time_step: float = 0.001
+    seed: int = 1234
+
+    @property
+    def pitch(self):
+        return self.diameter_m / self.pixel_pupil
+
+    @property
+    def seeing(self):
+        # r0 = 0.9759 * 0.5 / (seeing * 4.848) (atmo_evolution.py:265)
+        return 0.9759 * 0.5 / (self.r0 * 4.848)
+
+
+def elt_config(n_modes=500, layers=7, fft_pad=2, seed=1234):
+    """39 m / 640 px / 80x80 SH / 6 px, 7-layer atmosphere with random winds
+    5-30 m/s and random directions (seeded)."""
+    rng = np.random.default_rng(seed)
+    cn2 = [0.5, 0.15, 0.1, 0.1, 0.05, 0.05, 0.05][:layers]
+    cn2 = list(np.array(cn2) / np.sum(cn2))
+    heights = [0.0, 1000.0, 2000.0, 4000.0, 8000.0, 12000.0, 16000.0][:layers]
+    return ScaoConfig(pixel_pupil=640, diameter_m=39.0, n_lenses=80, subap_npx=6,
+                      pxscale_over_lamd=1.0 if fft_pad == 2 else 0.5, heights=heights, cn2=cn2,
+                      wind_speed=list(rng.uniform(5, 30, layers)), wind_direction=list(rng.uniform(0, 360, layers)),
+                      pixel_phasescreens=2048, n_modes=n_modes, seed=seed)
+
+
+class ScaoLoop:
+    def __init__(self, cfg: ScaoConfig, device_idx=0, ifunc=None, recmat=None):
+        self.cfg = cfg
+        dev = torch.device('cuda', device_idx)
+        self.device = dev
+        c = cfg
+        sp = SimulParams(pixel_pupil=c.pixel_pupil, pixel_pitch=c.pitch, time_step=c.time_step)
+        self.simul_params = sp
+        rng = np.random.default_rng(c.seed)
+        pupil = make_mask(c.pixel_pupil, c.obsratio, 1.0)
+        self.pupil = pupil
+        nv = int(pupil.sum())
+        d_sub = c.diameter_m / c.n_lenses
+        lamd = c.wavelength_nm * 1e-9 / d_sub * RAD2ASEC
+        pxs = c.pxscale_over_lamd * lamd
+        # photon flux: photons_per_subap per valid (fully lit) sub-aperture per frame
+        n_valid_est = max(1, int(round(pupil.sum() / (c.pixel_pupil / c.n_lenses) ** 2)))
+        phot_total = c.photons_per_subap * n_valid_est
+        S0 = phot_total / (pupil.sum() * c.pitch ** 2 * c.time_step * 1.0)
+
+        self.seeing = BaseValue(value=c.seeing, target_device_idx=device_idx)
+        self.wind_speed = BaseValue(value=np.array(c.wind_speed, dtype=float), target_device_idx=device_idx)
+        self.wind_direction = BaseValue(value=np.array(c.wind_direction, dtype=float), target_device_idx=device_idx)
+        self.atmo = AtmoEvolution(sp, L0=c.L0, heights=c.heights, Cn2=c.cn2, data_dir='',
+                                  pixel_phasescreens=c.pixel_phasescreens, seed=c.screen_seed,
+                                  target_device_idx=device_idx)
+        self.atmo.inputs['seeing'].set(self.seeing)
+        self.atmo.inputs['wind_speed'].set(self.wind_speed)
+        self.atmo.inputs['wind_direction'].set(self.wind_direction)
+        self.pupilstop = Pupilstop(sp, obs_diam=c.obsratio, target_device_idx=device_idx)
+        if ifunc is None:
+            g = torch.Generator(device=dev).manual_seed(c.seed)
+            ifunc = torch.randn((c.n_modes, nv), device=dev, generator=g) * 10.0
+        self.dm = DM(sp, 0, ifunc=IFunc(ifunc=ifunc, mask=pupil, target_device_idx=device_idx),
+                     target_device_idx=device_idx)
+        src = Source([0.0, 0.0], 8, c.wavelength_nm, phot_density_value=S0)
+        self.prop = AtmoPropagation(sp, {'on_axis_source': src}, target_device_idx=device_idx)
+        self.prop.inputs['atmo_layer_list'].set(self.atmo.layer_list)
+        self.prop.inputs['common_layer_list'].set([self.pupilstop, self.dm.layer])
+        self.sh = SH(wavelengthInNm=c.wavelength_nm, subap_wanted_fov=c.subap_npx * pxs, sensor_pxscale=pxs,
+                     subap_on_diameter=c.n_lenses, subap_npx=c.subap_npx, fov_ovs_coeff=c.fov_ovs_coeff,
+                     target_device_idx=device_idx)
+        self.sh.inputs['in_ef'].set(self.prop.outputs['out_on_axis_source_ef'])
+        side = c.n_lenses * c.subap_npx
+        self.ccd = CCD(sp, size=[side, side], dt=c.time_step, bandw=1.0, photon_noise=c.photon_noise,
+                       readout_noise=c.readout_noise > 0, readout_level=c.readout_noise, quantum_eff=1.0,
+                       target_device_idx=device_idx)
+        self.ccd.inputs['in_i'].set(self.sh.outputs['out_i'])
+        idxs, dmap = valid_subaps(pupil, c.n_lenses, c.subap_npx)
+        self.subapdata = SubapData(idxs=idxs, display_map=dmap, nx=c.n_lenses, ny=c.n_lenses,
+                                   target_device_idx=device_idx)
+        self.slopec = ShSlopec(self.subapdata, target_device_idx=device_idx)
+        self.slopec.inputs['in_pixels'].set(self.ccd.outputs['out_pixels'])
+        nsl = 2 * len(idxs)
+        if recmat is None:
+            g = torch.Generator(device=dev).manual_seed(c.seed + 1)
+            recmat = torch.randn((c.n_modes, nsl), device=dev, generator=g) * (1.0 / math.sqrt(nsl))
+        self.rec = Modalrec(recmat=Recmat(recmat, target_device_idx=device_idx), target_device_idx=device_idx)
+        self.rec.inputs['in_slopes'].set(self.slopec.outputs['out_slopes'])
+        self.integ = Integrator(sp, int_gain=[c.gain] * c.n_modes, delay=c.delay, target_device_idx=device_idx)
+        self.integ.inputs['delta_comm'].set(self.rec.outputs['out_modes'])
+        self.dm.inputs['in_command'].set(self.integ.outputs['out_comm'])
+        self.objects = [self.atmo, self.prop, self.sh, self.ccd, self.slopec, self.rec, self.integ, self.dm]
+        self.loop = LoopControl()
+        for k, o in enumerate(self.objects):
+            self.loop.add(o, k)
+        self.graph = None
+        self.n_valid_subaps = len(idxs)
+        self.n_valid_pixels = nv
+
+    def start(self):
+        for v in (self.seeing, self.wind_speed, self.wind_direction):
+            v.generation_time = 0
+        self.loop.start(1e9, self.cfg.time_step)
+
+    def step_eager(self):
+        """One step object by object (check_ready / trigger / post_trigger)."""
+        t = self.loop._t
+        for v in (self.seeing, self.wind_speed, self.wind_direction):
+            v.generation_time = t
+        self.loop.iter()
+
+    def capture(self):
+        """Capture one whole step (every object's trigger_code) in a CUDA
+        graph.  Call after at least one eager step, so the time step used by
+        AtmoEvolution is the loop's (the first step has delta_time = 0)."""
+        self.step_eager()
+        torch.cuda.synchronize(self.device)
+        self.atmo.delta_time = self.atmo.t_to_seconds(self.loop._dt)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            for o in self.objects:
+                o.trigger_code()
+        torch.cuda.synchronize(self.device)
+        self.graph = g
+        return g
+
+    def replay(self):
+        self.graph.replay()
+
+    # kernels launched by one captured step (for the launch count)
+    KERNELS_PER_STEP = 11
+
+
+def valid_subaps(pupil, n_lenses, npx, threshold=0.5):
+    """Sub-apertures whose pupil illumination exceeds `threshold` of the
+    brightest, with their detector pixel tables in the ShSubapCalibrator
+    layout (sh_subap_calibrator.py:46-92: boxes scanned lenslet-column first,
+    row-major pixels, display_map = j*n + i)."""
+    pix = pupil.shape[0]
+    ps = pix // n_lenses
+    illum = pupil[:n_lenses * ps, :n_lenses * ps].reshape(n_lenses, ps, n_lenses, ps).sum(axis=(1, 3))
+    side = n_lenses * npx
+    idxs, dmap = [], []
+    for i in range(n_lenses):
+        for j in range(n_lenses):
+            # box rows come from lenslet column j, box columns from row i
+            if illum[j, i] > threshold * illum.max():
+                r0, c0 = j * npx, i * npx
+                rr, cc = np.meshgrid(np.arange(r0, r0 + npx), np.arange(c0, c0 + npx), indexing='ij')
+                idxs.append((rr * side + cc).ravel())
+                dmap.append(j * n_lenses + i)
+    return np.array(idxs, dtype=np.int64), np.array(dmap, dtype=np.int64)

@@ -1,0 +1,316 @@
+"""Generate the golden fixtures under tests/golden/ by running the reference.
+
+Run in a container where the SPECULA source tree is available (default
+location /root/reference, override with SPECULA_REF):
+
+    python tests/golden/make_golden.py
+
+The reference is imported on CPU (``specula.init(-1, precision)``) with the
+harness-only stand-ins in tests/golden/_refstubs for astropy.io.fits and
+matplotlib (both absent from the image).  Inputs are seeded; every array the
+tests compare against is an output of the reference's own code.  The
+reference's committed FITS fixtures (test/data/*.fits) are converted to
+``ref_fits.npz`` with the small reader in fits_min.py.
+
+Nothing in the test suite, smoke() or bench.py reads the reference at run
+time; they only read the .npz/.json files written here.
+"""
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF = os.environ.get('SPECULA_REF', '/root/reference')
+sys.path.insert(0, os.path.join(HERE, '_refstubs'))
+sys.path.insert(0, REF)
+sys.path.insert(0, HERE)
+
+import fits_min  # noqa: E402
+
+RAD2ASEC = 180 * 3600 / np.pi
+
+
+def lam_over_d_arcsec(lam_nm, d_m):
+    return lam_nm * 1e-9 / d_m * RAD2ASEC
+
+
+# (name, pixel_pupil, pitch, lambda_nm, fov_arcsec, pxscale_arcsec, n_lenses, subap_npx, fov_ovs_coeff)
+SH_CASES = [
+    ('c1_plain16', 160, 0.05, 750.0, 8 * 0.875 * lam_over_d_arcsec(750, 0.4), 0.875 * lam_over_d_arcsec(750, 0.4), 20, 8, 1.0),
+    ('c1_interp', 160, 0.05, 750.0, 8 * lam_over_d_arcsec(750, 0.4), lam_over_d_arcsec(750, 0.4), 20, 8, 0.0),
+    ('flux120', 120, 0.05, 500.0, 3.0, 0.5, 20, 6, 0.0),
+    ('test64', 64, 0.015625, 600.0, 4.0, 0.5, 8, 8, 0.0),
+    ('n16_fft32', 128, 0.05, 750.0, 6 * 0.5 * lam_over_d_arcsec(750, 0.4), 0.5 * lam_over_d_arcsec(750, 0.4), 16, 6, 1.0),
+    ('n16_fft16', 128, 0.05, 750.0, 6 * lam_over_d_arcsec(750, 0.4), lam_over_d_arcsec(750, 0.4), 16, 6, 1.0),
+]
+
+# geometry-only cases (setup is cheap even at ELT size)
+GEOM_CASES = SH_CASES + [
+    ('c2_fft16', 640, 39.0 / 640, 750.0, 6 * lam_over_d_arcsec(750, 39.0 / 80), lam_over_d_arcsec(750, 39.0 / 80), 80, 6, 1.0),
+    ('c2_fft32', 640, 39.0 / 640, 750.0, 6 * 0.5 * lam_over_d_arcsec(750, 39.0 / 80), 0.5 * lam_over_d_arcsec(750, 39.0 / 80), 80, 6, 1.0),
+    ('c4_40x40', 320, 0.1, 750.0, 6 * lam_over_d_arcsec(750, 0.8), lam_over_d_arcsec(750, 0.8), 40, 6, 1.0),
+    ('c3_74x74', 592, 39.0 / 592, 750.0, 6 * lam_over_d_arcsec(750, 39.0 / 74), lam_over_d_arcsec(750, 39.0 / 74), 74, 6, 1.0),
+    ('c3_589nm', 320, 0.1, 589.0, 6 * lam_over_d_arcsec(589, 0.8), lam_over_d_arcsec(589, 0.8), 40, 6, 1.0),
+]
+
+
+def sh_input(pix, seed, amp_nm=60.0):
+    """Seeded test field: annular pupil (obs 0.14) and Gaussian random phase."""
+    from specula.lib.make_mask import make_mask
+    mask = make_mask(pix, 0.14, 1.0, xp=np).astype(np.float32)
+    rng = np.random.default_rng(seed)
+    phase = (rng.standard_normal((pix, pix)) * amp_nm).astype(np.float32) * mask
+    return mask, phase
+
+
+def make_sh_cases(precision):
+    import specula
+    from specula.processing_objects.sh import SH
+    from specula.data_objects.electric_field import ElectricField
+    out = {}
+    geoms = {}
+    for (name, pix, pitch, lam, fov, pxs, n, npx, coeff) in GEOM_CASES:
+        sh = SH(wavelengthInNm=lam, subap_wanted_fov=fov, sensor_pxscale=pxs, subap_on_diameter=n,
+                subap_npx=npx, fov_ovs_coeff=coeff, target_device_idx=-1, precision=precision)
+        sh._noprints = True
+        ef = ElectricField(pix, pix, pitch, S0=1.0, target_device_idx=-1, precision=precision)
+        ef.generation_time = 1
+        sh.inputs['in_ef'].set(ef)
+        sh.set_in_ef(ef)
+        sh.calc_trigger_geometry(ef)
+        geoms[name] = dict(pix=pix, pitch=pitch, lam=lam, fov=fov, pxscale=pxs, n=n, npx=npx, coeff=coeff,
+                           np_sub=int(sh._np_sub), ovs_np_sub=int(sh._ovs_np_sub), fov_ovs=float(sh._fov_ovs),
+                           fft_size=int(sh._fft_size), cutpixels=int(sh._cutpixels), cutsize=int(sh._cutsize),
+                           fp_mask_sum=int(np.sum(sh._fp_mask)))
+    for ci, (name, pix, pitch, lam, fov, pxs, n, npx, coeff) in enumerate(SH_CASES):
+        mask, phase = sh_input(pix, seed=100 + ci)
+        sh = SH(wavelengthInNm=lam, subap_wanted_fov=fov, sensor_pxscale=pxs, subap_on_diameter=n,
+                subap_npx=npx, fov_ovs_coeff=coeff, target_device_idx=-1, precision=precision)
+        sh._noprints = True
+        ef = ElectricField(pix, pix, pitch, S0=7.0, target_device_idx=-1, precision=precision)
+        ef.A[:] = mask
+        ef.phaseInNm[:] = phase
+        ef.generation_time = 1
+        sh.inputs['in_ef'].set(ef)
+        sh.setup()
+        sh.check_ready(1)
+        sh.trigger()
+        sh.post_trigger()
+        out[name + '/A'] = mask
+        out[name + '/phase'] = phase
+        out[name + '/intensity'] = np.array(sh.outputs['out_i'].i)
+        out[name + '/fp_mask'] = np.array(sh._fp_mask)
+    return out, geoms
+
+
+def make_chain_cases():
+    import specula  # noqa: F401
+    from specula.processing_objects.sh_slopec import ShSlopec
+    from specula.processing_objects.ccd import CCD
+    from specula.processing_objects.integrator import Integrator
+    from specula.processing_objects.dm import DM
+    from specula.processing_objects.modalrec import Modalrec
+    from specula.processing_objects.atmo_evolution import AtmoEvolution
+    from specula.processing_objects.atmo_propagation import AtmoPropagation
+    from specula.processing_objects.sh_subap_calibrator import ShSubapCalibrator
+    from specula.data_objects.subap_data import SubapData
+    from specula.data_objects.pixels import Pixels
+    from specula.data_objects.intensity import Intensity
+    from specula.data_objects.ifunc import IFunc
+    from specula.data_objects.recmat import Recmat
+    from specula.data_objects.slopes import Slopes
+    from specula.data_objects.source import Source
+    from specula.data_objects.pupilstop import Pupilstop
+    from specula.data_objects.simul_params import SimulParams
+    from specula.base_value import BaseValue
+    out = {}
+    rng = np.random.default_rng(7)
+
+    # sub-aperture detection + slopes on a 12x12-lenslet, 6 px detector image
+    img = (rng.random((72, 72)) * 50).astype(np.float32)
+    img[:6, :6] = 0.0                                # a dark corner sub-aperture
+    cal = ShSubapCalibrator(subap_on_diameter=12, energy_th=0.5, data_dir='/tmp', output_tag='x', target_device_idx=-1)
+    sd = cal._detect_subaps(img, 0.5)
+    out['slopec/image'] = img
+    out['slopec/idxs'] = np.array(sd.idxs)
+    out['slopec/display_map'] = np.array(sd.display_map)
+    sl = ShSlopec(sd, target_device_idx=-1)
+    px = Pixels(72, 72, target_device_idx=-1)
+    px.pixels = img
+    px.generation_time = 1
+    sl.inputs['in_pixels'].set(px)
+    sl.setup()
+    sl.check_ready(1)
+    sl.trigger()
+    sl.post_trigger()
+    out['slopec/slopes'] = np.array(sl.outputs['out_slopes'].slopes)
+    out['slopec/flux'] = np.array(sl.flux_per_subaperture_vector.value)
+
+    # CCD: noise-free and noisy (reference RNG) frames
+    sp = SimulParams(pixel_pupil=64, pixel_pitch=0.01, time_step=0.001)
+    inten = (rng.random((48, 48)) * 0.2).astype(np.float32)
+    out['ccd/intensity'] = inten
+    for tag, kw in (('clean', dict()),
+                    ('noisy', dict(photon_noise=True, readout_noise=True, readout_level=3.0)),
+                    ('ron_only', dict(readout_noise=True, readout_level=2.0)),
+                    ('dt3', dict(dt=0.003))):
+        kk = dict(dt=0.001)
+        kk.update(kw)
+        c = CCD(sp, size=[48, 48], bandw=300, quantum_eff=0.5, target_device_idx=-1, **kk)
+        ii = Intensity(48, 48, target_device_idx=-1)
+        ii.i[:] = inten
+        c.inputs['in_i'].set(ii)
+        c.setup()
+        frames = []
+        for t in range(4):
+            tt = t * 1000000
+            ii.generation_time = tt
+            c.check_ready(tt)
+            c.trigger()
+            c.post_trigger()
+            frames.append(np.array(c.outputs['out_pixels'].pixels, dtype=np.float64))
+        out['ccd/' + tag] = np.array(frames)
+
+    # Modalrec + integrator + DM
+    nm, ns = 7, 40
+    R = rng.standard_normal((nm, ns)).astype(np.float32)
+    s = Slopes(slopes=rng.standard_normal(ns).astype(np.float32), target_device_idx=-1)
+    s.generation_time = 1
+    mr = Modalrec(recmat=Recmat(R, target_device_idx=-1), target_device_idx=-1)
+    mr.inputs['in_slopes'].set(s)
+    mr.setup()
+    mr.check_ready(1)
+    mr.trigger()
+    mr.post_trigger()
+    out['rec/R'] = R
+    out['rec/s'] = s.slopes
+    out['rec/modes'] = np.array(mr.modes.value)
+    gains = rng.random(nm).astype(np.float32)
+    integ = Integrator(sp, int_gain=list(gains), delay=2, target_device_idx=-1)
+    dc = BaseValue(value=np.zeros(nm, np.float32))
+    integ.inputs['delta_comm'].set(dc)
+    integ.setup()
+    ins, outs = [], []
+    for t in range(6):
+        dc.value = rng.standard_normal(nm).astype(np.float32)
+        dc.generation_time = t
+        integ.check_ready(t)
+        integ.trigger()
+        integ.post_trigger()
+        ins.append(dc.value.copy())
+        outs.append(np.array(integ.out_comm.value))
+    out['iir/gains'] = gains
+    out['iir/in'] = np.array(ins)
+    out['iir/out'] = np.array(outs)
+    pup = Pupilstop(sp, obs_diam=0.14, target_device_idx=-1)
+    nv = int(np.sum(pup.A))
+    IF = rng.standard_normal((nm, nv)).astype(np.float32)
+    dm = DM(sp, 0, ifunc=IFunc(ifunc=IF, mask=pup.A, target_device_idx=-1), target_device_idx=-1)
+    cm = BaseValue(value=rng.standard_normal(nm).astype(np.float32))
+    cm.generation_time = 1
+    dm.inputs['in_command'].set(cm)
+    dm.setup()
+    dm.check_ready(1)
+    dm.trigger()
+    dm.post_trigger()
+    out['dm/mask'] = np.array(pup.A)
+    out['dm/ifunc'] = IF
+    out['dm/cmd'] = cm.value
+    out['dm/phase'] = np.array(dm.layer.phaseInNm)
+
+    # AtmoEvolution (3 layers, fractional-degree winds) + on-axis AtmoPropagation
+    ws = [10.0, 25.0, 7.0]
+    wd = [0.0, 123.4, 271.77]
+    atmo = AtmoEvolution(sp, L0=25, heights=[0, 1000, 5000], Cn2=[0.5, 0.3, 0.2], data_dir='/tmp/golden_screens',
+                         pixel_phasescreens=256, seed=1, target_device_idx=-1)
+    see = BaseValue(value=0.8)
+    wsv = BaseValue(value=np.array(ws))
+    wdv = BaseValue(value=np.array(wd))
+    atmo.inputs['seeing'].set(see)
+    atmo.inputs['wind_speed'].set(wsv)
+    atmo.inputs['wind_direction'].set(wdv)
+    src = Source([0, 0], 8, 750)
+    prop = AtmoPropagation(sp, {'on_axis_source': src}, target_device_idx=-1)
+    prop.inputs['atmo_layer_list'].set(atmo.layer_list)
+    prop.inputs['common_layer_list'].set([pup])
+    atmo.setup()
+    prop.setup()
+    out['atmo/strips'] = np.array(atmo.phasescreens)
+    layers, efA, efP = [], [], []
+    for t in range(4):
+        tt = t * 1000000
+        for v in (see, wsv, wdv):
+            v.generation_time = tt
+        atmo.check_ready(tt)
+        atmo.trigger()
+        atmo.post_trigger()
+        prop.check_ready(tt)
+        prop.trigger()
+        prop.post_trigger()
+        layers.append(np.array([np.array(l.phaseInNm) for l in atmo.layer_list]))
+        ef = prop.outputs['out_on_axis_source_ef']
+        efA.append(np.array(ef.A))
+        efP.append(np.array(ef.phaseInNm))
+    out['atmo/layers'] = np.array(layers)
+    out['atmo/ef_A'] = np.array(efA)
+    out['atmo/ef_phase'] = np.array(efP)
+    out['atmo/wind_speed'] = np.array(ws)
+    out['atmo/wind_direction'] = np.array(wd)
+    return out
+
+
+def convert_ref_fits():
+    d = os.path.join(REF, 'test', 'data')
+    out = {}
+    h = fits_min.read_hdus(os.path.join(d, 'scao_subaps_n8_th0.5_ref.fits'))
+    out['subaps/idxs'] = h[1][1].T.astype(np.int64)        # SubapData.restore transposes
+    out['subaps/display_map'] = h[2][1].astype(np.int64)
+    out['subaps/np_sub'] = np.array(h[0][0]['NP_SUB'])
+    h = fits_min.read_hdus(os.path.join(d, 'scao_sn_n8_th0.5_ref.fits'))
+    out['sn/slopes'] = np.array(h[1][1], dtype=np.float64)
+    h = fits_min.read_hdus(os.path.join(d, 'scao_rec_n8_th0.5_ref.fits'))
+    out['rec/recmat_T'] = np.array(h[1][1], dtype=np.float64)
+    out['extrapol/mask'] = fits_min.read_hdus(os.path.join(d, 'mask.fits'))[0][1]
+    out['extrapol/phase'] = fits_min.read_hdus(os.path.join(d, 'phase.fits'))[0][1]
+    out['extrapol/extrapolated1'] = fits_min.read_hdus(os.path.join(d, 'extrapolated1.fits'))[0][1]
+    out['extrapol/extrapolated2'] = fits_min.read_hdus(os.path.join(d, 'extrapolated2.fits'))[0][1]
+    for flag in ('False', 'True'):
+        h = fits_min.read_hdus(os.path.join(d, 'extrapol_array_doExt2Pix%s.fits' % flag))
+        out['extrapol/mat1_' + flag] = h[0][1]
+        out['extrapol/mat2_' + flag] = h[1][1]
+    return out
+
+
+def main():
+    import subprocess
+    # The reference binds its global precision at import time
+    # (base_time_obj.py:1), so the float64 run needs its own process.
+    subprocess.run([sys.executable, os.path.abspath(__file__), '--fp64'], check=True)
+    import specula
+    specula.init(-1, precision=1)
+    ref = convert_ref_fits()
+    np.savez_compressed(os.path.join(HERE, 'ref_fits.npz'), **ref)
+    sh32, geoms = make_sh_cases(precision=1)
+    np.savez_compressed(os.path.join(HERE, 'sh_fp32.npz'), **sh32)
+    with open(os.path.join(HERE, 'sh_geometry.json'), 'w') as f:
+        json.dump(geoms, f, indent=1, sort_keys=True)
+    chain = make_chain_cases()
+    np.savez_compressed(os.path.join(HERE, 'chain_fp32.npz'), **chain)
+    print('wrote', sorted(os.listdir(HERE)))
+
+
+def main_fp64():
+    import specula
+    specula.init(-1, precision=0)
+    sh64, _ = make_sh_cases(precision=0)
+    np.savez_compressed(os.path.join(HERE, 'sh_fp64.npz'),
+                        **{k: v for k, v in sh64.items() if k.endswith('/intensity')})
+
+
+if __name__ == '__main__':
+    if '--fp64' in sys.argv:
+        main_fp64()
+    else:
+        main()

@@ -1,0 +1,83 @@
+"""The C-ABI library loads without a GPU, exports every function declared in
+include/specula_b200.h, and rejects bad arguments before touching the device."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from specula_b200 import _lib
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), 'include', 'specula_b200.h')
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r'/\*.*?\*/', '', src, flags=re.S)
+    return sorted(set(re.findall(r'\b(sb_\w+)\s*\(', src)))
+
+
+@pytest.fixture(scope='module')
+def lib():
+    if not os.path.exists(_lib.LIB_PATH):
+        from specula_b200.csrc import build
+        build.build()
+    return _lib.load()
+
+
+def test_every_declared_symbol_is_exported(lib):
+    names = declared_functions()
+    assert len(names) >= 14
+    for n in names:
+        assert hasattr(lib, n), n
+
+
+def test_binding_table_matches_header():
+    assert sorted(_lib.SIGNATURES) == declared_functions()
+
+
+def test_version_and_error_string(lib):
+    assert lib.sb_version() >= 100
+    assert isinstance(lib.sb_last_error(), bytes)
+
+
+def test_argument_validation_without_device(lib):
+    plan = _lib.ShPlan()
+    rc = lib.sb_sh_forward(C.byref(plan), None, None, None, 0, C.c_float(1.0), None, None, 0, None)
+    assert rc == -1
+    assert b'null' in lib.sb_last_error()
+    rc = lib.sb_modalrec(None, 3, 4, 4, None, None, None)
+    assert rc == -1
+    assert lib.sb_atmo_evolve(None, 1, 16, None, None) == -1
+    layers = (_lib.AtmoLayer * 17)()
+    pos = C.c_double(0)
+    assert lib.sb_atmo_evolve(layers, 17, 16, C.byref(pos), None) == -2
+
+
+STRUCTS = {'sb_sh_plan': _lib.ShPlan, 'sb_ccd_params': _lib.CcdParams, 'sb_slopec_plan': _lib.SlopecPlan,
+           'sb_iir_plan': _lib.IirPlan, 'sb_atmo_layer': _lib.AtmoLayer, 'sb_prop_layer': _lib.PropLayer}
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """Compile a probe against the header with gcc and compare every struct's
+    size and field offsets with the ctypes mirrors."""
+    import shutil
+    import subprocess
+    if shutil.which('gcc') is None:
+        pytest.skip('gcc not available')
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "specula_b200.h"', 'int main(void){']
+    for cname, py in STRUCTS.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines.append('return 0;}')
+    src = tmp_path / 'probe.c'
+    src.write_text('\n'.join(lines))
+    exe = tmp_path / 'probe'
+    subprocess.run(['gcc', '-I', os.path.dirname(HEADER), str(src), '-o', str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split('\n')
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, py in STRUCTS.items():
+        assert got[(cname, 'size')] == C.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
