@@ -40,8 +40,8 @@ WORKLOAD = 'elt_80x80_fft16_7layers_500modes'
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument('--gpus', type=int, default=1)
-    p.add_argument('--steps', type=int, default=200)
-    p.add_argument('--warmup', type=int, default=5)
+    p.add_argument('--steps', type=int, default=4000)
+    p.add_argument('--warmup', type=int, default=10)
     p.add_argument('--impl', default='b200', choices=['b200', 'reference'])
     p.add_argument('--cpu-baseline-seconds', type=float, default=20.0)
     p.add_argument('--no-cpu-baseline', action='store_true')
@@ -70,7 +70,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(['nvidia-smi', '-i', self.gpu, f'--query-gpu={self.FIELDS}',
-                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                          '--format=csv,noheader,nounits', '-lms', '50'],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()

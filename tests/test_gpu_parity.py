@@ -161,6 +161,7 @@ def test_ccd_noise_statistics(cuda):
     ii.i.copy_(torch.as_tensor(lam_img / (0.5 * 0.3)))
     frames = []
     for t in range(6):
+        ii.generation_time = t * 1000000
         ccd.check_ready(t * 1000000)
         ccd.trigger()
         ccd.post_trigger()
@@ -185,12 +186,15 @@ def test_ccd_is_deterministic_across_runs(cuda):
     img = torch.rand(64, 64, device='cuda') * 100
     ia.i.copy_(img)
     ib.i.copy_(img)
-    for obj in (a, b):
+    for obj, ii in ((a, ia), (b, ib)):
         for t in range(3):
+            ii.generation_time = t * 1000000
             obj.check_ready(t * 1000000)
             obj.trigger()
             obj.post_trigger()
-    assert torch.equal(a.outputs['out_pixels'].pixels, b.outputs['out_pixels'].pixels)
+    pa = a.outputs['out_pixels'].pixels
+    assert torch.equal(pa, b.outputs['out_pixels'].pixels)
+    assert float(pa.abs().sum()) > 0
 
 
 def _philox_numpy(key0, key1, counters):
