@@ -29,63 +29,94 @@ __global__ void atmo_advance_kernel(EvolveArgs a) {
     a.pos[k] = np;
 }
 
-struct Window {
-    const float *row0;
-    int ld;
-    float frac;
-};
-
-// lerped strip value at (r, c) of the un-rotated layer (atmo_evolution.py:290)
-__device__ __forceinline__ float lerp_at(const Window &w, int r, int c) {
-    const float *row = w.row0 + (size_t)r * w.ld + c;
-    const float w0 = __fsub_rn(1.0f, w.frac);
-    return __fadd_rn(__fmul_rn(w0, row[0]), __fmul_rn(w.frac, row[1]));
-}
-
-// value of rot90(lerped, k) at (y, x)
-__device__ __forceinline__ float rot90_at(const Window &w, int k, int L, int y, int x) {
-    switch (k) {
-        case 1: return lerp_at(w, x, L - 1 - y);
-        case 2: return lerp_at(w, L - 1 - y, L - 1 - x);
-        case 3: return lerp_at(w, L - 1 - x, y);
-        default: return lerp_at(w, y, x);
-    }
-}
+// Output tiles of 32 x 32 pixels per CTA (32 x 8 threads, 4 rows each).
+// The tile's footprint in the rot90'd, lerped layer is staged in shared
+// memory first: that read is ordered so consecutive threads touch
+// consecutive screen columns whatever the rot90 quarter, which keeps the
+// strip reads coalesced (a direct gather is column-strided for odd k).
+constexpr int kTile = 32;
+constexpr int kBox = kTile + 8;   // footprint of a tile rotated by < 1 degree, plus the bilinear +1
 
 __global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgs a) {
+    __shared__ float Q[kBox][kBox + 1];
     const sb_atmo_layer &ly = a.layer[blockIdx.z];
     const int L = a.L;
     // integer position and float32 remainder (atmo_evolution.py:278-279)
     const double np = a.pos[blockIdx.z];
     const double q = floor(np);
-    Window w;
-    w.row0 = ly.screen + (long long)q;
-    w.ld = ly.screen_ld;
-    w.frac = (float)(np - q);
+    const float *row0 = ly.screen + (long long)q;
+    const int ld = ly.screen_ld;
+    const float frac = (float)(np - q);
+    const float w0 = __fsub_rn(1.0f, frac);
     const int k = ly.rot90;
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (x >= L || y >= L) return;
-    float v;
-    if (!ly.rotate) {
-        v = rot90_at(w, k, L, y, x);
-    } else {
-        const double ir = __dadd_rn(__dadd_rn(__dmul_rn(ly.m00, (double)y), __dmul_rn(ly.m01, (double)x)), ly.off0);
-        const double ic = __dadd_rn(__dadd_rn(__dmul_rn(ly.m10, (double)y), __dmul_rn(ly.m11, (double)x)), ly.off1);
-        if (!(ir >= 0.0 && ir <= (double)(L - 1) && ic >= 0.0 && ic <= (double)(L - 1))) {
-            v = 0.0f;
-        } else {
-            const int r0 = (int)floor(ir), c0 = (int)floor(ic);
-            const double fr = ir - r0, fc = ic - c0;
-            const int r1 = r0 + 1, c1 = c0 + 1;
-            const double q00 = rot90_at(w, k, L, r0, c0);
-            const double q01 = c1 < L ? (double)rot90_at(w, k, L, r0, c1) : 0.0;
-            const double q10 = r1 < L ? (double)rot90_at(w, k, L, r1, c0) : 0.0;
-            const double q11 = (r1 < L && c1 < L) ? (double)rot90_at(w, k, L, r1, c1) : 0.0;
-            v = (float)(q00 * (1 - fr) * (1 - fc) + q01 * (1 - fr) * fc + q10 * fr * (1 - fc) + q11 * fr * fc);
-        }
+    const int x0 = blockIdx.x * kTile, y0 = blockIdx.y * kTile;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+
+    // footprint [br0, br1] x [bc0, bc1] in the rot90'd layer
+    int br0 = y0, br1 = min(y0 + kTile, L) - 1, bc0 = x0, bc1 = min(x0 + kTile, L) - 1;
+    if (ly.rotate) {
+        double rmin = 1e300, rmax = -1e300, cmin = 1e300, cmax = -1e300;
+        for (int cy = 0; cy < 2; ++cy)
+            for (int cx = 0; cx < 2; ++cx) {
+                const double yy = cy ? br1 : br0, xx = cx ? bc1 : bc0;
+                const double ir = __dadd_rn(__dadd_rn(__dmul_rn(ly.m00, yy), __dmul_rn(ly.m01, xx)), ly.off0);
+                const double ic = __dadd_rn(__dadd_rn(__dmul_rn(ly.m10, yy), __dmul_rn(ly.m11, xx)), ly.off1);
+                rmin = fmin(rmin, ir); rmax = fmax(rmax, ir);
+                cmin = fmin(cmin, ic); cmax = fmax(cmax, ic);
+            }
+        br0 = max(0, (int)floor(rmin) - 1);
+        br1 = min(L - 1, (int)floor(rmax) + 2);
+        bc0 = max(0, (int)floor(cmin) - 1);
+        bc1 = min(L - 1, (int)floor(cmax) + 2);
+        // a footprint wider than the staging box means |angle| >= ~6 degrees,
+        // which the fractional-degree rotation never produces; clip safely
+        br1 = min(br1, br0 + kBox - 1);
+        bc1 = min(bc1, bc0 + kBox - 1);
     }
-    ly.out[(size_t)y * L + x] = __fmul_rn(v, ly.scale);
+    const int R = br1 - br0 + 1, Cc = bc1 - bc0 + 1;
+    for (int idx = tid; idx < R * Cc; idx += 256) {
+        int ra, cb;
+        if (k & 1) { ra = idx % R; cb = idx / R; } else { cb = idx % Cc; ra = idx / Cc; }
+        const int yy = br0 + ra, xx = bc0 + cb;
+        int sr, sc;   // screen row / column of rot90(lerped)[yy][xx] (atmo_evolution.py:291)
+        switch (k) {
+            case 1: sr = xx; sc = L - 1 - yy; break;
+            case 2: sr = L - 1 - yy; sc = L - 1 - xx; break;
+            case 3: sr = L - 1 - xx; sc = yy; break;
+            default: sr = yy; sc = xx;
+        }
+        const float *p = row0 + (size_t)sr * ld + sc;
+        Q[ra][cb] = __fadd_rn(__fmul_rn(w0, p[0]), __fmul_rn(frac, p[1]));
+    }
+    __syncthreads();
+    const int x = x0 + threadIdx.x;
+    for (int yi = threadIdx.y; yi < kTile; yi += blockDim.y) {
+        const int y = y0 + yi;
+        if (x >= L || y >= L) continue;
+        float v;
+        if (!ly.rotate) {
+            v = Q[y - br0][x - bc0];
+        } else {
+            // scipy.ndimage.rotate(order=1, mode='constant'): samples outside
+            // [0, L-1] give 0; neighbours off the grid count 0
+            const double ir = __dadd_rn(__dadd_rn(__dmul_rn(ly.m00, (double)y), __dmul_rn(ly.m01, (double)x)), ly.off0);
+            const double ic = __dadd_rn(__dadd_rn(__dmul_rn(ly.m10, (double)y), __dmul_rn(ly.m11, (double)x)), ly.off1);
+            if (!(ir >= 0.0 && ir <= (double)(L - 1) && ic >= 0.0 && ic <= (double)(L - 1))) {
+                v = 0.0f;
+            } else {
+                const int r0 = (int)floor(ir), c0 = (int)floor(ic);
+                const double fr = ir - r0, fc = ic - c0;
+                const int r1 = r0 + 1, c1 = c0 + 1;
+                const int qr = r0 - br0, qc = c0 - bc0;
+                const double q00 = Q[qr][qc];
+                const double q01 = c1 < L ? (double)Q[qr][qc + 1] : 0.0;
+                const double q10 = r1 < L ? (double)Q[qr + 1][qc] : 0.0;
+                const double q11 = (r1 < L && c1 < L) ? (double)Q[qr + 1][qc + 1] : 0.0;
+                v = (float)(q00 * (1 - fr) * (1 - fc) + q01 * (1 - fr) * fc + q10 * fr * (1 - fc) + q11 * fr * fc);
+            }
+        }
+        ly.out[(size_t)y * L + x] = __fmul_rn(v, ly.scale);   // atmo_evolution.py:294
+    }
 }
 
 struct PropArgs {
@@ -124,6 +155,10 @@ extern "C" int sb_atmo_evolve(const sb_atmo_layer *layers, int n_layers, int L, 
         if (!l.screen || !l.out || l.screen_cols < L + 1 || l.screen_ld < l.screen_cols || l.rot90 < 0 ||
             l.rot90 > 3 || !(l.delta >= 0.0))
             return sb::fail(SB_EINVAL, "sb_atmo_evolve: layer %d: bad screen window", k);
+        // the fractional-degree rotation is below 1 degree: the staged
+        // footprint of a tile is sized for that
+        if (l.rotate && !(fabs(l.m01) < 0.0175 && fabs(l.m10) < 0.0175 && l.m00 > 0.9998 && l.m11 > 0.9998))
+            return sb::fail(SB_EINVAL, "sb_atmo_evolve: layer %d: rotation must be below one degree", k);
         a.layer[k] = l;
     }
     a.n = n_layers;
@@ -133,7 +168,7 @@ extern "C" int sb_atmo_evolve(const sb_atmo_layer *layers, int n_layers, int L, 
     atmo_advance_kernel<<<1, 32, 0, st>>>(a);
     int rc = sb::check_launch("atmo_advance_kernel");
     if (rc) return rc;
-    dim3 block(32, 8), grid((L + 31) / 32, (L + 7) / 8, n_layers);
+    dim3 block(32, 8), grid((L + kTile - 1) / kTile, (L + kTile - 1) / kTile, n_layers);
     atmo_evolve_kernel<<<grid, block, 0, st>>>(a);
     return sb::check_launch("atmo_evolve_kernel");
 }

@@ -22,6 +22,7 @@ __global__ void __launch_bounds__(256) gemv_rows_kernel(const float *__restrict_
         const float4 *r4 = reinterpret_cast<const float4 *>(row);
         const float4 *s4 = reinterpret_cast<const float4 *>(s);
         float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+#pragma unroll 4
         for (int j = threadIdx.x; j < n4; j += blockDim.x) {
             const float4 r = __ldg(r4 + j), v = __ldg(s4 + j);
             a0 = fmaf(r.x, v.x, a0);

@@ -6,8 +6,8 @@
 // from Philox4x32-10 (Salmon, Moraes, Dror & Shaw, SC'11), a counter-based
 // generator: the draw of pixel e in frame f is a pure function of
 // (seed, f, e, draw), so results do not depend on the launch shape.
-// Poisson sampling: sequential-search inversion below mean 10, Hormann's
-// PTRS transformed rejection (1993) above.
+// Poisson sampling (float32): sequential-search inversion below mean 10,
+// Hormann's PTRS transformed rejection (1993) above.
 //
 // ShSlopec (sh_slopec.py:308-438): one warp per valid sub-aperture gathers
 // its pixels through the index table and reduces flux, denominator and the
@@ -47,55 +47,57 @@ __host__ __device__ __forceinline__ u4 philox4x32_10(u4 c, uint32_t k0, uint32_t
     return c;
 }
 
-// uniform in (0,1) with 53 random bits from two words
-__device__ __forceinline__ double u01(uint32_t a, uint32_t b) {
-    const uint64_t m = ((uint64_t)(a >> 5) << 26) | (uint64_t)(b >> 6);  // 27 + 26 bits
-    return ((double)m + 0.5) * (1.0 / 9007199254740992.0);
-}
+// uniform in (0,1) from the top 24 bits of a word
+__device__ __forceinline__ float u01f(uint32_t a) { return ((float)(a >> 8) + 0.5f) * (1.0f / 16777216.0f); }
 
 constexpr uint32_t kPhotonTag = 0x50484f54u;   // "PHOT"
 constexpr uint32_t kReadoutTag = 0x52454144u;  // "READ"
 
-__device__ double poisson_sample(double lam, uint32_t e, uint64_t frame, uint64_t seed) {
-    if (!(lam > 0.0)) return 0.0;
+// Poisson(lam) in float32 arithmetic.  lam < 10: sequential-search
+// inversion of one uniform.  lam >= 10: PTRS transformed rejection
+// (Hormann 1993), two uniforms per try, at most 64 tries (acceptance per try
+// is above 0.9, so the bound is never reached in practice).
+__device__ float poisson_sample(float lam, uint32_t e, uint64_t frame, uint64_t seed) {
+    if (!(lam > 0.0f)) return 0.0f;
     const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32) ^ kPhotonTag;
-    if (lam < 10.0) {
-        // inversion by sequential search: smallest k with CDF(k) >= u
+    if (lam < 10.0f) {
         const u4 r = philox4x32_10({e, (uint32_t)frame, (uint32_t)(frame >> 32), 0u}, k0, k1);
-        const double u = u01(r.x, r.y);
-        double pk = exp(-lam), cdf = pk;
+        const float u = u01f(r.x);
+        float pk = expf(-lam), cdf = pk;
         int k = 0;
-        while (u > cdf && k < 200) {
+        while (u > cdf && k < 100) {
             ++k;
-            pk *= lam / k;
+            pk *= lam / (float)k;
             cdf += pk;
         }
-        return (double)k;
+        return (float)k;
     }
-    // PTRS (Hormann 1993): transformed rejection with squeeze
-    const double slam = sqrt(lam), loglam = log(lam);
-    const double b = 0.931 + 2.53 * slam;
-    const double a = -0.059 + 0.02483 * b;
-    const double inv_alpha = 1.1239 + 1.1328 / (b - 3.4);
-    const double vr = 0.9277 - 3.6224 / (b - 2.0);
-    for (uint32_t it = 0; it < 64; ++it) {
+    const float slam = sqrtf(lam), loglam = logf(lam);
+    const float b = 0.931f + 2.53f * slam;
+    const float a = -0.059f + 0.02483f * b;
+    const float log_inv_alpha = logf(1.1239f + 1.1328f / (b - 3.4f));
+    const float vr = 0.9277f - 3.6224f / (b - 2.0f);
+    for (uint32_t it = 0; it < 32; ++it) {
         const u4 r = philox4x32_10({e, (uint32_t)frame, (uint32_t)(frame >> 32), 1u + it}, k0, k1);
-        const double U = u01(r.x, r.y) - 0.5;
-        const double V = u01(r.z, r.w);
-        const double us = 0.5 - fabs(U);
-        const double k = floor((2.0 * a / us + b) * U + lam + 0.43);
-        if (us >= 0.07 && V <= vr) return k;
-        if (k < 0.0 || (us < 0.013 && V > us)) continue;
-        if (log(V) + log(inv_alpha) - log(a / (us * us) + b) <= -lam + k * loglam - lgamma(k + 1.0)) return k;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const float U = u01f(h ? r.z : r.x) - 0.5f;
+            const float V = u01f(h ? r.w : r.y);
+            const float us = 0.5f - fabsf(U);
+            const float k = floorf((2.0f * a / us + b) * U + lam + 0.43f);
+            if (us >= 0.07f && V <= vr) return k;
+            if (k < 0.0f || (us < 0.013f && V > us)) continue;
+            if (logf(V) + log_inv_alpha - logf(a / (us * us) + b) <= -lam + k * loglam - lgammaf(k + 1.0f)) return k;
+        }
     }
-    return floor(lam + 0.5);  // unreachable in practice (acceptance > 0.9 per try)
+    return floorf(lam + 0.5f);
 }
 
-__device__ __forceinline__ double std_normal(uint32_t e, uint64_t frame, uint64_t seed) {
+// N(0,1) by Box-Muller from one Philox block
+__device__ __forceinline__ float std_normal(uint32_t e, uint64_t frame, uint64_t seed) {
     const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32) ^ kReadoutTag;
     const u4 r = philox4x32_10({e, (uint32_t)frame, (uint32_t)(frame >> 32), 0u}, k0, k1);
-    const double u1 = u01(r.x, r.y), u2 = u01(r.z, r.w);
-    return sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);   // Box-Muller
+    return sqrtf(-2.0f * logf(u01f(r.x))) * cospif(2.0f * u01f(r.y));
 }
 
 __global__ void __launch_bounds__(256) ccd_kernel(sb_ccd_params p, const float *__restrict__ in,
@@ -118,8 +120,8 @@ __global__ void __launch_bounds__(256) ccd_kernel(sb_ccd_params p, const float *
         f = __fadd_rn(f, p.bg_plus_dark);                           // ccd.py:220-221
         float outv;
         if (p.photon_noise) {
-            double v = poisson_sample((double)f, (uint32_t)e, frame, p.photon_seed);
-            if (p.readout_noise) v += trunc(std_normal((uint32_t)e, frame, p.readout_seed) * p.readout_level);
+            double v = poisson_sample(f, (uint32_t)e, frame, p.photon_seed);
+            if (p.readout_noise) v += truncf(std_normal((uint32_t)e, frame, p.readout_seed) * p.readout_level);
             // ADU: round(x*g)+bias, clamp at 0, -bias, /g, back to the
             // integer dtype of the Poisson draw (ccd.py:247-258)
             double x = rint(v * (double)p.adu_gain) + (double)p.adu_bias;
@@ -130,7 +132,7 @@ __global__ void __launch_bounds__(256) ccd_kernel(sb_ccd_params p, const float *
             outv = (float)x;
         } else {
             if (p.readout_noise)
-                f = __fadd_rn(f, (float)(std_normal((uint32_t)e, frame, p.readout_seed) * p.readout_level));
+                f = __fadd_rn(f, __fmul_rn(std_normal((uint32_t)e, frame, p.readout_seed), p.readout_level));
             outv = f;
         }
         pix[e] = outv;
@@ -166,13 +168,15 @@ __global__ void philox_raw_kernel(uint32_t k0, uint32_t k1, uint32_t c1, uint32_
 
 __global__ void __launch_bounds__(256) slopec_sums_kernel(sb_slopec_plan pl, const float *__restrict__ pix,
                                                           float *__restrict__ flux, float *__restrict__ tot,
-                                                          float *__restrict__ sxn, float *__restrict__ syn) {
-    const int lane = threadIdx.x & 31;
+                                                          float *__restrict__ sxn, float *__restrict__ syn,
+                                                          float *__restrict__ part_tot) {
+    __shared__ float wsum[8];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (s >= pl.n_subaps) return;
-    const int32_t *ix = pl.idxs + (size_t)s * pl.npx2;
+    const bool valid = s < pl.n_subaps;
+    const int32_t *ix = pl.idxs + (size_t)(valid ? s : 0) * pl.npx2;
     float f = 0.f, t = 0.f, x = 0.f, y = 0.f;
-    for (int e = lane; e < pl.npx2; e += 32) {
+    for (int e = lane; valid && e < pl.npx2; e += 32) {
         const float v = pix[ix[e]];
         f += v;
         float w = v - pl.thr;                 // pixels -= thr; clamp < 0 -> 0
@@ -186,20 +190,31 @@ __global__ void __launch_bounds__(256) slopec_sums_kernel(sb_slopec_plan pl, con
     x = sb::warp_sum(x);
     y = sb::warp_sum(y);
     if (lane == 0) {
-        flux[s] = f;
-        tot[s] = t;
-        sxn[s] = x;
-        syn[s] = y;
+        if (valid) {
+            flux[s] = f;
+            tot[s] = t;
+            sxn[s] = x;
+            syn[s] = y;
+        }
+        wsum[warp] = valid ? t : 0.f;
+    }
+    __syncthreads();
+    // per-block partial of the denominators, summed in warp order
+    if (threadIdx.x == 0) {
+        float b = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) b += wsum[w];
+        part_tot[blockIdx.x] = b;
     }
 }
 
 __global__ void __launch_bounds__(256) slopec_finish_kernel(int n, const float *__restrict__ tot,
                                                             const float *__restrict__ sxn,
                                                             const float *__restrict__ syn,
+                                                            const float *__restrict__ part_tot, int nparts,
                                                             float *__restrict__ slopes) {
     __shared__ double red[33];
     double acc = 0.0;
-    for (int e = threadIdx.x; e < n; e += blockDim.x) acc += tot[e];
+    for (int e = threadIdx.x; e < nparts; e += blockDim.x) acc += part_tot[e];
     acc = sb::block_sum_all_d(acc, red);
     const float mean = (float)(acc / n);
     const float cut = 1.0f / (mean * 1e-3f);   // sh_slopec.py:393-400
@@ -239,7 +254,8 @@ extern "C" int sb_philox_raw(uint32_t key0, uint32_t key1, uint32_t c1, uint32_t
 
 extern "C" size_t sb_slopec_scratch_bytes(const sb_slopec_plan *pl) {
     if (!pl || pl->n_subaps < 0) return 0;
-    return ((size_t)3 * pl->n_subaps * sizeof(float) + 255) & ~(size_t)255;
+    const size_t nparts = ((size_t)pl->n_subaps + 7) / 8;
+    return ((size_t)(3 * pl->n_subaps + nparts) * sizeof(float) + 255) & ~(size_t)255;
 }
 
 extern "C" int sb_slopec(const sb_slopec_plan *pl, const float *pixels, float *slopes, float *flux, void *scratch,
@@ -257,11 +273,12 @@ extern "C" int sb_slopec(const sb_slopec_plan *pl, const float *pixels, float *s
     cudaStream_t st = sb::as_stream(stream);
     const int warps_per_block = 8;
     const int nblk = (pl->n_subaps + warps_per_block - 1) / warps_per_block;
-    slopec_sums_kernel<<<nblk, 32 * warps_per_block, 0, st>>>(*pl, pixels, flux, tot, sxn, syn);
+    float *part = syn + pl->n_subaps;
+    slopec_sums_kernel<<<nblk, 32 * warps_per_block, 0, st>>>(*pl, pixels, flux, tot, sxn, syn, part);
     int rc = sb::check_launch("slopec_sums_kernel");
     if (rc) return rc;
     int nb2 = (pl->n_subaps + 255) / 256;
     nb2 = nb2 > 148 ? 148 : nb2;
-    slopec_finish_kernel<<<nb2, 256, 0, st>>>(pl->n_subaps, tot, sxn, syn, slopes);
+    slopec_finish_kernel<<<nb2, 256, 0, st>>>(pl->n_subaps, tot, sxn, syn, part, nblk, slopes);
     return sb::check_launch("slopec_finish_kernel");
 }

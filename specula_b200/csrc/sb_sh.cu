@@ -36,33 +36,40 @@ struct ShSmem {
     int tw, tilt, mask, rebin, per_warp_E, per_warp_G, per_warp_I, per_warp_H, tables, per_warp;
 };
 
+// Shared-memory layout.  The twiddles are stored transposed, twT[c][b], so
+// the lanes of a warp (consecutive output frequencies b) read consecutive
+// words; the field rows are padded to np+1 to keep rows in distinct banks.
 __host__ __device__ inline ShSmem sh_smem_layout(int p, int cs, int npx) {
     ShSmem s;
-    // float2 arrays first (8-byte aligned), then floats; offsets in bytes
     s.tw = 0;
     s.tilt = s.tw + cs * p * 8;
     s.mask = s.tilt + p * p * 8;
     s.rebin = s.mask + cs * cs * 4;
     s.tables = ((s.rebin + npx * cs * 4) + 15) & ~15;
     s.per_warp_E = 0;
-    s.per_warp_G = s.per_warp_E + p * p * 8;
+    s.per_warp_G = s.per_warp_E + p * (p + 1) * 8;
     s.per_warp_I = s.per_warp_G + p * cs * 8;
     s.per_warp_H = s.per_warp_I + cs * cs * 4;
     s.per_warp = ((s.per_warp_H + cs * npx * 4) + 15) & ~15;
     return s;
 }
 
-__global__ void __launch_bounds__(256) sh_forward_kernel(ShArgs a) {
+constexpr int kU = 4;   // independent accumulators per lane
+
+__global__ void __launch_bounds__(256, 4) sh_forward_kernel(ShArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const ShSmem L = sh_smem_layout(a.p, a.cs, a.npx);
-    float2 *tw = reinterpret_cast<float2 *>(smem + L.tw);
+    float2 *twT = reinterpret_cast<float2 *>(smem + L.tw);
     float2 *tilt = reinterpret_cast<float2 *>(smem + L.tilt);
     float *mask = reinterpret_cast<float *>(smem + L.mask);
     float *R = reinterpret_cast<float *>(smem + L.rebin);
     __shared__ float red[33];
 
     const int p = a.p, cs = a.cs, npx = a.npx;
-    for (int e = threadIdx.x; e < cs * p; e += blockDim.x) tw[e] = a.tw[e];
+    for (int e = threadIdx.x; e < cs * p; e += blockDim.x) {
+        const int b = e / p, c = e - b * p;
+        twT[c * cs + b] = a.tw[e];
+    }
     for (int e = threadIdx.x; e < p * p; e += blockDim.x) tilt[e] = a.tilt[e];
     for (int e = threadIdx.x; e < cs * cs; e += blockDim.x) mask[e] = a.mask[e];
     for (int e = threadIdx.x; e < npx * cs; e += blockDim.x) R[e] = a.rebin[e];
@@ -72,10 +79,11 @@ __global__ void __launch_bounds__(256) sh_forward_kernel(ShArgs a) {
     const int i = blockIdx.y;                       // lenslet row
     const int j = blockIdx.x * a.spc + warp;        // lenslet column
     unsigned char *wbase = smem + L.tables + warp * L.per_warp;
-    float2 *E = reinterpret_cast<float2 *>(wbase + L.per_warp_E);
-    float2 *G = reinterpret_cast<float2 *>(wbase + L.per_warp_G);
-    float *I = reinterpret_cast<float *>(wbase + L.per_warp_I);
-    float *H = reinterpret_cast<float *>(wbase + L.per_warp_H);
+    float2 *E = reinterpret_cast<float2 *>(wbase + L.per_warp_E);   // [p][p+1]
+    float2 *G = reinterpret_cast<float2 *>(wbase + L.per_warp_G);   // [p][cs]
+    float *I = reinterpret_cast<float *>(wbase + L.per_warp_I);     // [cs][cs]
+    float *H = reinterpret_cast<float *>(wbase + L.per_warp_H);     // [cs][npx]
+    const int pe = p + 1;
 
     float local = 0.f;
     if (j < a.n) {
@@ -87,41 +95,67 @@ __global__ void __launch_bounds__(256) sh_forward_kernel(ShArgs a) {
             const size_t g = (row0 + r) * (size_t)a.ld + col0 + c;
             const float amp = a.A[g];
             const float phi = a.ph[g] * a.k;
-            float s, co;
-            sincosf(phi, &s, &co);
-            const float re = co * amp, im = s * amp;
+            float sn, co;
+            sincosf(phi, &sn, &co);
+            const float re = co * amp, im = sn * amp;
             const float2 t = tilt[e];
-            E[e] = make_float2(re * t.x - im * t.y, re * t.y + im * t.x);
+            E[r * pe + c] = make_float2(re * t.x - im * t.y, re * t.y + im * t.x);
         }
         __syncwarp();
-        // DFT along columns, kept frequencies only
-        for (int e = lane; e < p * cs; e += 32) {
-            const int r = e / cs, b = e - r * cs;
-            float xr = 0.f, xi = 0.f;
-            const float2 *er = E + r * p;
-            const float2 *wb = tw + b * p;
-            for (int c = 0; c < p; ++c) {
-                const float2 u = er[c], w = wb[c];
-                xr = fmaf(u.x, w.x, fmaf(-u.y, w.y, xr));
-                xi = fmaf(u.x, w.y, fmaf(u.y, w.x, xi));
+        // DFT along columns on the kept frequencies: G[r][b] = sum_c E[r][c] W[b][c]
+        for (int e0 = lane; e0 < p * cs; e0 += 32 * kU) {
+            int rr[kU], bb[kU];
+            float xr[kU], xi[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int e = min(e0 + 32 * u, p * cs - 1);
+                rr[u] = e / cs;
+                bb[u] = e - rr[u] * cs;
+                xr[u] = 0.f;
+                xi[u] = 0.f;
             }
-            G[e] = make_float2(xr, xi);
+            for (int c = 0; c < p; ++c) {
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const float2 x = E[rr[u] * pe + c], w = twT[c * cs + bb[u]];
+                    xr[u] = fmaf(x.x, w.x, fmaf(-x.y, w.y, xr[u]));
+                    xi[u] = fmaf(x.x, w.y, fmaf(x.y, w.x, xi[u]));
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kU; ++u)
+                if (e0 + 32 * u < p * cs) G[rr[u] * cs + bb[u]] = make_float2(xr[u], xi[u]);
         }
         __syncwarp();
         // DFT along rows, |F|^2 and field stop (sh.py:378-399)
-        for (int e = lane; e < cs * cs; e += 32) {
-            const int aa = e / cs, b = e - aa * cs;
-            float xr = 0.f, xi = 0.f;
-            const float2 *wa = tw + aa * p;
-            for (int r = 0; r < p; ++r) {
-                const float2 u = G[r * cs + b], w = wa[r];
-                xr = fmaf(u.x, w.x, fmaf(-u.y, w.y, xr));
-                xi = fmaf(u.x, w.y, fmaf(u.y, w.x, xi));
+        for (int e0 = lane; e0 < cs * cs; e0 += 32 * kU) {
+            int aa[kU], bb[kU];
+            float xr[kU], xi[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int e = min(e0 + 32 * u, cs * cs - 1);
+                aa[u] = e / cs;
+                bb[u] = e - aa[u] * cs;
+                xr[u] = 0.f;
+                xi[u] = 0.f;
             }
-            I[e] = (xr * xr + xi * xi) * mask[e];
+            for (int r = 0; r < p; ++r) {
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const float2 x = G[r * cs + bb[u]], w = twT[r * cs + aa[u]];
+                    xr[u] = fmaf(x.x, w.x, fmaf(-x.y, w.y, xr[u]));
+                    xi[u] = fmaf(x.x, w.y, fmaf(x.y, w.x, xi[u]));
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kU; ++u)
+                if (e0 + 32 * u < cs * cs) {
+                    const int e = aa[u] * cs + bb[u];
+                    I[e] = (xr[u] * xr[u] + xi[u] * xi[u]) * mask[e];
+                }
         }
         __syncwarp();
-        // LCM area rebin, separable (toccd.py:55-61)
+        // LCM area rebin, separable (toccd.py:55-61): H = I R^T, D = R H
         for (int e = lane; e < cs * npx; e += 32) {
             const int aa = e / npx, q = e - aa * npx;
             float acc = 0.f;
