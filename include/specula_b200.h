@@ -180,6 +180,11 @@ typedef struct sb_iir_plan {
     float *ist;             /* [n][2] */
     float *ost;             /* [n][2] */
     float *state;           /* [n][total] */
+    float *out_next;        /* optional [n]: the output the NEXT step will
+                               emit (state[:, k_out-1] after this update),
+                               for integer delays >= 1; NULL to skip.  Lets a
+                               caller start the next step's DM projection
+                               before that step's integrator runs.          */
 } sb_iir_plan;
 
 int sb_integrator(const sb_iir_plan *plan, const float *delta, float *out, void *stream);

@@ -42,7 +42,7 @@ class SlopecPlan(C.Structure):
 class IirPlan(C.Structure):
     _fields_ = [('n', C.c_int), ('total', C.c_int), ('shift', C.c_int), ('k_out', C.c_int),
                 ('rem', C.c_float), ('one_minus_rem', C.c_float),
-                ('num', fp), ('den', fp), ('ist', fp), ('ost', fp), ('state', fp)]
+                ('num', fp), ('den', fp), ('ist', fp), ('ost', fp), ('state', fp), ('out_next', fp)]
 
 
 class AtmoLayer(C.Structure):

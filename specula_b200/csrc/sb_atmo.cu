@@ -50,7 +50,6 @@ __global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgs a) {
     const float w0 = __fsub_rn(1.0f, frac);
     const int k = ly.rot90;
     const int x0 = blockIdx.x * kTile, y0 = blockIdx.y * kTile;
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
 
     // footprint [br0, br1] x [bc0, bc1] in the rot90'd layer
     int br0 = y0, br1 = min(y0 + kTile, L) - 1, bc0 = x0, bc1 = min(x0 + kTile, L) - 1;
@@ -74,19 +73,25 @@ __global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgs a) {
         bc1 = min(bc1, bc0 + kBox - 1);
     }
     const int R = br1 - br0 + 1, Cc = bc1 - bc0 + 1;
-    for (int idx = tid; idx < R * Cc; idx += 256) {
-        int ra, cb;
-        if (k & 1) { ra = idx % R; cb = idx / R; } else { cb = idx % Cc; ra = idx / Cc; }
-        const int yy = br0 + ra, xx = bc0 + cb;
-        int sr, sc;   // screen row / column of rot90(lerped)[yy][xx] (atmo_evolution.py:291)
-        switch (k) {
-            case 1: sr = xx; sc = L - 1 - yy; break;
-            case 2: sr = L - 1 - yy; sc = L - 1 - xx; break;
-            case 3: sr = L - 1 - xx; sc = yy; break;
-            default: sr = yy; sc = xx;
+    // thread (tx, ty) of the 32 x 8 block walks the footprint so that tx
+    // always runs along the screen's columns: along the footprint's columns
+    // for even k, along its rows for odd k (rot90 swaps the axes)
+    const bool odd = k & 1;
+    const int n_fast = odd ? R : Cc, n_slow = odd ? Cc : R;
+    for (int sl = threadIdx.y; sl < n_slow; sl += blockDim.y) {
+        for (int fa = threadIdx.x; fa < n_fast; fa += blockDim.x) {
+            const int ra = odd ? fa : sl, cb = odd ? sl : fa;
+            const int yy = br0 + ra, xx = bc0 + cb;
+            int sr, sc;   // screen row / column of rot90(lerped)[yy][xx] (atmo_evolution.py:291)
+            switch (k) {
+                case 1: sr = xx; sc = L - 1 - yy; break;
+                case 2: sr = L - 1 - yy; sc = L - 1 - xx; break;
+                case 3: sr = L - 1 - xx; sc = yy; break;
+                default: sr = yy; sc = xx;
+            }
+            const float *p = row0 + (size_t)sr * ld + sc;
+            Q[ra][cb] = __fadd_rn(__fmul_rn(w0, p[0]), __fmul_rn(frac, p[1]));
         }
-        const float *p = row0 + (size_t)sr * ld + sc;
-        Q[ra][cb] = __fadd_rn(__fmul_rn(w0, p[0]), __fmul_rn(frac, p[1]));
     }
     __syncthreads();
     const int x = x0 + threadIdx.x;

@@ -67,6 +67,7 @@ __global__ void integrator_kernel(sb_iir_plan p, const float *__restrict__ delta
         o = __fadd_rn(__fmul_rn(p.rem, st[p.k_out]), __fmul_rn(p.one_minus_rem, st[p.k_out - 1]));
     }
     out[e] = o;
+    if (p.out_next) p.out_next[e] = st[p.k_out - 1];
 }
 
 // phase[idx[p]] = sum_m c[m] * IF[m][p]; CTA = 8 warps sharing a strip of
@@ -159,6 +160,8 @@ extern "C" int sb_integrator(const sb_iir_plan *p, const float *delta, float *ou
         return sb::fail(SB_EINVAL, "sb_integrator: null pointer");
     if (p->n < 0 || p->total < 1 || p->k_out < 0 || p->k_out >= p->total || (p->rem != 0.f && p->k_out < 1))
         return sb::fail(SB_EINVAL, "sb_integrator: bad state layout");
+    if (p->out_next && (p->rem != 0.f || p->k_out < 1))
+        return sb::fail(SB_EINVAL, "sb_integrator: out_next needs an integer delay >= 1");
     if (p->n == 0) return SB_OK;
     integrator_kernel<<<(p->n + 127) / 128, 128, 0, sb::as_stream(stream)>>>(*p, delta, out);
     return sb::check_launch("integrator_kernel");

@@ -65,14 +65,19 @@ class AtmoPropagation(BaseProcessingObj):
                 if layer.size[0] < self.pixel_pupil or layer.size[1] < self.pixel_pupil:
                     raise ValueError(f'AtmoPropagation: layer {layer.size} smaller than the pupil')
 
-    def _descriptors(self):
+    def _descriptors(self, phase_override=None):
         arr = (_lib.PropLayer * len(self._layers))()
         P = self.pixel_pupil
         for k, layer in enumerate(self._layers):
             d = arr[k]
             unit = getattr(layer, '_unit_amplitude', False)
             d.A = None if unit else layer.A.data_ptr()
-            d.phase = layer.phaseInNm.data_ptr()
+            ph = layer.phaseInNm
+            if phase_override and id(layer) in phase_override:
+                ph = phase_override[id(layer)]
+                if ph.shape != layer.phaseInNm.shape or ph.stride() != layer.phaseInNm.stride():
+                    raise ValueError('AtmoPropagation: phase override must match the layer layout')
+            d.phase = ph.data_ptr()
             d.ld = layer.phaseInNm.stride(0)
             if not unit and layer.A.stride(0) != d.ld:
                 raise ValueError('AtmoPropagation: layer amplitude and phase must share a row stride')
@@ -80,8 +85,11 @@ class AtmoPropagation(BaseProcessingObj):
             d.left = (layer.size[1] - P) // 2
         return arr
 
-    def trigger_code(self):
-        arr = self._descriptors()
+    def trigger_code(self, phase_override=None):
+        """``phase_override``: {id(layer): tensor} reads another buffer in place
+        of a layer's phase (used for the double-buffered DM of the pipelined
+        loop graph)."""
+        arr = self._descriptors(phase_override)
         for name in self.source_dict:
             ef = self.outputs['out_' + name + '_ef']
             _lib.call('sb_propagate_on_axis', arr, len(self._layers), self.pixel_pupil, ef.A.data_ptr(),

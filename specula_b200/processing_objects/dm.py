@@ -74,7 +74,10 @@ class DM(BaseProcessingObj):
             self._cmd = torch.zeros(self._m2c.shape[0], dtype=torch.float32, device=self.device)
 
     def trigger_code(self):
-        c = self.local_inputs['in_command'].value
+        self.project(self.local_inputs['in_command'].value, self.layer.phaseInNm)
+
+    def project(self, c, out_phase):
+        """phase[mask] = (sign * m2c @ c) @ IF into ``out_phase`` (pix x pix)."""
         if not isinstance(c, torch.Tensor) or c.device != self.device or c.dtype != torch.float32:
             c = torch.as_tensor(c, dtype=torch.float32, device=self.device)
         if self.nmodes is not None:
@@ -86,9 +89,10 @@ class DM(BaseProcessingObj):
             _lib.call('sb_modalrec', self._m2c.data_ptr(), self._m2c.shape[0], self._m2c.shape[1],
                       self._m2c.stride(0), self.m2c_commands.data_ptr(), self._cmd.data_ptr(), st)
             c = self._cmd
+        if out_phase.shape != self.layer.phaseInNm.shape or not out_phase.is_contiguous():
+            raise ValueError('DM.project: output must be a contiguous array shaped like the layer')
         _lib.call('sb_dm_project', self._IF.data_ptr(), self._IF.shape[0], int(self._idx.numel()), self._ld,
-                  c.data_ptr(), int(c.numel()), float(self.sign), self._idx.data_ptr(),
-                  self.layer.phaseInNm.data_ptr(), st)
+                  c.data_ptr(), int(c.numel()), float(self.sign), self._idx.data_ptr(), out_phase.data_ptr(), st)
 
     def post_trigger(self):
         self.layer.generation_time = self.current_time

@@ -54,14 +54,30 @@ class IirFilter(BaseProcessingObj):
         self._plan = _lib.IirPlan(n=self._n, total=self._total_length, shift=int(self.delay > 0), k_out=k_out,
                                   rem=float(np.float32(rem)), one_minus_rem=float(np.float32(1 - rem)),
                                   num=self._num.data_ptr(), den=self._den.data_ptr(), ist=self._ist.data_ptr(),
-                                  ost=self._ost.data_ptr(), state=self.state.data_ptr())
+                                  ost=self._ost.data_ptr(), state=self.state.data_ptr(), out_next=None)
 
-    def trigger_code(self):
+    @property
+    def next_output_available(self):
+        """True when the next step's output is known one step ahead
+        (integer delay >= 1), see trigger_code(out_next=...)."""
+        return self.delay % 1 == 0 and self.delay >= 1
+
+    def next_output(self):
+        """The output the next step will emit, from the current state."""
+        return self.state[:, int(self.delay) - 1]
+
+    def trigger_code(self, out_next=None):
+        """One filter step; with ``out_next`` (a float32 device vector) the
+        kernel also writes the output of the following step."""
         d = self.local_inputs['delta_comm'].value
         if not isinstance(d, torch.Tensor) or d.device != self.device or d.dtype != torch.float32:
             d = torch.as_tensor(d, dtype=torch.float32, device=self.device)
-        _lib.call('sb_integrator', _byref(self._plan), d.contiguous().data_ptr(),
-                  self.out_comm.value.data_ptr(), self.stream_handle())
+        self._plan.out_next = None if out_next is None else out_next.data_ptr()
+        try:
+            _lib.call('sb_integrator', _byref(self._plan), d.contiguous().data_ptr(),
+                      self.out_comm.value.data_ptr(), self.stream_handle())
+        finally:
+            self._plan.out_next = None
 
     def post_trigger(self):
         self.out_comm.generation_time = self.current_time

@@ -155,6 +155,8 @@ class ScaoLoop:
         for k, o in enumerate(self.objects):
             self.loop.add(o, k)
         self.graph = None
+        self.pipelined = False
+        self.steps_per_replay = 1
         self.n_valid_subaps = len(idxs)
         self.n_valid_pixels = nv
 
@@ -170,25 +172,68 @@ class ScaoLoop:
             v.generation_time = t
         self.loop.iter()
 
-    def capture(self):
-        """Capture one whole step (every object's trigger_code) in a CUDA
-        graph.  Call after at least one eager step, so the time step used by
-        AtmoEvolution is the loop's (the first step has delta_time = 0)."""
+    def capture(self, pipelined=True):
+        """Capture whole steps in a CUDA graph.  Call after at least one eager
+        step, so the time step used by AtmoEvolution is the loop's (the first
+        step has delta_time = 0).
+
+        Sequential form: one step, every object's trigger_code in trigger order.
+
+        Pipelined form (integer integrator delay >= 1): the DM command of step
+        t is the integrator output computed at step t-delay, known when step t
+        starts, so the DM projection of step t (HBM-bound) runs on a second
+        stream concurrently with AtmoEvolution..Integrator of step t
+        (latency-bound).  The DM phase is double-buffered: step t writes
+        buffer t%2 while the propagation of step t reads buffer (t-1)%2,
+        which is the reference's ``dm.out_layer:-1`` input.  The graph holds
+        two steps so the buffers alternate statically; after each replay the
+        DM layer tensor holds the latest DM phase, as in the sequential form.
+        """
         self.step_eager()
         torch.cuda.synchronize(self.device)
         self.atmo.delta_time = self.atmo.t_to_seconds(self.loop._dt)
         g = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(g):
-            for o in self.objects:
-                o.trigger_code()
+        self.pipelined = bool(pipelined and self.integ.next_output_available)
+        if not self.pipelined:
+            with torch.cuda.graph(g):
+                for o in self.objects:
+                    o.trigger_code()
+            self.steps_per_replay = 1
+        else:
+            dm_buf = [self.dm.layer.phaseInNm, torch.empty_like(self.dm.layer.phaseInNm)]
+            dm_buf[1].copy_(dm_buf[0])
+            nxt = [torch.empty_like(self.integ.out_comm.value) for _ in range(2)]
+            # after the eager step t0 (even), step t0+1 will emit state[:, delay-1]
+            nxt[1].copy_(self.integ.next_output())
+            side = torch.cuda.Stream(self.device)
+            self._side = side
+            self._bufs = (dm_buf, nxt)
+            chain = [self.atmo, self.prop, self.sh, self.ccd, self.slopec, self.rec]
+            with torch.cuda.graph(g):
+                main = torch.cuda.current_stream(self.device)
+                for par in (1, 0):              # odd step, then even step
+                    side.wait_stream(main)
+                    with torch.cuda.stream(side):
+                        self.dm.project(nxt[par], dm_buf[par])
+                    for o in chain:
+                        if o is self.prop:
+                            o.trigger_code(phase_override={id(self.dm.layer): dm_buf[1 - par]})
+                        else:
+                            o.trigger_code()
+                    self.integ.trigger_code(out_next=nxt[1 - par])
+                    main.wait_stream(side)
+            self.steps_per_replay = 2
         torch.cuda.synchronize(self.device)
         self.graph = g
         return g
 
     def replay(self):
+        """Run the captured graph: ``steps_per_replay`` loop steps."""
         self.graph.replay()
 
-    # kernels launched by one captured step (for the launch count)
+    # kernels launched by one step (for the launch count): atmo advance +
+    # evolve, propagate, SH forward + normalise, CCD, slopes (2), modal
+    # reconstructor, integrator, DM projection
     KERNELS_PER_STEP = 11
 
 
