@@ -70,71 +70,94 @@ __global__ void integrator_kernel(sb_iir_plan p, const float *__restrict__ delta
     if (p.out_next) p.out_next[e] = st[p.k_out - 1];
 }
 
-// phase[idx[p]] = sum_m c[m] * IF[m][p]; CTA = 8 warps sharing a strip of
-// 32*W columns, warp w takes modes w, w+8, ...; partial strips are reduced
-// across warps in shared memory (fixed order).  W = 4 (float4) when the rows
-// are 16-byte aligned, else 1.
+// phase[idx[p]] = sum_m c[m] * IF[m][p].
+// Persistent kernel: one 512-thread CTA per SM walks column tiles of
+// 32*W pixels (tile += gridDim.x).  Inside a tile the 16 warps split the
+// modes (warp w takes w, w+16, ...), each lane keeps W columns, and 8 rows
+// are loaded back to back so 8 x 16 bytes are in flight per thread
+// (~9.7 MB GPU-wide, enough to cover HBM latency).  Partial tiles are
+// reduced across warps in shared memory in a fixed order.  Holding one CTA
+// per SM leaves room on every SM for kernels running concurrently on other
+// streams (the SH chain of the pipelined loop step).
+constexpr int kDmWarps = 16;
+constexpr int kDmUnroll = 8;
+
 template <int W>
-__global__ void __launch_bounds__(256) dm_project_kernel(const float *__restrict__ IF, int nmodes, int nvalid,
-                                                         int ld, const float *__restrict__ cmd, int ncmd, float sign,
-                                                         const int32_t *__restrict__ idx,
-                                                         float *__restrict__ phase) {
+__global__ void __launch_bounds__(32 * kDmWarps, 2) dm_project_kernel(const float *__restrict__ IF, int nmodes,
+                                                                      int nvalid, int ld,
+                                                                      const float *__restrict__ cmd, int ncmd,
+                                                                      float sign, const int32_t *__restrict__ idx,
+                                                                      float *__restrict__ phase) {
     extern __shared__ float sm[];
-    float *c = sm;                     // nmodes
-    float *part = sm + nmodes;         // 8 warps x 32*W
+    float *c = sm;                               // nmodes (sign applied)
+    float *part = sm + ((nmodes + 3) & ~3);      // kDmWarps x 32*W
     for (int m = threadIdx.x; m < nmodes; m += blockDim.x) c[m] = m < ncmd ? sign * cmd[m] : 0.f;
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int col0 = blockIdx.x * 32 * W + lane * W;
-    float acc[W];
+    const int ntiles = (nvalid + 32 * W - 1) / (32 * W);
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int col0 = tile * 32 * W + lane * W;
+        float acc[W];
 #pragma unroll
-    for (int k = 0; k < W; ++k) acc[k] = 0.f;
-    if (col0 < nvalid) {
+        for (int k = 0; k < W; ++k) acc[k] = 0.f;
         if (W == 4 && col0 + 3 < nvalid) {
             const float *base = IF + col0;
             int m = warp;
-            for (; m + 24 < nmodes; m += 32) {
-                const float4 v0 = __ldg(reinterpret_cast<const float4 *>(base + (size_t)m * ld));
-                const float4 v1 = __ldg(reinterpret_cast<const float4 *>(base + (size_t)(m + 8) * ld));
-                const float4 v2 = __ldg(reinterpret_cast<const float4 *>(base + (size_t)(m + 16) * ld));
-                const float4 v3 = __ldg(reinterpret_cast<const float4 *>(base + (size_t)(m + 24) * ld));
-                const float c0 = c[m], c1 = c[m + 8], c2 = c[m + 16], c3 = c[m + 24];
-                acc[0] = fmaf(c0, v0.x, acc[0]); acc[1] = fmaf(c0, v0.y, acc[1]);
-                acc[2] = fmaf(c0, v0.z, acc[2]); acc[3] = fmaf(c0, v0.w, acc[3]);
-                acc[0] = fmaf(c1, v1.x, acc[0]); acc[1] = fmaf(c1, v1.y, acc[1]);
-                acc[2] = fmaf(c1, v1.z, acc[2]); acc[3] = fmaf(c1, v1.w, acc[3]);
-                acc[0] = fmaf(c2, v2.x, acc[0]); acc[1] = fmaf(c2, v2.y, acc[1]);
-                acc[2] = fmaf(c2, v2.z, acc[2]); acc[3] = fmaf(c2, v2.w, acc[3]);
-                acc[0] = fmaf(c3, v3.x, acc[0]); acc[1] = fmaf(c3, v3.y, acc[1]);
-                acc[2] = fmaf(c3, v3.z, acc[2]); acc[3] = fmaf(c3, v3.w, acc[3]);
+            for (; m + (kDmUnroll - 1) * kDmWarps < nmodes; m += kDmUnroll * kDmWarps) {
+                float4 v[kDmUnroll];
+#pragma unroll
+                for (int u = 0; u < kDmUnroll; ++u)
+                    v[u] = __ldg(reinterpret_cast<const float4 *>(base + (size_t)(m + u * kDmWarps) * ld));
+#pragma unroll
+                for (int u = 0; u < kDmUnroll; ++u) {
+                    const float cm = c[m + u * kDmWarps];
+                    acc[0] = fmaf(cm, v[u].x, acc[0]);
+                    acc[1] = fmaf(cm, v[u].y, acc[1]);
+                    acc[2] = fmaf(cm, v[u].z, acc[2]);
+                    acc[3] = fmaf(cm, v[u].w, acc[3]);
+                }
             }
-            for (; m < nmodes; m += 8) {
+            for (; m < nmodes; m += kDmWarps) {
                 const float4 v = __ldg(reinterpret_cast<const float4 *>(base + (size_t)m * ld));
                 const float cm = c[m];
-                acc[0] = fmaf(cm, v.x, acc[0]); acc[1] = fmaf(cm, v.y, acc[1]);
-                acc[2] = fmaf(cm, v.z, acc[2]); acc[3] = fmaf(cm, v.w, acc[3]);
+                acc[0] = fmaf(cm, v.x, acc[0]);
+                acc[1] = fmaf(cm, v.y, acc[1]);
+                acc[2] = fmaf(cm, v.z, acc[2]);
+                acc[3] = fmaf(cm, v.w, acc[3]);
             }
-        } else {
-            for (int m = warp; m < nmodes; m += 8) {
+        } else if (col0 < nvalid) {
+            for (int m = warp; m < nmodes; m += kDmWarps) {
                 const float cm = c[m];
 #pragma unroll
                 for (int k = 0; k < W; ++k)
                     if (col0 + k < nvalid) acc[k] = fmaf(cm, __ldg(IF + (size_t)m * ld + col0 + k), acc[k]);
             }
         }
-    }
 #pragma unroll
-    for (int k = 0; k < W; ++k) part[warp * 32 * W + lane * W + k] = acc[k];
-    __syncthreads();
-    for (int t = threadIdx.x; t < 32 * W; t += blockDim.x) {
-        const int col = blockIdx.x * 32 * W + t;
-        if (col < nvalid) {
-            float s = 0.f;
+        for (int k = 0; k < W; ++k) part[warp * 32 * W + lane * W + k] = acc[k];
+        __syncthreads();
+        for (int t = threadIdx.x; t < 32 * W; t += blockDim.x) {
+            const int col = tile * 32 * W + t;
+            if (col < nvalid) {
+                float s = 0.f;
 #pragma unroll
-            for (int w = 0; w < 8; ++w) s += part[w * 32 * W + t];
-            phase[idx[col]] = s;
+                for (int w = 0; w < kDmWarps; ++w) s += part[w * 32 * W + t];
+                phase[idx[col]] = s;
+            }
         }
+        __syncthreads();
     }
+}
+
+int sm_count() {
+    static int n = 0;
+    if (n == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
 }
 
 }  // namespace
@@ -177,17 +200,20 @@ extern "C" int sb_dm_project(const float *ifunc, int n_modes, int n_valid, int l
     cudaStream_t st = sb::as_stream(stream);
     const bool vec = (ld_if % 4 == 0) && ((uintptr_t)ifunc % 16 == 0);
     const int W = vec ? 4 : 1;
-    const size_t smem = (size_t)(n_modes + 8 * 32 * W) * sizeof(float);
+    const size_t smem = (size_t)(((n_modes + 3) & ~3) + kDmWarps * 32 * W) * sizeof(float);
     if (smem > 200 * 1024) return sb::fail(SB_ESHAPE, "sb_dm_project: too many modes (%d)", n_modes);
-    const int nblk = (n_valid + 32 * W - 1) / (32 * W);
+    const int ntiles = (n_valid + 32 * W - 1) / (32 * W);
+    const int nblk = ntiles < sm_count() ? ntiles : sm_count();
     if (vec) {
         if (smem > 48 * 1024)
             cudaFuncSetAttribute(dm_project_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        dm_project_kernel<4><<<nblk, 256, smem, st>>>(ifunc, n_modes, n_valid, ld_if, cmd, n_cmd, sign, mask_idx, phase);
+        dm_project_kernel<4><<<nblk, 32 * kDmWarps, smem, st>>>(ifunc, n_modes, n_valid, ld_if, cmd, n_cmd, sign,
+                                                                mask_idx, phase);
     } else {
         if (smem > 48 * 1024)
             cudaFuncSetAttribute(dm_project_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        dm_project_kernel<1><<<nblk, 256, smem, st>>>(ifunc, n_modes, n_valid, ld_if, cmd, n_cmd, sign, mask_idx, phase);
+        dm_project_kernel<1><<<nblk, 32 * kDmWarps, smem, st>>>(ifunc, n_modes, n_valid, ld_if, cmd, n_cmd, sign,
+                                                                mask_idx, phase);
     }
     return sb::check_launch("dm_project_kernel");
 }

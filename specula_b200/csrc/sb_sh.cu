@@ -191,6 +191,187 @@ __global__ void __launch_bounds__(256, 4) sh_forward_kernel(ShArgs a) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Compile-time-sized variant for the common geometries.  Same math as
+// sh_forward_kernel; every DFT product is a small complex matrix product
+// computed by the warp with a register block of RB x CB outputs per lane
+// (operands loaded once per k and reused RB*CB times), loops unrolled.
+// ---------------------------------------------------------------------------
+
+// cost of an RB x CB block for an M x N output (infeasible: huge)
+__host__ __device__ constexpr int blk_cost(int M, int N, int rb, int cb) {
+    return (M % rb || N % cb || (M / rb) * (N / cb) > 32) ? 1 << 20 : rb * cb * 64 + rb + cb;
+}
+__host__ __device__ constexpr int best_rb(int M, int N) {
+    int best = 1, bestc = 1 << 30;
+    for (int rb = 1; rb <= M; ++rb)
+        for (int cb = 1; cb <= N; ++cb)
+            if (blk_cost(M, N, rb, cb) < bestc) { bestc = blk_cost(M, N, rb, cb); best = rb; }
+    return best;
+}
+__host__ __device__ constexpr int best_cb(int M, int N) {
+    int best = 1, bestc = 1 << 30;
+    for (int rb = 1; rb <= M; ++rb)
+        for (int cb = 1; cb <= N; ++cb)
+            if (blk_cost(M, N, rb, cb) < bestc) { bestc = blk_cost(M, N, rb, cb); best = cb; }
+    return best;
+}
+
+// C(M x N) = A(M x K) * B(K x N), complex, A(i,k) = A[i*SAI + k*SAK],
+// B(k,j) = B[k*SBK + j]; each result goes to store(i, j, re, im).
+template <int M, int N, int K, int SAI, int SAK, int SBK, typename Store>
+__device__ __forceinline__ void warp_cgemm(const float2 *A, const float2 *B, int lane, Store store) {
+    constexpr int RB = best_rb(M, N), CB = best_cb(M, N);
+    constexpr int NBC = N / CB;
+    if (lane < (M / RB) * NBC) {
+        const int i0 = (lane / NBC) * RB, j0 = (lane % NBC) * CB;
+        float xr[RB][CB], xi[RB][CB];
+#pragma unroll
+        for (int i = 0; i < RB; ++i)
+#pragma unroll
+            for (int j = 0; j < CB; ++j) xr[i][j] = xi[i][j] = 0.f;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            float2 av[RB], bv[CB];
+#pragma unroll
+            for (int i = 0; i < RB; ++i) av[i] = A[(i0 + i) * SAI + k * SAK];
+#pragma unroll
+            for (int j = 0; j < CB; ++j) bv[j] = B[k * SBK + j0 + j];
+#pragma unroll
+            for (int i = 0; i < RB; ++i)
+#pragma unroll
+                for (int j = 0; j < CB; ++j) {
+                    xr[i][j] = fmaf(av[i].x, bv[j].x, fmaf(-av[i].y, bv[j].y, xr[i][j]));
+                    xi[i][j] = fmaf(av[i].x, bv[j].y, fmaf(av[i].y, bv[j].x, xi[i][j]));
+                }
+        }
+#pragma unroll
+        for (int i = 0; i < RB; ++i)
+#pragma unroll
+            for (int j = 0; j < CB; ++j) store(i0 + i, j0 + j, xr[i][j], xi[i][j]);
+    }
+}
+
+template <int P, int CS, int NPX>
+__global__ void __launch_bounds__(256, 4) sh_forward_fixed_kernel(ShArgs a) {
+    constexpr int PE = P + 1;
+    __shared__ float2 twT[P * CS];          // twT[c][b] = W[b][c]
+    __shared__ float2 tilt[P * P];
+    __shared__ float mask[CS * CS];
+    __shared__ float R[NPX * CS];
+    __shared__ float2 Es[8][P * PE];
+    __shared__ float2 Gs[8][P * CS > (CS * NPX + 1) / 2 ? P * CS : (CS * NPX + 1) / 2];
+    __shared__ float Is[8][CS * CS];
+    __shared__ float red[33];
+    for (int e = threadIdx.x; e < CS * P; e += blockDim.x) {
+        const int b = e / P, c = e - b * P;
+        twT[c * CS + b] = a.tw[e];
+    }
+    for (int e = threadIdx.x; e < P * P; e += blockDim.x) tilt[e] = a.tilt[e];
+    for (int e = threadIdx.x; e < CS * CS; e += blockDim.x) mask[e] = a.mask[e];
+    for (int e = threadIdx.x; e < NPX * CS; e += blockDim.x) R[e] = a.rebin[e];
+    __syncthreads();
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.y;
+    const int j = blockIdx.x * a.spc + warp;
+    float2 *E = Es[warp];
+    float2 *G = Gs[warp];
+    float *I = Is[warp];
+    float local = 0.f;
+    if (j < a.n) {
+        const size_t row0 = (size_t)i * P, col0 = (size_t)j * P;
+#pragma unroll
+        for (int e = lane; e < P * P; e += 32) {
+            const int r = e / P, c = e % P;
+            const size_t g = (row0 + r) * (size_t)a.ld + col0 + c;
+            const float amp = a.A[g];
+            const float phi = a.ph[g] * a.k;
+            float sn, co;
+            sincosf(phi, &sn, &co);
+            const float re = co * amp, im = sn * amp;
+            const float2 t = tilt[e];
+            E[r * PE + c] = make_float2(re * t.x - im * t.y, re * t.y + im * t.x);
+        }
+        __syncwarp();
+        // G = E W^T  (P x CS)
+        warp_cgemm<P, CS, P, PE, 1, CS>(E, twT, lane, [&](int r, int b, float xr, float xi) {
+            G[r * CS + b] = make_float2(xr, xi);
+        });
+        __syncwarp();
+        // F = W G  (CS x CS); I = |F|^2 * field stop  (sh.py:378-399)
+        warp_cgemm<CS, CS, P, 1, CS, CS>(twT, G, lane, [&](int aa, int b, float xr, float xi) {
+            I[aa * CS + b] = (xr * xr + xi * xi) * mask[aa * CS + b];
+        });
+        __syncwarp();
+        const int out_ld = a.n * NPX;
+        if constexpr (CS % NPX == 0) {
+            // integer rebin factor: each detector pixel is a BF x BF box of
+            // the cut window, weighted 1/BF^2 (R holds 1/BF on its band)
+            constexpr int BF = CS / NPX;
+            const float wgt = R[0] * R[0];
+#pragma unroll
+            for (int e = lane; e < NPX * NPX; e += 32) {
+                const int pp = e / NPX, q = e % NPX;
+                float acc = 0.f;
+#pragma unroll
+                for (int u = 0; u < BF; ++u)
+#pragma unroll
+                    for (int v = 0; v < BF; ++v) acc += I[(pp * BF + u) * CS + q * BF + v];
+                acc *= wgt;
+                a.out[((size_t)i * NPX + pp) * out_ld + (size_t)j * NPX + q] = acc;
+                local += acc;
+            }
+        } else {
+            // general LCM rebin (toccd.py:55-61): H = I R^T, D = R H
+            float *H = reinterpret_cast<float *>(G);   // G is consumed
+#pragma unroll
+            for (int e = lane; e < CS * NPX; e += 32) {
+                const int aa = e / NPX, q = e % NPX;
+                float acc = 0.f;
+#pragma unroll
+                for (int b = 0; b < CS; ++b) acc = fmaf(I[aa * CS + b], R[q * CS + b], acc);
+                H[e] = acc;
+            }
+            __syncwarp();
+#pragma unroll
+            for (int e = lane; e < NPX * NPX; e += 32) {
+                const int pp = e / NPX, q = e % NPX;
+                float acc = 0.f;
+#pragma unroll
+                for (int aa = 0; aa < CS; ++aa) acc = fmaf(R[pp * CS + aa], H[aa * NPX + q], acc);
+                a.out[((size_t)i * NPX + pp) * out_ld + (size_t)j * NPX + q] = acc;
+                local += acc;
+            }
+        }
+    }
+    const int bid = blockIdx.y * gridDim.x + blockIdx.x;
+    const float tot = sb::block_sum(local, red);
+    const int nblk = gridDim.x * gridDim.y;
+    const int chunk = (a.n_norm + nblk - 1) / nblk;
+    const int lo = bid * chunk;
+    const int hi = min(a.n_norm, lo + chunk);
+    float sa = 0.f;
+    for (int e = lo + threadIdx.x; e < hi; e += blockDim.x) sa += a.A_norm[e];
+    const float tota = sb::block_sum(sa, red);
+    if (threadIdx.x == 0) {
+        a.part_I[bid] = tot;
+        a.part_A[bid] = tota;
+    }
+}
+
+typedef void (*ShKernel)(ShArgs);
+
+// geometries with a compile-time kernel: (np_sub, cutsize, subap_npx)
+ShKernel fixed_kernel(int p, int cs, int npx) {
+    if (p == 8 && cs == 12 && npx == 6) return sh_forward_fixed_kernel<8, 12, 6>;
+    if (p == 8 && cs == 14 && npx == 8) return sh_forward_fixed_kernel<8, 14, 8>;
+    if (p == 8 && cs == 16 && npx == 8) return sh_forward_fixed_kernel<8, 16, 8>;
+    if (p == 8 && cs == 8 && npx == 8) return sh_forward_fixed_kernel<8, 8, 8>;
+    if (p == 16 && cs == 16 && npx == 8) return sh_forward_fixed_kernel<16, 16, 8>;
+    return nullptr;
+}
+
 __global__ void __launch_bounds__(256) sh_normalize_kernel(const float *part_I, const float *part_A, int nparts,
                                                            float photon_scale, float *out, int n_out) {
     __shared__ double red[33];
@@ -303,11 +484,18 @@ extern "C" int sb_sh_forward(const sb_sh_plan *pl, const float *A, const float *
     a.part_I = static_cast<float *>(scratch);
     a.part_A = static_cast<float *>(scratch) + nb;
     cudaStream_t st = sb::as_stream(stream);
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(sh_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return sb::fail(SB_ECUDA, "sb_sh_forward: smem attribute: %s", cudaGetErrorString(e));
+    ShKernel fk = (spc == 8 || spc == pl->n_lenses) ? fixed_kernel(a.p, a.cs, a.npx) : nullptr;
+    if (fk) {
+        fk<<<grid, 32 * spc, 0, st>>>(a);
+    } else {
+        if (smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(sh_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem);
+            if (e != cudaSuccess)
+                return sb::fail(SB_ECUDA, "sb_sh_forward: smem attribute: %s", cudaGetErrorString(e));
+        }
+        sh_forward_kernel<<<grid, 32 * spc, smem, st>>>(a);
     }
-    sh_forward_kernel<<<grid, 32 * spc, smem, st>>>(a);
     int rc = sb::check_launch("sh_forward_kernel");
     if (rc) return rc;
     const int n_out = pl->n_lenses * pl->subap_npx * pl->n_lenses * pl->subap_npx;

@@ -205,11 +205,16 @@ class ScaoLoop:
             nxt = [torch.empty_like(self.integ.out_comm.value) for _ in range(2)]
             # after the eager step t0 (even), step t0+1 will emit state[:, delay-1]
             nxt[1].copy_(self.integ.next_output())
-            side = torch.cuda.Stream(self.device)
+            # the chain is latency-bound and on the critical path: capture it
+            # on a high-priority stream; the DM projection (HBM-bound, one
+            # CTA per SM) runs on a low-priority side stream
+            side = torch.cuda.Stream(self.device, priority=0)
+            cap = torch.cuda.Stream(self.device, priority=-1)
             self._side = side
+            self._cap = cap
             self._bufs = (dm_buf, nxt)
             chain = [self.atmo, self.prop, self.sh, self.ccd, self.slopec, self.rec]
-            with torch.cuda.graph(g):
+            with torch.cuda.graph(g, stream=cap):
                 main = torch.cuda.current_stream(self.device)
                 for par in (1, 0):              # odd step, then even step
                     side.wait_stream(main)
