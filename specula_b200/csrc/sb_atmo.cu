@@ -7,8 +7,8 @@
 // a sample outside [0, L-1] on either axis gives 0, otherwise bilinear from
 // the four neighbours, neighbours off the grid counting 0) and the r0 scale
 // (:294).  Float32 operations keep NumPy's order (no FMA contraction) and the
-// rotation coordinates and weights are computed in double like SciPy, so
-// results track the reference to the last bits.
+// rotation coordinates are computed in double like SciPy, so the boundary
+// and neighbour choices are the reference's; the bilinear blend is float32.
 #include "sb_common.cuh"
 
 namespace {
@@ -95,6 +95,9 @@ __global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgs a) {
     }
     __syncthreads();
     const int x = x0 + threadIdx.x;
+    const double xd = (double)x;
+    const double cx0 = __dmul_rn(ly.m01, xd), cx1 = __dmul_rn(ly.m11, xd);
+    const double Lm1 = (double)(L - 1);
     for (int yi = threadIdx.y; yi < kTile; yi += blockDim.y) {
         const int y = y0 + yi;
         if (x >= L || y >= L) continue;
@@ -102,22 +105,29 @@ __global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgs a) {
         if (!ly.rotate) {
             v = Q[y - br0][x - bc0];
         } else {
-            // scipy.ndimage.rotate(order=1, mode='constant'): samples outside
-            // [0, L-1] give 0; neighbours off the grid count 0
-            const double ir = __dadd_rn(__dadd_rn(__dmul_rn(ly.m00, (double)y), __dmul_rn(ly.m01, (double)x)), ly.off0);
-            const double ic = __dadd_rn(__dadd_rn(__dmul_rn(ly.m10, (double)y), __dmul_rn(ly.m11, (double)x)), ly.off1);
-            if (!(ir >= 0.0 && ir <= (double)(L - 1) && ic >= 0.0 && ic <= (double)(L - 1))) {
+            // scipy.ndimage.rotate(order=1, mode='constant'): a sample
+            // outside [0, L-1] gives 0, neighbours off the grid count 0.
+            // Coordinates in double with SciPy's operation order (the
+            // boundary and floor decisions are exact); the weights and the
+            // blend in float32, which is the output precision.
+            const double yd = (double)y;
+            const double ir = __dadd_rn(__dadd_rn(__dmul_rn(ly.m00, yd), cx0), ly.off0);
+            const double ic = __dadd_rn(__dadd_rn(__dmul_rn(ly.m10, yd), cx1), ly.off1);
+            if (!(ir >= 0.0 && ir <= Lm1 && ic >= 0.0 && ic <= Lm1)) {
                 v = 0.0f;
             } else {
-                const int r0 = (int)floor(ir), c0 = (int)floor(ic);
-                const double fr = ir - r0, fc = ic - c0;
-                const int r1 = r0 + 1, c1 = c0 + 1;
+                const double fr0 = floor(ir), fc0 = floor(ic);
+                const int r0 = (int)fr0, c0 = (int)fc0;
+                const float fr = (float)(ir - fr0), fc = (float)(ic - fc0);
                 const int qr = r0 - br0, qc = c0 - bc0;
-                const double q00 = Q[qr][qc];
-                const double q01 = c1 < L ? (double)Q[qr][qc + 1] : 0.0;
-                const double q10 = r1 < L ? (double)Q[qr + 1][qc] : 0.0;
-                const double q11 = (r1 < L && c1 < L) ? (double)Q[qr + 1][qc + 1] : 0.0;
-                v = (float)(q00 * (1 - fr) * (1 - fc) + q01 * (1 - fr) * fc + q10 * fr * (1 - fc) + q11 * fr * fc);
+                const bool rin = r0 + 1 < L, cin = c0 + 1 < L;
+                const float q00 = Q[qr][qc];
+                const float q01 = cin ? Q[qr][qc + 1] : 0.0f;
+                const float q10 = rin ? Q[qr + 1][qc] : 0.0f;
+                const float q11 = (rin && cin) ? Q[qr + 1][qc + 1] : 0.0f;
+                const float top = fmaf(fc, q01 - q00, q00);
+                const float bot = fmaf(fc, q11 - q10, q10);
+                v = fmaf(fr, bot - top, top);
             }
         }
         ly.out[(size_t)y * L + x] = __fmul_rn(v, ly.scale);   // atmo_evolution.py:294

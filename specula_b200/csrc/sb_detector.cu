@@ -100,7 +100,7 @@ __device__ __forceinline__ float std_normal(uint32_t e, uint64_t frame, uint64_t
     return sqrtf(-2.0f * logf(u01f(r.x))) * cospif(2.0f * u01f(r.y));
 }
 
-__global__ void __launch_bounds__(256) ccd_kernel(sb_ccd_params p, const float *__restrict__ in,
+__global__ void __launch_bounds__(256, 6) ccd_kernel(sb_ccd_params p, const float *__restrict__ in,
                                                   float *__restrict__ integ, float *__restrict__ pix) {
     // frame bookkeeping lives on the device; every block reads it before the
     // last block to finish advances it (see the end of the kernel)
