@@ -7,7 +7,7 @@
 #include <stdio.h>
 #include <stdint.h>
 
-#include "../../include/specula_b200.h"
+#include "specula_b200.h"
 
 namespace sb {
 
