@@ -77,6 +77,27 @@ int sb_sh_forward(const sb_sh_plan *plan, const float *A, const float *phase_nm,
                   const float *A_norm, int n_norm, float photon_scale, float *intensity,
                   void *scratch, size_t scratch_bytes, void *stream);
 
+/*
+ * No counterpart in the reference.  Same computation as sb_sh_forward, for
+ * callers that cannot allocate device memory: a real-time control thread
+ * that must not allocate once the loop runs, or a foreign-language binding
+ * that holds device buffers for its inputs and outputs but has no CUDA
+ * allocator of its own.  The caller still passes inputs and outputs; the
+ * scratch is a file-scope device array of SB_SH_STATIC_SCRATCH_BYTES bytes
+ * (every GPU that loads the library keeps it until the process exits).
+ * Geometries whose sb_sh_scratch_bytes() exceeds that size are rejected with
+ * SB_ESCRATCH.  The first call on a device resolves the array's device
+ * address (cudaGetSymbolAddress) with that device current; make that first
+ * call before any stream capture.  All calls share the array: the kernels
+ * overwrite every partial sum they read, so no clearing is needed, but calls
+ * that overlap on the GPU (different streams, or concurrent graphs) race on
+ * it and must be serialised by the caller.
+ */
+#define SB_SH_STATIC_SCRATCH_BYTES (64 * 1024)
+int sb_sh_forward_static(const sb_sh_plan *plan, const float *A, const float *phase_nm,
+                         const float *A_norm, int n_norm, float photon_scale, float *intensity,
+                         void *stream);
+
 /* replaces specula/lib/extrapolate_edge_pixel.py:4-28.
  * out[p] = phase[p] if src1[p] < 0; phase[src1[p]] if src2[p] < 0;
  * else 2*phase[src1[p]] - phase[src2[p]].  Tables from the host restatement

@@ -14,6 +14,7 @@ SB_OK = 0
 STATUS_NAMES = {0: 'SB_OK', -1: 'SB_EINVAL', -2: 'SB_ESHAPE', -3: 'SB_ECUDA', -4: 'SB_ESCRATCH',
                 -5: 'SB_ETIMEOUT', -6: 'SB_EUNSUPPORTED'}
 SB_MAX_LAYERS = 16
+SB_SH_STATIC_SCRATCH_BYTES = 64 * 1024
 
 vp = C.c_void_p
 fp = C.c_void_p   # device float*
@@ -62,6 +63,7 @@ SIGNATURES = {
     'sb_last_error': (C.c_char_p, []),
     'sb_sh_scratch_bytes': (C.c_size_t, [C.POINTER(ShPlan)]),
     'sb_sh_forward': (C.c_int, [C.POINTER(ShPlan), fp, fp, fp, C.c_int, C.c_float, fp, vp, C.c_size_t, vp]),
+    'sb_sh_forward_static': (C.c_int, [C.POINTER(ShPlan), fp, fp, fp, C.c_int, C.c_float, fp, vp]),
     'sb_edge_extrapolate': (C.c_int, [fp, ip, ip, C.c_int, fp, vp]),
     'sb_interp2d_field': (C.c_int, [fp, fp, C.c_int, C.c_int, fp, fp, C.c_int, fp, fp, vp]),
     'sb_ccd_step': (C.c_int, [C.POINTER(CcdParams), fp, fp, fp, vp]),

@@ -530,3 +530,55 @@ extern "C" int sb_interp2d_field(const float *A_in, const float *phase_in, int i
                                                                     A_out, phase_out);
     return sb::check_launch("interp2d_field_kernel");
 }
+
+// ---------------------------------------------------------------------------
+// No-allocation variant of sb_sh_forward: the partial sums live in a
+// file-scope device array instead of caller scratch.  Host code must not
+// pass the array's name to a kernel (on the host it is only a stand-in for
+// the symbol); its device address is looked up once per device with
+// cudaGetSymbolAddress while that device is current.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace {
+static __device__ __align__(256) unsigned char g_sh_static_scratch[SB_SH_STATIC_SCRATCH_BYTES];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_static_mutex;
+void *g_static_ptr[kMaxDevices] = {};
+
+int static_scratch_address(void **out) {
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return sb::fail(SB_ECUDA, "sb_sh_forward_static: cudaGetDevice: %s", cudaGetErrorString(e));
+    if (dev < 0 || dev >= kMaxDevices) return sb::fail(SB_EUNSUPPORTED, "sb_sh_forward_static: device %d", dev);
+    std::lock_guard<std::mutex> lock(g_static_mutex);
+    if (!g_static_ptr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_sh_static_scratch);
+        if (e != cudaSuccess || !p)
+            return sb::fail(SB_ECUDA, "sb_sh_forward_static: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+        g_static_ptr[dev] = p;
+    }
+    *out = g_static_ptr[dev];
+    return SB_OK;
+}
+}  // namespace
+
+extern "C" int sb_sh_forward_static(const sb_sh_plan *pl, const float *A, const float *phase_nm, const float *A_norm,
+                                    int n_norm, float photon_scale, float *intensity, void *stream) {
+    sb::clear_error();
+    if (!pl) return sb::fail(SB_EINVAL, "sb_sh_forward_static: null plan");
+    const size_t need = sb_sh_scratch_bytes(pl);
+    if (need == 0) return sb::fail(SB_ESHAPE, "sb_sh_forward_static: geometry does not fit the kernel limits");
+    if (need > (size_t)SB_SH_STATIC_SCRATCH_BYTES)
+        return sb::fail(SB_ESCRATCH,
+                        "sb_sh_forward_static: this geometry needs %zu bytes of scratch, the static array holds %d; "
+                        "use sb_sh_forward with caller scratch",
+                        need, SB_SH_STATIC_SCRATCH_BYTES);
+    void *scratch = nullptr;
+    const int rc = static_scratch_address(&scratch);
+    if (rc) return rc;
+    return sb_sh_forward(pl, A, phase_nm, A_norm, n_norm, photon_scale, intensity, scratch,
+                         (size_t)SB_SH_STATIC_SCRATCH_BYTES, stream);
+}
