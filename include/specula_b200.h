@@ -210,6 +210,13 @@ typedef struct sb_iir_plan {
 
 int sb_integrator(const sb_iir_plan *plan, const float *delta, float *out, void *stream);
 
+/* Modalrec followed by the Integrator in one launch (modalrec.py:159 then
+ * iir_filter.py:100-211): modes = R @ slopes, then the filter of mode m
+ * consumes modes[m].  Results are identical to sb_modalrec + sb_integrator;
+ * used when both objects are captured in one loop graph. */
+int sb_modalrec_integrator(const float *R, int n_modes, int n_slopes, int ldr, const float *slopes,
+                           float *modes, const sb_iir_plan *plan, float *out, void *stream);
+
 /* ------------------------------------------------------------------------
  * DM — replaces specula/processing_objects/dm.py:72-86:
  * phase[mask_idx[p]] = sum_m (sign * cmd[m]) * IF[m][p]; IF row-major

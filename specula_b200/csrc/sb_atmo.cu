@@ -73,24 +73,26 @@ __global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgs a) {
         bc1 = min(bc1, bc0 + kBox - 1);
     }
     const int R = br1 - br0 + 1, Cc = bc1 - bc0 + 1;
-    // thread (tx, ty) of the 32 x 8 block walks the footprint so that tx
-    // always runs along the screen's columns: along the footprint's columns
-    // for even k, along its rows for odd k (rot90 swaps the axes)
+    // rot90(lerped)[yy][xx] reads screen element base + ra*dR + cb*dC
+    // (ra, cb: footprint row / column); thread (tx, ty) of the 32 x 8 block
+    // walks the footprint so that tx always runs along screen columns:
+    // along footprint columns for even k, along footprint rows for odd k
+    long long dR, dC, b0;
+    switch (k) {
+        case 1: dR = -1; dC = ld; b0 = (long long)bc0 * ld + (L - 1 - br0); break;
+        case 2: dR = -(long long)ld; dC = -1; b0 = (long long)(L - 1 - br0) * ld + (L - 1 - bc0); break;
+        case 3: dR = 1; dC = -(long long)ld; b0 = (long long)(L - 1 - bc0) * ld + br0; break;
+        default: dR = ld; dC = 1; b0 = (long long)br0 * ld + bc0;
+    }
     const bool odd = k & 1;
     const int n_fast = odd ? R : Cc, n_slow = odd ? Cc : R;
+    const long long d_fast = odd ? dR : dC, d_slow = odd ? dC : dR;
     for (int sl = threadIdx.y; sl < n_slow; sl += blockDim.y) {
+        const float *ps = row0 + b0 + sl * d_slow;
         for (int fa = threadIdx.x; fa < n_fast; fa += blockDim.x) {
-            const int ra = odd ? fa : sl, cb = odd ? sl : fa;
-            const int yy = br0 + ra, xx = bc0 + cb;
-            int sr, sc;   // screen row / column of rot90(lerped)[yy][xx] (atmo_evolution.py:291)
-            switch (k) {
-                case 1: sr = xx; sc = L - 1 - yy; break;
-                case 2: sr = L - 1 - yy; sc = L - 1 - xx; break;
-                case 3: sr = L - 1 - xx; sc = yy; break;
-                default: sr = yy; sc = xx;
-            }
-            const float *p = row0 + (size_t)sr * ld + sc;
-            Q[ra][cb] = __fadd_rn(__fmul_rn(w0, p[0]), __fmul_rn(frac, p[1]));
+            const float *p = ps + fa * d_fast;
+            const float v = __fadd_rn(__fmul_rn(w0, p[0]), __fmul_rn(frac, p[1]));
+            if (odd) Q[fa][sl] = v; else Q[sl][fa] = v;
         }
     }
     __syncthreads();

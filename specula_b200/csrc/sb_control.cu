@@ -39,11 +39,9 @@ __global__ void __launch_bounds__(256) gemv_rows_kernel(const float *__restrict_
     if (threadIdx.x == 0) y[m] = acc;
 }
 
-// 2-tap IIR per mode, operation order of iir_filter.py:100-211 (no FMA
+// 2-tap IIR for mode e, operation order of iir_filter.py:100-211 (no FMA
 // contraction, so float32 results match the reference bit for bit)
-__global__ void integrator_kernel(sb_iir_plan p, const float *__restrict__ delta, float *__restrict__ out) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= p.n) return;
+__device__ __forceinline__ void iir_update(const sb_iir_plan &p, int e, float delta, float *__restrict__ out) {
     float *st = p.state + (size_t)e * p.total;
     if (p.shift)
         for (int k = p.total - 1; k >= 1; --k) st[k] = st[k - 1];
@@ -53,7 +51,7 @@ __global__ void integrator_kernel(sb_iir_plan p, const float *__restrict__ delta
     ost[1] = 0.f;
     ist[0] = ist[1];
     ist[1] = 0.f;
-    ist[1] = delta[e];
+    ist[1] = delta;
     const float factor = __fdiv_rn(1.0f, den[1]);
     const float num_c = __fadd_rn(__fmul_rn(num[0], ist[0]), __fmul_rn(num[1], ist[1]));
     const float den_c = __fmul_rn(den[0], ost[0]);
@@ -68,6 +66,47 @@ __global__ void integrator_kernel(sb_iir_plan p, const float *__restrict__ delta
     }
     out[e] = o;
     if (p.out_next) p.out_next[e] = st[p.k_out - 1];
+}
+
+__global__ void integrator_kernel(sb_iir_plan p, const float *__restrict__ delta, float *__restrict__ out) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= p.n) return;
+    iir_update(p, e, delta[e], out);
+}
+
+// reconstructor row m (as gemv_rows_kernel) followed by the integrator update
+// of mode m in the same CTA: one launch for Modalrec + Integrator
+template <bool VEC>
+__global__ void __launch_bounds__(256) gemv_iir_kernel(const float *__restrict__ R, int ncols, int ldr,
+                                                       const float *__restrict__ s, float *__restrict__ y,
+                                                       sb_iir_plan p, float *__restrict__ out) {
+    __shared__ float red[33];
+    const int m = blockIdx.x;
+    const float *row = R + (size_t)m * ldr;
+    float acc = 0.f;
+    if (VEC) {
+        const int n4 = ncols >> 2;
+        const float4 *r4 = reinterpret_cast<const float4 *>(row);
+        const float4 *s4 = reinterpret_cast<const float4 *>(s);
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+#pragma unroll 4
+        for (int j = threadIdx.x; j < n4; j += blockDim.x) {
+            const float4 r = __ldg(r4 + j), v = __ldg(s4 + j);
+            a0 = fmaf(r.x, v.x, a0);
+            a1 = fmaf(r.y, v.y, a1);
+            a2 = fmaf(r.z, v.z, a2);
+            a3 = fmaf(r.w, v.w, a3);
+        }
+        acc = (a0 + a1) + (a2 + a3);
+        for (int j = (n4 << 2) + threadIdx.x; j < ncols; j += blockDim.x) acc = fmaf(row[j], s[j], acc);
+    } else {
+        for (int j = threadIdx.x; j < ncols; j += blockDim.x) acc = fmaf(row[j], s[j], acc);
+    }
+    acc = sb::block_sum(acc, red);
+    if (threadIdx.x == 0) {
+        y[m] = acc;
+        if (m < p.n) iir_update(p, m, acc, out);
+    }
 }
 
 // phase[idx[p]] = sum_m c[m] * IF[m][p]; CTA = 8 warps sharing a strip of
@@ -152,6 +191,28 @@ extern "C" int sb_modalrec(const float *R, int n_modes, int n_slopes, int ldr, c
     else
         gemv_rows_kernel<false><<<n_modes, 256, 0, st>>>(R, n_slopes, ldr, slopes, modes);
     return sb::check_launch("gemv_rows_kernel");
+}
+
+extern "C" int sb_modalrec_integrator(const float *R, int n_modes, int n_slopes, int ldr, const float *slopes,
+                                      float *modes, const sb_iir_plan *p, float *out, void *stream) {
+    sb::clear_error();
+    if (!R || !slopes || !modes || !p || !out || n_modes < 0 || n_slopes < 0 || ldr < n_slopes)
+        return sb::fail(SB_EINVAL, "sb_modalrec_integrator: bad args");
+    if (!p->num || !p->den || !p->ist || !p->ost || !p->state)
+        return sb::fail(SB_EINVAL, "sb_modalrec_integrator: null integrator state");
+    if (p->n != n_modes) return sb::fail(SB_ESHAPE, "sb_modalrec_integrator: %d filters for %d modes", p->n, n_modes);
+    if (p->total < 1 || p->k_out < 0 || p->k_out >= p->total || (p->rem != 0.f && p->k_out < 1))
+        return sb::fail(SB_EINVAL, "sb_modalrec_integrator: bad state layout");
+    if (p->out_next && (p->rem != 0.f || p->k_out < 1))
+        return sb::fail(SB_EINVAL, "sb_modalrec_integrator: out_next needs an integer delay >= 1");
+    if (n_modes == 0) return SB_OK;
+    cudaStream_t st = sb::as_stream(stream);
+    const bool vec = (ldr % 4 == 0) && ((uintptr_t)R % 16 == 0) && ((uintptr_t)slopes % 16 == 0);
+    if (vec)
+        gemv_iir_kernel<true><<<n_modes, 256, 0, st>>>(R, n_slopes, ldr, slopes, modes, *p, out);
+    else
+        gemv_iir_kernel<false><<<n_modes, 256, 0, st>>>(R, n_slopes, ldr, slopes, modes, *p, out);
+    return sb::check_launch("gemv_iir_kernel");
 }
 
 extern "C" int sb_integrator(const sb_iir_plan *p, const float *delta, float *out, void *stream) {

@@ -105,9 +105,12 @@ __global__ void __launch_bounds__(256, 6) ccd_kernel(sb_ccd_params p, const floa
     // frame bookkeeping lives on the device; every block reads it before the
     // last block to finish advances it (see the end of the kernel)
     volatile sb_ccd_state *vs = p.state;
+    __shared__ unsigned int warps_done;
+    if (threadIdx.x == 0) warps_done = 0u;
     const uint64_t frame = vs->frame_index;
     const int nint = vs->n_integrated + 1;
     const bool readout = nint >= p.frames_per_read;
+    __syncthreads();
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < p.n_pixels; e += gridDim.x * blockDim.x) {
         // integrated_i += i * (loop_dt * bandw)   (ccd.py:205)
         float acc = __fadd_rn(integ[e], __fmul_rn(in[e], p.rate));
@@ -138,20 +141,21 @@ __global__ void __launch_bounds__(256, 6) ccd_kernel(sb_ccd_params p, const floa
         pix[e] = outv;
         integ[e] = 0.0f;                                            // ccd.py:216
     }
-    // the last block to finish advances the frame state
-    __shared__ bool last;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        const unsigned int prev = atomicAdd(&p.state->blocks_done, 1u);
-        last = (prev == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (last && threadIdx.x == 0) {
-        vs->n_integrated = readout ? 0 : nint;
-        if (readout) vs->frame_index = frame + 1;
-        vs->blocks_done = 0u;
-        __threadfence();
+    // the last warp to finish in the last block to finish advances the frame
+    // state; warps that are done do not wait for the slower ones (the noise
+    // sampling loops diverge)
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) {
+        const unsigned int nwarps = (blockDim.x + 31) >> 5;
+        if (atomicAdd(&warps_done, 1u) == nwarps - 1) {
+            __threadfence();
+            if (atomicAdd(&p.state->blocks_done, 1u) == gridDim.x - 1) {
+                vs->n_integrated = readout ? 0 : nint;
+                if (readout) vs->frame_index = frame + 1;
+                vs->blocks_done = 0u;
+                __threadfence();
+            }
+        }
     }
 }
 

@@ -10,12 +10,14 @@ every object's ``trigger_code`` for a step; all loop state (layer positions,
 CCD frame counter, integrator state, DM shape) lives on the device, so each
 graph replay is a full new step.
 """
+import ctypes
 import math
 from dataclasses import dataclass, field
 
 import numpy as np
 import torch
 
+from specula_b200 import _lib
 from specula_b200.base_value import BaseValue
 from specula_b200.data_objects.ifunc import IFunc
 from specula_b200.data_objects.pupilstop import Pupilstop
@@ -196,8 +198,10 @@ class ScaoLoop:
         self.pipelined = bool(pipelined and self.integ.next_output_available)
         if not self.pipelined:
             with torch.cuda.graph(g):
-                for o in self.objects:
+                for o in self.objects[:5]:
                     o.trigger_code()
+                self._rec_integ()
+                self.dm.trigger_code()
             self.steps_per_replay = 1
         else:
             dm_buf = [self.dm.layer.phaseInNm, torch.empty_like(self.dm.layer.phaseInNm)]
@@ -213,7 +217,7 @@ class ScaoLoop:
             self._side = side
             self._cap = cap
             self._bufs = (dm_buf, nxt)
-            chain = [self.atmo, self.prop, self.sh, self.ccd, self.slopec, self.rec]
+            chain = [self.atmo, self.prop, self.sh, self.ccd, self.slopec]
             with torch.cuda.graph(g, stream=cap):
                 main = torch.cuda.current_stream(self.device)
                 for par in (1, 0):              # odd step, then even step
@@ -225,21 +229,40 @@ class ScaoLoop:
                             o.trigger_code(phase_override={id(self.dm.layer): dm_buf[1 - par]})
                         else:
                             o.trigger_code()
-                    self.integ.trigger_code(out_next=nxt[1 - par])
+                    self._rec_integ(out_next=nxt[1 - par])
                     main.wait_stream(side)
             self.steps_per_replay = 2
         torch.cuda.synchronize(self.device)
         self.graph = g
         return g
 
+    def _rec_integ(self, out_next=None):
+        """Modalrec + Integrator of this loop as one launch
+        (sb_modalrec_integrator), falling back to the two objects when the
+        reconstructor output is sliced."""
+        rec, integ = self.rec, self.integ
+        full = rec.output_slice == slice(None, None, None) and integ._n == rec._R.shape[0]
+        if not full:
+            rec.trigger_code()
+            integ.trigger_code(out_next=out_next)
+            return
+        s = rec.local_inputs['in_slopes'].slopes
+        integ._plan.out_next = None if out_next is None else out_next.data_ptr()
+        try:
+            _lib.call('sb_modalrec_integrator', rec._R.data_ptr(), rec._R.shape[0], rec._R.shape[1],
+                      rec._R.stride(0), s.data_ptr(), rec._all_modes.data_ptr(), ctypes.byref(integ._plan),
+                      integ.out_comm.value.data_ptr(), rec.stream_handle())
+        finally:
+            integ._plan.out_next = None
+
     def replay(self):
         """Run the captured graph: ``steps_per_replay`` loop steps."""
         self.graph.replay()
 
-    # kernels launched by one step (for the launch count): atmo advance +
-    # evolve, propagate, SH forward + normalise, CCD, slopes (2), modal
-    # reconstructor, integrator, DM projection
-    KERNELS_PER_STEP = 11
+    # kernels launched by one captured step (for the launch count): atmo
+    # advance + evolve, propagate, SH forward + normalise, CCD, slopes (2),
+    # reconstructor with the integrator, DM projection
+    KERNELS_PER_STEP = 10
 
 
 def valid_subaps(pupil, n_lenses, npx, threshold=0.5):
