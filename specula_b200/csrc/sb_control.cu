@@ -42,30 +42,46 @@ __global__ void __launch_bounds__(256) gemv_rows_kernel(const float *__restrict_
 // 2-tap IIR for mode e, operation order of iir_filter.py:100-211 (no FMA
 // contraction, so float32 results match the reference bit for bit)
 __device__ __forceinline__ void iir_update(const sb_iir_plan &p, int e, float delta, float *__restrict__ out) {
+    // every load is issued before any store (the arrays may alias as far as
+    // the compiler knows), so the update costs two memory round trips
+    constexpr int kMaxTotal = 8;
     float *st = p.state + (size_t)e * p.total;
-    if (p.shift)
-        for (int k = p.total - 1; k >= 1; --k) st[k] = st[k - 1];
     float *ist = p.ist + 2 * e, *ost = p.ost + 2 * e;
-    const float *num = p.num + 2 * e, *den = p.den + 2 * e;
-    ost[0] = ost[1];
-    ost[1] = 0.f;
-    ist[0] = ist[1];
-    ist[1] = 0.f;
-    ist[1] = delta;
-    const float factor = __fdiv_rn(1.0f, den[1]);
-    const float num_c = __fadd_rn(__fmul_rn(num[0], ist[0]), __fmul_rn(num[1], ist[1]));
-    const float den_c = __fmul_rn(den[0], ost[0]);
+    const float2 num = *reinterpret_cast<const float2 *>(p.num + 2 * e);
+    const float2 den = *reinterpret_cast<const float2 *>(p.den + 2 * e);
+    const float ist1 = ist[1], ost1 = ost[1];
+    float sv[kMaxTotal];
+    const int total = p.total;
+#pragma unroll
+    for (int k = 0; k < kMaxTotal; ++k) sv[k] = k < total ? st[k] : 0.f;
+    // prepare_trigger: shift the state buffer
+    if (p.shift) {
+#pragma unroll
+        for (int k = kMaxTotal - 1; k >= 1; --k) sv[k] = sv[k - 1];
+    }
+    // trigger_code: ost/ist shift left, new input in the last column
+    const float ist0 = ist1, ost0 = ost1;
+    const float factor = __fdiv_rn(1.0f, den.y);
+    const float num_c = __fadd_rn(__fmul_rn(num.x, ist0), __fmul_rn(num.y, delta));
+    const float den_c = __fmul_rn(den.x, ost0);
     const float y = __fmul_rn(factor, __fsub_rn(num_c, den_c));
-    ost[1] = y;
-    st[0] = y;
+    sv[0] = y;
+    // post_trigger: delayed output
     float o;
     if (p.rem == 0.f) {
-        o = st[p.k_out];
+        o = sv[p.k_out];
     } else {
-        o = __fadd_rn(__fmul_rn(p.rem, st[p.k_out]), __fmul_rn(p.one_minus_rem, st[p.k_out - 1]));
+        o = __fadd_rn(__fmul_rn(p.rem, sv[p.k_out]), __fmul_rn(p.one_minus_rem, sv[p.k_out - 1]));
     }
+    ist[0] = ist0;
+    ist[1] = delta;
+    ost[0] = ost0;
+    ost[1] = y;
+#pragma unroll
+    for (int k = 0; k < kMaxTotal; ++k)
+        if (k < total) st[k] = sv[k];
     out[e] = o;
-    if (p.out_next) p.out_next[e] = st[p.k_out - 1];
+    if (p.out_next) p.out_next[e] = sv[p.k_out - 1];
 }
 
 __global__ void integrator_kernel(sb_iir_plan p, const float *__restrict__ delta, float *__restrict__ out) {
@@ -201,8 +217,8 @@ extern "C" int sb_modalrec_integrator(const float *R, int n_modes, int n_slopes,
     if (!p->num || !p->den || !p->ist || !p->ost || !p->state)
         return sb::fail(SB_EINVAL, "sb_modalrec_integrator: null integrator state");
     if (p->n != n_modes) return sb::fail(SB_ESHAPE, "sb_modalrec_integrator: %d filters for %d modes", p->n, n_modes);
-    if (p->total < 1 || p->k_out < 0 || p->k_out >= p->total || (p->rem != 0.f && p->k_out < 1))
-        return sb::fail(SB_EINVAL, "sb_modalrec_integrator: bad state layout");
+    if (p->total < 1 || p->total > 8 || p->k_out < 0 || p->k_out >= p->total || (p->rem != 0.f && p->k_out < 1))
+        return sb::fail(SB_EINVAL, "sb_modalrec_integrator: bad state layout (delay up to 7 frames)");
     if (p->out_next && (p->rem != 0.f || p->k_out < 1))
         return sb::fail(SB_EINVAL, "sb_modalrec_integrator: out_next needs an integer delay >= 1");
     if (n_modes == 0) return SB_OK;
@@ -219,8 +235,9 @@ extern "C" int sb_integrator(const sb_iir_plan *p, const float *delta, float *ou
     sb::clear_error();
     if (!p || !delta || !out || !p->num || !p->den || !p->ist || !p->ost || !p->state)
         return sb::fail(SB_EINVAL, "sb_integrator: null pointer");
-    if (p->n < 0 || p->total < 1 || p->k_out < 0 || p->k_out >= p->total || (p->rem != 0.f && p->k_out < 1))
-        return sb::fail(SB_EINVAL, "sb_integrator: bad state layout");
+    if (p->n < 0 || p->total < 1 || p->total > 8 || p->k_out < 0 || p->k_out >= p->total ||
+        (p->rem != 0.f && p->k_out < 1))
+        return sb::fail(SB_EINVAL, "sb_integrator: bad state layout (delay up to 7 frames)");
     if (p->out_next && (p->rem != 0.f || p->k_out < 1))
         return sb::fail(SB_EINVAL, "sb_integrator: out_next needs an integer delay >= 1");
     if (p->n == 0) return SB_OK;

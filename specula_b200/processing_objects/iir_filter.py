@@ -30,6 +30,8 @@ class IirFilter(BaseProcessingObj):
         if iir_filter_data.num_np.shape[1] != 2 or iir_filter_data.den_np.shape[1] != 2:
             raise NotImplementedError('IirFilter: only 2-tap filters (integrators) are on the specula_b200 path')
         self.delay = delay if delay is not None else 0
+        if int(np.ceil(self.delay)) + 1 > 8:
+            raise NotImplementedError('IirFilter: delays above 7 frames are not on the specula_b200 path')
         self._n = iir_filter_data.nfilter
         self._total_length = int(np.ceil(self.delay)) + 1
         self.state = torch.zeros((self._n, self._total_length), dtype=self.dtype, device=self.device)
