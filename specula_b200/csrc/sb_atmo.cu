@@ -6,9 +6,10 @@
 // order-1 fractional-degree rotation with scipy's 'constant' boundary (:293;
 // a sample outside [0, L-1] on either axis gives 0, otherwise bilinear from
 // the four neighbours, neighbours off the grid counting 0) and the r0 scale
-// (:294).  Float32 operations keep NumPy's order (no FMA contraction) and the
-// rotation coordinates are computed in double like SciPy, so the boundary
-// and neighbour choices are the reference's; the bilinear blend is float32.
+// (:294).  The lerp and scale keep NumPy's float32 operation order (no FMA
+// contraction); the rotation samples are evaluated as small float32 offsets
+// from the output pixel, with SciPy's exact float64 expression deciding the
+// edge test wherever it is within 1e-4 px.
 #include "sb_common.cuh"
 
 namespace {
@@ -97,9 +98,17 @@ __global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgs a) {
     }
     __syncthreads();
     const int x = x0 + threadIdx.x;
-    const double xd = (double)x;
-    const double cx0 = __dmul_rn(ly.m01, xd), cx1 = __dmul_rn(ly.m11, xd);
-    const double Lm1 = (double)(L - 1);
+    // the rotation is below one degree: sample = (y + dr, x + dc) with
+    // dr = (m00-1) y + m01 x + off0 and dc = m10 y + (m11-1) x + off1 small
+    // (|dr|, |dc| < ~12 px), so they are evaluated in float32 to ~1e-6 px.
+    // Only the edge test (sample outside [0, L-1] gives 0) is discontinuous;
+    // within 1e-4 px of an edge it is redone with SciPy's exact float64
+    // expression (m00*y + m01*x) + off0.
+    const float a00 = (float)(ly.m00 - 1.0), a01 = (float)ly.m01, a10 = (float)ly.m10, a11 = (float)(ly.m11 - 1.0);
+    const float b0f = (float)ly.off0, b1f = (float)ly.off1;
+    const float xf = (float)x;
+    const float dr_x = fmaf(a01, xf, b0f), dc_x = fmaf(a11, xf, b1f);
+    const float Lm1 = (float)(L - 1);
     for (int yi = threadIdx.y; yi < kTile; yi += blockDim.y) {
         const int y = y0 + yi;
         if (x >= L || y >= L) continue;
@@ -107,20 +116,28 @@ __global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgs a) {
         if (!ly.rotate) {
             v = Q[y - br0][x - bc0];
         } else {
-            // scipy.ndimage.rotate(order=1, mode='constant'): a sample
-            // outside [0, L-1] gives 0, neighbours off the grid count 0.
-            // Coordinates in double with SciPy's operation order (the
-            // boundary and floor decisions are exact); the weights and the
-            // blend in float32, which is the output precision.
-            const double yd = (double)y;
-            const double ir = __dadd_rn(__dadd_rn(__dmul_rn(ly.m00, yd), cx0), ly.off0);
-            const double ic = __dadd_rn(__dadd_rn(__dmul_rn(ly.m10, yd), cx1), ly.off1);
-            if (!(ir >= 0.0 && ir <= Lm1 && ic >= 0.0 && ic <= Lm1)) {
+            const float yf = (float)y;
+            const float dr = fmaf(a00, yf, dr_x), dc = fmaf(a10, yf, dc_x);
+            const float irf = yf + dr, icf = xf + dc;
+            bool inside = irf >= 0.f && irf <= Lm1 && icf >= 0.f && icf <= Lm1;
+            const float eps = 1e-4f;
+            if (irf < eps || irf > Lm1 - eps || icf < eps || icf > Lm1 - eps) {
+                const double yd = (double)y, xd = (double)x;
+                const double ir = __dadd_rn(__dadd_rn(__dmul_rn(ly.m00, yd), __dmul_rn(ly.m01, xd)), ly.off0);
+                const double ic = __dadd_rn(__dadd_rn(__dmul_rn(ly.m10, yd), __dmul_rn(ly.m11, xd)), ly.off1);
+                inside = ir >= 0.0 && ir <= (double)(L - 1) && ic >= 0.0 && ic <= (double)(L - 1);
+            }
+            if (!inside) {
                 v = 0.0f;
             } else {
-                const double fr0 = floor(ir), fc0 = floor(ic);
-                const int r0 = (int)fr0, c0 = (int)fc0;
-                const float fr = (float)(ir - fr0), fc = (float)(ic - fc0);
+                const float fdr = floorf(dr), fdc = floorf(dc);
+                int r0 = y + (int)fdr, c0 = x + (int)fdc;
+                float fr = dr - fdr, fc = dc - fdc;
+                // clamp to the grid (only reachable within 1e-4 px of an edge)
+                if (r0 < 0) { r0 = 0; fr = 0.f; }
+                if (c0 < 0) { c0 = 0; fc = 0.f; }
+                if (r0 > L - 1) { r0 = L - 1; fr = 0.f; }
+                if (c0 > L - 1) { c0 = L - 1; fc = 0.f; }
                 const int qr = r0 - br0, qc = c0 - bc0;
                 const bool rin = r0 + 1 < L, cin = c0 + 1 < L;
                 const float q00 = Q[qr][qc];

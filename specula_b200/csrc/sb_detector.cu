@@ -53,11 +53,23 @@ __device__ __forceinline__ float u01f(uint32_t a) { return ((float)(a >> 8) + 0.
 constexpr uint32_t kPhotonTag = 0x50484f54u;   // "PHOT"
 constexpr uint32_t kReadoutTag = 0x52454144u;  // "READ"
 
+// log(k!) for k < 32 (math.lgamma(k + 1) rounded to float)
+__constant__ float c_logfact[32] = {0.0f, 0.0f, 0.693147181f, 1.79175947f, 3.17805383f, 4.78749174f, 6.57925121f, 8.52516136f, 10.6046029f, 12.8018275f, 15.1044126f, 17.5023078f, 19.9872145f, 22.5521639f, 25.1912212f, 27.8992714f, 30.6718601f, 33.5050735f, 36.3954452f, 39.3398842f, 42.3356165f, 45.3801389f, 48.4711814f, 51.6066756f, 54.7847294f, 58.0036052f, 61.2617018f, 64.5575386f, 67.8897431f, 71.257039f, 74.6582363f, 78.0922236f};
+
+// log(k!) for integer-valued k >= 0: table below 32 (staged in shared memory
+// by the caller), Stirling's series for log Gamma(k + 1) above (error < 1e-9
+// relative there)
+__device__ __forceinline__ float log_factorial(float k, const float *tbl) {
+    if (k < 32.0f) return tbl[(int)k];
+    const float z = k + 1.0f, iz = 1.0f / z, iz2 = iz * iz;
+    return (z - 0.5f) * logf(z) - z + 0.91893853f + iz * (0.083333333f - iz2 * (0.0027777778f - iz2 * 0.00079365079f));
+}
+
 // Poisson(lam) in float32 arithmetic.  lam < 10: sequential-search
 // inversion of one uniform.  lam >= 10: PTRS transformed rejection
 // (Hormann 1993), two uniforms per try, at most 64 tries (acceptance per try
 // is above 0.9, so the bound is never reached in practice).
-__device__ float poisson_sample(float lam, uint32_t e, uint64_t frame, uint64_t seed) {
+__device__ float poisson_sample(float lam, uint32_t e, uint64_t frame, uint64_t seed, const float *logfact) {
     if (!(lam > 0.0f)) return 0.0f;
     const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32) ^ kPhotonTag;
     if (lam < 10.0f) {
@@ -67,7 +79,7 @@ __device__ float poisson_sample(float lam, uint32_t e, uint64_t frame, uint64_t 
         int k = 0;
         while (u > cdf && k < 100) {
             ++k;
-            pk *= lam / (float)k;
+            pk *= __fdividef(lam, (float)k);
             cdf += pk;
         }
         return (float)k;
@@ -87,7 +99,8 @@ __device__ float poisson_sample(float lam, uint32_t e, uint64_t frame, uint64_t 
             const float k = floorf((2.0f * a / us + b) * U + lam + 0.43f);
             if (us >= 0.07f && V <= vr) return k;
             if (k < 0.0f || (us < 0.013f && V > us)) continue;
-            if (logf(V) + log_inv_alpha - logf(a / (us * us) + b) <= -lam + k * loglam - lgammaf(k + 1.0f)) return k;
+            if (logf(V) + log_inv_alpha - logf(a / (us * us) + b) <= -lam + k * loglam - log_factorial(k, logfact))
+                return k;
         }
     }
     return floorf(lam + 0.5f);
@@ -106,7 +119,9 @@ __global__ void __launch_bounds__(256, 6) ccd_kernel(sb_ccd_params p, const floa
     // last block to finish advances it (see the end of the kernel)
     volatile sb_ccd_state *vs = p.state;
     __shared__ unsigned int warps_done;
+    __shared__ float logfact[32];
     if (threadIdx.x == 0) warps_done = 0u;
+    if (threadIdx.x < 32) logfact[threadIdx.x] = c_logfact[threadIdx.x];
     const uint64_t frame = vs->frame_index;
     const int nint = vs->n_integrated + 1;
     const bool readout = nint >= p.frames_per_read;
@@ -123,7 +138,7 @@ __global__ void __launch_bounds__(256, 6) ccd_kernel(sb_ccd_params p, const floa
         f = __fadd_rn(f, p.bg_plus_dark);                           // ccd.py:220-221
         float outv;
         if (p.photon_noise) {
-            double v = poisson_sample(f, (uint32_t)e, frame, p.photon_seed);
+            double v = poisson_sample(f, (uint32_t)e, frame, p.photon_seed, logfact);
             if (p.readout_noise) v += truncf(std_normal((uint32_t)e, frame, p.readout_seed) * p.readout_level);
             // ADU: round(x*g)+bias, clamp at 0, -bias, /g, back to the
             // integer dtype of the Poisson draw (ccd.py:247-258)
