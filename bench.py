@@ -45,6 +45,7 @@ def parse():
     p.add_argument('--impl', default='b200', choices=['b200', 'reference'])
     p.add_argument('--cpu-baseline-seconds', type=float, default=20.0)
     p.add_argument('--no-cpu-baseline', action='store_true')
+    p.add_argument('--no-adjoint', action='store_true', help='skip the adjoint interaction-matrix leg')
     return p.parse_args()
 
 
@@ -180,6 +181,93 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def bench_adjoint_im(dev, reps, cpu_budget_s):
+    """Adjoint interaction matrix against push-pull on the 40x40 / 320 px /
+    FFT 16 / 500-Zernike calibration system (one B200).  Each timed call is
+    bracketed by CUDA events on the launching stream with an L2 flush
+    (256 MB write) between calls."""
+    import torch
+    from specula_b200.calibration import ShCalibrationSystem
+    cal = ShCalibrationSystem(device_idx=dev.index)
+    st = torch.cuda.current_stream(dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    amp = 10.0
+
+    def timed(fn, n):
+        ms = []
+        out = None
+        for _ in range(n):
+            flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            out = fn()
+            e1.record(st)
+            torch.cuda.synchronize(dev)
+            ms.append(e0.elapsed_time(e1))
+        return statistics.median(ms), out
+
+    for _ in range(3):
+        cal.adjoint_intmat()
+        cal.pushpull_intmat(amp)
+    torch.cuda.synchronize(dev)
+    adj_ms, im_a = timed(cal.adjoint_intmat, reps)
+    pp_ms, im_p = timed(lambda: cal.pushpull_intmat(amp), max(2, reps // 2))
+    adj = cal.adjoint
+    active = adj.active(cal.A, cal._flat)
+    jac_ms, jac = timed(lambda: adj.jacobian(cal.A, cal._flat, active), reps)
+    con_ms, _ = timed(lambda: adj.intmat(cal.A, cal._flat, cal.dm, jac=jac, pix2col=cal._pix2col), reps)
+    n_in = cal.pixels_under_valid_subaps()
+    con_bytes = cal.contract_bytes(cal.n_modes, n_in, cal.n_valid, adj.np_sub ** 2)
+    peak, peak_kind = measured_peak_hbm()
+    con_gbs = con_bytes / (con_ms / 1e3) / 1e9
+    err = float((im_a - im_p).abs().max() / im_p.abs().max())
+    out = {'workload': 'calib_40x40_320px_fft16_500zernike', 'n_modes': cal.n_modes, 'n_slopes': 2 * cal.n_valid,
+           'adjoint_ms': adj_ms, 'pushpull_ms': pp_ms, 'speedup_vs_gpu_pushpull': pp_ms / adj_ms,
+           'pushpull_amplitude': amp, 'pushpull_steps': 2 * cal.n_modes,
+           'pushpull_form': 'same CUDA chain, one influence function projected per step, whole sequence in one '
+                            'CUDA graph',
+           'rel_diff_vs_gpu_pushpull': err,
+           'jacobian_kernel_us': jac_ms * 1e3, 'contract_kernel_us': con_ms * 1e3,
+           'contract_roofline': {'bound': 'hbm', 'achieved': con_gbs, 'peak': peak, 'peak_kind': peak_kind,
+                                 'unit': 'GB/s', 'frac': con_gbs / peak, 'algorithmic_bytes': con_bytes},
+           'l2': 'flushed (256 MB write) before every timed call'}
+    if cpu_budget_s > 0:
+        out['cpu_baseline'] = cpu_pushpull(cal, amp, cpu_budget_s)
+    return out
+
+
+def cpu_pushpull(cal, amp, budget_s):
+    """The reference's push-pull on the host cores (CPU oracle, float32):
+    as many modes as fit in the budget, scaled to all modes."""
+    from oracle import sh as osh, slopec as osl, control as octl
+    g = cal.sh.geometry
+    geom = osh.sh_geometry(cal.sh._wavelengthInNm, cal.sh._subap_wanted_fov_arcsec, cal.sh._sensor_pxscale_arcsec,
+                           g.n_lenses, g.subap_npx, cal.pupil.shape[0], cal.simul_params.pixel_pitch,
+                           fov_ovs_coeff=1.0)
+    o = osh.SHOracle(geom, cal.sh._wavelengthInNm, precision=1)
+    A = cal.pupil.astype(np.float32)
+    IF = cal.dm._ifunc.influence_function.cpu().numpy()
+    idxs = cal.subapdata.idxs
+    pitch = cal.simul_params.pixel_pitch
+
+    def slopes_fn(k, a):
+        cmd = np.zeros(IF.shape[0], np.float32)
+        cmd[k] = a
+        ph = octl.dm_phase(IF, cal.pupil, cmd, sign=cal.dm.sign)
+        return osl.sh_slopes(o.forward(A, ph, 1.0, pitch), idxs)[0]
+
+    slopes_fn(0, amp)                     # untimed: first call
+    t0 = time.perf_counter()
+    k = 0
+    while k < IF.shape[0] and time.perf_counter() - t0 < budget_s:
+        octl.pushpull_intmat(lambda _, a: slopes_fn(k, a), 1, [amp])
+        k += 1
+    dt = time.perf_counter() - t0
+    return {'value': dt / k * IF.shape[0], 'unit': 's per interaction matrix', 'cores': blas_threads(),
+            'kind': 'port', 'sample': f'{k} of {IF.shape[0]} modes pushed and pulled in {dt:.1f} s, scaled'}
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
@@ -290,6 +378,11 @@ def run_b200(args):
         cpu = {'value': v, 'unit': UNIT, 'cores': blas_threads(), 'kind': 'port',
                'sample': f'{n} CPU-oracle loop steps of the same system after 1 untimed step ({dt:.1f} s)'}
 
+    adjoint_im = None
+    if world == 1 and not args.no_adjoint:
+        adjoint_im = bench_adjoint_im(dev, reps=max(3, min(args.steps, 10)),
+                                      cpu_budget_s=0 if args.no_cpu_baseline else 10.0)
+
     if rank == 0:
         line = {'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': steps,
                 'warmup': max(3, args.warmup), 'ms_per_step': ms_max / steps, 'higher_is_better': True,
@@ -306,7 +399,7 @@ def run_b200(args):
                 'step_roofline': {'algorithmic_bytes': step_bytes,
                                   'achieved_gbs': step_bytes / (ms_max / steps / 1e3) / 1e9,
                                   'frac': step_bytes / (ms_max / steps / 1e3) / 1e9 / peak},
-                'clocks': clk, 'cpu_baseline': cpu}
+                'clocks': clk, 'cpu_baseline': cpu, 'adjoint_im': adjoint_im}
         print(json.dumps(line), flush=True)
     del loop
     if world > 1:

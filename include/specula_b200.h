@@ -228,6 +228,57 @@ int sb_dm_project(const float *ifunc, int n_modes, int n_valid, int ld_if,
                   float *phase, void *stream);
 
 /* ------------------------------------------------------------------------
+ * Adjoint of the noise-free SH -> ShSlopec chain, and the interaction
+ * matrix built from it.  No counterpart in the reference, which measures
+ * the interaction matrix by push-pull (im_rec_calibrator.py:42-71 with
+ * lib/modal_pushpull_signal.py:35-65: 2 x n_modes forward loop steps).
+ *
+ * A linear detector (no noise) leaves the CoG slopes of a sub-aperture a
+ * function of that sub-aperture's phase samples only; the photon
+ * normalisation (sh.py:426-427) cancels in the CoG (sh_slopec.py:392-404).
+ * So d(slopes)/d(phase) is a 2 x np_sub^2 block per valid sub-aperture.
+ *   lenslet[s]  lenslet index (row * n_lenses + column) of valid
+ *               sub-aperture s, in slope order
+ *   xw/yw/mw    the ShSlopec weights (subap_npx^2 each)
+ *   active[s]   nonzero where the reference keeps the sub-aperture
+ *               (1/flux <= 1/(1e-3 * mean flux), sh_slopec.py:400) at the
+ *               linearisation point; zero rows stay zero.  NULL: every
+ *               sub-aperture with flux (then apply the cut-off from
+ *               tot_out, as sb_intmat_contract does)
+ * Threshold 0 only (the thresholded CoG is not differentiable).
+ * ---------------------------------------------------------------------- */
+
+/* jac[axis][s][r * np_sub + c] = d slope(axis, s) / d phase_nm at pixel
+ * (r, c) of sub-aperture s; axis 0 = x, 1 = y.  tot_out (optional,
+ * n_valid): each sub-aperture's CoG denominator, sum_px D * mw, at the
+ * linearisation point (unnormalised: only ratios are meaningful). */
+int sb_sh_slopes_jacobian(const sb_sh_plan *plan, const float *A, const float *phase_nm, int n_valid,
+                          const int32_t *lenslet, const float *xw, const float *yw, const float *mw,
+                          const float *active, float *jac, float *tot_out, void *stream);
+
+/* Vector-Jacobian product: grad_phase[pixel] = sum_j seed[j] d slope_j /
+ * d phase_nm[pixel], seed laid out like the slopes ([sx..., sy...]).
+ * Writes the pixels of the valid sub-apertures only (grad_phase has the
+ * field's row stride plan->field_ld; clear it first). */
+int sb_sh_slopes_vjp(const sb_sh_plan *plan, const float *A, const float *phase_nm, int n_valid,
+                     const int32_t *lenslet, const float *xw, const float *yw, const float *mw,
+                     const float *active, const float *seed, float *grad_phase, void *stream);
+
+/* intmat[m][j] = scale * sum_px jac[j][px] * ifunc[m][pix2col[px]] over the
+ * pixels of slope j's sub-aperture.  slot[i * n_lenses + j]: valid
+ * sub-aperture index of lenslet (i, j) or -1; pix2col: field pixel ->
+ * influence-function column, -1 outside the mirror's mask (field row
+ * stride field_ld).  tot (optional): the sb_sh_slopes_jacobian flux; when
+ * given, sub-apertures below the CoG cut-off get zero columns.  intmat is
+ * n_modes x (2 n_valid), row-major.  With scale = 2 * sign this is the
+ * reference's push-pull matrix (s+ - s-)/a in the limit of small a (DM
+ * phase = sign * cmd @ IF, dm.py:72-86).  np_sub in {4, 8, 16};
+ * n_lenses * np_sub <= 1024 (512 for np_sub = 16). */
+int sb_intmat_contract(const float *jac, const float *tot, int n_valid, int np_sub, int n_lenses, int field_ld,
+                       const int32_t *slot, const int32_t *pix2col, const float *ifunc, int n_modes,
+                       int ld_if, float scale, float *intmat, void *stream);
+
+/* ------------------------------------------------------------------------
  * AtmoEvolution — replaces specula/processing_objects/atmo_evolution.py:
  * 286-294: per layer, (1-f)*P[:, q:q+L] + f*P[:, q+1:q+1+L], rot90 by k,
  * order-1 rotation by the fractional part of the wind direction in degrees

@@ -76,6 +76,10 @@ SIGNATURES = {
     'sb_dm_project': (C.c_int, [fp, C.c_int, C.c_int, C.c_int, fp, C.c_int, C.c_float, ip, fp, vp]),
     'sb_atmo_evolve': (C.c_int, [C.POINTER(AtmoLayer), C.c_int, C.c_int, vp, vp]),
     'sb_propagate_on_axis': (C.c_int, [C.POINTER(PropLayer), C.c_int, C.c_int, fp, fp, vp]),
+    'sb_sh_slopes_jacobian': (C.c_int, [C.POINTER(ShPlan), fp, fp, C.c_int, ip, fp, fp, fp, fp, fp, fp, vp]),
+    'sb_sh_slopes_vjp': (C.c_int, [C.POINTER(ShPlan), fp, fp, C.c_int, ip, fp, fp, fp, fp, fp, fp, vp]),
+    'sb_intmat_contract': (C.c_int, [fp, fp, C.c_int, C.c_int, C.c_int, C.c_int, ip, ip, fp, C.c_int, C.c_int,
+                                     C.c_float, fp, vp]),
 }
 
 _lib = None

@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
 ROOT = os.path.dirname(PKG)
 OUT = os.path.join(PKG, 'libspecula_b200.so')
-SOURCES = ['sb_common.cu', 'sb_sh.cu', 'sb_detector.cu', 'sb_control.cu', 'sb_atmo.cu']
+SOURCES = ['sb_common.cu', 'sb_sh.cu', 'sb_detector.cu', 'sb_control.cu', 'sb_atmo.cu', 'sb_adjoint.cu']
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 
 
@@ -29,7 +29,7 @@ def needs_build():
     if not os.path.exists(OUT):
         return True
     t = os.path.getmtime(OUT)
-    deps = [os.path.join(HERE, s) for s in SOURCES] + [os.path.join(HERE, 'sb_common.cuh'),
+    deps = [os.path.join(HERE, s) for s in SOURCES] + [os.path.join(HERE, 'sb_common.cuh'), os.path.join(HERE, 'sb_dft.cuh'),
                                                        os.path.join(ROOT, 'include', 'specula_b200.h'),
                                                        __file__]
     return any(os.path.getmtime(d) > t for d in deps)

@@ -283,6 +283,20 @@ def convert_ref_fits():
     return out
 
 
+def make_zernike_cases():
+    """IFunc(type_str='zernike') tables (compute_zern_ifunc.py:6-29)."""
+    from specula.lib.compute_zern_ifunc import compute_zern_ifunc
+    out = {}
+    for dim, nz, obs in ZERNIKE_CASES:
+        z, m = compute_zern_ifunc(dim, nz, xp=np, dtype=np.float32, obsratio=obs)
+        out['zern_%d_%d/ifunc' % (dim, nz)] = z
+        out['zern_%d_%d/mask' % (dim, nz)] = m
+    return out
+
+
+ZERNIKE_CASES = [(32, 10, 0.14), (48, 21, 0.0)]
+
+
 def main():
     import subprocess
     # The reference binds its global precision at import time
@@ -298,6 +312,7 @@ def main():
         json.dump(geoms, f, indent=1, sort_keys=True)
     chain = make_chain_cases()
     np.savez_compressed(os.path.join(HERE, 'chain_fp32.npz'), **chain)
+    np.savez_compressed(os.path.join(HERE, 'zernike_fp32.npz'), **make_zernike_cases())
     print('wrote', sorted(os.listdir(HERE)))
 
 
@@ -312,5 +327,9 @@ def main_fp64():
 if __name__ == '__main__':
     if '--fp64' in sys.argv:
         main_fp64()
+    elif '--zernike' in sys.argv:      # only the Zernike influence-function tables
+        import specula
+        specula.init(-1, precision=1)
+        np.savez_compressed(os.path.join(HERE, 'zernike_fp32.npz'), **make_zernike_cases())
     else:
         main()

@@ -1,0 +1,237 @@
+"""GPU parity of the SH slopes adjoint and the adjoint interaction matrix
+(sb_sh_slopes_jacobian, sb_sh_slopes_vjp, sb_intmat_contract) against the
+float64 oracle: central finite differences of the oracle forward (SH then
+CoG) and the oracle's push-pull matrix at a small amplitude.
+
+Tolerances (written per test): directional derivatives and interaction
+matrices max|d|/max|ref| <= 1e-4; internal consistency of the VJP with the
+Jacobian <= 1e-5.
+"""
+import math
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip('torch')
+
+from oracle import sh as osh, slopec as osl, control as octl  # noqa: E402
+from oracle.masks import make_mask  # noqa: E402
+from tests.cases import SH_CASES, rel_max_err  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+ADJ_TOL = 1e-4
+VJP_TOL = 1e-5
+S0 = 5.0
+FLAT_CASES = [c for c in SH_CASES if c[8] == 1.0]    # one phase sample per lenslet pixel
+
+
+def smooth_field(pix, rng, rms, kmax=5):
+    """Seeded smooth random field (sum of low spatial frequencies), given RMS."""
+    y, x = np.mgrid[0:pix, 0:pix] / pix
+    f = np.zeros((pix, pix))
+    for kx in range(-kmax, kmax + 1):
+        for ky in range(0, kmax + 1):
+            if kx == 0 and ky == 0:
+                continue
+            amp = rng.standard_normal() / (kx * kx + ky * ky) ** (11 / 12)
+            f += amp * np.cos(2 * np.pi * (kx * x + ky * y) + rng.uniform(0, 2 * np.pi))
+    return f * (rms / f.std())
+
+
+def _setup(case):
+    from specula_b200.processing_objects.sh import SH
+    from specula_b200.processing_objects.sh_slopec import ShSlopec
+    from specula_b200.data_objects.electric_field import ElectricField
+    from specula_b200.data_objects.pixels import Pixels
+    from specula_b200.data_objects.subap_data import SubapData
+    from specula_b200.lib.sh_adjoint import ShSlopesAdjoint
+    name, pix, pitch, lam, fov, pxs, n, npx, coeff = case
+    sh = SH(wavelengthInNm=lam, subap_wanted_fov=fov, sensor_pxscale=pxs, subap_on_diameter=n, subap_npx=npx,
+            fov_ovs_coeff=coeff, target_device_idx=0)
+    ef = ElectricField(pix, pix, pitch, S0=S0, target_device_idx=0)
+    A = make_mask(pix, 0.14, 1.0).astype(np.float32)
+    ef.A.copy_(torch.as_tensor(A))
+    sh.inputs['in_ef'].set(ef)
+    sh.setup()
+    geom = osh.sh_geometry(lam, fov, pxs, n, npx, pix, pitch, fov_ovs_coeff=coeff)
+    flat = osh.SHOracle(geom, lam, precision=1).forward(A, np.zeros_like(A), S0, pitch)
+    idxs, dmap = osl.detect_subaps(flat, n, 0.5)
+    px = Pixels(n * npx, n * npx, target_device_idx=0)
+    sl = ShSlopec(SubapData(idxs=idxs, display_map=dmap, nx=n, ny=n, target_device_idx=0), target_device_idx=0)
+    sl.inputs['in_pixels'].set(px)
+    sl.setup()
+    adj = ShSlopesAdjoint(sh, sl)
+    oracle64 = osh.SHOracle(geom, lam, precision=0)
+
+    def slopes64(phase):
+        img = oracle64.forward(A.astype(np.float64), phase, S0, pitch)
+        return osl.sh_slopes(img, idxs, precision=0)[0]
+
+    return dict(sh=sh, sl=sl, adj=adj, A=A, idxs=idxs, lam=lam, pix=pix, n=n, slopes64=slopes64)
+
+
+def _dir_derivative(jac, idxs_lenslet, n, p, delta):
+    """sum_px J[j][px] delta[px] on the host (float64) from the Jacobian blocks."""
+    jac = jac.detach().cpu().numpy().astype(np.float64)
+    out = np.zeros(2 * jac.shape[1])
+    nv = jac.shape[1]
+    for s, L in enumerate(idxs_lenslet):
+        li, lj = divmod(int(L), n)
+        blk = delta[li * p:(li + 1) * p, lj * p:(lj + 1) * p].ravel()
+        out[s] = jac[0, s] @ blk
+        out[nv + s] = jac[1, s] @ blk
+    return out
+
+
+@pytest.mark.parametrize('case', FLAT_CASES, ids=[c[0] for c in FLAT_CASES])
+def test_jacobian_matches_fp64_finite_differences(case, cuda):
+    c = _setup(case)
+    adj, A, lam, pix = c['adj'], c['A'], c['lam'], c['pix']
+    rng = np.random.default_rng(7)
+    nm_per_rad = lam / (2 * math.pi)
+    phase0 = (smooth_field(pix, rng, 0.6) * nm_per_rad * A).astype(np.float32)
+    jac = adj.jacobian(torch.as_tensor(A), torch.as_tensor(phase0))
+    lens = adj._lenslet.cpu().numpy()
+    eps = 1e-3                                   # rad RMS of the probe step
+    for probe in range(4):
+        delta = smooth_field(pix, np.random.default_rng(100 + probe), 1.0) * nm_per_rad
+        ad = _dir_derivative(jac, lens, c['n'], adj.np_sub, delta)
+        p64 = phase0.astype(np.float64)
+        fd = (c['slopes64'](p64 + eps * delta) - c['slopes64'](p64 - eps * delta)) / (2 * eps)
+        assert rel_max_err(ad, fd) <= ADJ_TOL, probe
+
+
+@pytest.mark.parametrize('case', FLAT_CASES[:2], ids=[c[0] for c in FLAT_CASES[:2]])
+def test_vjp_equals_jacobian_transpose(case, cuda):
+    c = _setup(case)
+    adj, A, pix, n = c['adj'], c['A'], c['pix'], c['n']
+    rng = np.random.default_rng(3)
+    phase0 = (smooth_field(pix, rng, 80.0) * A).astype(np.float32)
+    jac = adj.jacobian(torch.as_tensor(A), torch.as_tensor(phase0)).cpu().numpy().astype(np.float64)
+    seed = rng.standard_normal(2 * adj.n_valid).astype(np.float32)
+    got = adj.vjp(torch.as_tensor(A), torch.as_tensor(phase0), torch.as_tensor(seed)).cpu().numpy()
+    ref = np.zeros((pix, pix))
+    p, nv = adj.np_sub, adj.n_valid
+    for s, L in enumerate(adj._lenslet.cpu().numpy()):
+        li, lj = divmod(int(L), n)
+        blk = seed[s] * jac[0, s] + seed[nv + s] * jac[1, s]
+        ref[li * p:(li + 1) * p, lj * p:(lj + 1) * p] = blk.reshape(p, p)
+    assert rel_max_err(got, ref) <= VJP_TOL
+
+
+def _dm(c, n_modes, seed):
+    from specula_b200.processing_objects.dm import DM
+    from specula_b200.data_objects.ifunc import IFunc
+    from specula_b200.data_objects.simul_params import SimulParams
+    from specula_b200.base_value import BaseValue
+    pix, A = c['pix'], c['A']
+    mask = A > 0
+    rng = np.random.default_rng(seed)
+    IF = np.stack([smooth_field(pix, rng, 1.0, kmax=3 + k // 4)[mask] for k in range(n_modes)]).astype(np.float32)
+    sp = SimulParams(pixel_pupil=pix, pixel_pitch=0.05, time_step=0.001)
+    dm = DM(sp, 0, ifunc=IFunc(ifunc=IF, mask=mask.astype(np.float32), target_device_idx=0), target_device_idx=0)
+    dm.inputs['in_command'].set(BaseValue(value=np.zeros(n_modes, np.float32), target_device_idx=0))
+    dm.setup()
+    return dm, IF, mask
+
+
+@pytest.mark.parametrize('case', FLAT_CASES, ids=[c[0] for c in FLAT_CASES])
+def test_adjoint_intmat_matches_fp64_pushpull(case, cuda):
+    c = _setup(case)
+    adj, A, pix = c['adj'], c['A'], c['pix']
+    dm, IF, mask = _dm(c, 10, seed=5)
+    flat = torch.zeros((pix, pix), dtype=torch.float32, device='cuda')
+    im = adj.intmat(torch.as_tensor(A), flat, dm).cpu().numpy()
+    # the reference's push-pull (im_rec_calibrator.py:58-63) in float64 at
+    # a small amplitude (truncation O(a^2) far below the tolerance)
+    amp = 1e-2
+
+    def slopes_fn(k, a):
+        cmd = np.zeros(IF.shape[0])
+        cmd[k] = a
+        return c['slopes64'](octl.dm_phase(IF.astype(np.float64), mask, cmd, sign=dm.sign, precision=0))
+
+    ref = octl.pushpull_intmat(slopes_fn, IF.shape[0], [amp] * IF.shape[0])
+    assert im.shape == ref.shape
+    assert rel_max_err(im, ref) <= ADJ_TOL
+
+
+def test_intmat_contract_matches_host_contraction(cuda):
+    c = _setup(FLAT_CASES[0])
+    adj, A, pix, n = c['adj'], c['A'], c['pix'], c['n']
+    dm, IF, mask = _dm(c, 24, seed=9)
+    rng = np.random.default_rng(1)
+    phase0 = (smooth_field(pix, rng, 60.0) * A).astype(np.float32)
+    jac = adj.jacobian(torch.as_tensor(A), torch.as_tensor(phase0))
+    im = adj.intmat(torch.as_tensor(A), torch.as_tensor(phase0), dm, jac=jac).cpu().numpy()
+    J = jac.cpu().numpy().astype(np.float64)
+    col = np.full(pix * pix, -1)
+    col[np.flatnonzero(mask.ravel())] = np.arange(IF.shape[1])
+    p, nv = adj.np_sub, adj.n_valid
+    ref = np.zeros((IF.shape[0], 2 * nv))
+    for s, L in enumerate(adj._lenslet.cpu().numpy()):
+        li, lj = divmod(int(L), n)
+        cc = col.reshape(pix, pix)[li * p:(li + 1) * p, lj * p:(lj + 1) * p].ravel()
+        f = np.where(cc[None, :] >= 0, IF[:, np.maximum(cc, 0)], 0.0)
+        ref[:, s] = f @ J[0, s]
+        ref[:, nv + s] = f @ J[1, s]
+    ref *= 2 * dm.sign
+    assert rel_max_err(im, ref) <= VJP_TOL
+
+
+def test_gpu_pushpull_matches_fp64_pushpull(cuda):
+    c = _setup(FLAT_CASES[0])
+    adj, A, pix = c['adj'], c['A'], c['pix']
+    dm, IF, mask = _dm(c, 6, seed=4)
+    amp = 10.0
+    im, replay = adj.pushpull_intmat(torch.as_tensor(A), dm, amp)
+    im2 = replay()                                   # second replay of the captured graph
+
+    def slopes_fn(k, a):
+        cmd = np.zeros(IF.shape[0])
+        cmd[k] = a
+        return c['slopes64'](octl.dm_phase(IF.astype(np.float64), mask, cmd, sign=dm.sign, precision=0))
+
+    ref = octl.pushpull_intmat(slopes_fn, IF.shape[0], [amp] * IF.shape[0])
+    # float32 push-pull: the difference of two slope vectors loses digits
+    assert rel_max_err(im.cpu().numpy(), ref) <= 1e-3
+    assert torch.equal(im, im2)
+
+
+def test_calibration_system_adjoint_matches_fp64_pushpull_full_size(cuda):
+    """The 40x40 / 320 px / FFT 16 / 500-Zernike calibration system: the
+    adjoint matrix against the float64 oracle push-pull at a small amplitude
+    on sampled modes (per-mode max|d|/max|ref| <= 1e-4), and against the
+    float32 GPU push-pull at 10 nm (which carries its own O(a^2) truncation
+    and float32 cancellation)."""
+    from specula_b200.calibration import ShCalibrationSystem
+    cal = ShCalibrationSystem()
+    im = cal.adjoint_intmat().cpu().numpy()
+    assert im.shape == (500, 2 * cal.n_valid)
+    sh = cal.sh
+    g = sh.geometry
+    pix = cal.pupil.shape[0]
+    geom = osh.sh_geometry(sh._wavelengthInNm, sh._subap_wanted_fov_arcsec, sh._sensor_pxscale_arcsec, g.n_lenses,
+                           g.subap_npx, pix, cal.simul_params.pixel_pitch, fov_ovs_coeff=1.0)
+    o64 = osh.SHOracle(geom, sh._wavelengthInNm, precision=0)
+    A = cal.pupil.astype(np.float64)
+    IF = cal.dm._ifunc.influence_function.cpu().numpy().astype(np.float64)
+    idxs = cal.subapdata.idxs
+    amp = 1e-2
+
+    def s64(k, a):
+        cmd = np.zeros(IF.shape[0])
+        cmd[k] = a
+        ph = octl.dm_phase(IF, cal.pupil, cmd, sign=cal.dm.sign, precision=0)
+        return osl.sh_slopes(o64.forward(A, ph, 1.0, cal.simul_params.pixel_pitch), idxs, precision=0)[0]
+
+    for k in (0, 1, 4, 20, 100, 250, 499):
+        ref = (s64(k, amp) - s64(k, -amp)) / amp
+        assert rel_max_err(im[k], ref) <= ADJ_TOL, k
+    # the GPU push-pull at 10 nm against the float64 push-pull at 10 nm (same
+    # O(a^2) truncation, which reaches several percent on high-order modes)
+    pp = cal.pushpull_intmat(10.0).cpu().numpy()
+    for k in (0, 20, 499):
+        ref = (s64(k, 10.0) - s64(k, -10.0)) / 10.0
+        assert rel_max_err(pp[k], ref) <= 1e-3, k

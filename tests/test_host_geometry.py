@@ -110,3 +110,14 @@ def test_time_conversion_matches_reference():
     for s, ns in ((0.001, 1000000), (1.0, 1000000000), (0.0015, 1500000), (2.5e-4, 250000), (0.1, 100000000)):
         assert t.seconds_to_t(s) == ns
         assert t.t_to_seconds(ns) == ns / 1e9
+
+
+@pytest.mark.parametrize('dim,nz,obs', [(32, 10, 0.14), (48, 21, 0.0)])
+def test_zernike_ifunc_matches_reference(golden, dim, nz, obs):
+    """specula_b200.lib.zernike against the reference's compute_zern_ifunc
+    output (bit-exact: same float64 evaluation, float32 QR)."""
+    from specula_b200.lib.zernike import compute_zern_ifunc
+    z, m = compute_zern_ifunc(dim, nz, obsratio=obs)
+    ref = golden['zernike_fp32']
+    assert np.array_equal(m, ref['zern_%d_%d/mask' % (dim, nz)])
+    assert np.array_equal(z, ref['zern_%d_%d/ifunc' % (dim, nz)])
