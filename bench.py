@@ -46,6 +46,8 @@ def parse():
     p.add_argument('--cpu-baseline-seconds', type=float, default=20.0)
     p.add_argument('--no-cpu-baseline', action='store_true')
     p.add_argument('--no-adjoint', action='store_true', help='skip the adjoint interaction-matrix leg')
+    p.add_argument('--adjoint-only', action='store_true',
+                   help='run only the adjoint interaction-matrix leg (one GPU) and print its JSON object')
     return p.parse_args()
 
 
@@ -185,19 +187,23 @@ def bench_adjoint_im(dev, reps, cpu_budget_s):
     """Adjoint interaction matrix against push-pull on the 40x40 / 320 px /
     FFT 16 / 500-Zernike calibration system (one B200).  Each timed call is
     bracketed by CUDA events on the launching stream with an L2 flush
-    (256 MB write) between calls."""
+    (256 MB written, then 256 MB read) between calls."""
     import torch
     from specula_b200.calibration import ShCalibrationSystem
     cal = ShCalibrationSystem(device_idx=dev.index)
     st = torch.cuda.current_stream(dev)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    clean = torch.ones(64 * 1024 * 1024, dtype=torch.float32, device=dev)
     amp = 10.0
 
     def timed(fn, n):
         ms = []
         out = None
         for _ in range(n):
+            # evict L2 by writing 256 MB, then read another 256 MB so the
+            # dirty lines are written back before the timed call
             flush.fill_(1.0)
+            clean.sum()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(st)
@@ -231,7 +237,7 @@ def bench_adjoint_im(dev, reps, cpu_budget_s):
            'jacobian_kernel_us': jac_ms * 1e3, 'contract_kernel_us': con_ms * 1e3,
            'contract_roofline': {'bound': 'hbm', 'achieved': con_gbs, 'peak': peak, 'peak_kind': peak_kind,
                                  'unit': 'GB/s', 'frac': con_gbs / peak, 'algorithmic_bytes': con_bytes},
-           'l2': 'flushed (256 MB write) before every timed call'}
+           'l2': 'flushed before every timed call (256 MB written, then 256 MB read)'}
     if cpu_budget_s > 0:
         out['cpu_baseline'] = cpu_pushpull(cal, amp, cpu_budget_s)
     return out
@@ -308,6 +314,7 @@ def run_b200(args):
     e1.record(st)
     torch.cuda.synchronize(dev)
     ms = e0.elapsed_time(e1)
+    _lib.call('sb_device_status')         # raises if a bounded in-kernel wait gave up
     if world > 1:
         dist.barrier()
     clk = clocks.stop()
@@ -409,6 +416,14 @@ def run_b200(args):
 
 def main():
     args = parse()
+    if args.adjoint_only:
+        import torch
+        dev = torch.device('cuda', 0)
+        torch.cuda.set_device(dev)
+        out = bench_adjoint_im(dev, reps=max(3, min(args.steps, 10)),
+                               cpu_budget_s=0 if args.no_cpu_baseline else 10.0)
+        print(json.dumps({'adjoint_im': out}), flush=True)
+        return
     if args.impl == 'reference':
         run_reference(args)
     else:

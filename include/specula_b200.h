@@ -221,11 +221,18 @@ int sb_modalrec_integrator(const float *R, int n_modes, int n_slopes, int ldr, c
  * DM — replaces specula/processing_objects/dm.py:72-86:
  * phase[mask_idx[p]] = sum_m (sign * cmd[m]) * IF[m][p]; IF row-major
  * (n_modes x n_valid) with row stride ld_if >= n_valid.  Pixels outside the
- * mask are not written.
+ * mask are not written.  With 16-byte aligned rows and up to 4096 modes the
+ * influence functions are streamed by 2-D TMA loads (one CTA per SM, small
+ * register and shared-memory footprint so concurrent kernels co-reside).
  * ---------------------------------------------------------------------- */
 int sb_dm_project(const float *ifunc, int n_modes, int n_valid, int ld_if,
                   const float *cmd, int n_cmd, float sign, const int32_t *mask_idx,
                   float *phase, void *stream);
+
+/* Diagnostics: SB_OK, or SB_ETIMEOUT when a bounded wait inside a kernel
+ * (the shared-memory pipeline of sb_dm_project) gave up since the last call;
+ * reading clears it.  Synchronous (waits for the device); not for the step. */
+int sb_device_status(void);
 
 /* ------------------------------------------------------------------------
  * Adjoint of the noise-free SH -> ShSlopec chain, and the interaction

@@ -74,6 +74,7 @@ SIGNATURES = {
     'sb_integrator': (C.c_int, [C.POINTER(IirPlan), fp, fp, vp]),
     'sb_modalrec_integrator': (C.c_int, [fp, C.c_int, C.c_int, C.c_int, fp, fp, C.POINTER(IirPlan), fp, vp]),
     'sb_dm_project': (C.c_int, [fp, C.c_int, C.c_int, C.c_int, fp, C.c_int, C.c_float, ip, fp, vp]),
+    'sb_device_status': (C.c_int, []),
     'sb_atmo_evolve': (C.c_int, [C.POINTER(AtmoLayer), C.c_int, C.c_int, vp, vp]),
     'sb_propagate_on_axis': (C.c_int, [C.POINTER(PropLayer), C.c_int, C.c_int, fp, fp, vp]),
     'sb_sh_slopes_jacobian': (C.c_int, [C.POINTER(ShPlan), fp, fp, C.c_int, ip, fp, fp, fp, fp, fp, fp, vp]),

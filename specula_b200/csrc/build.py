@@ -29,7 +29,7 @@ def needs_build():
     if not os.path.exists(OUT):
         return True
     t = os.path.getmtime(OUT)
-    deps = [os.path.join(HERE, s) for s in SOURCES] + [os.path.join(HERE, 'sb_common.cuh'), os.path.join(HERE, 'sb_dft.cuh'),
+    deps = [os.path.join(HERE, s) for s in SOURCES] + [os.path.join(HERE, 'sb_common.cuh'), os.path.join(HERE, 'sb_dft.cuh'), os.path.join(HERE, 'sb_tma.cuh'),
                                                        os.path.join(ROOT, 'include', 'specula_b200.h'),
                                                        __file__]
     return any(os.path.getmtime(d) > t for d in deps)

@@ -113,18 +113,45 @@ __global__ void __launch_bounds__(256) sh_slopes_adjoint_kernel(AdjArgs a) {
     });
     __syncwarp();
     // detector pixels of the sub-aperture: D = R (|F|^2 M) R^T
-    for (int e = lane; e < NPX2; e += 32) {
-        const int pp = e / NPX, q = e % NPX;
-        float acc = 0.f;
-        for (int aa = 0; aa < CS; ++aa) {
+    if constexpr (CS % NPX == 0) {
+        // integer rebin factor: BF x BF boxes weighted 1/BF^2 (R holds 1/BF
+        // on its band), as in the forward kernel
+        constexpr int BF = CS / NPX;
+        const float wgt = R[0] * R[0];
+        for (int e = lane; e < NPX2; e += 32) {
+            const int pp = e / NPX, q = e % NPX;
+            float acc = 0.f;
+#pragma unroll
+            for (int u = 0; u < BF; ++u)
+#pragma unroll
+                for (int v = 0; v < BF; ++v) {
+                    const int i = (pp * BF + u) * CS + q * BF + v;
+                    const float2 f = F[i];
+                    acc += (f.x * f.x + f.y * f.y) * mask[i];
+                }
+            D[e] = acc * wgt;
+        }
+    } else {
+        // separable: H = I R^T (CS x NPX, in Gf's storage), D = R H
+        float *H = reinterpret_cast<float *>(Gf);
+        for (int e = lane; e < CS * NPX; e += 32) {
+            const int aa = e / NPX, q = e % NPX;
             float h = 0.f;
+#pragma unroll
             for (int b = 0; b < CS; ++b) {
                 const float2 f = F[aa * CS + b];
                 h = fmaf((f.x * f.x + f.y * f.y) * mask[aa * CS + b], R[q * CS + b], h);
             }
-            acc = fmaf(R[pp * CS + aa], h, acc);
+            H[e] = h;
         }
-        D[e] = acc;
+        __syncwarp();
+        for (int e = lane; e < NPX2; e += 32) {
+            const int pp = e / NPX, q = e % NPX;
+            float acc = 0.f;
+#pragma unroll
+            for (int aa = 0; aa < CS; ++aa) acc = fmaf(R[pp * CS + aa], H[aa * NPX + q], acc);
+            D[e] = acc;
+        }
     }
     __syncwarp();
     float tot = 0.f, nx = 0.f, ny = 0.f;
@@ -155,23 +182,37 @@ __global__ void __launch_bounds__(256) sh_slopes_adjoint_kernel(AdjArgs a) {
             D[e] = (a.seed ? vx * gx + vy * gy : (axis == 0 ? gx : gy)) * inv;
         }
         __syncwarp();
-        // T = g R   (NPX x CS), in Y's storage (free until the first GEMM)
-        float *T = reinterpret_cast<float *>(Y);
-        for (int e = lane; e < NPX * CS; e += 32) {
-            const int pp = e / CS, b = e % CS;
-            float t = 0.f;
-            for (int q = 0; q < NPX; ++q) t = fmaf(D[pp * NPX + q], R[q * CS + b], t);
-            T[e] = t;
-        }
-        __syncwarp();
-        // dL/dF = 2 (R^T g R) M F
-        for (int e = lane; e < CS * CS; e += 32) {
-            const int aa = e / CS, b = e % CS;
-            float h = 0.f;
-            for (int pp = 0; pp < NPX; ++pp) h = fmaf(R[pp * CS + aa], T[pp * CS + b], h);
-            const float2 f = F[e];
-            const float gm = 2.0f * h * mask[e];
-            Gf[e] = make_float2(gm * f.x, gm * f.y);
+        if constexpr (CS % NPX == 0) {
+            // R^T g R = g[a / BF][b / BF] / BF^2
+            constexpr int BF = CS / NPX;
+            const float wgt2 = 2.0f * R[0] * R[0];
+            for (int e = lane; e < CS * CS; e += 32) {
+                const int aa = e / CS, b = e % CS;
+                const float2 f = F[e];
+                const float gm = wgt2 * D[(aa / BF) * NPX + b / BF] * mask[e];
+                Gf[e] = make_float2(gm * f.x, gm * f.y);
+            }
+        } else {
+            // T = g R   (NPX x CS), in Y's storage (free until the first GEMM)
+            float *T = reinterpret_cast<float *>(Y);
+            for (int e = lane; e < NPX * CS; e += 32) {
+                const int pp = e / CS, b = e % CS;
+                float t = 0.f;
+#pragma unroll
+                for (int q = 0; q < NPX; ++q) t = fmaf(D[pp * NPX + q], R[q * CS + b], t);
+                T[e] = t;
+            }
+            __syncwarp();
+            // dL/dF = 2 (R^T g R) M F
+            for (int e = lane; e < CS * CS; e += 32) {
+                const int aa = e / CS, b = e % CS;
+                float h = 0.f;
+#pragma unroll
+                for (int pp = 0; pp < NPX; ++pp) h = fmaf(R[pp * CS + aa], T[pp * CS + b], h);
+                const float2 f = F[e];
+                const float gm = 2.0f * h * mask[e];
+                Gf[e] = make_float2(gm * f.x, gm * f.y);
+            }
         }
         __syncwarp();
         // Y = Gf conj(W)   (CS x P)

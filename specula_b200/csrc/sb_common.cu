@@ -20,3 +20,51 @@ void clear_error() { g_last_error[0] = '\0'; }
 extern "C" int sb_version(void) { return 100; }
 
 extern "C" const char *sb_last_error(void) { return sb::g_last_error; }
+
+// ---- TMA tensor maps and device properties (declared in sb_tma.cuh) ----
+#include "sb_tma.cuh"
+
+namespace sb {
+
+namespace {
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+}  // namespace
+
+int tensor_map_2d_f32(CUtensorMap *map, const float *base, int rows, int cols, int ld, int box_rows, int box_cols) {
+    static EncodeTiledFn enc = nullptr;
+    if (!enc) {
+        cudaDriverEntryPointQueryResult qr;
+        void *fn = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &qr) != cudaSuccess ||
+            qr != cudaDriverEntryPointSuccess || !fn)
+            return fail(SB_ECUDA, "cuTensorMapEncodeTiled is not available from the driver");
+        enc = reinterpret_cast<EncodeTiledFn>(fn);
+    }
+    if ((reinterpret_cast<uintptr_t>(base) & 15) || ((size_t)ld * 4) % 16 || ((size_t)box_cols * 4) % 16)
+        return fail(SB_EINVAL, "tensor map: base, row stride and box width must be 16-byte multiples");
+    cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)ld * 4};
+    cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(base), dims, strides, box,
+                           estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(SB_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return SB_OK;
+}
+
+int sm_count() {
+    static int cache[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+    if (cache[dev] == 0) {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+        cache[dev] = n;
+    }
+    return cache[dev];
+}
+
+}  // namespace sb

@@ -2,10 +2,13 @@
 //
 // All three are HBM-streaming: the reconstructor reads R once per step
 // (n_modes x n_slopes), the DM projection reads the influence functions once
-// per step (n_modes x n_valid, the largest array of the loop).  Both kernels
-// issue 16-byte loads with several in flight per thread and reduce in a
-// fixed order, so results are bit-reproducible run to run.
+// per step (n_modes x n_valid, the largest array of the loop).  The
+// reconstructor issues 16-byte loads with several in flight per thread; the
+// DM projection streams the influence functions through shared memory with
+// 2-D TMA loads.  Sums run in a fixed order, so results are bit-reproducible
+// run to run.
 #include "sb_common.cuh"
+#include "sb_tma.cuh"
 
 namespace {
 
@@ -192,7 +195,122 @@ __global__ void __launch_bounds__(256) dm_project_kernel(const float *__restrict
     }
 }
 
+// ---------------------------------------------------------------------------
+// DM projection with TMA.  One CTA per SM.  A producer lane streams boxes of
+// 16 IF rows x 256 columns (16 KB) through a 6-stage ring in shared memory
+// with 2-D TMA loads (L2 evict-first: each IF byte is read once per step);
+// 8 consumer warps, one column per thread, accumulate sum_m c[m] IF[m][col]
+// in mode order and release each stage on an mbarrier.  The CTA keeps ~100 KB
+// of shared memory, 288 threads and few registers, so the latency-bound
+// kernels of the SH chain, running concurrently on another stream, find room
+// on every SM while the copy engine keeps HBM busy.  Every wait is bounded:
+// on timeout the kernel records it in g_dm_status, stops issuing, lets the
+// copies already issued land (bounded as well) and returns.
+// ---------------------------------------------------------------------------
+constexpr int kDmRows = 16;            // IF rows per box
+constexpr int kDmCols = 256;           // IF columns per box (one per consumer thread)
+constexpr int kDmStages = 6;
+constexpr int kDmConsumerWarps = kDmCols / 32;
+constexpr int kDmMaxModes = 4096;      // command vector staged in shared memory
+
+__device__ int g_dm_status = 0;        // nonzero: a bounded wait timed out
+
+size_t dm_tma_smem_bytes(int nmodes) {
+    const int nst = (nmodes + kDmRows - 1) / kDmRows;
+    return 1024 + (size_t)kDmStages * kDmRows * kDmCols * 4 + 2 * kDmStages * 8 + (size_t)nst * kDmRows * 4;
+}
+
+__global__ void __launch_bounds__(32 * (kDmConsumerWarps + 1), 1)
+    dm_project_tma_kernel(const __grid_constant__ CUtensorMap map, int nmodes, int nvalid,
+                          const float *__restrict__ cmd, int ncmd, float sign, const int32_t *__restrict__ idx,
+                          float *__restrict__ phase) {
+    extern __shared__ unsigned char smem_raw[];
+    // TMA destinations aligned to 1024 bytes
+    unsigned char *base = smem_raw + ((1024 - (sb::smem_u32(smem_raw) & 1023)) & 1023);
+    float *ring = reinterpret_cast<float *>(base);
+    uint64_t *full = reinterpret_cast<uint64_t *>(base + (size_t)kDmStages * kDmRows * kDmCols * 4);
+    uint64_t *empty = full + kDmStages;
+    float *c = reinterpret_cast<float *>(empty + kDmStages);
+    __shared__ int abort_flag, issued;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nst = (nmodes + kDmRows - 1) / kDmRows;
+    if (tid == 0) {
+        for (int s = 0; s < kDmStages; ++s) {
+            sb::mbar_init(&full[s], 1);
+            sb::mbar_init(&empty[s], kDmConsumerWarps);
+        }
+        sb::mbar_init_fence();
+        abort_flag = 0;
+        issued = 0;
+    }
+    for (int m = tid; m < nst * kDmRows; m += blockDim.x) c[m] = (m < ncmd && m < nmodes) ? sign * cmd[m] : 0.f;
+    __syncthreads();
+    const int ntiles = (nvalid + kDmCols - 1) / kDmCols;
+    const int bid = blockIdx.x, nblk = gridDim.x;
+    const int my_tiles = bid < ntiles ? (ntiles - 1 - bid) / nblk + 1 : 0;
+    const int total = my_tiles * nst;          // boxes this CTA streams
+    if (warp == kDmConsumerWarps) {
+        if (lane == 0) {
+            const uint64_t pol = sb::l2_evict_first_policy();
+            int q = 0;
+            for (; q < total; ++q) {
+                const int slot = q % kDmStages;
+                // reuse a slot once all consumer warps released its last use
+                if (q >= kDmStages && !sb::mbar_wait(&empty[slot], ((q / kDmStages) - 1) & 1)) {
+                    atomicExch(&g_dm_status, 1);
+                    abort_flag = 1;
+                    break;
+                }
+                if (*(volatile int *)&abort_flag) break;
+                const int tile = bid + (q / nst) * nblk;
+                sb::mbar_arrive_expect_tx(&full[slot], kDmRows * kDmCols * 4);
+                sb::tma_load_2d(ring + (size_t)slot * kDmRows * kDmCols, &map, tile * kDmCols, (q % nst) * kDmRows,
+                                &full[slot], pol);
+            }
+            issued = q;
+        }
+    } else {
+        float acc = 0.f;
+        for (int q = 0; q < total; ++q) {
+            const int slot = q % kDmStages;
+            if (!sb::mbar_wait(&full[slot], (q / kDmStages) & 1)) {
+                atomicExch(&g_dm_status, 2);
+                abort_flag = 1;
+                break;
+            }
+            if (*(volatile int *)&abort_flag) break;
+            const int sg = q % nst;
+            const float *buf = ring + (size_t)slot * kDmRows * kDmCols + tid;
+            const float *cm = c + sg * kDmRows;
+#pragma unroll
+            for (int r = 0; r < kDmRows; ++r) acc = fmaf(cm[r], buf[r * kDmCols], acc);
+            __syncwarp();
+            if (lane == 0) sb::mbar_arrive(&empty[slot]);
+            if (sg == nst - 1) {
+                const int col = (bid + (q / nst) * nblk) * kDmCols + tid;
+                if (col < nvalid) phase[idx[col]] = acc;
+                acc = 0.f;
+            }
+        }
+    }
+    __syncthreads();
+    if (abort_flag && tid == 0) {
+        // let every issued copy land before the shared memory is released
+        for (int q = 0; q < issued; ++q) sb::mbar_wait(&full[q % kDmStages], (q / kDmStages) & 1);
+    }
+}
+
 }  // namespace
+
+extern "C" int sb_device_status(void) {
+    int v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_dm_status, sizeof(int)) != cudaSuccess)
+        return sb::fail(SB_ECUDA, "sb_device_status: %s", cudaGetErrorString(cudaGetLastError()));
+    if (v == 0) return SB_OK;
+    const int zero = 0;
+    cudaMemcpyToSymbol(g_dm_status, &zero, sizeof(int));
+    return sb::fail(SB_ETIMEOUT, "a DM projection wait timed out (%s side)", v == 1 ? "producer" : "consumer");
+}
 
 extern "C" int sb_modalrec(const float *R, int n_modes, int n_slopes, int ldr, const float *slopes, float *modes,
                            void *stream) {
@@ -254,6 +372,28 @@ extern "C" int sb_dm_project(const float *ifunc, int n_modes, int n_valid, int l
     if (n_valid == 0) return SB_OK;
     cudaStream_t st = sb::as_stream(stream);
     const bool vec = (ld_if % 4 == 0) && ((uintptr_t)ifunc % 16 == 0);
+    if (vec && n_modes <= kDmMaxModes) {
+        CUtensorMap map;
+        const int nsm = sb::sm_count();
+        if (nsm > 0 && sb::tensor_map_2d_f32(&map, ifunc, n_modes, ld_if, ld_if, kDmRows, kDmCols) == SB_OK) {
+            const size_t smem = dm_tma_smem_bytes(n_modes);
+            static bool attr_set[64] = {false};
+            int dev = 0;
+            cudaGetDevice(&dev);
+            if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+                const size_t max_smem = dm_tma_smem_bytes(kDmMaxModes);
+                if (cudaFuncSetAttribute(dm_project_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)max_smem) != cudaSuccess)
+                    return sb::fail(SB_ECUDA, "sb_dm_project: %s", cudaGetErrorString(cudaGetLastError()));
+                attr_set[dev] = true;
+            }
+            const int ntiles = (n_valid + kDmCols - 1) / kDmCols;
+            dm_project_tma_kernel<<<ntiles < nsm ? ntiles : nsm, 32 * (kDmConsumerWarps + 1), smem, st>>>(
+                map, n_modes, n_valid, cmd, n_cmd, sign, mask_idx, phase);
+            return sb::check_launch("dm_project_tma_kernel");
+        }
+        sb::clear_error();    // no tensor map: the load/store kernel below
+    }
     const int W = vec ? 4 : 1;
     const size_t smem = (size_t)(n_modes + 8 * 32 * W) * sizeof(float);
     if (smem > 200 * 1024) return sb::fail(SB_ESHAPE, "sb_dm_project: too many modes (%d)", n_modes);

@@ -260,3 +260,30 @@ class ShSlopesAdjoint:
         replay.graph = g
         replay.buffers = (A, phase, pm, S, amps)
         return replay(), replay
+
+
+class ShSlopesFunction(torch.autograd.Function):
+    """slopes = SH+CoG(phase) as a differentiable torch operation: forward
+    through sb_sh_forward + sb_slopec, backward through sb_sh_slopes_vjp
+    (the CoG cut-off is held at the forward point)."""
+
+    @staticmethod
+    def forward(ctx, phase, adj, A):
+        phase = phase.detach().contiguous()
+        slopes, flux = adj.slopes(A, phase)
+        active = adj.active_from_flux(flux)
+        ctx.adj, ctx.A = adj, A
+        ctx.save_for_backward(phase, active)
+        return slopes.clone()
+
+    @staticmethod
+    def backward(ctx, grad_slopes):
+        phase, active = ctx.saved_tensors
+        g = ctx.adj.vjp(ctx.A, phase, grad_slopes.contiguous(), active=active)
+        return g, None, None
+
+
+def sh_slopes(adj, A, phase):
+    """Differentiable noise-free slopes of ``adj``'s SH + ShSlopec at
+    (A, phase); ``phase`` may require grad."""
+    return ShSlopesFunction.apply(phase, adj, A)

@@ -72,7 +72,7 @@ def compute_zern_ifunc(dim, nzern, obsratio=0.0, diaratio=1.0, start_mode=0, mas
     2..nzern+1) on ``mask`` (default: make_mask(dim, obsratio, diaratio)),
     and the mask as ``dtype``."""
     if mask is None:
-        mask = make_mask(dim, obsratio, diaratio)
+        mask = make_mask(dim, 0.0 if obsratio is None else obsratio, 1.0 if diaratio is None else diaratio)
     mask = np.asarray(mask).astype(float)
     idx = np.where(mask)
     mask = mask.astype(dtype)

@@ -235,3 +235,81 @@ def test_calibration_system_adjoint_matches_fp64_pushpull_full_size(cuda):
     for k in (0, 20, 499):
         ref = (s64(k, 10.0) - s64(k, -10.0)) / 10.0
         assert rel_max_err(pp[k], ref) <= 1e-3, k
+
+
+def test_im_rec_calibrator_loop_matches_chain_pushpull(cuda):
+    """The reference's calibration loop, object by object: FuncGenerator
+    ('PUSHPULL') -> DM -> AtmoPropagation -> SH -> CCD (noise off) ->
+    ShSlopec -> ImRecCalibrator, against the graph-captured push-pull of
+    ShSlopesAdjoint on the same chain and the adjoint matrix."""
+    from specula_b200.loop_control import LoopControl
+    from specula_b200.processing_objects.func_generator import FuncGenerator
+    from specula_b200.processing_objects.dm import DM
+    from specula_b200.processing_objects.atmo_propagation import AtmoPropagation
+    from specula_b200.processing_objects.sh import SH
+    from specula_b200.processing_objects.ccd import CCD
+    from specula_b200.processing_objects.sh_slopec import ShSlopec
+    from specula_b200.processing_objects.im_rec_calibrator import ImRecCalibrator
+    from specula_b200.data_objects.ifunc import IFunc
+    from specula_b200.data_objects.pupilstop import Pupilstop
+    from specula_b200.data_objects.simul_params import SimulParams
+    from specula_b200.data_objects.source import Source
+    from specula_b200.data_objects.subap_data import SubapData
+    from specula_b200.lib.sh_adjoint import ShSlopesAdjoint
+    from specula_b200.scao import valid_subaps
+    name, pix, pitch, lam, fov, pxs, n, npx, coeff = FLAT_CASES[0]
+    sp = SimulParams(pixel_pupil=pix, pixel_pitch=pitch, time_step=0.001)
+    pupil = make_mask(pix, 0.14, 1.0)
+    n_modes, amp = 6, 10.0
+    rng = np.random.default_rng(21)
+    IF = np.stack([smooth_field(pix, rng, 1.0, kmax=4)[pupil > 0] for _ in range(n_modes)]).astype(np.float32)
+    func = FuncGenerator('PUSHPULL', nmodes=n_modes, vect_amplitude=[amp] * n_modes, target_device_idx=0)
+    dm = DM(sp, 0, ifunc=IFunc(ifunc=IF, mask=pupil, target_device_idx=0), target_device_idx=0)
+    dm.inputs['in_command'].set(func.outputs['output'])
+    pup = Pupilstop(sp, obs_diam=0.14, target_device_idx=0)
+    prop = AtmoPropagation(sp, {'src': Source([0, 0], 8, lam, phot_density_value=50.0)}, target_device_idx=0)
+    prop.inputs['common_layer_list'].set([pup, dm.layer])
+    sh = SH(wavelengthInNm=lam, subap_wanted_fov=fov, sensor_pxscale=pxs, subap_on_diameter=n, subap_npx=npx,
+            fov_ovs_coeff=coeff, target_device_idx=0)
+    sh.inputs['in_ef'].set(prop.outputs['out_src_ef'])
+    ccd = CCD(sp, size=[n * npx, n * npx], dt=0.001, bandw=300, quantum_eff=0.8, target_device_idx=0)
+    ccd.inputs['in_i'].set(sh.outputs['out_i'])
+    idxs, dmap = valid_subaps(pupil, n, npx)
+    sl = ShSlopec(SubapData(idxs=idxs, display_map=dmap, nx=n, ny=n, target_device_idx=0), target_device_idx=0)
+    sl.inputs['in_pixels'].set(ccd.outputs['out_pixels'])
+    cal = ImRecCalibrator(nmodes=n_modes, rec_tag='rec', target_device_idx=0)
+    cal.inputs['in_slopes'].set(sl.outputs['out_slopes'])
+    cal.inputs['in_commands'].set(func.outputs['output'])
+    loop = LoopControl()
+    for k, obj in enumerate([func, dm, prop, sh, ccd, sl, cal]):
+        loop.add(obj, k)
+    loop.start(2 * n_modes * 0.001, 0.001)
+    for _ in range(2 * n_modes):
+        loop.iter()
+    loop.finish()
+    im_loop = cal.intmat.intmat.cpu().numpy()
+    assert cal.rec.recmat.shape == (n_modes, 2 * len(idxs))
+    adj = ShSlopesAdjoint(sh, sl)
+    A = torch.as_tensor(pupil.astype(np.float32), device='cuda')
+    im_pp, _ = adj.pushpull_intmat(A, dm, amp)
+    assert rel_max_err(im_loop, im_pp.cpu().numpy()) <= 1e-3
+    im_adj = adj.intmat(A, torch.zeros_like(A), dm).cpu().numpy()
+    assert rel_max_err(im_loop, im_adj) <= 1e-2       # push-pull carries its O(a^2) truncation at 10 nm
+
+
+def test_autograd_function_gradient_matches_jacobian(cuda):
+    from specula_b200.lib.sh_adjoint import sh_slopes
+    c = _setup(FLAT_CASES[1])
+    adj, A, pix = c['adj'], c['A'], c['pix']
+    rng = np.random.default_rng(12)
+    phase0 = torch.as_tensor((smooth_field(pix, rng, 50.0) * A).astype(np.float32), device='cuda')
+    At = torch.as_tensor(A, device='cuda')
+    w = torch.as_tensor(rng.standard_normal(2 * adj.n_valid).astype(np.float32), device='cuda')
+    ph = phase0.clone().requires_grad_(True)
+    s = sh_slopes(adj, At, ph)
+    (s * w).sum().backward()
+    ref = adj.vjp(At, phase0, w)
+    assert torch.allclose(ph.grad, ref, rtol=0, atol=1e-6 * float(ref.abs().max()))
+    # and the forward equals the processing objects' slopes
+    sl_fwd, _ = adj.slopes(At, phase0)
+    assert torch.equal(s.detach(), sl_fwd)
