@@ -40,8 +40,40 @@ constexpr int kBox = kTile + 8;   // footprint of a tile rotated by < 1 degree, 
 
 __global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgs a) {
     __shared__ float Q[kBox][kBox + 1];
+    __shared__ int fp[5];                 // footprint br0, br1, bc0, bc1 and the interior flag
     const sb_atmo_layer &ly = a.layer[blockIdx.z];
     const int L = a.L;
+    const int x0 = blockIdx.x * kTile, y0 = blockIdx.y * kTile;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    if (tid == 0) {
+        // footprint [br0, br1] x [bc0, bc1] of the tile in the rot90'd layer
+        int br0 = y0, br1 = min(y0 + kTile, L) - 1, bc0 = x0, bc1 = min(x0 + kTile, L) - 1;
+        int interior = 0;
+        if (ly.rotate) {
+            double rmin = 1e300, rmax = -1e300, cmin = 1e300, cmax = -1e300;
+            for (int cy = 0; cy < 2; ++cy)
+                for (int cx = 0; cx < 2; ++cx) {
+                    const double yy = cy ? br1 : br0, xx = cx ? bc1 : bc0;
+                    const double ir = __dadd_rn(__dadd_rn(__dmul_rn(ly.m00, yy), __dmul_rn(ly.m01, xx)), ly.off0);
+                    const double ic = __dadd_rn(__dadd_rn(__dmul_rn(ly.m10, yy), __dmul_rn(ly.m11, xx)), ly.off1);
+                    rmin = fmin(rmin, ir); rmax = fmax(rmax, ir);
+                    cmin = fmin(cmin, ic); cmax = fmax(cmax, ic);
+                }
+            // every sample of the tile at least 0.01 px inside [0, L-1) on
+            // both axes: no edge test, no clamp, all four neighbours on the
+            // grid (the float32 sample positions are within 1e-4 px of these)
+            interior = rmin >= 0.01 && rmax <= L - 1 - 0.01 && cmin >= 0.01 && cmax <= L - 1 - 0.01;
+            br0 = max(0, (int)floor(rmin) - 1);
+            br1 = min(L - 1, (int)floor(rmax) + 2);
+            bc0 = max(0, (int)floor(cmin) - 1);
+            bc1 = min(L - 1, (int)floor(cmax) + 2);
+            // a footprint wider than the staging box means |angle| >= ~6
+            // degrees, which the fractional-degree rotation never produces
+            br1 = min(br1, br0 + kBox - 1);
+            bc1 = min(bc1, bc0 + kBox - 1);
+        }
+        fp[0] = br0; fp[1] = br1; fp[2] = bc0; fp[3] = bc1; fp[4] = interior;
+    }
     // integer position and float32 remainder (atmo_evolution.py:278-279)
     const double np = a.pos[blockIdx.z];
     const double q = floor(np);
@@ -50,106 +82,118 @@ __global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgs a) {
     const float frac = (float)(np - q);
     const float w0 = __fsub_rn(1.0f, frac);
     const int k = ly.rot90;
-    const int x0 = blockIdx.x * kTile, y0 = blockIdx.y * kTile;
-
-    // footprint [br0, br1] x [bc0, bc1] in the rot90'd layer
-    int br0 = y0, br1 = min(y0 + kTile, L) - 1, bc0 = x0, bc1 = min(x0 + kTile, L) - 1;
-    if (ly.rotate) {
-        double rmin = 1e300, rmax = -1e300, cmin = 1e300, cmax = -1e300;
-        for (int cy = 0; cy < 2; ++cy)
-            for (int cx = 0; cx < 2; ++cx) {
-                const double yy = cy ? br1 : br0, xx = cx ? bc1 : bc0;
-                const double ir = __dadd_rn(__dadd_rn(__dmul_rn(ly.m00, yy), __dmul_rn(ly.m01, xx)), ly.off0);
-                const double ic = __dadd_rn(__dadd_rn(__dmul_rn(ly.m10, yy), __dmul_rn(ly.m11, xx)), ly.off1);
-                rmin = fmin(rmin, ir); rmax = fmax(rmax, ir);
-                cmin = fmin(cmin, ic); cmax = fmax(cmax, ic);
-            }
-        br0 = max(0, (int)floor(rmin) - 1);
-        br1 = min(L - 1, (int)floor(rmax) + 2);
-        bc0 = max(0, (int)floor(cmin) - 1);
-        bc1 = min(L - 1, (int)floor(cmax) + 2);
-        // a footprint wider than the staging box means |angle| >= ~6 degrees,
-        // which the fractional-degree rotation never produces; clip safely
-        br1 = min(br1, br0 + kBox - 1);
-        bc1 = min(bc1, bc0 + kBox - 1);
-    }
+    __syncthreads();
+    const int br0 = fp[0], br1 = fp[1], bc0 = fp[2], bc1 = fp[3];
+    const bool interior = fp[4] != 0;
     const int R = br1 - br0 + 1, Cc = bc1 - bc0 + 1;
     // rot90(lerped)[yy][xx] reads screen element base + ra*dR + cb*dC
     // (ra, cb: footprint row / column); thread (tx, ty) of the 32 x 8 block
     // walks the footprint so that tx always runs along screen columns:
-    // along footprint columns for even k, along footprint rows for odd k
-    long long dR, dC, b0;
+    // along footprint columns for even k, along footprint rows for odd k.
+    // Offsets fit in 32 bits (strip rows x row stride < 2^31, checked on the host).
+    int dR, dC, b0;
     switch (k) {
-        case 1: dR = -1; dC = ld; b0 = (long long)bc0 * ld + (L - 1 - br0); break;
-        case 2: dR = -(long long)ld; dC = -1; b0 = (long long)(L - 1 - br0) * ld + (L - 1 - bc0); break;
-        case 3: dR = 1; dC = -(long long)ld; b0 = (long long)(L - 1 - bc0) * ld + br0; break;
-        default: dR = ld; dC = 1; b0 = (long long)br0 * ld + bc0;
+        case 1: dR = -1; dC = ld; b0 = bc0 * ld + (L - 1 - br0); break;
+        case 2: dR = -ld; dC = -1; b0 = (L - 1 - br0) * ld + (L - 1 - bc0); break;
+        case 3: dR = 1; dC = -ld; b0 = (L - 1 - bc0) * ld + br0; break;
+        default: dR = ld; dC = 1; b0 = br0 * ld + bc0;
     }
     const bool odd = k & 1;
     const int n_fast = odd ? R : Cc, n_slow = odd ? Cc : R;
-    const long long d_fast = odd ? dR : dC, d_slow = odd ? dC : dR;
-    for (int sl = threadIdx.y; sl < n_slow; sl += blockDim.y) {
-        const float *ps = row0 + b0 + sl * d_slow;
-        for (int fa = threadIdx.x; fa < n_fast; fa += blockDim.x) {
-            const float *p = ps + fa * d_fast;
-            const float v = __fadd_rn(__fmul_rn(w0, p[0]), __fmul_rn(frac, p[1]));
-            if (odd) Q[fa][sl] = v; else Q[sl][fa] = v;
+    const int d_fast = odd ? dR : dC, d_slow = odd ? dC : dR;
+    {
+        // Q strides of the fast and slow walk: Q[sl][fa] for even k, Q[fa][sl] for odd k
+        const int qs_fast = odd ? kBox + 1 : 1, qs_slow = odd ? 1 : kBox + 1;
+        float *qbase = &Q[0][0];
+        for (int sl = threadIdx.y; sl < n_slow; sl += blockDim.y) {
+            int off = b0 + sl * d_slow + threadIdx.x * d_fast;
+            int qo = sl * qs_slow + threadIdx.x * qs_fast;
+            for (int fa = threadIdx.x; fa < n_fast; fa += blockDim.x) {
+                const float *p = row0 + off;
+                qbase[qo] = __fadd_rn(__fmul_rn(w0, p[0]), __fmul_rn(frac, p[1]));
+                off += 32 * d_fast;
+                qo += 32 * qs_fast;
+            }
         }
     }
     __syncthreads();
     const int x = x0 + threadIdx.x;
+    if (x >= L) return;
+    float *out = ly.out + x;
+    const float scale = ly.scale;
+    if (!ly.rotate) {
+        for (int yi = threadIdx.y; yi < kTile; yi += blockDim.y) {
+            const int y = y0 + yi;
+            if (y < L) out[(size_t)y * L] = __fmul_rn(Q[y - br0][x - bc0], scale);   // atmo_evolution.py:294
+        }
+        return;
+    }
     // the rotation is below one degree: sample = (y + dr, x + dc) with
     // dr = (m00-1) y + m01 x + off0 and dc = m10 y + (m11-1) x + off1 small
     // (|dr|, |dc| < ~12 px), so they are evaluated in float32 to ~1e-6 px.
-    // Only the edge test (sample outside [0, L-1] gives 0) is discontinuous;
-    // within 1e-4 px of an edge it is redone with SciPy's exact float64
-    // expression (m00*y + m01*x) + off0.
     const float a00 = (float)(ly.m00 - 1.0), a01 = (float)ly.m01, a10 = (float)ly.m10, a11 = (float)(ly.m11 - 1.0);
     const float b0f = (float)ly.off0, b1f = (float)ly.off1;
     const float xf = (float)x;
     const float dr_x = fmaf(a01, xf, b0f), dc_x = fmaf(a11, xf, b1f);
+    if (interior) {
+        // every sample of this tile is well inside the layer
+        const float *qb = &Q[0][0] - br0 * (kBox + 1) - bc0;
+        for (int yi = threadIdx.y; yi < kTile; yi += blockDim.y) {
+            const int y = y0 + yi;
+            if (y >= L) break;
+            const float yf = (float)y;
+            const float dr = fmaf(a00, yf, dr_x), dc = fmaf(a10, yf, dc_x);
+            const float fdr = floorf(dr), fdc = floorf(dc);
+            const float fr = dr - fdr, fc = dc - fdc;
+            const float *p = qb + (y + (int)fdr) * (kBox + 1) + x + (int)fdc;
+            const float q00 = p[0], q01 = p[1], q10 = p[kBox + 1], q11 = p[kBox + 2];
+            const float top = fmaf(fc, q01 - q00, q00);
+            const float bot = fmaf(fc, q11 - q10, q10);
+            out[(size_t)y * L] = __fmul_rn(fmaf(fr, bot - top, top), scale);
+        }
+        return;
+    }
+    // tiles near the layer edge: only the edge test (sample outside [0, L-1]
+    // gives 0) is discontinuous; within 1e-4 px of an edge it is redone with
+    // SciPy's exact float64 expression (m00*y + m01*x) + off0
     const float Lm1 = (float)(L - 1);
     for (int yi = threadIdx.y; yi < kTile; yi += blockDim.y) {
         const int y = y0 + yi;
-        if (x >= L || y >= L) continue;
+        if (y >= L) break;
         float v;
-        if (!ly.rotate) {
-            v = Q[y - br0][x - bc0];
-        } else {
-            const float yf = (float)y;
-            const float dr = fmaf(a00, yf, dr_x), dc = fmaf(a10, yf, dc_x);
-            const float irf = yf + dr, icf = xf + dc;
-            bool inside = irf >= 0.f && irf <= Lm1 && icf >= 0.f && icf <= Lm1;
-            const float eps = 1e-4f;
-            if (irf < eps || irf > Lm1 - eps || icf < eps || icf > Lm1 - eps) {
-                const double yd = (double)y, xd = (double)x;
-                const double ir = __dadd_rn(__dadd_rn(__dmul_rn(ly.m00, yd), __dmul_rn(ly.m01, xd)), ly.off0);
-                const double ic = __dadd_rn(__dadd_rn(__dmul_rn(ly.m10, yd), __dmul_rn(ly.m11, xd)), ly.off1);
-                inside = ir >= 0.0 && ir <= (double)(L - 1) && ic >= 0.0 && ic <= (double)(L - 1);
-            }
-            if (!inside) {
-                v = 0.0f;
-            } else {
-                const float fdr = floorf(dr), fdc = floorf(dc);
-                int r0 = y + (int)fdr, c0 = x + (int)fdc;
-                float fr = dr - fdr, fc = dc - fdc;
-                // clamp to the grid (only reachable within 1e-4 px of an edge)
-                if (r0 < 0) { r0 = 0; fr = 0.f; }
-                if (c0 < 0) { c0 = 0; fc = 0.f; }
-                if (r0 > L - 1) { r0 = L - 1; fr = 0.f; }
-                if (c0 > L - 1) { c0 = L - 1; fc = 0.f; }
-                const int qr = r0 - br0, qc = c0 - bc0;
-                const bool rin = r0 + 1 < L, cin = c0 + 1 < L;
-                const float q00 = Q[qr][qc];
-                const float q01 = cin ? Q[qr][qc + 1] : 0.0f;
-                const float q10 = rin ? Q[qr + 1][qc] : 0.0f;
-                const float q11 = (rin && cin) ? Q[qr + 1][qc + 1] : 0.0f;
-                const float top = fmaf(fc, q01 - q00, q00);
-                const float bot = fmaf(fc, q11 - q10, q10);
-                v = fmaf(fr, bot - top, top);
-            }
+        const float yf = (float)y;
+        const float dr = fmaf(a00, yf, dr_x), dc = fmaf(a10, yf, dc_x);
+        const float irf = yf + dr, icf = xf + dc;
+        bool inside = irf >= 0.f && irf <= Lm1 && icf >= 0.f && icf <= Lm1;
+        const float eps = 1e-4f;
+        if (irf < eps || irf > Lm1 - eps || icf < eps || icf > Lm1 - eps) {
+            const double yd = (double)y, xd = (double)x;
+            const double ir = __dadd_rn(__dadd_rn(__dmul_rn(ly.m00, yd), __dmul_rn(ly.m01, xd)), ly.off0);
+            const double ic = __dadd_rn(__dadd_rn(__dmul_rn(ly.m10, yd), __dmul_rn(ly.m11, xd)), ly.off1);
+            inside = ir >= 0.0 && ir <= (double)(L - 1) && ic >= 0.0 && ic <= (double)(L - 1);
         }
-        ly.out[(size_t)y * L + x] = __fmul_rn(v, ly.scale);   // atmo_evolution.py:294
+        if (!inside) {
+            v = 0.0f;
+        } else {
+            const float fdr = floorf(dr), fdc = floorf(dc);
+            int r0 = y + (int)fdr, c0 = x + (int)fdc;
+            float fr = dr - fdr, fc = dc - fdc;
+            // clamp to the grid (only reachable within 1e-4 px of an edge)
+            if (r0 < 0) { r0 = 0; fr = 0.f; }
+            if (c0 < 0) { c0 = 0; fc = 0.f; }
+            if (r0 > L - 1) { r0 = L - 1; fr = 0.f; }
+            if (c0 > L - 1) { c0 = L - 1; fc = 0.f; }
+            const int qr = r0 - br0, qc = c0 - bc0;
+            const bool rin = r0 + 1 < L, cin = c0 + 1 < L;
+            const float q00 = Q[qr][qc];
+            const float q01 = cin ? Q[qr][qc + 1] : 0.0f;
+            const float q10 = rin ? Q[qr + 1][qc] : 0.0f;
+            const float q11 = (rin && cin) ? Q[qr + 1][qc + 1] : 0.0f;
+            const float top = fmaf(fc, q01 - q00, q00);
+            const float bot = fmaf(fc, q11 - q10, q10);
+            v = fmaf(fr, bot - top, top);
+        }
+        out[(size_t)y * L] = __fmul_rn(v, scale);   // atmo_evolution.py:294
     }
 }
 
@@ -189,6 +233,9 @@ extern "C" int sb_atmo_evolve(const sb_atmo_layer *layers, int n_layers, int L, 
         if (!l.screen || !l.out || l.screen_cols < L + 1 || l.screen_ld < l.screen_cols || l.rot90 < 0 ||
             l.rot90 > 3 || !(l.delta >= 0.0))
             return sb::fail(SB_EINVAL, "sb_atmo_evolve: layer %d: bad screen window", k);
+        // element offsets inside the strip window are 32-bit
+        if ((long long)L * l.screen_ld + l.screen_cols >= (1LL << 31))
+            return sb::fail(SB_ESHAPE, "sb_atmo_evolve: layer %d: strip too large", k);
         // the fractional-degree rotation is below 1 degree: the staged
         // footprint of a tile is sized for that
         if (l.rotate && !(fabs(l.m01) < 0.0175 && fabs(l.m10) < 0.0175 && l.m00 > 0.9998 && l.m11 > 0.9998))

@@ -197,20 +197,20 @@ __global__ void __launch_bounds__(256) dm_project_kernel(const float *__restrict
 
 // ---------------------------------------------------------------------------
 // DM projection with TMA.  One CTA per SM.  A producer lane streams boxes of
-// 16 IF rows x 256 columns (16 KB) through a 6-stage ring in shared memory
-// with 2-D TMA loads (L2 evict-first: each IF byte is read once per step);
-// 8 consumer warps, one column per thread, accumulate sum_m c[m] IF[m][col]
-// in mode order and release each stage on an mbarrier.  The CTA keeps ~100 KB
-// of shared memory, 288 threads and few registers, so the latency-bound
+// 32 IF rows x 256 columns (32 KB, one TMA load each) through a 3-stage ring
+// in shared memory (L2 evict-first: each IF byte is read once per step);
+// 2 consumer warps, four columns per thread, accumulate sum_m c[m] IF[m][col]
+// in mode order and release each stage on an mbarrier.  The CTA keeps ~97 KB
+// of shared memory, 96 threads and few registers, so the latency-bound
 // kernels of the SH chain, running concurrently on another stream, find room
 // on every SM while the copy engine keeps HBM busy.  Every wait is bounded:
 // on timeout the kernel records it in g_dm_status, stops issuing, lets the
 // copies already issued land (bounded as well) and returns.
 // ---------------------------------------------------------------------------
-constexpr int kDmRows = 16;            // IF rows per box
-constexpr int kDmCols = 256;           // IF columns per box (one per consumer thread)
-constexpr int kDmStages = 6;
-constexpr int kDmConsumerWarps = kDmCols / 32;
+constexpr int kDmRows = 32;            // IF rows per box (multiple of 4)
+constexpr int kDmCols = 256;           // IF columns per box (four per consumer thread)
+constexpr int kDmStages = 3;
+constexpr int kDmConsumerWarps = kDmCols / 128;   // 4 columns per thread
 constexpr int kDmMaxModes = 4096;      // command vector staged in shared memory
 
 __device__ int g_dm_status = 0;        // nonzero: a bounded wait timed out
@@ -270,7 +270,7 @@ __global__ void __launch_bounds__(32 * (kDmConsumerWarps + 1), 1)
             issued = q;
         }
     } else {
-        float acc = 0.f;
+        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
         for (int q = 0; q < total; ++q) {
             const int slot = q % kDmStages;
             if (!sb::mbar_wait(&full[slot], (q / kDmStages) & 1)) {
@@ -280,16 +280,30 @@ __global__ void __launch_bounds__(32 * (kDmConsumerWarps + 1), 1)
             }
             if (*(volatile int *)&abort_flag) break;
             const int sg = q % nst;
-            const float *buf = ring + (size_t)slot * kDmRows * kDmCols + tid;
-            const float *cm = c + sg * kDmRows;
+            const float4 *buf = reinterpret_cast<const float4 *>(ring + (size_t)slot * kDmRows * kDmCols) + tid;
+            const float4 *cm4 = reinterpret_cast<const float4 *>(c + sg * kDmRows);
 #pragma unroll
-            for (int r = 0; r < kDmRows; ++r) acc = fmaf(cm[r], buf[r * kDmCols], acc);
+            for (int r4 = 0; r4 < kDmRows / 4; ++r4) {
+                const float4 cc = cm4[r4];
+                const float cr[4] = {cc.x, cc.y, cc.z, cc.w};
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const float4 v = buf[(r4 * 4 + k) * (kDmCols / 4)];
+                    acc.x = fmaf(cr[k], v.x, acc.x);
+                    acc.y = fmaf(cr[k], v.y, acc.y);
+                    acc.z = fmaf(cr[k], v.z, acc.z);
+                    acc.w = fmaf(cr[k], v.w, acc.w);
+                }
+            }
             __syncwarp();
             if (lane == 0) sb::mbar_arrive(&empty[slot]);
             if (sg == nst - 1) {
-                const int col = (bid + (q / nst) * nblk) * kDmCols + tid;
-                if (col < nvalid) phase[idx[col]] = acc;
-                acc = 0.f;
+                const int col = (bid + (q / nst) * nblk) * kDmCols + 4 * tid;
+                if (col < nvalid) phase[idx[col]] = acc.x;
+                if (col + 1 < nvalid) phase[idx[col + 1]] = acc.y;
+                if (col + 2 < nvalid) phase[idx[col + 2]] = acc.z;
+                if (col + 3 < nvalid) phase[idx[col + 3]] = acc.w;
+                acc = make_float4(0.f, 0.f, 0.f, 0.f);
             }
         }
     }

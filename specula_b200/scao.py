@@ -187,9 +187,11 @@ class ScaoLoop:
         stream concurrently with AtmoEvolution..Integrator of step t
         (latency-bound).  The DM phase is double-buffered: step t writes
         buffer t%2 while the propagation of step t reads buffer (t-1)%2,
-        which is the reference's ``dm.out_layer:-1`` input.  The graph holds
-        two steps so the buffers alternate statically; after each replay the
-        DM layer tensor holds the latest DM phase, as in the sequential form.
+        which is the reference's ``dm.out_layer:-1`` input; only that
+        propagation waits for DM(t-1), so AtmoEvolution of step t overlaps
+        the end of DM(t-1).  The graph holds two steps so the buffers
+        alternate statically; after each replay the DM layer tensor holds the
+        latest DM phase, as in the sequential form.
         """
         self.step_eager()
         torch.cuda.synchronize(self.device)
@@ -217,20 +219,29 @@ class ScaoLoop:
             self._side = side
             self._cap = cap
             self._bufs = (dm_buf, nxt)
-            chain = [self.atmo, self.prop, self.sh, self.ccd, self.slopec]
+            chain = [self.sh, self.ccd, self.slopec]
             with torch.cuda.graph(g, stream=cap):
                 main = torch.cuda.current_stream(self.device)
+                dm_done = None
                 for par in (1, 0):              # odd step, then even step
+                    # DM(t) needs the integrator output of step t-1
                     side.wait_stream(main)
                     with torch.cuda.stream(side):
                         self.dm.project(nxt[par], dm_buf[par])
+                        ev = torch.cuda.Event()
+                        ev.record(side)
+                    # AtmoEvolution(t) does not depend on the mirror
+                    self.atmo.trigger_code()
+                    # the propagation of step t reads DM(t-1): the previous
+                    # replay (already complete) for the first step of the graph
+                    if dm_done is not None:
+                        main.wait_event(dm_done)
+                    self.prop.trigger_code(phase_override={id(self.dm.layer): dm_buf[1 - par]})
                     for o in chain:
-                        if o is self.prop:
-                            o.trigger_code(phase_override={id(self.dm.layer): dm_buf[1 - par]})
-                        else:
-                            o.trigger_code()
+                        o.trigger_code()
                     self._rec_integ(out_next=nxt[1 - par])
-                    main.wait_stream(side)
+                    dm_done = ev
+                main.wait_stream(side)
             self.steps_per_replay = 2
         torch.cuda.synchronize(self.device)
         self.graph = g
