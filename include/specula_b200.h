@@ -311,6 +311,31 @@ typedef struct sb_atmo_layer {
 int sb_atmo_evolve(const sb_atmo_layer *layers, int n_layers, int L, double *positions,
                    void *stream);
 
+/* Device-resident per-step inputs of AtmoEvolution (the seeing and wind
+ * FuncGenerator outputs) and the constants of atmo_evolution.py:262-294. */
+typedef struct sb_atmo_inputs {
+    const double *seeing;          /* device, 1 value [arcsec]                          */
+    const double *wind_speed;      /* device, n_wind_speed values [m/s] (1: all layers)  */
+    const double *wind_direction;  /* device, n_wind_direction values [deg]              */
+    int n_wind_speed;
+    int n_wind_direction;
+    double delta_time;             /* [s] since the previous step                        */
+    double pixel_pitch;            /* [m]                                                */
+    float pixel_pitch_f;           /* the pitch rounded to float32 (r0-scale arithmetic) */
+    float airmass_pow;             /* float32(airmass) ** (-3/5), as NumPy computes it   */
+    float lambda_factor;           /* float32((wavelength_nm / 500) ** (6/5))            */
+} sb_atmo_inputs;
+
+size_t sb_atmo_work_bytes(int n_layers);
+
+/* sb_atmo_evolve with each layer's shift, rot90, fractional rotation and r0
+ * scale computed on the device from device-resident inputs (the delta,
+ * rot90, rotate, m.., off.. and scale fields of layers[] are not read), so
+ * a captured CUDA graph of this call follows new seeing / wind values.
+ * work: device scratch of sb_atmo_work_bytes(n_layers) bytes. */
+int sb_atmo_evolve_inputs(const sb_atmo_layer *layers, int n_layers, int L, double *positions,
+                          const sb_atmo_inputs *in, void *work, size_t work_bytes, void *stream);
+
 /* ------------------------------------------------------------------------
  * AtmoPropagation, on-axis branch — replaces
  * specula/processing_objects/atmo_propagation.py:105-125 with

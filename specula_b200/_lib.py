@@ -53,6 +53,12 @@ class AtmoLayer(C.Structure):
                 ('off0', C.c_double), ('off1', C.c_double), ('scale', C.c_float), ('out', fp)]
 
 
+class AtmoInputs(C.Structure):
+    _fields_ = [('seeing', vp), ('wind_speed', vp), ('wind_direction', vp), ('n_wind_speed', C.c_int),
+                ('n_wind_direction', C.c_int), ('delta_time', C.c_double), ('pixel_pitch', C.c_double),
+                ('pixel_pitch_f', C.c_float), ('airmass_pow', C.c_float), ('lambda_factor', C.c_float)]
+
+
 class PropLayer(C.Structure):
     _fields_ = [('A', fp), ('phase', fp), ('ld', C.c_int), ('top', C.c_int), ('left', C.c_int)]
 
@@ -76,6 +82,9 @@ SIGNATURES = {
     'sb_dm_project': (C.c_int, [fp, C.c_int, C.c_int, C.c_int, fp, C.c_int, C.c_float, ip, fp, vp]),
     'sb_device_status': (C.c_int, []),
     'sb_atmo_evolve': (C.c_int, [C.POINTER(AtmoLayer), C.c_int, C.c_int, vp, vp]),
+    'sb_atmo_work_bytes': (C.c_size_t, [C.c_int]),
+    'sb_atmo_evolve_inputs': (C.c_int, [C.POINTER(AtmoLayer), C.c_int, C.c_int, vp, C.POINTER(AtmoInputs), vp,
+                                        C.c_size_t, vp]),
     'sb_propagate_on_axis': (C.c_int, [C.POINTER(PropLayer), C.c_int, C.c_int, fp, fp, vp]),
     'sb_sh_slopes_jacobian': (C.c_int, [C.POINTER(ShPlan), fp, fp, C.c_int, ip, fp, fp, fp, fp, fp, fp, vp]),
     'sb_sh_slopes_vjp': (C.c_int, [C.POINTER(ShPlan), fp, fp, C.c_int, ip, fp, fp, fp, fp, fp, fp, vp]),

@@ -14,18 +14,81 @@
 
 namespace {
 
+// per-step layer parameters (atmo_evolution.py:262-294)
+struct LayerDyn {
+    double delta;
+    double m00, m01, m10, m11, off0, off1;
+    int rot90, rotate;
+    float scale;
+};
+
 struct EvolveArgs {
     sb_atmo_layer layer[SB_MAX_LAYERS];
     int n, L;
     double *pos;
+    // per-step parameters computed on the device from device inputs (NULL:
+    // the delta / rot90 / rotation / scale fields of layer[] are used)
+    sb_atmo_inputs in;
+    LayerDyn *dyn;
 };
+
+// Per-step layer parameters from device-resident seeing / wind inputs, with
+// the reference's float64 / float32 arithmetic (atmo_evolution.py:262-294):
+// r0 = 0.9759*0.5/(seeing*4.848) * airmass^(-3/5) and the r0 scale in float32
+// (NumPy promotes the Python-float products to the float32 airmass), shift
+// wind_speed*dt/pitch, rot90 by trunc(dir/90) mod 4 and the fractional-degree
+// rotation about the layer centre (scipy.ndimage.rotate's output->input map).
+__device__ LayerDyn layer_dyn(const sb_atmo_inputs &in, int k, int L) {
+    LayerDyn d;
+    const double seeing = in.seeing[0];
+    const double ws = in.wind_speed[in.n_wind_speed > 1 ? k : 0];
+    const double wd = in.wind_direction[in.n_wind_direction > 1 ? k : 0];
+    const double r0d = __ddiv_rn(__dmul_rn(0.9759, 0.5), __dmul_rn(seeing, 4.848));
+    const float r0 = __fmul_rn((float)r0d, in.airmass_pow);
+    const float r0l = __fmul_rn(r0, in.lambda_factor);
+    const float x = __fdiv_rn(in.pixel_pitch_f, r0l);
+    d.scale = (float)pow((double)x, (double)(5.0f / 6.0f));
+    d.delta = __ddiv_rn(__dmul_rn(ws, in.delta_time), in.pixel_pitch);
+    const double q90 = trunc(__ddiv_rn(wd, 90.0));
+    int k90 = (int)fmod(q90, 4.0);
+    d.rot90 = k90 < 0 ? k90 + 4 : k90;
+    const double frac = wd - trunc(wd);
+    d.rotate = frac != 0.0;
+    double c = 1.0, sn = 0.0;
+    if (d.rotate) {
+        const double t = __ddiv_rn(frac, 180.0);
+        c = cospi(t);
+        sn = sinpi(t);
+    }
+    const double ctr = (L - 1) / 2.0;
+    d.m00 = c; d.m01 = sn; d.m10 = -sn; d.m11 = c;
+    d.off0 = __dsub_rn(ctr, __dadd_rn(__dmul_rn(c, ctr), __dmul_rn(sn, ctr)));
+    d.off1 = __dsub_rn(ctr, __dadd_rn(__dmul_rn(-sn, ctr), __dmul_rn(c, ctr)));
+    return d;
+}
+
+__device__ __forceinline__ LayerDyn static_dyn(const sb_atmo_layer &l) {
+    LayerDyn d;
+    d.delta = l.delta;
+    d.m00 = l.m00; d.m01 = l.m01; d.m10 = l.m10; d.m11 = l.m11; d.off0 = l.off0; d.off1 = l.off1;
+    d.rot90 = l.rot90;
+    d.rotate = l.rotate;
+    d.scale = l.scale;
+    return d;
+}
 
 // new = last + delta; cycle to 0 when new + L reaches the strip width;
 // float64 like the reference's NumPy arithmetic (atmo_evolution.py:269-277)
 __global__ void atmo_advance_kernel(EvolveArgs a) {
     const int k = threadIdx.x;
     if (k >= a.n) return;
-    double np = __dadd_rn(a.pos[k], a.layer[k].delta);
+    double delta = a.layer[k].delta;
+    if (a.dyn) {
+        const LayerDyn d = layer_dyn(a.in, k, a.L);
+        a.dyn[k] = d;
+        delta = d.delta;
+    }
+    double np = __dadd_rn(a.pos[k], delta);
     if (__dadd_rn(np, (double)a.L) >= (double)a.layer[k].screen_cols) np = 0.0;
     a.pos[k] = np;
 }
@@ -41,11 +104,14 @@ constexpr int kBox = kTile + 8;   // footprint of a tile rotated by < 1 degree, 
 __global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgs a) {
     __shared__ float Q[kBox][kBox + 1];
     __shared__ int fp[5];                 // footprint br0, br1, bc0, bc1 and the interior flag
-    const sb_atmo_layer &ly = a.layer[blockIdx.z];
+    __shared__ LayerDyn lyd;              // this layer's per-step parameters
+    const sb_atmo_layer &lys = a.layer[blockIdx.z];
+    const LayerDyn &ly = lyd;
     const int L = a.L;
     const int x0 = blockIdx.x * kTile, y0 = blockIdx.y * kTile;
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
     if (tid == 0) {
+        lyd = a.dyn ? a.dyn[blockIdx.z] : static_dyn(lys);
         // footprint [br0, br1] x [bc0, bc1] of the tile in the rot90'd layer
         int br0 = y0, br1 = min(y0 + kTile, L) - 1, bc0 = x0, bc1 = min(x0 + kTile, L) - 1;
         int interior = 0;
@@ -77,12 +143,12 @@ __global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgs a) {
     // integer position and float32 remainder (atmo_evolution.py:278-279)
     const double np = a.pos[blockIdx.z];
     const double q = floor(np);
-    const float *row0 = ly.screen + (long long)q;
-    const int ld = ly.screen_ld;
+    const float *row0 = lys.screen + (long long)q;
+    const int ld = lys.screen_ld;
     const float frac = (float)(np - q);
     const float w0 = __fsub_rn(1.0f, frac);
+    __syncthreads();                      // lyd and fp written by thread 0
     const int k = ly.rot90;
-    __syncthreads();
     const int br0 = fp[0], br1 = fp[1], bc0 = fp[2], bc1 = fp[3];
     const bool interior = fp[4] != 0;
     const int R = br1 - br0 + 1, Cc = bc1 - bc0 + 1;
@@ -119,7 +185,7 @@ __global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgs a) {
     __syncthreads();
     const int x = x0 + threadIdx.x;
     if (x >= L) return;
-    float *out = ly.out + x;
+    float *out = lys.out + x;
     const float scale = ly.scale;
     if (!ly.rotate) {
         for (int yi = threadIdx.y; yi < kTile; yi += blockDim.y) {
@@ -220,31 +286,35 @@ __global__ void __launch_bounds__(256) propagate_kernel(PropArgs a, float *__res
 
 }  // namespace
 
-extern "C" int sb_atmo_evolve(const sb_atmo_layer *layers, int n_layers, int L, double *positions, void *stream) {
-    sb::clear_error();
-    if (!layers || !positions || n_layers < 0 || L < 1) return sb::fail(SB_EINVAL, "sb_atmo_evolve: bad args");
-    if (n_layers > SB_MAX_LAYERS) return sb::fail(SB_ESHAPE, "sb_atmo_evolve: at most %d layers", SB_MAX_LAYERS);
+namespace {
+
+int launch_evolve(const char *who, const sb_atmo_layer *layers, int n_layers, int L, double *positions,
+                  const sb_atmo_inputs *in, LayerDyn *dyn, void *stream) {
+    if (!layers || !positions || n_layers < 0 || L < 1) return sb::fail(SB_EINVAL, "%s: bad args", who);
+    if (n_layers > SB_MAX_LAYERS) return sb::fail(SB_ESHAPE, "%s: at most %d layers", who, SB_MAX_LAYERS);
     if (n_layers == 0) return SB_OK;
     EvolveArgs a;
     for (int k = 0; k < n_layers; ++k) {
         const sb_atmo_layer &l = layers[k];
         // the window [pos, pos + L] must stay inside the strip for every
         // position the cycling rule allows: pos + L < screen_cols
-        if (!l.screen || !l.out || l.screen_cols < L + 1 || l.screen_ld < l.screen_cols || l.rot90 < 0 ||
-            l.rot90 > 3 || !(l.delta >= 0.0))
-            return sb::fail(SB_EINVAL, "sb_atmo_evolve: layer %d: bad screen window", k);
+        if (!l.screen || !l.out || l.screen_cols < L + 1 || l.screen_ld < l.screen_cols ||
+            (!in && (l.rot90 < 0 || l.rot90 > 3 || !(l.delta >= 0.0))))
+            return sb::fail(SB_EINVAL, "%s: layer %d: bad screen window", who, k);
         // element offsets inside the strip window are 32-bit
         if ((long long)L * l.screen_ld + l.screen_cols >= (1LL << 31))
-            return sb::fail(SB_ESHAPE, "sb_atmo_evolve: layer %d: strip too large", k);
+            return sb::fail(SB_ESHAPE, "%s: layer %d: strip too large", who, k);
         // the fractional-degree rotation is below 1 degree: the staged
         // footprint of a tile is sized for that
-        if (l.rotate && !(fabs(l.m01) < 0.0175 && fabs(l.m10) < 0.0175 && l.m00 > 0.9998 && l.m11 > 0.9998))
-            return sb::fail(SB_EINVAL, "sb_atmo_evolve: layer %d: rotation must be below one degree", k);
+        if (!in && l.rotate && !(fabs(l.m01) < 0.0175 && fabs(l.m10) < 0.0175 && l.m00 > 0.9998 && l.m11 > 0.9998))
+            return sb::fail(SB_EINVAL, "%s: layer %d: rotation must be below one degree", who, k);
         a.layer[k] = l;
     }
     a.n = n_layers;
     a.L = L;
     a.pos = positions;
+    a.dyn = dyn;
+    if (in) a.in = *in;
     cudaStream_t st = sb::as_stream(stream);
     atmo_advance_kernel<<<1, 32, 0, st>>>(a);
     int rc = sb::check_launch("atmo_advance_kernel");
@@ -252,6 +322,33 @@ extern "C" int sb_atmo_evolve(const sb_atmo_layer *layers, int n_layers, int L, 
     dim3 block(32, 8), grid((L + kTile - 1) / kTile, (L + kTile - 1) / kTile, n_layers);
     atmo_evolve_kernel<<<grid, block, 0, st>>>(a);
     return sb::check_launch("atmo_evolve_kernel");
+}
+
+}  // namespace
+
+extern "C" int sb_atmo_evolve(const sb_atmo_layer *layers, int n_layers, int L, double *positions, void *stream) {
+    sb::clear_error();
+    return launch_evolve("sb_atmo_evolve", layers, n_layers, L, positions, nullptr, nullptr, stream);
+}
+
+extern "C" size_t sb_atmo_work_bytes(int n_layers) {
+    if (n_layers < 0 || n_layers > SB_MAX_LAYERS) return 0;
+    return ((size_t)n_layers * sizeof(LayerDyn) + 255) & ~(size_t)255;
+}
+
+extern "C" int sb_atmo_evolve_inputs(const sb_atmo_layer *layers, int n_layers, int L, double *positions,
+                                     const sb_atmo_inputs *in, void *work, size_t work_bytes, void *stream) {
+    sb::clear_error();
+    if (!in || !in->seeing || !in->wind_speed || !in->wind_direction || in->n_wind_speed < 1 ||
+        in->n_wind_direction < 1 || !(in->pixel_pitch > 0.0) || !(in->delta_time >= 0.0))
+        return sb::fail(SB_EINVAL, "sb_atmo_evolve_inputs: bad inputs");
+    if ((in->n_wind_speed != 1 && in->n_wind_speed != n_layers) ||
+        (in->n_wind_direction != 1 && in->n_wind_direction != n_layers))
+        return sb::fail(SB_ESHAPE, "sb_atmo_evolve_inputs: wind vectors must have 1 or %d values", n_layers);
+    if (!work || work_bytes < sb_atmo_work_bytes(n_layers))
+        return sb::fail(SB_ESCRATCH, "sb_atmo_evolve_inputs: work needs %zu bytes", sb_atmo_work_bytes(n_layers));
+    return launch_evolve("sb_atmo_evolve_inputs", layers, n_layers, L, positions, in,
+                         static_cast<LayerDyn *>(work), stream);
 }
 
 extern "C" int sb_propagate_on_axis(const sb_prop_layer *layers, int n_layers, int pupil, float *A_out,

@@ -62,7 +62,7 @@ __constant__ float c_logfact[32] = {0.0f, 0.0f, 0.693147181f, 1.79175947f, 3.178
 __device__ __forceinline__ float log_factorial(float k, const float *tbl) {
     if (k < 32.0f) return tbl[(int)k];
     const float z = k + 1.0f, iz = 1.0f / z, iz2 = iz * iz;
-    return (z - 0.5f) * logf(z) - z + 0.91893853f + iz * (0.083333333f - iz2 * (0.0027777778f - iz2 * 0.00079365079f));
+    return (z - 0.5f) * __logf(z) - z + 0.91893853f + iz * (0.083333333f - iz2 * (0.0027777778f - iz2 * 0.00079365079f));
 }
 
 // Poisson(lam) in float32 arithmetic.  lam < 10: sequential-search
@@ -75,7 +75,7 @@ __device__ float poisson_sample(float lam, uint32_t e, uint64_t frame, uint64_t 
     if (lam < 10.0f) {
         const u4 r = philox4x32_10({e, (uint32_t)frame, (uint32_t)(frame >> 32), 0u}, k0, k1);
         const float u = u01f(r.x);
-        float pk = expf(-lam), cdf = pk;
+        float pk = __expf(-lam), cdf = pk;
         int k = 0;
         while (u > cdf && k < 100) {
             ++k;
@@ -84,11 +84,14 @@ __device__ float poisson_sample(float lam, uint32_t e, uint64_t frame, uint64_t 
         }
         return (float)k;
     }
-    const float slam = sqrtf(lam), loglam = logf(lam);
+    // acceptance tests use the fast log / divide intrinsics: their few-ulp
+    // errors move only decisions that sit on the acceptance boundary
+    const float slam = sqrtf(lam), loglam = __logf(lam);
     const float b = 0.931f + 2.53f * slam;
     const float a = -0.059f + 0.02483f * b;
-    const float log_inv_alpha = logf(1.1239f + 1.1328f / (b - 3.4f));
-    const float vr = 0.9277f - 3.6224f / (b - 2.0f);
+    const float log_inv_alpha = __logf(1.1239f + __fdividef(1.1328f, b - 3.4f));
+    const float vr = 0.9277f - __fdividef(3.6224f, b - 2.0f);
+    const float two_a = 2.0f * a;
     for (uint32_t it = 0; it < 32; ++it) {
         const u4 r = philox4x32_10({e, (uint32_t)frame, (uint32_t)(frame >> 32), 1u + it}, k0, k1);
 #pragma unroll
@@ -96,10 +99,11 @@ __device__ float poisson_sample(float lam, uint32_t e, uint64_t frame, uint64_t 
             const float U = u01f(h ? r.z : r.x) - 0.5f;
             const float V = u01f(h ? r.w : r.y);
             const float us = 0.5f - fabsf(U);
-            const float k = floorf((2.0f * a / us + b) * U + lam + 0.43f);
+            const float k = floorf((__fdividef(two_a, us) + b) * U + lam + 0.43f);
             if (us >= 0.07f && V <= vr) return k;
             if (k < 0.0f || (us < 0.013f && V > us)) continue;
-            if (logf(V) + log_inv_alpha - logf(a / (us * us) + b) <= -lam + k * loglam - log_factorial(k, logfact))
+            if (__logf(V) + log_inv_alpha - __logf(__fdividef(a, us * us) + b) <=
+                -lam + k * loglam - log_factorial(k, logfact))
                 return k;
         }
     }
@@ -110,10 +114,10 @@ __device__ float poisson_sample(float lam, uint32_t e, uint64_t frame, uint64_t 
 __device__ __forceinline__ float std_normal(uint32_t e, uint64_t frame, uint64_t seed) {
     const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32) ^ kReadoutTag;
     const u4 r = philox4x32_10({e, (uint32_t)frame, (uint32_t)(frame >> 32), 0u}, k0, k1);
-    return sqrtf(-2.0f * logf(u01f(r.x))) * cospif(2.0f * u01f(r.y));
+    return sqrtf(-2.0f * __logf(u01f(r.x))) * cospif(2.0f * u01f(r.y));
 }
 
-__global__ void __launch_bounds__(256, 6) ccd_kernel(sb_ccd_params p, const float *__restrict__ in,
+__global__ void __launch_bounds__(256, 5) ccd_kernel(sb_ccd_params p, const float *__restrict__ in,
                                                   float *__restrict__ integ, float *__restrict__ pix) {
     // frame bookkeeping lives on the device; every block reads it before the
     // last block to finish advances it (see the end of the kernel)
@@ -125,6 +129,8 @@ __global__ void __launch_bounds__(256, 6) ccd_kernel(sb_ccd_params p, const floa
     const uint64_t frame = vs->frame_index;
     const int nint = vs->n_integrated + 1;
     const bool readout = nint >= p.frames_per_read;
+    const double inv_gain = 1.0 / (double)p.adu_gain;
+    const bool gain_pow2 = (__double_as_longlong((double)p.adu_gain) & 0x000FFFFFFFFFFFFFLL) == 0;
     __syncthreads();
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < p.n_pixels; e += gridDim.x * blockDim.x) {
         // integrated_i += i * (loop_dt * bandw)   (ccd.py:205)
@@ -145,7 +151,9 @@ __global__ void __launch_bounds__(256, 6) ccd_kernel(sb_ccd_params p, const floa
             double x = rint(v * (double)p.adu_gain) + (double)p.adu_bias;
             x = x < 0.0 ? 0.0 : x;
             x -= (double)p.adu_bias;
-            x = trunc(x / (double)p.adu_gain);
+            // a power-of-two gain (the default 8) divides exactly by its
+            // reciprocal; any other gain takes the float64 division
+            x = trunc(gain_pow2 ? x * inv_gain : x / (double)p.adu_gain);
             if (p.dark_noise) x -= (double)p.dark_level;
             outv = (float)x;
         } else {

@@ -4,11 +4,16 @@ specula/processing_objects/atmo_evolution.py:14-323).
 Screens are synthesised once at construction (float64 on the device,
 specula_b200.lib.phasescreen) and cut into per-layer strips exactly as
 atmo_evolution.py:164-226 does (sqrt(Cn2), de-mean, nm, odd layers
-flipped), then stored in float32.  Each step is one sb_atmo_evolve call:
-the layer positions live on the device in float64 and are advanced by
-wind_speed * dt / pitch with the reference's cycling rule, then every layer
-gets the column lerp, rot90, fractional-degree rotation and r0 scaling.
+flipped), then stored in float32.  Each step is one sb_atmo_evolve_inputs
+call: the seeing and wind inputs are read on the device (float64 CUDA
+tensors are used in place, anything else is staged into device buffers),
+the per-layer shift, rot90, fractional-degree rotation and r0 scale are
+computed there, the layer positions (float64, on the device) advance by
+wind_speed * dt / pitch with the reference's cycling rule, and every layer
+gets the column lerp, rot90, rotation and r0 scaling.  A captured CUDA
+graph of trigger_code() therefore follows new input values.
 """
+import ctypes
 import math
 
 import numpy as np
@@ -139,13 +144,59 @@ class AtmoEvolution(BaseProcessingObj):
         for s in self.phasescreens:
             if s.dtype != torch.float32 or s.device != self.device or not s.is_contiguous():
                 raise ValueError('AtmoEvolution: phase screens must be contiguous float32 on the device')
+        n = self.n_phasescreens
+        L = int(self.pixel_layer[0])
+        arr = (_lib.AtmoLayer * n)()
+        for k, (p, out) in enumerate(zip(self.phasescreens, self.layer_list)):
+            arr[k].screen = p.data_ptr()
+            arr[k].screen_ld = p.stride(0)
+            arr[k].screen_cols = p.shape[1]
+            arr[k].out = out.phaseInNm.data_ptr()
+        self._layers = arr
+        self._stage = {name: torch.zeros(1 if name == 'seeing' else n, dtype=torch.float64, device=self.device)
+                       for name in ('seeing', 'wind_speed', 'wind_direction')}
+        nb = _lib.load().sb_atmo_work_bytes(n)
+        self._work = torch.empty(max(nb, 1), dtype=torch.uint8, device=self.device)
+        # float32 constants of the r0 scale, with NumPy's promotion rules
+        # (atmo_evolution.py:265-267: Python floats meet the float32 airmass)
+        self._airmass_pow = float(self.airmass ** (-3. / 5.))
+        self._lambda_factor = float(np.float32((self.wavelengthInNm / 500.0) ** (6. / 5.)))
+        self._pitch_f = float(np.float32(self.pixel_pitch))
+        del L
 
     def prepare_trigger(self, t):
         super().prepare_trigger(t)
         self.delta_time = self.t_to_seconds(self.current_time - self.last_t) + self.extra_delta_time
 
+    def _device_input(self, name):
+        """(pointer, count) of a float64 device vector holding input `name`:
+        the input tensor itself when it already is one, else a staged copy."""
+        v = self.local_inputs[name].value
+        n_max = 1 if name == 'seeing' else self.n_phasescreens
+        if (isinstance(v, torch.Tensor) and v.device == self.device and v.dtype == torch.float64
+                and v.is_contiguous() and v.numel() in (1, n_max)):
+            return v.data_ptr(), v.numel()
+        dst = self._stage[name]
+        src = torch.as_tensor(np.asarray(cpuArray(v), dtype=np.float64) if not isinstance(v, torch.Tensor) else v)
+        src = src.to(device=self.device, dtype=torch.float64).reshape(-1)
+        if src.numel() not in (1, n_max):
+            raise ValueError(f'AtmoEvolution: {name} has {src.numel()} values for {n_max} layers')
+        dst.copy_(src.expand(dst.numel()) if src.numel() == 1 else src)
+        return dst.data_ptr(), dst.numel()
+
+    def inputs_struct(self, delta_time):
+        """sb_atmo_inputs for this step (device pointers to the inputs)."""
+        ps, _ = self._device_input('seeing')
+        pw, nw = self._device_input('wind_speed')
+        pd, nd = self._device_input('wind_direction')
+        return _lib.AtmoInputs(seeing=ps, wind_speed=pw, wind_direction=pd, n_wind_speed=nw, n_wind_direction=nd,
+                               delta_time=float(delta_time), pixel_pitch=float(self.pixel_pitch),
+                               pixel_pitch_f=self._pitch_f, airmass_pow=self._airmass_pow,
+                               lambda_factor=self._lambda_factor)
+
     def layer_params(self, delta_time):
-        """Per-layer kernel descriptors for this step (atmo_evolution.py:262-294)."""
+        """Per-layer kernel descriptors computed on the host
+        (atmo_evolution.py:262-294), for sb_atmo_evolve."""
         seeing = float(cpuArray(self.local_inputs['seeing'].value))
         ws = np.broadcast_to(np.asarray(cpuArray(self.local_inputs['wind_speed'].value), dtype=np.float64),
                              (self.n_phasescreens,))
@@ -179,10 +230,10 @@ class AtmoEvolution(BaseProcessingObj):
         return arr
 
     def trigger_code(self):
-        arr = self.layer_params(self.delta_time)
         L = int(self.pixel_layer[0])
-        _lib.call('sb_atmo_evolve', arr, len(self.phasescreens), L, self._positions.data_ptr(),
-                  self.stream_handle())
+        inp = self.inputs_struct(self.delta_time)
+        _lib.call('sb_atmo_evolve_inputs', self._layers, self.n_phasescreens, L, self._positions.data_ptr(),
+                  ctypes.byref(inp), self._work.data_ptr(), self._work.numel(), self.stream_handle())
 
     def post_trigger(self):
         for layer in self.layer_list:

@@ -110,9 +110,14 @@ class ScaoLoop:
         phot_total = c.photons_per_subap * n_valid_est
         S0 = phot_total / (pupil.sum() * c.pitch ** 2 * c.time_step * 1.0)
 
-        self.seeing = BaseValue(value=c.seeing, target_device_idx=device_idx)
-        self.wind_speed = BaseValue(value=np.array(c.wind_speed, dtype=float), target_device_idx=device_idx)
-        self.wind_direction = BaseValue(value=np.array(c.wind_direction, dtype=float), target_device_idx=device_idx)
+        # per-step inputs: float64 device vectors, read in place by AtmoEvolution
+        nl = len(c.heights)
+        self.n_inputs = 1 + 2 * nl
+        self._inputs = torch.tensor([c.seeing] + list(c.wind_speed) + list(c.wind_direction), dtype=torch.float64,
+                                    device=dev)
+        self.seeing = BaseValue(value=self._inputs[0:1], target_device_idx=device_idx)
+        self.wind_speed = BaseValue(value=self._inputs[1:1 + nl], target_device_idx=device_idx)
+        self.wind_direction = BaseValue(value=self._inputs[1 + nl:], target_device_idx=device_idx)
         self.atmo = AtmoEvolution(sp, L0=c.L0, heights=c.heights, Cn2=c.cn2, data_dir='',
                                   pixel_phasescreens=c.pixel_phasescreens, seed=c.screen_seed,
                                   target_device_idx=device_idx)
@@ -159,6 +164,8 @@ class ScaoLoop:
         self.graph = None
         self.pipelined = False
         self.steps_per_replay = 1
+        self.io_inputs = None
+        self.io_outputs = None
         self.n_valid_subaps = len(idxs)
         self.n_valid_pixels = nv
 
@@ -174,7 +181,15 @@ class ScaoLoop:
             v.generation_time = t
         self.loop.iter()
 
-    def capture(self, pipelined=True):
+    def _point_inputs(self, vec):
+        """Make the seeing / wind BaseValues views of a float64 device vector
+        laid out as [seeing, wind_speed (n), wind_direction (n)]."""
+        nl = len(self.cfg.heights)
+        self.seeing.value = vec[0:1]
+        self.wind_speed.value = vec[1:1 + nl]
+        self.wind_direction.value = vec[1 + nl:]
+
+    def capture(self, pipelined=True, io=False):
         """Capture whole steps in a CUDA graph.  Call after at least one eager
         step, so the time step used by AtmoEvolution is the loop's (the first
         step has delta_time = 0).
@@ -198,6 +213,8 @@ class ScaoLoop:
         self.atmo.delta_time = self.atmo.t_to_seconds(self.loop._dt)
         g = torch.cuda.CUDAGraph()
         self.pipelined = bool(pipelined and self.integ.next_output_available)
+        if io and not self.pipelined:
+            raise ValueError('ScaoLoop.capture: io slots need the pipelined form (integer integrator delay >= 1)')
         if not self.pipelined:
             with torch.cuda.graph(g):
                 for o in self.objects[:5]:
@@ -220,10 +237,15 @@ class ScaoLoop:
             self._cap = cap
             self._bufs = (dm_buf, nxt)
             chain = [self.sh, self.ccd, self.slopec]
+            if io:
+                nsl = self.slopec.slopes.slopes.numel()
+                nm = self.integ.out_comm.value.numel()
+                self.io_inputs = self._inputs.repeat(2, 1).contiguous()
+                self.io_outputs = torch.zeros((2, nsl + nm), dtype=torch.float32, device=self.device)
             with torch.cuda.graph(g, stream=cap):
                 main = torch.cuda.current_stream(self.device)
                 dm_done = None
-                for par in (1, 0):              # odd step, then even step
+                for step, par in enumerate((1, 0)):    # odd step, then even step
                     # DM(t) needs the integrator output of step t-1
                     side.wait_stream(main)
                     with torch.cuda.stream(side):
@@ -231,6 +253,8 @@ class ScaoLoop:
                         ev = torch.cuda.Event()
                         ev.record(side)
                     # AtmoEvolution(t) does not depend on the mirror
+                    if io:
+                        self._point_inputs(self.io_inputs[step])
                     self.atmo.trigger_code()
                     # the propagation of step t reads DM(t-1): the previous
                     # replay (already complete) for the first step of the graph
@@ -240,8 +264,13 @@ class ScaoLoop:
                     for o in chain:
                         o.trigger_code()
                     self._rec_integ(out_next=nxt[1 - par])
+                    if io:
+                        self.io_outputs[step, :nsl].copy_(self.slopec.slopes.slopes)
+                        self.io_outputs[step, nsl:].copy_(self.integ.out_comm.value)
                     dm_done = ev
                 main.wait_stream(side)
+            if io:
+                self._point_inputs(self._inputs)
             self.steps_per_replay = 2
         torch.cuda.synchronize(self.device)
         self.graph = g

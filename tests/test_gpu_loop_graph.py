@@ -51,3 +51,48 @@ def test_graph_step_matches_object_loop(mode, cuda):
 def test_fractional_delay_falls_back_to_sequential_graph(cuda):
     loop = _loop('pipelined', 4, cfg_kw=dict(delay=1.5))
     assert not loop.pipelined and loop.steps_per_replay == 1
+
+
+def test_io_graph_follows_per_step_inputs(cuda):
+    """capture(io=True): every replayed step reads its own seeing / wind row
+    from io_inputs and leaves its slopes and commands in io_outputs; the
+    results equal the object-by-object loop fed the same per-step inputs."""
+    from specula_b200.scao import ScaoConfig, ScaoLoop
+    cfg = ScaoConfig(heights=[0.0, 4000.0], cn2=[0.7, 0.3], wind_speed=[10.0, 25.0],
+                     wind_direction=[30.0, 212.7])
+    n_in = 5
+
+    def inputs(t):
+        # step-dependent seeing, wind speed and (fractional-degree) direction
+        return [0.7 + 0.05 * t, 10.0 + t, 25.0 - 0.5 * t, 30.0 + 0.37 * t, 212.7 - 0.61 * t]
+
+    ref = ScaoLoop(cfg, device_idx=0)
+    got = ScaoLoop(cfg, device_idx=0)
+    ref.start()
+    got.start()
+    outs_ref = []
+    # steps 0 and 1 eager in both (capture() runs one eager step itself)
+    for t in range(2):
+        ref._inputs.copy_(torch.tensor(inputs(t), dtype=torch.float64))
+        ref.step_eager()
+    got._inputs.copy_(torch.tensor(inputs(0), dtype=torch.float64))
+    got.step_eager()
+    got._inputs.copy_(torch.tensor(inputs(1), dtype=torch.float64))
+    got.capture(io=True)
+    assert tuple(got.io_inputs.shape) == (2, n_in)
+    nsl = got.slopec.slopes.slopes.numel()
+    for t in range(2, 8):
+        ref._inputs.copy_(torch.tensor(inputs(t), dtype=torch.float64))
+        ref.step_eager()
+        outs_ref.append(torch.cat([ref.slopec.slopes.slopes, ref.integ.out_comm.value]).clone())
+    outs_got = []
+    for r in range(3):
+        for s in range(2):
+            got.io_inputs[s].copy_(torch.tensor(inputs(2 + 2 * r + s), dtype=torch.float64))
+        got.replay()
+        outs_got.extend([got.io_outputs[0].clone(), got.io_outputs[1].clone()])
+    torch.cuda.synchronize()
+    for t, (a, b) in enumerate(zip(outs_ref, outs_got)):
+        assert torch.equal(a[:nsl], b[:nsl]), ('slopes', t)
+        assert torch.equal(a[nsl:], b[nsl:]), ('commands', t)
+    assert torch.equal(ref.atmo.layer_list[1].phaseInNm, got.atmo.layer_list[1].phaseInNm)
