@@ -33,6 +33,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = 'SH loop steps/s at 80x80 subaps'
+# dram__bytes_read.sum + dram__bytes_write.sum of one dm_project_tma_kernel
+# launch of this workload (ncu --set full capture of
+# `bench.py --steps 20 --warmup 3 --no-cpu-baseline --no-adjoint`)
+DM_TRAFFIC_BYTES = 636_357_120
 UNIT = 'steps/s'
 WORKLOAD = 'elt_80x80_fft16_7layers_500modes'
 
@@ -425,8 +429,9 @@ def run_b200(args):
                 'gpu_launches': ScaoLoop.KERNELS_PER_STEP * steps,
                 'step_graph': 'pipelined (DM projection concurrent with the SH chain)' if loop.pipelined
                 else 'sequential',
-                'roofline': {'bound': 'hbm', 'kernel': 'dm_project_kernel', 'achieved': achieved, 'peak': peak,
-                             'peak_kind': peak_kind, 'unit': 'GB/s', 'frac': achieved / peak, 'traffic': None,
+                'roofline': {'bound': 'hbm', 'kernel': 'dm_project_tma_kernel', 'achieved': achieved, 'peak': peak,
+                             'peak_kind': peak_kind, 'unit': 'GB/s', 'frac': achieved / peak, 'traffic': DM_TRAFFIC_BYTES,
+                             'traffic_over_algorithmic': DM_TRAFFIC_BYTES / dm_bytes,
                              'algorithmic_bytes_per_launch': dm_bytes, 'avg_launch_us': dm_ms * 1e3},
                 'step_roofline': {'algorithmic_bytes': step_bytes,
                                   'achieved_gbs': step_bytes / (ms_max / steps / 1e3) / 1e9,
