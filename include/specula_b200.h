@@ -352,6 +352,31 @@ typedef struct sb_prop_layer {
 int sb_propagate_on_axis(const sb_prop_layer *layers, int n_layers, int pupil,
                          float *A_out, float *phase_out, void *stream);
 
+/* ------------------------------------------------------------------------
+ * PSF — replaces specula/processing_objects/psf.py:56-137 (PSF.calc_psf,
+ * the Strehl ratio of trigger_code and the integration of post_trigger).
+ * scratch: sb_psf_scratch_bytes() bytes, zero-filled before the first call
+ * (the Strehl reduction keeps a completion counter there and resets it).
+ * ---------------------------------------------------------------------- */
+size_t sb_psf_scratch_bytes(void);
+
+/* sr = |sum A e^{i phi}|^2 / (sum A)^2 with phi = phase_nm * phase_to_rad,
+ * which equals the reference's centre pixel of the normalised, fftshift-ed
+ * PSF over the flat-phase reference (Parseval); float64 accumulation.
+ * integrate != 0: int_sr[0] += sr, int_sr[1] += 1 (device float64 pair). */
+int sb_strehl(const float *A, const float *phase_nm, int n_pixels, float phase_to_rad, float *sr,
+              double *int_sr, int integrate, void *scratch, size_t scratch_bytes, void *stream);
+
+/* field[e] = A[e] * exp(i * phase_nm[e] * phase_to_rad) as complex64
+ * (interleaved re, im): the input of the PSF's two DFT products. */
+int sb_psf_field(const float *A, const float *phase_nm, int n_pixels, float phase_to_rad, void *field,
+                 void *stream);
+
+/* psf = |F|^2 / sum |F|^2 from the focal-plane field F (complex64), and,
+ * when int_psf is not NULL, int_psf += psf. */
+int sb_psf_finish(const void *focal_field, long long n_pixels, float *psf, float *int_psf, void *scratch,
+                  size_t scratch_bytes, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

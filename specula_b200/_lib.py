@@ -86,6 +86,10 @@ SIGNATURES = {
     'sb_atmo_evolve_inputs': (C.c_int, [C.POINTER(AtmoLayer), C.c_int, C.c_int, vp, C.POINTER(AtmoInputs), vp,
                                         C.c_size_t, vp]),
     'sb_propagate_on_axis': (C.c_int, [C.POINTER(PropLayer), C.c_int, C.c_int, fp, fp, vp]),
+    'sb_psf_scratch_bytes': (C.c_size_t, []),
+    'sb_strehl': (C.c_int, [fp, fp, C.c_int, C.c_float, fp, vp, C.c_int, vp, C.c_size_t, vp]),
+    'sb_psf_field': (C.c_int, [fp, fp, C.c_int, C.c_float, vp, vp]),
+    'sb_psf_finish': (C.c_int, [vp, C.c_longlong, fp, fp, vp, C.c_size_t, vp]),
     'sb_sh_slopes_jacobian': (C.c_int, [C.POINTER(ShPlan), fp, fp, C.c_int, ip, fp, fp, fp, fp, fp, fp, vp]),
     'sb_sh_slopes_vjp': (C.c_int, [C.POINTER(ShPlan), fp, fp, C.c_int, ip, fp, fp, fp, fp, fp, fp, vp]),
     'sb_intmat_contract': (C.c_int, [fp, fp, C.c_int, C.c_int, C.c_int, C.c_int, ip, ip, fp, C.c_int, C.c_int,

@@ -20,7 +20,7 @@ def golden():
     """Golden fixtures written by tests/golden/make_golden.py from the reference."""
     import json
     out = {}
-    for name in ('ref_fits', 'sh_fp32', 'sh_fp64', 'chain_fp32', 'zernike_fp32'):
+    for name in ('ref_fits', 'sh_fp32', 'sh_fp64', 'chain_fp32', 'zernike_fp32', 'psf_fp32'):
         with np.load(os.path.join(GOLDEN, name + '.npz')) as z:
             out[name] = {k: z[k] for k in z.files}
     with open(os.path.join(GOLDEN, 'sh_geometry.json')) as f:

@@ -296,6 +296,41 @@ def make_zernike_cases():
 
 ZERNIKE_CASES = [(32, 10, 0.14), (48, 21, 0.0)]
 
+# PSF cases: (pupil px, nd, wavelength nm, start_time s, phase RMS nm)
+PSF_CASES = [(32, 2, 1650.0, 0.002, 120.0), (25, 3, 750.0, 0.0, 60.0)]
+
+
+def make_psf_cases():
+    """The reference PSF object (psf.py:17-137) over 4 steps of seeded
+    fields: per-step PSF and SR, integrated PSF and SR."""
+    from specula.processing_objects.psf import PSF
+    from specula.data_objects.electric_field import ElectricField
+    out = {}
+    for pix, nd, lam, t0, rms in PSF_CASES:
+        rng = np.random.default_rng(pix + nd)
+        key = 'psf_%d_%d' % (pix, nd)
+        ef = ElectricField(pix, pix, 0.05, S0=1.0, target_device_idx=-1)
+        A, _ = sh_input(pix, 1)
+        ef.A[:] = A
+        psf = PSF(wavelengthInNm=lam, nd=nd, start_time=t0, target_device_idx=-1)
+        psf.inputs['in_ef'].set(ef)
+        psf.setup()
+        out[key + '/A'] = A
+        for step in range(4):
+            ph = (rng.standard_normal((pix, pix)) * rms).astype(np.float32) * A
+            ef.phaseInNm[:] = ph
+            t = step * 1000000
+            ef.generation_time = t
+            psf.check_ready(t)
+            psf.trigger()
+            psf.post_trigger()
+            out[key + '/phase%d' % step] = ph
+            out[key + '/psf%d' % step] = np.array(psf.psf.value, dtype=np.float32)
+            out[key + '/sr%d' % step] = np.float64(psf.sr.value)
+        out[key + '/int_psf'] = np.array(psf.int_psf.value, dtype=np.float32)
+        out[key + '/int_sr'] = np.float64(psf.int_sr.value)
+    return out
+
 
 def main():
     import subprocess
@@ -313,6 +348,7 @@ def main():
     chain = make_chain_cases()
     np.savez_compressed(os.path.join(HERE, 'chain_fp32.npz'), **chain)
     np.savez_compressed(os.path.join(HERE, 'zernike_fp32.npz'), **make_zernike_cases())
+    np.savez_compressed(os.path.join(HERE, 'psf_fp32.npz'), **make_psf_cases())
     print('wrote', sorted(os.listdir(HERE)))
 
 
@@ -327,6 +363,10 @@ def main_fp64():
 if __name__ == '__main__':
     if '--fp64' in sys.argv:
         main_fp64()
+    elif '--psf' in sys.argv:          # only the PSF / Strehl fixtures
+        import specula
+        specula.init(-1, precision=1)
+        np.savez_compressed(os.path.join(HERE, 'psf_fp32.npz'), **make_psf_cases())
     elif '--zernike' in sys.argv:      # only the Zernike influence-function tables
         import specula
         specula.init(-1, precision=1)

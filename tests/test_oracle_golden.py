@@ -152,3 +152,20 @@ def test_slope_nulls_match_reference_calibration_fits(golden):
     frame = _calibration_image()
     s, _ = osl.sh_slopes(frame, r['subaps/idxs'])
     np.testing.assert_array_almost_equal(s, r['sn/slopes'], decimal=5)
+
+
+@pytest.mark.parametrize('pix,nd,lam,t0', [(32, 2, 1650.0, 0.002), (25, 3, 750.0, 0.0)])
+def test_psf_oracle_matches_reference(golden, pix, nd, lam, t0):
+    """oracle.psf against the reference PSF object over 4 steps: per-step PSF
+    and Strehl, integrated PSF and Strehl after start_time."""
+    from oracle.psf import PSFOracle
+    g = golden['psf_fp32']
+    key = 'psf_%d_%d' % (pix, nd)
+    A = g[key + '/A']
+    o = PSFOracle(A.shape, lam, nd=nd, start_time=t0)
+    for step in range(4):
+        psf, sr = o.step(A, g[key + '/phase%d' % step], step * 1e-3)
+        np.testing.assert_allclose(psf, g[key + '/psf%d' % step], rtol=1e-5, atol=1e-7 * float(psf.max()))
+        assert abs(sr - float(g[key + '/sr%d' % step])) <= 1e-5 * abs(float(g[key + '/sr%d' % step]))
+    np.testing.assert_allclose(o.int_psf, g[key + '/int_psf'], rtol=1e-5, atol=1e-7 * float(o.int_psf.max()))
+    assert abs(o.int_sr - float(g[key + '/int_sr'])) <= 1e-5 * abs(float(g[key + '/int_sr']))
