@@ -50,6 +50,9 @@ def parse():
     p.add_argument('--cpu-baseline-seconds', type=float, default=20.0)
     p.add_argument('--no-cpu-baseline', action='store_true')
     p.add_argument('--no-adjoint', action='store_true', help='skip the adjoint interaction-matrix leg')
+    p.add_argument('--no-gradient', action='store_true',
+                   help='skip the checkpointed loop-gradient leg (1000 ELT steps, finite-difference check)')
+    p.add_argument('--gradient-only', action='store_true', help='run only the loop-gradient leg (one GPU)')
     p.add_argument('--adjoint-only', action='store_true',
                    help='run only the adjoint interaction-matrix leg (one GPU) and print its JSON object')
     return p.parse_args()
@@ -278,6 +281,64 @@ def cpu_pushpull(cal, amp, budget_s):
             'kind': 'port', 'sample': f'{k} of {IF.shape[0]} modes pushed and pulled in {dt:.1f} s, scaled'}
 
 
+def bench_loop_gradient(dev, n_steps=1000, checkpoint_every=50, n_dirs=8, fd_eps=2e-2):
+    """Gradient of the mean residual wavefront variance of the ELT loop
+    (noise-free detector, every one of the 80x80 sub-apertures valid, 500
+    Zernike modes, reconstructor = pseudo-inverse of the adjoint interaction
+    matrix calibrated with DM sign +1, gains 0.5) with respect to the 500 integrator gains and the
+    reconstructor, checkpoints every 50 steps, against central finite
+    differences on seeded random gain directions."""
+    import torch
+    from specula_b200.data_objects.intmat import Intmat
+    from specula_b200.lib.loop_gradient import LoopGradient
+    from specula_b200.lib.sh_adjoint import ShSlopesAdjoint
+    from specula_b200.lib.zernike import compute_zern_ifunc
+    from specula_b200.scao import ScaoLoop, elt_config
+    cfg = elt_config()
+    cfg.photon_noise = False
+    cfg.readout_noise = 0.0
+    cfg.subap_threshold = -1.0
+    t0 = time.perf_counter()
+    from specula_b200.lib.make_mask import make_mask
+    pupil = make_mask(cfg.pixel_pupil, cfg.obsratio, 1.0)
+    ifunc, _ = compute_zern_ifunc(cfg.pixel_pupil, cfg.n_modes, mask=pupil)
+    loop = ScaoLoop(cfg, device_idx=dev.index, ifunc=torch.as_tensor(ifunc, device=dev))
+    lg = LoopGradient(loop, n_steps, checkpoint_every=checkpoint_every)
+    adj = ShSlopesAdjoint(loop.sh, loop.slopec)
+    flat = torch.zeros_like(loop.dm.layer.phaseInNm)
+    # calibrated with the DM sign flipped (+1), as the reference's calibration
+    # configuration does, so the loop (DM sign -1) has negative feedback
+    im = adj.intmat(lg.ef.A, flat, loop.dm) * (-1.0)
+    R = Intmat(im, target_device_idx=dev.index).pseudo_invert(im).t().contiguous().float()
+    setup_s = time.perf_counter() - t0
+    g = torch.full((lg.nm,), 0.5, dtype=torch.float32, device=dev)
+    lg.gradient(g, R)                      # warm-up
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    L, dg, dR = lg.gradient(g, R)
+    torch.cuda.synchronize(dev)
+    grad_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    L_fwd = lg.loss(g, R)
+    fwd_s = time.perf_counter() - t0
+    gen = torch.Generator(device=dev).manual_seed(7)
+    rel = []
+    t0 = time.perf_counter()
+    for _ in range(n_dirs):
+        d = torch.randn(lg.nm, device=dev, generator=gen)
+        d /= d.norm()
+        fd = (lg.loss(g + fd_eps * d, R) - lg.loss(g - fd_eps * d, R)) / (2 * fd_eps)
+        ad = float((dg.double() * d.double()).sum())
+        rel.append(abs(ad - fd) / max(abs(fd), 1e-300))
+    fd_s = time.perf_counter() - t0
+    return {'workload': 'elt_80x80_all_subaps_7layers_500zernike_1000steps', 'steps': n_steps,
+            'checkpoint_every': checkpoint_every, 'n_slopes': lg.nsl, 'loss_nm2': L, 'loss_forward_only_nm2': L_fwd,
+            'gradient_s': grad_s, 'forward_s': fwd_s, 'gradient_over_forward': grad_s / fwd_s,
+            'fd_directions': n_dirs, 'fd_eps': fd_eps, 'fd_seconds': fd_s,
+            'fd_rel_err_max': max(rel), 'fd_rel_err': rel, 'setup_s': setup_s,
+            'dR_shape': list(dR.shape), 'reconstructor': 'pinv of the adjoint interaction matrix'}
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
@@ -411,6 +472,10 @@ def run_b200(args):
         cpu = {'value': v, 'unit': UNIT, 'cores': blas_threads(), 'kind': 'port',
                'sample': f'{n} CPU-oracle loop steps of the same system after 1 untimed step ({dt:.1f} s)'}
 
+    loop_grad = None
+    if world == 1 and not args.no_gradient:
+        loop_grad = bench_loop_gradient(dev)
+
     adjoint_im = None
     if world == 1 and not args.no_adjoint:
         adjoint_im = bench_adjoint_im(dev, reps=max(3, min(args.steps, 10)),
@@ -436,7 +501,7 @@ def run_b200(args):
                 'step_roofline': {'algorithmic_bytes': step_bytes,
                                   'achieved_gbs': step_bytes / (ms_max / steps / 1e3) / 1e9,
                                   'frac': step_bytes / (ms_max / steps / 1e3) / 1e9 / peak},
-                'clocks': clk, 'cpu_baseline': cpu, 'adjoint_im': adjoint_im}
+                'clocks': clk, 'cpu_baseline': cpu, 'adjoint_im': adjoint_im, 'loop_gradient': loop_grad}
         print(json.dumps(line), flush=True)
     del loop
     if world > 1:
@@ -446,6 +511,12 @@ def run_b200(args):
 
 def main():
     args = parse()
+    if args.gradient_only:
+        import torch
+        dev = torch.device('cuda', 0)
+        torch.cuda.set_device(dev)
+        print(json.dumps({'loop_gradient': bench_loop_gradient(dev)}), flush=True)
+        return
     if args.adjoint_only:
         import torch
         dev = torch.device('cuda', 0)

@@ -66,6 +66,7 @@ class ScaoConfig:
     photon_noise: bool = True
     time_step: float = 0.001
     seed: int = 1234
+    subap_threshold: float = 0.5           # valid sub-apertures: illumination above this fraction (< 0: all)
 
     @property
     def pitch(self):
@@ -143,7 +144,7 @@ class ScaoLoop:
                        readout_noise=c.readout_noise > 0, readout_level=c.readout_noise, quantum_eff=1.0,
                        target_device_idx=device_idx)
         self.ccd.inputs['in_i'].set(self.sh.outputs['out_i'])
-        idxs, dmap = valid_subaps(pupil, c.n_lenses, c.subap_npx)
+        idxs, dmap = valid_subaps(pupil, c.n_lenses, c.subap_npx, c.subap_threshold)
         self.subapdata = SubapData(idxs=idxs, display_map=dmap, nx=c.n_lenses, ny=c.n_lenses,
                                    target_device_idx=device_idx)
         self.slopec = ShSlopec(self.subapdata, target_device_idx=device_idx)
@@ -318,7 +319,7 @@ def valid_subaps(pupil, n_lenses, npx, threshold=0.5):
     for i in range(n_lenses):
         for j in range(n_lenses):
             # box rows come from lenslet column j, box columns from row i
-            if illum[j, i] > threshold * illum.max():
+            if threshold < 0 or illum[j, i] > threshold * illum.max():
                 r0, c0 = j * npx, i * npx
                 rr, cc = np.meshgrid(np.arange(r0, r0 + npx), np.arange(c0, c0 + npx), indexing='ij')
                 idxs.append((rr * side + cc).ravel())
