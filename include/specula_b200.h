@@ -229,6 +229,21 @@ int sb_dm_project(const float *ifunc, int n_modes, int n_valid, int ld_if,
                   const float *cmd, int n_cmd, float sign, const int32_t *mask_idx,
                   float *phase, void *stream);
 
+/* Batched form for Monte-Carlo realisations sharing one mirror: for
+ * b < n_batch, phase[b * phase_stride + mask_idx[p]] =
+ * sum_m (sign * cmd[b * ld_cmd + m]) * IF[m][p].  Each influence-function
+ * element is read once per 16 realisations (same TMA pipeline as
+ * sb_dm_project); up to 2048 modes, 16-byte aligned IF rows. */
+int sb_dm_project_batched(const float *ifunc, int n_modes, int n_valid, int ld_if, const float *cmd,
+                          int ld_cmd, int n_batch, float sign, const int32_t *mask_idx, float *phase,
+                          long long phase_stride, void *stream);
+
+/* Batched Modalrec (modalrec.py:159) for realisations sharing one
+ * reconstructor: modes[b * ldm + m] = sum_j R[m][j] * slopes[b * lds + j];
+ * R is read once per 16 realisations. */
+int sb_modalrec_batched(const float *R, int n_modes, int n_slopes, int ldr, const float *slopes, int lds,
+                        int n_batch, float *modes, int ldm, void *stream);
+
 /* Diagnostics: SB_OK, or SB_ETIMEOUT when a bounded wait inside a kernel
  * (the shared-memory pipeline of sb_dm_project) gave up since the last call;
  * reading clears it.  Synchronous (waits for the device); not for the step. */

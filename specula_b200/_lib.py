@@ -81,6 +81,9 @@ SIGNATURES = {
     'sb_modalrec_integrator': (C.c_int, [fp, C.c_int, C.c_int, C.c_int, fp, fp, C.POINTER(IirPlan), fp, vp]),
     'sb_dm_project': (C.c_int, [fp, C.c_int, C.c_int, C.c_int, fp, C.c_int, C.c_float, ip, fp, vp]),
     'sb_device_status': (C.c_int, []),
+    'sb_dm_project_batched': (C.c_int, [fp, C.c_int, C.c_int, C.c_int, fp, C.c_int, C.c_int, C.c_float, ip, fp,
+                                        C.c_longlong, vp]),
+    'sb_modalrec_batched': (C.c_int, [fp, C.c_int, C.c_int, C.c_int, fp, C.c_int, C.c_int, fp, C.c_int, vp]),
     'sb_atmo_evolve': (C.c_int, [C.POINTER(AtmoLayer), C.c_int, C.c_int, vp, vp]),
     'sb_atmo_work_bytes': (C.c_size_t, [C.c_int]),
     'sb_atmo_evolve_inputs': (C.c_int, [C.POINTER(AtmoLayer), C.c_int, C.c_int, vp, C.POINTER(AtmoInputs), vp,

@@ -1,0 +1,205 @@
+"""Batched Monte-Carlo of uneven SCAO SH systems on one B200.
+
+Realisations come in geometry groups (same pupil, sub-aperture grid,
+wavelength, mirror and reconstructor; their own atmosphere (r0, seed) and
+detector noise seeds).  Each realisation's chain (AtmoEvolution,
+AtmoPropagation, SH, CCD, ShSlopec) is one ``ScaoLoop``'s objects; within a
+group the slope vectors and the DM layers are rows of group matrices, so the
+group's reconstructor, integrator and mirror run as one launch each for all
+its realisations: ``sb_modalrec_batched`` and ``sb_dm_project_batched`` read
+the reconstructor and the influence functions once per step per group (the
+plain form reads them once per realisation), and one ``sb_integrator`` call
+updates every realisation's filter.  ``capture()`` puts the whole step of
+every realisation and group into one CUDA graph, the realisations' chains
+spread over several streams so that they run concurrently.
+
+``BatchedScao.replay_plain()`` runs the same realisations the plain way (each
+``ScaoLoop``'s own captured step, its own reconstructor and mirror), for
+comparison.
+"""
+import ctypes
+import math
+from dataclasses import replace
+
+import numpy as np
+import torch
+
+from specula_b200 import _lib
+from specula_b200.base_value import BaseValue
+from specula_b200.processing_objects.integrator import Integrator
+from specula_b200.lib.make_mask import make_mask
+from specula_b200.scao import ScaoConfig, ScaoLoop, elt_config, valid_subaps
+
+
+def seeing_from_r0(r0):
+    """Seeing [arcsec] giving r0 [m] at 500 nm (atmo_evolution.py:265)."""
+    return 0.9759 * 0.5 / (r0 * 4.848)
+
+
+def mc_groups(seed=7, n_real=(55, 27, 14), wavelengths=(589.0, 750.0)):
+    """The Monte-Carlo mix: 20x20 sub-apertures on 160 px (8 m, 1 layer, 54
+    modes), 40x40 on 320 px (8 m, 3 layers, 300 modes) and 74x74 on 592 px
+    (39 m, 7 layers, 500 modes) in the given counts, each split between the
+    two wavelengths; r0 uniform in [0.08, 0.20] m and the screen / noise seeds
+    per realisation.  Returns [(ScaoConfig template, [per-realisation
+    ScaoConfig])]."""
+    rng = np.random.default_rng(seed)
+    e = elt_config()
+    sizes = [
+        ScaoConfig(pixel_pupil=160, diameter_m=8.0, n_lenses=20, subap_npx=8, n_modes=54),
+        ScaoConfig(pixel_pupil=320, diameter_m=8.0, n_lenses=40, subap_npx=6, pxscale_over_lamd=1.0, n_modes=300,
+                   heights=[0.0, 4000.0, 10000.0], cn2=[0.6, 0.25, 0.15], wind_speed=[8.0, 15.0, 25.0],
+                   wind_direction=[10.0, 130.3, 250.6], pixel_phasescreens=1024),
+        ScaoConfig(pixel_pupil=592, diameter_m=39.0, n_lenses=74, subap_npx=6, pxscale_over_lamd=1.0, n_modes=500,
+                   heights=e.heights, cn2=e.cn2, wind_speed=e.wind_speed, wind_direction=e.wind_direction,
+                   pixel_phasescreens=2048),
+    ]
+    groups = []
+    k = 0
+    for cfg, n in zip(sizes, n_real):
+        for w, lam in enumerate(wavelengths):
+            cnt = (n + 1 - w) // 2
+            reals = []
+            for _ in range(cnt):
+                r0 = float(rng.uniform(0.08, 0.20))
+                reals.append(replace(cfg, wavelength_nm=lam, r0=r0, screen_seed=100 + k, seed=1000 + 17 * k))
+                k += 1
+            if reals:
+                groups.append((replace(cfg, wavelength_nm=lam), reals))
+    return groups
+
+
+class _Group:
+    def __init__(self, template, reals, device_idx):
+        dev = torch.device('cuda', device_idx)
+        self.device = dev
+        self.n = len(reals)
+        c0 = template
+        # shared mirror and reconstructor of the group (random, as ScaoLoop's defaults)
+        pupil = make_mask(c0.pixel_pupil, c0.obsratio, 1.0)
+        nv, nm = int(pupil.sum()), c0.n_modes
+        nsl = 2 * len(valid_subaps(pupil, c0.n_lenses, c0.subap_npx, c0.subap_threshold)[0])
+        g = torch.Generator(device=dev).manual_seed(c0.seed)
+        self.ifunc = torch.randn((nm, nv), device=dev, generator=g) * 10.0
+        g = torch.Generator(device=dev).manual_seed(c0.seed + 1)
+        self.recmat = torch.randn((nm, nsl), device=dev, generator=g) * (1.0 / math.sqrt(nsl))
+        self.loops = [ScaoLoop(c, device_idx=device_idx, ifunc=self.ifunc, recmat=self.recmat) for c in reals]
+        L = c0.pixel_pupil
+        self.nm, self.nsl, self.L = nm, nsl, L
+        # group matrices: rows are the realisations
+        self.S = torch.zeros((self.n, nsl), dtype=torch.float32, device=dev)
+        self.M = torch.zeros((self.n, nm), dtype=torch.float32, device=dev)
+        self.dm_phase = torch.zeros((self.n, L, L), dtype=torch.float32, device=dev)
+        for b, lp in enumerate(self.loops):
+            lp.slopec.slopes.slopes = self.S[b]
+            lp.dm.layer.phaseInNm = self.dm_phase[b]
+        self.integ = Integrator(self.loops[0].simul_params, int_gain=[c0.gain] * (nm * self.n), delay=c0.delay,
+                                target_device_idx=device_idx)
+        self.integ.inputs['delta_comm'].set(BaseValue(value=self.M.view(-1), target_device_idx=device_idx))
+
+    def start(self):
+        for lp in self.loops:
+            lp.start()
+            lp.step_eager()
+        self.integ.setup()
+        self.dm = self.loops[0].dm        # its padded IF copy and mask index serve the group
+        self.sync_from_loops()
+
+    def sync_from_loops(self):
+        """Group integrator state <- the realisations' own integrators."""
+        nm = self.nm
+        for b, lp in enumerate(self.loops):
+            self.integ.state[b * nm:(b + 1) * nm].copy_(lp.integ.state)
+            self.integ._ist[b * nm:(b + 1) * nm].copy_(lp.integ._ist)
+            self.integ._ost[b * nm:(b + 1) * nm].copy_(lp.integ._ost)
+            self.integ.out_comm.value[b * nm:(b + 1) * nm].copy_(lp.integ.out_comm.value)
+
+    def chain(self, b):
+        lp = self.loops[b]
+        for o in (lp.atmo, lp.prop, lp.sh, lp.ccd, lp.slopec):
+            o.trigger_code()
+
+    def group_ops(self):
+        st = torch.cuda.current_stream(self.device).cuda_stream
+        lp = self.loops[0]
+        R = lp.rec._R
+        _lib.call('sb_modalrec_batched', R.data_ptr(), self.nm, self.nsl, R.stride(0), self.S.data_ptr(),
+                  self.nsl, self.n, self.M.data_ptr(), self.nm, st)
+        _lib.call('sb_integrator', ctypes.byref(self.integ._plan), self.M.data_ptr(),
+                  self.integ.out_comm.value.data_ptr(), st)
+        dm = self.dm
+        _lib.call('sb_dm_project_batched', dm._IF.data_ptr(), self.nm, int(dm._idx.numel()), dm._ld,
+                  self.integ.out_comm.value.data_ptr(), self.nm, self.n, float(dm.sign), dm._idx.data_ptr(),
+                  self.dm_phase.data_ptr(), self.L * self.L, st)
+
+
+class BatchedScao:
+    def __init__(self, groups, device_idx=0, streams=8):
+        self.device = torch.device('cuda', device_idx)
+        self.groups = [_Group(t, reals, device_idx) for t, reals in groups]
+        self.n_streams = streams
+        self.graph = None
+        self.plain_graphs = None
+
+    @property
+    def n_realisations(self):
+        return sum(g.n for g in self.groups)
+
+    def start(self):
+        for g in self.groups:
+            g.start()
+        for g in self.groups:
+            for lp in g.loops:
+                lp.atmo.delta_time = lp.atmo.t_to_seconds(lp.loop._dt)
+        torch.cuda.synchronize(self.device)
+
+    def step_eager(self):
+        """One batched step without a graph (every chain, then the group launches)."""
+        for g in self.groups:
+            for b in range(g.n):
+                g.chain(b)
+            g.group_ops()
+
+    def capture(self):
+        """The batched step of every realisation in one CUDA graph."""
+        self.step_eager()
+        torch.cuda.synchronize(self.device)
+        streams = [torch.cuda.Stream(self.device) for _ in range(self.n_streams)]
+        cap = torch.cuda.Stream(self.device)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=cap):
+            main = torch.cuda.current_stream(self.device)
+            for s in streams:
+                s.wait_stream(main)
+            k = 0
+            for grp in self.groups:
+                for b in range(grp.n):
+                    with torch.cuda.stream(streams[k % self.n_streams]):
+                        grp.chain(b)
+                    k += 1
+            for s in streams:
+                main.wait_stream(s)
+            for grp in self.groups:
+                grp.group_ops()
+        torch.cuda.synchronize(self.device)
+        self.graph = g
+        return g
+
+    def replay(self):
+        self.graph.replay()
+
+    def capture_plain(self):
+        """Every realisation's own sequential step graph (its own
+        reconstructor, integrator and mirror: the plain form)."""
+        for grp in self.groups:
+            for lp in grp.loops:
+                lp.capture(pipelined=False)
+        torch.cuda.synchronize(self.device)
+
+    def replay_plain(self):
+        for grp in self.groups:
+            for lp in grp.loops:
+                lp.replay()
+
+    def slopes(self):
+        return [grp.S.clone() for grp in self.groups]

@@ -314,6 +314,154 @@ __global__ void __launch_bounds__(32 * (kDmConsumerWarps + 1), 1)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Batched (multi-right-hand-side) forms for Monte-Carlo realisations that
+// share one mirror and one reconstructor: every influence-function and
+// reconstructor element is read once per step for all realisations.
+// ---------------------------------------------------------------------------
+
+// phase_b[idx[p]] = sum_m c_b[m] IF[m][p] for b < NB.  Same TMA ring as
+// dm_project_tma_kernel (32 x 256 boxes, 3 stages, evict-first); 8 consumer
+// warps, one column per thread and NB accumulators; the NB command vectors
+// are staged in shared memory as [mode][NB].
+constexpr int kDbWarps = 8;
+template <int NB>
+size_t dm_batched_smem_bytes(int nmodes) {
+    const int nst = (nmodes + kDmRows - 1) / kDmRows;
+    return 1024 + (size_t)kDmStages * kDmRows * kDmCols * 4 + 2 * kDmStages * 8 + (size_t)nst * kDmRows * NB * 4;
+}
+
+template <int NB>
+__global__ void __launch_bounds__(32 * (kDbWarps + 1), 1)
+    dm_project_batched_kernel(const __grid_constant__ CUtensorMap map, int nmodes, int nvalid,
+                              const float *__restrict__ cmd, int ldc, int nb, float sign,
+                              const int32_t *__restrict__ idx, float *__restrict__ phase, long long phase_stride) {
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char *base = smem_raw + ((1024 - (sb::smem_u32(smem_raw) & 1023)) & 1023);
+    float *ring = reinterpret_cast<float *>(base);
+    uint64_t *full = reinterpret_cast<uint64_t *>(base + (size_t)kDmStages * kDmRows * kDmCols * 4);
+    uint64_t *empty = full + kDmStages;
+    float *c = reinterpret_cast<float *>(empty + kDmStages);       // [mode][NB]
+    __shared__ int abort_flag, issued;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nst = (nmodes + kDmRows - 1) / kDmRows;
+    if (tid == 0) {
+        for (int s = 0; s < kDmStages; ++s) {
+            sb::mbar_init(&full[s], 1);
+            sb::mbar_init(&empty[s], kDbWarps);
+        }
+        sb::mbar_init_fence();
+        abort_flag = 0;
+        issued = 0;
+    }
+    for (int e = tid; e < nst * kDmRows * NB; e += blockDim.x) {
+        const int m = e / NB, b = e - m * NB;
+        c[e] = (m < nmodes && b < nb) ? sign * cmd[(size_t)b * ldc + m] : 0.f;
+    }
+    __syncthreads();
+    const int ntiles = (nvalid + kDmCols - 1) / kDmCols;
+    const int bid = blockIdx.x, nblk = gridDim.x;
+    const int my_tiles = bid < ntiles ? (ntiles - 1 - bid) / nblk + 1 : 0;
+    const int total = my_tiles * nst;
+    if (warp == kDbWarps) {
+        if (lane == 0) {
+            const uint64_t pol = sb::l2_evict_first_policy();
+            int q = 0;
+            for (; q < total; ++q) {
+                const int slot = q % kDmStages;
+                if (q >= kDmStages && !sb::mbar_wait(&empty[slot], ((q / kDmStages) - 1) & 1)) {
+                    atomicExch(&g_dm_status, 3);
+                    abort_flag = 1;
+                    break;
+                }
+                if (*(volatile int *)&abort_flag) break;
+                const int tile = bid + (q / nst) * nblk;
+                sb::mbar_arrive_expect_tx(&full[slot], kDmRows * kDmCols * 4);
+                sb::tma_load_2d(ring + (size_t)slot * kDmRows * kDmCols, &map, tile * kDmCols, (q % nst) * kDmRows,
+                                &full[slot], pol);
+            }
+            issued = q;
+        }
+    } else {
+        float acc[NB];
+#pragma unroll
+        for (int b = 0; b < NB; ++b) acc[b] = 0.f;
+        for (int q = 0; q < total; ++q) {
+            const int slot = q % kDmStages;
+            if (!sb::mbar_wait(&full[slot], (q / kDmStages) & 1)) {
+                atomicExch(&g_dm_status, 4);
+                abort_flag = 1;
+                break;
+            }
+            if (*(volatile int *)&abort_flag) break;
+            const int sg = q % nst;
+            const float *buf = ring + (size_t)slot * kDmRows * kDmCols + tid;
+            const float4 *cm = reinterpret_cast<const float4 *>(c + (size_t)sg * kDmRows * NB);
+#pragma unroll 4
+            for (int r = 0; r < kDmRows; ++r) {
+                const float v = buf[r * kDmCols];
+#pragma unroll
+                for (int b4 = 0; b4 < NB / 4; ++b4) {
+                    const float4 cc = cm[r * (NB / 4) + b4];
+                    acc[4 * b4 + 0] = fmaf(cc.x, v, acc[4 * b4 + 0]);
+                    acc[4 * b4 + 1] = fmaf(cc.y, v, acc[4 * b4 + 1]);
+                    acc[4 * b4 + 2] = fmaf(cc.z, v, acc[4 * b4 + 2]);
+                    acc[4 * b4 + 3] = fmaf(cc.w, v, acc[4 * b4 + 3]);
+                }
+            }
+            __syncwarp();
+            if (lane == 0) sb::mbar_arrive(&empty[slot]);
+            if (sg == nst - 1) {
+                const int col = (bid + (q / nst) * nblk) * kDmCols + tid;
+                if (col < nvalid) {
+                    const int pix = idx[col];
+#pragma unroll
+                    for (int b = 0; b < NB; ++b)
+                        if (b < nb) phase[(size_t)b * phase_stride + pix] = acc[b];
+                }
+#pragma unroll
+                for (int b = 0; b < NB; ++b) acc[b] = 0.f;
+            }
+        }
+    }
+    __syncthreads();
+    if (abort_flag && tid == 0) {
+        for (int q = 0; q < issued; ++q) sb::mbar_wait(&full[q % kDmStages], (q / kDmStages) & 1);
+    }
+}
+
+// modes_b[m] = sum_j R[m][j] s_b[j] for b < NB: one CTA per reconstructor
+// row, read once for all NB slope vectors
+template <int NB>
+__global__ void __launch_bounds__(256) gemv_rows_batched_kernel(const float *__restrict__ R, int ncols, int ldr,
+                                                                const float *__restrict__ S, int lds, int nb,
+                                                                float *__restrict__ M, int ldm) {
+    __shared__ float red[NB][33];
+    const int m = blockIdx.x;
+    const float *row = R + (size_t)m * ldr;
+    float acc[NB];
+#pragma unroll
+    for (int b = 0; b < NB; ++b) acc[b] = 0.f;
+    for (int j = threadIdx.x; j < ncols; j += blockDim.x) {
+        const float r = __ldg(row + j);
+#pragma unroll
+        for (int b = 0; b < NB; ++b)
+            if (b < nb) acc[b] = fmaf(r, __ldg(S + (size_t)b * lds + j), acc[b]);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+        const float v = sb::warp_sum(acc[b]);
+        if (lane == 0) red[b][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < NB && threadIdx.x < nb) {
+        float t = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[threadIdx.x][w];
+        M[(size_t)threadIdx.x * ldm + m] = t;
+    }
+}
+
 }  // namespace
 
 extern "C" int sb_device_status(void) {
@@ -422,4 +570,78 @@ extern "C" int sb_dm_project(const float *ifunc, int n_modes, int n_valid, int l
         dm_project_kernel<1><<<nblk, 256, smem, st>>>(ifunc, n_modes, n_valid, ld_if, cmd, n_cmd, sign, mask_idx, phase);
     }
     return sb::check_launch("dm_project_kernel");
+}
+
+namespace {
+
+template <int NB>
+int launch_dm_batched(const CUtensorMap &map, int n_modes, int n_valid, const float *cmd, int ldc, int nb, float sign,
+                      const int32_t *mask_idx, float *phase, long long phase_stride, cudaStream_t st) {
+    static bool attr_set[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const size_t smem = dm_batched_smem_bytes<NB>(n_modes);
+    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+        if (cudaFuncSetAttribute(dm_project_batched_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)dm_batched_smem_bytes<NB>(kDmMaxModes / 2)) != cudaSuccess)
+            return sb::fail(SB_ECUDA, "sb_dm_project_batched: %s", cudaGetErrorString(cudaGetLastError()));
+        attr_set[dev] = true;
+    }
+    const int nsm = sb::sm_count();
+    const int ntiles = (n_valid + kDmCols - 1) / kDmCols;
+    dm_project_batched_kernel<NB><<<ntiles < nsm ? ntiles : nsm, 32 * (kDbWarps + 1), smem, st>>>(
+        map, n_modes, n_valid, cmd, ldc, nb, sign, mask_idx, phase, phase_stride);
+    return sb::check_launch("dm_project_batched_kernel");
+}
+
+}  // namespace
+
+extern "C" int sb_dm_project_batched(const float *ifunc, int n_modes, int n_valid, int ld_if, const float *cmd,
+                                     int ld_cmd, int n_batch, float sign, const int32_t *mask_idx, float *phase,
+                                     long long phase_stride, void *stream) {
+    sb::clear_error();
+    if (!ifunc || !cmd || !mask_idx || !phase || n_modes < 1 || n_valid < 0 || ld_if < n_valid || n_batch < 1 ||
+        ld_cmd < n_modes || phase_stride < 1)
+        return sb::fail(SB_EINVAL, "sb_dm_project_batched: bad args");
+    if (n_modes > kDmMaxModes / 2)
+        return sb::fail(SB_ESHAPE, "sb_dm_project_batched: at most %d modes", kDmMaxModes / 2);
+    if (ld_if % 4 || (uintptr_t)ifunc % 16)
+        return sb::fail(SB_EINVAL, "sb_dm_project_batched: influence-function rows must be 16-byte aligned");
+    if (n_valid == 0) return SB_OK;
+    CUtensorMap map;
+    int rc = sb::tensor_map_2d_f32(&map, ifunc, n_modes, ld_if, ld_if, kDmRows, kDmCols);
+    if (rc) return rc;
+    cudaStream_t st = sb::as_stream(stream);
+    // chunks of up to 16 realisations; every chunk re-reads the IF once
+    for (int b0 = 0; b0 < n_batch; b0 += 16) {
+        const int nb = n_batch - b0 < 16 ? n_batch - b0 : 16;
+        const float *c = cmd + (size_t)b0 * ld_cmd;
+        float *ph = phase + (size_t)b0 * phase_stride;
+        if (nb <= 4) rc = launch_dm_batched<4>(map, n_modes, n_valid, c, ld_cmd, nb, sign, mask_idx, ph, phase_stride, st);
+        else if (nb <= 8) rc = launch_dm_batched<8>(map, n_modes, n_valid, c, ld_cmd, nb, sign, mask_idx, ph, phase_stride, st);
+        else rc = launch_dm_batched<16>(map, n_modes, n_valid, c, ld_cmd, nb, sign, mask_idx, ph, phase_stride, st);
+        if (rc) return rc;
+    }
+    return SB_OK;
+}
+
+extern "C" int sb_modalrec_batched(const float *R, int n_modes, int n_slopes, int ldr, const float *slopes, int lds,
+                                   int n_batch, float *modes, int ldm, void *stream) {
+    sb::clear_error();
+    if (!R || !slopes || !modes || n_modes < 0 || n_slopes < 0 || ldr < n_slopes || n_batch < 1 ||
+        lds < n_slopes || ldm < n_modes)
+        return sb::fail(SB_EINVAL, "sb_modalrec_batched: bad args");
+    if (n_modes == 0) return SB_OK;
+    cudaStream_t st = sb::as_stream(stream);
+    for (int b0 = 0; b0 < n_batch; b0 += 16) {
+        const int nb = n_batch - b0 < 16 ? n_batch - b0 : 16;
+        const float *S = slopes + (size_t)b0 * lds;
+        float *M = modes + (size_t)b0 * ldm;
+        if (nb <= 4) gemv_rows_batched_kernel<4><<<n_modes, 256, 0, st>>>(R, n_slopes, ldr, S, lds, nb, M, ldm);
+        else if (nb <= 8) gemv_rows_batched_kernel<8><<<n_modes, 256, 0, st>>>(R, n_slopes, ldr, S, lds, nb, M, ldm);
+        else gemv_rows_batched_kernel<16><<<n_modes, 256, 0, st>>>(R, n_slopes, ldr, S, lds, nb, M, ldm);
+        const int rc = sb::check_launch("gemv_rows_batched_kernel");
+        if (rc) return rc;
+    }
+    return SB_OK;
 }
