@@ -53,6 +53,8 @@ def parse():
     p.add_argument('--no-gradient', action='store_true',
                    help='skip the checkpointed loop-gradient leg (1000 ELT steps, finite-difference check)')
     p.add_argument('--gradient-only', action='store_true', help='run only the loop-gradient leg (one GPU)')
+    p.add_argument('--batched-only', action='store_true',
+                   help='run only the 96-realisation batched Monte-Carlo leg (one GPU)')
     p.add_argument('--adjoint-only', action='store_true',
                    help='run only the adjoint interaction-matrix leg (one GPU) and print its JSON object')
     return p.parse_args()
@@ -339,6 +341,73 @@ def bench_loop_gradient(dev, n_steps=1000, checkpoint_every=50, n_dirs=8, fd_eps
             'dR_shape': list(dR.shape), 'reconstructor': 'pinv of the adjoint interaction matrix'}
 
 
+def bench_batched(dev, steps, cpu_budget_s):
+    """The 96-realisation Monte-Carlo mix (55 x 20x20 / 160 px, 27 x 40x40 /
+    320 px, 14 x 74x74 / 592 px, two wavelengths, r0 ~ U(0.08, 0.20) m):
+    realisation-steps/s of the batched graph against the plain form (every
+    realisation its own step graph, reconstructor and mirror), CUDA events
+    around `steps` steps of each after warm-up."""
+    import torch
+    from specula_b200.batched import BatchedScao, mc_groups
+    t0 = time.perf_counter()
+    groups = mc_groups()
+    sys_b = BatchedScao(groups, device_idx=dev.index)
+    sys_b.start()
+    sys_b.capture_plain()
+    sys_b.capture()
+    setup_s = time.perf_counter() - t0
+    n_real = sys_b.n_realisations
+    st = torch.cuda.current_stream(dev)
+
+    def timed(fn, n):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(n):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / n
+
+    plain_ms = timed(sys_b.replay_plain, steps)
+    batched_ms = timed(sys_b.replay, steps)
+    _lib_status()
+    by_size = {}
+    for (tmpl, reals) in groups:
+        key = f'{tmpl.n_lenses}x{tmpl.n_lenses}/{tmpl.pixel_pupil}px'
+        by_size[key] = by_size.get(key, 0) + len(reals)
+    out = {'workload': 'mc96_20x20_40x40_74x74_2wavelengths', 'realisations': n_real, 'split': by_size,
+           'groups': len(groups), 'steps_timed': steps,
+           'batched_ms_per_step': batched_ms, 'plain_ms_per_step': plain_ms,
+           'batched_realisation_steps_per_s': n_real / (batched_ms / 1e3),
+           'plain_realisation_steps_per_s': n_real / (plain_ms / 1e3),
+           'speedup_batched_vs_plain': plain_ms / batched_ms, 'setup_s': setup_s,
+           'graph': 'one CUDA graph per step for all 96 realisations (chains over 16 streams, each group\'s batched launches on its own stream after its chains)'}
+    if cpu_budget_s > 0:
+        # the reference has no batched mode: the sum of per-realisation CPU runs,
+        # sampled per geometry (steps/s of each size, weighted by its count)
+        per = {}
+        total_s = 0.0
+        for tmpl, reals in groups:
+            key = f'{tmpl.n_lenses}x{tmpl.n_lenses}'
+            if key not in per:
+                v, n, dt = time_cpu_oracle(reals[0], budget_s=cpu_budget_s / 3, max_steps=50)
+                per[key] = v
+            total_s += len(reals) / per[key]
+        out['cpu_baseline'] = {'value': n_real / total_s, 'unit': 'realisation-steps/s', 'cores': blas_threads(),
+                               'kind': 'port', 'sample': 'CPU-oracle steps of one realisation per geometry, '
+                               'weighted by the realisation counts: ' + json.dumps({k: round(v, 3) for k, v in per.items()})}
+    return out
+
+
+def _lib_status():
+    from specula_b200 import _lib
+    _lib.call('sb_device_status')
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
@@ -511,6 +580,14 @@ def run_b200(args):
 
 def main():
     args = parse()
+    if args.batched_only:
+        import torch
+        dev = torch.device('cuda', 0)
+        torch.cuda.set_device(dev)
+        out = bench_batched(dev, steps=max(5, min(args.steps, 200)),
+                            cpu_budget_s=0 if args.no_cpu_baseline else 15.0)
+        print(json.dumps({'batched_mc': out}), flush=True)
+        return
     if args.gradient_only:
         import torch
         dev = torch.device('cuda', 0)

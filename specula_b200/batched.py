@@ -134,7 +134,7 @@ class _Group:
 
 
 class BatchedScao:
-    def __init__(self, groups, device_idx=0, streams=8):
+    def __init__(self, groups, device_idx=0, streams=16):
         self.device = torch.device('cuda', device_idx)
         self.groups = [_Group(t, reals, device_idx) for t, reals in groups]
         self.n_streams = streams
@@ -161,26 +161,34 @@ class BatchedScao:
             g.group_ops()
 
     def capture(self):
-        """The batched step of every realisation in one CUDA graph."""
+        """The batched step of every realisation in one CUDA graph.  Each
+        realisation's chain runs on one of ``streams`` streams; each group's
+        batched launches run on a stream of their own as soon as that group's
+        chains are done, so groups overlap one another."""
         self.step_eager()
         torch.cuda.synchronize(self.device)
         streams = [torch.cuda.Stream(self.device) for _ in range(self.n_streams)]
+        gstreams = [torch.cuda.Stream(self.device) for _ in self.groups]
         cap = torch.cuda.Stream(self.device)
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g, stream=cap):
             main = torch.cuda.current_stream(self.device)
-            for s in streams:
+            for s in streams + gstreams:
                 s.wait_stream(main)
             k = 0
-            for grp in self.groups:
+            for grp, gs in zip(self.groups, gstreams):
                 for b in range(grp.n):
-                    with torch.cuda.stream(streams[k % self.n_streams]):
+                    s = streams[k % self.n_streams]
+                    with torch.cuda.stream(s):
                         grp.chain(b)
+                        ev = torch.cuda.Event()
+                        ev.record(s)
+                    gs.wait_event(ev)
                     k += 1
-            for s in streams:
+                with torch.cuda.stream(gs):
+                    grp.group_ops()
+            for s in streams + gstreams:
                 main.wait_stream(s)
-            for grp in self.groups:
-                grp.group_ops()
         torch.cuda.synchronize(self.device)
         self.graph = g
         return g
