@@ -98,6 +98,16 @@ int sb_sh_forward_static(const sb_sh_plan *plan, const float *A, const float *ph
                          const float *A_norm, int n_norm, float photon_scale, float *intensity,
                          void *stream);
 
+/* Batched form for Monte-Carlo realisations sharing one plan: realisation b
+ * (blockIdx.z) reads A + b*A_stride, phase_nm + b*phase_stride, A_norm +
+ * b*A_norm_stride (strides in floats; 0 shares one array) and writes its
+ * normalised frame at intensity + b*intensity_stride.  scratch: n_batch *
+ * sb_sh_scratch_bytes(plan) bytes.  Each frame equals sb_sh_forward's. */
+int sb_sh_forward_batched(const sb_sh_plan *plan, const float *A, long long A_stride, const float *phase_nm,
+                          long long phase_stride, const float *A_norm, long long A_norm_stride, int n_norm,
+                          float photon_scale, float *intensity, long long intensity_stride, int n_batch,
+                          void *scratch, size_t scratch_bytes, void *stream);
+
 /* replaces specula/lib/extrapolate_edge_pixel.py:4-28.
  * out[p] = phase[p] if src1[p] < 0; phase[src1[p]] if src2[p] < 0;
  * else 2*phase[src1[p]] - phase[src2[p]].  Tables from the host restatement
@@ -151,6 +161,14 @@ typedef struct sb_ccd_params {
 int sb_ccd_step(const sb_ccd_params *p, const float *intensity, float *integrated,
                 float *pixels, void *stream);
 
+/* Batched CCD step: n_batch frames of p->n_pixels each, contiguous in
+ * intensity / integrated / pixels; frame b draws its noise with
+ * photon_seeds[b] / readout_seeds[b] (device arrays) and its own pixel
+ * indices, so it equals sb_ccd_step with those seeds.  One frame state
+ * (p->state) for all: the realisations integrate and read out in step. */
+int sb_ccd_step_batched(const sb_ccd_params *p, const uint64_t *photon_seeds, const uint64_t *readout_seeds,
+                        int n_batch, const float *intensity, float *integrated, float *pixels, void *stream);
+
 /* Raw Philox4x32-10 stream, for determinism tests: out[4*i..4*i+3] is the
  * block for counter (i, c1, c2, c3) under key (key0, key1). */
 int sb_philox_raw(uint32_t key0, uint32_t key1, uint32_t c1, uint32_t c2, uint32_t c3,
@@ -175,6 +193,13 @@ typedef struct sb_slopec_plan {
 size_t sb_slopec_scratch_bytes(const sb_slopec_plan *plan);
 int sb_slopec(const sb_slopec_plan *plan, const float *pixels, float *slopes, float *flux,
               void *scratch, size_t scratch_bytes, void *stream);
+
+/* Batched: frame b at pixels + b*frame_stride, slopes at slopes +
+ * b*slopes_stride, flux at flux + b*flux_stride; scratch n_batch *
+ * sb_slopec_scratch_bytes(plan) bytes. */
+int sb_slopec_batched(const sb_slopec_plan *plan, const float *pixels, long long frame_stride, float *slopes,
+                      int slopes_stride, float *flux, int flux_stride, int n_batch, void *scratch,
+                      size_t scratch_bytes, void *stream);
 
 /* ------------------------------------------------------------------------
  * Modalrec — replaces specula/processing_objects/modalrec.py:159
@@ -233,7 +258,7 @@ int sb_dm_project(const float *ifunc, int n_modes, int n_valid, int ld_if,
  * b < n_batch, phase[b * phase_stride + mask_idx[p]] =
  * sum_m (sign * cmd[b * ld_cmd + m]) * IF[m][p].  Each influence-function
  * element is read once per 16 realisations (same TMA pipeline as
- * sb_dm_project); up to 2048 modes, 16-byte aligned IF rows. */
+ * sb_dm_project, 5 stages); up to 1024 modes, 16-byte aligned IF rows. */
 int sb_dm_project_batched(const float *ifunc, int n_modes, int n_valid, int ld_if, const float *cmd,
                           int ld_cmd, int n_batch, float sign, const int32_t *mask_idx, float *phase,
                           long long phase_stride, void *stream);
@@ -351,6 +376,21 @@ size_t sb_atmo_work_bytes(int n_layers);
 int sb_atmo_evolve_inputs(const sb_atmo_layer *layers, int n_layers, int L, double *positions,
                           const sb_atmo_inputs *in, void *work, size_t work_bytes, void *stream);
 
+/* Batched form: many layers (of many realisations) in one launch (chunks of
+ * 64), each with its own device pointers to its seeing value, wind speed,
+ * wind direction and position; the constants (delta_time, pitch, airmass,
+ * wavelength factor) are shared and constants' pointers are not read.
+ * work: n_layers * sb_atmo_work_bytes(1) bytes or more. */
+typedef struct sb_atmo_layer_inputs {
+    const double *seeing;
+    const double *wind_speed;
+    const double *wind_direction;
+    double *position;
+} sb_atmo_layer_inputs;
+
+int sb_atmo_evolve_batched(const sb_atmo_layer *layers, const sb_atmo_layer_inputs *inputs, int n_layers, int L,
+                           const sb_atmo_inputs *constants, void *work, size_t work_bytes, void *stream);
+
 /* ------------------------------------------------------------------------
  * AtmoPropagation, on-axis branch — replaces
  * specula/processing_objects/atmo_propagation.py:105-125 with
@@ -366,6 +406,18 @@ typedef struct sb_prop_layer {
 
 int sb_propagate_on_axis(const sb_prop_layer *layers, int n_layers, int pupil,
                          float *A_out, float *phase_out, void *stream);
+
+/* Batched propagation of realisations sharing the layer structure of the
+ * SCAO chain: n_atm unit-amplitude turbulence layers (realisation b's layer k
+ * at atm + b*atm_real_stride + k*atm_layer_stride), the pupil stop (stop_A,
+ * stop_phase, shared; either may be NULL) and the mirror (dm_A shared or
+ * NULL, phase at dm_phase + b*dm_stride); all pupil x pupil, no crop.
+ * Outputs at A_out / phase_out + b*out_stride.  Same operation order as
+ * sb_propagate_on_axis over [turbulence..., stop, mirror]. */
+int sb_propagate_batched(const float *atm, int n_atm, long long atm_layer_stride, long long atm_real_stride,
+                         const float *stop_A, const float *stop_phase, const float *dm_A, const float *dm_phase,
+                         long long dm_stride, int n_batch, int pupil, float *A_out, float *phase_out,
+                         long long out_stride, void *stream);
 
 /* ------------------------------------------------------------------------
  * PSF — replaces specula/processing_objects/psf.py:56-137 (PSF.calc_psf,

@@ -59,6 +59,10 @@ class AtmoInputs(C.Structure):
                 ('pixel_pitch_f', C.c_float), ('airmass_pow', C.c_float), ('lambda_factor', C.c_float)]
 
 
+class AtmoLayerInputs(C.Structure):
+    _fields_ = [('seeing', vp), ('wind_speed', vp), ('wind_direction', vp), ('position', vp)]
+
+
 class PropLayer(C.Structure):
     _fields_ = [('A', fp), ('phase', fp), ('ld', C.c_int), ('top', C.c_int), ('left', C.c_int)]
 
@@ -81,6 +85,15 @@ SIGNATURES = {
     'sb_modalrec_integrator': (C.c_int, [fp, C.c_int, C.c_int, C.c_int, fp, fp, C.POINTER(IirPlan), fp, vp]),
     'sb_dm_project': (C.c_int, [fp, C.c_int, C.c_int, C.c_int, fp, C.c_int, C.c_float, ip, fp, vp]),
     'sb_device_status': (C.c_int, []),
+    'sb_atmo_evolve_batched': (C.c_int, [C.POINTER(AtmoLayer), C.POINTER(AtmoLayerInputs), C.c_int, C.c_int,
+                                         C.POINTER(AtmoInputs), vp, C.c_size_t, vp]),
+    'sb_propagate_batched': (C.c_int, [fp, C.c_int, C.c_longlong, C.c_longlong, fp, fp, fp, fp, C.c_longlong, C.c_int,
+                                       C.c_int, fp, fp, C.c_longlong, vp]),
+    'sb_sh_forward_batched': (C.c_int, [C.POINTER(ShPlan), fp, C.c_longlong, fp, C.c_longlong, fp, C.c_longlong,
+                                        C.c_int, C.c_float, fp, C.c_longlong, C.c_int, vp, C.c_size_t, vp]),
+    'sb_ccd_step_batched': (C.c_int, [C.POINTER(CcdParams), vp, vp, C.c_int, fp, fp, fp, vp]),
+    'sb_slopec_batched': (C.c_int, [C.POINTER(SlopecPlan), fp, C.c_longlong, fp, C.c_int, fp, C.c_int, C.c_int, vp,
+                                    C.c_size_t, vp]),
     'sb_dm_project_batched': (C.c_int, [fp, C.c_int, C.c_int, C.c_int, fp, C.c_int, C.c_int, C.c_float, ip, fp,
                                         C.c_longlong, vp]),
     'sb_modalrec_batched': (C.c_int, [fp, C.c_int, C.c_int, C.c_int, fp, C.c_int, C.c_int, fp, C.c_int, vp]),

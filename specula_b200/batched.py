@@ -2,16 +2,19 @@
 
 Realisations come in geometry groups (same pupil, sub-aperture grid,
 wavelength, mirror and reconstructor; their own atmosphere (r0, seed) and
-detector noise seeds).  Each realisation's chain (AtmoEvolution,
-AtmoPropagation, SH, CCD, ShSlopec) is one ``ScaoLoop``'s objects; within a
-group the slope vectors and the DM layers are rows of group matrices, so the
-group's reconstructor, integrator and mirror run as one launch each for all
-its realisations: ``sb_modalrec_batched`` and ``sb_dm_project_batched`` read
-the reconstructor and the influence functions once per step per group (the
-plain form reads them once per realisation), and one ``sb_integrator`` call
-updates every realisation's filter.  ``capture()`` puts the whole step of
-every realisation and group into one CUDA graph, the realisations' chains
-spread over several streams so that they run concurrently.
+detector noise seeds).  Each realisation is one ``ScaoLoop``'s objects, and
+within a group its field, detector frames, slopes and DM layer are rows of
+group stacks.  Per step, each realisation's AtmoEvolution and
+AtmoPropagation run on their own (different screens); then every group
+makes one launch each for the SH forward (``sb_sh_forward_batched``), the
+CCD (``sb_ccd_step_batched``, per-realisation seeds), the slopes
+(``sb_slopec_batched``), the reconstructor (``sb_modalrec_batched``: R read
+once for up to 16 realisations), the integrators (one ``sb_integrator`` call)
+and the mirror (``sb_dm_project_batched``: the influence functions read once
+for up to 16 realisations).  ``capture()`` puts the whole step of every
+realisation and group into one CUDA graph: the atmosphere/propagation chains
+over several streams, each group's launches on a stream of their own once its
+realisations' chains are done.
 
 ``BatchedScao.replay_plain()`` runs the same realisations the plain way (each
 ``ScaoLoop``'s own captured step, its own reconstructor and mirror), for
@@ -62,7 +65,7 @@ def mc_groups(seed=7, n_real=(55, 27, 14), wavelengths=(589.0, 750.0)):
             reals = []
             for _ in range(cnt):
                 r0 = float(rng.uniform(0.08, 0.20))
-                reals.append(replace(cfg, wavelength_nm=lam, r0=r0, screen_seed=100 + k, seed=1000 + 17 * k))
+                reals.append(replace(cfg, wavelength_nm=lam, r0=r0, screen_seed=100 + k, noise_seed=1000 + 17 * k))
                 k += 1
             if reals:
                 groups.append((replace(cfg, wavelength_nm=lam), reals))
@@ -90,19 +93,75 @@ class _Group:
         self.S = torch.zeros((self.n, nsl), dtype=torch.float32, device=dev)
         self.M = torch.zeros((self.n, nm), dtype=torch.float32, device=dev)
         self.dm_phase = torch.zeros((self.n, L, L), dtype=torch.float32, device=dev)
+        side = c0.n_lenses * c0.subap_npx
+        self.side = side
+        # per-realisation buffers as rows of group stacks, so the SH, CCD and
+        # slope computer run as one batched launch each for the group
+        self.EA = torch.zeros((self.n, L, L), dtype=torch.float32, device=dev)
+        self.EP = torch.zeros((self.n, L, L), dtype=torch.float32, device=dev)
+        self.I = torch.zeros((self.n, side, side), dtype=torch.float32, device=dev)
+        self.INT = torch.zeros((self.n, side, side), dtype=torch.float32, device=dev)
+        self.PIX = torch.zeros((self.n, side, side), dtype=torch.float32, device=dev)
+        self.FLUX = torch.zeros((self.n, nsl // 2), dtype=torch.float32, device=dev)
+        self.n_atm = len(c0.heights)
+        self.ATM = torch.zeros((self.n, self.n_atm, L, L), dtype=torch.float32, device=dev)
         for b, lp in enumerate(self.loops):
+            for k, layer in enumerate(lp.atmo.layer_list):
+                layer.phaseInNm = self.ATM[b, k]
             lp.slopec.slopes.slopes = self.S[b]
             lp.dm.layer.phaseInNm = self.dm_phase[b]
+            ef = lp.prop.outputs['out_on_axis_source_ef']
+            ef.A = self.EA[b]
+            ef.phaseInNm = self.EP[b]
+            lp.sh._out_i.i = self.I[b]
+            lp.ccd._integrated_i.i = self.INT[b]
+            lp.ccd._pixels.pixels = self.PIX[b]
         self.integ = Integrator(self.loops[0].simul_params, int_gain=[c0.gain] * (nm * self.n), delay=c0.delay,
                                 target_device_idx=device_idx)
         self.integ.inputs['delta_comm'].set(BaseValue(value=self.M.view(-1), target_device_idx=device_idx))
 
     def start(self):
-        for lp in self.loops:
+        for b, lp in enumerate(self.loops):
             lp.start()
+            lp.slopec._flux = self.FLUX[b]
+            lp.slopec.flux_per_subaperture_vector.value = self.FLUX[b]
             lp.step_eager()
         self.integ.setup()
         self.dm = self.loops[0].dm        # its padded IF copy and mask index serve the group
+        lp0 = self.loops[0]
+        if lp0.sh.geometry.do_interpolation:
+            raise NotImplementedError('BatchedScao: SH geometries that resample the field are not batched')
+        if any(lp.sh._photon_scale != lp0.sh._photon_scale for lp in self.loops):
+            raise ValueError('BatchedScao: the realisations of a group must share the photon flux')
+        dev = self.device
+        self.pseeds = torch.tensor([lp.ccd._photon_seed for lp in self.loops], dtype=torch.int64, device=dev)
+        self.rseeds = torch.tensor([lp.ccd._readout_seed for lp in self.loops], dtype=torch.int64, device=dev)
+        lib = _lib.load()
+        self.sh_scratch = torch.empty(self.n * lib.sb_sh_scratch_bytes(ctypes.byref(lp0.sh._plan)),
+                                      dtype=torch.uint8, device=dev)
+        self.sc_scratch = torch.empty(self.n * lib.sb_slopec_scratch_bytes(ctypes.byref(lp0.slopec._plan)),
+                                      dtype=torch.uint8, device=dev)
+        # every turbulence layer of every realisation in one atmosphere launch:
+        # per layer its strip, output row, position and its realisation's inputs
+        nl = self.n_atm
+        n_all = self.n * nl
+        self.atmo_layers = (_lib.AtmoLayer * n_all)()
+        self.atmo_inputs = (_lib.AtmoLayerInputs * n_all)()
+        for b, lp in enumerate(self.loops):
+            if lp.prop._layers[-1] is not lp.dm.layer or any(
+                    ly.phaseInNm.shape != (self.L, self.L) for ly in lp.prop._layers):
+                raise NotImplementedError('BatchedScao: pupil-sized layers in the SCAO order are batched only')
+            base = lp._inputs.data_ptr()
+            for k in range(nl):
+                i = b * nl + k
+                ctypes.memmove(ctypes.byref(self.atmo_layers[i]), ctypes.byref(lp.atmo._layers[k]),
+                               ctypes.sizeof(_lib.AtmoLayer))
+                self.atmo_inputs[i].seeing = base
+                self.atmo_inputs[i].wind_speed = base + 8 * (1 + k)
+                self.atmo_inputs[i].wind_direction = base + 8 * (1 + nl + k)
+                self.atmo_inputs[i].position = lp.atmo._positions.data_ptr() + 8 * k
+        self.atmo_work = torch.empty(n_all * 128, dtype=torch.uint8, device=dev)
+        self.stop = lp0.pupilstop
         self.sync_from_loops()
 
     def sync_from_loops(self):
@@ -115,13 +174,31 @@ class _Group:
             self.integ.out_comm.value[b * nm:(b + 1) * nm].copy_(lp.integ.out_comm.value)
 
     def chain(self, b):
-        lp = self.loops[b]
-        for o in (lp.atmo, lp.prop, lp.sh, lp.ccd, lp.slopec):
-            o.trigger_code()
+        """Nothing left per realisation: the group's launches cover its whole step."""
 
     def group_ops(self):
+        """The whole step of every realisation of the group, one launch each:
+        atmosphere (every layer), propagation, SH, CCD, slopes, the shared
+        reconstructor, the integrators and the shared mirror."""
         st = torch.cuda.current_stream(self.device).cuda_stream
         lp = self.loops[0]
+        L2 = self.L * self.L
+        consts = lp.atmo.inputs_struct(lp.atmo.delta_time)
+        _lib.call('sb_atmo_evolve_batched', self.atmo_layers, self.atmo_inputs, self.n * self.n_atm, self.L,
+                  ctypes.byref(consts), self.atmo_work.data_ptr(), self.atmo_work.numel(), st)
+        _lib.call('sb_propagate_batched', self.ATM.data_ptr(), self.n_atm, L2, self.n_atm * L2,
+                  self.stop.A.data_ptr(), self.stop.phaseInNm.data_ptr(), lp.dm.layer.A.data_ptr(),
+                  self.dm_phase.data_ptr(), L2, self.n, self.L, self.EA.data_ptr(), self.EP.data_ptr(), L2, st)
+        lp = self.loops[0]
+        L2, F2 = self.L * self.L, self.side * self.side
+        _lib.call('sb_sh_forward_batched', ctypes.byref(lp.sh._plan), self.EA.data_ptr(), L2, self.EP.data_ptr(), L2,
+                  self.EA.data_ptr(), L2, L2, lp.sh._photon_scale, self.I.data_ptr(), F2, self.n,
+                  self.sh_scratch.data_ptr(), self.sh_scratch.numel(), st)
+        _lib.call('sb_ccd_step_batched', ctypes.byref(lp.ccd._params), self.pseeds.data_ptr(), self.rseeds.data_ptr(),
+                  self.n, self.I.data_ptr(), self.INT.data_ptr(), self.PIX.data_ptr(), st)
+        _lib.call('sb_slopec_batched', ctypes.byref(lp.slopec._plan), self.PIX.data_ptr(), F2, self.S.data_ptr(),
+                  self.nsl, self.FLUX.data_ptr(), self.nsl // 2, self.n, self.sc_scratch.data_ptr(),
+                  self.sc_scratch.numel(), st)
         R = lp.rec._R
         _lib.call('sb_modalrec_batched', R.data_ptr(), self.nm, self.nsl, R.stride(0), self.S.data_ptr(),
                   self.nsl, self.n, self.M.data_ptr(), self.nm, st)

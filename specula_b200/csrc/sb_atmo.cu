@@ -22,15 +22,24 @@ struct LayerDyn {
     float scale;
 };
 
-struct EvolveArgs {
-    sb_atmo_layer layer[SB_MAX_LAYERS];
-    int n, L;
+// per-layer device pointers: the layer's seeing / wind inputs and position
+struct LayerPtrs {
+    const double *seeing, *wind_speed, *wind_direction;
     double *pos;
-    // per-step parameters computed on the device from device inputs (NULL:
-    // the delta / rot90 / rotation / scale fields of layer[] are used)
+};
+
+template <int CAP>
+struct EvolveArgsT {
+    sb_atmo_layer layer[CAP];
+    LayerPtrs ptr[CAP];
+    int n, L;
+    // constants of the per-step parameters (its pointers are not read here)
     sb_atmo_inputs in;
+    // per-step parameters computed on the device from the inputs (NULL: the
+    // delta / rot90 / rotation / scale fields of layer[] are used)
     LayerDyn *dyn;
 };
+constexpr int kBatchLayers = 64;   // layers per batched launch
 
 // Per-step layer parameters from device-resident seeing / wind inputs, with
 // the reference's float64 / float32 arithmetic (atmo_evolution.py:262-294):
@@ -38,11 +47,11 @@ struct EvolveArgs {
 // (NumPy promotes the Python-float products to the float32 airmass), shift
 // wind_speed*dt/pitch, rot90 by trunc(dir/90) mod 4 and the fractional-degree
 // rotation about the layer centre (scipy.ndimage.rotate's output->input map).
-__device__ LayerDyn layer_dyn(const sb_atmo_inputs &in, int k, int L) {
+__device__ LayerDyn layer_dyn(const sb_atmo_inputs &in, const LayerPtrs &p, int L) {
     LayerDyn d;
-    const double seeing = in.seeing[0];
-    const double ws = in.wind_speed[in.n_wind_speed > 1 ? k : 0];
-    const double wd = in.wind_direction[in.n_wind_direction > 1 ? k : 0];
+    const double seeing = p.seeing[0];
+    const double ws = p.wind_speed[0];
+    const double wd = p.wind_direction[0];
     const double r0d = __ddiv_rn(__dmul_rn(0.9759, 0.5), __dmul_rn(seeing, 4.848));
     const float r0 = __fmul_rn((float)r0d, in.airmass_pow);
     const float r0l = __fmul_rn(r0, in.lambda_factor);
@@ -79,18 +88,20 @@ __device__ __forceinline__ LayerDyn static_dyn(const sb_atmo_layer &l) {
 
 // new = last + delta; cycle to 0 when new + L reaches the strip width;
 // float64 like the reference's NumPy arithmetic (atmo_evolution.py:269-277)
-__global__ void atmo_advance_kernel(EvolveArgs a) {
+template <int CAP>
+__global__ void atmo_advance_kernel(EvolveArgsT<CAP> a) {
     const int k = threadIdx.x;
     if (k >= a.n) return;
     double delta = a.layer[k].delta;
     if (a.dyn) {
-        const LayerDyn d = layer_dyn(a.in, k, a.L);
+        const LayerDyn d = layer_dyn(a.in, a.ptr[k], a.L);
         a.dyn[k] = d;
         delta = d.delta;
     }
-    double np = __dadd_rn(a.pos[k], delta);
+    double *pos = a.ptr[k].pos;
+    double np = __dadd_rn(*pos, delta);
     if (__dadd_rn(np, (double)a.L) >= (double)a.layer[k].screen_cols) np = 0.0;
-    a.pos[k] = np;
+    *pos = np;
 }
 
 // Output tiles of 32 x 32 pixels per CTA (32 x 8 threads, 4 rows each).
@@ -101,7 +112,8 @@ __global__ void atmo_advance_kernel(EvolveArgs a) {
 constexpr int kTile = 32;
 constexpr int kBox = kTile + 8;   // footprint of a tile rotated by < 1 degree, plus the bilinear +1
 
-__global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgs a) {
+template <int CAP>
+__global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgsT<CAP> a) {
     __shared__ float Q[kBox][kBox + 1];
     __shared__ int fp[5];                 // footprint br0, br1, bc0, bc1 and the interior flag
     __shared__ LayerDyn lyd;              // this layer's per-step parameters
@@ -141,7 +153,7 @@ __global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgs a) {
         fp[0] = br0; fp[1] = br1; fp[2] = bc0; fp[3] = bc1; fp[4] = interior;
     }
     // integer position and float32 remainder (atmo_evolution.py:278-279)
-    const double np = a.pos[blockIdx.z];
+    const double np = *a.ptr[blockIdx.z].pos;
     const double q = floor(np);
     const float *row0 = lys.screen + (long long)q;
     const int ld = lys.screen_ld;
@@ -288,19 +300,19 @@ __global__ void __launch_bounds__(256) propagate_kernel(PropArgs a, float *__res
 
 namespace {
 
-int launch_evolve(const char *who, const sb_atmo_layer *layers, int n_layers, int L, double *positions,
-                  const sb_atmo_inputs *in, LayerDyn *dyn, void *stream) {
-    if (!layers || !positions || n_layers < 0 || L < 1) return sb::fail(SB_EINVAL, "%s: bad args", who);
-    if (n_layers > SB_MAX_LAYERS) return sb::fail(SB_ESHAPE, "%s: at most %d layers", who, SB_MAX_LAYERS);
-    if (n_layers == 0) return SB_OK;
-    EvolveArgs a;
+template <int CAP>
+int launch_evolve_t(const char *who, const sb_atmo_layer *layers, const LayerPtrs *ptrs, int n_layers, int L,
+                    const sb_atmo_inputs *in, LayerDyn *dyn, void *stream) {
+    EvolveArgsT<CAP> a;
     for (int k = 0; k < n_layers; ++k) {
         const sb_atmo_layer &l = layers[k];
         // the window [pos, pos + L] must stay inside the strip for every
         // position the cycling rule allows: pos + L < screen_cols
-        if (!l.screen || !l.out || l.screen_cols < L + 1 || l.screen_ld < l.screen_cols ||
+        if (!l.screen || !l.out || l.screen_cols < L + 1 || l.screen_ld < l.screen_cols || !ptrs[k].pos ||
             (!in && (l.rot90 < 0 || l.rot90 > 3 || !(l.delta >= 0.0))))
             return sb::fail(SB_EINVAL, "%s: layer %d: bad screen window", who, k);
+        if (in && (!ptrs[k].seeing || !ptrs[k].wind_speed || !ptrs[k].wind_direction))
+            return sb::fail(SB_EINVAL, "%s: layer %d: null input pointer", who, k);
         // element offsets inside the strip window are 32-bit
         if ((long long)L * l.screen_ld + l.screen_cols >= (1LL << 31))
             return sb::fail(SB_ESHAPE, "%s: layer %d: strip too large", who, k);
@@ -309,22 +321,85 @@ int launch_evolve(const char *who, const sb_atmo_layer *layers, int n_layers, in
         if (!in && l.rotate && !(fabs(l.m01) < 0.0175 && fabs(l.m10) < 0.0175 && l.m00 > 0.9998 && l.m11 > 0.9998))
             return sb::fail(SB_EINVAL, "%s: layer %d: rotation must be below one degree", who, k);
         a.layer[k] = l;
+        a.ptr[k] = ptrs[k];
     }
     a.n = n_layers;
     a.L = L;
-    a.pos = positions;
     a.dyn = dyn;
     if (in) a.in = *in;
     cudaStream_t st = sb::as_stream(stream);
-    atmo_advance_kernel<<<1, 32, 0, st>>>(a);
+    atmo_advance_kernel<CAP><<<1, CAP < 32 ? 32 : CAP, 0, st>>>(a);
     int rc = sb::check_launch("atmo_advance_kernel");
     if (rc) return rc;
     dim3 block(32, 8), grid((L + kTile - 1) / kTile, (L + kTile - 1) / kTile, n_layers);
-    atmo_evolve_kernel<<<grid, block, 0, st>>>(a);
+    atmo_evolve_kernel<CAP><<<grid, block, 0, st>>>(a);
     return sb::check_launch("atmo_evolve_kernel");
 }
 
+int launch_evolve(const char *who, const sb_atmo_layer *layers, int n_layers, int L, double *positions,
+                  const sb_atmo_inputs *in, LayerDyn *dyn, void *stream) {
+    if (!layers || !positions || n_layers < 0 || L < 1) return sb::fail(SB_EINVAL, "%s: bad args", who);
+    if (n_layers > SB_MAX_LAYERS) return sb::fail(SB_ESHAPE, "%s: at most %d layers", who, SB_MAX_LAYERS);
+    if (n_layers == 0) return SB_OK;
+    LayerPtrs ptrs[SB_MAX_LAYERS];
+    for (int k = 0; k < n_layers; ++k) {
+        ptrs[k].pos = positions + k;
+        ptrs[k].seeing = in ? in->seeing : nullptr;
+        ptrs[k].wind_speed = in ? in->wind_speed + (in->n_wind_speed > 1 ? k : 0) : nullptr;
+        ptrs[k].wind_direction = in ? in->wind_direction + (in->n_wind_direction > 1 ? k : 0) : nullptr;
+    }
+    return launch_evolve_t<SB_MAX_LAYERS>(who, layers, ptrs, n_layers, L, in, dyn, stream);
+}
+
+// Batched on-axis propagation of realisations with the same layer structure:
+// n_atm unit-amplitude turbulence layers (rows of a stack), one shared
+// amplitude/phase layer (the pupil stop) and a mirror layer with a shared
+// amplitude and a per-realisation phase; same operation order as
+// propagate_kernel, every layer pupil-sized (no crop).
+__global__ void __launch_bounds__(256) propagate_batched_kernel(const float *__restrict__ atm, int n_atm,
+                                                                long long atm_layer_stride,
+                                                                long long atm_real_stride,
+                                                                const float *__restrict__ stop_A,
+                                                                const float *__restrict__ stop_phase,
+                                                                const float *__restrict__ dm_A,
+                                                                const float *__restrict__ dm_phase,
+                                                                long long dm_stride, int n, float *__restrict__ A,
+                                                                float *__restrict__ P, long long out_stride) {
+    const long long b = blockIdx.y;
+    const float *at = atm + b * atm_real_stride;
+    const float *dp = dm_phase + b * dm_stride;
+    float *Ao = A + b * out_stride;
+    float *Po = P + b * out_stride;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        float amp = 1.0f, ph = 0.0f;
+        for (int k = 0; k < n_atm; ++k) ph = __fadd_rn(ph, at[k * atm_layer_stride + e]);
+        if (stop_A) amp = __fmul_rn(amp, stop_A[e]);
+        if (stop_phase) ph = __fadd_rn(ph, stop_phase[e]);
+        if (dm_A) amp = __fmul_rn(amp, dm_A[e]);
+        ph = __fadd_rn(ph, dp[e]);
+        Ao[e] = amp;
+        Po[e] = ph;
+    }
+}
+
 }  // namespace
+
+extern "C" int sb_propagate_batched(const float *atm, int n_atm, long long atm_layer_stride, long long atm_real_stride,
+                                    const float *stop_A, const float *stop_phase, const float *dm_A,
+                                    const float *dm_phase, long long dm_stride, int n_batch, int pupil, float *A_out,
+                                    float *phase_out, long long out_stride, void *stream) {
+    sb::clear_error();
+    const long long n = (long long)pupil * pupil;
+    if ((n_atm > 0 && !atm) || !dm_phase || !A_out || !phase_out || n_atm < 0 || n_batch < 1 || n_batch > 65535 ||
+        pupil < 1 || atm_layer_stride < (n_atm > 0 ? n : 0) || dm_stride < n || out_stride < n)
+        return sb::fail(SB_EINVAL, "sb_propagate_batched: bad args");
+    int nblk = (int)((n + 255) / 256);
+    nblk = nblk > 296 ? 296 : nblk;
+    propagate_batched_kernel<<<dim3(nblk, n_batch), 256, 0, sb::as_stream(stream)>>>(
+        atm, n_atm, atm_layer_stride, atm_real_stride, stop_A, stop_phase, dm_A, dm_phase, dm_stride, (int)n, A_out,
+        phase_out, out_stride);
+    return sb::check_launch("propagate_batched_kernel");
+}
 
 extern "C" int sb_atmo_evolve(const sb_atmo_layer *layers, int n_layers, int L, double *positions, void *stream) {
     sb::clear_error();
@@ -349,6 +424,33 @@ extern "C" int sb_atmo_evolve_inputs(const sb_atmo_layer *layers, int n_layers, 
         return sb::fail(SB_ESCRATCH, "sb_atmo_evolve_inputs: work needs %zu bytes", sb_atmo_work_bytes(n_layers));
     return launch_evolve("sb_atmo_evolve_inputs", layers, n_layers, L, positions, in,
                          static_cast<LayerDyn *>(work), stream);
+}
+
+extern "C" int sb_atmo_evolve_batched(const sb_atmo_layer *layers, const sb_atmo_layer_inputs *inputs, int n_layers,
+                                      int L, const sb_atmo_inputs *constants, void *work, size_t work_bytes,
+                                      void *stream) {
+    sb::clear_error();
+    if (!layers || !inputs || !constants || n_layers < 0 || L < 1 || !(constants->pixel_pitch > 0.0) ||
+        !(constants->delta_time >= 0.0))
+        return sb::fail(SB_EINVAL, "sb_atmo_evolve_batched: bad args");
+    if (n_layers == 0) return SB_OK;
+    if (!work || work_bytes < (size_t)n_layers * sizeof(LayerDyn))
+        return sb::fail(SB_ESCRATCH, "sb_atmo_evolve_batched: work needs %zu bytes", (size_t)n_layers * sizeof(LayerDyn));
+    LayerPtrs ptrs[kBatchLayers];
+    for (int k0 = 0; k0 < n_layers; k0 += kBatchLayers) {
+        const int n = n_layers - k0 < kBatchLayers ? n_layers - k0 : kBatchLayers;
+        for (int k = 0; k < n; ++k) {
+            const sb_atmo_layer_inputs &li = inputs[k0 + k];
+            ptrs[k].seeing = li.seeing;
+            ptrs[k].wind_speed = li.wind_speed;
+            ptrs[k].wind_direction = li.wind_direction;
+            ptrs[k].pos = li.position;
+        }
+        const int rc = launch_evolve_t<kBatchLayers>("sb_atmo_evolve_batched", layers + k0, ptrs, n, L, constants,
+                                                     static_cast<LayerDyn *>(work) + k0, stream);
+        if (rc) return rc;
+    }
+    return SB_OK;
 }
 
 extern "C" int sb_propagate_on_axis(const sb_prop_layer *layers, int n_layers, int pupil, float *A_out,

@@ -325,10 +325,15 @@ __global__ void __launch_bounds__(32 * (kDmConsumerWarps + 1), 1)
 // warps, one column per thread and NB accumulators; the NB command vectors
 // are staged in shared memory as [mode][NB].
 constexpr int kDbWarps = 8;
+// more stages than the single-vector kernel: the NB accumulators make each
+// stage's consumption longer, and this kernel need not leave room for
+// concurrent kernels
+constexpr int kDbStages = 5;
+constexpr int kDbMaxModes = 1024;
 template <int NB>
 size_t dm_batched_smem_bytes(int nmodes) {
     const int nst = (nmodes + kDmRows - 1) / kDmRows;
-    return 1024 + (size_t)kDmStages * kDmRows * kDmCols * 4 + 2 * kDmStages * 8 + (size_t)nst * kDmRows * NB * 4;
+    return 1024 + (size_t)kDbStages * kDmRows * kDmCols * 4 + 2 * kDbStages * 8 + (size_t)nst * kDmRows * NB * 4;
 }
 
 template <int NB>
@@ -339,14 +344,14 @@ __global__ void __launch_bounds__(32 * (kDbWarps + 1), 1)
     extern __shared__ unsigned char smem_raw[];
     unsigned char *base = smem_raw + ((1024 - (sb::smem_u32(smem_raw) & 1023)) & 1023);
     float *ring = reinterpret_cast<float *>(base);
-    uint64_t *full = reinterpret_cast<uint64_t *>(base + (size_t)kDmStages * kDmRows * kDmCols * 4);
-    uint64_t *empty = full + kDmStages;
-    float *c = reinterpret_cast<float *>(empty + kDmStages);       // [mode][NB]
+    uint64_t *full = reinterpret_cast<uint64_t *>(base + (size_t)kDbStages * kDmRows * kDmCols * 4);
+    uint64_t *empty = full + kDbStages;
+    float *c = reinterpret_cast<float *>(empty + kDbStages);       // [mode][NB]
     __shared__ int abort_flag, issued;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nst = (nmodes + kDmRows - 1) / kDmRows;
     if (tid == 0) {
-        for (int s = 0; s < kDmStages; ++s) {
+        for (int s = 0; s < kDbStages; ++s) {
             sb::mbar_init(&full[s], 1);
             sb::mbar_init(&empty[s], kDbWarps);
         }
@@ -368,8 +373,8 @@ __global__ void __launch_bounds__(32 * (kDbWarps + 1), 1)
             const uint64_t pol = sb::l2_evict_first_policy();
             int q = 0;
             for (; q < total; ++q) {
-                const int slot = q % kDmStages;
-                if (q >= kDmStages && !sb::mbar_wait(&empty[slot], ((q / kDmStages) - 1) & 1)) {
+                const int slot = q % kDbStages;
+                if (q >= kDbStages && !sb::mbar_wait(&empty[slot], ((q / kDbStages) - 1) & 1)) {
                     atomicExch(&g_dm_status, 3);
                     abort_flag = 1;
                     break;
@@ -387,8 +392,8 @@ __global__ void __launch_bounds__(32 * (kDbWarps + 1), 1)
 #pragma unroll
         for (int b = 0; b < NB; ++b) acc[b] = 0.f;
         for (int q = 0; q < total; ++q) {
-            const int slot = q % kDmStages;
-            if (!sb::mbar_wait(&full[slot], (q / kDmStages) & 1)) {
+            const int slot = q % kDbStages;
+            if (!sb::mbar_wait(&full[slot], (q / kDbStages) & 1)) {
                 atomicExch(&g_dm_status, 4);
                 abort_flag = 1;
                 break;
@@ -426,7 +431,7 @@ __global__ void __launch_bounds__(32 * (kDbWarps + 1), 1)
     }
     __syncthreads();
     if (abort_flag && tid == 0) {
-        for (int q = 0; q < issued; ++q) sb::mbar_wait(&full[q % kDmStages], (q / kDmStages) & 1);
+        for (int q = 0; q < issued; ++q) sb::mbar_wait(&full[q % kDbStages], (q / kDbStages) & 1);
     }
 }
 
@@ -583,7 +588,7 @@ int launch_dm_batched(const CUtensorMap &map, int n_modes, int n_valid, const fl
     const size_t smem = dm_batched_smem_bytes<NB>(n_modes);
     if (dev >= 0 && dev < 64 && !attr_set[dev]) {
         if (cudaFuncSetAttribute(dm_project_batched_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)dm_batched_smem_bytes<NB>(kDmMaxModes / 2)) != cudaSuccess)
+                                 (int)dm_batched_smem_bytes<NB>(kDbMaxModes)) != cudaSuccess)
             return sb::fail(SB_ECUDA, "sb_dm_project_batched: %s", cudaGetErrorString(cudaGetLastError()));
         attr_set[dev] = true;
     }
@@ -603,8 +608,8 @@ extern "C" int sb_dm_project_batched(const float *ifunc, int n_modes, int n_vali
     if (!ifunc || !cmd || !mask_idx || !phase || n_modes < 1 || n_valid < 0 || ld_if < n_valid || n_batch < 1 ||
         ld_cmd < n_modes || phase_stride < 1)
         return sb::fail(SB_EINVAL, "sb_dm_project_batched: bad args");
-    if (n_modes > kDmMaxModes / 2)
-        return sb::fail(SB_ESHAPE, "sb_dm_project_batched: at most %d modes", kDmMaxModes / 2);
+    if (n_modes > kDbMaxModes)
+        return sb::fail(SB_ESHAPE, "sb_dm_project_batched: at most %d modes", kDbMaxModes);
     if (ld_if % 4 || (uintptr_t)ifunc % 16)
         return sb::fail(SB_EINVAL, "sb_dm_project_batched: influence-function rows must be 16-byte aligned");
     if (n_valid == 0) return SB_OK;

@@ -117,8 +117,14 @@ __device__ __forceinline__ float std_normal(uint32_t e, uint64_t frame, uint64_t
     return sqrtf(-2.0f * __logf(u01f(r.x))) * cospif(2.0f * u01f(r.y));
 }
 
+// Batched launches (seeds != NULL): the pixels of n_batch realisations are
+// contiguous, n_per each; realisation b draws with photon_seeds[b] /
+// readout_seeds[b] and its own pixel index, so its frame equals what a
+// single-realisation launch with those seeds gives.
 __global__ void __launch_bounds__(256, 5) ccd_kernel(sb_ccd_params p, const float *__restrict__ in,
-                                                  float *__restrict__ integ, float *__restrict__ pix) {
+                                                  float *__restrict__ integ, float *__restrict__ pix,
+                                                  const uint64_t *__restrict__ photon_seeds,
+                                                  const uint64_t *__restrict__ readout_seeds, int n_per) {
     // frame bookkeeping lives on the device; every block reads it before the
     // last block to finish advances it (see the end of the kernel)
     volatile sb_ccd_state *vs = p.state;
@@ -143,9 +149,17 @@ __global__ void __launch_bounds__(256, 5) ccd_kernel(sb_ccd_params p, const floa
         if (p.qe != 1.0f) f = __fmul_rn(f, p.qe);                  // ccd.py:282-287
         f = __fadd_rn(f, p.bg_plus_dark);                           // ccd.py:220-221
         float outv;
+        uint32_t eloc = (uint32_t)e;
+        uint64_t pseed = p.photon_seed, rseed = p.readout_seed;
+        if (photon_seeds) {
+            const int b = e / n_per;
+            eloc = (uint32_t)(e - b * n_per);
+            pseed = photon_seeds[b];
+            rseed = readout_seeds[b];
+        }
         if (p.photon_noise) {
-            double v = poisson_sample(f, (uint32_t)e, frame, p.photon_seed, logfact);
-            if (p.readout_noise) v += truncf(std_normal((uint32_t)e, frame, p.readout_seed) * p.readout_level);
+            double v = poisson_sample(f, eloc, frame, pseed, logfact);
+            if (p.readout_noise) v += truncf(std_normal(eloc, frame, rseed) * p.readout_level);
             // ADU: round(x*g)+bias, clamp at 0, -bias, /g, back to the
             // integer dtype of the Poisson draw (ccd.py:247-258)
             double x = rint(v * (double)p.adu_gain) + (double)p.adu_bias;
@@ -158,7 +172,7 @@ __global__ void __launch_bounds__(256, 5) ccd_kernel(sb_ccd_params p, const floa
             outv = (float)x;
         } else {
             if (p.readout_noise)
-                f = __fadd_rn(f, __fmul_rn(std_normal((uint32_t)e, frame, p.readout_seed), p.readout_level));
+                f = __fadd_rn(f, __fmul_rn(std_normal(eloc, frame, rseed), p.readout_level));
             outv = f;
         }
         pix[e] = outv;
@@ -196,8 +210,16 @@ __global__ void philox_raw_kernel(uint32_t k0, uint32_t k1, uint32_t c1, uint32_
 __global__ void __launch_bounds__(256) slopec_sums_kernel(sb_slopec_plan pl, const float *__restrict__ pix,
                                                           float *__restrict__ flux, float *__restrict__ tot,
                                                           float *__restrict__ sxn, float *__restrict__ syn,
-                                                          float *__restrict__ part_tot) {
+                                                          float *__restrict__ part_tot, long long frame_stride,
+                                                          int flux_stride, int work_stride) {
     __shared__ float wsum[8];
+    // batched launches: blockIdx.y selects the realisation
+    pix += blockIdx.y * frame_stride;
+    flux += (size_t)blockIdx.y * flux_stride;
+    tot += (size_t)blockIdx.y * work_stride;
+    sxn += (size_t)blockIdx.y * work_stride;
+    syn += (size_t)blockIdx.y * work_stride;
+    part_tot += (size_t)blockIdx.y * gridDim.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const bool valid = s < pl.n_subaps;
@@ -238,8 +260,14 @@ __global__ void __launch_bounds__(256) slopec_finish_kernel(int n, const float *
                                                             const float *__restrict__ sxn,
                                                             const float *__restrict__ syn,
                                                             const float *__restrict__ part_tot, int nparts,
-                                                            float *__restrict__ slopes) {
+                                                            float *__restrict__ slopes, int slopes_stride,
+                                                            int work_stride) {
     __shared__ double red[33];
+    tot += (size_t)blockIdx.y * work_stride;
+    sxn += (size_t)blockIdx.y * work_stride;
+    syn += (size_t)blockIdx.y * work_stride;
+    part_tot += (size_t)blockIdx.y * nparts;
+    slopes += (size_t)blockIdx.y * slopes_stride;
     double acc = 0.0;
     for (int e = threadIdx.x; e < nparts; e += blockDim.x) acc += part_tot[e];
     acc = sb::block_sum_all_d(acc, red);
@@ -264,7 +292,27 @@ extern "C" int sb_ccd_step(const sb_ccd_params *p, const float *intensity, float
     if (p->photon_noise && !(p->adu_gain > 0.f)) return sb::fail(SB_EINVAL, "sb_ccd_step: ADU gain must be > 0");
     int nblk = (p->n_pixels + 255) / 256;
     nblk = nblk < 1 ? 1 : (nblk > 1184 ? 1184 : nblk);
-    ccd_kernel<<<nblk, 256, 0, sb::as_stream(stream)>>>(*p, intensity, integrated, pixels);
+    ccd_kernel<<<nblk, 256, 0, sb::as_stream(stream)>>>(*p, intensity, integrated, pixels, nullptr, nullptr,
+                                                        p->n_pixels);
+    return sb::check_launch("ccd_kernel");
+}
+
+extern "C" int sb_ccd_step_batched(const sb_ccd_params *p, const uint64_t *photon_seeds,
+                                   const uint64_t *readout_seeds, int n_batch, const float *intensity,
+                                   float *integrated, float *pixels, void *stream) {
+    sb::clear_error();
+    if (!p || !photon_seeds || !readout_seeds || !intensity || !integrated || !pixels || !p->state || n_batch < 1)
+        return sb::fail(SB_EINVAL, "sb_ccd_step_batched: null pointer");
+    if (p->n_pixels < 1 || p->frames_per_read < 1 || (long long)p->n_pixels * n_batch > 0x7fffffffLL)
+        return sb::fail(SB_EINVAL, "sb_ccd_step_batched: bad sizes");
+    if (p->photon_noise && !(p->adu_gain > 0.f))
+        return sb::fail(SB_EINVAL, "sb_ccd_step_batched: ADU gain must be > 0");
+    sb_ccd_params q = *p;
+    q.n_pixels = p->n_pixels * n_batch;
+    int nblk = (q.n_pixels + 255) / 256;
+    nblk = nblk > 1184 ? 1184 : nblk;
+    ccd_kernel<<<nblk, 256, 0, sb::as_stream(stream)>>>(q, intensity, integrated, pixels, photon_seeds, readout_seeds,
+                                                        p->n_pixels);
     return sb::check_launch("ccd_kernel");
 }
 
@@ -285,27 +333,54 @@ extern "C" size_t sb_slopec_scratch_bytes(const sb_slopec_plan *pl) {
     return ((size_t)(3 * pl->n_subaps + nparts) * sizeof(float) + 255) & ~(size_t)255;
 }
 
+namespace {
+
+int slopec_impl(const char *who, const sb_slopec_plan *pl, const float *pixels, long long frame_stride, float *slopes,
+                int slopes_stride, float *flux, int flux_stride, int n_batch, void *scratch, size_t scratch_bytes,
+                void *stream) {
+    if (!pl || !pixels || !slopes || !flux || !pl->idxs || !pl->xw || !pl->yw || !pl->mw)
+        return sb::fail(SB_EINVAL, "%s: null pointer", who);
+    if (pl->n_subaps < 1 || pl->npx2 < 1 || n_batch < 1 || n_batch > 65535)
+        return sb::fail(SB_EINVAL, "%s: empty sub-aperture set", who);
+    const size_t one = sb_slopec_scratch_bytes(pl);
+    const size_t need = one * (size_t)n_batch;
+    if (!scratch || scratch_bytes < need)
+        return sb::fail(SB_ESCRATCH, "%s: scratch needs %zu bytes, got %zu", who, need, scratch_bytes);
+    // per realisation: tot, sxn, syn (n_subaps each) in one region, then the block partials
+    const int n = pl->n_subaps;
+    const int work_stride = 3 * n;
+    float *tot = static_cast<float *>(scratch);
+    float *sxn = tot + n;
+    float *syn = sxn + n;
+    cudaStream_t st = sb::as_stream(stream);
+    const int warps_per_block = 8;
+    const int nblk = (n + warps_per_block - 1) / warps_per_block;
+    float *part = tot + (size_t)work_stride * n_batch;
+    slopec_sums_kernel<<<dim3(nblk, n_batch), 32 * warps_per_block, 0, st>>>(*pl, pixels, flux, tot, sxn, syn, part,
+                                                                            frame_stride, flux_stride, work_stride);
+    int rc = sb::check_launch("slopec_sums_kernel");
+    if (rc) return rc;
+    int nb2 = (n + 255) / 256;
+    nb2 = nb2 > 148 ? 148 : nb2;
+    slopec_finish_kernel<<<dim3(nb2, n_batch), 256, 0, st>>>(n, tot, sxn, syn, part, nblk, slopes, slopes_stride,
+                                                             work_stride);
+    return sb::check_launch("slopec_finish_kernel");
+}
+
+}  // namespace
+
 extern "C" int sb_slopec(const sb_slopec_plan *pl, const float *pixels, float *slopes, float *flux, void *scratch,
                          size_t scratch_bytes, void *stream) {
     sb::clear_error();
-    if (!pl || !pixels || !slopes || !flux || !pl->idxs || !pl->xw || !pl->yw || !pl->mw)
-        return sb::fail(SB_EINVAL, "sb_slopec: null pointer");
-    if (pl->n_subaps < 1 || pl->npx2 < 1) return sb::fail(SB_EINVAL, "sb_slopec: empty sub-aperture set");
-    const size_t need = sb_slopec_scratch_bytes(pl);
-    if (!scratch || scratch_bytes < need)
-        return sb::fail(SB_ESCRATCH, "sb_slopec: scratch needs %zu bytes, got %zu", need, scratch_bytes);
-    float *tot = static_cast<float *>(scratch);
-    float *sxn = tot + pl->n_subaps;
-    float *syn = sxn + pl->n_subaps;
-    cudaStream_t st = sb::as_stream(stream);
-    const int warps_per_block = 8;
-    const int nblk = (pl->n_subaps + warps_per_block - 1) / warps_per_block;
-    float *part = syn + pl->n_subaps;
-    slopec_sums_kernel<<<nblk, 32 * warps_per_block, 0, st>>>(*pl, pixels, flux, tot, sxn, syn, part);
-    int rc = sb::check_launch("slopec_sums_kernel");
-    if (rc) return rc;
-    int nb2 = (pl->n_subaps + 255) / 256;
-    nb2 = nb2 > 148 ? 148 : nb2;
-    slopec_finish_kernel<<<nb2, 256, 0, st>>>(pl->n_subaps, tot, sxn, syn, part, nblk, slopes);
-    return sb::check_launch("slopec_finish_kernel");
+    return slopec_impl("sb_slopec", pl, pixels, 0, slopes, 0, flux, 0, 1, scratch, scratch_bytes, stream);
+}
+
+extern "C" int sb_slopec_batched(const sb_slopec_plan *pl, const float *pixels, long long frame_stride, float *slopes,
+                                 int slopes_stride, float *flux, int flux_stride, int n_batch, void *scratch,
+                                 size_t scratch_bytes, void *stream) {
+    sb::clear_error();
+    if (pl && (slopes_stride < 2 * pl->n_subaps || flux_stride < pl->n_subaps || frame_stride < 1))
+        return sb::fail(SB_EINVAL, "sb_slopec_batched: strides smaller than one realisation");
+    return slopec_impl("sb_slopec_batched", pl, pixels, frame_stride, slopes, slopes_stride, flux, flux_stride,
+                       n_batch, scratch, scratch_bytes, stream);
 }

@@ -31,7 +31,22 @@ struct ShArgs {
     float *out;
     float *part_I;
     float *part_A;
+    // batched launches: blockIdx.z selects the realisation (strides in
+    // elements; 0 and gridDim.z = 1 for a single field)
+    long long sA, sph, sAn, sout;
+    int nbp;                       // partial sums per realisation
 };
+
+// the realisation's slice of a batched launch
+__device__ __forceinline__ void batch_slice(ShArgs &a) {
+    const long long z = blockIdx.z;
+    a.A += z * a.sA;
+    a.ph += z * a.sph;
+    a.A_norm += z * a.sAn;
+    a.out += z * a.sout;
+    a.part_I += z * a.nbp;
+    a.part_A += z * a.nbp;
+}
 
 struct ShSmem {
     int tw, tilt, mask, rebin, per_warp_E, per_warp_G, per_warp_I, per_warp_H, tables, per_warp;
@@ -58,6 +73,7 @@ __host__ __device__ inline ShSmem sh_smem_layout(int p, int cs, int npx) {
 constexpr int kU = 4;   // independent accumulators per lane
 
 __global__ void __launch_bounds__(256, 4) sh_forward_kernel(ShArgs a) {
+    batch_slice(a);
     extern __shared__ __align__(16) unsigned char smem[];
     const ShSmem L = sh_smem_layout(a.p, a.cs, a.npx);
     float2 *twT = reinterpret_cast<float2 *>(smem + L.tw);
@@ -201,6 +217,7 @@ __global__ void __launch_bounds__(256, 4) sh_forward_kernel(ShArgs a) {
 
 template <int P, int CS, int NPX>
 __global__ void __launch_bounds__(256, 4) sh_forward_fixed_kernel(ShArgs a) {
+    batch_slice(a);
     constexpr int PE = P + 1;
     __shared__ float2 twT[P * CS];          // twT[c][b] = W[b][c]
     __shared__ float2 tilt[P * P];
@@ -322,6 +339,10 @@ ShKernel fixed_kernel(int p, int cs, int npx) {
 __global__ void __launch_bounds__(256) sh_normalize_kernel(const float *part_I, const float *part_A, int nparts,
                                                            float photon_scale, float *out, int n_out) {
     __shared__ double red[33];
+    // batched launches: blockIdx.y selects the realisation
+    part_I += (size_t)blockIdx.y * nparts;
+    part_A += (size_t)blockIdx.y * nparts;
+    out += (size_t)blockIdx.y * n_out;
     double si = 0.0, sa = 0.0;
     for (int e = threadIdx.x; e < nparts; e += blockDim.x) {
         si += part_I[e];
@@ -391,27 +412,28 @@ extern "C" size_t sb_sh_scratch_bytes(const sb_sh_plan *pl) {
     return ((2 * nb * sizeof(float)) + 255) & ~(size_t)255;
 }
 
-extern "C" int sb_sh_forward(const sb_sh_plan *pl, const float *A, const float *phase_nm, const float *A_norm,
-                             int n_norm, float photon_scale, float *intensity, void *scratch,
-                             size_t scratch_bytes, void *stream) {
-    sb::clear_error();
+namespace {
+
+int sh_forward_impl(const char *who, const sb_sh_plan *pl, const float *A, long long sA, const float *phase_nm,
+                    long long sph, const float *A_norm, long long sAn, int n_norm, float photon_scale,
+                    float *intensity, long long sout, int n_batch, void *scratch, size_t scratch_bytes, void *stream) {
     if (!pl || !A || !phase_nm || !A_norm || !intensity || !pl->twiddle || !pl->tilt || !pl->fp_mask ||
         !pl->rebin)
-        return sb::fail(SB_EINVAL, "sb_sh_forward: null pointer");
+        return sb::fail(SB_EINVAL, "%s: null pointer", who);
     if (pl->n_lenses < 1 || pl->np_sub < 1 || pl->cutsize < 1 || pl->subap_npx < 1 || n_norm < 0 ||
-        pl->field_ld < pl->n_lenses * pl->np_sub)
-        return sb::fail(SB_EINVAL, "sb_sh_forward: bad geometry");
+        pl->field_ld < pl->n_lenses * pl->np_sub || n_batch < 1 || n_batch > 65535)
+        return sb::fail(SB_EINVAL, "%s: bad geometry", who);
     int spc;
     dim3 grid;
     size_t smem;
     if (sh_grid(pl, &spc, &grid, &smem))
-        return sb::fail(SB_ESHAPE, "sb_sh_forward: sub-aperture (np=%d, cut=%d, npx=%d) does not fit in shared memory",
+        return sb::fail(SB_ESHAPE, "%s: sub-aperture (np=%d, cut=%d, npx=%d) does not fit in shared memory", who,
                         pl->np_sub, pl->cutsize, pl->subap_npx);
-    const size_t need = sb_sh_scratch_bytes(pl);
+    const size_t need = sb_sh_scratch_bytes(pl) * (size_t)n_batch;
     if (!scratch || scratch_bytes < need)
-        return sb::fail(SB_ESCRATCH, "sb_sh_forward: scratch needs %zu bytes, got %zu", need, scratch_bytes);
+        return sb::fail(SB_ESCRATCH, "%s: scratch needs %zu bytes, got %zu", who, need, scratch_bytes);
     const int nb = grid.x * grid.y;
-    ShArgs a;
+    ShArgs a = {};
     a.n = pl->n_lenses;
     a.p = pl->np_sub;
     a.cs = pl->cutsize;
@@ -428,8 +450,15 @@ extern "C" int sb_sh_forward(const sb_sh_plan *pl, const float *A, const float *
     a.A_norm = A_norm;
     a.n_norm = n_norm;
     a.out = intensity;
+    // partial sums: part_I for every realisation, then part_A
     a.part_I = static_cast<float *>(scratch);
-    a.part_A = static_cast<float *>(scratch) + nb;
+    a.part_A = static_cast<float *>(scratch) + (size_t)nb * n_batch;
+    a.sA = sA;
+    a.sph = sph;
+    a.sAn = sAn;
+    a.sout = sout;
+    a.nbp = nb;
+    grid.z = n_batch;
     cudaStream_t st = sb::as_stream(stream);
     ShKernel fk = (spc == 8 || spc == pl->n_lenses) ? fixed_kernel(a.p, a.cs, a.npx) : nullptr;
     if (fk) {
@@ -438,8 +467,7 @@ extern "C" int sb_sh_forward(const sb_sh_plan *pl, const float *A, const float *
         if (smem > 48 * 1024) {
             cudaError_t e = cudaFuncSetAttribute(sh_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  (int)smem);
-            if (e != cudaSuccess)
-                return sb::fail(SB_ECUDA, "sb_sh_forward: smem attribute: %s", cudaGetErrorString(e));
+            if (e != cudaSuccess) return sb::fail(SB_ECUDA, "%s: smem attribute: %s", who, cudaGetErrorString(e));
         }
         sh_forward_kernel<<<grid, 32 * spc, smem, st>>>(a);
     }
@@ -448,8 +476,29 @@ extern "C" int sb_sh_forward(const sb_sh_plan *pl, const float *A, const float *
     const int n_out = pl->n_lenses * pl->subap_npx * pl->n_lenses * pl->subap_npx;
     int nblk = (n_out + 255) / 256;
     nblk = nblk > 592 ? 592 : nblk;
-    sh_normalize_kernel<<<nblk, 256, 0, st>>>(a.part_I, a.part_A, nb, photon_scale, intensity, n_out);
+    sh_normalize_kernel<<<dim3(nblk, n_batch), 256, 0, st>>>(a.part_I, a.part_A, nb, photon_scale, intensity, n_out);
     return sb::check_launch("sh_normalize_kernel");
+}
+
+}  // namespace
+
+extern "C" int sb_sh_forward(const sb_sh_plan *pl, const float *A, const float *phase_nm, const float *A_norm,
+                             int n_norm, float photon_scale, float *intensity, void *scratch,
+                             size_t scratch_bytes, void *stream) {
+    sb::clear_error();
+    return sh_forward_impl("sb_sh_forward", pl, A, 0, phase_nm, 0, A_norm, 0, n_norm, photon_scale, intensity, 0, 1,
+                           scratch, scratch_bytes, stream);
+}
+
+extern "C" int sb_sh_forward_batched(const sb_sh_plan *pl, const float *A, long long A_stride, const float *phase_nm,
+                                     long long phase_stride, const float *A_norm, long long A_norm_stride, int n_norm,
+                                     float photon_scale, float *intensity, long long intensity_stride, int n_batch,
+                                     void *scratch, size_t scratch_bytes, void *stream) {
+    sb::clear_error();
+    if (pl && intensity_stride < (long long)pl->n_lenses * pl->subap_npx * pl->n_lenses * pl->subap_npx)
+        return sb::fail(SB_EINVAL, "sb_sh_forward_batched: intensity stride smaller than a frame");
+    return sh_forward_impl("sb_sh_forward_batched", pl, A, A_stride, phase_nm, phase_stride, A_norm, A_norm_stride,
+                           n_norm, photon_scale, intensity, intensity_stride, n_batch, scratch, scratch_bytes, stream);
 }
 
 extern "C" int sb_edge_extrapolate(const float *phase, const int32_t *src1, const int32_t *src2, int n_pixels,

@@ -67,6 +67,7 @@ class ScaoConfig:
     time_step: float = 0.001
     seed: int = 1234
     subap_threshold: float = 0.5           # valid sub-apertures: illumination above this fraction (< 0: all)
+    noise_seed: int = 1                    # detector seeds: photon noise_seed, read-out noise_seed + 1
 
     @property
     def pitch(self):
@@ -142,7 +143,7 @@ class ScaoLoop:
         side = c.n_lenses * c.subap_npx
         self.ccd = CCD(sp, size=[side, side], dt=c.time_step, bandw=1.0, photon_noise=c.photon_noise,
                        readout_noise=c.readout_noise > 0, readout_level=c.readout_noise, quantum_eff=1.0,
-                       target_device_idx=device_idx)
+                       photon_seed=c.noise_seed, readout_seed=c.noise_seed + 1, target_device_idx=device_idx)
         self.ccd.inputs['in_i'].set(self.sh.outputs['out_i'])
         idxs, dmap = valid_subaps(pupil, c.n_lenses, c.subap_npx, c.subap_threshold)
         self.subapdata = SubapData(idxs=idxs, display_map=dmap, nx=c.n_lenses, ny=c.n_lenses,
