@@ -53,6 +53,7 @@ def parse():
     p.add_argument('--no-gradient', action='store_true',
                    help='skip the checkpointed loop-gradient leg (1000 ELT steps, finite-difference check)')
     p.add_argument('--gradient-only', action='store_true', help='run only the loop-gradient leg (one GPU)')
+    p.add_argument('--no-batched', action='store_true', help='skip the batched Monte-Carlo leg')
     p.add_argument('--batched-only', action='store_true',
                    help='run only the 96-realisation batched Monte-Carlo leg (one GPU)')
     p.add_argument('--adjoint-only', action='store_true',
@@ -385,7 +386,9 @@ def bench_batched(dev, steps, cpu_budget_s):
            'batched_realisation_steps_per_s': n_real / (batched_ms / 1e3),
            'plain_realisation_steps_per_s': n_real / (plain_ms / 1e3),
            'speedup_batched_vs_plain': plain_ms / batched_ms, 'setup_s': setup_s,
-           'graph': 'one CUDA graph per step for all 96 realisations (chains over 16 streams, each group\'s batched launches on its own stream after its chains)'}
+           'graph': 'one CUDA graph per step for all 96 realisations: each geometry group on a stream of its own, '
+                    'one batched launch per stage (atmosphere, propagation, SH, CCD, slopes, reconstructor, '
+                    'integrator, mirror)'}
     if cpu_budget_s > 0:
         # the reference has no batched mode: the sum of per-realisation CPU runs,
         # sampled per geometry (steps/s of each size, weighted by its count)
@@ -550,6 +553,10 @@ def run_b200(args):
         adjoint_im = bench_adjoint_im(dev, reps=max(3, min(args.steps, 10)),
                                       cpu_budget_s=0 if args.no_cpu_baseline else 10.0)
 
+    batched_mc = None
+    if world == 1 and not args.no_batched:
+        batched_mc = bench_batched(dev, steps=50, cpu_budget_s=0 if args.no_cpu_baseline else 15.0)
+
     if rank == 0:
         line = {'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': steps,
                 'warmup': max(3, args.warmup), 'ms_per_step': ms_max / steps, 'higher_is_better': True,
@@ -570,7 +577,8 @@ def run_b200(args):
                 'step_roofline': {'algorithmic_bytes': step_bytes,
                                   'achieved_gbs': step_bytes / (ms_max / steps / 1e3) / 1e9,
                                   'frac': step_bytes / (ms_max / steps / 1e3) / 1e9 / peak},
-                'clocks': clk, 'cpu_baseline': cpu, 'adjoint_im': adjoint_im, 'loop_gradient': loop_grad}
+                'clocks': clk, 'cpu_baseline': cpu, 'adjoint_im': adjoint_im, 'loop_gradient': loop_grad,
+                'batched_mc': batched_mc}
         print(json.dumps(line), flush=True)
     del loop
     if world > 1:
