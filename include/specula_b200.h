@@ -108,6 +108,25 @@ int sb_sh_forward_batched(const sb_sh_plan *plan, const float *A, long long A_st
                           float photon_scale, float *intensity, long long intensity_stride, int n_batch,
                           void *scratch, size_t scratch_bytes, void *stream);
 
+/* Split-BF16 tensor-core form of sb_sh_forward / sb_sh_forward_batched (same
+ * arguments, scratch and outputs; the reference computes the same quantity
+ * in sh.py:348-428 with complex64 FFTs).  Both small DFT products run on
+ * the tcgen05 tensor cores with every operand split into bf16 hi + lo parts
+ * and hi*hi + lo*hi + hi*lo accumulated in FP32 (relative error of order
+ * 1e-5 of the field, against about 1e-7 for the FP32 form).  Geometries:
+ * np_sub 8 with (cutsize, subap_npx) in (12,6) (8,8) (12,8) (14,8) (16,8);
+ * others return SB_EUNSUPPORTED.  A timed-out wait on the tensor cores is
+ * reported by sb_device_status. */
+int sb_sh_split_bf16_supported(const sb_sh_plan *plan);
+int sb_sh_forward_split_bf16(const sb_sh_plan *plan, const float *A, const float *phase_nm,
+                             const float *A_norm, int n_norm, float photon_scale, float *intensity,
+                             void *scratch, size_t scratch_bytes, void *stream);
+int sb_sh_forward_split_bf16_batched(const sb_sh_plan *plan, const float *A, long long A_stride,
+                                     const float *phase_nm, long long phase_stride, const float *A_norm,
+                                     long long A_norm_stride, int n_norm, float photon_scale, float *intensity,
+                                     long long intensity_stride, int n_batch, void *scratch,
+                                     size_t scratch_bytes, void *stream);
+
 /* replaces specula/lib/extrapolate_edge_pixel.py:4-28.
  * out[p] = phase[p] if src1[p] < 0; phase[src1[p]] if src2[p] < 0;
  * else 2*phase[src1[p]] - phase[src2[p]].  Tables from the host restatement
@@ -270,7 +289,8 @@ int sb_modalrec_batched(const float *R, int n_modes, int n_slopes, int ldr, cons
                         int n_batch, float *modes, int ldm, void *stream);
 
 /* Diagnostics: SB_OK, or SB_ETIMEOUT when a bounded wait inside a kernel
- * (the shared-memory pipeline of sb_dm_project) gave up since the last call;
+ * (the shared-memory pipeline of sb_dm_project, the tensor-core waits of
+ * sb_sh_forward_split_bf16) gave up since the last call;
  * reading clears it.  Synchronous (waits for the device); not for the step. */
 int sb_device_status(void);
 

@@ -91,6 +91,11 @@ SIGNATURES = {
                                        C.c_int, fp, fp, C.c_longlong, vp]),
     'sb_sh_forward_batched': (C.c_int, [C.POINTER(ShPlan), fp, C.c_longlong, fp, C.c_longlong, fp, C.c_longlong,
                                         C.c_int, C.c_float, fp, C.c_longlong, C.c_int, vp, C.c_size_t, vp]),
+    'sb_sh_split_bf16_supported': (C.c_int, [C.POINTER(ShPlan)]),
+    'sb_sh_forward_split_bf16': (C.c_int, [C.POINTER(ShPlan), fp, fp, fp, C.c_int, C.c_float, fp, vp, C.c_size_t, vp]),
+    'sb_sh_forward_split_bf16_batched': (C.c_int, [C.POINTER(ShPlan), fp, C.c_longlong, fp, C.c_longlong, fp,
+                                                   C.c_longlong, C.c_int, C.c_float, fp, C.c_longlong, C.c_int, vp,
+                                                   C.c_size_t, vp]),
     'sb_ccd_step_batched': (C.c_int, [C.POINTER(CcdParams), vp, vp, C.c_int, fp, fp, fp, vp]),
     'sb_slopec_batched': (C.c_int, [C.POINTER(SlopecPlan), fp, C.c_longlong, fp, C.c_int, fp, C.c_int, C.c_int, vp,
                                     C.c_size_t, vp]),

@@ -14,6 +14,8 @@ namespace sb {
 // Record a failure message for sb_last_error() and return the status.
 int fail(int status, const char *fmt, ...);
 void clear_error();
+// read and clear the timeout flag of the tensor-core SH kernels (0: none, <0: query failed)
+int sh_tc_status_take();
 
 // Check the launch that just happened on this thread.
 inline int check_launch(const char *what) {

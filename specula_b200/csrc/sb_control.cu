@@ -473,7 +473,10 @@ extern "C" int sb_device_status(void) {
     int v = 0;
     if (cudaMemcpyFromSymbol(&v, g_dm_status, sizeof(int)) != cudaSuccess)
         return sb::fail(SB_ECUDA, "sb_device_status: %s", cudaGetErrorString(cudaGetLastError()));
-    if (v == 0) return SB_OK;
+    const int sh = sb::sh_tc_status_take();
+    if (sh < 0) return sb::fail(SB_ECUDA, "sb_device_status: %s", cudaGetErrorString(cudaGetLastError()));
+    if (v == 0 && sh == 0) return SB_OK;
+    if (v == 0) return sb::fail(SB_ETIMEOUT, "a tensor-core SH wait timed out (stage %d)", sh);
     const int zero = 0;
     cudaMemcpyToSymbol(g_dm_status, &zero, sizeof(int));
     return sb::fail(SB_ETIMEOUT, "a DM projection wait timed out (%s side)", v == 1 ? "producer" : "consumer");

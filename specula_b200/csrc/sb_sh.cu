@@ -14,6 +14,7 @@
 // the photon normalisation of sh.py:425-427 in a fixed (deterministic) order.
 #include "sb_common.cuh"
 #include "sb_dft.cuh"
+#include "sb_umma.cuh"
 
 namespace {
 
@@ -324,7 +325,321 @@ __global__ void __launch_bounds__(256, 4) sh_forward_fixed_kernel(ShArgs a) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Split-BF16 tensor-core form (tcgen05).  One CTA of 128 threads takes 16
+// consecutive sub-apertures of a lenslet row and runs both DFT products as
+// real GEMMs on the tensor cores, every operand split as x = hi + lo (bf16)
+// and each product as hi*hi + lo*hi + hi*lo: three K=16 MMAs, FP32
+// accumulation in tensor memory.
+//   stage 1  rows (sub-aperture s, field row r): 16 x 8 = 128
+//            K    [Re E[r][c], Im E[r][c]]  (c < 8)
+//            N    [Re G[r][b], Im G[r][b]]  (b < cutsize, padded to 16/32)
+//   stage 2  rows (s, kept column b): two tiles of 8 sub-apertures x 16
+//            K    [Re G[r][b], Im G[r][b]]  (r < 8)
+//            N    [Re F[a][b], Im F[a][b]]  (a < cutsize)
+// Both stages multiply by the same B, the real form of the pruned DFT rows
+// W[b][c].  Between the stages G goes from tensor memory to shared memory
+// in FP32 (transposed to column-major per sub-aperture) and is split again.
+// The field build, |F|^2, the field stop, the rebin and the photon
+// partials run on the CUDA cores as in the FP32 form.
+// ---------------------------------------------------------------------------
+
+constexpr int kTcSub = 16;              // sub-apertures per CTA
+constexpr int kTcThreads = 128;         // one thread per MMA row
+constexpr uint32_t kTcTmemCols = 64;    // stage 1 in columns 0-31, then stage 2 tiles in 0-31 and 32-63
+constexpr int kTcOperandBytes = 128 * 32;   // one 128-row x 16 bf16 operand
+
+__device__ int g_sh_tc_status = 0;      // nonzero: a bounded wait on the tensor cores timed out
+
+template <int CS>
+struct TcShape {
+    static constexpr int NB = 2 * CS <= 16 ? 16 : 32;   // MMA N
+    static constexpr int GS = CS * 8 + 8;                // float2 per sub-aperture in the G buffer (bank offset)
+};
+
+// Dynamic shared memory per CTA: the operands and tables, and at least
+// 52 KB, which bounds any operand read that the descriptors can express
+// (8-row groups and K segments at the larger of the two strides) inside the
+// allocation; it also caps residency at 4 CTAs (256 tensor-memory columns)
+// per SM.
+constexpr size_t kTcSmemFloor = 52 * 1024;
+template <int P, int CS, int NPX>
+__host__ __device__ constexpr size_t tc_smem_bytes() {
+    const size_t used = 6 * (size_t)kTcOperandBytes + 2 * (size_t)TcShape<CS>::NB * 32 +
+                        (size_t)kTcSub * TcShape<CS>::GS * 8 + (size_t)P * P * 8 + (size_t)CS * CS * 4 +
+                        (size_t)NPX * CS * 4 + 8 + 16;
+    return used > kTcSmemFloor ? used : kTcSmemFloor;
+}
+
+template <int P, int CS, int NPX>
+__global__ void __launch_bounds__(kTcThreads) sh_forward_tc_kernel(ShArgs a) {
+    static_assert(P == 8, "one 16-byte K segment per field row");
+    static_assert(CS <= 16, "one 16-row stage-2 block per sub-aperture");
+    static_assert(kTcSub * CS * CS <= kTcSub * TcShape<CS>::GS * 2, "intensity buffer aliases the G buffer");
+    constexpr int NB = TcShape<CS>::NB;
+    constexpr int GS = TcShape<CS>::GS;
+    constexpr uint32_t IDESC = sb::umma_idesc_bf16_f32(128, NB);
+    constexpr uint32_t LBO_A = 128 * 16, LBO_B = NB * 16;
+    batch_slice(a);
+    extern __shared__ __align__(128) unsigned char smem[];
+    unsigned char *A1h = smem, *A1l = smem + kTcOperandBytes;
+    unsigned char *A2h = smem + 2 * kTcOperandBytes;   // two tiles
+    unsigned char *A2l = smem + 4 * kTcOperandBytes;   // two tiles
+    unsigned char *Bh = smem + 6 * kTcOperandBytes, *Bl = Bh + NB * 32;
+    float2 *Gb = reinterpret_cast<float2 *>(Bl + NB * 32);
+    float *Ib = reinterpret_cast<float *>(Gb);        // |F|^2 after G is consumed
+    float2 *tilt = Gb + kTcSub * GS;
+    float *mask = reinterpret_cast<float *>(tilt + P * P);
+    float *R = mask + CS * CS;
+    uint64_t *bar = reinterpret_cast<uint64_t *>((reinterpret_cast<uintptr_t>(R + NPX * CS) + 7) & ~(uintptr_t)7);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar + 1);
+    __shared__ float red[33];
+
+    const int t = threadIdx.x, warp = t >> 5;
+    if (warp == 0) {
+        sb::tmem_alloc(tmem_slot, kTcTmemCols);
+        sb::tmem_relinquish();
+    }
+    if (t == 0) {
+        sb::mbar_init(bar, 1);
+        sb::mbar_init_fence();
+    }
+    for (int e = t; e < P * P; e += kTcThreads) tilt[e] = a.tilt[e];
+    for (int e = t; e < CS * CS; e += kTcThreads) mask[e] = a.mask[e];
+    for (int e = t; e < NPX * CS; e += kTcThreads) R[e] = a.rebin[e];
+    // B: real form of W.  Row n < CS gives Re of output b = n, row CS + b its
+    // Im; K segment 0 multiplies the real parts, segment 1 the imaginary ones.
+    for (int e = t; e < NB * 2; e += kTcThreads) {
+        const int n = e >> 1, seg = e & 1;
+        float x[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            float v = 0.f;
+            if (n < 2 * CS) {
+                const float2 w = a.tw[(n < CS ? n : n - CS) * P + c];
+                v = n < CS ? (seg == 0 ? w.x : -w.y) : (seg == 0 ? w.y : w.x);
+            }
+            x[c] = v;
+        }
+        uint4 h, l;
+        sb::split_bf16x8(x, h, l);
+        *reinterpret_cast<uint4 *>(Bh + seg * LBO_B + n * 16) = h;
+        *reinterpret_cast<uint4 *>(Bl + seg * LBO_B + n * 16) = l;
+    }
+    if constexpr (CS < 16) {
+        // stage-2 rows b >= cutsize of every sub-aperture block stay zero
+        const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+        for (int e = t; e < kTcSub * (16 - CS); e += kTcThreads) {
+            const int s2 = e / (16 - CS), b = CS + e % (16 - CS);
+            const int off = (s2 >> 3) * kTcOperandBytes + ((s2 & 7) * 16 + b) * 16;
+            *reinterpret_cast<uint4 *>(A2h + off) = z;
+            *reinterpret_cast<uint4 *>(A2h + off + LBO_A) = z;
+            *reinterpret_cast<uint4 *>(A2l + off) = z;
+            *reinterpret_cast<uint4 *>(A2l + off + LBO_A) = z;
+        }
+    }
+    __syncthreads();
+
+    // field build (electric_field.py:60-75 and sh.py:376): thread t holds row r of sub-aperture s
+    const int i = blockIdx.y;
+    const int s = t >> 3, r = t & 7;
+    const int j = blockIdx.x * kTcSub + s;
+    {
+        float er[8], ei[8];
+        if (j < a.n) {
+            const size_t g = (size_t)(i * P + r) * a.ld + (size_t)j * P;
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                const float amp = a.A[g + c];
+                const float phi = a.ph[g + c] * a.k;
+                float sn, co;
+                sincosf(phi, &sn, &co);
+                const float re = co * amp, im = sn * amp;
+                const float2 tl = tilt[r * P + c];
+                er[c] = re * tl.x - im * tl.y;
+                ei[c] = re * tl.y + im * tl.x;
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < 8; ++c) er[c] = ei[c] = 0.f;
+        }
+        uint4 h, l;
+        sb::split_bf16x8(er, h, l);
+        *reinterpret_cast<uint4 *>(A1h + t * 16) = h;
+        *reinterpret_cast<uint4 *>(A1l + t * 16) = l;
+        sb::split_bf16x8(ei, h, l);
+        *reinterpret_cast<uint4 *>(A1h + LBO_A + t * 16) = h;
+        *reinterpret_cast<uint4 *>(A1l + LBO_A + t * 16) = l;
+    }
+    sb::fence_proxy_async_smem();
+    sb::tc_fence_before_sync();
+    __syncthreads();
+    sb::tc_fence_after_sync();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+    const uint64_t bh = sb::umma_desc_kmajor(Bh, LBO_B), bl = sb::umma_desc_kmajor(Bl, LBO_B);
+
+    // stage 1: G = E W^T
+    if (t == 0) {
+        const uint64_t ah = sb::umma_desc_kmajor(A1h, LBO_A), al = sb::umma_desc_kmajor(A1l, LBO_A);
+        sb::umma_bf16(tmem, ah, bh, IDESC, 0u);
+        sb::umma_bf16(tmem, al, bh, IDESC, 1u);
+        sb::umma_bf16(tmem, ah, bl, IDESC, 1u);
+        sb::umma_commit(bar);
+    }
+    int pending = 0;                    // parity of the commit still to be waited for after a timeout
+    int failed = __syncthreads_or(!sb::mbar_wait(bar, 0));
+    float local = 0.f;
+    if (!failed) {
+        sb::tc_fence_after_sync();
+        uint32_t v[2][16];
+        sb::tmem_ld16(tmem + lane_base, v[0]);
+        if constexpr (NB == 32) sb::tmem_ld16(tmem + lane_base + 16, v[1]);
+        sb::tmem_wait_ld(v[0]);
+        if constexpr (NB == 32) sb::tmem_wait_ld(v[1]);
+#pragma unroll
+        for (int b = 0; b < CS; ++b) {
+            const int nr = b, ni = CS + b;
+            Gb[s * GS + b * 8 + r] = make_float2(__uint_as_float(v[nr >> 4][nr & 15]),
+                                                 __uint_as_float(v[ni >> 4][ni & 15]));
+        }
+        sb::tc_fence_before_sync();
+        __syncthreads();
+        // stage-2 operand rows (s2, b): column b of G_s2, split
+        for (int e = t; e < kTcSub * CS; e += kTcThreads) {
+            const int s2 = e / CS, b = e - s2 * CS;
+            const float4 *g = reinterpret_cast<const float4 *>(Gb + s2 * GS + b * 8);
+            float gr[8], gi[8];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float4 x = g[q];
+                gr[2 * q] = x.x;
+                gi[2 * q] = x.y;
+                gr[2 * q + 1] = x.z;
+                gi[2 * q + 1] = x.w;
+            }
+            const int off = (s2 >> 3) * kTcOperandBytes + ((s2 & 7) * 16 + b) * 16;
+            uint4 h, l;
+            sb::split_bf16x8(gr, h, l);
+            *reinterpret_cast<uint4 *>(A2h + off) = h;
+            *reinterpret_cast<uint4 *>(A2l + off) = l;
+            sb::split_bf16x8(gi, h, l);
+            *reinterpret_cast<uint4 *>(A2h + off + LBO_A) = h;
+            *reinterpret_cast<uint4 *>(A2l + off + LBO_A) = l;
+        }
+        sb::fence_proxy_async_smem();
+        __syncthreads();
+        sb::tc_fence_after_sync();
+        // stage 2: F^T = G^T W^T per sub-aperture, tile k into columns 32k..32k+31
+        if (t == 0) {
+#pragma unroll
+            for (int tile = 0; tile < 2; ++tile) {
+                const uint64_t ah = sb::umma_desc_kmajor(A2h + tile * kTcOperandBytes, LBO_A);
+                const uint64_t al = sb::umma_desc_kmajor(A2l + tile * kTcOperandBytes, LBO_A);
+                const uint32_t d = tmem + 32u * tile;
+                sb::umma_bf16(d, ah, bh, IDESC, 0u);
+                sb::umma_bf16(d, al, bh, IDESC, 1u);
+                sb::umma_bf16(d, ah, bl, IDESC, 1u);
+            }
+            sb::umma_commit(bar);
+        }
+        failed = __syncthreads_or(!sb::mbar_wait(bar, 1));
+        pending = 1;
+        if (!failed) {
+            sb::tc_fence_after_sync();
+            // |F|^2 and the field stop (sh.py:378-399): thread t holds column b of sub-aperture s2
+#pragma unroll
+            for (int tile = 0; tile < 2; ++tile) {
+                uint32_t w[2][16];
+                sb::tmem_ld16(tmem + lane_base + 32u * tile, w[0]);
+                if constexpr (NB == 32) sb::tmem_ld16(tmem + lane_base + 32u * tile + 16, w[1]);
+                sb::tmem_wait_ld(w[0]);
+                if constexpr (NB == 32) sb::tmem_wait_ld(w[1]);
+                const int s2 = tile * 8 + (t >> 4), b = t & 15;
+                if (b < CS) {
+#pragma unroll
+                    for (int aa = 0; aa < CS; ++aa) {
+                        const int nr = aa, ni = CS + aa;
+                        const float fr = __uint_as_float(w[nr >> 4][nr & 15]);
+                        const float fi = __uint_as_float(w[ni >> 4][ni & 15]);
+                        Ib[s2 * CS * CS + aa * CS + b] = (fr * fr + fi * fi) * mask[aa * CS + b];
+                    }
+                }
+            }
+            __syncthreads();
+            // rebin (toccd.py:55-61) and output; consecutive threads write consecutive pixels of a detector row
+            const int out_ld = a.n * NPX;
+            for (int e = t; e < NPX * kTcSub * NPX; e += kTcThreads) {
+                const int pp = e / (kTcSub * NPX), rem = e - pp * (kTcSub * NPX);
+                const int s2 = rem / NPX, q = rem - s2 * NPX;
+                const int j2 = blockIdx.x * kTcSub + s2;
+                if (j2 >= a.n) continue;
+                const float *I = Ib + s2 * CS * CS;
+                float acc = 0.f;
+                if constexpr (CS % NPX == 0) {
+                    constexpr int BF = CS / NPX;
+#pragma unroll
+                    for (int u = 0; u < BF; ++u)
+#pragma unroll
+                        for (int vv = 0; vv < BF; ++vv) acc += I[(pp * BF + u) * CS + q * BF + vv];
+                    acc *= R[0] * R[0];
+                } else {
+#pragma unroll
+                    for (int aa = 0; aa < CS; ++aa) {
+                        float h = 0.f;
+#pragma unroll
+                        for (int b = 0; b < CS; ++b) h = fmaf(I[aa * CS + b], R[q * CS + b], h);
+                        acc = fmaf(R[pp * CS + aa], h, acc);
+                    }
+                }
+                a.out[((size_t)i * NPX + pp) * out_ld + (size_t)j2 * NPX + q] = acc;
+                local += acc;
+            }
+        }
+    }
+    if (failed) {
+        // record, then give the MMAs in flight one more bounded wait before the
+        // tensor memory is released; the frame of this launch is not valid
+        if (t == 0) atomicExch(&g_sh_tc_status, 1 + pending);
+        sb::mbar_wait(bar, pending);
+    }
+    const int bid = blockIdx.y * gridDim.x + blockIdx.x;
+    const float tot = sb::block_sum(local, red);
+    const int nblk = gridDim.x * gridDim.y;
+    const int chunk = (a.n_norm + nblk - 1) / nblk;
+    const int lo = bid * chunk;
+    const int hi = min(a.n_norm, lo + chunk);
+    float sa = 0.f;
+    for (int e = lo + t; e < hi; e += kTcThreads) sa += a.A_norm[e];
+    const float tota = sb::block_sum(sa, red);
+    if (t == 0) {
+        a.part_I[bid] = tot;
+        a.part_A[bid] = tota;
+    }
+    sb::tc_fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        sb::tc_fence_after_sync();
+        sb::tmem_dealloc(tmem, kTcTmemCols);
+    }
+}
+
 typedef void (*ShKernel)(ShArgs);
+
+struct ShTcKernel {
+    ShKernel fn;
+    size_t smem;
+};
+
+// geometries with a split-BF16 tensor-core kernel: (np_sub, cutsize, subap_npx)
+ShTcKernel tc_kernel(int p, int cs, int npx) {
+    if (p == 8 && cs == 12 && npx == 6) return {sh_forward_tc_kernel<8, 12, 6>, tc_smem_bytes<8, 12, 6>()};
+    if (p == 8 && cs == 14 && npx == 8) return {sh_forward_tc_kernel<8, 14, 8>, tc_smem_bytes<8, 14, 8>()};
+    if (p == 8 && cs == 16 && npx == 8) return {sh_forward_tc_kernel<8, 16, 8>, tc_smem_bytes<8, 16, 8>()};
+    if (p == 8 && cs == 8 && npx == 8) return {sh_forward_tc_kernel<8, 8, 8>, tc_smem_bytes<8, 8, 8>()};
+    if (p == 8 && cs == 12 && npx == 8) return {sh_forward_tc_kernel<8, 12, 8>, tc_smem_bytes<8, 12, 8>()};
+    return {nullptr, 0};
+}
 
 // geometries with a compile-time kernel: (np_sub, cutsize, subap_npx)
 ShKernel fixed_kernel(int p, int cs, int npx) {
@@ -414,9 +729,11 @@ extern "C" size_t sb_sh_scratch_bytes(const sb_sh_plan *pl) {
 
 namespace {
 
+// mode 0: FP32 CUDA-core DFTs; mode 1: split-BF16 tensor-core DFTs
 int sh_forward_impl(const char *who, const sb_sh_plan *pl, const float *A, long long sA, const float *phase_nm,
                     long long sph, const float *A_norm, long long sAn, int n_norm, float photon_scale,
-                    float *intensity, long long sout, int n_batch, void *scratch, size_t scratch_bytes, void *stream) {
+                    float *intensity, long long sout, int n_batch, void *scratch, size_t scratch_bytes, void *stream,
+                    int mode = 0) {
     if (!pl || !A || !phase_nm || !A_norm || !intensity || !pl->twiddle || !pl->tilt || !pl->fp_mask ||
         !pl->rebin)
         return sb::fail(SB_EINVAL, "%s: null pointer", who);
@@ -432,6 +749,15 @@ int sh_forward_impl(const char *who, const sb_sh_plan *pl, const float *A, long 
     const size_t need = sb_sh_scratch_bytes(pl) * (size_t)n_batch;
     if (!scratch || scratch_bytes < need)
         return sb::fail(SB_ESCRATCH, "%s: scratch needs %zu bytes, got %zu", who, need, scratch_bytes);
+    ShTcKernel tk = {nullptr, 0};
+    if (mode == 1) {
+        tk = tc_kernel(pl->np_sub, pl->cutsize, pl->subap_npx);
+        if (!tk.fn)
+            return sb::fail(SB_EUNSUPPORTED, "%s: no split-BF16 kernel for (np=%d, cut=%d, npx=%d)", who, pl->np_sub,
+                            pl->cutsize, pl->subap_npx);
+        // 16 sub-apertures per CTA (never more CTAs than the FP32 grid, so the scratch size holds)
+        grid = dim3((pl->n_lenses + kTcSub - 1) / kTcSub, pl->n_lenses, 1);
+    }
     const int nb = grid.x * grid.y;
     ShArgs a = {};
     a.n = pl->n_lenses;
@@ -461,7 +787,13 @@ int sh_forward_impl(const char *who, const sb_sh_plan *pl, const float *A, long 
     grid.z = n_batch;
     cudaStream_t st = sb::as_stream(stream);
     ShKernel fk = (spc == 8 || spc == pl->n_lenses) ? fixed_kernel(a.p, a.cs, a.npx) : nullptr;
-    if (fk) {
+    if (tk.fn) {
+        if (tk.smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(tk.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tk.smem);
+            if (e != cudaSuccess) return sb::fail(SB_ECUDA, "%s: smem attribute: %s", who, cudaGetErrorString(e));
+        }
+        tk.fn<<<grid, kTcThreads, tk.smem, st>>>(a);
+    } else if (fk) {
         fk<<<grid, 32 * spc, 0, st>>>(a);
     } else {
         if (smem > 48 * 1024) {
@@ -500,6 +832,44 @@ extern "C" int sb_sh_forward_batched(const sb_sh_plan *pl, const float *A, long 
     return sh_forward_impl("sb_sh_forward_batched", pl, A, A_stride, phase_nm, phase_stride, A_norm, A_norm_stride,
                            n_norm, photon_scale, intensity, intensity_stride, n_batch, scratch, scratch_bytes, stream);
 }
+
+extern "C" int sb_sh_split_bf16_supported(const sb_sh_plan *pl) {
+    return (pl && tc_kernel(pl->np_sub, pl->cutsize, pl->subap_npx).fn) ? 1 : 0;
+}
+
+extern "C" int sb_sh_forward_split_bf16(const sb_sh_plan *pl, const float *A, const float *phase_nm,
+                                        const float *A_norm, int n_norm, float photon_scale, float *intensity,
+                                        void *scratch, size_t scratch_bytes, void *stream) {
+    sb::clear_error();
+    return sh_forward_impl("sb_sh_forward_split_bf16", pl, A, 0, phase_nm, 0, A_norm, 0, n_norm, photon_scale,
+                           intensity, 0, 1, scratch, scratch_bytes, stream, 1);
+}
+
+extern "C" int sb_sh_forward_split_bf16_batched(const sb_sh_plan *pl, const float *A, long long A_stride,
+                                                const float *phase_nm, long long phase_stride, const float *A_norm,
+                                                long long A_norm_stride, int n_norm, float photon_scale,
+                                                float *intensity, long long intensity_stride, int n_batch,
+                                                void *scratch, size_t scratch_bytes, void *stream) {
+    sb::clear_error();
+    if (pl && intensity_stride < (long long)pl->n_lenses * pl->subap_npx * pl->n_lenses * pl->subap_npx)
+        return sb::fail(SB_EINVAL, "sb_sh_forward_split_bf16_batched: intensity stride smaller than a frame");
+    return sh_forward_impl("sb_sh_forward_split_bf16_batched", pl, A, A_stride, phase_nm, phase_stride, A_norm,
+                           A_norm_stride, n_norm, photon_scale, intensity, intensity_stride, n_batch, scratch,
+                           scratch_bytes, stream, 1);
+}
+
+namespace sb {
+// read and clear the tensor-core SH timeout flag (0: none)
+int sh_tc_status_take() {
+    int v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_sh_tc_status, sizeof(int)) != cudaSuccess) return -1;
+    if (v) {
+        const int zero = 0;
+        cudaMemcpyToSymbol(g_sh_tc_status, &zero, sizeof(int));
+    }
+    return v;
+}
+}  // namespace sb
 
 extern "C" int sb_edge_extrapolate(const float *phase, const int32_t *src1, const int32_t *src2, int n_pixels,
                                    float *out, void *stream) {

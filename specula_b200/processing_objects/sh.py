@@ -9,6 +9,11 @@ build_stream).  ``trigger_code()`` makes one C-ABI call, sb_sh_forward
 (preceded by sb_edge_extrapolate + sb_interp2d_field when the geometry
 oversamples the field), which also applies the photon normalisation of
 sh.py:422-428 on the device.
+
+``dft='split_bf16'`` (an addition; the reference has one FFT path) runs the
+two small DFT products on the tcgen05 tensor cores in split-BF16
+(sb_sh_forward_split_bf16); geometries without such a kernel raise
+ValueError at setup.
 """
 import math
 
@@ -46,8 +51,12 @@ class SH(BaseProcessingObj):
                  set_fov_res_to_turbpxsc: bool = False,
                  laser_launch_tel=None,
                  target_device_idx: int = None,
-                 precision: int = None):
+                 precision: int = None,
+                 dft: str = 'fp32'):
         super().__init__(target_device_idx=target_device_idx, precision=precision)
+        if dft not in ('fp32', 'split_bf16'):
+            raise ValueError(f"SH: dft must be 'fp32' or 'split_bf16', not {dft!r}")
+        self._dft = dft
         if laser_launch_tel is not None:
             raise NotImplementedError('SH: the LGS convolution-kernel branch (sh.py:382-394) is not on this path')
         self._wavelengthInNm = wavelengthInNm
@@ -130,6 +139,10 @@ class SH(BaseProcessingObj):
         nbytes = _lib.load().sb_sh_scratch_bytes(self._plan)
         if nbytes == 0:
             raise ValueError('SH: geometry does not fit the kernel limits')
+        if self._dft == 'split_bf16' and not _lib.load().sb_sh_split_bf16_supported(self._plan):
+            raise ValueError(f'SH: no split-BF16 tensor-core kernel for np_sub={p}, cutsize={g.cutsize}, '
+                             f'subap_npx={g.subap_npx}')
+        self._forward = 'sb_sh_forward' if self._dft == 'fp32' else 'sb_sh_forward_split_bf16'
         self._scratch = torch.empty(nbytes, dtype=torch.uint8, device=dev)
         self._in_ef = in_ef
         if g.do_interpolation:
@@ -165,7 +178,7 @@ class SH(BaseProcessingObj):
             A, P = self._wf1_A, self._wf1_phase
         else:
             A, P = ef.A, ef.phaseInNm
-        _lib.call('sb_sh_forward', C_plan(self._plan), A.data_ptr(), P.data_ptr(), ef.A.data_ptr(), ef.A.numel(),
+        _lib.call(self._forward, C_plan(self._plan), A.data_ptr(), P.data_ptr(), ef.A.data_ptr(), ef.A.numel(),
                   self._photon_scale, self._out_i.i.data_ptr(), self._scratch.data_ptr(), self._scratch.numel(), st)
 
     def prepare_trigger(self, t):
