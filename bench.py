@@ -374,7 +374,20 @@ def bench_batched(dev, steps, cpu_budget_s):
         return e0.elapsed_time(e1) / n
 
     plain_ms = timed(sys_b.replay_plain, steps)
+    untuned_ms = timed(sys_b.replay, steps)
+    # tile shapes from the autotuner (timed on each group's own buffers), graph captured again
+    from specula_b200.autotune import Autotuner
+    tuner = Autotuner(dev)
+    t_tune = time.perf_counter()
+    sys_b.autotune(tuner)
+    sys_b.capture()
     batched_ms = timed(sys_b.replay, steps)
+    # the same batched graph with the split-BF16 tensor-core SH
+    sys_b.set_dft('split_bf16')
+    sys_b.autotune(tuner)
+    sys_b.capture()
+    tune_s = time.perf_counter() - t_tune
+    bf16_ms = timed(sys_b.replay, steps)
     _lib_status()
     by_size = {}
     for (tmpl, reals) in groups:
@@ -382,10 +395,17 @@ def bench_batched(dev, steps, cpu_budget_s):
         by_size[key] = by_size.get(key, 0) + len(reals)
     out = {'workload': 'mc96_20x20_40x40_74x74_2wavelengths', 'realisations': n_real, 'split': by_size,
            'groups': len(groups), 'steps_timed': steps,
-           'batched_ms_per_step': batched_ms, 'plain_ms_per_step': plain_ms,
+           'batched_ms_per_step': batched_ms, 'batched_untuned_ms_per_step': untuned_ms,
+           'plain_ms_per_step': plain_ms,
            'batched_realisation_steps_per_s': n_real / (batched_ms / 1e3),
            'plain_realisation_steps_per_s': n_real / (plain_ms / 1e3),
-           'speedup_batched_vs_plain': plain_ms / batched_ms, 'setup_s': setup_s,
+           'speedup_batched_vs_plain': plain_ms / batched_ms,
+           'batched_split_bf16_ms_per_step': bf16_ms,
+           'batched_split_bf16_realisation_steps_per_s': n_real / (bf16_ms / 1e3),
+           'speedup_batched_split_bf16_vs_plain': plain_ms / bf16_ms, 'setup_s': setup_s,
+           'autotune_s': tune_s,
+           'autotune': [{k: r[k] for k in ('family', 'shape', 'variant', 'name', 'times_us', 'speedup_vs_variant0',
+                                           'cached')} for r in tuner.results],
            'graph': 'one CUDA graph per step for all 96 realisations: each geometry group on a stream of its own, '
                     'one batched launch per stage (atmosphere, propagation, SH, CCD, slopes, reconstructor, '
                     'integrator, mirror)'}
@@ -403,6 +423,57 @@ def bench_batched(dev, steps, cpu_budget_s):
         out['cpu_baseline'] = {'value': n_real / total_s, 'unit': 'realisation-steps/s', 'cores': blas_threads(),
                                'kind': 'port', 'sample': 'CPU-oracle steps of one realisation per geometry, '
                                'weighted by the realisation counts: ' + json.dumps({k: round(v, 3) for k, v in per.items()})}
+    return out
+
+
+def bench_sh_forms(dev, reps=200):
+    """Device time of one SH forward (FP32 CUDA-core DFTs against split-BF16
+    tensor-core DFTs) on the 80x80 ELT field and on a batch of 7 fields of
+    74x74 sub-apertures, CUDA events over `reps` launches after warm-up."""
+    import ctypes
+    import torch
+    from specula_b200 import _lib
+    from specula_b200.scao import ScaoLoop, elt_config
+    from specula_b200.batched import mc_groups
+    out = {}
+    cfgs = [('elt_80x80_640px', elt_config(), 1), ('mc_74x74_592px_x7', mc_groups()[-1][0], 7)]
+    for name, cfg, nb in cfgs:
+        loop = ScaoLoop(cfg, device_idx=dev.index)
+        loop.start()
+        loop.step_eager()
+        sh = loop.sh
+        ef = sh._in_ef
+        L2 = ef.A.numel()
+        side = cfg.n_lenses * cfg.subap_npx
+        A = ef.A.reshape(1, -1).repeat(nb, 1).contiguous()
+        P = ef.phaseInNm.reshape(1, -1).repeat(nb, 1).contiguous()
+        I = torch.empty((nb, side * side), device=dev)
+        scratch = torch.zeros(nb * _lib.load().sb_sh_scratch_bytes(ctypes.byref(sh._plan)), dtype=torch.uint8,
+                              device=dev)
+        st = torch.cuda.current_stream(dev)
+        res = {}
+        for form, fn in (('fp32', 'sb_sh_forward_batched'), ('split_bf16', 'sb_sh_forward_split_bf16_batched')):
+            def call():
+                _lib.call(fn, ctypes.byref(sh._plan), A.data_ptr(), L2, P.data_ptr(), L2, A.data_ptr(), L2, L2,
+                          sh._photon_scale, I.data_ptr(), side * side, nb, scratch.data_ptr(), scratch.numel(),
+                          st.cuda_stream)
+            for _ in range(5):
+                call()
+            torch.cuda.synchronize(dev)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(reps):
+                call()
+            e1.record(st)
+            torch.cuda.synchronize(dev)
+            res[form + '_us'] = e0.elapsed_time(e1) / reps * 1e3
+        res['speedup_split_bf16_vs_fp32'] = res['fp32_us'] / res['split_bf16_us']
+        res['fields'] = nb
+        res['sub_apertures_per_field'] = cfg.n_lenses ** 2
+        out[name] = res
+        del loop
+    _lib_status()
     return out
 
 
@@ -553,6 +624,10 @@ def run_b200(args):
         adjoint_im = bench_adjoint_im(dev, reps=max(3, min(args.steps, 10)),
                                       cpu_budget_s=0 if args.no_cpu_baseline else 10.0)
 
+    sh_forms = None
+    if world == 1 and not args.no_batched:
+        sh_forms = bench_sh_forms(dev)
+
     batched_mc = None
     if world == 1 and not args.no_batched:
         batched_mc = bench_batched(dev, steps=50, cpu_budget_s=0 if args.no_cpu_baseline else 15.0)
@@ -578,7 +653,7 @@ def run_b200(args):
                                   'achieved_gbs': step_bytes / (ms_max / steps / 1e3) / 1e9,
                                   'frac': step_bytes / (ms_max / steps / 1e3) / 1e9 / peak},
                 'clocks': clk, 'cpu_baseline': cpu, 'adjoint_im': adjoint_im, 'loop_gradient': loop_grad,
-                'batched_mc': batched_mc}
+                'sh_forms': sh_forms, 'batched_mc': batched_mc}
         print(json.dumps(line), flush=True)
     del loop
     if world > 1:
@@ -594,7 +669,7 @@ def main():
         torch.cuda.set_device(dev)
         out = bench_batched(dev, steps=max(5, min(args.steps, 200)),
                             cpu_budget_s=0 if args.no_cpu_baseline else 15.0)
-        print(json.dumps({'batched_mc': out}), flush=True)
+        print(json.dumps({'sh_forms': bench_sh_forms(dev), 'batched_mc': out}), flush=True)
         return
     if args.gradient_only:
         import torch

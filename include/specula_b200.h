@@ -288,6 +288,26 @@ int sb_dm_project_batched(const float *ifunc, int n_modes, int n_valid, int ld_i
 int sb_modalrec_batched(const float *R, int n_modes, int n_slopes, int ldr, const float *slopes, int lds,
                         int n_batch, float *modes, int ldm, void *stream);
 
+/* ------------------------------------------------------------------------
+ * Tile-shape tuning (an addition; the reference has no tuned kernels).  A
+ * tunable kernel family has several compiled tile shapes ("variants"); a
+ * launch uses the variant registered for its shape key, variant 0 when none
+ * is.  specula_b200.autotune times every variant on the caller's shapes and
+ * registers the fastest.  Registration is host state read when a launch is
+ * made (so a captured graph keeps the variant it was captured with).
+ *   SB_TUNE_DM_BATCHED  sb_dm_project_batched; key sb_tune_key(n_modes, n_valid, n_batch);
+ *                       realisations per pass (16, 8, 4) x mode rows of a stage split over 1 or 2 warp groups
+ *   SB_TUNE_SH_FP32     sb_sh_forward / sb_sh_forward_batched; key sb_tune_key(n_lenses, cutsize, n_batch);
+ *                       sub-apertures per CTA (8, 4, 2)
+ * ------------------------------------------------------------------------ */
+#define SB_TUNE_DM_BATCHED 0
+#define SB_TUNE_SH_FP32 1
+int sb_tune_variants(int family);                         /* 0 for an unknown family */
+const char *sb_tune_variant_name(int family, int variant);
+unsigned long long sb_tune_key(int a, int b, int c);
+int sb_tune_set(int family, unsigned long long key, int variant);   /* variant < 0: remove */
+int sb_tune_get(int family, unsigned long long key);               /* -1 for an unknown family */
+
 /* Diagnostics: SB_OK, or SB_ETIMEOUT when a bounded wait inside a kernel
  * (the shared-memory pipeline of sb_dm_project, the tensor-core waits of
  * sb_sh_forward_split_bf16) gave up since the last call;

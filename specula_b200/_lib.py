@@ -96,6 +96,11 @@ SIGNATURES = {
     'sb_sh_forward_split_bf16_batched': (C.c_int, [C.POINTER(ShPlan), fp, C.c_longlong, fp, C.c_longlong, fp,
                                                    C.c_longlong, C.c_int, C.c_float, fp, C.c_longlong, C.c_int, vp,
                                                    C.c_size_t, vp]),
+    'sb_tune_variants': (C.c_int, [C.c_int]),
+    'sb_tune_variant_name': (C.c_char_p, [C.c_int, C.c_int]),
+    'sb_tune_key': (C.c_ulonglong, [C.c_int, C.c_int, C.c_int]),
+    'sb_tune_set': (C.c_int, [C.c_int, C.c_ulonglong, C.c_int]),
+    'sb_tune_get': (C.c_int, [C.c_int, C.c_ulonglong]),
     'sb_ccd_step_batched': (C.c_int, [C.POINTER(CcdParams), vp, vp, C.c_int, fp, fp, fp, vp]),
     'sb_slopec_batched': (C.c_int, [C.POINTER(SlopecPlan), fp, C.c_longlong, fp, C.c_int, fp, C.c_int, C.c_int, vp,
                                     C.c_size_t, vp]),
@@ -118,6 +123,11 @@ SIGNATURES = {
 }
 
 _lib = None
+
+
+# tunable kernel families (specula_b200.h)
+SB_TUNE_DM_BATCHED = 0
+SB_TUNE_SH_FP32 = 1
 
 
 def load():

@@ -3,22 +3,22 @@
 Realisations come in geometry groups (same pupil, sub-aperture grid,
 wavelength, mirror and reconstructor; their own atmosphere (r0, seed) and
 detector noise seeds).  Each realisation is one ``ScaoLoop``'s objects, and
-within a group its field, detector frames, slopes and DM layer are rows of
-group stacks.  Per step, each realisation's AtmoEvolution and
-AtmoPropagation run on their own (different screens); then every group
-makes one launch each for the SH forward (``sb_sh_forward_batched``), the
-CCD (``sb_ccd_step_batched``, per-realisation seeds), the slopes
+within a group its turbulence layers, field, detector frames, slopes and DM
+layer are rows of group stacks.  Per step every group makes one launch per
+stage for all its realisations: the atmosphere (``sb_atmo_evolve_batched``,
+every layer of every realisation), the propagation
+(``sb_propagate_batched``), the SH forward (``sb_sh_forward_batched``, or
+``sb_sh_forward_split_bf16_batched`` with ``dft='split_bf16'``), the CCD
+(``sb_ccd_step_batched``, per-realisation seeds), the slopes
 (``sb_slopec_batched``), the reconstructor (``sb_modalrec_batched``: R read
 once for up to 16 realisations), the integrators (one ``sb_integrator`` call)
 and the mirror (``sb_dm_project_batched``: the influence functions read once
-for up to 16 realisations).  ``capture()`` puts the whole step of every
-realisation and group into one CUDA graph: the atmosphere/propagation chains
-over several streams, each group's launches on a stream of their own once its
-realisations' chains are done.
+for up to 16 realisations).  ``capture()`` puts the step of every group into
+one CUDA graph, each group on a stream of its own.
 
 ``BatchedScao.replay_plain()`` runs the same realisations the plain way (each
-``ScaoLoop``'s own captured step, its own reconstructor and mirror), for
-comparison.
+``ScaoLoop``'s own captured step with the FP32 SH, its own reconstructor and
+mirror), for comparison.
 """
 import ctypes
 import math
@@ -72,8 +72,14 @@ def mc_groups(seed=7, n_real=(55, 27, 14), wavelengths=(589.0, 750.0)):
     return groups
 
 
+SH_FORWARD = {'fp32': 'sb_sh_forward_batched', 'split_bf16': 'sb_sh_forward_split_bf16_batched'}
+
+
 class _Group:
-    def __init__(self, template, reals, device_idx):
+    def __init__(self, template, reals, device_idx, dft='fp32'):
+        if dft not in SH_FORWARD:
+            raise ValueError(f"dft must be one of {sorted(SH_FORWARD)}, not {dft!r}")
+        self.sh_forward = SH_FORWARD[dft]
         dev = torch.device('cuda', device_idx)
         self.device = dev
         self.n = len(reals)
@@ -137,6 +143,10 @@ class _Group:
         self.pseeds = torch.tensor([lp.ccd._photon_seed for lp in self.loops], dtype=torch.int64, device=dev)
         self.rseeds = torch.tensor([lp.ccd._readout_seed for lp in self.loops], dtype=torch.int64, device=dev)
         lib = _lib.load()
+        if self.sh_forward != SH_FORWARD['fp32'] and not lib.sb_sh_split_bf16_supported(ctypes.byref(lp0.sh._plan)):
+            g = lp0.sh.geometry
+            raise ValueError(f'BatchedScao: no split-BF16 SH kernel for np_sub={g.ovs_np_sub}, cutsize={g.cutsize}, '
+                             f'subap_npx={g.subap_npx}')
         self.sh_scratch = torch.empty(self.n * lib.sb_sh_scratch_bytes(ctypes.byref(lp0.sh._plan)),
                                       dtype=torch.uint8, device=dev)
         self.sc_scratch = torch.empty(self.n * lib.sb_slopec_scratch_bytes(ctypes.byref(lp0.slopec._plan)),
@@ -191,7 +201,7 @@ class _Group:
                   self.dm_phase.data_ptr(), L2, self.n, self.L, self.EA.data_ptr(), self.EP.data_ptr(), L2, st)
         lp = self.loops[0]
         L2, F2 = self.L * self.L, self.side * self.side
-        _lib.call('sb_sh_forward_batched', ctypes.byref(lp.sh._plan), self.EA.data_ptr(), L2, self.EP.data_ptr(), L2,
+        _lib.call(self.sh_forward, ctypes.byref(lp.sh._plan), self.EA.data_ptr(), L2, self.EP.data_ptr(), L2,
                   self.EA.data_ptr(), L2, L2, lp.sh._photon_scale, self.I.data_ptr(), F2, self.n,
                   self.sh_scratch.data_ptr(), self.sh_scratch.numel(), st)
         _lib.call('sb_ccd_step_batched', ctypes.byref(lp.ccd._params), self.pseeds.data_ptr(), self.rseeds.data_ptr(),
@@ -211,12 +221,51 @@ class _Group:
 
 
 class BatchedScao:
-    def __init__(self, groups, device_idx=0, streams=16):
+    def __init__(self, groups, device_idx=0, streams=16, dft='fp32'):
         self.device = torch.device('cuda', device_idx)
-        self.groups = [_Group(t, reals, device_idx) for t, reals in groups]
+        self.dft = dft
+        self.groups = [_Group(t, reals, device_idx, dft=dft) for t, reals in groups]
         self.n_streams = streams
         self.graph = None
         self.plain_graphs = None
+
+    def set_dft(self, dft):
+        """Switch the groups' SH forward between 'fp32' and 'split_bf16'; the
+        step graph must be captured again."""
+        if dft not in SH_FORWARD:
+            raise ValueError(f"dft must be one of {sorted(SH_FORWARD)}, not {dft!r}")
+        lib = _lib.load()
+        for g in self.groups:
+            sh = g.loops[0].sh
+            plan = getattr(sh, '_plan', None)      # set up by start(); checked there otherwise
+            if dft != 'fp32' and plan is not None and not lib.sb_sh_split_bf16_supported(ctypes.byref(plan)):
+                raise ValueError(f'BatchedScao: no split-BF16 SH kernel for cutsize={sh.geometry.cutsize}, '
+                                 f'subap_npx={sh.geometry.subap_npx}')
+        for g in self.groups:
+            g.sh_forward = SH_FORWARD[dft]
+        self.dft = dft
+        self.graph = None
+
+    def autotune(self, tuner=None):
+        """Tune the tile shapes of every group's batched mirror projection (and
+        of its SH forward, in the FP32 form) on the group's own buffers with a
+        specula_b200.autotune.Autotuner; the launches are idempotent, so the
+        simulation state is unchanged.  Capture the step graph afterwards.
+        Returns the tuner's records."""
+        from specula_b200.autotune import Autotuner
+        tuner = tuner or Autotuner(self.device)
+        torch.cuda.synchronize(self.device)
+        for g in self.groups:
+            lp = g.loops[0]
+            dm = g.dm
+            tuner.tune_dm_batched(dm._IF, g.nm, int(dm._idx.numel()), dm._ld, g.integ.out_comm.value, g.nm, g.n,
+                                  float(dm.sign), dm._idx, g.dm_phase, g.L * g.L)
+            if g.sh_forward == SH_FORWARD['fp32']:
+                L2, F2 = g.L * g.L, g.side * g.side
+                tuner.tune_sh_fp32(lp.sh._plan, g.EA, L2, g.EP, L2, g.EA, L2, L2, lp.sh._photon_scale, g.I, F2, g.n,
+                                   g.sh_scratch)
+        self.graph = None
+        return tuner.results
 
     @property
     def n_realisations(self):

@@ -68,3 +68,65 @@ int sm_count() {
 }
 
 }  // namespace sb
+
+// ---------------------------------------------------------------------------
+// Tile-shape tuning registry: (kernel family, shape key) -> variant.
+// ---------------------------------------------------------------------------
+#include <map>
+#include <mutex>
+#include <utility>
+
+namespace {
+std::mutex g_tune_mutex;
+std::map<std::pair<int, unsigned long long>, int> g_tune;
+const char *const kDmBatchedVariants[] = {
+    "16 realisations per pass, 1 mode-row group", "16 realisations per pass, 2 mode-row groups",
+    "8 realisations per pass, 1 mode-row group",  "8 realisations per pass, 2 mode-row groups",
+    "4 realisations per pass, 1 mode-row group",  "4 realisations per pass, 2 mode-row groups"};
+const char *const kShFp32Variants[] = {"8 sub-apertures per CTA", "4 sub-apertures per CTA",
+                                       "2 sub-apertures per CTA"};
+}  // namespace
+
+namespace sb {
+int tune_lookup(int family, unsigned long long key) {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    auto it = g_tune.find({family, key});
+    return it == g_tune.end() ? 0 : it->second;
+}
+}  // namespace sb
+
+extern "C" int sb_tune_variants(int family) {
+    switch (family) {
+        case SB_TUNE_DM_BATCHED: return (int)(sizeof(kDmBatchedVariants) / sizeof(kDmBatchedVariants[0]));
+        case SB_TUNE_SH_FP32: return (int)(sizeof(kShFp32Variants) / sizeof(kShFp32Variants[0]));
+        default: return 0;
+    }
+}
+
+extern "C" const char *sb_tune_variant_name(int family, int variant) {
+    if (variant < 0 || variant >= sb_tune_variants(family)) return "";
+    return family == SB_TUNE_DM_BATCHED ? kDmBatchedVariants[variant] : kShFp32Variants[variant];
+}
+
+extern "C" unsigned long long sb_tune_key(int a, int b, int c) {
+    return ((unsigned long long)(unsigned)a << 40) ^ ((unsigned long long)(unsigned)b << 12) ^
+           (unsigned long long)(unsigned)c;
+}
+
+extern "C" int sb_tune_set(int family, unsigned long long key, int variant) {
+    sb::clear_error();
+    const int n = sb_tune_variants(family);
+    if (n == 0) return sb::fail(SB_EINVAL, "sb_tune_set: unknown kernel family %d", family);
+    if (variant >= n) return sb::fail(SB_EINVAL, "sb_tune_set: family %d has %d variants", family, n);
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    if (variant < 0)
+        g_tune.erase({family, key});
+    else
+        g_tune[{family, key}] = variant;
+    return SB_OK;
+}
+
+extern "C" int sb_tune_get(int family, unsigned long long key) {
+    if (sb_tune_variants(family) == 0) return -1;
+    return sb::tune_lookup(family, key);
+}

@@ -321,9 +321,13 @@ __global__ void __launch_bounds__(32 * (kDmConsumerWarps + 1), 1)
 // ---------------------------------------------------------------------------
 
 // phase_b[idx[p]] = sum_m c_b[m] IF[m][p] for b < NB.  Same TMA ring as
-// dm_project_tma_kernel (32 x 256 boxes, 3 stages, evict-first); 8 consumer
-// warps, one column per thread and NB accumulators; the NB command vectors
-// are staged in shared memory as [mode][NB].
+// dm_project_tma_kernel (32 x 256 boxes, evict-first), with NB accumulators
+// per column and the NB command vectors staged in shared memory as
+// [mode][NB].  RS = 1: 8 consumer warps, one column per thread.  RS = 2: 16
+// consumer warps of 16 columns each; the two half-warps take the first and
+// the second 16 mode rows of every stage and their partial sums meet by a
+// shuffle at the end of the tile (twice the warps to hide shared-memory
+// latency; another summation order, so not bit-identical to RS = 1).
 constexpr int kDbWarps = 8;
 // more stages than the single-vector kernel: the NB accumulators make each
 // stage's consumption longer, and this kernel need not leave room for
@@ -336,11 +340,14 @@ size_t dm_batched_smem_bytes(int nmodes) {
     return 1024 + (size_t)kDbStages * kDmRows * kDmCols * 4 + 2 * kDbStages * 8 + (size_t)nst * kDmRows * NB * 4;
 }
 
-template <int NB>
-__global__ void __launch_bounds__(32 * (kDbWarps + 1), 1)
+template <int NB, int RS>
+__global__ void __launch_bounds__(32 * (kDbWarps * RS + 1), 1)
     dm_project_batched_kernel(const __grid_constant__ CUtensorMap map, int nmodes, int nvalid,
                               const float *__restrict__ cmd, int ldc, int nb, float sign,
                               const int32_t *__restrict__ idx, float *__restrict__ phase, long long phase_stride) {
+    static_assert(RS == 1 || RS == 2, "one or two mode-row groups");
+    constexpr int NCW = kDbWarps * RS;            // consumer warps
+    constexpr int RR = kDmRows / RS;              // mode rows per thread and stage
     extern __shared__ unsigned char smem_raw[];
     unsigned char *base = smem_raw + ((1024 - (sb::smem_u32(smem_raw) & 1023)) & 1023);
     float *ring = reinterpret_cast<float *>(base);
@@ -353,7 +360,7 @@ __global__ void __launch_bounds__(32 * (kDbWarps + 1), 1)
     if (tid == 0) {
         for (int s = 0; s < kDbStages; ++s) {
             sb::mbar_init(&full[s], 1);
-            sb::mbar_init(&empty[s], kDbWarps);
+            sb::mbar_init(&empty[s], NCW);
         }
         sb::mbar_init_fence();
         abort_flag = 0;
@@ -368,7 +375,7 @@ __global__ void __launch_bounds__(32 * (kDbWarps + 1), 1)
     const int bid = blockIdx.x, nblk = gridDim.x;
     const int my_tiles = bid < ntiles ? (ntiles - 1 - bid) / nblk + 1 : 0;
     const int total = my_tiles * nst;
-    if (warp == kDbWarps) {
+    if (warp == NCW) {
         if (lane == 0) {
             const uint64_t pol = sb::l2_evict_first_policy();
             int q = 0;
@@ -388,22 +395,26 @@ __global__ void __launch_bounds__(32 * (kDbWarps + 1), 1)
             issued = q;
         }
     } else {
+        // this thread's column within the tile and first mode row within a stage
+        const int col_l = RS == 1 ? warp * 32 + lane : warp * 16 + (lane & 15);
+        const int r0 = RS == 1 ? 0 : (lane >> 4) * RR;
         float acc[NB];
 #pragma unroll
         for (int b = 0; b < NB; ++b) acc[b] = 0.f;
         for (int q = 0; q < total; ++q) {
             const int slot = q % kDbStages;
-            if (!sb::mbar_wait(&full[slot], (q / kDbStages) & 1)) {
-                atomicExch(&g_dm_status, 4);
+            // warp-uniform decisions: the lanes meet in shuffles below
+            if (!__all_sync(0xffffffffu, sb::mbar_wait(&full[slot], (q / kDbStages) & 1))) {
+                if (lane == 0) atomicExch(&g_dm_status, 4);
                 abort_flag = 1;
                 break;
             }
-            if (*(volatile int *)&abort_flag) break;
+            if (__any_sync(0xffffffffu, *(volatile int *)&abort_flag)) break;
             const int sg = q % nst;
-            const float *buf = ring + (size_t)slot * kDmRows * kDmCols + tid;
-            const float4 *cm = reinterpret_cast<const float4 *>(c + (size_t)sg * kDmRows * NB);
+            const float *buf = ring + (size_t)slot * kDmRows * kDmCols + (size_t)r0 * kDmCols + col_l;
+            const float4 *cm = reinterpret_cast<const float4 *>(c + ((size_t)sg * kDmRows + r0) * NB);
 #pragma unroll 4
-            for (int r = 0; r < kDmRows; ++r) {
+            for (int r = 0; r < RR; ++r) {
                 const float v = buf[r * kDmCols];
 #pragma unroll
                 for (int b4 = 0; b4 < NB / 4; ++b4) {
@@ -417,8 +428,12 @@ __global__ void __launch_bounds__(32 * (kDbWarps + 1), 1)
             __syncwarp();
             if (lane == 0) sb::mbar_arrive(&empty[slot]);
             if (sg == nst - 1) {
-                const int col = (bid + (q / nst) * nblk) * kDmCols + tid;
-                if (col < nvalid) {
+                if constexpr (RS == 2) {
+#pragma unroll
+                    for (int b = 0; b < NB; ++b) acc[b] += __shfl_xor_sync(0xffffffffu, acc[b], 16);
+                }
+                const int col = (bid + (q / nst) * nblk) * kDmCols + col_l;
+                if ((RS == 1 || lane < 16) && col < nvalid) {
                     const int pix = idx[col];
 #pragma unroll
                     for (int b = 0; b < NB; ++b)
@@ -582,7 +597,7 @@ extern "C" int sb_dm_project(const float *ifunc, int n_modes, int n_valid, int l
 
 namespace {
 
-template <int NB>
+template <int NB, int RS>
 int launch_dm_batched(const CUtensorMap &map, int n_modes, int n_valid, const float *cmd, int ldc, int nb, float sign,
                       const int32_t *mask_idx, float *phase, long long phase_stride, cudaStream_t st) {
     static bool attr_set[64] = {false};
@@ -590,16 +605,24 @@ int launch_dm_batched(const CUtensorMap &map, int n_modes, int n_valid, const fl
     cudaGetDevice(&dev);
     const size_t smem = dm_batched_smem_bytes<NB>(n_modes);
     if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-        if (cudaFuncSetAttribute(dm_project_batched_kernel<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if (cudaFuncSetAttribute(dm_project_batched_kernel<NB, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)dm_batched_smem_bytes<NB>(kDbMaxModes)) != cudaSuccess)
             return sb::fail(SB_ECUDA, "sb_dm_project_batched: %s", cudaGetErrorString(cudaGetLastError()));
         attr_set[dev] = true;
     }
     const int nsm = sb::sm_count();
     const int ntiles = (n_valid + kDmCols - 1) / kDmCols;
-    dm_project_batched_kernel<NB><<<ntiles < nsm ? ntiles : nsm, 32 * (kDbWarps + 1), smem, st>>>(
+    dm_project_batched_kernel<NB, RS><<<ntiles < nsm ? ntiles : nsm, 32 * (kDbWarps * RS + 1), smem, st>>>(
         map, n_modes, n_valid, cmd, ldc, nb, sign, mask_idx, phase, phase_stride);
     return sb::check_launch("dm_project_batched_kernel");
+}
+
+template <int RS>
+int launch_dm_batched_rs(const CUtensorMap &map, int n_modes, int n_valid, const float *c, int ldc, int nb,
+                         float sign, const int32_t *mask_idx, float *ph, long long phase_stride, cudaStream_t st) {
+    if (nb <= 4) return launch_dm_batched<4, RS>(map, n_modes, n_valid, c, ldc, nb, sign, mask_idx, ph, phase_stride, st);
+    if (nb <= 8) return launch_dm_batched<8, RS>(map, n_modes, n_valid, c, ldc, nb, sign, mask_idx, ph, phase_stride, st);
+    return launch_dm_batched<16, RS>(map, n_modes, n_valid, c, ldc, nb, sign, mask_idx, ph, phase_stride, st);
 }
 
 }  // namespace
@@ -620,14 +643,16 @@ extern "C" int sb_dm_project_batched(const float *ifunc, int n_modes, int n_vali
     int rc = sb::tensor_map_2d_f32(&map, ifunc, n_modes, ld_if, ld_if, kDmRows, kDmCols);
     if (rc) return rc;
     cudaStream_t st = sb::as_stream(stream);
-    // chunks of up to 16 realisations; every chunk re-reads the IF once
-    for (int b0 = 0; b0 < n_batch; b0 += 16) {
-        const int nb = n_batch - b0 < 16 ? n_batch - b0 : 16;
+    // tile variant: realisations per pass (every pass re-reads the IF once) and mode-row groups
+    const int v = sb::tune_lookup(SB_TUNE_DM_BATCHED, sb_tune_key(n_modes, n_valid, n_batch));
+    const int pass = v < 2 ? 16 : (v < 4 ? 8 : 4);
+    const bool rs2 = (v & 1) != 0;
+    for (int b0 = 0; b0 < n_batch; b0 += pass) {
+        const int nb = n_batch - b0 < pass ? n_batch - b0 : pass;
         const float *c = cmd + (size_t)b0 * ld_cmd;
         float *ph = phase + (size_t)b0 * phase_stride;
-        if (nb <= 4) rc = launch_dm_batched<4>(map, n_modes, n_valid, c, ld_cmd, nb, sign, mask_idx, ph, phase_stride, st);
-        else if (nb <= 8) rc = launch_dm_batched<8>(map, n_modes, n_valid, c, ld_cmd, nb, sign, mask_idx, ph, phase_stride, st);
-        else rc = launch_dm_batched<16>(map, n_modes, n_valid, c, ld_cmd, nb, sign, mask_idx, ph, phase_stride, st);
+        rc = rs2 ? launch_dm_batched_rs<2>(map, n_modes, n_valid, c, ld_cmd, nb, sign, mask_idx, ph, phase_stride, st)
+                 : launch_dm_batched_rs<1>(map, n_modes, n_valid, c, ld_cmd, nb, sign, mask_idx, ph, phase_stride, st);
         if (rc) return rc;
     }
     return SB_OK;

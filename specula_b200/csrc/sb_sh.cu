@@ -36,6 +36,7 @@ struct ShArgs {
     // elements; 0 and gridDim.z = 1 for a single field)
     long long sA, sph, sAn, sout;
     int nbp;                       // partial sums per realisation
+    int vec;                       // field rows may be read as float4 (16-byte aligned rows and strides)
 };
 
 // the realisation's slice of a batched launch
@@ -357,19 +358,15 @@ struct TcShape {
     static constexpr int GS = CS * 8 + 8;                // float2 per sub-aperture in the G buffer (bank offset)
 };
 
-// Dynamic shared memory per CTA: the operands and tables, and at least
-// 52 KB, which bounds any operand read that the descriptors can express
-// (8-row groups and K segments at the larger of the two strides) inside the
-// allocation; it also caps residency at 4 CTAs (256 tensor-memory columns)
-// per SM.
-constexpr size_t kTcSmemFloor = 52 * 1024;
+// Dynamic shared memory per CTA: operands, G / |F|^2 buffer and tables
+// (35-46 KB), so at most 6 CTAs, 384 tensor-memory columns, share an SM and
+// the allocation never waits.
 template <int P, int CS, int NPX>
 __host__ __device__ constexpr size_t tc_smem_bytes() {
-    const size_t used = 6 * (size_t)kTcOperandBytes + 2 * (size_t)TcShape<CS>::NB * 32 +
-                        (size_t)kTcSub * TcShape<CS>::GS * 8 + (size_t)P * P * 8 + (size_t)CS * CS * 4 +
-                        (size_t)NPX * CS * 4 + 8 + 16;
-    return used > kTcSmemFloor ? used : kTcSmemFloor;
+    return 6 * (size_t)kTcOperandBytes + 2 * (size_t)TcShape<CS>::NB * 32 + (size_t)kTcSub * TcShape<CS>::GS * 8 +
+           (size_t)P * P * 8 + (size_t)CS * CS * 4 + (size_t)NPX * CS * 4 + 8 + 16;
 }
+static_assert(tc_smem_bytes<8, 8, 8>() * 8 > 228 * 1024, "more than 8 CTAs per SM would exceed tensor memory");
 
 template <int P, int CS, int NPX>
 __global__ void __launch_bounds__(kTcThreads) sh_forward_tc_kernel(ShArgs a) {
@@ -381,11 +378,11 @@ __global__ void __launch_bounds__(kTcThreads) sh_forward_tc_kernel(ShArgs a) {
     constexpr uint32_t IDESC = sb::umma_idesc_bf16_f32(128, NB);
     constexpr uint32_t LBO_A = 128 * 16, LBO_B = NB * 16;
     batch_slice(a);
-    extern __shared__ __align__(128) unsigned char smem[];
-    unsigned char *A1h = smem, *A1l = smem + kTcOperandBytes;
-    unsigned char *A2h = smem + 2 * kTcOperandBytes;   // two tiles
-    unsigned char *A2l = smem + 4 * kTcOperandBytes;   // two tiles
-    unsigned char *Bh = smem + 6 * kTcOperandBytes, *Bl = Bh + NB * 32;
+    extern __shared__ __align__(128) unsigned char tc_smem[];
+    unsigned char *A1h = tc_smem, *A1l = tc_smem + kTcOperandBytes;
+    unsigned char *A2h = tc_smem + 2 * kTcOperandBytes;   // two tiles
+    unsigned char *A2l = tc_smem + 4 * kTcOperandBytes;   // two tiles
+    unsigned char *Bh = tc_smem + 6 * kTcOperandBytes, *Bl = Bh + NB * 32;
     float2 *Gb = reinterpret_cast<float2 *>(Bl + NB * 32);
     float *Ib = reinterpret_cast<float *>(Gb);        // |F|^2 after G is consumed
     float2 *tilt = Gb + kTcSub * GS;
@@ -396,6 +393,43 @@ __global__ void __launch_bounds__(kTcThreads) sh_forward_tc_kernel(ShArgs a) {
     __shared__ float red[33];
 
     const int t = threadIdx.x, warp = t >> 5;
+    // issue the global loads first: this thread's field row and its share of
+    // the normalising amplitude; the table set-up below overlaps them
+    const int i = blockIdx.y;
+    const int s = t >> 3, r = t & 7;
+    const int j = blockIdx.x * kTcSub + s;
+    float amp[8], phv[8];
+    if (j < a.n) {
+        const size_t g = (size_t)(i * P + r) * a.ld + (size_t)j * P;
+        if (a.vec) {
+            const float4 a0 = *reinterpret_cast<const float4 *>(a.A + g);
+            const float4 a1 = *reinterpret_cast<const float4 *>(a.A + g + 4);
+            const float4 p0 = *reinterpret_cast<const float4 *>(a.ph + g);
+            const float4 p1 = *reinterpret_cast<const float4 *>(a.ph + g + 4);
+            amp[0] = a0.x; amp[1] = a0.y; amp[2] = a0.z; amp[3] = a0.w;
+            amp[4] = a1.x; amp[5] = a1.y; amp[6] = a1.z; amp[7] = a1.w;
+            phv[0] = p0.x; phv[1] = p0.y; phv[2] = p0.z; phv[3] = p0.w;
+            phv[4] = p1.x; phv[5] = p1.y; phv[6] = p1.z; phv[7] = p1.w;
+        } else {
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                amp[c] = a.A[g + c];
+                phv[c] = a.ph[g + c];
+            }
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) amp[c] = phv[c] = 0.f;
+    }
+    const int bid = blockIdx.y * gridDim.x + blockIdx.x;
+    float sa = 0.f;
+    {
+        const int nblk = gridDim.x * gridDim.y;
+        const int chunk = (a.n_norm + nblk - 1) / nblk;
+        const int lo = bid * chunk;
+        const int hi = min(a.n_norm, lo + chunk);
+        for (int e = lo + t; e < hi; e += kTcThreads) sa += a.A_norm[e];
+    }
     if (warp == 0) {
         sb::tmem_alloc(tmem_slot, kTcTmemCols);
         sb::tmem_relinquish();
@@ -441,27 +475,17 @@ __global__ void __launch_bounds__(kTcThreads) sh_forward_tc_kernel(ShArgs a) {
     __syncthreads();
 
     // field build (electric_field.py:60-75 and sh.py:376): thread t holds row r of sub-aperture s
-    const int i = blockIdx.y;
-    const int s = t >> 3, r = t & 7;
-    const int j = blockIdx.x * kTcSub + s;
     {
         float er[8], ei[8];
-        if (j < a.n) {
-            const size_t g = (size_t)(i * P + r) * a.ld + (size_t)j * P;
 #pragma unroll
-            for (int c = 0; c < 8; ++c) {
-                const float amp = a.A[g + c];
-                const float phi = a.ph[g + c] * a.k;
-                float sn, co;
-                sincosf(phi, &sn, &co);
-                const float re = co * amp, im = sn * amp;
-                const float2 tl = tilt[r * P + c];
-                er[c] = re * tl.x - im * tl.y;
-                ei[c] = re * tl.y + im * tl.x;
-            }
-        } else {
-#pragma unroll
-            for (int c = 0; c < 8; ++c) er[c] = ei[c] = 0.f;
+        for (int c = 0; c < 8; ++c) {
+            const float phi = phv[c] * a.k;
+            float sn, co;
+            sincosf(phi, &sn, &co);
+            const float re = co * amp[c], im = sn * amp[c];
+            const float2 tl = tilt[r * P + c];
+            er[c] = re * tl.x - im * tl.y;
+            ei[c] = re * tl.y + im * tl.x;
         }
         uint4 h, l;
         sb::split_bf16x8(er, h, l);
@@ -603,14 +627,7 @@ __global__ void __launch_bounds__(kTcThreads) sh_forward_tc_kernel(ShArgs a) {
         if (t == 0) atomicExch(&g_sh_tc_status, 1 + pending);
         sb::mbar_wait(bar, pending);
     }
-    const int bid = blockIdx.y * gridDim.x + blockIdx.x;
     const float tot = sb::block_sum(local, red);
-    const int nblk = gridDim.x * gridDim.y;
-    const int chunk = (a.n_norm + nblk - 1) / nblk;
-    const int lo = bid * chunk;
-    const int hi = min(a.n_norm, lo + chunk);
-    float sa = 0.f;
-    for (int e = lo + t; e < hi; e += kTcThreads) sa += a.A_norm[e];
     const float tota = sb::block_sum(sa, red);
     if (t == 0) {
         a.part_I[bid] = tot;
@@ -702,12 +719,16 @@ __global__ void interp2d_field_kernel(const float *A, const float *P, int rows, 
     }
 }
 
-int sh_grid(const sb_sh_plan *pl, int *spc, dim3 *grid, size_t *smem) {
+// smallest sub-apertures-per-CTA of the SB_TUNE_SH_FP32 variants (8, 4, 2):
+// the scratch size covers its grid
+constexpr int kShMinSpc = 2;
+
+int sh_grid(const sb_sh_plan *pl, int *spc, dim3 *grid, size_t *smem, int spc_cap = 8) {
     const ShSmem L = sh_smem_layout(pl->np_sub, pl->cutsize, pl->subap_npx);
     const int budget = 200 * 1024;
     if (L.tables + L.per_warp > budget) return -1;
     int s = (budget - L.tables) / L.per_warp;
-    s = s > 8 ? 8 : s;
+    s = s > spc_cap ? spc_cap : s;
     if (s > pl->n_lenses) s = pl->n_lenses;
     *spc = s;
     *grid = dim3((pl->n_lenses + s - 1) / s, pl->n_lenses, 1);
@@ -722,7 +743,7 @@ extern "C" size_t sb_sh_scratch_bytes(const sb_sh_plan *pl) {
     int spc;
     dim3 grid;
     size_t smem;
-    if (sh_grid(pl, &spc, &grid, &smem)) return 0;
+    if (sh_grid(pl, &spc, &grid, &smem, kShMinSpc)) return 0;
     const size_t nb = (size_t)grid.x * grid.y;
     return ((2 * nb * sizeof(float)) + 255) & ~(size_t)255;
 }
@@ -743,7 +764,8 @@ int sh_forward_impl(const char *who, const sb_sh_plan *pl, const float *A, long 
     int spc;
     dim3 grid;
     size_t smem;
-    if (sh_grid(pl, &spc, &grid, &smem))
+    const int variant = mode == 0 ? sb::tune_lookup(SB_TUNE_SH_FP32, sb_tune_key(pl->n_lenses, pl->cutsize, n_batch)) : 0;
+    if (sh_grid(pl, &spc, &grid, &smem, 8 >> variant))
         return sb::fail(SB_ESHAPE, "%s: sub-aperture (np=%d, cut=%d, npx=%d) does not fit in shared memory", who,
                         pl->np_sub, pl->cutsize, pl->subap_npx);
     const size_t need = sb_sh_scratch_bytes(pl) * (size_t)n_batch;
@@ -784,9 +806,12 @@ int sh_forward_impl(const char *who, const sb_sh_plan *pl, const float *A, long 
     a.sAn = sAn;
     a.sout = sout;
     a.nbp = nb;
+    a.vec = (a.ld % 4 == 0) && (sA % 4 == 0) && (sph % 4 == 0) && ((uintptr_t)A % 16 == 0) &&
+            ((uintptr_t)phase_nm % 16 == 0) && (a.p % 4 == 0);
     grid.z = n_batch;
     cudaStream_t st = sb::as_stream(stream);
-    ShKernel fk = (spc == 8 || spc == pl->n_lenses) ? fixed_kernel(a.p, a.cs, a.npx) : nullptr;
+    // the compile-time kernel holds per-warp buffers for up to 8 warps
+    ShKernel fk = spc <= 8 ? fixed_kernel(a.p, a.cs, a.npx) : nullptr;
     if (tk.fn) {
         if (tk.smem > 48 * 1024) {
             cudaError_t e = cudaFuncSetAttribute(tk.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tk.smem);
