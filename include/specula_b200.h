@@ -299,9 +299,12 @@ int sb_modalrec_batched(const float *R, int n_modes, int n_slopes, int ldr, cons
  *                       realisations per pass (16, 8, 4) x mode rows of a stage split over 1 or 2 warp groups
  *   SB_TUNE_SH_FP32     sb_sh_forward / sb_sh_forward_batched; key sb_tune_key(n_lenses, cutsize, n_batch);
  *                       sub-apertures per CTA (8, 4, 2)
+ *   SB_TUNE_MODALREC_BATCHED  sb_modalrec_batched; key sb_tune_key(n_modes, n_slopes, n_batch);
+ *                       reconstructor rows per CTA (2, 1, 4)
  * ------------------------------------------------------------------------ */
 #define SB_TUNE_DM_BATCHED 0
 #define SB_TUNE_SH_FP32 1
+#define SB_TUNE_MODALREC_BATCHED 2
 int sb_tune_variants(int family);                         /* 0 for an unknown family */
 const char *sb_tune_variant_name(int family, int variant);
 unsigned long long sb_tune_key(int a, int b, int c);

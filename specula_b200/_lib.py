@@ -128,6 +128,7 @@ _lib = None
 # tunable kernel families (specula_b200.h)
 SB_TUNE_DM_BATCHED = 0
 SB_TUNE_SH_FP32 = 1
+SB_TUNE_MODALREC_BATCHED = 2
 
 
 def load():

@@ -18,7 +18,9 @@ Families wired here:
 * ``dm_batched``: ``sb_dm_project_batched``, realisations per pass x mode-row
   groups (6 variants);
 * ``sh_fp32``: ``sb_sh_forward_batched`` (FP32 form), sub-apertures per CTA
-  (8, 4, 2).
+  (8, 4, 2);
+* ``modalrec_batched``: ``sb_modalrec_batched``, reconstructor rows per CTA
+  (2, 1, 4).
 """
 import ctypes
 import json
@@ -29,7 +31,8 @@ import torch
 
 from specula_b200 import _lib
 
-FAMILIES = {'dm_batched': _lib.SB_TUNE_DM_BATCHED, 'sh_fp32': _lib.SB_TUNE_SH_FP32}
+FAMILIES = {'dm_batched': _lib.SB_TUNE_DM_BATCHED, 'sh_fp32': _lib.SB_TUNE_SH_FP32,
+            'modalrec_batched': _lib.SB_TUNE_MODALREC_BATCHED}
 
 
 class Autotuner:
@@ -60,7 +63,7 @@ class Autotuner:
         os.replace(tmp, self.cache_path)
 
     def tune(self, family, shape, launch, output):
-        """Tune ``family`` ('dm_batched' or 'sh_fp32') for ``shape`` (the three
+        """Tune ``family`` (a key of FAMILIES) for ``shape`` (the three
         ints of its sb_tune_key).  ``launch()`` makes one launch of the kernel
         on the current stream; it must be idempotent (same inputs, same output
         tensor).  ``output`` is the tensor it writes, compared across variants."""
@@ -135,3 +138,9 @@ class Autotuner:
                       intensity_stride, n_batch, scratch.data_ptr(), scratch.numel(),
                       torch.cuda.current_stream(self.device).cuda_stream)
         return self.tune('sh_fp32', (plan.n_lenses, plan.cutsize, n_batch), launch, intensity)
+
+    def tune_modalrec_batched(self, R, n_modes, n_slopes, ldr, slopes, lds, n_batch, modes, ldm):
+        def launch():
+            _lib.call('sb_modalrec_batched', R.data_ptr(), n_modes, n_slopes, ldr, slopes.data_ptr(), lds, n_batch,
+                      modes.data_ptr(), ldm, torch.cuda.current_stream(self.device).cuda_stream)
+        return self.tune('modalrec_batched', (n_modes, n_slopes, n_batch), launch, modes)

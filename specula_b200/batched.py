@@ -247,8 +247,9 @@ class BatchedScao:
         self.graph = None
 
     def autotune(self, tuner=None):
-        """Tune the tile shapes of every group's batched mirror projection (and
-        of its SH forward, in the FP32 form) on the group's own buffers with a
+        """Tune the tile shapes of every group's batched mirror projection and
+        reconstructor (and of its SH forward, in the FP32 form) on the group's
+        own buffers with a
         specula_b200.autotune.Autotuner; the launches are idempotent, so the
         simulation state is unchanged.  Capture the step graph afterwards.
         Returns the tuner's records."""
@@ -260,6 +261,8 @@ class BatchedScao:
             dm = g.dm
             tuner.tune_dm_batched(dm._IF, g.nm, int(dm._idx.numel()), dm._ld, g.integ.out_comm.value, g.nm, g.n,
                                   float(dm.sign), dm._idx, g.dm_phase, g.L * g.L)
+            R = lp.rec._R
+            tuner.tune_modalrec_batched(R, g.nm, g.nsl, R.stride(0), g.S, g.nsl, g.n, g.M, g.nm)
             if g.sh_forward == SH_FORWARD['fp32']:
                 L2, F2 = g.L * g.L, g.side * g.side
                 tuner.tune_sh_fp32(lp.sh._plan, g.EA, L2, g.EP, L2, g.EA, L2, L2, lp.sh._photon_scale, g.I, F2, g.n,

@@ -85,6 +85,8 @@ const char *const kDmBatchedVariants[] = {
     "4 realisations per pass, 1 mode-row group",  "4 realisations per pass, 2 mode-row groups"};
 const char *const kShFp32Variants[] = {"8 sub-apertures per CTA", "4 sub-apertures per CTA",
                                        "2 sub-apertures per CTA"};
+const char *const kModalrecVariants[] = {"2 reconstructor rows per CTA", "1 reconstructor row per CTA",
+                                         "4 reconstructor rows per CTA"};
 }  // namespace
 
 namespace sb {
@@ -99,13 +101,18 @@ extern "C" int sb_tune_variants(int family) {
     switch (family) {
         case SB_TUNE_DM_BATCHED: return (int)(sizeof(kDmBatchedVariants) / sizeof(kDmBatchedVariants[0]));
         case SB_TUNE_SH_FP32: return (int)(sizeof(kShFp32Variants) / sizeof(kShFp32Variants[0]));
+        case SB_TUNE_MODALREC_BATCHED: return (int)(sizeof(kModalrecVariants) / sizeof(kModalrecVariants[0]));
         default: return 0;
     }
 }
 
 extern "C" const char *sb_tune_variant_name(int family, int variant) {
     if (variant < 0 || variant >= sb_tune_variants(family)) return "";
-    return family == SB_TUNE_DM_BATCHED ? kDmBatchedVariants[variant] : kShFp32Variants[variant];
+    switch (family) {
+        case SB_TUNE_DM_BATCHED: return kDmBatchedVariants[variant];
+        case SB_TUNE_SH_FP32: return kShFp32Variants[variant];
+        default: return kModalrecVariants[variant];
+    }
 }
 
 extern "C" unsigned long long sb_tune_key(int a, int b, int c) {

@@ -450,35 +450,65 @@ __global__ void __launch_bounds__(32 * (kDbWarps * RS + 1), 1)
     }
 }
 
-// modes_b[m] = sum_j R[m][j] s_b[j] for b < NB: one CTA per reconstructor
-// row, read once for all NB slope vectors
-template <int NB>
-__global__ void __launch_bounds__(256) gemv_rows_batched_kernel(const float *__restrict__ R, int ncols, int ldr,
-                                                                const float *__restrict__ S, int lds, int nb,
-                                                                float *__restrict__ M, int ldm) {
-    __shared__ float red[NB][33];
-    const int m = blockIdx.x;
-    const float *row = R + (size_t)m * ldr;
-    float acc[NB];
+// modes_b[m] = sum_j R[m][j] s_b[j] for b < NB.  A CTA of 256 threads takes
+// RB reconstructor rows; each thread walks the slope index in pairs (8-byte
+// loads when the strides allow), loads the NB slope pairs once and uses them
+// for all RB rows, so S is read from L2 once per RB rows and R streams from
+// HBM once.  Per (row, vector): warp sums, then a fixed-order sum over the
+// 8 warps (deterministic).  RB (1, 2, 4) is the SB_TUNE_MODALREC_BATCHED
+// variant.
+template <int NB, int RB>
+__global__ void __launch_bounds__(256) gemv_rows_batched_kernel(const float *__restrict__ R, int nrows, int ncols,
+                                                                int ldr, const float *__restrict__ S, int lds,
+                                                                int nb, float *__restrict__ M, int ldm, int vec2) {
+    __shared__ float red[RB * NB][9];
+    const int m0 = blockIdx.x * RB;
+    float acc[RB][NB];
 #pragma unroll
-    for (int b = 0; b < NB; ++b) acc[b] = 0.f;
-    for (int j = threadIdx.x; j < ncols; j += blockDim.x) {
-        const float r = __ldg(row + j);
+    for (int r = 0; r < RB; ++r)
 #pragma unroll
-        for (int b = 0; b < NB; ++b)
-            if (b < nb) acc[b] = fmaf(r, __ldg(S + (size_t)b * lds + j), acc[b]);
+        for (int b = 0; b < NB; ++b) acc[r][b] = 0.f;
+    const float *rows[RB];
+#pragma unroll
+    for (int r = 0; r < RB; ++r) rows[r] = R + (size_t)(m0 + r < nrows ? m0 + r : m0) * ldr;
+    for (int k = 2 * threadIdx.x; k < ncols; k += 2 * blockDim.x) {
+        const bool pair = k + 1 < ncols;
+        float2 sv[NB];
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            sv[b] = make_float2(0.f, 0.f);
+            if (b < nb) {
+                const float *sp = S + (size_t)b * lds + k;
+                if (vec2 && pair) sv[b] = __ldg(reinterpret_cast<const float2 *>(sp));
+                else sv[b] = make_float2(__ldg(sp), pair ? __ldg(sp + 1) : 0.f);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < RB; ++r) {
+            if (m0 + r >= nrows) break;
+            float2 rv;
+            if (vec2 && pair) rv = __ldg(reinterpret_cast<const float2 *>(rows[r] + k));
+            else rv = make_float2(__ldg(rows[r] + k), pair ? __ldg(rows[r] + k + 1) : 0.f);
+#pragma unroll
+            for (int b = 0; b < NB; ++b) acc[r][b] = fmaf(rv.y, sv[b].y, fmaf(rv.x, sv[b].x, acc[r][b]));
+        }
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-    for (int b = 0; b < NB; ++b) {
-        const float v = sb::warp_sum(acc[b]);
-        if (lane == 0) red[b][warp] = v;
-    }
+    for (int r = 0; r < RB; ++r)
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            const float v = sb::warp_sum(acc[r][b]);
+            if (lane == 0) red[r * NB + b][warp] = v;
+        }
     __syncthreads();
-    if (threadIdx.x < NB && threadIdx.x < nb) {
-        float t = 0.f;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[threadIdx.x][w];
-        M[(size_t)threadIdx.x * ldm + m] = t;
+    for (int e = threadIdx.x; e < RB * NB; e += blockDim.x) {
+        const int r = e / NB, b = e - r * NB;
+        if (m0 + r < nrows && b < nb) {
+            float t = 0.f;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[e][w];
+            M[(size_t)b * ldm + m0 + r] = t;
+        }
     }
 }
 
@@ -617,6 +647,22 @@ int launch_dm_batched(const CUtensorMap &map, int n_modes, int n_valid, const fl
     return sb::check_launch("dm_project_batched_kernel");
 }
 
+template <int NB, int RB>
+int launch_gemv_batched_rb(const float *R, int nrows, int ncols, int ldr, const float *S, int lds, int nb, float *M,
+                           int ldm, int vec2, cudaStream_t st) {
+    gemv_rows_batched_kernel<NB, RB><<<(nrows + RB - 1) / RB, 256, 0, st>>>(R, nrows, ncols, ldr, S, lds, nb, M, ldm,
+                                                                           vec2);
+    return sb::check_launch("gemv_rows_batched_kernel");
+}
+
+template <int NB>
+int launch_gemv_batched(int rb, const float *R, int nrows, int ncols, int ldr, const float *S, int lds, int nb,
+                        float *M, int ldm, int vec2, cudaStream_t st) {
+    if (rb == 4) return launch_gemv_batched_rb<NB, 4>(R, nrows, ncols, ldr, S, lds, nb, M, ldm, vec2, st);
+    if (rb == 1) return launch_gemv_batched_rb<NB, 1>(R, nrows, ncols, ldr, S, lds, nb, M, ldm, vec2, st);
+    return launch_gemv_batched_rb<NB, 2>(R, nrows, ncols, ldr, S, lds, nb, M, ldm, vec2, st);
+}
+
 template <int RS>
 int launch_dm_batched_rs(const CUtensorMap &map, int n_modes, int n_valid, const float *c, int ldc, int nb,
                          float sign, const int32_t *mask_idx, float *ph, long long phase_stride, cudaStream_t st) {
@@ -666,14 +712,18 @@ extern "C" int sb_modalrec_batched(const float *R, int n_modes, int n_slopes, in
         return sb::fail(SB_EINVAL, "sb_modalrec_batched: bad args");
     if (n_modes == 0) return SB_OK;
     cudaStream_t st = sb::as_stream(stream);
+    const int vec2 = (ldr % 2 == 0) && (lds % 2 == 0) && ((uintptr_t)R % 8 == 0) && ((uintptr_t)slopes % 8 == 0);
+    // rows per CTA: the SB_TUNE_MODALREC_BATCHED variant (2, 1, 4)
+    const int v = sb::tune_lookup(SB_TUNE_MODALREC_BATCHED, sb_tune_key(n_modes, n_slopes, n_batch));
+    const int rb = v == 1 ? 1 : (v == 2 ? 4 : 2);
     for (int b0 = 0; b0 < n_batch; b0 += 16) {
         const int nb = n_batch - b0 < 16 ? n_batch - b0 : 16;
         const float *S = slopes + (size_t)b0 * lds;
         float *M = modes + (size_t)b0 * ldm;
-        if (nb <= 4) gemv_rows_batched_kernel<4><<<n_modes, 256, 0, st>>>(R, n_slopes, ldr, S, lds, nb, M, ldm);
-        else if (nb <= 8) gemv_rows_batched_kernel<8><<<n_modes, 256, 0, st>>>(R, n_slopes, ldr, S, lds, nb, M, ldm);
-        else gemv_rows_batched_kernel<16><<<n_modes, 256, 0, st>>>(R, n_slopes, ldr, S, lds, nb, M, ldm);
-        const int rc = sb::check_launch("gemv_rows_batched_kernel");
+        int rc;
+        if (nb <= 4) rc = launch_gemv_batched<4>(rb, R, n_modes, n_slopes, ldr, S, lds, nb, M, ldm, vec2, st);
+        else if (nb <= 8) rc = launch_gemv_batched<8>(rb, R, n_modes, n_slopes, ldr, S, lds, nb, M, ldm, vec2, st);
+        else rc = launch_gemv_batched<16>(rb, R, n_modes, n_slopes, ldr, S, lds, nb, M, ldm, vec2, st);
         if (rc) return rc;
     }
     return SB_OK;

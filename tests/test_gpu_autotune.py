@@ -57,6 +57,33 @@ def test_dm_batched_variants_agree(cuda, nm, nv, B):
             assert torch.equal(o, outs[0]), v
 
 
+@pytest.mark.parametrize('nm,nsl,B', [(54, 496, 28), (500, 8618, 7), (37, 5003, 19)])
+def test_modalrec_batched_variants_bit_identical(cuda, nm, nsl, B):
+    """Rows per CTA change only which CTA computes a row: every variant gives
+    the same bits, within 1e-5 of float64 (odd slope counts take the scalar loads)."""
+    from specula_b200 import _lib
+    lib = _lib.load()
+    gen = torch.Generator(device='cuda').manual_seed(nm)
+    R = torch.randn((nm, nsl), device='cuda', generator=gen)
+    S = torch.randn((B, nsl), device='cuda', generator=gen)
+    key = lib.sb_tune_key(nm, nsl, B)
+    outs = []
+    try:
+        for v in range(lib.sb_tune_variants(_lib.SB_TUNE_MODALREC_BATCHED)):
+            _lib.call('sb_tune_set', _lib.SB_TUNE_MODALREC_BATCHED, key, v)
+            M = torch.full((B, nm), float('nan'), device='cuda')
+            _lib.call('sb_modalrec_batched', R.data_ptr(), nm, nsl, nsl, S.data_ptr(), nsl, B, M.data_ptr(), nm,
+                      torch.cuda.current_stream().cuda_stream)
+            torch.cuda.synchronize()
+            outs.append(M)
+    finally:
+        _lib.call('sb_tune_set', _lib.SB_TUNE_MODALREC_BATCHED, key, -1)
+    ref = S.double() @ R.double().t()
+    assert float((outs[0].double() - ref).abs().max()) <= 1e-5 * float(ref.abs().max())
+    for o in outs[1:]:
+        assert torch.equal(o, outs[0])
+
+
 def test_sh_fp32_variants_bit_identical(cuda):
     from specula_b200 import _lib
     from tests.test_gpu_sh_split_bf16 import _sh, _elt_case, _turbulent_phase

@@ -113,9 +113,11 @@ def test_batched_dm_projection_matches_single(cuda):
             _lib.call('sb_dm_project', IF.data_ptr(), nm, nv, ld, C[b].contiguous().data_ptr(), nm, -1.0,
                       idx.data_ptr(), ref.data_ptr(), st)
             assert torch.equal(out[b], ref), (B, b)
-        M = torch.empty((B, nm), device='cuda')
-        S = torch.randn((B, nv), device='cuda', generator=gen)
-        _lib.call('sb_modalrec_batched', IF.data_ptr(), nm, nv, ld, S.data_ptr(), nv, B, M.data_ptr(), nm, st)
-        ref = S.double() @ IF[:, :nv].double().t()
-        assert rel_max_err(M.cpu().numpy(), ref.cpu().numpy()) <= 1e-5
+        # reconstructor: slope rows of odd length (scalar loads) and padded to 16 bytes (vector loads)
+        for lds in (nv, ld):
+            M = torch.empty((B, nm), device='cuda')
+            S = torch.randn((B, lds), device='cuda', generator=gen)
+            _lib.call('sb_modalrec_batched', IF.data_ptr(), nm, nv, ld, S.data_ptr(), lds, B, M.data_ptr(), nm, st)
+            ref = S[:, :nv].double() @ IF[:, :nv].double().t()
+            assert rel_max_err(M.cpu().numpy(), ref.cpu().numpy()) <= 1e-5, (B, lds)
     _lib.call('sb_device_status')

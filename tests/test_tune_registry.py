@@ -9,6 +9,8 @@ def test_families_and_names():
     lib = _lib.load()
     assert lib.sb_tune_variants(_lib.SB_TUNE_DM_BATCHED) == 6
     assert lib.sb_tune_variants(_lib.SB_TUNE_SH_FP32) == 3
+    assert lib.sb_tune_variants(_lib.SB_TUNE_MODALREC_BATCHED) == 3
+    assert b'rows per CTA' in lib.sb_tune_variant_name(_lib.SB_TUNE_MODALREC_BATCHED, 2)
     assert lib.sb_tune_variants(99) == 0
     assert b'per pass' in lib.sb_tune_variant_name(_lib.SB_TUNE_DM_BATCHED, 3)
     assert lib.sb_tune_variant_name(_lib.SB_TUNE_SH_FP32, 7) == b''
