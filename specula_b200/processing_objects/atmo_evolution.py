@@ -2,7 +2,9 @@
 specula/processing_objects/atmo_evolution.py:14-323).
 
 Screens are synthesised once at construction (float64 on the device,
-specula_b200.lib.phasescreen) and cut into per-layer strips exactly as
+specula_b200.lib.phasescreen; read from / written to the reference's FITS
+cache in ``data_dir`` when one is given, or read from
+``user_defined_phasescreen``) and cut into per-layer strips exactly as
 atmo_evolution.py:164-226 does (sqrt(Cn2), de-mean, nm, odd layers
 flipped), then stored in float32.  Each step is one sb_atmo_evolve_inputs
 call: the seeing and wind inputs are read on the device (float64 CUDA
@@ -24,7 +26,9 @@ from specula_b200.base_processing_obj import BaseProcessingObj
 from specula_b200.base_value import BaseValue
 from specula_b200.connections import InputValue
 from specula_b200.data_objects.layer import Layer
+from specula_b200.lib import fits_io
 from specula_b200.lib.phasescreen import calc_phasescreen
+from specula_b200.lib.phasescreen_manager import phasescreens_manager
 
 
 def _cosdg_sindg(angle):
@@ -42,9 +46,7 @@ class AtmoEvolution(BaseProcessingObj):
         super().__init__(target_device_idx=target_device_idx, precision=precision)
         if make_cycle:
             raise NotImplementedError('make_cycle is not implemented')
-        if user_defined_phasescreen:
-            raise NotImplementedError('AtmoEvolution: user-defined screen files are not read by specula_b200; '
-                                      'assign .phasescreens instead')
+        self.user_defined_phasescreen = user_defined_phasescreen
         npdt = np.float32 if self.precision == 1 else np.float64
         self.simul_params = simul_params
         self.pixel_pupil = simul_params.pixel_pupil
@@ -98,15 +100,26 @@ class AtmoEvolution(BaseProcessingObj):
         self.compute()
 
     def compute(self):
-        """Square screens -> per-layer strips (atmo_evolution.py:142-252)."""
+        """Square screens -> per-layer strips (atmo_evolution.py:142-252).
+        With a non-empty ``data_dir`` the square screens go through the FITS
+        cache of specula_b200.lib.phasescreen_manager (the reference's file
+        names); an empty ``data_dir`` keeps them in memory only."""
         L = int(self.pixel_layer[0])
+        if self.user_defined_phasescreen:
+            self._user_defined_screen(L)
+            return
         if len(np.unique(np.atleast_1d(self.L0))) != 1:
             raise NotImplementedError('AtmoEvolution: per-layer L0 is not on the specula_b200 path')
         L0 = float(np.atleast_1d(self.L0)[0])
         per_square = self.pixel_square_phasescreens // L
         n_sq = int(math.ceil(self.n_phasescreens / per_square))
-        squares = [calc_phasescreen(L0, self.pixel_square_phasescreens, self.pixel_pitch, seed=self._seed + k,
-                                    device=self.device) for k in range(n_sq)]
+        if self.data_dir:
+            squares = phasescreens_manager([L0], self.pixel_square_phasescreens, self.pixel_pitch, self.data_dir,
+                                           precision=self.precision, seed=np.arange(self._seed, self._seed + n_sq),
+                                           device=self.device)
+        else:
+            squares = [calc_phasescreen(L0, self.pixel_square_phasescreens, self.pixel_pitch, seed=self._seed + k,
+                                        device=self.device) for k in range(n_sq)]
         strips = []
         for i in range(self.n_phasescreens):
             sq, k = divmod(i, per_square)
@@ -120,6 +133,27 @@ class AtmoEvolution(BaseProcessingObj):
         del squares
         self.phasescreens = strips
         self.phasescreens_sizes = [s.shape[1] for s in strips]
+        self._positions = torch.zeros(self.n_phasescreens, dtype=torch.float64, device=self.device)
+
+    def _user_defined_screen(self, L):
+        """One layer from a FITS screen (atmo_evolution.py:150-165): made at
+        least as tall as wide, de-meaned and converted to nm in the file's
+        precision, then stored as float32."""
+        if len(self.Cn2) > 1:
+            raise ValueError('The user-defined phasescreen works only if the total phasescreens are 1.')
+        scr = np.array(fits_io.getdata(self.user_defined_phasescreen))
+        if scr.ndim != 2:
+            raise ValueError('AtmoEvolution: the user-defined phasescreen must be a 2-D image')
+        if scr.shape[0] < scr.shape[1]:
+            scr = scr.T
+        if scr.shape[0] < L or scr.shape[1] < L + 1:
+            raise ValueError(f'AtmoEvolution: the user-defined phasescreen {scr.shape} is smaller than the '
+                             f'{L} x {L + 1} pixels a layer reads')
+        scr = scr - np.mean(scr)
+        scr = scr * (self.wavelengthInNm / (2 * np.pi))
+        strip = torch.as_tensor(np.ascontiguousarray(scr), device=self.device).to(self.dtype).contiguous()
+        self.phasescreens = [strip]
+        self.phasescreens_sizes = [strip.shape[1]]
         self._positions = torch.zeros(self.n_phasescreens, dtype=torch.float64, device=self.device)
 
     def set_last_position(self, last_position):

@@ -332,6 +332,31 @@ def make_psf_cases():
     return out
 
 
+PS_NAME_CASES = [
+    # (L0 list, dimension, pixel_pitch, seeds, precision)
+    ([25.0], 64, 0.05, [1, 2], 1),
+    ([30.5], 100, 0.0609375, [7], 0),
+    ([25.0, 40.0], 32, 0.125, [3, 4], 1),
+]
+
+
+def make_phasescreen_names():
+    """File names the reference's phasescreen cache writes
+    (lib/phasescreen_manager.py), captured through the harness fits stand-in."""
+    import tempfile
+    from astropy.io import fits
+    from specula.lib.phasescreen_manager import phasescreens_manager
+    out = []
+    for L0, dim, pitch, seeds, precision in PS_NAME_CASES:
+        with tempfile.TemporaryDirectory() as d:
+            fits._store.clear()
+            phasescreens_manager(np.array(L0), dim, pitch, d, xp=np, precision=precision, seed=np.array(seeds))
+            names = [os.path.basename(k) for k in fits._store]
+        out.append({'L0': L0, 'dimension': dim, 'pixel_pitch': pitch, 'seeds': seeds, 'precision': precision,
+                    'names': names})
+    return out
+
+
 def main():
     import subprocess
     # The reference binds its global precision at import time
@@ -349,6 +374,8 @@ def main():
     np.savez_compressed(os.path.join(HERE, 'chain_fp32.npz'), **chain)
     np.savez_compressed(os.path.join(HERE, 'zernike_fp32.npz'), **make_zernike_cases())
     np.savez_compressed(os.path.join(HERE, 'psf_fp32.npz'), **make_psf_cases())
+    with open(os.path.join(HERE, 'phasescreen_names.json'), 'w') as f:
+        json.dump(make_phasescreen_names(), f, indent=1)
     print('wrote', sorted(os.listdir(HERE)))
 
 
@@ -367,6 +394,11 @@ if __name__ == '__main__':
         import specula
         specula.init(-1, precision=1)
         np.savez_compressed(os.path.join(HERE, 'psf_fp32.npz'), **make_psf_cases())
+    elif '--psnames' in sys.argv:      # only the phase-screen cache file names
+        import specula
+        specula.init(-1, precision=1)
+        with open(os.path.join(HERE, 'phasescreen_names.json'), 'w') as f:
+            json.dump(make_phasescreen_names(), f, indent=1)
     elif '--zernike' in sys.argv:      # only the Zernike influence-function tables
         import specula
         specula.init(-1, precision=1)
