@@ -349,21 +349,28 @@ def bench_batched(dev, steps, cpu_budget_s):
     realisation its own step graph, reconstructor and mirror), CUDA events
     around `steps` steps of each after warm-up."""
     import torch
+    from specula_b200 import replicas
     from specula_b200.batched import BatchedScao, mc_groups
     t0 = time.perf_counter()
-    groups = mc_groups()
+    all_groups = mc_groups()
+    rank, ws = replicas.world()
+    # N > 1: every rank steps its share of every geometry group (no data-path collective)
+    groups = replicas.shard_groups(all_groups, ws, rank)
     sys_b = BatchedScao(groups, device_idx=dev.index)
     sys_b.start()
     sys_b.capture_plain()
     sys_b.capture()
     setup_s = time.perf_counter() - t0
-    n_real = sys_b.n_realisations
+    n_local = sys_b.n_realisations
+    n_real = int(replicas.sum_over_ranks(n_local, device=dev))
     st = torch.cuda.current_stream(dev)
 
     def timed(fn, n):
         for _ in range(3):
             fn()
         torch.cuda.synchronize(dev)
+        if ws > 1:
+            torch.distributed.barrier()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(st)
@@ -371,7 +378,7 @@ def bench_batched(dev, steps, cpu_budget_s):
             fn()
         e1.record(st)
         torch.cuda.synchronize(dev)
-        return e0.elapsed_time(e1) / n
+        return replicas.max_over_ranks(e0.elapsed_time(e1) / n, device=dev)
 
     plain_ms = timed(sys_b.replay_plain, steps)
     untuned_ms = timed(sys_b.replay, steps)
@@ -390,11 +397,12 @@ def bench_batched(dev, steps, cpu_budget_s):
     bf16_ms = timed(sys_b.replay, steps)
     _lib_status()
     by_size = {}
-    for (tmpl, reals) in groups:
+    for (tmpl, reals) in all_groups:
         key = f'{tmpl.n_lenses}x{tmpl.n_lenses}/{tmpl.pixel_pupil}px'
         by_size[key] = by_size.get(key, 0) + len(reals)
     out = {'workload': 'mc96_20x20_40x40_74x74_2wavelengths', 'realisations': n_real, 'split': by_size,
-           'groups': len(groups), 'steps_timed': steps,
+           'groups': len(all_groups), 'steps_timed': steps, 'n_gpus': ws,
+           'scaling': 'strong (the 96 realisations split across the GPUs)',
            'batched_ms_per_step': batched_ms, 'batched_untuned_ms_per_step': untuned_ms,
            'plain_ms_per_step': plain_ms,
            'batched_realisation_steps_per_s': n_real / (batched_ms / 1e3),
@@ -409,12 +417,12 @@ def bench_batched(dev, steps, cpu_budget_s):
            'graph': 'one CUDA graph per step for all 96 realisations: each geometry group on a stream of its own, '
                     'one batched launch per stage (atmosphere, propagation, SH, CCD, slopes, reconstructor, '
                     'integrator, mirror)'}
-    if cpu_budget_s > 0:
+    if cpu_budget_s > 0 and ws == 1:
         # the reference has no batched mode: the sum of per-realisation CPU runs,
         # sampled per geometry (steps/s of each size, weighted by its count)
         per = {}
         total_s = 0.0
-        for tmpl, reals in groups:
+        for tmpl, reals in all_groups:
             key = f'{tmpl.n_lenses}x{tmpl.n_lenses}'
             if key not in per:
                 v, n, dt = time_cpu_oracle(reals[0], budget_s=cpu_budget_s / 3, max_steps=50)
@@ -629,8 +637,8 @@ def run_b200(args):
         sh_forms = bench_sh_forms(dev)
 
     batched_mc = None
-    if world == 1 and not args.no_batched:
-        batched_mc = bench_batched(dev, steps=50, cpu_budget_s=0 if args.no_cpu_baseline else 15.0)
+    if not args.no_batched:
+        batched_mc = bench_batched(dev, steps=50, cpu_budget_s=0 if args.no_cpu_baseline or world > 1 else 15.0)
 
     if rank == 0:
         line = {'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': steps,
