@@ -127,6 +127,29 @@ int sb_sh_forward_split_bf16_batched(const sb_sh_plan *plan, const float *A, lon
                                      long long intensity_stride, int n_batch, void *scratch,
                                      size_t scratch_bytes, void *stream);
 
+/* Laser-guide-star SH (replaces the kernel branch of sh.py:382-394 with the
+ * kernel spectra of data_objects/convolution_kernel.py:260-276): per
+ * sub-aperture the unshifted |FFT|^2 of the tilted, zero-padded field on
+ * the full fft_size grid is correlated with the sub-aperture's sodium-spot
+ * kernel, psf = Re(IFFT(FFT(|F|^2) * K)) with an unnormalised inverse, then
+ * field stop, cut, rebin and photon normalisation as in sb_sh_forward.
+ * Tables (complex64, host-built): w_full_t[c][k] = exp(-2 pi i k c / N)
+ * (np_sub x N), w_dft[u][x] = exp(-2 pi i u x / N) (N x N), v_inv_t[u][a] =
+ * exp(+2 pi i (a + cutpixels/2) u / N) (N x cutsize); kernel_spectra: one
+ * N x N spectrum per lenslet, lenslet row-major.  Geometries: np_sub 8 with
+ * (N, cutsize, npx) in (16,12,6) (32,12,6) (16,14,8) (32,16,8). */
+typedef struct sb_sh_lgs_tables {
+    int fft_size;
+    const void *w_full_t;
+    const void *w_dft;
+    const void *v_inv_t;
+    const void *kernel_spectra;
+} sb_sh_lgs_tables;
+int sb_sh_lgs_supported(const sb_sh_plan *plan, int fft_size);
+int sb_sh_forward_lgs(const sb_sh_plan *plan, const sb_sh_lgs_tables *lgs, const float *A, const float *phase_nm,
+                      const float *A_norm, int n_norm, float photon_scale, float *intensity, void *scratch,
+                      size_t scratch_bytes, void *stream);
+
 /* replaces specula/lib/extrapolate_edge_pixel.py:4-28.
  * out[p] = phase[p] if src1[p] < 0; phase[src1[p]] if src2[p] < 0;
  * else 2*phase[src1[p]] - phase[src2[p]].  Tables from the host restatement

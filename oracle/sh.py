@@ -3,7 +3,10 @@
 Restates specula/processing_objects/sh.py (geometry solve :112-323, trigger
 :348-420, photon normalisation :422-428, tilt :469-477), specula/lib/toccd.py
 (CPU branch :33-63 with specula/lib/rebin.py), specula/lib/interp2d.py
-(:48-122, CPU branch) and specula/lib/extrapolate_edge_pixel*.py.
+(:48-122, CPU branch) and specula/lib/extrapolate_edge_pixel*.py; the
+laser-guide-star branch (sh.py:289-321 and :382-394) with the kernel maps
+of specula/data_objects/convolution_kernel.py:14-131 (lgs_map_sh) and
+:260-276 (process_kernels).
 
 Everything is vectorised over all sub-apertures at once; per-sub-aperture
 arithmetic follows the reference's dtype rules at ``precision=1`` (float32 /
@@ -309,8 +312,11 @@ class SHOracle:
                 raise ValueError('the interpolating geometry needs the pupil amplitude for its tables')
             self.tables = extrapol_tables(np.asarray(ef_A_for_tables), do_ext_2_pix=True)
 
-    def psf_cut(self, A, phase):
-        """Masked, cut focal-plane cube (n*n, cutsize, cutsize) before toccd."""
+    def psf_cut(self, A, phase, kernels_fft=None):
+        """Masked, cut focal-plane cube (n*n, cutsize, cutsize) before toccd.
+        ``kernels_fft`` (n*n, fft, fft): the LGS branch, where the unshifted
+        |FFT|^2 goes through fft2, times the kernel spectrum, and an
+        unnormalised inverse (sh.py:382-394) instead of the fftshift."""
         g = self.g
         A = np.asarray(A, dtype=self.dtype)
         phase = np.asarray(phase, dtype=self.dtype)
@@ -329,18 +335,22 @@ class SHOracle:
         wf3[:, :p, :p] = cube * self.tltf[np.newaxis]
         fp4 = np.fft.fft2(wf3, axes=(1, 2))
         psf = np.real(fp4 * np.conj(fp4))
-        psf = np.fft.fftshift(psf, axes=(1, 2))
+        if kernels_fft is None:
+            psf = np.fft.fftshift(psf, axes=(1, 2))
+        else:
+            spec = np.fft.fft2(psf, axes=(1, 2)) * np.asarray(kernels_fft)
+            psf = np.real(np.fft.ifft2(spec, axes=(1, 2), norm='forward')).astype(self.dtype)
         psf *= self.fp_mask[np.newaxis]
         c = g.cutpixels
         if c > 0:
             psf = psf[:, c // 2: -c // 2, c // 2: -c // 2]
         return psf
 
-    def forward(self, A, phase, S0, pixel_pitch):
+    def forward(self, A, phase, S0, pixel_pitch, kernels_fft=None):
         """Normalised detector-plane intensity (ccd_side x ccd_side)."""
         g = self.g
         n = g.n_lenses
-        psf = self.psf_cut(A, phase)
+        psf = self.psf_cut(A, phase, kernels_fft)
         cs = psf.shape[1]
         img = psf.reshape(n, n, cs, cs).transpose(0, 2, 1, 3).reshape(n * cs, n * cs)
         out = toccd(img, (g.ccd_side, g.ccd_side)).astype(self.dtype)
@@ -348,3 +358,58 @@ class SHOracle:
         phot = S0 * ((pixel_pitch ** 2) * np.sum(A))
         out *= (phot / out.sum())
         return out
+
+
+ASEC2RAD = 1.0 / RAD2ASEC
+
+
+def lgs_map_sh(nsh, diam, rl, zb, dz, profz, fwhmb, ps, ssp, theta=(0.0, 0.0)):
+    """Geometric sodium-beacon images behind an nsh x nsh lenslet array
+    (convolution_kernel.py:14-131, Gaussian radial profile, oversampling 1,
+    no pupil weighting), in float64.  Returns (nsh*nsh, ssp, ssp) with
+    index (lenslet column) * nsh + (lenslet row), as the reference's cube.
+
+    For lenslet centre s, focal-plane sample f (angle times zb) and the
+    on-axis point at distance dz from zb, the distance of the point seen from
+    s to the beacon axis (launched from rl towards zb with tip-tilt theta):
+    d2 = |f + dz (f - s)/zb - (b + dz e)|^2, e = (zb k + b - rl) / (zb + b_z - rl_z);
+    each sample sums profz * exp(-d2 / (2 sigma^2)) / (sigma pi sqrt 2)."""
+    s_ax = np.linspace(-diam / 2, diam / 2, nsh)
+    f_ax = np.linspace(-ssp * ps / 2, ssp * ps / 2, ssp) * ASEC2RAD * zb
+    sigma = fwhmb * ASEC2RAD * zb / (2 * np.sqrt(2 * np.log(2)))
+    b = np.array([theta[0] * ASEC2RAD * zb, theta[1] * ASEC2RAD * zb, 0.0])
+    axis = np.array([0.0, 0.0, float(zb)]) + b - np.broadcast_to(np.asarray(rl, dtype=np.float64), (3,))
+    e = axis / axis[2]
+    # full grid: rows = (lenslet row, sample row), columns = (lenslet column, sample column)
+    fx = np.tile(f_ax, nsh)[np.newaxis, :]
+    fy = np.tile(f_ax, nsh)[:, np.newaxis]
+    sx = np.repeat(s_ax, ssp)[np.newaxis, :]
+    sy = np.repeat(s_ax, ssp)[:, np.newaxis]
+    fmap = np.zeros((nsh * ssp, nsh * ssp))
+    gnorm = 1.0 / (sigma * np.pi * np.sqrt(2.0))
+    for z, w in zip(np.atleast_1d(dz), np.atleast_1d(profz)):
+        if w <= 0:
+            continue
+        dx = fx + z * (fx - sx) / zb - (b[0] + z * e[0])
+        dy = fy + z * (fy - sy) / zb - (b[1] + z * e[1])
+        dzz = z - (b[2] + z * e[2])
+        fmap += gnorm * w * np.exp(-(dx * dx + dy * dy + dzz * dzz) / (2 * sigma ** 2))
+    cube = fmap.reshape(nsh, ssp, nsh, ssp).transpose(2, 0, 1, 3).reshape(nsh * nsh, ssp, ssp)
+    return cube
+
+
+def lgs_kernel_spectra(real_kernels, nsh):
+    """Per lenslet (row-major) the spectrum the SH multiplies by
+    (convolution_kernel.py:260-276): each map normalised to unit sum and
+    transformed with the normalised inverse FFT; map (column c, row r) goes
+    to lenslet (r, c)."""
+    rk = np.asarray(real_kernels, dtype=np.float64)
+    out = np.zeros(rk.shape, dtype=np.complex128)
+    for c in range(nsh):
+        for r in range(nsh):
+            k = rk[c * nsh + r]
+            t = k.sum()
+            if t > 0:
+                k = k / t
+            out[r * nsh + c] = np.fft.ifft2(k)
+    return out

@@ -27,6 +27,10 @@ class ShPlan(C.Structure):
                 ('twiddle', fp), ('tilt', fp), ('fp_mask', fp), ('rebin', fp)]
 
 
+class ShLgsTables(C.Structure):
+    _fields_ = [('fft_size', C.c_int), ('w_full_t', vp), ('w_dft', vp), ('v_inv_t', vp), ('kernel_spectra', vp)]
+
+
 class CcdParams(C.Structure):
     _fields_ = [('n_pixels', C.c_int), ('frames_per_read', C.c_int), ('rate', C.c_float), ('qe', C.c_float),
                 ('bg_plus_dark', C.c_float), ('photon_noise', C.c_int), ('readout_noise', C.c_int),
@@ -96,6 +100,9 @@ SIGNATURES = {
     'sb_sh_forward_split_bf16_batched': (C.c_int, [C.POINTER(ShPlan), fp, C.c_longlong, fp, C.c_longlong, fp,
                                                    C.c_longlong, C.c_int, C.c_float, fp, C.c_longlong, C.c_int, vp,
                                                    C.c_size_t, vp]),
+    'sb_sh_lgs_supported': (C.c_int, [C.POINTER(ShPlan), C.c_int]),
+    'sb_sh_forward_lgs': (C.c_int, [C.POINTER(ShPlan), C.POINTER(ShLgsTables), fp, fp, fp, C.c_int, C.c_float, fp,
+                                    vp, C.c_size_t, vp]),
     'sb_tune_variants': (C.c_int, [C.c_int]),
     'sb_tune_variant_name': (C.c_char_p, [C.c_int, C.c_int]),
     'sb_tune_key': (C.c_ulonglong, [C.c_int, C.c_int, C.c_int]),

@@ -641,6 +641,181 @@ __global__ void __launch_bounds__(kTcThreads) sh_forward_tc_kernel(ShArgs a) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Laser-guide-star form (sh.py:382-394): the sub-aperture's unshifted
+// |FFT|^2 on the full N x N grid is correlated with its sodium-spot kernel
+// through FFTs, psf = Re(IFFT_unnormalised(FFT(|F|^2) * K)), then field stop,
+// cut and rebin as usual (the kernel is centred, so no fftshift).  One warp
+// per sub-aperture, every transform a small complex matrix product:
+//   G  = E Wf^T                       (P x N)      Wf[k][c] = e^{-2 pi i k c / N}
+//   I  = |Wf G|^2                     (N x N)
+//   H  = I W                          (N x N)      W[u][x]  = e^{-2 pi i u x / N}
+//   S  = (W H) .* K_s                 (N x N)      K_s: the kernel spectrum
+//   T  = S V^T                        (N x CS)     V[a][u]  = e^{+2 pi i (a + c0) u / N}
+//   Ic = Re(V T) .* field stop        (CS x CS)    c0 = cutpixels / 2
+// ---------------------------------------------------------------------------
+
+struct LgsArgs {
+    const float2 *wf_t;     // [P][N]: Wf transposed
+    const float2 *w;        // [N][N]
+    const float2 *v_t;      // [N][CS]: V transposed
+    const float2 *kspec;    // [n*n][N][N]
+};
+
+template <int N>
+__host__ __device__ constexpr int lgs_warps() { return N >= 32 ? 4 : 8; }
+
+template <int P, int N, int CS, int NPX>
+constexpr size_t lgs_smem_bytes() {
+    return ((size_t)P * N + (size_t)N * N + (size_t)N * CS + (size_t)P * P) * 8 + (size_t)CS * CS * 4 +
+           (size_t)NPX * CS * 4 + (size_t)lgs_warps<N>() * ((size_t)P * (P + 1) + 2 * (size_t)N * N) * 8;
+}
+
+template <int P, int N, int CS, int NPX>
+__global__ void __launch_bounds__(32 * lgs_warps<N>()) sh_forward_lgs_kernel(ShArgs a, LgsArgs g) {
+    static_assert(CS <= N && P <= N, "cut window and field inside the FFT grid");
+    constexpr int PE = P + 1;
+    constexpr int WPC = lgs_warps<N>();
+    extern __shared__ __align__(16) unsigned char lgs_smem[];
+    float2 *wf_t = reinterpret_cast<float2 *>(lgs_smem);   // [P][N]
+    float2 *w = wf_t + P * N;                               // [N][N]
+    float2 *v_t = w + N * N;                                // [N][CS]
+    float2 *tilt = v_t + N * CS;                            // [P][P]
+    float *mask = reinterpret_cast<float *>(tilt + P * P);  // [CS][CS]
+    float *R = mask + CS * CS;                              // [NPX][CS]
+    float2 *per_warp = reinterpret_cast<float2 *>(R + NPX * CS);
+    __shared__ float red[33];
+    for (int e = threadIdx.x; e < P * N; e += blockDim.x) wf_t[e] = g.wf_t[e];
+    for (int e = threadIdx.x; e < N * N; e += blockDim.x) w[e] = g.w[e];
+    for (int e = threadIdx.x; e < N * CS; e += blockDim.x) v_t[e] = g.v_t[e];
+    for (int e = threadIdx.x; e < P * P; e += blockDim.x) tilt[e] = a.tilt[e];
+    for (int e = threadIdx.x; e < CS * CS; e += blockDim.x) mask[e] = a.mask[e];
+    for (int e = threadIdx.x; e < NPX * CS; e += blockDim.x) R[e] = a.rebin[e];
+    __syncthreads();
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.y;
+    const int j = blockIdx.x * WPC + warp;
+    float2 *E = per_warp + (size_t)warp * (P * PE + 2 * N * N);
+    float2 *bufA = E + P * PE;
+    float2 *bufB = bufA + N * N;
+    float local = 0.f;
+    if (j < a.n) {
+        const size_t row0 = (size_t)i * P, col0 = (size_t)j * P;
+#pragma unroll
+        for (int e = lane; e < P * P; e += 32) {
+            const int r = e / P, c = e % P;
+            const size_t gi = (row0 + r) * (size_t)a.ld + col0 + c;
+            const float amp = a.A[gi];
+            const float phi = a.ph[gi] * a.k;
+            float sn, co;
+            sincosf(phi, &sn, &co);
+            const float re = co * amp, im = sn * amp;
+            const float2 t = tilt[e];
+            E[r * PE + c] = make_float2(re * t.x - im * t.y, re * t.y + im * t.x);
+        }
+        __syncwarp();
+        sb::warp_cgemm<P, N, P, PE, 1, N>(E, wf_t, lane, [&](int r, int k, float xr, float xi) {
+            bufA[r * N + k] = make_float2(xr, xi);
+        });
+        __syncwarp();
+        sb::warp_cgemm<N, N, P, 1, N, N>(wf_t, bufA, lane, [&](int u, int v, float xr, float xi) {
+            bufB[u * N + v] = make_float2(xr * xr + xi * xi, 0.f);
+        });
+        __syncwarp();
+        sb::warp_cgemm<N, N, N, N, 1, N>(bufB, w, lane, [&](int x, int v, float xr, float xi) {
+            bufA[x * N + v] = make_float2(xr, xi);
+        });
+        __syncwarp();
+        const float2 *ks = g.kspec + ((size_t)i * a.n + j) * (N * N);
+        sb::warp_cgemm<N, N, N, N, 1, N>(w, bufA, lane, [&](int u, int v, float xr, float xi) {
+            const float2 kk = __ldg(ks + u * N + v);
+            bufB[u * N + v] = make_float2(xr * kk.x - xi * kk.y, xr * kk.y + xi * kk.x);
+        });
+        __syncwarp();
+        sb::warp_cgemm<N, CS, N, N, 1, CS>(bufB, v_t, lane, [&](int u, int b, float xr, float xi) {
+            bufA[u * CS + b] = make_float2(xr, xi);
+        });
+        __syncwarp();
+        float *Ic = reinterpret_cast<float *>(bufB);
+        sb::warp_cgemm<CS, CS, N, 1, CS, CS>(v_t, bufA, lane, [&](int aa, int b, float xr, float xi) {
+            Ic[aa * CS + b] = xr * mask[aa * CS + b];
+        });
+        __syncwarp();
+        const int out_ld = a.n * NPX;
+        if constexpr (CS % NPX == 0) {
+            constexpr int BF = CS / NPX;
+            const float wgt = R[0] * R[0];
+#pragma unroll
+            for (int e = lane; e < NPX * NPX; e += 32) {
+                const int pp = e / NPX, q = e % NPX;
+                float acc = 0.f;
+#pragma unroll
+                for (int u = 0; u < BF; ++u)
+#pragma unroll
+                    for (int v = 0; v < BF; ++v) acc += Ic[(pp * BF + u) * CS + q * BF + v];
+                acc *= wgt;
+                a.out[((size_t)i * NPX + pp) * out_ld + (size_t)j * NPX + q] = acc;
+                local += acc;
+            }
+        } else {
+            float *H = reinterpret_cast<float *>(bufA);
+#pragma unroll
+            for (int e = lane; e < CS * NPX; e += 32) {
+                const int aa = e / NPX, q = e % NPX;
+                float acc = 0.f;
+#pragma unroll
+                for (int b = 0; b < CS; ++b) acc = fmaf(Ic[aa * CS + b], R[q * CS + b], acc);
+                H[e] = acc;
+            }
+            __syncwarp();
+#pragma unroll
+            for (int e = lane; e < NPX * NPX; e += 32) {
+                const int pp = e / NPX, q = e % NPX;
+                float acc = 0.f;
+#pragma unroll
+                for (int aa = 0; aa < CS; ++aa) acc = fmaf(R[pp * CS + aa], H[aa * NPX + q], acc);
+                a.out[((size_t)i * NPX + pp) * out_ld + (size_t)j * NPX + q] = acc;
+                local += acc;
+            }
+        }
+    }
+    const int bid = blockIdx.y * gridDim.x + blockIdx.x;
+    const float tot = sb::block_sum(local, red);
+    const int nblk = gridDim.x * gridDim.y;
+    const int chunk = (a.n_norm + nblk - 1) / nblk;
+    const int lo = bid * chunk;
+    const int hi = min(a.n_norm, lo + chunk);
+    float sa = 0.f;
+    for (int e = lo + threadIdx.x; e < hi; e += blockDim.x) sa += a.A_norm[e];
+    const float tota = sb::block_sum(sa, red);
+    if (threadIdx.x == 0) {
+        a.part_I[bid] = tot;
+        a.part_A[bid] = tota;
+    }
+}
+
+typedef void (*ShLgsKernel)(ShArgs, LgsArgs);
+
+struct ShLgsEntry {
+    ShLgsKernel fn;
+    int warps;
+    size_t smem;
+};
+
+// geometries with an LGS kernel: (np_sub, fft_size, cutsize, subap_npx)
+template <int P, int N, int CS, int NPX>
+ShLgsEntry lgs_entry() {
+    return {sh_forward_lgs_kernel<P, N, CS, NPX>, lgs_warps<N>(), lgs_smem_bytes<P, N, CS, NPX>()};
+}
+ShLgsEntry lgs_kernel(int p, int n_fft, int cs, int npx) {
+    if (p == 8 && n_fft == 16 && cs == 12 && npx == 6) return lgs_entry<8, 16, 12, 6>();
+    if (p == 8 && n_fft == 32 && cs == 12 && npx == 6) return lgs_entry<8, 32, 12, 6>();
+    if (p == 8 && n_fft == 16 && cs == 14 && npx == 8) return lgs_entry<8, 16, 14, 8>();
+    if (p == 8 && n_fft == 32 && cs == 16 && npx == 8) return lgs_entry<8, 32, 16, 8>();
+    return {nullptr, 0, 0};
+}
+
 typedef void (*ShKernel)(ShArgs);
 
 struct ShTcKernel {
@@ -856,6 +1031,67 @@ extern "C" int sb_sh_forward_batched(const sb_sh_plan *pl, const float *A, long 
         return sb::fail(SB_EINVAL, "sb_sh_forward_batched: intensity stride smaller than a frame");
     return sh_forward_impl("sb_sh_forward_batched", pl, A, A_stride, phase_nm, phase_stride, A_norm, A_norm_stride,
                            n_norm, photon_scale, intensity, intensity_stride, n_batch, scratch, scratch_bytes, stream);
+}
+
+extern "C" int sb_sh_lgs_supported(const sb_sh_plan *pl, int fft_size) {
+    return (pl && lgs_kernel(pl->np_sub, fft_size, pl->cutsize, pl->subap_npx).fn) ? 1 : 0;
+}
+
+extern "C" int sb_sh_forward_lgs(const sb_sh_plan *pl, const sb_sh_lgs_tables *lgs, const float *A,
+                                 const float *phase_nm, const float *A_norm, int n_norm, float photon_scale,
+                                 float *intensity, void *scratch, size_t scratch_bytes, void *stream) {
+    sb::clear_error();
+    if (!pl || !lgs || !A || !phase_nm || !A_norm || !intensity || !pl->tilt || !pl->fp_mask || !pl->rebin ||
+        !lgs->w_full_t || !lgs->w_dft || !lgs->v_inv_t || !lgs->kernel_spectra)
+        return sb::fail(SB_EINVAL, "sb_sh_forward_lgs: null pointer");
+    if (pl->n_lenses < 1 || n_norm < 0 || pl->field_ld < pl->n_lenses * pl->np_sub)
+        return sb::fail(SB_EINVAL, "sb_sh_forward_lgs: bad geometry");
+    const ShLgsEntry ke = lgs_kernel(pl->np_sub, lgs->fft_size, pl->cutsize, pl->subap_npx);
+    if (!ke.fn)
+        return sb::fail(SB_EUNSUPPORTED, "sb_sh_forward_lgs: no kernel for (np=%d, fft=%d, cut=%d, npx=%d)",
+                        pl->np_sub, lgs->fft_size, pl->cutsize, pl->subap_npx);
+    const size_t need = sb_sh_scratch_bytes(pl);
+    if (!scratch || scratch_bytes < need)
+        return sb::fail(SB_ESCRATCH, "sb_sh_forward_lgs: scratch needs %zu bytes, got %zu", need, scratch_bytes);
+    const dim3 grid((pl->n_lenses + ke.warps - 1) / ke.warps, pl->n_lenses, 1);
+    const int nb = grid.x * grid.y;
+    ShArgs a = {};
+    a.n = pl->n_lenses;
+    a.p = pl->np_sub;
+    a.cs = pl->cutsize;
+    a.npx = pl->subap_npx;
+    a.ld = pl->field_ld;
+    a.spc = ke.warps;
+    a.k = pl->phase_to_rad;
+    a.tilt = reinterpret_cast<const float2 *>(pl->tilt);
+    a.mask = pl->fp_mask;
+    a.rebin = pl->rebin;
+    a.A = A;
+    a.ph = phase_nm;
+    a.A_norm = A_norm;
+    a.n_norm = n_norm;
+    a.out = intensity;
+    a.part_I = static_cast<float *>(scratch);
+    a.part_A = static_cast<float *>(scratch) + nb;
+    a.nbp = nb;
+    LgsArgs g;
+    g.wf_t = static_cast<const float2 *>(lgs->w_full_t);
+    g.w = static_cast<const float2 *>(lgs->w_dft);
+    g.v_t = static_cast<const float2 *>(lgs->v_inv_t);
+    g.kspec = static_cast<const float2 *>(lgs->kernel_spectra);
+    cudaStream_t st = sb::as_stream(stream);
+    if (ke.smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(ke.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ke.smem);
+        if (e != cudaSuccess) return sb::fail(SB_ECUDA, "sb_sh_forward_lgs: smem attribute: %s", cudaGetErrorString(e));
+    }
+    ke.fn<<<grid, 32 * ke.warps, ke.smem, st>>>(a, g);
+    int rc = sb::check_launch("sh_forward_lgs_kernel");
+    if (rc) return rc;
+    const int n_out = pl->n_lenses * pl->subap_npx * pl->n_lenses * pl->subap_npx;
+    int nblk = (n_out + 255) / 256;
+    nblk = nblk > 592 ? 592 : nblk;
+    sh_normalize_kernel<<<dim3(nblk, 1), 256, 0, st>>>(a.part_I, a.part_A, nb, photon_scale, intensity, n_out);
+    return sb::check_launch("sh_normalize_kernel");
 }
 
 extern "C" int sb_sh_split_bf16_supported(const sb_sh_plan *pl) {

@@ -7,7 +7,8 @@ FITS (NASA/IAU FITS Standard 4.0): a header of 80-character ASCII cards
 ending with ``END``, padded with spaces to a multiple of 2880 bytes, then the
 image in big-endian order with NAXIS1 the fastest axis, padded with zeros to
 a multiple of 2880 bytes.  Reading follows IMAGE extensions (``ext``) and
-applies BSCALE / BZERO; writing makes a primary HDU.
+applies BSCALE / BZERO; writing makes a primary HDU and, with write_hdus,
+IMAGE extensions after it.
 """
 import os
 
@@ -113,18 +114,21 @@ def _card(key, value, comment=''):
     return text.ljust(CARD)
 
 
-def writeto(path, data, header=None, overwrite=False):
-    """Write ``data`` as the primary image of a new FITS file; ``header``:
-    extra (key, value) cards (keys of at most 8 characters)."""
-    if os.path.exists(path) and not overwrite:
-        raise OSError(f'FITS: {path} exists')
-    a = np.asarray(data)
-    if a.dtype not in _DTYPE_BITPIX:
-        raise ValueError(f'FITS: unsupported dtype {a.dtype}')
-    cards = [_card('SIMPLE', True, 'conforms to FITS standard'), _card('BITPIX', _DTYPE_BITPIX[a.dtype]),
-             _card('NAXIS', a.ndim)]
-    cards += [_card('NAXIS%d' % (i + 1), n) for i, n in enumerate(reversed(a.shape))]
-    cards.append(_card('EXTEND', True))
+def _hdu_bytes(data, header, primary):
+    if data is None:
+        a, bitpix, shape = None, 8, ()
+    else:
+        a = np.asarray(data)
+        if a.dtype not in _DTYPE_BITPIX:
+            raise ValueError(f'FITS: unsupported dtype {a.dtype}')
+        bitpix, shape = _DTYPE_BITPIX[a.dtype], a.shape
+    if primary:
+        cards = [_card('SIMPLE', True, 'conforms to FITS standard')]
+    else:
+        cards = [_card('XTENSION', 'IMAGE', 'image extension')]
+    cards += [_card('BITPIX', bitpix), _card('NAXIS', len(shape))]
+    cards += [_card('NAXIS%d' % (i + 1), n) for i, n in enumerate(reversed(shape))]
+    cards += [_card('EXTEND', True)] if primary else [_card('PCOUNT', 0), _card('GCOUNT', 1)]
     for k, v in (header or {}).items():
         if len(k) > 8:
             raise ValueError(f'FITS: keyword {k} longer than 8 characters')
@@ -132,10 +136,25 @@ def writeto(path, data, header=None, overwrite=False):
     cards.append('END'.ljust(CARD))
     head = ''.join(cards).encode('ascii')
     head += b' ' * (-len(head) % BLOCK)
+    if a is None:
+        return head
     body = np.ascontiguousarray(a).astype(a.dtype.newbyteorder('>'), copy=False).tobytes()
-    body += b'\0' * (-len(body) % BLOCK)
+    return head + body + b'\0' * (-len(body) % BLOCK)
+
+
+def write_hdus(path, hdus, overwrite=False):
+    """Write [(data or None, header dict), ...]: the first as the primary HDU,
+    the others as IMAGE extensions."""
+    if os.path.exists(path) and not overwrite:
+        raise OSError(f'FITS: {path} exists')
     tmp = path + '.tmp'
     with open(tmp, 'wb') as f:
-        f.write(head)
-        f.write(body)
+        for k, (data, header) in enumerate(hdus):
+            f.write(_hdu_bytes(data, header, primary=(k == 0)))
     os.replace(tmp, path)
+
+
+def writeto(path, data, header=None, overwrite=False):
+    """Write ``data`` as the primary image of a new FITS file; ``header``:
+    extra (key, value) cards (keys of at most 8 characters)."""
+    write_hdus(path, [(data, header)], overwrite=overwrite)

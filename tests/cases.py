@@ -21,7 +21,9 @@ SH_S0 = 7.0
 
 
 def rel_max_err(a, b):
-    """max |a - b| / max |b| (the intensity / slope tolerance metric)."""
-    a = np.asarray(a, dtype=np.float64)
-    b = np.asarray(b, dtype=np.float64)
+    """max |a - b| / max |b| (the intensity / slope tolerance metric; complex
+    arrays compare as complex numbers)."""
+    cplx = np.iscomplexobj(a) or np.iscomplexobj(b)
+    a = np.asarray(a, dtype=np.complex128 if cplx else np.float64)
+    b = np.asarray(b, dtype=np.complex128 if cplx else np.float64)
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))

@@ -29,6 +29,13 @@ def golden():
 
 
 @pytest.fixture(scope='session')
+def lgs():
+    """Laser-guide-star fixtures (make_golden.py --lgs)."""
+    with np.load(os.path.join(GOLDEN, 'lgs_fp32.npz')) as z:
+        return {k: z[k] for k in z.files}
+
+
+@pytest.fixture(scope='session')
 def cuda():
     import torch
     if not torch.cuda.is_available():

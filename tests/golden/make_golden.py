@@ -332,6 +332,79 @@ def make_psf_cases():
     return out
 
 
+# LGS SH cases: (name, pix, pitch, lam, pxscale / (lambda/d), n, npx, spot arcsec, launcher position or [],
+#                 sodium altitudes, beacon tip-tilt)
+LGS_CASES = [
+    ('lgs_gauss', 160, 0.05, 589.0, 1.0, 20, 6, 1.0, [], None, [0.0, 0.0]),
+    ('lgs_elong', 160, 0.05, 589.0, 0.5, 20, 6, 0.8, [4.0, -2.5, 0.0], (85e3, 95e3, 7), [0.1, -0.05]),
+]
+
+
+def make_lgs_cases():
+    """The reference SH with a laser launch telescope (sh.py:289-321, 382-394):
+    Gaussian kernel (no launcher position) and elongated sodium-profile kernel."""
+    import tempfile
+    from specula.processing_objects.sh import SH
+    from specula.data_objects.electric_field import ElectricField
+    from specula.data_objects.laser_launch_telescope import LaserLaunchTelescope
+    from specula.base_value import BaseValue
+    out = {}
+    cwd = os.getcwd()
+    for ci, (name, pix, pitch, lam, pxf, n, npx, spot, tel, sod, btt) in enumerate(LGS_CASES):
+        pxs = pxf * lam_over_d_arcsec(lam, pix * pitch / n)
+        mask, phase = sh_input(pix, seed=300 + ci)
+        llt = LaserLaunchTelescope(spot_size=spot, tel_position=tel, beacon_focus=90e3, beacon_tt=btt)
+        sh = SH(wavelengthInNm=lam, subap_wanted_fov=npx * pxs, sensor_pxscale=pxs, subap_on_diameter=n,
+                subap_npx=npx, fov_ovs_coeff=1.0, laser_launch_tel=llt, target_device_idx=-1, precision=1)
+        sh._noprints = True
+        ef = ElectricField(pix, pix, pitch, S0=7.0, target_device_idx=-1, precision=1)
+        ef.A[:] = mask
+        ef.phaseInNm[:] = phase
+        ef.generation_time = 1
+        sh.inputs['in_ef'].set(ef)
+        if sod is not None:
+            z = np.linspace(sod[0], sod[1], sod[2])
+            prof = np.exp(-0.5 * ((z - 90e3) / 3e3) ** 2)
+            prof /= prof.sum()
+            alt = BaseValue(value=z, target_device_idx=-1)
+            inten = BaseValue(value=prof, target_device_idx=-1)
+            alt.generation_time = inten.generation_time = 1
+            sh.inputs['sodium_altitude'].set(alt)
+            sh.inputs['sodium_intensity'].set(inten)
+            out[name + '/sodium_altitude'] = z
+            out[name + '/sodium_intensity'] = prof
+        with tempfile.TemporaryDirectory() as d:
+            os.chdir(d)                # the kernel object caches by file name in the working directory
+            try:
+                sh.setup()
+                sh.check_ready(1)
+                sh.trigger()
+                sh.post_trigger()
+            finally:
+                os.chdir(cwd)
+        out[name + '/A'] = mask
+        out[name + '/phase'] = phase
+        out[name + '/pxscale'] = np.float64(pxs)
+        out[name + '/intensity'] = np.array(sh.outputs['out_i'].i)
+        # a spot-check subset of the kernel maps (the full cubes are MBs)
+        out[name + '/kernel_index'] = LGS_KERNEL_INDEX
+        out[name + '/real_kernels'] = np.array(sh._kernelobj.real_kernels, dtype=np.float32)[LGS_KERNEL_INDEX]
+        out[name + '/fft_size'] = np.int64(sh._fft_size)
+        out[name + '/cutpixels'] = np.int64(sh._cutpixels)
+    # the reference's own golden LGS map (test/test_convolution_kernel.py:test_lgs_map_sh)
+    h = fits_min.read_hdus(os.path.join(REF, 'test', 'data', 'lgs_map_sh_ref.fits'))
+    ref = np.array(h[0][1], dtype=np.float64)
+    out['lgs_map_sh_ref/sum'] = np.float64(ref.sum())
+    out['lgs_map_sh_ref/blocks_ji'] = LGS_MAP_BLOCKS
+    out['lgs_map_sh_ref/blocks'] = np.stack([ref[j * 64:(j + 1) * 64, i * 64:(i + 1) * 64]
+                                             for j, i in LGS_MAP_BLOCKS]).astype(np.float32)
+    return out
+
+
+LGS_KERNEL_INDEX = np.array([0, 7, 19, 133, 210, 399])
+LGS_MAP_BLOCKS = np.array([[0, 0], [2, 7], [5, 5], [9, 1], [9, 9]])
+
+
 PS_NAME_CASES = [
     # (L0 list, dimension, pixel_pitch, seeds, precision)
     ([25.0], 64, 0.05, [1, 2], 1),
@@ -376,6 +449,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, 'psf_fp32.npz'), **make_psf_cases())
     with open(os.path.join(HERE, 'phasescreen_names.json'), 'w') as f:
         json.dump(make_phasescreen_names(), f, indent=1)
+    np.savez_compressed(os.path.join(HERE, 'lgs_fp32.npz'), **make_lgs_cases())
     print('wrote', sorted(os.listdir(HERE)))
 
 
@@ -394,6 +468,10 @@ if __name__ == '__main__':
         import specula
         specula.init(-1, precision=1)
         np.savez_compressed(os.path.join(HERE, 'psf_fp32.npz'), **make_psf_cases())
+    elif '--lgs' in sys.argv:          # only the LGS SH fixtures
+        import specula
+        specula.init(-1, precision=1)
+        np.savez_compressed(os.path.join(HERE, 'lgs_fp32.npz'), **make_lgs_cases())
     elif '--psnames' in sys.argv:      # only the phase-screen cache file names
         import specula
         specula.init(-1, precision=1)
