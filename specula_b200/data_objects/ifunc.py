@@ -2,9 +2,13 @@
 (mirrors specula/data_objects/ifunc.py:16-165).
 
 ``type_str='zernike'`` builds orthonormalised Zernike modes on the mask with
-specula_b200.lib.zernike (the reference's compute_zern_ifunc); 'zonal',
-'kl' and 'mixed' are not built here (the reference's 'kl' and 'mixed' raise
-NotImplementedError too): pass ``ifunc=`` explicitly.
+specula_b200.lib.zernike (the reference's compute_zern_ifunc); 'zonal'
+builds thin-plate-spline actuator functions with
+specula_b200.lib.zonal_ifunc on the object's device (the reference's
+compute_zonal_ifunc).  'kl' and 'mixed' raise NotImplementedError, as in the
+reference: a KL basis comes from
+specula_b200.lib.modal_basis.make_modal_base_from_ifs_fft (zonal functions
+plus an M2C), passed here as ``ifunc=``.
 """
 import numpy as np
 import torch
@@ -31,8 +35,18 @@ class IFunc(BaseDataObj):
                 from specula_b200.lib.zernike import compute_zern_ifunc
                 ifunc, mask = compute_zern_ifunc(npixels, nzern=nmodes, obsratio=obsratio, diaratio=diaratio,
                                                  mask=mask)
-            elif t in ('kl', 'mixed', 'zonal'):
-                raise NotImplementedError(f'IFunc type {type_str!r} is not built by specula_b200; pass ifunc=')
+            elif t == 'zonal':
+                from specula_b200.lib.zonal_ifunc import compute_zonal_ifunc
+                ifunc, mask = compute_zonal_ifunc(npixels, n_act, dtype=self.dtype, circ_geom=circ_geom,
+                                                  angle_offset=angle_offset, do_mech_coupling=do_mech_coupling,
+                                                  coupling_coeffs=coupling_coeffs, do_slaving=do_slaving,
+                                                  slaving_thr=slaving_thr,
+                                                  obsratio=0.0 if obsratio is None else obsratio,
+                                                  diaratio=1.0 if diaratio is None else diaratio, mask=mask,
+                                                  device=self.device)
+            elif t in ('kl', 'mixed'):
+                raise NotImplementedError(f'IFunc type {type_str!r}: build the basis with '
+                                          'specula_b200.lib.modal_basis.make_modal_base_from_ifs_fft')
             else:
                 raise ValueError(f'Invalid ifunc type {type_str}')
         ifunc = np.asarray(ifunc.cpu() if isinstance(ifunc, torch.Tensor) else ifunc)

@@ -405,6 +405,47 @@ LGS_KERNEL_INDEX = np.array([0, 7, 19, 133, 210, 399])
 LGS_MAP_BLOCKS = np.array([[0, 0], [2, 7], [5, 5], [9, 1], [9, 9]])
 
 
+# zonal influence functions: (name, dim, n_act, circ_geom, mech coupling, slaving, obsratio)
+ZONAL_CASES = [
+    ('sq64', 64, 8, False, False, False, 0.0),
+    ('circ128_slaved', 128, 8, True, False, True, 0.4),    # test/test_modal_basis.py:test_kl_basis_rms
+    ('sq32_coupled', 32, 5, False, True, False, 0.0),
+]
+# KL bases: (zonal case, diameter, r0, L0, zern_modes, oversampling)
+KL_CASES = [('sq64', 8.0, 0.2, 25.0, 0, 2), ('circ128_slaved', 8.0, 0.2, 25.0, 5, 1)]
+KL_STORED_MODES = 12
+
+
+def make_kl_cases():
+    """Zonal influence functions (lib/compute_zonal_ifunc.py) and KL bases
+    (lib/modal_base_generator.py:make_modal_base_from_ifs_fft) from the reference."""
+    from specula.lib.compute_zonal_ifunc import compute_zonal_ifunc
+    from specula.lib.modal_base_generator import make_modal_base_from_ifs_fft
+    out = {}
+    ifs = {}
+    for name, dim, n_act, circ, coup, slav, obs in ZONAL_CASES:
+        f, m, c = compute_zonal_ifunc(dim, n_act, xp=np, dtype=np.float32, circ_geom=circ, do_mech_coupling=coup,
+                                      do_slaving=slav, obsratio=obs, return_coordinates=True)
+        ifs[name] = (f, m)
+        sel = np.linspace(0, f.shape[0] - 1, min(6, f.shape[0])).astype(int)   # a spot-check subset
+        out['zonal/%s/n_act' % name] = np.int64(f.shape[0])
+        out['zonal/%s/ifs_index' % name] = sel
+        out['zonal/%s/ifs' % name] = np.asarray(f, dtype=np.float32)[sel]
+        out['zonal/%s/mask' % name] = np.asarray(m, dtype=np.float32)
+        out['zonal/%s/coords' % name] = np.asarray(c, dtype=np.float64)
+    for name, diam, r0, L0, nz, ovs in KL_CASES:
+        f, m = ifs[name]
+        kl, m2c, sv = make_modal_base_from_ifs_fft(m, diam, f, r0, L0, zern_modes=nz, oversampling=ovs, xp=np,
+                                                   dtype=np.float32)
+        key = 'kl/%s' % name
+        out[key + '/n_modes'] = np.int64(kl.shape[0])
+        out[key + '/kl_basis'] = np.asarray(kl, dtype=np.float32)[:KL_STORED_MODES]
+        out[key + '/m2c'] = np.asarray(m2c, dtype=np.float32)
+        out[key + '/S1'] = np.asarray(sv['S1'], dtype=np.float64)
+        out[key + '/S2'] = np.asarray(sv['S2'], dtype=np.float64)
+    return out
+
+
 PS_NAME_CASES = [
     # (L0 list, dimension, pixel_pitch, seeds, precision)
     ([25.0], 64, 0.05, [1, 2], 1),
@@ -450,6 +491,7 @@ def main():
     with open(os.path.join(HERE, 'phasescreen_names.json'), 'w') as f:
         json.dump(make_phasescreen_names(), f, indent=1)
     np.savez_compressed(os.path.join(HERE, 'lgs_fp32.npz'), **make_lgs_cases())
+    np.savez_compressed(os.path.join(HERE, 'kl_fp32.npz'), **make_kl_cases())
     print('wrote', sorted(os.listdir(HERE)))
 
 
@@ -468,6 +510,10 @@ if __name__ == '__main__':
         import specula
         specula.init(-1, precision=1)
         np.savez_compressed(os.path.join(HERE, 'psf_fp32.npz'), **make_psf_cases())
+    elif '--kl' in sys.argv:           # only the zonal influence functions and KL bases
+        import specula
+        specula.init(-1, precision=1)
+        np.savez_compressed(os.path.join(HERE, 'kl_fp32.npz'), **make_kl_cases())
     elif '--lgs' in sys.argv:          # only the LGS SH fixtures
         import specula
         specula.init(-1, precision=1)
