@@ -54,6 +54,9 @@ def parse():
                    help='skip the checkpointed loop-gradient leg (1000 ELT steps, finite-difference check)')
     p.add_argument('--gradient-only', action='store_true', help='run only the loop-gradient leg (one GPU)')
     p.add_argument('--no-batched', action='store_true', help='skip the batched Monte-Carlo leg')
+    p.add_argument('--profile-batched', action='store_true',
+                   help='set up the batched Monte-Carlo graph (split-BF16 SH, autotuned), then run one replay '
+                        'between cudaProfilerStart/Stop (for ncu --profile-from-start off) and exit')
     p.add_argument('--batched-only', action='store_true',
                    help='run only the 96-realisation batched Monte-Carlo leg (one GPU)')
     p.add_argument('--adjoint-only', action='store_true',
@@ -479,10 +482,46 @@ def bench_sh_forms(dev, reps=200):
         res['speedup_split_bf16_vs_fp32'] = res['fp32_us'] / res['split_bf16_us']
         res['fields'] = nb
         res['sub_apertures_per_field'] = cfg.n_lenses ** 2
+        if nb == 1:
+            res['lgs_us'] = _time_lgs(dev, cfg, loop, reps)
         out[name] = res
         del loop
     _lib_status()
     return out
+
+
+def _time_lgs(dev, cfg, loop, reps):
+    """Device time of the laser-guide-star SH (sb_sh_forward_lgs, Gaussian 1 arcsec spot) on the loop's field."""
+    import ctypes
+    import torch
+    from specula_b200 import _lib
+    from specula_b200.processing_objects.sh import SH
+    from specula_b200.data_objects.laser_launch_telescope import LaserLaunchTelescope
+    s0 = loop.sh
+    ef = s0._in_ef
+    sh = SH(wavelengthInNm=s0._wavelengthInNm, subap_wanted_fov=s0._subap_wanted_fov_arcsec,
+            sensor_pxscale=s0._sensor_pxscale_arcsec, subap_on_diameter=cfg.n_lenses, subap_npx=cfg.subap_npx,
+            fov_ovs_coeff=cfg.fov_ovs_coeff, laser_launch_tel=LaserLaunchTelescope(spot_size=1.0),
+            target_device_idx=dev.index)
+    sh.inputs['in_ef'].set(ef)
+    sh.setup()
+    st = torch.cuda.current_stream(dev)
+
+    def call():
+        _lib.call('sb_sh_forward_lgs', ctypes.byref(sh._plan), ctypes.byref(sh._lgs), ef.A.data_ptr(),
+                  ef.phaseInNm.data_ptr(), ef.A.data_ptr(), ef.A.numel(), sh._photon_scale,
+                  sh._out_i.i.data_ptr(), sh._scratch.data_ptr(), sh._scratch.numel(), st.cuda_stream)
+    for _ in range(5):
+        call()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(reps):
+        call()
+    e1.record(st)
+    torch.cuda.synchronize(dev)
+    return e0.elapsed_time(e1) / reps * 1e3
 
 
 def _lib_status():
@@ -669,8 +708,32 @@ def run_b200(args):
         dist.destroy_process_group()
 
 
+def profile_batched(dev):
+    """One replay of the batched graph bracketed for a profiler."""
+    import torch
+    from specula_b200.batched import BatchedScao, mc_groups
+    sys_b = BatchedScao(mc_groups(), device_idx=dev.index, dft='split_bf16')
+    sys_b.start()
+    sys_b.autotune()
+    sys_b.capture()
+    for _ in range(3):
+        sys_b.replay()
+    torch.cuda.synchronize(dev)
+    torch.cuda.cudart().cudaProfilerStart()
+    sys_b.replay()
+    torch.cuda.synchronize(dev)
+    torch.cuda.cudart().cudaProfilerStop()
+    _lib_status()
+
+
 def main():
     args = parse()
+    if args.profile_batched:
+        import torch
+        dev = torch.device('cuda', 0)
+        torch.cuda.set_device(dev)
+        profile_batched(dev)
+        return
     if args.batched_only:
         import torch
         dev = torch.device('cuda', 0)
