@@ -121,15 +121,55 @@ __device__ __forceinline__ float std_normal(uint32_t e, uint64_t frame, uint64_t
 // contiguous, n_per each; realisation b draws with photon_seeds[b] /
 // readout_seeds[b] and its own pixel index, so its frame equals what a
 // single-realisation launch with those seeds gives.
-__global__ void __launch_bounds__(256, 5) ccd_kernel(sb_ccd_params p, const float *__restrict__ in,
-                                                  float *__restrict__ integ, float *__restrict__ pix,
-                                                  const uint64_t *__restrict__ photon_seeds,
-                                                  const uint64_t *__restrict__ readout_seeds, int n_per) {
+//
+// With photon noise the block's 256 pixels are first ordered by sampler
+// branch (mean < 10: sequential inversion, else PTRS) through shared memory,
+// so that most warps run one branch with all lanes; each pixel's draw
+// depends only on its mean, index, frame and seeds, so the frame is the same
+// bit for bit as with pixels sampled in place.
+constexpr int kCcdThreads = 256;
+
+__device__ __forceinline__ float ccd_sample(const sb_ccd_params &p, float f, int e, uint64_t frame,
+                                            const uint64_t *photon_seeds, const uint64_t *readout_seeds, int n_per,
+                                            const float *logfact, double inv_gain, bool gain_pow2) {
+    uint32_t eloc = (uint32_t)e;
+    uint64_t pseed = p.photon_seed, rseed = p.readout_seed;
+    if (photon_seeds) {
+        const int b = e / n_per;
+        eloc = (uint32_t)(e - b * n_per);
+        pseed = photon_seeds[b];
+        rseed = readout_seeds[b];
+    }
+    if (p.photon_noise) {
+        double v = poisson_sample(f, eloc, frame, pseed, logfact);
+        if (p.readout_noise) v += truncf(std_normal(eloc, frame, rseed) * p.readout_level);
+        // ADU: round(x*g)+bias, clamp at 0, -bias, /g, back to the integer
+        // dtype of the Poisson draw (ccd.py:247-258)
+        double x = rint(v * (double)p.adu_gain) + (double)p.adu_bias;
+        x = x < 0.0 ? 0.0 : x;
+        x -= (double)p.adu_bias;
+        // a power-of-two gain (the default 8) divides exactly by its
+        // reciprocal; any other gain takes the float64 division
+        x = trunc(gain_pow2 ? x * inv_gain : x / (double)p.adu_gain);
+        if (p.dark_noise) x -= (double)p.dark_level;
+        return (float)x;
+    }
+    if (p.readout_noise) f = __fadd_rn(f, __fmul_rn(std_normal(eloc, frame, rseed), p.readout_level));
+    return f;
+}
+
+__global__ void __launch_bounds__(kCcdThreads, 4) ccd_kernel(sb_ccd_params p, const float *__restrict__ in,
+                                                          float *__restrict__ integ, float *__restrict__ pix,
+                                                          const uint64_t *__restrict__ photon_seeds,
+                                                          const uint64_t *__restrict__ readout_seeds, int n_per) {
     // frame bookkeeping lives on the device; every block reads it before the
     // last block to finish advances it (see the end of the kernel)
     volatile sb_ccd_state *vs = p.state;
     __shared__ unsigned int warps_done;
     __shared__ float logfact[32];
+    __shared__ int s_idx[kCcdThreads];
+    __shared__ float s_mean[kCcdThreads];
+    __shared__ int s_small[kCcdThreads / 32];
     if (threadIdx.x == 0) warps_done = 0u;
     if (threadIdx.x < 32) logfact[threadIdx.x] = c_logfact[threadIdx.x];
     const uint64_t frame = vs->frame_index;
@@ -137,52 +177,62 @@ __global__ void __launch_bounds__(256, 5) ccd_kernel(sb_ccd_params p, const floa
     const bool readout = nint >= p.frames_per_read;
     const double inv_gain = 1.0 / (double)p.adu_gain;
     const bool gain_pow2 = (__double_as_longlong((double)p.adu_gain) & 0x000FFFFFFFFFFFFFLL) == 0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     __syncthreads();
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < p.n_pixels; e += gridDim.x * blockDim.x) {
-        // integrated_i += i * (loop_dt * bandw)   (ccd.py:205)
-        float acc = __fadd_rn(integ[e], __fmul_rn(in[e], p.rate));
-        if (!readout) {
-            integ[e] = acc;
+    // block-uniform loop: every thread takes part in the shared-memory ordering
+    for (int base = blockIdx.x * kCcdThreads; base < p.n_pixels; base += gridDim.x * kCcdThreads) {
+        const int e = base + threadIdx.x;
+        const bool valid = e < p.n_pixels;
+        float f = 0.f;
+        if (valid) {
+            // integrated_i += i * (loop_dt * bandw)   (ccd.py:205)
+            const float acc = __fadd_rn(integ[e], __fmul_rn(in[e], p.rate));
+            if (!readout) {
+                integ[e] = acc;
+            } else {
+                f = acc;
+                if (p.qe != 1.0f) f = __fmul_rn(f, p.qe);                  // ccd.py:282-287
+                f = __fadd_rn(f, p.bg_plus_dark);                           // ccd.py:220-221
+            }
+        }
+        if (!readout) continue;
+        if (!p.photon_noise) {
+            if (valid) {
+                pix[e] = ccd_sample(p, f, e, frame, photon_seeds, readout_seeds, n_per, logfact, inv_gain, gain_pow2);
+                integ[e] = 0.0f;                                            // ccd.py:216
+            }
             continue;
         }
-        float f = acc;
-        if (p.qe != 1.0f) f = __fmul_rn(f, p.qe);                  // ccd.py:282-287
-        f = __fadd_rn(f, p.bg_plus_dark);                           // ccd.py:220-221
-        float outv;
-        uint32_t eloc = (uint32_t)e;
-        uint64_t pseed = p.photon_seed, rseed = p.readout_seed;
-        if (photon_seeds) {
-            const int b = e / n_per;
-            eloc = (uint32_t)(e - b * n_per);
-            pseed = photon_seeds[b];
-            rseed = readout_seeds[b];
+        // order by sampler branch: means below 10 first, then the rest
+        const bool small = valid && f < 10.0f;
+        const unsigned int bal = __ballot_sync(0xffffffffu, small);
+        if (lane == 0) s_small[warp] = __popc(bal);
+        __syncthreads();
+        int before = 0, total = 0;
+#pragma unroll
+        for (int w = 0; w < kCcdThreads / 32; ++w) {
+            const int c = s_small[w];
+            before += w < warp ? c : 0;
+            total += c;
         }
-        if (p.photon_noise) {
-            double v = poisson_sample(f, eloc, frame, pseed, logfact);
-            if (p.readout_noise) v += truncf(std_normal(eloc, frame, rseed) * p.readout_level);
-            // ADU: round(x*g)+bias, clamp at 0, -bias, /g, back to the
-            // integer dtype of the Poisson draw (ccd.py:247-258)
-            double x = rint(v * (double)p.adu_gain) + (double)p.adu_bias;
-            x = x < 0.0 ? 0.0 : x;
-            x -= (double)p.adu_bias;
-            // a power-of-two gain (the default 8) divides exactly by its
-            // reciprocal; any other gain takes the float64 division
-            x = trunc(gain_pow2 ? x * inv_gain : x / (double)p.adu_gain);
-            if (p.dark_noise) x -= (double)p.dark_level;
-            outv = (float)x;
-        } else {
-            if (p.readout_noise)
-                f = __fadd_rn(f, __fmul_rn(std_normal(eloc, frame, rseed), p.readout_level));
-            outv = f;
+        const int rank = __popc(bal & ((1u << lane) - 1u));
+        const int slot = small ? before + rank : total + (warp * 32 - before) + (lane - rank);
+        s_idx[slot] = valid ? e : -1;
+        s_mean[slot] = f;
+        __syncthreads();
+        const int ei = s_idx[threadIdx.x];
+        const float fi = s_mean[threadIdx.x];
+        __syncthreads();                        // the tables are refilled by the next pass
+        if (ei >= 0) {
+            pix[ei] = ccd_sample(p, fi, ei, frame, photon_seeds, readout_seeds, n_per, logfact, inv_gain, gain_pow2);
+            integ[ei] = 0.0f;                                               // ccd.py:216
         }
-        pix[e] = outv;
-        integ[e] = 0.0f;                                            // ccd.py:216
     }
     // the last warp to finish in the last block to finish advances the frame
     // state; warps that are done do not wait for the slower ones (the noise
     // sampling loops diverge)
     __syncwarp();
-    if ((threadIdx.x & 31) == 0) {
+    if (lane == 0) {
         const unsigned int nwarps = (blockDim.x + 31) >> 5;
         if (atomicAdd(&warps_done, 1u) == nwarps - 1) {
             __threadfence();
