@@ -183,9 +183,6 @@ class _Group:
             self.integ._ost[b * nm:(b + 1) * nm].copy_(lp.integ._ost)
             self.integ.out_comm.value[b * nm:(b + 1) * nm].copy_(lp.integ.out_comm.value)
 
-    def chain(self, b):
-        """Nothing left per realisation: the group's launches cover its whole step."""
-
     def group_ops(self):
         """The whole step of every realisation of the group, one launch each:
         atmosphere (every layer), propagation, SH, CCD, slopes, the shared
@@ -221,11 +218,10 @@ class _Group:
 
 
 class BatchedScao:
-    def __init__(self, groups, device_idx=0, streams=16, dft='fp32'):
+    def __init__(self, groups, device_idx=0, dft='fp32'):
         self.device = torch.device('cuda', device_idx)
         self.dft = dft
         self.groups = [_Group(t, reals, device_idx, dft=dft) for t, reals in groups]
-        self.n_streams = streams
         self.graph = None
         self.plain_graphs = None
 
@@ -283,41 +279,26 @@ class BatchedScao:
         torch.cuda.synchronize(self.device)
 
     def step_eager(self):
-        """One batched step without a graph (every chain, then the group launches)."""
+        """One batched step without a graph (every group's launches in turn)."""
         for g in self.groups:
-            for b in range(g.n):
-                g.chain(b)
             g.group_ops()
 
     def capture(self):
-        """The batched step of every realisation in one CUDA graph.  Each
-        realisation's chain runs on one of ``streams`` streams; each group's
-        batched launches run on a stream of their own as soon as that group's
-        chains are done, so groups overlap one another."""
+        """The batched step of every group in one CUDA graph, each group's
+        launches on a stream of its own so the groups overlap one another."""
         self.step_eager()
         torch.cuda.synchronize(self.device)
-        streams = [torch.cuda.Stream(self.device) for _ in range(self.n_streams)]
         gstreams = [torch.cuda.Stream(self.device) for _ in self.groups]
         cap = torch.cuda.Stream(self.device)
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g, stream=cap):
             main = torch.cuda.current_stream(self.device)
-            for s in streams + gstreams:
-                s.wait_stream(main)
-            k = 0
             for grp, gs in zip(self.groups, gstreams):
-                for b in range(grp.n):
-                    s = streams[k % self.n_streams]
-                    with torch.cuda.stream(s):
-                        grp.chain(b)
-                        ev = torch.cuda.Event()
-                        ev.record(s)
-                    gs.wait_event(ev)
-                    k += 1
+                gs.wait_stream(main)
                 with torch.cuda.stream(gs):
                     grp.group_ops()
-            for s in streams + gstreams:
-                main.wait_stream(s)
+            for gs in gstreams:
+                main.wait_stream(gs)
         torch.cuda.synchronize(self.device)
         self.graph = g
         return g

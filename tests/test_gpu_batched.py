@@ -45,7 +45,7 @@ def test_batched_graph_matches_plain_realisations(cuda, noise):
     plain = BatchedScao(_groups(noise))
     plain.start()
     plain.capture_plain()
-    bat = BatchedScao(_groups(noise), streams=3)
+    bat = BatchedScao(_groups(noise))
     bat.start()
     bat.capture()          # one eager batched step, as capture_plain() ran one per loop
     torch.cuda.synchronize()
@@ -72,7 +72,7 @@ def test_batched_split_bf16_matches_plain_fp32(cuda):
     plain = BatchedScao(_groups(False))
     plain.start()
     plain.capture_plain()
-    bat = BatchedScao(_groups(False), streams=3, dft='split_bf16')
+    bat = BatchedScao(_groups(False), dft='split_bf16')
     bat.start()
     bat.capture()
     torch.cuda.synchronize()
