@@ -473,6 +473,24 @@ typedef struct sb_prop_layer {
 int sb_propagate_on_axis(const sb_prop_layer *layers, int n_layers, int pupil,
                          float *A_out, float *phase_out, void *stream);
 
+/* General propagation (atmo_propagation.py:104-209 with lib/interp2d.py):
+ * like sb_propagate_on_axis, but a layer with yy / xx set is resampled at
+ * those per-output-pixel coordinates (row, column; clamped by the caller)
+ * by bilinear interpolation in float64 on its rows x cols grid, as the
+ * reference's Interp2D (off-axis sources, LGS cone effect, shifted, rotated
+ * or magnified layers); the interpolated values are rounded to float32
+ * before A *= ..., phase += ... */
+typedef struct sb_prop_sampling {
+    const float *A;         /* NULL: all ones                                 */
+    const float *phase;     /* NULL: all zeros                                */
+    int ld;
+    int rows, cols;         /* layer size                                     */
+    int top, left;          /* crop offsets (yy == NULL)                      */
+    const float *yy, *xx;   /* pupil x pupil sample coordinates, or NULL      */
+} sb_prop_sampling;
+int sb_propagate(const sb_prop_sampling *layers, int n_layers, int pupil, float *A_out, float *phase_out,
+                 void *stream);
+
 /* Batched propagation of realisations sharing the layer structure of the
  * SCAO chain: n_atm unit-amplitude turbulence layers (realisation b's layer k
  * at atm + b*atm_real_stride + k*atm_layer_stride), the pupil stop (stop_A,

@@ -31,6 +31,11 @@ class ShLgsTables(C.Structure):
     _fields_ = [('fft_size', C.c_int), ('w_full_t', vp), ('w_dft', vp), ('v_inv_t', vp), ('kernel_spectra', vp)]
 
 
+class PropSampling(C.Structure):
+    _fields_ = [('A', fp), ('phase', fp), ('ld', C.c_int), ('rows', C.c_int), ('cols', C.c_int), ('top', C.c_int),
+                ('left', C.c_int), ('yy', fp), ('xx', fp)]
+
+
 class CcdParams(C.Structure):
     _fields_ = [('n_pixels', C.c_int), ('frames_per_read', C.c_int), ('rate', C.c_float), ('qe', C.c_float),
                 ('bg_plus_dark', C.c_float), ('photon_noise', C.c_int), ('readout_noise', C.c_int),
@@ -103,6 +108,7 @@ SIGNATURES = {
     'sb_sh_lgs_supported': (C.c_int, [C.POINTER(ShPlan), C.c_int]),
     'sb_sh_forward_lgs': (C.c_int, [C.POINTER(ShPlan), C.POINTER(ShLgsTables), fp, fp, fp, C.c_int, C.c_float, fp,
                                     vp, C.c_size_t, vp]),
+    'sb_propagate': (C.c_int, [C.POINTER(PropSampling), C.c_int, C.c_int, fp, fp, vp]),
     'sb_tune_variants': (C.c_int, [C.c_int]),
     'sb_tune_variant_name': (C.c_char_p, [C.c_int, C.c_int]),
     'sb_tune_key': (C.c_ulonglong, [C.c_int, C.c_int, C.c_int]),

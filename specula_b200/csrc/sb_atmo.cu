@@ -453,6 +453,72 @@ extern "C" int sb_atmo_evolve_batched(const sb_atmo_layer *layers, const sb_atmo
     return SB_OK;
 }
 
+namespace {
+struct PropSampArgs {
+    sb_prop_sampling layer[SB_MAX_LAYERS];
+    int n, pupil;
+};
+
+// bilinear at (y, x) on the integer grid, in double (RegularGridInterpolator)
+__device__ __forceinline__ float bilinear(const float *v, int ld, int rows, int cols, double y, double x) {
+    int y0 = (int)floor(y), x0 = (int)floor(x);
+    y0 = max(0, min(y0, rows - 2));
+    x0 = max(0, min(x0, cols - 2));
+    const double fy = y - y0, fx = x - x0;
+    const size_t i00 = (size_t)y0 * ld + x0;
+    return (float)(v[i00] * ((1 - fy) * (1 - fx)) + v[i00 + 1] * ((1 - fy) * fx) + v[i00 + ld] * (fy * (1 - fx)) +
+                   v[i00 + ld + 1] * (fy * fx));
+}
+
+__global__ void __launch_bounds__(256) propagate_sampling_kernel(PropSampArgs a, float *__restrict__ A,
+                                                                 float *__restrict__ P) {
+    const int n = a.pupil * a.pupil;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const int r = e / a.pupil, c = e - r * a.pupil;
+        float amp = 1.0f, ph = 0.0f;                       // ElectricField.reset()
+        for (int k = 0; k < a.n; ++k) {
+            const sb_prop_sampling &l = a.layer[k];
+            if (l.yy) {
+                const double y = l.yy[e], x = l.xx[e];
+                if (l.A) amp = __fmul_rn(amp, bilinear(l.A, l.ld, l.rows, l.cols, y, x));
+                if (l.phase) ph = __fadd_rn(ph, bilinear(l.phase, l.ld, l.rows, l.cols, y, x));
+            } else {
+                const size_t g = (size_t)(r + l.top) * l.ld + (c + l.left);
+                if (l.A) amp = __fmul_rn(amp, l.A[g]);
+                if (l.phase) ph = __fadd_rn(ph, l.phase[g]);
+            }
+        }
+        A[e] = amp;
+        P[e] = ph;
+    }
+}
+}  // namespace
+
+extern "C" int sb_propagate(const sb_prop_sampling *layers, int n_layers, int pupil, float *A_out, float *phase_out,
+                            void *stream) {
+    sb::clear_error();
+    if (!layers || !A_out || !phase_out || n_layers < 0 || pupil < 1)
+        return sb::fail(SB_EINVAL, "sb_propagate: bad args");
+    if (n_layers > SB_MAX_LAYERS) return sb::fail(SB_ESHAPE, "sb_propagate: at most %d layers", SB_MAX_LAYERS);
+    PropSampArgs a;
+    for (int k = 0; k < n_layers; ++k) {
+        const sb_prop_sampling &l = layers[k];
+        if (l.yy || l.xx) {
+            if (!l.yy || !l.xx || l.rows < 2 || l.cols < 2 || l.ld < l.cols)
+                return sb::fail(SB_EINVAL, "sb_propagate: layer %d: bad sampling grid", k);
+        } else if (l.top < 0 || l.left < 0 || l.ld < pupil + l.left || (l.rows && l.rows < pupil + l.top)) {
+            return sb::fail(SB_EINVAL, "sb_propagate: layer %d: bad crop", k);
+        }
+        a.layer[k] = l;
+    }
+    a.n = n_layers;
+    a.pupil = pupil;
+    int nblk = (pupil * pupil + 255) / 256;
+    nblk = nblk > 1184 ? 1184 : nblk;
+    propagate_sampling_kernel<<<nblk, 256, 0, sb::as_stream(stream)>>>(a, A_out, phase_out);
+    return sb::check_launch("propagate_sampling_kernel");
+}
+
 extern "C" int sb_propagate_on_axis(const sb_prop_layer *layers, int n_layers, int pupil, float *A_out,
                                     float *phase_out, void *stream) {
     sb::clear_error();

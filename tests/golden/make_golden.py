@@ -446,6 +446,61 @@ def make_kl_cases():
     return out
 
 
+def make_prop_cases():
+    """AtmoPropagation with interpolated layers (atmo_propagation.py:104-209): an
+    LGS at 90 km (cone effect), an off-axis NGS, layers with a shift, a rotation
+    and a magnification, with the pupil stop and a ground layer cropped."""
+    from specula.processing_objects.atmo_propagation import AtmoPropagation
+    from specula.data_objects.layer import Layer
+    from specula.data_objects.pupilstop import Pupilstop
+    from specula.data_objects.source import Source
+    from specula.data_objects.simul_params import SimulParams
+    out = {}
+    P, pitch, L = 64, 0.05, 160
+    sp = SimulParams(pixel_pupil=P, pixel_pitch=pitch, time_step=0.001)
+    rng = np.random.default_rng(77)
+    specs = [  # height, shiftXY, rot, magnification, amplitude with zeros
+        (0.0, (0.0, 0.0), 0.0, 1.0, False),
+        (4000.0, (1.5, -2.0), 0.0, 1.0, False),
+        (9000.0, (0.0, 0.0), 10.0, 1.0, False),
+        (12000.0, (0.0, 0.0), 0.0, 1.3, True),
+    ]
+    layers = []
+    for k, (h, sh, rot, mag, holes) in enumerate(specs):
+        lay = Layer(L, L, pitch, h, shiftXYinPixel=sh, rotInDeg=rot, magnification=mag, target_device_idx=-1,
+                    precision=1)
+        ph = (rng.standard_normal((L, L)) * 50).astype(np.float32)
+        A = np.ones((L, L), np.float32)
+        if holes:
+            A[rng.random((L, L)) < 0.1] = 0.0
+        lay.phaseInNm[:] = ph
+        lay.A[:] = A
+        out['prop/layer%d/phase' % k] = ph
+        out['prop/layer%d/A' % k] = A
+        layers.append(lay)
+    pup = Pupilstop(sp, mask_diam=1.0, obs_diam=0.14, target_device_idx=-1, precision=1)
+    sources = {'lgs': Source([0.0, 0.0], 8.0, 589.0, height=90e3), 'ngs_off': Source([30.0, 45.0], 8.0, 750.0),
+               'lgs_off': Source([20.0, -60.0], 8.0, 589.0, height=90e3)}
+    prop = AtmoPropagation(sp, sources, target_device_idx=-1, precision=1)
+    prop.inputs['atmo_layer_list'].set(layers)
+    prop.inputs['common_layer_list'].set([pup])
+    for lay in layers:
+        lay.generation_time = 1
+    pup.generation_time = 1
+    prop.setup()
+    prop.check_ready(1)
+    prop.trigger()
+    prop.post_trigger()
+    for name in sources:
+        ef = prop.outputs['out_%s_ef' % name]
+        out['prop/%s/A' % name] = np.array(ef.A, dtype=np.float32)
+        out['prop/%s/phase' % name] = np.array(ef.phaseInNm, dtype=np.float32)
+    # the layer with holes had its phase at A == 0 set to the mean (in place)
+    out['prop/layer3/phase_after'] = np.array(layers[3].phaseInNm, dtype=np.float32)
+    out['prop/pupil_A'] = np.array(pup.A, dtype=np.float32)
+    return out
+
+
 PS_NAME_CASES = [
     # (L0 list, dimension, pixel_pitch, seeds, precision)
     ([25.0], 64, 0.05, [1, 2], 1),
@@ -492,6 +547,7 @@ def main():
         json.dump(make_phasescreen_names(), f, indent=1)
     np.savez_compressed(os.path.join(HERE, 'lgs_fp32.npz'), **make_lgs_cases())
     np.savez_compressed(os.path.join(HERE, 'kl_fp32.npz'), **make_kl_cases())
+    np.savez_compressed(os.path.join(HERE, 'prop_fp32.npz'), **make_prop_cases())
     print('wrote', sorted(os.listdir(HERE)))
 
 
@@ -510,6 +566,10 @@ if __name__ == '__main__':
         import specula
         specula.init(-1, precision=1)
         np.savez_compressed(os.path.join(HERE, 'psf_fp32.npz'), **make_psf_cases())
+    elif '--prop' in sys.argv:         # only the interpolated-layer propagation fixtures
+        import specula
+        specula.init(-1, precision=1)
+        np.savez_compressed(os.path.join(HERE, 'prop_fp32.npz'), **make_prop_cases())
     elif '--kl' in sys.argv:           # only the zonal influence functions and KL bases
         import specula
         specula.init(-1, precision=1)

@@ -57,7 +57,7 @@ def test_argument_validation_without_device(lib):
 STRUCTS = {'sb_sh_plan': _lib.ShPlan, 'sb_ccd_params': _lib.CcdParams, 'sb_slopec_plan': _lib.SlopecPlan,
            'sb_iir_plan': _lib.IirPlan, 'sb_atmo_layer': _lib.AtmoLayer, 'sb_prop_layer': _lib.PropLayer,
            'sb_atmo_inputs': _lib.AtmoInputs, 'sb_atmo_layer_inputs': _lib.AtmoLayerInputs,
-           'sb_sh_lgs_tables': _lib.ShLgsTables}
+           'sb_sh_lgs_tables': _lib.ShLgsTables, 'sb_prop_sampling': _lib.PropSampling}
 
 
 def test_struct_layouts_match_header(tmp_path):
