@@ -501,6 +501,55 @@ def make_prop_cases():
     return out
 
 
+def make_polc_cases():
+    """Modalrec with POLC (modalrec.py:126-156): pseudo-open-loop slopes
+    s + IM c, modes R s - c, without and with a projection matrix, over three
+    steps (the first without commands)."""
+    from specula.processing_objects.modalrec import Modalrec
+    from specula.data_objects.recmat import Recmat
+    from specula.data_objects.intmat import Intmat
+    from specula.data_objects.slopes import Slopes
+    from specula.base_value import BaseValue
+    out = {}
+    rng = np.random.default_rng(91)
+    ns, nm, npj = 40, 12, 9
+    R = rng.standard_normal((nm, ns)).astype(np.float32)
+    Pm = rng.standard_normal((npj, nm)).astype(np.float32)
+    out['polc/R'], out['polc/P'] = R, Pm
+    for case, proj in (('plain', None), ('proj', Pm)):
+        ncmd = nm if proj is None else npj
+        # slopes x commands, as the POLC product IM @ commands uses it
+        IM = rng.standard_normal((ns, ncmd)).astype(np.float32)
+        out['polc/%s/IM' % case] = IM
+        rec = Modalrec(recmat=Recmat(R.copy(), target_device_idx=-1, precision=1),
+                       projmat=None if proj is None else Recmat(proj.copy(), target_device_idx=-1, precision=1),
+                       intmat=Intmat(IM.copy(), target_device_idx=-1, precision=1), polc=True,
+                       target_device_idx=-1, precision=1)
+        sl = Slopes(ns, target_device_idx=-1, precision=1)
+        cmd = BaseValue(target_device_idx=-1)
+        rec.inputs['in_slopes'].set(sl)
+        rec.inputs['in_commands'].set(cmd)
+        for t in range(3):
+            s = rng.standard_normal(ns).astype(np.float32)
+            sl.slopes[:] = s
+            sl.generation_time = t + 1
+            if t > 0:
+                c = rng.standard_normal(ncmd).astype(np.float32)
+                cmd.value = c.copy()
+                cmd.generation_time = t + 1
+                out['polc/%s/commands%d' % (case, t)] = c
+            if t == 0:
+                rec.setup()
+            rec.check_ready(t + 1)
+            rec.trigger()
+            rec.post_trigger()
+            out['polc/%s/slopes_in%d' % (case, t)] = s
+            out['polc/%s/slopes_after%d' % (case, t)] = np.array(sl.slopes, dtype=np.float32)
+            out['polc/%s/modes%d' % (case, t)] = np.array(rec.modes.value, dtype=np.float32)
+            out['polc/%s/pol%d' % (case, t)] = np.array(rec.pseudo_ol_modes.value, dtype=np.float32)
+    return out
+
+
 PS_NAME_CASES = [
     # (L0 list, dimension, pixel_pitch, seeds, precision)
     ([25.0], 64, 0.05, [1, 2], 1),
@@ -548,6 +597,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, 'lgs_fp32.npz'), **make_lgs_cases())
     np.savez_compressed(os.path.join(HERE, 'kl_fp32.npz'), **make_kl_cases())
     np.savez_compressed(os.path.join(HERE, 'prop_fp32.npz'), **make_prop_cases())
+    np.savez_compressed(os.path.join(HERE, 'polc_fp32.npz'), **make_polc_cases())
     print('wrote', sorted(os.listdir(HERE)))
 
 
@@ -566,6 +616,10 @@ if __name__ == '__main__':
         import specula
         specula.init(-1, precision=1)
         np.savez_compressed(os.path.join(HERE, 'psf_fp32.npz'), **make_psf_cases())
+    elif '--polc' in sys.argv:         # only the POLC reconstructor fixtures
+        import specula
+        specula.init(-1, precision=1)
+        np.savez_compressed(os.path.join(HERE, 'polc_fp32.npz'), **make_polc_cases())
     elif '--prop' in sys.argv:         # only the interpolated-layer propagation fixtures
         import specula
         specula.init(-1, precision=1)
