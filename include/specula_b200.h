@@ -254,7 +254,8 @@ int sb_modalrec(const float *R, int n_modes, int n_slopes, int ldr, const float 
  * Integrator — replaces specula/processing_objects/iir_filter.py:100-211
  * for the 2-tap filters built by iir_filter_data.py:264-292 (num=[0,g],
  * den=[-ff,1]); state is (n x total) with total = ceil(delay)+1, ist/ost are
- * (n x 2).  Output = state[:, delay] (integer delay) or the fractional mix.
+ * (n x 2, or n x n_num / n x n_den for general filters of up to 8 taps).
+ * Output = state[:, delay] (integer delay) or the fractional mix.
  * ---------------------------------------------------------------------- */
 typedef struct sb_iir_plan {
     int n;
@@ -273,6 +274,8 @@ typedef struct sb_iir_plan {
                                for integer delays >= 1; NULL to skip.  Lets a
                                caller start the next step's DM projection
                                before that step's integrator runs.          */
+    int n_num, n_den;       /* taps of num / den (and of ist / ost), 2..8;
+                               0 means 2 (the integrator)                    */
 } sb_iir_plan;
 
 int sb_integrator(const sb_iir_plan *plan, const float *delta, float *out, void *stream);

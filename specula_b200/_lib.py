@@ -52,7 +52,8 @@ class SlopecPlan(C.Structure):
 class IirPlan(C.Structure):
     _fields_ = [('n', C.c_int), ('total', C.c_int), ('shift', C.c_int), ('k_out', C.c_int),
                 ('rem', C.c_float), ('one_minus_rem', C.c_float),
-                ('num', fp), ('den', fp), ('ist', fp), ('ost', fp), ('state', fp), ('out_next', fp)]
+                ('num', fp), ('den', fp), ('ist', fp), ('ost', fp), ('state', fp), ('out_next', fp),
+                ('n_num', C.c_int), ('n_den', C.c_int)]
 
 
 class AtmoLayer(C.Structure):

@@ -42,9 +42,81 @@ __global__ void __launch_bounds__(256) gemv_rows_kernel(const float *__restrict_
     if (threadIdx.x == 0) y[m] = acc;
 }
 
-// 2-tap IIR for mode e, operation order of iir_filter.py:100-211 (no FMA
-// contraction, so float32 results match the reference bit for bit)
+constexpr int kIirMaxTaps = 8;
+
+// sum of t float32 terms in NumPy's order along a row: sequential below 8
+// terms, the 8-accumulator pairwise tree at exactly 8
+__device__ __forceinline__ float numpy_row_sum(const float (&v)[kIirMaxTaps], int t) {
+    if (t == 8)
+        return __fadd_rn(__fadd_rn(__fadd_rn(v[0], v[1]), __fadd_rn(v[2], v[3])),
+                         __fadd_rn(__fadd_rn(v[4], v[5]), __fadd_rn(v[6], v[7])));
+    float acc = 0.f;
+#pragma unroll
+    for (int k = 0; k < kIirMaxTaps; ++k)
+        if (k < t) acc = __fadd_rn(acc, v[k]);
+    return acc;
+}
+
+// general IIR filter (n_num / n_den taps) for mode e: returns the new output
+// and updates ist / ost in place (iir_filter.py:169-197)
+__device__ __forceinline__ float iir_taps(const sb_iir_plan &p, int e, float delta) {
+    const int ni = p.n_num, no = p.n_den;
+    float *ist = p.ist + (size_t)ni * e, *ost = p.ost + (size_t)no * e;
+    const float *num = p.num + (size_t)ni * e, *den = p.den + (size_t)no * e;
+    float is[kIirMaxTaps], os[kIirMaxTaps], prod[kIirMaxTaps];
+#pragma unroll
+    for (int k = 0; k < kIirMaxTaps; ++k) {
+        is[k] = (k + 1 < ni) ? ist[k + 1] : 0.f;       // delay the vectors (shift left, last column 0)
+        os[k] = (k + 1 < no) ? ost[k + 1] : 0.f;
+    }
+#pragma unroll
+    for (int k = 0; k < kIirMaxTaps; ++k)
+        if (k == ni - 1) is[k] = delta;                // new input
+    const float factor = __fdiv_rn(1.0f, den[no - 1]);
+#pragma unroll
+    for (int k = 0; k < kIirMaxTaps; ++k) prod[k] = k < ni ? __fmul_rn(num[k], is[k]) : 0.f;
+    const float num_c = numpy_row_sum(prod, ni);
+#pragma unroll
+    for (int k = 0; k < kIirMaxTaps; ++k) prod[k] = k < no - 1 ? __fmul_rn(den[k], os[k]) : 0.f;
+    const float den_c = numpy_row_sum(prod, no - 1);
+    const float y = __fmul_rn(factor, __fsub_rn(num_c, den_c));
+#pragma unroll
+    for (int k = 0; k < kIirMaxTaps; ++k) {
+        if (k < ni) ist[k] = is[k];
+        if (k < no) ost[k] = (k == no - 1) ? y : os[k];
+    }
+    return y;
+}
+
+// IIR for mode e, operation order of iir_filter.py:100-211 (no FMA
+// contraction, so float32 results match the reference bit for bit); the
+// 2-tap integrator has its own straight-line path
 __device__ __forceinline__ void iir_update(const sb_iir_plan &p, int e, float delta, float *__restrict__ out) {
+    if (p.n_num != 2 || p.n_den != 2) {
+        constexpr int kMaxTotal = 8;
+        float *st = p.state + (size_t)e * p.total;
+        float sv[kMaxTotal];
+        const int total = p.total;
+#pragma unroll
+        for (int k = 0; k < kMaxTotal; ++k) sv[k] = k < total ? st[k] : 0.f;
+        if (p.shift) {
+#pragma unroll
+            for (int k = kMaxTotal - 1; k >= 1; --k) sv[k] = sv[k - 1];
+        }
+        sv[0] = iir_taps(p, e, delta);
+        float o;
+        if (p.rem == 0.f) {
+            o = sv[p.k_out];
+        } else {
+            o = __fadd_rn(__fmul_rn(p.rem, sv[p.k_out]), __fmul_rn(p.one_minus_rem, sv[p.k_out - 1]));
+        }
+#pragma unroll
+        for (int k = 0; k < kMaxTotal; ++k)
+            if (k < total) st[k] = sv[k];
+        out[e] = o;
+        if (p.out_next) p.out_next[e] = sv[p.k_out - 1];
+        return;
+    }
     // every load is issued before any store (the arrays may alias as far as
     // the compiler knows), so the update costs two memory round trips
     constexpr int kMaxTotal = 8;
@@ -542,11 +614,27 @@ extern "C" int sb_modalrec(const float *R, int n_modes, int n_slopes, int ldr, c
     return sb::check_launch("gemv_rows_kernel");
 }
 
+namespace {
+// copy of the plan with the tap counts filled in (0 means the 2-tap integrator)
+int iir_taps_checked(const sb_iir_plan *p, sb_iir_plan *q, const char *who) {
+    *q = *p;
+    if (q->n_num == 0) q->n_num = 2;
+    if (q->n_den == 0) q->n_den = 2;
+    if (q->n_num < 1 || q->n_num > kIirMaxTaps || q->n_den < 1 || q->n_den > kIirMaxTaps)
+        return sb::fail(SB_EINVAL, "%s: filters of 1 to %d taps", who, kIirMaxTaps);
+    return SB_OK;
+}
+}  // namespace
+
 extern "C" int sb_modalrec_integrator(const float *R, int n_modes, int n_slopes, int ldr, const float *slopes,
-                                      float *modes, const sb_iir_plan *p, float *out, void *stream) {
+                                      float *modes, const sb_iir_plan *plan, float *out, void *stream) {
     sb::clear_error();
-    if (!R || !slopes || !modes || !p || !out || n_modes < 0 || n_slopes < 0 || ldr < n_slopes)
+    if (!R || !slopes || !modes || !plan || !out || n_modes < 0 || n_slopes < 0 || ldr < n_slopes)
         return sb::fail(SB_EINVAL, "sb_modalrec_integrator: bad args");
+    sb_iir_plan q;
+    const int trc = iir_taps_checked(plan, &q, "sb_modalrec_integrator");
+    if (trc) return trc;
+    const sb_iir_plan *p = &q;
     if (!p->num || !p->den || !p->ist || !p->ost || !p->state)
         return sb::fail(SB_EINVAL, "sb_modalrec_integrator: null integrator state");
     if (p->n != n_modes) return sb::fail(SB_ESHAPE, "sb_modalrec_integrator: %d filters for %d modes", p->n, n_modes);
@@ -564,10 +652,14 @@ extern "C" int sb_modalrec_integrator(const float *R, int n_modes, int n_slopes,
     return sb::check_launch("gemv_iir_kernel");
 }
 
-extern "C" int sb_integrator(const sb_iir_plan *p, const float *delta, float *out, void *stream) {
+extern "C" int sb_integrator(const sb_iir_plan *plan, const float *delta, float *out, void *stream) {
     sb::clear_error();
-    if (!p || !delta || !out || !p->num || !p->den || !p->ist || !p->ost || !p->state)
+    if (!plan || !delta || !out || !plan->num || !plan->den || !plan->ist || !plan->ost || !plan->state)
         return sb::fail(SB_EINVAL, "sb_integrator: null pointer");
+    sb_iir_plan q;
+    const int trc = iir_taps_checked(plan, &q, "sb_integrator");
+    if (trc) return trc;
+    const sb_iir_plan *p = &q;
     if (p->n < 0 || p->total < 1 || p->total > 8 || p->k_out < 0 || p->k_out >= p->total ||
         (p->rem != 0.f && p->k_out < 1))
         return sb::fail(SB_EINVAL, "sb_integrator: bad state layout (delay up to 7 frames)");

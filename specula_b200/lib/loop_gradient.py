@@ -41,6 +41,8 @@ class LoopGradient:
         delay = integ.delay
         if delay != int(delay):
             raise NotImplementedError('LoopGradient: fractional integrator delays are not supported')
+        if integ._n_num != 2 or integ._n_den != 2:
+            raise NotImplementedError('LoopGradient: the loop filter must be a 2-tap integrator')
         self.loop = loop
         self.T = int(n_steps)
         self.K = int(checkpoint_every)

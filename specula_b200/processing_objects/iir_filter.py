@@ -1,8 +1,10 @@
 """IIR temporal filter on the B200 (mirrors specula/processing_objects/iir_filter.py:9-211)
-for 2-tap filters (integrators with forgetting factor).  One sb_integrator
-call per step performs the state shift of prepare_trigger, the filter update
-of trigger_code and the delayed output of post_trigger, with the reference's
-float32 operation order (bit-exact)."""
+for filters of up to 8 numerator / denominator taps (the 2-tap integrator
+with forgetting factor has a straight-line path).  One sb_integrator call
+per step performs the state shift of prepare_trigger, the filter update of
+trigger_code and the delayed output of post_trigger, with the reference's
+float32 operation order, including NumPy's summation order of the tap
+products (bit-exact)."""
 import math
 
 import numpy as np
@@ -27,16 +29,18 @@ class IirFilter(BaseProcessingObj):
         self.simul_params = simul_params
         self.time_step = simul_params.time_step
         self.iir_filter_data = iir_filter_data
-        if iir_filter_data.num_np.shape[1] != 2 or iir_filter_data.den_np.shape[1] != 2:
-            raise NotImplementedError('IirFilter: only 2-tap filters (integrators) are on the specula_b200 path')
+        self._n_num = iir_filter_data.num_np.shape[1]
+        self._n_den = iir_filter_data.den_np.shape[1]
+        if not (1 <= self._n_num <= 8 and 1 <= self._n_den <= 8):
+            raise NotImplementedError('IirFilter: filters of up to 8 taps are on the specula_b200 path')
         self.delay = delay if delay is not None else 0
         if int(np.ceil(self.delay)) + 1 > 8:
             raise NotImplementedError('IirFilter: delays above 7 frames are not on the specula_b200 path')
         self._n = iir_filter_data.nfilter
         self._total_length = int(np.ceil(self.delay)) + 1
         self.state = torch.zeros((self._n, self._total_length), dtype=self.dtype, device=self.device)
-        self._ist = torch.zeros((self._n, 2), dtype=self.dtype, device=self.device)
-        self._ost = torch.zeros((self._n, 2), dtype=self.dtype, device=self.device)
+        self._ist = torch.zeros((self._n, self._n_num), dtype=self.dtype, device=self.device)
+        self._ost = torch.zeros((self._n, self._n_den), dtype=self.dtype, device=self.device)
         self.out_comm = BaseValue(value=torch.zeros(self._n, dtype=self.dtype, device=self.device),
                                   target_device_idx=target_device_idx)
         self.inputs['delta_comm'] = InputValue(type=BaseValue)
@@ -56,7 +60,8 @@ class IirFilter(BaseProcessingObj):
         self._plan = _lib.IirPlan(n=self._n, total=self._total_length, shift=int(self.delay > 0), k_out=k_out,
                                   rem=float(np.float32(rem)), one_minus_rem=float(np.float32(1 - rem)),
                                   num=self._num.data_ptr(), den=self._den.data_ptr(), ist=self._ist.data_ptr(),
-                                  ost=self._ost.data_ptr(), state=self.state.data_ptr(), out_next=None)
+                                  ost=self._ost.data_ptr(), state=self.state.data_ptr(), out_next=None,
+                                  n_num=self._n_num, n_den=self._n_den)
 
     @property
     def next_output_available(self):

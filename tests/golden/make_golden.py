@@ -501,6 +501,50 @@ def make_prop_cases():
     return out
 
 
+# general IIR filters: (name, n filters, num taps, den taps, delay, orders shorter than the taps in row 0)
+IIR_CASES = [('taps3x3_d2', 5, 3, 3, 2.0, False), ('taps4x2_d1.5', 4, 4, 2, 1.5, True),
+             ('taps8x8_d0', 3, 8, 8, 0.0, False), ('taps1x1_d1', 2, 1, 1, 1.0, False)]
+
+
+def make_iir_cases():
+    """IirFilter (iir_filter.py:100-211) with general filters: the output of
+    each of 6 steps of random inputs."""
+    from specula.processing_objects.iir_filter import IirFilter
+    from specula.data_objects.iir_filter_data import IirFilterData
+    from specula.data_objects.simul_params import SimulParams
+    from specula.base_value import BaseValue
+    out = {}
+    rng = np.random.default_rng(5)
+    sp = SimulParams(pixel_pupil=8, pixel_pitch=0.1, time_step=0.001)
+    for name, n, ni, no, delay, short in IIR_CASES:
+        num = rng.standard_normal((n, ni)).astype(np.float32) * 0.5
+        den = rng.standard_normal((n, no)).astype(np.float32) * 0.2
+        den[:, -1] = 1.0 + np.abs(den[:, -1])
+        ordnum = [ni] * n
+        ordden = [no] * n
+        if short and ni > 2:
+            num[0, ni - 1:] = 0.0                 # a row of lower order: right-aligned by set_num
+            ordnum[0] = ni - 1
+        fd = IirFilterData(ordnum, ordden, num, den, target_device_idx=-1, precision=1)
+        filt = IirFilter(sp, fd, delay=delay, target_device_idx=-1, precision=1)
+        d = BaseValue(value=np.zeros(n, np.float32), target_device_idx=-1)
+        filt.inputs['delta_comm'].set(d)
+        filt.setup()
+        key = 'iir/%s' % name
+        out[key + '/num'], out[key + '/den'] = num, den
+        out[key + '/ordnum'], out[key + '/ordden'] = np.array(ordnum), np.array(ordden)
+        for t in range(6):
+            x = rng.standard_normal(n).astype(np.float32)
+            d.value = x.copy()
+            d.generation_time = (t + 1) * 1000000
+            filt.check_ready((t + 1) * 1000000)
+            filt.trigger()
+            filt.post_trigger()
+            out[key + '/in%d' % t] = x
+            out[key + '/out%d' % t] = np.array(filt.out_comm.value, dtype=np.float32)
+    return out
+
+
 def make_polc_cases():
     """Modalrec with POLC (modalrec.py:126-156): pseudo-open-loop slopes
     s + IM c, modes R s - c, without and with a projection matrix, over three
@@ -598,6 +642,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, 'kl_fp32.npz'), **make_kl_cases())
     np.savez_compressed(os.path.join(HERE, 'prop_fp32.npz'), **make_prop_cases())
     np.savez_compressed(os.path.join(HERE, 'polc_fp32.npz'), **make_polc_cases())
+    np.savez_compressed(os.path.join(HERE, 'iir_fp32.npz'), **make_iir_cases())
     print('wrote', sorted(os.listdir(HERE)))
 
 
@@ -616,6 +661,10 @@ if __name__ == '__main__':
         import specula
         specula.init(-1, precision=1)
         np.savez_compressed(os.path.join(HERE, 'psf_fp32.npz'), **make_psf_cases())
+    elif '--iir' in sys.argv:          # only the general IIR filter fixtures
+        import specula
+        specula.init(-1, precision=1)
+        np.savez_compressed(os.path.join(HERE, 'iir_fp32.npz'), **make_iir_cases())
     elif '--polc' in sys.argv:         # only the POLC reconstructor fixtures
         import specula
         specula.init(-1, precision=1)
