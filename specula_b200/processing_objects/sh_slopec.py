@@ -93,12 +93,15 @@ class ShSlopec(Slopec):
         nb = _lib.load().sb_slopec_scratch_bytes(self._plan)
         self._scratch = torch.empty(nb, dtype=torch.uint8, device=self.device)
         self._pix = pix
+        self._target = self._setup_products(2 * n)
         self.slopes.single_mask = sd.single_mask()
         self.slopes.display_map = sd.display_map
 
     def trigger_code(self):
-        _lib.call('sb_slopec', _byref(self._plan), self._pix.pixels.data_ptr(), self.slopes.slopes.data_ptr(),
-                  self._flux.data_ptr(), self._scratch.data_ptr(), self._scratch.numel(), self.stream_handle())
+        st = self.stream_handle()
+        _lib.call('sb_slopec', _byref(self._plan), self._pix.pixels.data_ptr(), self._target.data_ptr(),
+                  self._flux.data_ptr(), self._scratch.data_ptr(), self._scratch.numel(), st)
+        self._apply_products(st)
 
     def post_trigger(self):
         t = self.current_time

@@ -545,6 +545,36 @@ def make_iir_cases():
     return out
 
 
+def make_slopec_filter_cases(ref):
+    """ShSlopec with slope filtering (slopec.py:92-101 through filtmat) on the
+    reference's own sub-aperture table (8x8, 52 valid) and random frames."""
+    from specula.processing_objects.sh_slopec import ShSlopec
+    from specula.data_objects.subap_data import SubapData
+    from specula.data_objects.pixels import Pixels
+    out = {}
+    rng = np.random.default_rng(33)
+    idxs = ref['subaps/idxs']
+    dmap = ref['subaps/display_map']
+    sd = SubapData(idxs=idxs, display_map=dmap, nx=8, ny=8, target_device_idx=-1, precision=1)
+    ns = 2 * idxs.shape[0]
+    F = rng.standard_normal((2, ns, 6)).astype(np.float32) * 0.1
+    sc = ShSlopec(sd, filtmat=F, target_device_idx=-1, precision=1)
+    pix = Pixels(64, 64, target_device_idx=-1, precision=1)
+    sc.inputs['in_pixels'].set(pix)
+    sc.setup()
+    out['slopec_filt/filtmat'] = F
+    for t in range(2):
+        frame = (rng.random((64, 64)) * 100).astype(np.float32)
+        pix.pixels[:] = frame
+        pix.generation_time = t + 1
+        sc.check_ready(t + 1)
+        sc.trigger()
+        sc.post_trigger()
+        out['slopec_filt/frame%d' % t] = frame
+        out['slopec_filt/slopes%d' % t] = np.array(sc.slopes.slopes, dtype=np.float32)
+    return out
+
+
 def make_polc_cases():
     """Modalrec with POLC (modalrec.py:126-156): pseudo-open-loop slopes
     s + IM c, modes R s - c, without and with a projection matrix, over three
@@ -643,6 +673,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, 'prop_fp32.npz'), **make_prop_cases())
     np.savez_compressed(os.path.join(HERE, 'polc_fp32.npz'), **make_polc_cases())
     np.savez_compressed(os.path.join(HERE, 'iir_fp32.npz'), **make_iir_cases())
+    np.savez_compressed(os.path.join(HERE, 'slopec_filt_fp32.npz'), **make_slopec_filter_cases(ref))
     print('wrote', sorted(os.listdir(HERE)))
 
 
@@ -661,6 +692,12 @@ if __name__ == '__main__':
         import specula
         specula.init(-1, precision=1)
         np.savez_compressed(os.path.join(HERE, 'psf_fp32.npz'), **make_psf_cases())
+    elif '--slopec-filter' in sys.argv:  # only the slope-filtering fixtures
+        import specula
+        specula.init(-1, precision=1)
+        with np.load(os.path.join(HERE, 'ref_fits.npz')) as z:
+            ref = {k: z[k] for k in z.files}
+        np.savez_compressed(os.path.join(HERE, 'slopec_filt_fp32.npz'), **make_slopec_filter_cases(ref))
     elif '--iir' in sys.argv:          # only the general IIR filter fixtures
         import specula
         specula.init(-1, precision=1)
