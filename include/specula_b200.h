@@ -203,6 +203,16 @@ typedef struct sb_ccd_params {
 int sb_ccd_step(const sb_ccd_params *p, const float *intensity, float *integrated,
                 float *pixels, void *stream);
 
+/* CCD with b x b binning (ccd.py:198-216, 262-280): p->n_pixels is the full
+ * rows x cols frame, integrated every step; on a readout step the block sums
+ * S are formed and scaled as the reference does, S * b^2 * (sum(frame) /
+ * sum(S)), and the QE / noise / ADU model of sb_ccd_step runs on the
+ * (rows/b) x (cols/b) binned pixels (RNG counter: the binned index).
+ * Scratch: sb_ccd_binned_scratch_bytes (0 when the frame is not divisible). */
+size_t sb_ccd_binned_scratch_bytes(int rows, int cols, int binning);
+int sb_ccd_step_binned(const sb_ccd_params *p, int rows, int cols, int binning, const float *intensity,
+                       float *integrated, float *pixels, void *scratch, size_t scratch_bytes, void *stream);
+
 /* Batched CCD step: n_batch frames of p->n_pixels each, contiguous in
  * intensity / integrated / pixels; frame b draws its noise with
  * photon_seeds[b] / readout_seeds[b] (device arrays) and its own pixel

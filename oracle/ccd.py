@@ -5,6 +5,12 @@ QE, background/dark, Poisson photon noise, Gaussian readout noise, ADU
 quantisation).  Excess (EMCCD), CIC and CTE noise are not on the SCAO SH
 step and are not restated.
 
+Binning follows the reference's intended arithmetic (ccd.py:264-280: b x b
+block sums of the full-resolution integrated frame, scaled by
+b^2 * sum(frame) / sum(blocks)).  The reference itself cannot run it: its
+integrated frame is sized with `Pixels.size * binning` (ccd.py:113), a
+tuple repetition, so the frame has the binned shape and apply_binning fails.
+
 Noise draws use the same NumPy generators as the reference CPU path
 (``default_rng(photon_seed)``, ``default_rng(readout_seed)``), so with equal
 seeds this oracle reproduces the reference CPU CCD bit for bit.

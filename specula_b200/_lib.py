@@ -115,6 +115,8 @@ SIGNATURES = {
     'sb_tune_key': (C.c_ulonglong, [C.c_int, C.c_int, C.c_int]),
     'sb_tune_set': (C.c_int, [C.c_int, C.c_ulonglong, C.c_int]),
     'sb_tune_get': (C.c_int, [C.c_int, C.c_ulonglong]),
+    'sb_ccd_binned_scratch_bytes': (C.c_size_t, [C.c_int, C.c_int, C.c_int]),
+    'sb_ccd_step_binned': (C.c_int, [C.POINTER(CcdParams), C.c_int, C.c_int, C.c_int, fp, fp, fp, vp, C.c_size_t, vp]),
     'sb_ccd_step_batched': (C.c_int, [C.POINTER(CcdParams), vp, vp, C.c_int, fp, fp, fp, vp]),
     'sb_slopec_batched': (C.c_int, [C.POINTER(SlopecPlan), fp, C.c_longlong, fp, C.c_int, fp, C.c_int, C.c_int, vp,
                                     C.c_size_t, vp]),

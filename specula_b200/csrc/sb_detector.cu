@@ -246,6 +246,104 @@ __global__ void __launch_bounds__(kCcdThreads, 4) ccd_kernel(sb_ccd_params p, co
     }
 }
 
+// ---------------------------------------------------------------------------
+// Binned readout (ccd.py:198-216, 262-280).  Every step the full-resolution
+// frame is integrated; on a readout step the b x b block sums S are formed
+// and scaled as the reference does, S * b^2 * (sum(frame) / sum(S)), and the
+// QE / noise / ADU model runs on the binned pixels.  Three launches, each
+// reading the device frame state; the last one resets the integration and
+// advances the state.
+// ---------------------------------------------------------------------------
+constexpr int kBinBlocks = 592;
+
+__device__ __forceinline__ bool ccd_readout_now(const sb_ccd_params &p) {
+    volatile sb_ccd_state *vs = p.state;
+    return vs->n_integrated + 1 >= p.frames_per_read;
+}
+
+__global__ void __launch_bounds__(256) ccd_integrate_kernel(sb_ccd_params p, const float *__restrict__ in,
+                                                            float *__restrict__ integ, int n) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x)
+        integ[e] = __fadd_rn(integ[e], __fmul_rn(in[e], p.rate));     // ccd.py:205
+}
+
+// binned[e] = block sum; per-CTA partial sums (float64) of the full frame
+// and of the block sums
+__global__ void __launch_bounds__(256) ccd_bin_sums_kernel(sb_ccd_params p, const float *__restrict__ integ,
+                                                           int cols, int b, int out_rows, int out_cols,
+                                                           float *__restrict__ binned, double *__restrict__ part) {
+    __shared__ double red[33];
+    if (!ccd_readout_now(p)) return;
+    const int n_out = out_rows * out_cols;
+    double tot = 0.0, sb = 0.0;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_out; e += gridDim.x * blockDim.x) {
+        const int r = e / out_cols, c = e - r * out_cols;
+        double acc = 0.0;
+        for (int u = 0; u < b; ++u)
+            for (int v = 0; v < b; ++v) acc += integ[(size_t)(r * b + u) * cols + c * b + v];
+        const float s = (float)acc;
+        binned[e] = s;
+        tot += acc;
+        sb += s;
+    }
+    tot = sb::block_sum_all_d(tot, red);
+    sb = sb::block_sum_all_d(sb, red);
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = tot;
+        part[2 * blockIdx.x + 1] = sb;
+    }
+}
+
+__global__ void __launch_bounds__(kCcdThreads) ccd_bin_noise_kernel(sb_ccd_params p, const float *__restrict__ binned,
+                                                                   const double *__restrict__ part, int nparts,
+                                                                   int b, int n_out, float *__restrict__ pix,
+                                                                   float *__restrict__ integ, int n_full) {
+    volatile sb_ccd_state *vs = p.state;
+    __shared__ double red[33];
+    __shared__ float logfact[32];
+    __shared__ unsigned int warps_done;
+    if (threadIdx.x == 0) warps_done = 0u;
+    if (threadIdx.x < 32) logfact[threadIdx.x] = c_logfact[threadIdx.x];
+    const uint64_t frame = vs->frame_index;
+    const int nint = vs->n_integrated + 1;
+    const bool readout = nint >= p.frames_per_read;
+    const double inv_gain = 1.0 / (double)p.adu_gain;
+    const bool gain_pow2 = (__double_as_longlong((double)p.adu_gain) & 0x000FFFFFFFFFFFFFLL) == 0;
+    __syncthreads();
+    if (readout) {
+        double tot = 0.0, sb = 0.0;
+        for (int k = threadIdx.x; k < nparts; k += blockDim.x) {
+            tot += part[2 * k];
+            sb += part[2 * k + 1];
+        }
+        tot = sb::block_sum_all_d(tot, red);
+        sb = sb::block_sum_all_d(sb, red);
+        const float ratio = (float)sb != 0.f ? __fdiv_rn((float)tot, (float)sb) : 0.f;
+        const float b2 = (float)(b * b);
+        for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_out; e += gridDim.x * blockDim.x) {
+            float f = __fmul_rn(__fmul_rn(binned[e], b2), ratio);
+            if (p.qe != 1.0f) f = __fmul_rn(f, p.qe);                        // ccd.py:282-287
+            f = __fadd_rn(f, p.bg_plus_dark);                                 // ccd.py:220-221
+            pix[e] = ccd_sample(p, f, e, frame, nullptr, nullptr, n_out, logfact, inv_gain, gain_pow2);
+        }
+        for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_full; e += gridDim.x * blockDim.x)
+            integ[e] = 0.0f;                                                  // ccd.py:216
+    }
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) {
+        const unsigned int nwarps = (blockDim.x + 31) >> 5;
+        if (atomicAdd(&warps_done, 1u) == nwarps - 1) {
+            __threadfence();
+            if (atomicAdd(&p.state->blocks_done, 1u) == gridDim.x - 1) {
+                vs->n_integrated = readout ? 0 : nint;
+                if (readout) vs->frame_index = frame + 1;
+                vs->blocks_done = 0u;
+                __threadfence();
+            }
+        }
+    }
+}
+
 __global__ void philox_raw_kernel(uint32_t k0, uint32_t k1, uint32_t c1, uint32_t c2, uint32_t c3, int n,
                                   uint32_t *out) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -332,6 +430,49 @@ __global__ void __launch_bounds__(256) slopec_finish_kernel(int n, const float *
 }
 
 }  // namespace
+
+extern "C" size_t sb_ccd_binned_scratch_bytes(int rows, int cols, int binning) {
+    if (rows < 1 || cols < 1 || binning < 1 || rows % binning || cols % binning) return 0;
+    const size_t n_out = (size_t)(rows / binning) * (cols / binning);
+    return ((n_out * sizeof(float) + 255) & ~(size_t)255) + 2 * kBinBlocks * sizeof(double);
+}
+
+extern "C" int sb_ccd_step_binned(const sb_ccd_params *p, int rows, int cols, int binning, const float *intensity,
+                                  float *integrated, float *pixels, void *scratch, size_t scratch_bytes,
+                                  void *stream) {
+    sb::clear_error();
+    if (!p || !intensity || !integrated || !pixels || !p->state)
+        return sb::fail(SB_EINVAL, "sb_ccd_step_binned: null pointer");
+    if (p->frames_per_read < 1 || rows < 1 || cols < 1 || binning < 1 || p->n_pixels != rows * cols)
+        return sb::fail(SB_EINVAL, "sb_ccd_step_binned: bad sizes");
+    if (rows % binning || cols % binning)
+        return sb::fail(SB_ESHAPE, "sb_ccd_step_binned: %d x %d frame not divisible by binning %d", rows, cols, binning);
+    if (p->photon_noise && !(p->adu_gain > 0.f))
+        return sb::fail(SB_EINVAL, "sb_ccd_step_binned: ADU gain must be > 0");
+    const size_t need = sb_ccd_binned_scratch_bytes(rows, cols, binning);
+    if (!scratch || scratch_bytes < need)
+        return sb::fail(SB_ESCRATCH, "sb_ccd_step_binned: scratch needs %zu bytes", need);
+    const int orow = rows / binning, ocol = cols / binning, n_out = orow * ocol, n_full = rows * cols;
+    float *binned = static_cast<float *>(scratch);
+    double *part = reinterpret_cast<double *>(static_cast<char *>(scratch) +
+                                              (((size_t)n_out * sizeof(float) + 255) & ~(size_t)255));
+    cudaStream_t st = sb::as_stream(stream);
+    int nb = (n_full + 255) / 256;
+    nb = nb < 1 ? 1 : (nb > 1184 ? 1184 : nb);
+    ccd_integrate_kernel<<<nb, 256, 0, st>>>(*p, intensity, integrated, n_full);
+    int rc = sb::check_launch("ccd_integrate_kernel");
+    if (rc) return rc;
+    int ns = (n_out + 255) / 256;
+    ns = ns < 1 ? 1 : (ns > kBinBlocks ? kBinBlocks : ns);
+    ccd_bin_sums_kernel<<<ns, 256, 0, st>>>(*p, integrated, cols, binning, orow, ocol, binned, part);
+    rc = sb::check_launch("ccd_bin_sums_kernel");
+    if (rc) return rc;
+    int nn = (n_full + kCcdThreads - 1) / kCcdThreads;
+    nn = nn < 1 ? 1 : (nn > 1184 ? 1184 : nn);
+    ccd_bin_noise_kernel<<<nn, kCcdThreads, 0, st>>>(*p, binned, part, ns, binning, n_out, pixels, integrated,
+                                                     n_full);
+    return sb::check_launch("ccd_bin_noise_kernel");
+}
 
 extern "C" int sb_ccd_step(const sb_ccd_params *p, const float *intensity, float *integrated, float *pixels,
                            void *stream) {

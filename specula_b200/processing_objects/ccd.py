@@ -11,7 +11,9 @@ and independent of launch shape; the reference's own CPU and GPU streams
 already differ from each other, so only the distributions are shared.  The
 frame counter lives on the device, so the object can be replayed from a CUDA
 graph.  Not on this path (raise NotImplementedError): excess (EMCCD), CIC and
-CTE noise, binning > 1, pixel gains, start_time > 0, 'auto' noise levels.
+CTE noise, pixel gains, start_time > 0, 'auto' noise levels.  Binning (b x b)
+runs as sb_ccd_step_binned: block sums scaled as the reference does
+(ccd.py:262-280), then the same QE / noise / ADU model on the binned pixels.
 """
 import torch
 
@@ -63,7 +65,7 @@ class CCD(BaseProcessingObj):
             raise ValueError(f'integration time dt={dt} must be a multiple of the basic simulation '
                              f'time_step={simul_params.time_step}')
         for flag, what in ((excess_noise, 'excess (EMCCD) noise'), (cic_noise, 'CIC noise'),
-                           (cte_noise, 'CTE noise'), (binning != 1, 'binning > 1'),
+                           (cte_noise, 'CTE noise'),
                            (pixelGains is not None, 'pixel gains'), (start_time != 0, 'start_time > 0'),
                            ('auto' in (readout_level, darkcurrent_level, background_level), "'auto' levels")):
             if flag:
@@ -123,8 +125,21 @@ class CCD(BaseProcessingObj):
             dark_level=self._darkcurrent_level, dark_noise=int(self._darkcurrent_noise),
             photon_seed=self._photon_seed, readout_seed=self._readout_seed, state=self._state.data_ptr())
         self._in_i = in_i
+        self._bin_scratch = None
+        if self._binning > 1:
+            rows, cols = self._integrated_i.size
+            nb = _lib.load().sb_ccd_binned_scratch_bytes(rows, cols, self._binning)
+            if nb == 0:
+                raise ValueError('Warning: binning requested not applied')
+            self._bin_scratch = torch.zeros(nb, dtype=torch.uint8, device=self.device)
 
     def trigger_code(self):
+        if self._bin_scratch is not None:
+            rows, cols = self._integrated_i.size
+            _lib.call('sb_ccd_step_binned', _byref(self._params), rows, cols, self._binning, self._in_i.i.data_ptr(),
+                      self._integrated_i.i.data_ptr(), self._pixels.pixels.data_ptr(), self._bin_scratch.data_ptr(),
+                      self._bin_scratch.numel(), self.stream_handle())
+            return
         _lib.call('sb_ccd_step', _byref(self._params), self._in_i.i.data_ptr(), self._integrated_i.i.data_ptr(),
                   self._pixels.pixels.data_ptr(), self.stream_handle())
 
