@@ -15,7 +15,8 @@ with two ways to get the interaction matrix:
 
 Default sizes: 8 m pupil on 320 px, 40x40 sub-apertures of 8x8 phase
 samples, 6x6 detector pixels of lambda/d (FFT 16, cut 4), 750 nm, 500
-Zernike modes (IFunc 'zernike').
+Zernike modes (IFunc 'zernike'); ``modes='kl'`` uses the 500-mode KL basis
+of the same pupil (``kl_ifunc``) instead.
 """
 
 import numpy as np
@@ -35,9 +36,26 @@ from specula_b200.processing_objects.sh import SH
 from specula_b200.processing_objects.sh_slopec import ShSlopec
 
 
+def kl_ifunc(pupil, diameter_m, n_modes=500, r0=0.15, L0=25.0, n_act=26, device_idx=0):
+    """KL modes of a pupil as an (n_modes x n_pupil_pixels) float32 tensor on
+    the device: thin-plate-spline zonal functions on a circular actuator
+    layout (26 across: 547 actuators on 320 px), then the von Karman KL basis
+    with piston removed (lib/modal_base_generator.py:make_modal_base_from_ifs_fft).
+    Each mode has unit RMS over the pupil, so a command of a is a nm RMS."""
+    from specula_b200.lib.modal_basis import make_modal_base_from_ifs_fft
+    from specula_b200.lib.zonal_ifunc import compute_zonal_ifunc
+    dev = torch.device('cuda', device_idx)
+    f, mask = compute_zonal_ifunc(pupil.shape[0], n_act, circ_geom=True, mask=pupil, device=dev)
+    kl, _, _ = make_modal_base_from_ifs_fft(mask, diameter_m, f, r0, L0, oversampling=2)
+    if kl.shape[0] < n_modes:
+        raise ValueError(f'{n_act} actuators across give {kl.shape[0]} KL modes, fewer than {n_modes}')
+    return kl[:n_modes].contiguous()
+
+
 class ShCalibrationSystem:
     def __init__(self, pixel_pupil=320, diameter_m=8.0, n_lenses=40, subap_npx=6, wavelength_nm=750.0,
-                 n_modes=500, obsratio=0.14, ifunc=None, subap_threshold=0.5, sign=-1, device_idx=0):
+                 n_modes=500, obsratio=0.14, ifunc=None, subap_threshold=0.5, sign=-1, modes='zernike',
+                 device_idx=0):
         from specula_b200.scao import valid_subaps
         self.device = torch.device('cuda', device_idx)
         pitch = diameter_m / pixel_pupil
@@ -59,7 +77,10 @@ class ShCalibrationSystem:
         self.slopec.inputs['in_pixels'].set(Pixels(n_lenses * subap_npx, n_lenses * subap_npx,
                                                    target_device_idx=device_idx))
         self.slopec.setup()
-        if ifunc is None:
+        if ifunc is None and modes == 'kl':
+            ifunc = IFunc(ifunc=kl_ifunc(pupil, diameter_m, n_modes, device_idx=device_idx), mask=pupil,
+                          target_device_idx=device_idx)
+        elif ifunc is None:
             ifunc = IFunc(type_str='zernike', mask=pupil, npixels=pixel_pupil, nmodes=n_modes,
                           target_device_idx=device_idx)
         elif not isinstance(ifunc, IFunc):
