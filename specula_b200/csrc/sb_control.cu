@@ -522,6 +522,142 @@ __global__ void __launch_bounds__(32 * (kDbWarps * RS + 1), 1)
     }
 }
 
+// Register-blocked batched projection: every consumer thread keeps 4
+// adjacent columns x NB realisations in registers.  Per mode row it does one
+// 16-byte shared load of the box, NB/4 broadcast loads of the commands and
+// 4*NB FMAs, so FMAs are ~90 % of the consumer instructions (the scalar form
+// above spends a shared load per FMA group on one column).  A stage is NBX
+// boxes of (32/NBX) mode rows x 256 columns side by side (32 KB), so a tile
+// is 256*NBX columns with 2*NBX consumer warps, and every column still sums
+// its modes in order from 0: the phases are bit-identical to the scalar
+// form with one mode-row group.
+template <int NBX>
+size_t dm_c4_smem_bytes(int nmodes, int nb_max) {
+    constexpr int rows = kDmRows / NBX;
+    const int nst = (nmodes + rows - 1) / rows;
+    return 1024 + (size_t)kDbStages * kDmRows * kDmCols * 4 + 2 * kDbStages * 8 + (size_t)nst * rows * nb_max * 4;
+}
+
+template <int NB, int NBX>
+__global__ void __launch_bounds__(32 * (2 * NBX + 1), 1)
+    dm_project_batched_c4_kernel(const __grid_constant__ CUtensorMap map, int nmodes, int nvalid,
+                                 const float *__restrict__ cmd, int ldc, int nb, float sign,
+                                 const int32_t *__restrict__ idx, float *__restrict__ phase,
+                                 long long phase_stride) {
+    static_assert(NB % 4 == 0 && (NBX == 1 || NBX == 2 || NBX == 4), "NB multiple of 4, 1/2/4 boxes per stage");
+    constexpr int NCW = 2 * NBX;                  // consumer warps: 128 columns each
+    constexpr int ROWS = kDmRows / NBX;           // mode rows per stage
+    constexpr int TW = kDmCols * NBX;             // columns per tile
+    constexpr int BOX = ROWS * kDmCols;           // floats per box
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char *base = smem_raw + ((1024 - (sb::smem_u32(smem_raw) & 1023)) & 1023);
+    float *ring = reinterpret_cast<float *>(base);
+    uint64_t *full = reinterpret_cast<uint64_t *>(base + (size_t)kDbStages * kDmRows * kDmCols * 4);
+    uint64_t *empty = full + kDbStages;
+    float *c = reinterpret_cast<float *>(empty + kDbStages);       // [mode][NB]
+    __shared__ int abort_flag, issued;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nst = (nmodes + ROWS - 1) / ROWS;
+    if (tid == 0) {
+        for (int s = 0; s < kDbStages; ++s) {
+            sb::mbar_init(&full[s], 1);
+            sb::mbar_init(&empty[s], NCW);
+        }
+        sb::mbar_init_fence();
+        abort_flag = 0;
+        issued = 0;
+    }
+    for (int e = tid; e < nst * ROWS * NB; e += blockDim.x) {
+        const int m = e / NB, b = e - m * NB;
+        c[e] = (m < nmodes && b < nb) ? sign * cmd[(size_t)b * ldc + m] : 0.f;
+    }
+    __syncthreads();
+    const int ntiles = (nvalid + TW - 1) / TW;
+    const int bid = blockIdx.x, nblk = gridDim.x;
+    const int my_tiles = bid < ntiles ? (ntiles - 1 - bid) / nblk + 1 : 0;
+    const int total = my_tiles * nst;
+    if (warp == NCW) {
+        if (lane == 0) {
+            const uint64_t pol = sb::l2_evict_first_policy();
+            int q = 0;
+            for (; q < total; ++q) {
+                const int slot = q % kDbStages;
+                if (q >= kDbStages && !sb::mbar_wait(&empty[slot], ((q / kDbStages) - 1) & 1)) {
+                    atomicExch(&g_dm_status, 5);
+                    abort_flag = 1;
+                    break;
+                }
+                if (*(volatile int *)&abort_flag) break;
+                const int tile = bid + (q / nst) * nblk;
+                sb::mbar_arrive_expect_tx(&full[slot], kDmRows * kDmCols * 4);
+                float *dst = ring + (size_t)slot * kDmRows * kDmCols;
+#pragma unroll
+                for (int x = 0; x < NBX; ++x)
+                    sb::tma_load_2d(dst + x * BOX, &map, tile * TW + x * kDmCols, (q % nst) * ROWS, &full[slot], pol);
+            }
+            issued = q;
+        }
+    } else {
+        // this thread's 4 columns: box tid / 64, columns 4 * (tid % 64) .. +3 of the box
+        const int bx = tid >> 6, cb = 4 * (tid & 63);
+        float acc[4][NB];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int b = 0; b < NB; ++b) acc[j][b] = 0.f;
+        for (int q = 0; q < total; ++q) {
+            const int slot = q % kDbStages;
+            // warp-uniform decisions: the lanes meet in __syncwarp below
+            if (!__all_sync(0xffffffffu, sb::mbar_wait(&full[slot], (q / kDbStages) & 1))) {
+                if (lane == 0) atomicExch(&g_dm_status, 6);
+                abort_flag = 1;
+                break;
+            }
+            if (__any_sync(0xffffffffu, *(volatile int *)&abort_flag)) break;
+            const int sg = q % nst;
+            const float4 *buf =
+                reinterpret_cast<const float4 *>(ring + (size_t)slot * kDmRows * kDmCols + bx * BOX + cb);
+            const float4 *cm = reinterpret_cast<const float4 *>(c + (size_t)sg * ROWS * NB);
+#pragma unroll
+            for (int r = 0; r < ROWS; ++r) {
+                const float4 v = buf[r * (kDmCols / 4)];
+#pragma unroll
+                for (int b4 = 0; b4 < NB / 4; ++b4) {
+                    const float4 cc = cm[r * (NB / 4) + b4];
+                    const float cr[4] = {cc.x, cc.y, cc.z, cc.w};
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        acc[0][4 * b4 + k] = fmaf(cr[k], v.x, acc[0][4 * b4 + k]);
+                        acc[1][4 * b4 + k] = fmaf(cr[k], v.y, acc[1][4 * b4 + k]);
+                        acc[2][4 * b4 + k] = fmaf(cr[k], v.z, acc[2][4 * b4 + k]);
+                        acc[3][4 * b4 + k] = fmaf(cr[k], v.w, acc[3][4 * b4 + k]);
+                    }
+                }
+            }
+            __syncwarp();
+            if (lane == 0) sb::mbar_arrive(&empty[slot]);
+            if (sg == nst - 1) {
+                const int col0 = (bid + (q / nst) * nblk) * TW + bx * kDmCols + cb;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    if (col0 + j < nvalid) {
+                        const int pix = idx[col0 + j];
+#pragma unroll
+                        for (int b = 0; b < NB; ++b)
+                            if (b < nb) phase[(size_t)b * phase_stride + pix] = acc[j][b];
+                    }
+#pragma unroll
+                    for (int b = 0; b < NB; ++b) acc[j][b] = 0.f;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (abort_flag && tid == 0) {
+        for (int q = 0; q < issued; ++q) sb::mbar_wait(&full[q % kDbStages], (q / kDbStages) & 1);
+    }
+}
+
 // modes_b[m] = sum_j R[m][j] s_b[j] for b < NB.  A CTA of 256 threads takes
 // RB reconstructor rows; each thread walks the slope index in pairs (8-byte
 // loads when the strides allow), loads the NB slope pairs once and uses them
@@ -739,6 +875,33 @@ int launch_dm_batched(const CUtensorMap &map, int n_modes, int n_valid, const fl
     return sb::check_launch("dm_project_batched_kernel");
 }
 
+template <int NB, int NBX>
+int launch_dm_c4(const CUtensorMap &map, int n_modes, int n_valid, const float *cmd, int ldc, int nb, float sign,
+                 const int32_t *mask_idx, float *phase, long long phase_stride, cudaStream_t st) {
+    static bool attr_set[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+        if (cudaFuncSetAttribute(dm_project_batched_c4_kernel<NB, NBX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)dm_c4_smem_bytes<NBX>(kDbMaxModes, NB)) != cudaSuccess)
+            return sb::fail(SB_ECUDA, "sb_dm_project_batched: %s", cudaGetErrorString(cudaGetLastError()));
+        attr_set[dev] = true;
+    }
+    const int nsm = sb::sm_count();
+    const int ntiles = (n_valid + kDmCols * NBX - 1) / (kDmCols * NBX);
+    dm_project_batched_c4_kernel<NB, NBX><<<ntiles < nsm ? ntiles : nsm, 32 * (2 * NBX + 1),
+                                            dm_c4_smem_bytes<NBX>(n_modes, NB), st>>>(
+        map, n_modes, n_valid, cmd, ldc, nb, sign, mask_idx, phase, phase_stride);
+    return sb::check_launch("dm_project_batched_c4_kernel");
+}
+
+template <int NBX>
+int launch_dm_c4_nb(const CUtensorMap &map, int n_modes, int n_valid, const float *c, int ldc, int nb, float sign,
+                    const int32_t *mask_idx, float *ph, long long phase_stride, cudaStream_t st) {
+    if (nb <= 4) return launch_dm_c4<4, NBX>(map, n_modes, n_valid, c, ldc, nb, sign, mask_idx, ph, phase_stride, st);
+    return launch_dm_c4<8, NBX>(map, n_modes, n_valid, c, ldc, nb, sign, mask_idx, ph, phase_stride, st);
+}
+
 template <int NB, int RB>
 int launch_gemv_batched_rb(const float *R, int nrows, int ncols, int ldr, const float *S, int lds, int nb, float *M,
                            int ldm, int vec2, cudaStream_t st) {
@@ -777,12 +940,28 @@ extern "C" int sb_dm_project_batched(const float *ifunc, int n_modes, int n_vali
     if (ld_if % 4 || (uintptr_t)ifunc % 16)
         return sb::fail(SB_EINVAL, "sb_dm_project_batched: influence-function rows must be 16-byte aligned");
     if (n_valid == 0) return SB_OK;
-    CUtensorMap map;
-    int rc = sb::tensor_map_2d_f32(&map, ifunc, n_modes, ld_if, ld_if, kDmRows, kDmCols);
-    if (rc) return rc;
     cudaStream_t st = sb::as_stream(stream);
     // tile variant: realisations per pass (every pass re-reads the IF once) and mode-row groups
+    // (0-5), or the register-blocked form with 4, 2 or 1 boxes per stage (6-8)
     const int v = sb::tune_lookup(SB_TUNE_DM_BATCHED, sb_tune_key(n_modes, n_valid, n_batch));
+    CUtensorMap map;
+    if (v >= 6) {
+        const int nbx = v == 6 ? 4 : (v == 7 ? 2 : 1);
+        int rc = sb::tensor_map_2d_f32(&map, ifunc, n_modes, ld_if, ld_if, kDmRows / nbx, kDmCols);
+        if (rc) return rc;
+        for (int b0 = 0; b0 < n_batch; b0 += 8) {
+            const int nb = n_batch - b0 < 8 ? n_batch - b0 : 8;
+            const float *c = cmd + (size_t)b0 * ld_cmd;
+            float *ph = phase + (size_t)b0 * phase_stride;
+            rc = nbx == 4 ? launch_dm_c4_nb<4>(map, n_modes, n_valid, c, ld_cmd, nb, sign, mask_idx, ph, phase_stride, st)
+               : nbx == 2 ? launch_dm_c4_nb<2>(map, n_modes, n_valid, c, ld_cmd, nb, sign, mask_idx, ph, phase_stride, st)
+                          : launch_dm_c4_nb<1>(map, n_modes, n_valid, c, ld_cmd, nb, sign, mask_idx, ph, phase_stride, st);
+            if (rc) return rc;
+        }
+        return SB_OK;
+    }
+    int rc = sb::tensor_map_2d_f32(&map, ifunc, n_modes, ld_if, ld_if, kDmRows, kDmCols);
+    if (rc) return rc;
     const int pass = v < 2 ? 16 : (v < 4 ? 8 : 4);
     const bool rs2 = (v & 1) != 0;
     for (int b0 = 0; b0 < n_batch; b0 += pass) {
