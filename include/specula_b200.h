@@ -333,8 +333,9 @@ int sb_modalrec_batched(const float *R, int n_modes, int n_slopes, int ldr, cons
  * made (so a captured graph keeps the variant it was captured with).
  *   SB_TUNE_DM_BATCHED  sb_dm_project_batched; key sb_tune_key(n_modes, n_valid, n_batch);
  *                       realisations per pass (16, 8, 4) x mode rows of a stage split over 1 or 2 warp groups
- *                       (variants 0-5), or 8 per pass with 4 columns x 8 realisations per thread in
- *                       1024-, 512- or 256-column tiles (variants 6-8)
+ *                       (variants 0-5), or the register-blocked form (4 columns x 8 or 16 realisations
+ *                       per thread) with 8 (6-8) or 16 (9-11) realisations per pass in 1024-, 512- or
+ *                       256-column tiles
  *   SB_TUNE_SH_FP32     sb_sh_forward / sb_sh_forward_batched; key sb_tune_key(n_lenses, cutsize, n_batch);
  *                       sub-apertures per CTA (8, 4, 2)
  *   SB_TUNE_MODALREC_BATCHED  sb_modalrec_batched; key sb_tune_key(n_modes, n_slopes, n_batch);

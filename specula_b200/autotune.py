@@ -16,8 +16,8 @@ is given, in a JSON file, so a second process skips the timing.
 Families wired here:
 
 * ``dm_batched``: ``sb_dm_project_batched``, realisations per pass x mode-row
-  groups (6 variants), and the register-blocked form (4 columns x 8
-  realisations per thread) with 1024-, 512- or 256-column tiles (3 variants);
+  groups (6 variants), and the register-blocked form (4 columns x 8 or 16
+  realisations per thread) with 1024-, 512- or 256-column tiles (6 variants);
 * ``sh_fp32``: ``sb_sh_forward_batched`` (FP32 form), sub-apertures per CTA
   (8, 4, 2);
 * ``modalrec_batched``: ``sb_modalrec_batched``, reconstructor rows per CTA

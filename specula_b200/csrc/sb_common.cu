@@ -85,7 +85,10 @@ const char *const kDmBatchedVariants[] = {
     "4 realisations per pass, 1 mode-row group",  "4 realisations per pass, 2 mode-row groups",
     "8 realisations per pass, 4 columns per thread, 1024-column tiles",
     "8 realisations per pass, 4 columns per thread, 512-column tiles",
-    "8 realisations per pass, 4 columns per thread, 256-column tiles"};
+    "8 realisations per pass, 4 columns per thread, 256-column tiles",
+    "16 realisations per pass, 4 columns per thread, 1024-column tiles",
+    "16 realisations per pass, 4 columns per thread, 512-column tiles",
+    "16 realisations per pass, 4 columns per thread, 256-column tiles"};
 const char *const kShFp32Variants[] = {"8 sub-apertures per CTA", "4 sub-apertures per CTA",
                                        "2 sub-apertures per CTA"};
 const char *const kModalrecVariants[] = {"2 reconstructor rows per CTA", "1 reconstructor row per CTA",

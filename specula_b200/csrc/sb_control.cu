@@ -899,7 +899,8 @@ template <int NBX>
 int launch_dm_c4_nb(const CUtensorMap &map, int n_modes, int n_valid, const float *c, int ldc, int nb, float sign,
                     const int32_t *mask_idx, float *ph, long long phase_stride, cudaStream_t st) {
     if (nb <= 4) return launch_dm_c4<4, NBX>(map, n_modes, n_valid, c, ldc, nb, sign, mask_idx, ph, phase_stride, st);
-    return launch_dm_c4<8, NBX>(map, n_modes, n_valid, c, ldc, nb, sign, mask_idx, ph, phase_stride, st);
+    if (nb <= 8) return launch_dm_c4<8, NBX>(map, n_modes, n_valid, c, ldc, nb, sign, mask_idx, ph, phase_stride, st);
+    return launch_dm_c4<16, NBX>(map, n_modes, n_valid, c, ldc, nb, sign, mask_idx, ph, phase_stride, st);
 }
 
 template <int NB, int RB>
@@ -942,15 +943,17 @@ extern "C" int sb_dm_project_batched(const float *ifunc, int n_modes, int n_vali
     if (n_valid == 0) return SB_OK;
     cudaStream_t st = sb::as_stream(stream);
     // tile variant: realisations per pass (every pass re-reads the IF once) and mode-row groups
-    // (0-5), or the register-blocked form with 4, 2 or 1 boxes per stage (6-8)
+    // (0-5), or the register-blocked form with 4, 2 or 1 boxes per stage and 8 (6-8) or 16 (9-11)
+    // realisations per pass
     const int v = sb::tune_lookup(SB_TUNE_DM_BATCHED, sb_tune_key(n_modes, n_valid, n_batch));
     CUtensorMap map;
     if (v >= 6) {
-        const int nbx = v == 6 ? 4 : (v == 7 ? 2 : 1);
+        const int w = (v - 6) % 3, pass = v < 9 ? 8 : 16;
+        const int nbx = w == 0 ? 4 : (w == 1 ? 2 : 1);
         int rc = sb::tensor_map_2d_f32(&map, ifunc, n_modes, ld_if, ld_if, kDmRows / nbx, kDmCols);
         if (rc) return rc;
-        for (int b0 = 0; b0 < n_batch; b0 += 8) {
-            const int nb = n_batch - b0 < 8 ? n_batch - b0 : 8;
+        for (int b0 = 0; b0 < n_batch; b0 += pass) {
+            const int nb = n_batch - b0 < pass ? n_batch - b0 : pass;
             const float *c = cmd + (size_t)b0 * ld_cmd;
             float *ph = phase + (size_t)b0 * phase_stride;
             rc = nbx == 4 ? launch_dm_c4_nb<4>(map, n_modes, n_valid, c, ld_cmd, nb, sign, mask_idx, ph, phase_stride, st)

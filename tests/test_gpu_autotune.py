@@ -31,7 +31,7 @@ def _dm_problem(nm, nv, L, B, seed):
 
 
 # batched-mirror variants that sum every column's modes in order from 0
-MODE_ORDER_VARIANTS = (0, 2, 4, 6, 7, 8)
+MODE_ORDER_VARIANTS = (0, 2, 4, 6, 7, 8, 9, 10, 11)
 
 
 @pytest.mark.parametrize('nm,nv,B', [(37, 5003, 3), (500, 40000, 7), (300, 20011, 16), (54, 9000, 19)])

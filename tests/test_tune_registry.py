@@ -7,7 +7,7 @@ from specula_b200 import _lib
 
 def test_families_and_names():
     lib = _lib.load()
-    assert lib.sb_tune_variants(_lib.SB_TUNE_DM_BATCHED) == 9
+    assert lib.sb_tune_variants(_lib.SB_TUNE_DM_BATCHED) == 12
     assert lib.sb_tune_variants(_lib.SB_TUNE_SH_FP32) == 3
     assert lib.sb_tune_variants(_lib.SB_TUNE_MODALREC_BATCHED) == 3
     assert b'rows per CTA' in lib.sb_tune_variant_name(_lib.SB_TUNE_MODALREC_BATCHED, 2)
@@ -29,7 +29,7 @@ def test_set_get_remove():
     _lib.call('sb_tune_set', fam, k1, -1)
     assert lib.sb_tune_get(fam, k1) == 0
     with pytest.raises(RuntimeError, match='EINVAL'):
-        _lib.call('sb_tune_set', fam, k1, 9)
+        _lib.call('sb_tune_set', fam, k1, 12)
     with pytest.raises(RuntimeError, match='EINVAL'):
         _lib.call('sb_tune_set', 42, k1, 0)
     assert lib.sb_tune_get(42, k1) == -1
