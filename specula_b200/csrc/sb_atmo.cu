@@ -111,6 +111,23 @@ __global__ void atmo_advance_kernel(EvolveArgsT<CAP> a) {
 // strip reads coalesced (a direct gather is column-strided for odd k).
 constexpr int kTile = 32;
 constexpr int kBox = kTile + 8;   // footprint of a tile rotated by < 1 degree, plus the bilinear +1
+constexpr int kRowStep = 8;       // blockDim.y: output rows advance by 8 per thread
+
+// floor(v) for |v| < 2^22 on the FMA and integer pipes instead of the
+// conversion unit: the round-down sum with C = 1.5 * 2^23 lands on the
+// integer grid (spacing 1 in [2^23, 2^24)) at exactly C + floor(v), so
+// (sum - C) is floor(v) as a float and the bit difference is floor(v) as an
+// integer.
+__device__ __forceinline__ int floor_small(float v, float &fl) {
+    constexpr float C = 12582912.0f;
+    const float t = __fadd_rd(v, C);
+    fl = __fsub_rn(t, C);
+    return __float_as_int(t) - __float_as_int(C);
+}
+__device__ __forceinline__ int floor_small(float v) {
+    float fl;
+    return floor_small(v, fl);
+}
 
 template <int CAP>
 __global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgsT<CAP> a) {
@@ -191,6 +208,7 @@ __global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgsT<CAP> a) {
         constexpr int kPer = (kBox * kBox + 255) / 256;
         const int n_el = n_fast * n_slow;
         const float inv_nf = 1.0f / (float)n_fast;
+        const float e_half = (float)tid + 0.5f;
         float v0[kPer], v1[kPer];
         int qo[kPer];
 #pragma unroll
@@ -198,7 +216,7 @@ __global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgsT<CAP> a) {
             const int e = tid + 256 * j;
             qo[j] = -1;
             if (e < n_el) {
-                const int sl = (int)(((float)e + 0.5f) * inv_nf);
+                const int sl = floor_small((e_half + 256.0f * j) * inv_nf);
                 const int fa = e - sl * n_fast;
                 const float *p = row0 + (b0 + sl * d_slow + fa * d_fast);
                 v0[j] = p[0];
@@ -232,14 +250,15 @@ __global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgsT<CAP> a) {
     if (interior) {
         // every sample of this tile is well inside the layer
         const float *qb = &Q[0][0] - br0 * (kBox + 1) - bc0;
-        for (int yi = threadIdx.y; yi < kTile; yi += blockDim.y) {
+        float yf = (float)(y0 + (int)threadIdx.y);
+        for (int yi = threadIdx.y; yi < kTile; yi += blockDim.y, yf += (float)kRowStep) {
             const int y = y0 + yi;
             if (y >= L) break;
-            const float yf = (float)y;
             const float dr = fmaf(a00, yf, dr_x), dc = fmaf(a10, yf, dc_x);
-            const float fdr = floorf(dr), fdc = floorf(dc);
+            float fdr, fdc;
+            const int idr = floor_small(dr, fdr), idc = floor_small(dc, fdc);
             const float fr = dr - fdr, fc = dc - fdc;
-            const float *p = qb + (y + (int)fdr) * (kBox + 1) + x + (int)fdc;
+            const float *p = qb + (y + idr) * (kBox + 1) + x + idc;
             const float q00 = p[0], q01 = p[1], q10 = p[kBox + 1], q11 = p[kBox + 2];
             const float top = fmaf(fc, q01 - q00, q00);
             const float bot = fmaf(fc, q11 - q10, q10);
@@ -347,7 +366,7 @@ int launch_evolve_t(const char *who, const sb_atmo_layer *layers, const LayerPtr
     atmo_advance_kernel<CAP><<<1, CAP < 32 ? 32 : CAP, 0, st>>>(a);
     int rc = sb::check_launch("atmo_advance_kernel");
     if (rc) return rc;
-    dim3 block(32, 8), grid((L + kTile - 1) / kTile, (L + kTile - 1) / kTile, n_layers);
+    dim3 block(32, kRowStep), grid((L + kTile - 1) / kTile, (L + kTile - 1) / kTile, n_layers);
     atmo_evolve_kernel<CAP><<<grid, block, 0, st>>>(a);
     return sb::check_launch("atmo_evolve_kernel");
 }
