@@ -519,6 +519,19 @@ int sb_propagate_batched(const float *atm, int n_atm, long long atm_layer_stride
                          long long dm_stride, int n_batch, int pupil, float *A_out, float *phase_out,
                          long long out_stride, void *stream);
 
+/* sb_atmo_evolve_batched followed by sb_propagate_batched in one launch
+ * (replaces atmo_evolution.py:258-300 then atmo_propagation.py:105-144 for
+ * realisations whose n_atm layers are pupil-sized): layers / inputs hold
+ * n_atm * n_batch entries, realisation b's layer k at index b * n_atm + k;
+ * every layer is still written to its `out`, its values summed in layer
+ * order and the field formed as sb_propagate_batched does, with the same
+ * bits as the two calls. */
+int sb_atmo_propagate_batched(const sb_atmo_layer *layers, const sb_atmo_layer_inputs *inputs, int n_atm, int n_batch,
+                              int L, const sb_atmo_inputs *constants, void *work, size_t work_bytes,
+                              const float *stop_A, const float *stop_phase, const float *dm_A, const float *dm_phase,
+                              long long dm_stride, float *A_out, float *phase_out, long long out_stride,
+                              void *stream);
+
 /* ------------------------------------------------------------------------
  * PSF — replaces specula/processing_objects/psf.py:56-137 (PSF.calc_psf,
  * the Strehl ratio of trigger_code and the integration of post_trigger).

@@ -99,6 +99,9 @@ SIGNATURES = {
                                          C.POINTER(AtmoInputs), vp, C.c_size_t, vp]),
     'sb_propagate_batched': (C.c_int, [fp, C.c_int, C.c_longlong, C.c_longlong, fp, fp, fp, fp, C.c_longlong, C.c_int,
                                        C.c_int, fp, fp, C.c_longlong, vp]),
+    'sb_atmo_propagate_batched': (C.c_int, [C.POINTER(AtmoLayer), C.POINTER(AtmoLayerInputs), C.c_int, C.c_int,
+                                            C.c_int, C.POINTER(AtmoInputs), vp, C.c_size_t, fp, fp, fp, fp,
+                                            C.c_longlong, fp, fp, C.c_longlong, vp]),
     'sb_sh_forward_batched': (C.c_int, [C.POINTER(ShPlan), fp, C.c_longlong, fp, C.c_longlong, fp, C.c_longlong,
                                         C.c_int, C.c_float, fp, C.c_longlong, C.c_int, vp, C.c_size_t, vp]),
     'sb_sh_split_bf16_supported': (C.c_int, [C.POINTER(ShPlan)]),

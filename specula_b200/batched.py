@@ -80,6 +80,9 @@ class _Group:
         if dft not in SH_FORWARD:
             raise ValueError(f"dft must be one of {sorted(SH_FORWARD)}, not {dft!r}")
         self.sh_forward = SH_FORWARD[dft]
+        # atmosphere and propagation as one launch (sb_atmo_propagate_batched);
+        # False: sb_atmo_evolve_batched then sb_propagate_batched
+        self.fuse_atmo = True
         dev = torch.device('cuda', device_idx)
         self.device = dev
         self.n = len(reals)
@@ -191,11 +194,18 @@ class _Group:
         lp = self.loops[0]
         L2 = self.L * self.L
         consts = lp.atmo.inputs_struct(lp.atmo.delta_time)
-        _lib.call('sb_atmo_evolve_batched', self.atmo_layers, self.atmo_inputs, self.n * self.n_atm, self.L,
-                  ctypes.byref(consts), self.atmo_work.data_ptr(), self.atmo_work.numel(), st)
-        _lib.call('sb_propagate_batched', self.ATM.data_ptr(), self.n_atm, L2, self.n_atm * L2,
-                  self.stop.A.data_ptr(), self.stop.phaseInNm.data_ptr(), lp.dm.layer.A.data_ptr(),
-                  self.dm_phase.data_ptr(), L2, self.n, self.L, self.EA.data_ptr(), self.EP.data_ptr(), L2, st)
+        if self.fuse_atmo and self.n_atm > 0:
+            # layers and field in one launch (the same bits as the two calls below)
+            _lib.call('sb_atmo_propagate_batched', self.atmo_layers, self.atmo_inputs, self.n_atm, self.n, self.L,
+                      ctypes.byref(consts), self.atmo_work.data_ptr(), self.atmo_work.numel(),
+                      self.stop.A.data_ptr(), self.stop.phaseInNm.data_ptr(), lp.dm.layer.A.data_ptr(),
+                      self.dm_phase.data_ptr(), L2, self.EA.data_ptr(), self.EP.data_ptr(), L2, st)
+        else:
+            _lib.call('sb_atmo_evolve_batched', self.atmo_layers, self.atmo_inputs, self.n * self.n_atm, self.L,
+                      ctypes.byref(consts), self.atmo_work.data_ptr(), self.atmo_work.numel(), st)
+            _lib.call('sb_propagate_batched', self.ATM.data_ptr(), self.n_atm, L2, self.n_atm * L2,
+                      self.stop.A.data_ptr(), self.stop.phaseInNm.data_ptr(), lp.dm.layer.A.data_ptr(),
+                      self.dm_phase.data_ptr(), L2, self.n, self.L, self.EA.data_ptr(), self.EP.data_ptr(), L2, st)
         lp = self.loops[0]
         L2, F2 = self.L * self.L, self.side * self.side
         _lib.call(self.sh_forward, ctypes.byref(lp.sh._plan), self.EA.data_ptr(), L2, self.EP.data_ptr(), L2,

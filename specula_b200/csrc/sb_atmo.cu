@@ -129,18 +129,20 @@ __device__ __forceinline__ int floor_small(float v) {
     return floor_small(v, fl);
 }
 
-template <int CAP>
-__global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgsT<CAP> a) {
-    __shared__ float Q[kBox][kBox + 1];
-    __shared__ int fp[5];                 // footprint br0, br1, bc0, bc1 and the interior flag
-    __shared__ LayerDyn lyd;              // this layer's per-step parameters
-    const sb_atmo_layer &lys = a.layer[blockIdx.z];
+// One 32 x 32 output tile of layer li: thread (tx, ty) produces rows
+// y0 + ty + 8 j (j < 4) of column x0 + tx and hands each value to
+// sink(j, y, x, value).  Every thread of the CTA must call it (it holds two
+// CTA barriers); Q, fp and lyd are the CTA's shared staging.
+template <int CAP, class Sink>
+__device__ __forceinline__ void evolve_tile(const EvolveArgsT<CAP> &a, int li, float (&Q)[kBox][kBox + 1], int *fp,
+                                            LayerDyn &lyd, Sink &&sink) {
+    const sb_atmo_layer &lys = a.layer[li];
     const LayerDyn &ly = lyd;
     const int L = a.L;
     const int x0 = blockIdx.x * kTile, y0 = blockIdx.y * kTile;
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
     if (tid == 0) {
-        lyd = a.dyn ? a.dyn[blockIdx.z] : static_dyn(lys);
+        lyd = a.dyn ? a.dyn[li] : static_dyn(lys);
         // footprint [br0, br1] x [bc0, bc1] of the tile in the rot90'd layer
         int br0 = y0, br1 = min(y0 + kTile, L) - 1, bc0 = x0, bc1 = min(x0 + kTile, L) - 1;
         int interior = 0;
@@ -170,7 +172,7 @@ __global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgsT<CAP> a) {
         fp[0] = br0; fp[1] = br1; fp[2] = bc0; fp[3] = bc1; fp[4] = interior;
     }
     // integer position and float32 remainder (atmo_evolution.py:278-279)
-    const double np = *a.ptr[blockIdx.z].pos;
+    const double np = *a.ptr[li].pos;
     const double q = floor(np);
     const float *row0 = lys.screen + (long long)q;
     const int ld = lys.screen_ld;
@@ -231,12 +233,12 @@ __global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgsT<CAP> a) {
     __syncthreads();
     const int x = x0 + threadIdx.x;
     if (x >= L) return;
-    float *out = lys.out + x;
     const float scale = ly.scale;
     if (!ly.rotate) {
-        for (int yi = threadIdx.y; yi < kTile; yi += blockDim.y) {
-            const int y = y0 + yi;
-            if (y < L) out[(size_t)y * L] = __fmul_rn(Q[y - br0][x - bc0], scale);   // atmo_evolution.py:294
+#pragma unroll
+        for (int j = 0; j < kTile / kRowStep; ++j) {
+            const int y = y0 + (int)threadIdx.y + kRowStep * j;
+            if (y < L) sink(j, y, x, __fmul_rn(Q[y - br0][x - bc0], scale));   // atmo_evolution.py:294
         }
         return;
     }
@@ -251,8 +253,9 @@ __global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgsT<CAP> a) {
         // every sample of this tile is well inside the layer
         const float *qb = &Q[0][0] - br0 * (kBox + 1) - bc0;
         float yf = (float)(y0 + (int)threadIdx.y);
-        for (int yi = threadIdx.y; yi < kTile; yi += blockDim.y, yf += (float)kRowStep) {
-            const int y = y0 + yi;
+#pragma unroll
+        for (int j = 0; j < kTile / kRowStep; ++j, yf += (float)kRowStep) {
+            const int y = y0 + (int)threadIdx.y + kRowStep * j;
             if (y >= L) break;
             const float dr = fmaf(a00, yf, dr_x), dc = fmaf(a10, yf, dc_x);
             float fdr, fdc;
@@ -262,7 +265,7 @@ __global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgsT<CAP> a) {
             const float q00 = p[0], q01 = p[1], q10 = p[kBox + 1], q11 = p[kBox + 2];
             const float top = fmaf(fc, q01 - q00, q00);
             const float bot = fmaf(fc, q11 - q10, q10);
-            out[(size_t)y * L] = __fmul_rn(fmaf(fr, bot - top, top), scale);
+            sink(j, y, x, __fmul_rn(fmaf(fr, bot - top, top), scale));
         }
         return;
     }
@@ -270,8 +273,9 @@ __global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgsT<CAP> a) {
     // gives 0) is discontinuous; within 1e-4 px of an edge it is redone with
     // SciPy's exact float64 expression (m00*y + m01*x) + off0
     const float Lm1 = (float)(L - 1);
-    for (int yi = threadIdx.y; yi < kTile; yi += blockDim.y) {
-        const int y = y0 + yi;
+#pragma unroll
+    for (int j = 0; j < kTile / kRowStep; ++j) {
+        const int y = y0 + (int)threadIdx.y + kRowStep * j;
         if (y >= L) break;
         float v;
         const float yf = (float)y;
@@ -306,7 +310,65 @@ __global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgsT<CAP> a) {
             const float bot = fmaf(fc, q11 - q10, q10);
             v = fmaf(fr, bot - top, top);
         }
-        out[(size_t)y * L] = __fmul_rn(v, scale);   // atmo_evolution.py:294
+        sink(j, y, x, __fmul_rn(v, scale));   // atmo_evolution.py:294
+    }
+}
+
+template <int CAP>
+__global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgsT<CAP> a) {
+    __shared__ float Q[kBox][kBox + 1];
+    __shared__ int fp[5];                 // footprint br0, br1, bc0, bc1 and the interior flag
+    __shared__ LayerDyn lyd;              // this layer's per-step parameters
+    float *out = a.layer[blockIdx.z].out;
+    const int L = a.L;
+    evolve_tile(a, blockIdx.z, Q, fp, lyd, [&](int, int y, int x, float v) { out[(size_t)y * L + x] = v; });
+}
+
+// The on-axis propagation of pupil-sized layers fused in: blockIdx.z is a
+// realisation whose n_atm layers are layer[z * n_atm ...]; each layer is
+// written as by atmo_evolve_kernel and summed in registers in layer order,
+// then the stop and mirror layers are applied in propagate_batched_kernel's
+// operation order and the field written (the same bits as the two launches).
+struct FusedPropArgs {
+    const float *stop_A, *stop_phase, *dm_A, *dm_phase;
+    long long dm_stride, out_stride;
+    float *A, *P;
+    int n_atm, real0;   // layers per realisation; index of this launch's first realisation
+};
+
+template <int CAP>
+__global__ void __launch_bounds__(256) atmo_propagate_kernel(EvolveArgsT<CAP> a, FusedPropArgs f) {
+    __shared__ float Q[kBox][kBox + 1];
+    __shared__ int fp[5];
+    __shared__ LayerDyn lyd;
+    const int L = a.L;
+    float acc[kTile / kRowStep];
+#pragma unroll
+    for (int j = 0; j < kTile / kRowStep; ++j) acc[j] = 0.0f;          // ElectricField.reset()
+    for (int k = 0; k < f.n_atm; ++k) {
+        const int li = blockIdx.z * f.n_atm + k;
+        float *out = a.layer[li].out;
+        evolve_tile(a, li, Q, fp, lyd, [&](int j, int y, int x, float v) {
+            out[(size_t)y * L + x] = v;
+            acc[j] = __fadd_rn(acc[j], v);
+        });
+        __syncthreads();                  // Q, fp and lyd are restaged for the next layer
+    }
+    const int x = blockIdx.x * kTile + threadIdx.x;
+    if (x >= L) return;
+    const long long b = f.real0 + blockIdx.z;
+#pragma unroll
+    for (int j = 0; j < kTile / kRowStep; ++j) {
+        const int y = blockIdx.y * kTile + (int)threadIdx.y + kRowStep * j;
+        if (y >= L) break;
+        const long long e = (long long)y * L + x;
+        float amp = 1.0f, ph = acc[j];
+        if (f.stop_A) amp = __fmul_rn(amp, f.stop_A[e]);
+        if (f.stop_phase) ph = __fadd_rn(ph, f.stop_phase[e]);
+        if (f.dm_A) amp = __fmul_rn(amp, f.dm_A[e]);
+        ph = __fadd_rn(ph, f.dm_phase[b * f.dm_stride + e]);
+        f.A[b * f.out_stride + e] = amp;
+        f.P[b * f.out_stride + e] = ph;
     }
 }
 
@@ -337,7 +399,7 @@ namespace {
 
 template <int CAP>
 int launch_evolve_t(const char *who, const sb_atmo_layer *layers, const LayerPtrs *ptrs, int n_layers, int L,
-                    const sb_atmo_inputs *in, LayerDyn *dyn, void *stream) {
+                    const sb_atmo_inputs *in, LayerDyn *dyn, void *stream, const FusedPropArgs *fuse = nullptr) {
     EvolveArgsT<CAP> a;
     for (int k = 0; k < n_layers; ++k) {
         const sb_atmo_layer &l = layers[k];
@@ -366,6 +428,11 @@ int launch_evolve_t(const char *who, const sb_atmo_layer *layers, const LayerPtr
     atmo_advance_kernel<CAP><<<1, CAP < 32 ? 32 : CAP, 0, st>>>(a);
     int rc = sb::check_launch("atmo_advance_kernel");
     if (rc) return rc;
+    if (fuse) {
+        dim3 block(32, kRowStep), grid((L + kTile - 1) / kTile, (L + kTile - 1) / kTile, n_layers / fuse->n_atm);
+        atmo_propagate_kernel<CAP><<<grid, block, 0, st>>>(a, *fuse);
+        return sb::check_launch("atmo_propagate_kernel");
+    }
     dim3 block(32, kRowStep), grid((L + kTile - 1) / kTile, (L + kTile - 1) / kTile, n_layers);
     atmo_evolve_kernel<CAP><<<grid, block, 0, st>>>(a);
     return sb::check_launch("atmo_evolve_kernel");
@@ -483,6 +550,51 @@ extern "C" int sb_atmo_evolve_batched(const sb_atmo_layer *layers, const sb_atmo
         }
         const int rc = launch_evolve_t<kBatchLayers>("sb_atmo_evolve_batched", layers + k0, ptrs, n, L, constants,
                                                      static_cast<LayerDyn *>(work) + k0, stream);
+        if (rc) return rc;
+    }
+    return SB_OK;
+}
+
+extern "C" int sb_atmo_propagate_batched(const sb_atmo_layer *layers, const sb_atmo_layer_inputs *inputs, int n_atm,
+                                         int n_batch, int L, const sb_atmo_inputs *constants, void *work,
+                                         size_t work_bytes, const float *stop_A, const float *stop_phase,
+                                         const float *dm_A, const float *dm_phase, long long dm_stride, float *A_out,
+                                         float *phase_out, long long out_stride, void *stream) {
+    sb::clear_error();
+    const long long n = (long long)L * L;
+    if (!layers || !inputs || !constants || n_atm < 1 || n_atm > kBatchLayers || n_batch < 1 || L < 1 ||
+        !(constants->pixel_pitch > 0.0) || !(constants->delta_time >= 0.0) || !dm_phase || !A_out || !phase_out ||
+        dm_stride < n || out_stride < n)
+        return sb::fail(SB_EINVAL, "sb_atmo_propagate_batched: bad args");
+    const int n_layers = n_atm * n_batch;
+    if (!work || work_bytes < (size_t)n_layers * sizeof(LayerDyn))
+        return sb::fail(SB_ESCRATCH, "sb_atmo_propagate_batched: work needs %zu bytes",
+                        (size_t)n_layers * sizeof(LayerDyn));
+    // whole realisations per launch
+    const int per = (kBatchLayers / n_atm) * n_atm;
+    LayerPtrs ptrs[kBatchLayers];
+    for (int k0 = 0; k0 < n_layers; k0 += per) {
+        const int nl = n_layers - k0 < per ? n_layers - k0 : per;
+        for (int k = 0; k < nl; ++k) {
+            const sb_atmo_layer_inputs &li = inputs[k0 + k];
+            ptrs[k].seeing = li.seeing;
+            ptrs[k].wind_speed = li.wind_speed;
+            ptrs[k].wind_direction = li.wind_direction;
+            ptrs[k].pos = li.position;
+        }
+        FusedPropArgs f;
+        f.stop_A = stop_A;
+        f.stop_phase = stop_phase;
+        f.dm_A = dm_A;
+        f.dm_phase = dm_phase;
+        f.dm_stride = dm_stride;
+        f.out_stride = out_stride;
+        f.A = A_out;
+        f.P = phase_out;
+        f.n_atm = n_atm;
+        f.real0 = k0 / n_atm;
+        const int rc = launch_evolve_t<kBatchLayers>("sb_atmo_propagate_batched", layers + k0, ptrs, nl, L, constants,
+                                                     static_cast<LayerDyn *>(work) + k0, stream, &f);
         if (rc) return rc;
     }
     return SB_OK;

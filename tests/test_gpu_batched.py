@@ -121,3 +121,30 @@ def test_batched_dm_projection_matches_single(cuda):
             ref = S[:, :nv].double() @ IF[:, :nv].double().t()
             assert rel_max_err(M.cpu().numpy(), ref.cpu().numpy()) <= 1e-5, (B, lds)
     _lib.call('sb_device_status')
+
+
+def test_fused_atmosphere_propagation_matches_two_launches(cuda):
+    """sb_atmo_propagate_batched (layers and field in one launch) against
+    sb_atmo_evolve_batched + sb_propagate_batched: layers and field
+    bit-identical over three steps, with more realisations than one launch
+    of 64 layers holds (2 layers x 40 realisations)."""
+    from specula_b200.batched import BatchedScao
+    from specula_b200.scao import ScaoConfig
+    base = ScaoConfig(heights=[0.0, 4000.0], cn2=[0.7, 0.3], wind_speed=[10.0, 25.0],
+                      wind_direction=[30.0, 212.7], n_modes=20, photon_noise=False, readout_noise=0.0)
+    reals = [replace(base, r0=0.08 + 0.003 * i, screen_seed=10 + i, noise_seed=100 + i) for i in range(40)]
+    systems = []
+    for fused in (True, False):
+        b = BatchedScao([(base, reals)])
+        b.groups[0].fuse_atmo = fused
+        b.start()
+        systems.append(b)
+    for step in range(3):
+        for b in systems:
+            b.step_eager()
+        torch.cuda.synchronize()
+        f, t = systems[0].groups[0], systems[1].groups[0]
+        assert float(t.EP.abs().max()) > 0
+        assert torch.equal(f.ATM, t.ATM), step
+        assert torch.equal(f.EA, t.EA), step
+        assert torch.equal(f.EP, t.EP), step
