@@ -80,9 +80,10 @@ class _Group:
         if dft not in SH_FORWARD:
             raise ValueError(f"dft must be one of {sorted(SH_FORWARD)}, not {dft!r}")
         self.sh_forward = SH_FORWARD[dft]
-        # atmosphere and propagation as one launch (sb_atmo_propagate_batched);
-        # False: sb_atmo_evolve_batched then sb_propagate_batched
-        self.fuse_atmo = True
+        # True: atmosphere and propagation as one launch
+        # (sb_atmo_propagate_batched, the same bits); the default two launches
+        # (sb_atmo_evolve_batched, sb_propagate_batched) measured faster
+        self.fuse_atmo = False
         dev = torch.device('cuda', device_idx)
         self.device = dev
         self.n = len(reals)

@@ -337,7 +337,7 @@ struct FusedPropArgs {
 };
 
 template <int CAP>
-__global__ void __launch_bounds__(256) atmo_propagate_kernel(EvolveArgsT<CAP> a, FusedPropArgs f) {
+__global__ void __launch_bounds__(256, 4) atmo_propagate_kernel(EvolveArgsT<CAP> a, FusedPropArgs f) {
     __shared__ float Q[kBox][kBox + 1];
     __shared__ int fp[5];
     __shared__ LayerDyn lyd;
