@@ -281,7 +281,10 @@ __global__ void __launch_bounds__(256) dm_project_kernel(const float *__restrict
 // ---------------------------------------------------------------------------
 constexpr int kDmRows = 32;            // IF rows per box (multiple of 4)
 constexpr int kDmCols = 256;           // IF columns per box (four per consumer thread)
-constexpr int kDmStages = 3;
+#ifndef SB_DM_STAGES
+#define SB_DM_STAGES 3                 // ring depth (build-time: -DSB_DM_STAGES=n)
+#endif
+constexpr int kDmStages = SB_DM_STAGES;
 constexpr int kDmConsumerWarps = kDmCols / 128;   // 4 columns per thread
 constexpr int kDmMaxModes = 4096;      // command vector staged in shared memory
 
