@@ -264,22 +264,16 @@ AdjKernel adjoint_kernel(int p, int cs, int npx) {
 // rows in registers and the np_sub columns of each lenslet with shuffles
 // inside groups of np_sub lanes.  Every influence-function sample under a
 // valid sub-aperture is read exactly once.
-constexpr int kContractModes = 16;  // modes per CTA (a multiple of 4)
+constexpr int kContractModes = 16;  // modes per CTA (even)
 
 template <int P>
 constexpr int contract_max_threads() { return P >= 16 ? 512 : 1024; }
 
-// MI modes per iteration (MI * P independent gathers in flight); MAXT the
-// launch bound: the wide form (MI 2) takes fields up to
-// contract_max_threads<P>() columns within 64 registers, the narrow form
-// (MI 4) fields up to 512 columns with the registers the extra loads need.
-// Every (mode, slope) sums its P rows in the same order either way.
-template <int P, int MI, int MAXT>
-__global__ void __launch_bounds__(MAXT) intmat_contract_kernel(
+template <int P>
+__global__ void __launch_bounds__(contract_max_threads<P>()) intmat_contract_kernel(
     const float *__restrict__ jac, const float *__restrict__ tot, int n_valid, int n, int field_ld,
     const int32_t *__restrict__ slot, const int32_t *__restrict__ pix2col, const float *__restrict__ IF, int n_modes,
     int ld_if, float scale, float *__restrict__ im) {
-    static_assert(kContractModes % MI == 0, "modes per CTA a multiple of the modes per iteration");
     __shared__ double red[33];
     const int x = threadIdx.x;
     const int li = blockIdx.y;
@@ -312,41 +306,35 @@ __global__ void __launch_bounds__(MAXT) intmat_contract_kernel(
     const int m0 = blockIdx.x * kContractModes;
     const int m1 = min(n_modes, m0 + kContractModes);
     const size_t ld_im = 2 * (size_t)n_valid;
-    for (int m = m0; m < m1; m += MI) {
-        // MI modes per iteration: MI * P independent loads in flight
-        const float *row[MI];
-#pragma unroll
-        for (int q = 0; q < MI; ++q) row[q] = IF + (size_t)(m + q < m1 ? m + q : m) * ld_if;
-        float vx[MI], vy[MI];
-#pragma unroll
-        for (int q = 0; q < MI; ++q) vx[q] = vy[q] = 0.f;
+    for (int m = m0; m < m1; m += 2) {
+        // two modes per iteration: 2 P independent loads in flight
+        const bool two = m + 1 < m1;
+        const float *row0 = IF + (size_t)m * ld_if;
+        const float *row1 = IF + (size_t)(two ? m + 1 : m) * ld_if;
+        float vx0 = 0.f, vy0 = 0.f, vx1 = 0.f, vy1 = 0.f;
 #pragma unroll
         for (int rr = 0; rr < P; ++rr) {
             const bool in = col[rr] >= 0;
-            float f[MI];
-#pragma unroll
-            for (int q = 0; q < MI; ++q) f[q] = in ? __ldg(row[q] + col[rr]) : 0.f;
-#pragma unroll
-            for (int q = 0; q < MI; ++q) {
-                vx[q] = fmaf(jx[rr], f[q], vx[q]);
-                vy[q] = fmaf(jy[rr], f[q], vy[q]);
-            }
+            const float f0 = in ? __ldg(row0 + col[rr]) : 0.f;
+            const float f1 = in ? __ldg(row1 + col[rr]) : 0.f;
+            vx0 = fmaf(jx[rr], f0, vx0);
+            vy0 = fmaf(jy[rr], f0, vy0);
+            vx1 = fmaf(jx[rr], f1, vx1);
+            vy1 = fmaf(jy[rr], f1, vy1);
         }
 #pragma unroll
         for (int o = P / 2; o > 0; o >>= 1) {
-#pragma unroll
-            for (int q = 0; q < MI; ++q) {
-                vx[q] += __shfl_down_sync(0xffffffffu, vx[q], o, P);
-                vy[q] += __shfl_down_sync(0xffffffffu, vy[q], o, P);
-            }
+            vx0 += __shfl_down_sync(0xffffffffu, vx0, o, P);
+            vy0 += __shfl_down_sync(0xffffffffu, vy0, o, P);
+            vx1 += __shfl_down_sync(0xffffffffu, vx1, o, P);
+            vy1 += __shfl_down_sync(0xffffffffu, vy1, o, P);
         }
         if (c == 0 && s >= 0) {
-#pragma unroll
-            for (int q = 0; q < MI; ++q) {
-                if (m + q < m1) {
-                    im[(size_t)(m + q) * ld_im + s] = scale * vx[q];
-                    im[(size_t)(m + q) * ld_im + n_valid + s] = scale * vy[q];
-                }
+            im[(size_t)m * ld_im + s] = scale * vx0;
+            im[(size_t)m * ld_im + n_valid + s] = scale * vy0;
+            if (two) {
+                im[(size_t)(m + 1) * ld_im + s] = scale * vx1;
+                im[(size_t)(m + 1) * ld_im + n_valid + s] = scale * vy1;
             }
         }
     }
@@ -432,20 +420,21 @@ extern "C" int sb_intmat_contract(const float *jac, const float *tot, int n_vali
     if (n_modes == 0) return SB_OK;
     const dim3 grid((n_modes + kContractModes - 1) / kContractModes, n_lenses);
     cudaStream_t st = sb::as_stream(stream);
-    const bool narrow = threads <= 512;
-#define SB_CONTRACT(PP)                                                                                            \
-    (narrow ? (intmat_contract_kernel<PP, 4, 512><<<grid, threads, 0, st>>>(jac, tot, n_valid, n_lenses, field_ld,  \
-                                                                           slot, pix2col, ifunc, n_modes, ld_if,  \
-                                                                           scale, intmat), 0)                     \
-            : (intmat_contract_kernel<PP, 2, contract_max_threads<PP>()><<<grid, threads, 0, st>>>(                \
-                   jac, tot, n_valid, n_lenses, field_ld, slot, pix2col, ifunc, n_modes, ld_if, scale, intmat), 0))
     switch (np_sub) {
-    case 4: SB_CONTRACT(4); break;
-    case 8: SB_CONTRACT(8); break;
-    case 16: SB_CONTRACT(16); break;
+    case 4:
+        intmat_contract_kernel<4><<<grid, threads, 0, st>>>(jac, tot, n_valid, n_lenses, field_ld, slot, pix2col,
+                                                            ifunc, n_modes, ld_if, scale, intmat);
+        break;
+    case 8:
+        intmat_contract_kernel<8><<<grid, threads, 0, st>>>(jac, tot, n_valid, n_lenses, field_ld, slot, pix2col,
+                                                            ifunc, n_modes, ld_if, scale, intmat);
+        break;
+    case 16:
+        intmat_contract_kernel<16><<<grid, threads, 0, st>>>(jac, tot, n_valid, n_lenses, field_ld, slot, pix2col,
+                                                             ifunc, n_modes, ld_if, scale, intmat);
+        break;
     default:
         return sb::fail(SB_EUNSUPPORTED, "sb_intmat_contract: np_sub=%d (4, 8 or 16)", np_sub);
     }
-#undef SB_CONTRACT
     return sb::check_launch("intmat_contract_kernel");
 }
