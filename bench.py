@@ -444,15 +444,19 @@ def bench_batched(dev, steps, cpu_budget_s):
 
 def bench_sh_forms(dev, reps=200):
     """Device time of one SH forward (FP32 CUDA-core DFTs against split-BF16
-    tensor-core DFTs) on the 80x80 ELT field and on a batch of 7 fields of
-    74x74 sub-apertures, CUDA events over `reps` launches after warm-up."""
+    tensor-core DFTs) on the 80x80 ELT field (FFT 16 and FFT 32) and on a
+    batch of 7 fields of 74x74 sub-apertures, CUDA events over `reps`
+    launches after warm-up."""
     import ctypes
     import torch
     from specula_b200 import _lib
     from specula_b200.scao import ScaoLoop, elt_config
     from specula_b200.batched import mc_groups
     out = {}
-    cfgs = [('elt_80x80_640px', elt_config(), 1), ('mc_74x74_592px_x7', mc_groups()[-1][0], 7)]
+    cfgs = [('elt_80x80_640px', elt_config(), 1),
+            # the 4x-padded ELT variant: FFT 32, 0.5 lambda/d pixels (the mirror size does not enter the SH)
+            ('elt_80x80_640px_fft32', elt_config(n_modes=10, fft_pad=4), 1),
+            ('mc_74x74_592px_x7', mc_groups()[-1][0], 7)]
     for name, cfg, nb in cfgs:
         loop = ScaoLoop(cfg, device_idx=dev.index)
         loop.start()
@@ -487,7 +491,9 @@ def bench_sh_forms(dev, reps=200):
         res['speedup_split_bf16_vs_fp32'] = res['fp32_us'] / res['split_bf16_us']
         res['fields'] = nb
         res['sub_apertures_per_field'] = cfg.n_lenses ** 2
-        if nb == 1:
+        res['fft'] = int(sh.geometry.fft_size)
+        res['cutsize'] = int(sh._plan.cutsize)
+        if name == 'elt_80x80_640px':
             res['lgs_us'] = _time_lgs(dev, cfg, loop, reps)
         out[name] = res
         del loop
