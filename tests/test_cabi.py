@@ -54,6 +54,36 @@ def test_argument_validation_without_device(lib):
     assert lib.sb_atmo_evolve(layers, 17, 16, C.byref(pos), None) == -2
 
 
+def test_fused_atmosphere_and_batched_mirror_validation_without_device(lib):
+    """sb_atmo_propagate_batched and sb_dm_project_batched reject bad
+    arguments (status and message) before any device work."""
+    layers = (_lib.AtmoLayer * 4)()
+    inputs = (_lib.AtmoLayerInputs * 4)()
+    consts = _lib.AtmoInputs()
+    consts.pixel_pitch = 0.05
+    consts.delta_time = 0.001
+    buf = C.c_void_p(16)                     # never dereferenced: validation fails first
+    f = _lib.SIGNATURES['sb_atmo_propagate_batched']
+    assert len(f[1]) == 17
+    # no layers per realisation
+    rc = lib.sb_atmo_propagate_batched(layers, inputs, 0, 4, 16, C.byref(consts), buf, 1 << 20, None, None, None,
+                                       buf, 256, buf, buf, 256, None)
+    assert rc == -1 and b'sb_atmo_propagate_batched' in lib.sb_last_error()
+    # mirror phase stride below one pupil
+    rc = lib.sb_atmo_propagate_batched(layers, inputs, 2, 2, 16, C.byref(consts), buf, 1 << 20, None, None, None,
+                                       buf, 255, buf, buf, 256, None)
+    assert rc == -1
+    # work area too small for the per-layer parameters
+    rc = lib.sb_atmo_propagate_batched(layers, inputs, 2, 2, 16, C.byref(consts), buf, 8, None, None, None,
+                                       buf, 256, buf, buf, 256, None)
+    assert rc == -4 and b'work needs' in lib.sb_last_error()
+    # batched mirror: too many modes, misaligned rows
+    rc = lib.sb_dm_project_batched(buf, 2000, 100, 100, buf, 2000, 4, C.c_float(-1.0), buf, buf, 1000, None)
+    assert rc == -2 and b'at most' in lib.sb_last_error()
+    rc = lib.sb_dm_project_batched(buf, 10, 100, 101, buf, 10, 4, C.c_float(-1.0), buf, buf, 1000, None)
+    assert rc == -1 and b'16-byte' in lib.sb_last_error()
+
+
 STRUCTS = {'sb_sh_plan': _lib.ShPlan, 'sb_ccd_params': _lib.CcdParams, 'sb_slopec_plan': _lib.SlopecPlan,
            'sb_iir_plan': _lib.IirPlan, 'sb_atmo_layer': _lib.AtmoLayer, 'sb_prop_layer': _lib.PropLayer,
            'sb_atmo_inputs': _lib.AtmoInputs, 'sb_atmo_layer_inputs': _lib.AtmoLayerInputs,
