@@ -1,7 +1,8 @@
 // Tensor-memory-accelerator (TMA) helpers for sm_100a: mbarrier waits with an
 // iteration bound, 2-D tiled bulk loads into shared memory with an L2
-// eviction hint, and the host-side tensor-map encoding.  Loads are issued
-// without cluster multicast and only ever read this GPU's own memory.
+// eviction hint, and the host-side tensor-map encoding.  Every load goes to
+// the issuing CTA's own shared memory and only ever reads this GPU's own
+// memory.
 #pragma once
 
 #include <cuda.h>
