@@ -128,7 +128,6 @@ __device__ __forceinline__ float std_normal(uint32_t e, uint64_t frame, uint64_t
 // depends only on its mean, index, frame and seeds, so the frame is the same
 // bit for bit as with pixels sampled in place.
 constexpr int kCcdThreads = 256;
-constexpr int kCcdChunk = 8;   // grid-stride passes ordered per barrier round
 
 __device__ __forceinline__ float ccd_sample(const sb_ccd_params &p, float f, int e, uint64_t frame,
                                             const uint64_t *photon_seeds, const uint64_t *readout_seeds, int n_per,
@@ -168,12 +167,9 @@ __global__ void __launch_bounds__(kCcdThreads, 4) ccd_kernel(sb_ccd_params p, co
     volatile sb_ccd_state *vs = p.state;
     __shared__ unsigned int warps_done;
     __shared__ float logfact[32];
-    // kCcdChunk grid-stride passes of 256 pixels are ordered together, so the
-    // sampling of all of them runs between two barriers
-    __shared__ float s_f[kCcdChunk][kCcdThreads];
-    __shared__ int s_idx[kCcdChunk][kCcdThreads];
-    __shared__ float s_mean[kCcdChunk][kCcdThreads];
-    __shared__ int s_small[kCcdChunk][kCcdThreads / 32];
+    __shared__ int s_idx[kCcdThreads];
+    __shared__ float s_mean[kCcdThreads];
+    __shared__ int s_small[kCcdThreads / 32];
     if (threadIdx.x == 0) warps_done = 0u;
     if (threadIdx.x < 32) logfact[threadIdx.x] = c_logfact[threadIdx.x];
     const uint64_t frame = vs->frame_index;
@@ -183,73 +179,54 @@ __global__ void __launch_bounds__(kCcdThreads, 4) ccd_kernel(sb_ccd_params p, co
     const bool gain_pow2 = (__double_as_longlong((double)p.adu_gain) & 0x000FFFFFFFFFFFFFLL) == 0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     __syncthreads();
-    const int stride = gridDim.x * kCcdThreads;
-    // block-uniform loops: every thread takes part in the shared-memory ordering
-    for (int base0 = blockIdx.x * kCcdThreads; base0 < p.n_pixels; base0 += stride * kCcdChunk) {
-        int nq = 0;
-#pragma unroll 1
-        for (int q = 0; q < kCcdChunk; ++q) {
-            const int base = base0 + q * stride;
-            if (base >= p.n_pixels) break;
-            const int e = base + threadIdx.x;
-            const bool valid = e < p.n_pixels;
-            float f = 0.f;
+    // block-uniform loop: every thread takes part in the shared-memory ordering
+    for (int base = blockIdx.x * kCcdThreads; base < p.n_pixels; base += gridDim.x * kCcdThreads) {
+        const int e = base + threadIdx.x;
+        const bool valid = e < p.n_pixels;
+        float f = 0.f;
+        if (valid) {
+            // integrated_i += i * (loop_dt * bandw)   (ccd.py:205)
+            const float acc = __fadd_rn(integ[e], __fmul_rn(in[e], p.rate));
+            if (!readout) {
+                integ[e] = acc;
+            } else {
+                f = acc;
+                if (p.qe != 1.0f) f = __fmul_rn(f, p.qe);                  // ccd.py:282-287
+                f = __fadd_rn(f, p.bg_plus_dark);                           // ccd.py:220-221
+            }
+        }
+        if (!readout) continue;
+        if (!p.photon_noise) {
             if (valid) {
-                // integrated_i += i * (loop_dt * bandw)   (ccd.py:205)
-                const float acc = __fadd_rn(integ[e], __fmul_rn(in[e], p.rate));
-                if (!readout) {
-                    integ[e] = acc;
-                } else {
-                    f = acc;
-                    if (p.qe != 1.0f) f = __fmul_rn(f, p.qe);                  // ccd.py:282-287
-                    f = __fadd_rn(f, p.bg_plus_dark);                           // ccd.py:220-221
-                }
+                pix[e] = ccd_sample(p, f, e, frame, photon_seeds, readout_seeds, n_per, logfact, inv_gain, gain_pow2);
+                integ[e] = 0.0f;                                            // ccd.py:216
             }
-            if (!readout) continue;
-            if (!p.photon_noise) {
-                if (valid) {
-                    pix[e] = ccd_sample(p, f, e, frame, photon_seeds, readout_seeds, n_per, logfact, inv_gain,
-                                        gain_pow2);
-                    integ[e] = 0.0f;                                        // ccd.py:216
-                }
-                continue;
-            }
-            const unsigned int bal = __ballot_sync(0xffffffffu, valid && f < 10.0f);
-            if (lane == 0) s_small[q][warp] = __popc(bal);
-            s_f[q][threadIdx.x] = f;
-            nq = q + 1;
+            continue;
         }
-        if (!readout || !p.photon_noise) continue;
+        // order by sampler branch: means below 10 first, then the rest
+        const bool small = valid && f < 10.0f;
+        const unsigned int bal = __ballot_sync(0xffffffffu, small);
+        if (lane == 0) s_small[warp] = __popc(bal);
         __syncthreads();
-        // order each pass by sampler branch: means below 10 first, then the rest
-        for (int q = 0; q < nq; ++q) {
-            const int e = base0 + q * stride + threadIdx.x;
-            const bool valid = e < p.n_pixels;
-            const float f = s_f[q][threadIdx.x];
-            const bool small = valid && f < 10.0f;
-            const unsigned int bal = __ballot_sync(0xffffffffu, small);
-            int before = 0, total = 0;
+        int before = 0, total = 0;
 #pragma unroll
-            for (int w = 0; w < kCcdThreads / 32; ++w) {
-                const int c = s_small[q][w];
-                before += w < warp ? c : 0;
-                total += c;
-            }
-            const int rank = __popc(bal & ((1u << lane) - 1u));
-            const int slot = small ? before + rank : total + (warp * 32 - before) + (lane - rank);
-            s_idx[q][slot] = valid ? e : -1;
-            s_mean[q][slot] = f;
+        for (int w = 0; w < kCcdThreads / 32; ++w) {
+            const int c = s_small[w];
+            before += w < warp ? c : 0;
+            total += c;
         }
+        const int rank = __popc(bal & ((1u << lane) - 1u));
+        const int slot = small ? before + rank : total + (warp * 32 - before) + (lane - rank);
+        s_idx[slot] = valid ? e : -1;
+        s_mean[slot] = f;
         __syncthreads();
-        for (int q = 0; q < nq; ++q) {
-            const int ei = s_idx[q][threadIdx.x];
-            if (ei >= 0) {
-                pix[ei] = ccd_sample(p, s_mean[q][threadIdx.x], ei, frame, photon_seeds, readout_seeds, n_per,
-                                     logfact, inv_gain, gain_pow2);
-                integ[ei] = 0.0f;                                           // ccd.py:216
-            }
+        const int ei = s_idx[threadIdx.x];
+        const float fi = s_mean[threadIdx.x];
+        __syncthreads();                        // the tables are refilled by the next pass
+        if (ei >= 0) {
+            pix[ei] = ccd_sample(p, fi, ei, frame, photon_seeds, readout_seeds, n_per, logfact, inv_gain, gain_pow2);
+            integ[ei] = 0.0f;                                               // ccd.py:216
         }
-        __syncthreads();                        // the tables are refilled by the next chunk
     }
     // the last warp to finish in the last block to finish advances the frame
     // state; warps that are done do not wait for the slower ones (the noise
