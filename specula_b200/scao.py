@@ -191,7 +191,7 @@ class ScaoLoop:
         self.wind_speed.value = vec[1:1 + nl]
         self.wind_direction.value = vec[1 + nl:]
 
-    def capture(self, pipelined=True, io=False):
+    def capture(self, pipelined=True, io=False, fuse_atmo=False):
         """Capture whole steps in a CUDA graph.  Call after at least one eager
         step, so the time step used by AtmoEvolution is the loop's (the first
         step has delta_time = 0).
@@ -209,6 +209,10 @@ class ScaoLoop:
         the end of DM(t-1).  The graph holds two steps so the buffers
         alternate statically; after each replay the DM layer tensor holds the
         latest DM phase, as in the sequential form.
+
+        ``fuse_atmo`` (pipelined form): AtmoEvolution and AtmoPropagation as
+        one launch (sb_atmo_propagate_batched with one system; the same
+        bits), which then waits for DM(t-1) as the propagation does.
         """
         self.step_eager()
         torch.cuda.synchronize(self.device)
@@ -260,12 +264,17 @@ class ScaoLoop:
                     # AtmoEvolution(t) does not depend on the mirror
                     if io:
                         self._point_inputs(self.io_inputs[step])
-                    self.atmo.trigger_code()
-                    # the propagation of step t reads DM(t-1): the previous
-                    # replay (already complete) for the first step of the graph
-                    if dm_done is not None:
-                        main.wait_event(dm_done)
-                    self.prop.trigger_code(phase_override={id(self.dm.layer): dm_buf[1 - par]})
+                    if fuse_atmo:
+                        if dm_done is not None:
+                            main.wait_event(dm_done)
+                        self._atmo_propagate(dm_buf[1 - par])
+                    else:
+                        self.atmo.trigger_code()
+                        # the propagation of step t reads DM(t-1): the previous
+                        # replay (already complete) for the first step of the graph
+                        if dm_done is not None:
+                            main.wait_event(dm_done)
+                        self.prop.trigger_code(phase_override={id(self.dm.layer): dm_buf[1 - par]})
                     for o in chain:
                         o.trigger_code()
                     self._rec_integ(out_next=nxt[1 - par])
@@ -280,6 +289,30 @@ class ScaoLoop:
         torch.cuda.synchronize(self.device)
         self.graph = g
         return g
+
+    def _atmo_propagate(self, dm_phase):
+        """AtmoEvolution.trigger_code + AtmoPropagation.trigger_code in one
+        launch: pupil-sized turbulence layers, then the pupil stop and the
+        mirror (phase read from ``dm_phase``)."""
+        atmo, prop = self.atmo, self.prop
+        nl = atmo.n_phasescreens
+        if prop._interpolated or prop._layers[-1] is not self.dm.layer or prop._layers[-2] is not self.pupilstop or \
+                any(ly.phaseInNm.shape != (self.cfg.pixel_pupil,) * 2 for ly in prop._layers):
+            raise NotImplementedError('ScaoLoop: the fused atmosphere needs pupil-sized layers in the SCAO order')
+        consts = atmo.inputs_struct(atmo.delta_time)
+        ins = (_lib.AtmoLayerInputs * nl)()
+        for k in range(nl):
+            ins[k].seeing = consts.seeing
+            ins[k].wind_speed = consts.wind_speed + (8 * k if consts.n_wind_speed > 1 else 0)
+            ins[k].wind_direction = consts.wind_direction + (8 * k if consts.n_wind_direction > 1 else 0)
+            ins[k].position = atmo._positions.data_ptr() + 8 * k
+        ef = prop.outputs['out_on_axis_source_ef']
+        L = self.cfg.pixel_pupil
+        stop = self.pupilstop
+        _lib.call('sb_atmo_propagate_batched', atmo._layers, ins, nl, 1, L, ctypes.byref(consts),
+                  atmo._work.data_ptr(), atmo._work.numel(), stop.A.data_ptr(), stop.phaseInNm.data_ptr(),
+                  self.dm.layer.A.data_ptr(), dm_phase.data_ptr(), L * L, ef.A.data_ptr(), ef.phaseInNm.data_ptr(),
+                  L * L, atmo.stream_handle())
 
     def _rec_integ(self, out_next=None):
         """Modalrec + Integrator of this loop as one launch

@@ -21,7 +21,7 @@ def _loop(mode, n_steps, cfg_kw=None):
             loop.step_eager()
             done += 1
     else:
-        loop.capture(pipelined=(mode == 'pipelined'))
+        loop.capture(pipelined=mode.startswith('pipelined'), fuse_atmo=(mode == 'pipelined_fused'))
         done += 1
         while done < n_steps:
             loop.replay()
@@ -31,12 +31,13 @@ def _loop(mode, n_steps, cfg_kw=None):
     return loop
 
 
-@pytest.mark.parametrize('mode', ['sequential', 'pipelined'])
+@pytest.mark.parametrize('mode', ['sequential', 'pipelined', 'pipelined_fused'])
 def test_graph_step_matches_object_loop(mode, cuda):
+    """pipelined_fused: AtmoEvolution and AtmoPropagation as one launch."""
     n = 10
     ref = _loop('eager', n)
     got = _loop(mode, n)
-    if mode == 'pipelined':
+    if mode.startswith('pipelined'):
         assert got.pipelined and got.steps_per_replay == 2
     for name, a, b in (('slopes', ref.slopec.slopes.slopes, got.slopec.slopes.slopes),
                        ('dm phase', ref.dm.layer.phaseInNm, got.dm.layer.phaseInNm),
