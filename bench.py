@@ -700,7 +700,7 @@ def run_b200(args):
                         'steps': e2e_steps},
                 'e2e_object_api': {'value': obj_value, 'unit': UNIT, 'api': 'LoopControl.iter (object by object)',
                                    'steps': obj_steps},
-                'gpu_launches': ScaoLoop.KERNELS_PER_STEP * steps,
+                'gpu_launches': loop.kernels_per_step * steps,
                 'step_graph': 'pipelined (DM projection concurrent with the SH chain)' if loop.pipelined
                 else 'sequential',
                 'roofline': {'bound': 'hbm', 'kernel': 'dm_project_tma_kernel', 'achieved': achieved, 'peak': peak,

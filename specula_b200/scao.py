@@ -223,6 +223,8 @@ class ScaoLoop:
         self.pipelined = bool(pipelined and self.integ.next_output_available)
         if fuse_atmo is None:
             fuse_atmo = self._can_fuse_atmo()
+        fuse_atmo = bool(fuse_atmo and self.pipelined)
+        self.fused_atmo = fuse_atmo
         if io and not self.pipelined:
             raise ValueError('ScaoLoop.capture: io slots need the pipelined form (integer integrator delay >= 1)')
         if not self.pipelined:
@@ -353,6 +355,12 @@ class ScaoLoop:
     # advance + evolve, propagate, SH forward + normalise, CCD, slopes (2),
     # reconstructor with the integrator, DM projection
     KERNELS_PER_STEP = 10
+
+    @property
+    def kernels_per_step(self):
+        """Kernels of one captured step: one fewer with the atmosphere and
+        the propagation fused."""
+        return self.KERNELS_PER_STEP - (1 if getattr(self, 'fused_atmo', False) else 0)
 
 
 def valid_subaps(pupil, n_lenses, npx, threshold=0.5):
