@@ -525,7 +525,8 @@ int sb_propagate_batched(const float *atm, int n_atm, long long atm_layer_stride
  * n_atm * n_batch entries, realisation b's layer k at index b * n_atm + k;
  * every layer is still written to its `out`, its values summed in layer
  * order and the field formed as sb_propagate_batched does, with the same
- * bits as the two calls. */
+ * bits as the two calls.  n_batch = 1 serves a single system (the pipelined
+ * SCAO step graph calls it so). */
 int sb_atmo_propagate_batched(const sb_atmo_layer *layers, const sb_atmo_layer_inputs *inputs, int n_atm, int n_batch,
                               int L, const sb_atmo_inputs *constants, void *work, size_t work_bytes,
                               const float *stop_A, const float *stop_phase, const float *dm_A, const float *dm_phase,
