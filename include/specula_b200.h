@@ -88,7 +88,11 @@ int sb_sh_forward(const sb_sh_plan *plan, const float *A, const float *phase_nm,
  * Geometries whose sb_sh_scratch_bytes() exceeds that size are rejected with
  * SB_ESCRATCH.  The first call on a device resolves the array's device
  * address (cudaGetSymbolAddress) with that device current; make that first
- * call before any stream capture.  All calls share the array: the kernels
+ * call before any stream capture.  The address is kept for the life of the
+ * process, so the device must not be reset (cudaDeviceReset) after that first
+ * call.  With the default 64 KB the largest grid is 128 x 128 lenslets
+ * (sb_sh_scratch_bytes sizes for two sub-apertures per CTA:
+ * ceil(n/2) * n * 8 bytes).  All calls share the array: the kernels
  * overwrite every partial sum they read, so no clearing is needed, but calls
  * that overlap on the GPU (different streams, or concurrent graphs) race on
  * it and must be serialised by the caller.

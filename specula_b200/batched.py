@@ -286,7 +286,7 @@ class BatchedScao:
             g.start()
         for g in self.groups:
             for lp in g.loops:
-                lp.atmo.delta_time = lp.atmo.t_to_seconds(lp.loop._dt)
+                lp.atmo.delta_time = lp.atmo.t_to_seconds(lp.loop.dt)
         torch.cuda.synchronize(self.device)
 
     def step_eager(self):

@@ -29,9 +29,10 @@ def needs_build():
     if not os.path.exists(OUT):
         return True
     t = os.path.getmtime(OUT)
-    deps = [os.path.join(HERE, s) for s in SOURCES] + [os.path.join(HERE, 'sb_common.cuh'), os.path.join(HERE, 'sb_dft.cuh'), os.path.join(HERE, 'sb_tma.cuh'),
-                                                       os.path.join(ROOT, 'include', 'specula_b200.h'),
-                                                       __file__]
+    # every source, every private header of this directory, the ABI header and this script
+    headers = [os.path.join(HERE, f) for f in sorted(os.listdir(HERE)) if f.endswith('.cuh')]
+    deps = [os.path.join(HERE, s) for s in SOURCES] + headers + [os.path.join(ROOT, 'include', 'specula_b200.h'),
+                                                                 __file__]
     return any(os.path.getmtime(d) > t for d in deps)
 
 

@@ -62,7 +62,7 @@ class LoopGradient:
         self.IF, self.ld, self.idx = dm._IF, dm._ld, dm._idx
         self.nv = int(self.idx.numel())
         self.nsl = 2 * self.adj.n_valid
-        self.dt = loop.atmo.t_to_seconds(loop.loop._dt)
+        self.dt = loop.atmo.t_to_seconds(loop.loop.dt)
         self.pos0 = torch.zeros_like(loop.atmo._positions)
         self.ef = loop.prop.outputs[next(iter(loop.prop.outputs))]
         self.dm_buf = torch.zeros_like(dm.layer.phaseInNm)

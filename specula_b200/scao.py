@@ -178,7 +178,7 @@ class ScaoLoop:
 
     def step_eager(self):
         """One step object by object (check_ready / trigger / post_trigger)."""
-        t = self.loop._t
+        t = self.loop.t
         for v in (self.seeing, self.wind_speed, self.wind_direction):
             v.generation_time = t
         self.loop.iter()
@@ -218,7 +218,7 @@ class ScaoLoop:
         """
         self.step_eager()
         torch.cuda.synchronize(self.device)
-        self.atmo.delta_time = self.atmo.t_to_seconds(self.loop._dt)
+        self.atmo.delta_time = self.atmo.t_to_seconds(self.loop.dt)
         g = torch.cuda.CUDAGraph()
         self.pipelined = bool(pipelined and self.integ.next_output_available)
         if fuse_atmo is None:
@@ -297,11 +297,19 @@ class ScaoLoop:
         return g
 
     def _can_fuse_atmo(self):
+        """True when the fused atmosphere kernel reads every input in its
+        layout: pupil-sized dense layers in the SCAO order, and the stop's
+        and the mirror's amplitude and phase as dense L x L arrays."""
         prop = self.prop
         L = self.cfg.pixel_pupil
+
+        def dense(t):
+            return t is not None and tuple(t.shape) == (L, L) and t.is_contiguous() and t.dtype == torch.float32
+
         return (not prop._interpolated and len(prop._layers) >= 2 and prop._layers[-1] is self.dm.layer and
                 prop._layers[-2] is self.pupilstop and
-                all(ly.phaseInNm.shape == (L, L) and ly.phaseInNm.is_contiguous() for ly in prop._layers) and
+                all(dense(ly.phaseInNm) for ly in prop._layers) and
+                dense(self.pupilstop.A) and dense(self.dm.layer.A) and
                 len(prop._layers) - 2 == len(self.atmo.layer_list) and
                 all(a is b for a, b in zip(prop._layers[:-2], self.atmo.layer_list)))
 

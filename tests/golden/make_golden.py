@@ -1,9 +1,9 @@
 """Generate the golden fixtures under tests/golden/ by running the reference.
 
-Run in a container where the SPECULA source tree is available (default
-location /root/reference, override with SPECULA_REF):
+Run where a SPECULA source tree is available, naming its root in the
+SPECULA_REF environment variable (there is no default location):
 
-    python tests/golden/make_golden.py
+    SPECULA_REF=<path to the SPECULA checkout> python tests/golden/make_golden.py
 
 The reference is imported on CPU (``specula.init(-1, precision)``) with the
 harness-only stand-ins in tests/golden/_refstubs for astropy.io.fits and
@@ -22,7 +22,9 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get('SPECULA_REF', '/root/reference')
+REF = os.environ.get('SPECULA_REF')
+if not REF:
+    sys.exit('make_golden.py: set SPECULA_REF to the root of a SPECULA source tree')
 sys.path.insert(0, os.path.join(HERE, '_refstubs'))
 sys.path.insert(0, REF)
 sys.path.insert(0, HERE)

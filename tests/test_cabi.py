@@ -113,3 +113,19 @@ def test_struct_layouts_match_header(tmp_path):
         assert got[(cname, 'size')] == C.sizeof(py), cname
         for f, _ in py._fields_:
             assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
+
+
+def test_static_scratch_limit_without_device(lib):
+    """sb_sh_forward_static's 64 KB array holds the partial sums of grids up
+    to 128 x 128 lenslets; larger grids are rejected before any device work."""
+    plan = _lib.ShPlan()
+    plan.np_sub, plan.cutsize, plan.subap_npx = 8, 12, 6
+    plan.n_lenses = 128
+    plan.field_ld = 128 * 8
+    assert 0 < lib.sb_sh_scratch_bytes(C.byref(plan)) <= 64 * 1024
+    plan.n_lenses = 130
+    plan.field_ld = 130 * 8
+    assert lib.sb_sh_scratch_bytes(C.byref(plan)) > 64 * 1024
+    buf = C.c_void_p(16)                     # never dereferenced: the size check fails first
+    rc = lib.sb_sh_forward_static(C.byref(plan), buf, buf, buf, 16, C.c_float(1.0), buf, None)
+    assert rc == -4 and b'static array' in lib.sb_last_error()

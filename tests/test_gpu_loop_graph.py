@@ -8,11 +8,23 @@ torch = pytest.importorskip('torch')
 pytestmark = pytest.mark.gpu
 
 
-def _loop(mode, n_steps, cfg_kw=None):
+def _row_padded(t, pad=4):
+    """The same values as ``t`` in a view whose rows are ``pad`` floats longer."""
+    big = torch.zeros((t.shape[0], t.shape[1] + pad), dtype=t.dtype, device=t.device)
+    big[:, :t.shape[1]].copy_(t)
+    return big[:, :t.shape[1]]
+
+
+def _loop(mode, n_steps, cfg_kw=None, strided_stop=False):
     from specula_b200.scao import ScaoConfig, ScaoLoop
     cfg = ScaoConfig(heights=[0.0, 4000.0], cn2=[0.7, 0.3], wind_speed=[10.0, 25.0],
                      wind_direction=[30.0, 212.7], **(cfg_kw or {}))
     loop = ScaoLoop(cfg, device_idx=0)
+    if strided_stop:
+        # a pupil stop held in row-padded storage: the two-launch propagation
+        # reads it through its row stride, the fused kernel cannot
+        loop.pupilstop.A = _row_padded(loop.pupilstop.A)
+        loop.pupilstop.phaseInNm = _row_padded(loop.pupilstop.phaseInNm)
     loop.start()
     loop.step_eager()
     done = 1
@@ -21,7 +33,10 @@ def _loop(mode, n_steps, cfg_kw=None):
             loop.step_eager()
             done += 1
     else:
-        loop.capture(pipelined=mode.startswith('pipelined'), fuse_atmo=(mode == 'pipelined_fused'))
+        if mode == 'pipelined_default':
+            loop.capture()
+        else:
+            loop.capture(pipelined=mode.startswith('pipelined'), fuse_atmo=(mode == 'pipelined_fused'))
         done += 1
         while done < n_steps:
             loop.replay()
@@ -47,6 +62,36 @@ def test_graph_step_matches_object_loop(mode, cuda):
                        ('layers', ref.atmo.layer_list[1].phaseInNm, got.atmo.layer_list[1].phaseInNm)):
         assert torch.equal(a, b), name
     assert float(ref.dm.layer.phaseInNm.abs().max()) > 0
+
+
+def _assert_same_loop_state(ref, got):
+    for name, a, b in (('slopes', ref.slopec.slopes.slopes, got.slopec.slopes.slopes),
+                       ('dm phase', ref.dm.layer.phaseInNm, got.dm.layer.phaseInNm),
+                       ('commands', ref.integ.out_comm.value, got.integ.out_comm.value),
+                       ('pixels', ref.ccd.outputs['out_pixels'].pixels, got.ccd.outputs['out_pixels'].pixels)):
+        assert torch.equal(a, b), name
+
+
+def test_default_capture_fuses_the_atmosphere(cuda):
+    """capture() with no arguments picks the fused atmosphere for the SCAO
+    layout: 9 kernels per step, the same bits as the object loop."""
+    n = 6
+    ref = _loop('eager', n)
+    got = _loop('pipelined_default', n)
+    assert got.pipelined and got.fused_atmo and got.kernels_per_step == 9
+    _assert_same_loop_state(ref, got)
+
+
+def test_default_capture_falls_back_for_a_strided_stop(cuda):
+    """A pupil stop that is not a dense L x L array keeps the two launches
+    (10 kernels per step), with the same bits as the object loop."""
+    n = 6
+    ref = _loop('eager', n, strided_stop=True)
+    got = _loop('pipelined_default', n, strided_stop=True)
+    assert got.pipelined and not got.fused_atmo and got.kernels_per_step == 10
+    _assert_same_loop_state(ref, got)
+    plain = _loop('eager', n)
+    assert torch.equal(ref.slopec.slopes.slopes, plain.slopec.slopes.slopes)
 
 
 def test_fractional_delay_falls_back_to_sequential_graph(cuda):
