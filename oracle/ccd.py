@@ -79,7 +79,7 @@ class CCDOracle:
             f += (ron.reshape(f.shape) * self.readout_level).astype(f.dtype)
         if self.photon_noise:
             f = np.round(f * self.gain) + self.bias
-            f = np.where(f < 0, 0, f)
+            np.maximum(f, 0, out=f)                             # clamp < 0 -> 0, in place
             f -= self.bias
             f = (f / self.gain).astype(f.dtype)
             if self.darkcurrent_noise:

@@ -62,8 +62,10 @@ class IntegratorOracle:
         return rem * self.state[:, k] + (1 - rem) * self.state[:, k - 1]
 
 
-def dm_phase(ifunc, mask, commands, sign=-1, m2c=None, precision=1):
-    """DM layer phase: phase[mask] = (sign * m2c @ c) @ IF (dm.py:72-86)."""
+def dm_phase(ifunc, mask, commands, sign=-1, m2c=None, precision=1, idx=None):
+    """DM layer phase: phase[mask] = (sign * m2c @ c) @ IF (dm.py:72-86).
+    ``idx``: np.where(mask), when the caller keeps it (the reference computes
+    it once at construction, ifunc.py:66-73)."""
     dt = np.float32 if precision == 1 else np.float64
     cmd = np.asarray(commands, dtype=dt)
     if m2c is not None:
@@ -71,7 +73,7 @@ def dm_phase(ifunc, mask, commands, sign=-1, m2c=None, precision=1):
     ifc = np.zeros(ifunc.shape[0], dtype=dt)
     ifc[:len(cmd)] = sign * cmd
     out = np.zeros(mask.shape, dtype=dt)
-    out[np.where(mask)] = ifc @ ifunc
+    out[np.where(mask) if idx is None else idx] = ifc @ ifunc
     return out
 
 

@@ -46,6 +46,7 @@ class OracleScaoLoop:
                                   precision=precision)
         self.integ = octl.IntegratorOracle([c.gain] * c.n_modes, delay=c.delay, precision=precision)
         self.dm_phase = np.zeros((L, L), dtype=dt)
+        self.mask_idx = np.where(self.pupil)
         self.t = 0
         self.slopes = None
         self.frame = None
@@ -65,6 +66,6 @@ class OracleScaoLoop:
         self.slopes = s
         modes = octl.modalrec(self.recmat, s)
         comm = self.integ.step(modes)
-        self.dm_phase = octl.dm_phase(self.ifunc, self.pupil, comm)
+        self.dm_phase = octl.dm_phase(self.ifunc, self.pupil, comm, idx=self.mask_idx)
         self.t += int(round(c.time_step * 1e9))
         return s

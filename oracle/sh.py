@@ -330,21 +330,32 @@ class SHOracle:
         phi = phase * ((2 * np.pi) / self.lam)
         ef = np.exp(1j * phi, dtype=self.cdtype)
         ef *= A
-        cube = ef[:n * p, :n * p].reshape(n, p, n, p).transpose(0, 2, 1, 3).reshape(n * n, p, p)
-        wf3 = np.zeros((n * n, N, N), dtype=self.cdtype)
-        wf3[:, :p, :p] = cube * self.tltf[np.newaxis]
-        fp4 = np.fft.fft2(wf3, axes=(1, 2))
-        psf = np.real(fp4 * np.conj(fp4))
-        if kernels_fft is None:
-            psf = np.fft.fftshift(psf, axes=(1, 2))
-        else:
-            spec = np.fft.fft2(psf, axes=(1, 2)) * np.asarray(kernels_fft)
-            psf = np.real(np.fft.ifft2(spec, axes=(1, 2), norm='forward')).astype(self.dtype)
-        psf *= self.fp_mask[np.newaxis]
         c = g.cutpixels
-        if c > 0:
-            psf = psf[:, c // 2: -c // 2, c // 2: -c // 2]
-        return psf
+        cs = N - c
+        out = None
+        # a few lenslet rows at a time, as the reference's row loop
+        # (sh.py:364-413) does: every sub-aperture's transform is independent,
+        # so the chunking changes no value, only the working-set size
+        rows = 1
+        wf3 = np.zeros((rows * n, N, N), dtype=self.cdtype)   # the padding stays zero
+        for r0 in range(0, n, rows):
+            r1 = min(n, r0 + rows)
+            cube = ef[r0 * p:r1 * p, :n * p].reshape(r1 - r0, p, n, p).transpose(0, 2, 1, 3).reshape(-1, p, p)
+            wf3[:, :p, :p] = cube * self.tltf[np.newaxis]
+            fp4 = np.fft.fft2(wf3, axes=(1, 2))
+            psf = np.real(fp4 * np.conj(fp4))
+            if kernels_fft is None:
+                psf = np.fft.fftshift(psf, axes=(1, 2))
+            else:
+                spec = np.fft.fft2(psf, axes=(1, 2)) * np.asarray(kernels_fft)[r0 * n:r1 * n]
+                psf = np.real(np.fft.ifft2(spec, axes=(1, 2), norm='forward')).astype(self.dtype)
+            psf *= self.fp_mask[np.newaxis]
+            if c > 0:
+                psf = psf[:, c // 2: -c // 2, c // 2: -c // 2]
+            if out is None:
+                out = np.empty((n * n, cs if c > 0 else N, cs if c > 0 else N), dtype=psf.dtype)
+            out[r0 * n:r1 * n] = psf
+        return out
 
     def forward(self, A, phase, S0, pixel_pitch, kernels_fft=None):
         """Normalised detector-plane intensity (ccd_side x ccd_side)."""
