@@ -535,6 +535,40 @@ def _time_lgs(dev, cfg, loop, reps):
     return e0.elapsed_time(e1) / reps * 1e3
 
 
+def accuracy_vs_fp64(loop, A, phase):
+    """Error of the headline step's float32 kernels against float64 on one
+    noise-free frame: the loop's SH (sb_sh_forward) on the turbulent field
+    (A, phase) against the float64 oracle SH, and the loop's slope computer
+    (sb_slopec) on that frame against float64 CoG slopes of the float64
+    frame; max |d| / max |ref| over the frame and over the slopes."""
+    import torch
+    from oracle import sh as osh, slopec as osl
+    cfg = loop.cfg
+    ef = loop.sh._in_ef
+    ef.A.copy_(A)
+    ef.phaseInNm.copy_(phase)
+    loop.sh.trigger_code()
+    pix = loop.ccd.outputs['out_pixels'].pixels
+    pix.copy_(loop.sh.outputs['out_i'].i)
+    loop.slopec.trigger_code()
+    torch.cuda.synchronize(loop.device)
+    got_i = loop.sh.outputs['out_i'].i.cpu().numpy().astype(np.float64)
+    got_s = loop.slopec.slopes.slopes.cpu().numpy().astype(np.float64)
+    s = loop.sh
+    g = osh.sh_geometry(s._wavelengthInNm, s._subap_wanted_fov_arcsec, s._sensor_pxscale_arcsec, cfg.n_lenses,
+                        cfg.subap_npx, cfg.pixel_pupil, cfg.pitch, fov_ovs_coeff=cfg.fov_ovs_coeff)
+    ref_i = osh.SHOracle(g, s._wavelengthInNm, precision=0).forward(
+        A.cpu().numpy().astype(np.float64), phase.cpu().numpy().astype(np.float64), ef.S0, cfg.pitch)
+    ref_s, _ = osl.sh_slopes(ref_i, loop.subapdata.idxs, precision=0)
+
+    def rel(a, b):
+        return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+    return {'intensity_rel_err_vs_fp64': rel(got_i, ref_i), 'slopes_rel_err_vs_fp64': rel(got_s, ref_s),
+            'frame': 'the first step of the bench loop (7 turbulent layers, flat mirror), noise-free',
+            'metric': 'max |float32 - float64| / max |float64|',
+            'targets': {'intensity': 1e-5, 'slopes': 1e-4}}
+
+
 def _lib_status():
     from specula_b200 import _lib
     _lib.call('sb_device_status')
@@ -558,6 +592,9 @@ def run_b200(args):
     loop = ScaoLoop(cfg, device_idx=local)
     loop.start()
     loop.step_eager()                     # t = 0 (no screen motion yet)
+    # the turbulent field of that step (the mirror is still flat), kept for the accuracy check
+    ef0 = loop.sh._in_ef
+    acc_field = (ef0.A.clone(), ef0.phaseInNm.clone())
     loop.capture()
     for _ in range(max(3, args.warmup)):
         loop.replay()
@@ -667,6 +704,8 @@ def run_b200(args):
         dist.all_reduce(t_obj, op=dist.ReduceOp.MAX)
     obj_value = world * obj_steps / float(t_obj.item())
 
+    accuracy = accuracy_vs_fp64(loop, *acc_field) if rank == 0 else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, n, dt = time_cpu_oracle(cfg, budget_s=args.cpu_baseline_seconds, max_steps=200, loop=loop)
@@ -710,7 +749,7 @@ def run_b200(args):
                 'step_roofline': {'algorithmic_bytes': step_bytes,
                                   'achieved_gbs': step_bytes / (ms_max / steps / 1e3) / 1e9,
                                   'frac': step_bytes / (ms_max / steps / 1e3) / 1e9 / peak},
-                'clocks': clk, 'cpu_baseline': cpu, 'adjoint_im': adjoint_im, 'loop_gradient': loop_grad,
+                'accuracy': accuracy, 'clocks': clk, 'cpu_baseline': cpu, 'adjoint_im': adjoint_im, 'loop_gradient': loop_grad,
                 'sh_forms': sh_forms, 'batched_mc': batched_mc}
         print(json.dumps(line), flush=True)
     del loop

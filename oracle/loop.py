@@ -49,6 +49,7 @@ class OracleScaoLoop:
         self.mask_idx = np.where(self.pupil)
         self.t = 0
         self.slopes = None
+        self.comm = None
         self.frame = None
 
     def step(self):
@@ -66,6 +67,7 @@ class OracleScaoLoop:
         self.slopes = s
         modes = octl.modalrec(self.recmat, s)
         comm = self.integ.step(modes)
+        self.comm = comm
         self.dm_phase = octl.dm_phase(self.ifunc, self.pupil, comm, idx=self.mask_idx)
         self.t += int(round(c.time_step * 1e9))
         return s

@@ -1,11 +1,13 @@
 """Split-BF16 tensor-core SH (sb_sh_forward_split_bf16) against float64.
 
-The north-star bar for this form: slopes within 1e-4 (max |d| / max |ref|)
-of an FP64 run of the reference.  Intensities are held to 1e-4 of the peak
-(the FP32 form meets 1e-5; the split operands carry about 2^-16 relative
-error, twice per DFT stage).  Inputs: the reference's golden fields of the
-supported geometries, and seeded turbulent phases at the 80x80 ELT size
-against the float64 oracle.
+The bar for both forms: slopes within 1e-4 (max |d| / max |ref|) and
+normalised intensities within 1e-5 of the peak, against an FP64 run of the
+reference (measured: split-BF16 about 5e-6 / 1.4e-5, FP32 about 3e-7 /
+4e-7; the split operands carry about 2^-16 relative error, twice per DFT
+stage).  Inputs: the reference's golden fields of the supported geometries,
+and seeded turbulent phases at the 80x80 ELT size (FFT 16 and 32) against
+the float64 oracle; the FP32 form at the ELT size is also held against the
+float32 oracle.
 """
 import math
 
@@ -20,7 +22,7 @@ from tests.cases import SH_CASES, SH_S0, rel_max_err, lam_over_d_arcsec  # noqa:
 
 pytestmark = pytest.mark.gpu
 
-INTENSITY_TOL = 1e-4
+INTENSITY_TOL = 1e-5
 SLOPE_TOL = 1e-4
 
 SUPPORTED = ['c1_plain16', 'n16_fft32', 'n16_fft16']
@@ -105,10 +107,18 @@ def test_split_bf16_elt_matches_fp64_oracle(fft, cuda):
     s_ref = _slopes(ref, n, flat=flat)
     e_i, e_s = rel_max_err(out, ref), rel_max_err(_slopes(out, n, flat=flat), s_ref)
     e_i32, e_s32 = rel_max_err(out32, ref), rel_max_err(_slopes(out32, n, flat=flat), s_ref)
+    ref32 = osh.SHOracle(g, lam, precision=1).forward(A, ph, SH_S0, pitch)
+    e_i32o = rel_max_err(out32, ref32)
+    e_s32o = rel_max_err(_slopes(out32, n, flat=flat), _slopes(ref32, n, flat=flat))
     print(f'elt80 fft{fft} (cut {sh.geometry.cutsize}): split-BF16 intensity {e_i:.2e} slopes {e_s:.2e}; '
-          f'FP32 intensity {e_i32:.2e} slopes {e_s32:.2e}')
+          f'FP32 intensity {e_i32:.2e} slopes {e_s32:.2e} (vs FP32 oracle {e_i32o:.2e} / {e_s32o:.2e})')
     assert e_i <= INTENSITY_TOL
     assert e_s <= SLOPE_TOL
+    # the plain FP32 form, the bench's headline SH, at the ELT size
+    assert e_i32 <= INTENSITY_TOL
+    assert e_s32 <= SLOPE_TOL
+    assert e_i32o <= INTENSITY_TOL
+    assert e_s32o <= SLOPE_TOL
 
 
 def test_split_bf16_batched_equals_single(cuda):
