@@ -257,6 +257,33 @@ int sb_slopec_batched(const sb_slopec_plan *plan, const float *pixels, long long
                       int slopes_stride, float *flux, int flux_stride, int n_batch, void *scratch,
                       size_t scratch_bytes, void *stream);
 
+/*
+ * One loop step's per-sub-aperture chain, SH forward to slopes, in two
+ * launches: the SH forward of sb_sh_forward (dft_mode 0) or
+ * sb_sh_forward_split_bf16 (dft_mode 1) without its normalisation launch,
+ * then one kernel that applies the photon normalisation (sh.py:425-427),
+ * runs the detector of sb_ccd_step (ccd.py:198-287) and the CoG of sb_slopec
+ * (sh_slopec.py:308-438) on each lenslet's pixels while they are in shared
+ * memory, and lets its last CTA apply the 1e-3 * mean flux cut-off and
+ * advance the detector frame state.  Replaces the five launches of
+ * sb_sh_forward + sb_ccd_step + sb_slopec in the loop step
+ * (SH.trigger_code, CCD.trigger_code, ShSlopec.trigger_code) with the same
+ * results bit for bit: intensity (normalised), integrated, pixels, slopes
+ * (the [sx..., sy...] layout) and flux are written as those calls write them.
+ * Conditions: the detector reads out every loop step (frames_per_read 1) at
+ * the SH frame size with no binning, subap_npx <= 16, and the sub-aperture
+ * table lists each valid lenslet's npx x npx box row-major;
+ * lenslet_subap[i * n_lenses + j] is the valid sub-aperture index of lenslet
+ * (row i, column j) or -1.  scratch: sb_sh_ccd_slopec_scratch_bytes(sh,
+ * n_subaps) bytes, no initialisation needed.
+ */
+size_t sb_sh_ccd_slopec_scratch_bytes(const sb_sh_plan *sh, int n_subaps);
+int sb_sh_ccd_slopec(const sb_sh_plan *sh, int dft_mode, const float *A, const float *phase_nm,
+                     const float *A_norm, int n_norm, float photon_scale, float *intensity,
+                     const sb_ccd_params *ccd, float *integrated, float *pixels,
+                     const sb_slopec_plan *slopec, const int32_t *lenslet_subap, float *slopes,
+                     float *flux, void *scratch, size_t scratch_bytes, void *stream);
+
 /* ------------------------------------------------------------------------
  * Modalrec — replaces specula/processing_objects/modalrec.py:159
  * (modes = R @ slopes), R row-major (n_modes x n_slopes).

@@ -90,6 +90,10 @@ SIGNATURES = {
     'sb_philox_raw': (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, vp, vp]),
     'sb_slopec_scratch_bytes': (C.c_size_t, [C.POINTER(SlopecPlan)]),
     'sb_slopec': (C.c_int, [C.POINTER(SlopecPlan), fp, fp, fp, vp, C.c_size_t, vp]),
+    'sb_sh_ccd_slopec_scratch_bytes': (C.c_size_t, [C.POINTER(ShPlan), C.c_int]),
+    'sb_sh_ccd_slopec': (C.c_int, [C.POINTER(ShPlan), C.c_int, fp, fp, fp, C.c_int, C.c_float, fp,
+                                   C.POINTER(CcdParams), fp, fp, C.POINTER(SlopecPlan), ip, fp, fp, vp,
+                                   C.c_size_t, vp]),
     'sb_modalrec': (C.c_int, [fp, C.c_int, C.c_int, C.c_int, fp, fp, vp]),
     'sb_integrator': (C.c_int, [C.POINTER(IirPlan), fp, fp, vp]),
     'sb_modalrec_integrator': (C.c_int, [fp, C.c_int, C.c_int, C.c_int, fp, fp, C.POINTER(IirPlan), fp, vp]),

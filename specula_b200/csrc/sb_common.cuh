@@ -18,6 +18,13 @@ void clear_error();
 int sh_tc_status_take();
 // tile-shape variant registered for (family, key); 0 when none
 int tune_lookup(int family, unsigned long long key);
+// SH forward without its photon-normalisation launch: the unnormalised frame
+// in `intensity`, the per-CTA partial sums at the start of `scratch` (n_parts
+// sums of the frame, then n_parts sums of A_norm); *n_parts receives the
+// number of CTAs.  mode 0: FP32 DFTs, 1: split-BF16 tensor-core DFTs.
+int sh_forward_unnormalised(const char *who, const sb_sh_plan *pl, const float *A, const float *phase_nm,
+                            const float *A_norm, int n_norm, float *intensity, void *scratch, size_t scratch_bytes,
+                            void *stream, int mode, int *n_parts);
 
 // Check the launch that just happened on this thread.
 inline int check_launch(const char *what) {

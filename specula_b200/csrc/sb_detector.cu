@@ -429,6 +429,190 @@ __global__ void __launch_bounds__(256) slopec_finish_kernel(int n, const float *
     }
 }
 
+// ---------------------------------------------------------------------------
+// The per-sub-aperture chain of one loop step in one launch, after the SH
+// forward has left its unnormalised frame and per-CTA partial sums:
+//   photon normalisation (sh.py:425-427), CCD integrate / QE / noise / ADU
+//   (ccd.py:198-287, detector dt = loop dt, no binning), CoG sums of every
+//   valid sub-aperture (sh_slopec.py:368-404) and, in the last CTA, the
+//   1e-3 * mean flux cut-off and the detector frame state.
+// A CTA owns up to 8 lenslets of one lenslet row: their npx x 8 npx pixel
+// tile is sampled into shared memory and each warp reduces one lenslet's box.
+// Every sum is taken in the order of the separate kernels
+// (sh_normalize_kernel, ccd_kernel, slopec_sums_kernel, slopec_finish_kernel),
+// so the results are the same bits; the sub-aperture table must list each
+// valid box's pixels row-major (the caller checks it and passes the lenslet
+// -> sub-aperture map).
+// ---------------------------------------------------------------------------
+constexpr int kChainThreads = 256;
+constexpr int kChainLenses = kChainThreads / 32;
+constexpr int kChainMaxNpx = 16;
+
+struct ChainArgs {
+    sb_ccd_params p;
+    const float *part_I;          // SH partial sums of the frame
+    const float *part_A;          // SH partial sums of the normalising amplitude
+    int nparts;
+    float photon_scale;
+    float *I;                     // frame: unnormalised in, normalised out
+    float *integ;
+    float *pix;
+    int n, npx, side;
+    const int32_t *lenslet_subap; // [n*n] valid sub-aperture index or -1
+    int n_valid;
+    float thr;
+    const float *xw, *yw, *mw;
+    float *slopes, *flux, *tot, *sxn, *syn;
+};
+
+__global__ void __launch_bounds__(kChainThreads) sh_ccd_slopec_kernel(ChainArgs a) {
+    __shared__ double dred[33];
+    __shared__ float logfact[32];
+    __shared__ int s_idx[kChainThreads];
+    __shared__ float s_mean[kChainThreads];
+    __shared__ int s_small[kChainThreads / 32];
+    __shared__ float tile[kChainMaxNpx * kChainLenses * kChainMaxNpx];
+    __shared__ int s_last;
+    const sb_ccd_params &p = a.p;
+    volatile sb_ccd_state *vs = p.state;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid < 32) logfact[tid] = c_logfact[tid];
+    const uint64_t frame = vs->frame_index;
+    const double inv_gain = 1.0 / (double)p.adu_gain;
+    const bool gain_pow2 = (__double_as_longlong((double)p.adu_gain) & 0x000FFFFFFFFFFFFFLL) == 0;
+
+    // photon normalisation: the sums of sh_normalize_kernel, in its order
+    double si = 0.0, sa = 0.0;
+    for (int e = tid; e < a.nparts; e += kChainThreads) {
+        si += a.part_I[e];
+        sa += a.part_A[e];
+    }
+    si = sb::block_sum_all_d(si, dred);
+    sa = sb::block_sum_all_d(sa, dred);
+    const float phot = (float)(a.photon_scale * sa);
+    const float scale = phot / (float)si;
+
+    const int i = blockIdx.y, j0 = blockIdx.x * kChainLenses;
+    const int w = min(kChainLenses, a.n - j0);
+    const int npx = a.npx, wc = w * npx, P = npx * wc, tld = kChainLenses * npx;
+    // detector: every pass samples up to 256 pixels of the tile, ordered by
+    // Poisson sampler branch as in ccd_kernel (the draws do not depend on it)
+    for (int base = 0; base < P; base += kChainThreads) {
+        const int q = base + tid;
+        const bool valid = q < P;
+        float f = 0.f;
+        if (valid) {
+            const int r = q / wc, c = q - r * wc;
+            const int e = (i * npx + r) * a.side + j0 * npx + c;
+            const float v = a.I[e] * scale;
+            a.I[e] = v;
+            f = __fadd_rn(a.integ[e], __fmul_rn(v, p.rate));           // ccd.py:205
+            if (p.qe != 1.0f) f = __fmul_rn(f, p.qe);                  // ccd.py:282-287
+            f = __fadd_rn(f, p.bg_plus_dark);                           // ccd.py:220-221
+        }
+        int qi = valid ? q : -1;
+        float fi = f;
+        if (p.photon_noise) {
+            const bool small = valid && f < 10.0f;
+            const unsigned int bal = __ballot_sync(0xffffffffu, small);
+            if (lane == 0) s_small[warp] = __popc(bal);
+            __syncthreads();
+            int before = 0, total = 0;
+#pragma unroll
+            for (int k = 0; k < kChainThreads / 32; ++k) {
+                const int cnt = s_small[k];
+                before += k < warp ? cnt : 0;
+                total += cnt;
+            }
+            const int rank = __popc(bal & ((1u << lane) - 1u));
+            const int slot = small ? before + rank : total + (warp * 32 - before) + (lane - rank);
+            s_idx[slot] = qi;
+            s_mean[slot] = f;
+            __syncthreads();
+            qi = s_idx[tid];
+            fi = s_mean[tid];
+            __syncthreads();
+        }
+        if (qi >= 0) {
+            const int r = qi / wc, c = qi - r * wc;
+            const int e = (i * npx + r) * a.side + j0 * npx + c;
+            const float v = ccd_sample(p, fi, e, frame, nullptr, nullptr, p.n_pixels, logfact, inv_gain, gain_pow2);
+            a.pix[e] = v;
+            a.integ[e] = 0.0f;                                          // ccd.py:216
+            tile[r * tld + c] = v;
+        }
+    }
+    __syncthreads();
+
+    // CoG sums, one warp per lenslet, in slopec_sums_kernel's lane order
+    if (warp < w) {
+        const int s = a.lenslet_subap[i * a.n + j0 + warp];
+        if (s >= 0) {
+            float fl = 0.f, t = 0.f, x = 0.f, y = 0.f;
+            for (int e = lane; e < npx * npx; e += 32) {
+                const int r = e / npx, c = e - r * npx;
+                const float v = tile[r * tld + warp * npx + c];
+                fl += v;
+                float wv = v - a.thr;                 // pixels -= thr; clamp < 0 -> 0
+                wv = wv < 0.f ? 0.f : wv;
+                t = fmaf(wv, a.mw[e], t);
+                x = fmaf(wv, a.xw[e], x);
+                y = fmaf(wv, a.yw[e], y);
+            }
+            fl = sb::warp_sum(fl);
+            t = sb::warp_sum(t);
+            x = sb::warp_sum(x);
+            y = sb::warp_sum(y);
+            if (lane == 0) {
+                a.flux[s] = fl;
+                a.tot[s] = t;
+                a.sxn[s] = x;
+                a.syn[s] = y;
+                const float fac = 1.0f / t;
+                a.slopes[s] = x * fac;
+                a.slopes[a.n_valid + s] = y * fac;
+            }
+        }
+    }
+
+    // the last CTA to finish: frame state, then the flux cut-off
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) s_last = atomicAdd(&p.state->blocks_done, 1u) == gridDim.x * gridDim.y - 1u;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if (tid == 0) {
+        vs->n_integrated = 0;
+        vs->frame_index = frame + 1;
+        vs->blocks_done = 0u;
+    }
+    // mean of the denominators as slopec_finish_kernel forms it: partials of 8
+    // consecutive sub-apertures (slopec_sums_kernel's CTAs), summed in float
+    // in warp order, then in float64 over 256 threads (sh_slopec.py:393-400)
+    const int nv = a.n_valid, ngroups = (nv + 7) / 8;
+    double acc = 0.0;
+    for (int g = tid; g < ngroups; g += kChainThreads) {
+        float b = 0.f;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int s = 8 * g + k;
+            b += s < nv ? __ldcg(a.tot + s) : 0.f;
+        }
+        acc += b;
+    }
+    acc = sb::block_sum_all_d(acc, dred);
+    const float mean = (float)(acc / nv);
+    const float cut = 1.0f / (mean * 1e-3f);
+    for (int s = tid; s < nv; s += kChainThreads) {
+        const float fac = 1.0f / __ldcg(a.tot + s);
+        if (fac > cut) {
+            a.slopes[s] = __ldcg(a.sxn + s) * 0.0f;
+            a.slopes[nv + s] = __ldcg(a.syn + s) * 0.0f;
+        }
+    }
+}
+
 }  // namespace
 
 extern "C" size_t sb_ccd_binned_scratch_bytes(int rows, int cols, int binning) {
@@ -574,4 +758,70 @@ extern "C" int sb_slopec_batched(const sb_slopec_plan *pl, const float *pixels, 
         return sb::fail(SB_EINVAL, "sb_slopec_batched: strides smaller than one realisation");
     return slopec_impl("sb_slopec_batched", pl, pixels, frame_stride, slopes, slopes_stride, flux, flux_stride,
                        n_batch, scratch, scratch_bytes, stream);
+}
+
+extern "C" size_t sb_sh_ccd_slopec_scratch_bytes(const sb_sh_plan *sh, int n_valid) {
+    const size_t a = sb_sh_scratch_bytes(sh);
+    if (!a || n_valid < 1) return 0;
+    return a + ((3 * (size_t)n_valid * sizeof(float) + 255) & ~(size_t)255);
+}
+
+extern "C" int sb_sh_ccd_slopec(const sb_sh_plan *sh, int dft_mode, const float *A, const float *phase_nm,
+                                const float *A_norm, int n_norm, float photon_scale, float *intensity,
+                                const sb_ccd_params *ccd, float *integrated, float *pixels,
+                                const sb_slopec_plan *slopec, const int32_t *lenslet_subap, float *slopes,
+                                float *flux, void *scratch, size_t scratch_bytes, void *stream) {
+    sb::clear_error();
+    if (!sh || !A || !phase_nm || !A_norm || !intensity || !ccd || !ccd->state || !integrated || !pixels ||
+        !slopec || !slopec->xw || !slopec->yw || !slopec->mw || !lenslet_subap || !slopes || !flux)
+        return sb::fail(SB_EINVAL, "sb_sh_ccd_slopec: null pointer");
+    if (dft_mode != 0 && dft_mode != 1) return sb::fail(SB_EINVAL, "sb_sh_ccd_slopec: dft_mode must be 0 or 1");
+    const int n = sh->n_lenses, npx = sh->subap_npx, side = n * npx;
+    if (n < 1 || npx < 1 || npx > kChainMaxNpx)
+        return sb::fail(SB_ESHAPE, "sb_sh_ccd_slopec: %d detector pixels per sub-aperture (1..%d supported)", npx,
+                        kChainMaxNpx);
+    if (ccd->frames_per_read != 1)
+        return sb::fail(SB_EUNSUPPORTED, "sb_sh_ccd_slopec: the detector must read out every loop step");
+    if (ccd->n_pixels != side * side)
+        return sb::fail(SB_EINVAL, "sb_sh_ccd_slopec: detector of %d pixels for a %d x %d frame", ccd->n_pixels, side,
+                        side);
+    if (ccd->photon_noise && !(ccd->adu_gain > 0.f))
+        return sb::fail(SB_EINVAL, "sb_sh_ccd_slopec: ADU gain must be > 0");
+    if (slopec->npx2 != npx * npx || slopec->n_subaps < 1 || slopec->n_subaps > n * n)
+        return sb::fail(SB_EINVAL, "sb_sh_ccd_slopec: slope plan of %d sub-apertures x %d pixels", slopec->n_subaps,
+                        slopec->npx2);
+    const size_t need = sb_sh_ccd_slopec_scratch_bytes(sh, slopec->n_subaps);
+    if (!scratch || need == 0 || scratch_bytes < need)
+        return sb::fail(SB_ESCRATCH, "sb_sh_ccd_slopec: scratch needs %zu bytes, got %zu", need, scratch_bytes);
+    int nparts = 0;
+    const size_t sh_bytes = sb_sh_scratch_bytes(sh);
+    int rc = sb::sh_forward_unnormalised("sb_sh_ccd_slopec", sh, A, phase_nm, A_norm, n_norm, intensity, scratch,
+                                         sh_bytes, stream, dft_mode, &nparts);
+    if (rc) return rc;
+    ChainArgs a;
+    a.p = *ccd;
+    a.part_I = static_cast<const float *>(scratch);
+    a.part_A = static_cast<const float *>(scratch) + nparts;
+    a.nparts = nparts;
+    a.photon_scale = photon_scale;
+    a.I = intensity;
+    a.integ = integrated;
+    a.pix = pixels;
+    a.n = n;
+    a.npx = npx;
+    a.side = side;
+    a.lenslet_subap = lenslet_subap;
+    a.n_valid = slopec->n_subaps;
+    a.thr = slopec->thr;
+    a.xw = slopec->xw;
+    a.yw = slopec->yw;
+    a.mw = slopec->mw;
+    a.slopes = slopes;
+    a.flux = flux;
+    a.tot = reinterpret_cast<float *>(static_cast<char *>(scratch) + sh_bytes);
+    a.sxn = a.tot + a.n_valid;
+    a.syn = a.sxn + a.n_valid;
+    const dim3 grid((n + kChainLenses - 1) / kChainLenses, n);
+    sh_ccd_slopec_kernel<<<grid, kChainThreads, 0, sb::as_stream(stream)>>>(a);
+    return sb::check_launch("sh_ccd_slopec_kernel");
 }

@@ -929,7 +929,7 @@ namespace {
 int sh_forward_impl(const char *who, const sb_sh_plan *pl, const float *A, long long sA, const float *phase_nm,
                     long long sph, const float *A_norm, long long sAn, int n_norm, float photon_scale,
                     float *intensity, long long sout, int n_batch, void *scratch, size_t scratch_bytes, void *stream,
-                    int mode = 0) {
+                    int mode = 0, bool normalize = true, int *n_parts = nullptr) {
     if (!pl || !A || !phase_nm || !A_norm || !intensity || !pl->twiddle || !pl->tilt || !pl->fp_mask ||
         !pl->rebin)
         return sb::fail(SB_EINVAL, "%s: null pointer", who);
@@ -1005,6 +1005,8 @@ int sh_forward_impl(const char *who, const sb_sh_plan *pl, const float *A, long 
     }
     int rc = sb::check_launch("sh_forward_kernel");
     if (rc) return rc;
+    if (n_parts) *n_parts = nb;
+    if (!normalize) return SB_OK;
     const int n_out = pl->n_lenses * pl->subap_npx * pl->n_lenses * pl->subap_npx;
     int nblk = (n_out + 255) / 256;
     nblk = nblk > 592 ? 592 : nblk;
@@ -1013,6 +1015,15 @@ int sh_forward_impl(const char *who, const sb_sh_plan *pl, const float *A, long 
 }
 
 }  // namespace
+
+namespace sb {
+int sh_forward_unnormalised(const char *who, const sb_sh_plan *pl, const float *A, const float *phase_nm,
+                            const float *A_norm, int n_norm, float *intensity, void *scratch, size_t scratch_bytes,
+                            void *stream, int mode, int *n_parts) {
+    return sh_forward_impl(who, pl, A, 0, phase_nm, 0, A_norm, 0, n_norm, 1.0f, intensity, 0, 1, scratch,
+                           scratch_bytes, stream, mode, false, n_parts);
+}
+}  // namespace sb
 
 extern "C" int sb_sh_forward(const sb_sh_plan *pl, const float *A, const float *phase_nm, const float *A_norm,
                              int n_norm, float photon_scale, float *intensity, void *scratch,

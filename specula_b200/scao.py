@@ -68,6 +68,7 @@ class ScaoConfig:
     seed: int = 1234
     subap_threshold: float = 0.5           # valid sub-apertures: illumination above this fraction (< 0: all)
     noise_seed: int = 1                    # detector seeds: photon noise_seed, read-out noise_seed + 1
+    sh_dft: str = 'fp32'                   # SH DFTs: 'fp32' (CUDA cores) or 'split_bf16' (tensor cores)
 
     @property
     def pitch(self):
@@ -138,7 +139,7 @@ class ScaoLoop:
         self.prop.inputs['common_layer_list'].set([self.pupilstop, self.dm.layer])
         self.sh = SH(wavelengthInNm=c.wavelength_nm, subap_wanted_fov=c.subap_npx * pxs, sensor_pxscale=pxs,
                      subap_on_diameter=c.n_lenses, subap_npx=c.subap_npx, fov_ovs_coeff=c.fov_ovs_coeff,
-                     target_device_idx=device_idx)
+                     dft=c.sh_dft, target_device_idx=device_idx)
         self.sh.inputs['in_ef'].set(self.prop.outputs['out_on_axis_source_ef'])
         side = c.n_lenses * c.subap_npx
         self.ccd = CCD(sp, size=[side, side], dt=c.time_step, bandw=1.0, photon_noise=c.photon_noise,
@@ -191,7 +192,7 @@ class ScaoLoop:
         self.wind_speed.value = vec[1:1 + nl]
         self.wind_direction.value = vec[1 + nl:]
 
-    def capture(self, pipelined=True, io=False, fuse_atmo=None):
+    def capture(self, pipelined=True, io=False, fuse_atmo=None, fuse_chain=None):
         """Capture whole steps in a CUDA graph.  Call after at least one eager
         step, so the time step used by AtmoEvolution is the loop's (the first
         step has delta_time = 0).
@@ -215,6 +216,11 @@ class ScaoLoop:
         bits), which then waits for DM(t-1) as the propagation does; its
         smaller HBM traffic leaves more to the DM projection (ELT step 110.5
         against 113 us).  None: fused whenever the layers allow it.
+
+        ``fuse_chain`` (both forms): SH, CCD and ShSlopec as two launches
+        (sb_sh_ccd_slopec: the SH forward, then normalisation, detector and
+        CoG on each lenslet's pixels in shared memory) instead of five; the
+        same bits.  None: fused whenever the objects allow it.
         """
         self.step_eager()
         torch.cuda.synchronize(self.device)
@@ -225,12 +231,18 @@ class ScaoLoop:
             fuse_atmo = self._can_fuse_atmo()
         fuse_atmo = bool(fuse_atmo and self.pipelined)
         self.fused_atmo = fuse_atmo
+        if fuse_chain is None:
+            fuse_chain = self._can_fuse_chain()
+        self.fused_chain = bool(fuse_chain)
+        if self.fused_chain:
+            self._setup_chain()
         if io and not self.pipelined:
             raise ValueError('ScaoLoop.capture: io slots need the pipelined form (integer integrator delay >= 1)')
         if not self.pipelined:
             with torch.cuda.graph(g):
-                for o in self.objects[:5]:
-                    o.trigger_code()
+                self.atmo.trigger_code()
+                self.prop.trigger_code()
+                self._chain()
                 self._rec_integ()
                 self.dm.trigger_code()
             self.steps_per_replay = 1
@@ -251,7 +263,6 @@ class ScaoLoop:
             self._side = side
             self._cap = cap
             self._bufs = (dm_buf, nxt)
-            chain = [self.sh, self.ccd, self.slopec]
             if io:
                 nsl = self.slopec.slopes.slopes.numel()
                 nm = self.integ.out_comm.value.numel()
@@ -281,8 +292,7 @@ class ScaoLoop:
                         if dm_done is not None:
                             main.wait_event(dm_done)
                         self.prop.trigger_code(phase_override={id(self.dm.layer): dm_buf[1 - par]})
-                    for o in chain:
-                        o.trigger_code()
+                    self._chain()
                     self._rec_integ(out_next=nxt[1 - par])
                     if io:
                         self.io_outputs[step, :nsl].copy_(self.slopec.slopes.slopes)
@@ -295,6 +305,73 @@ class ScaoLoop:
         torch.cuda.synchronize(self.device)
         self.graph = g
         return g
+
+    def _chain(self):
+        """SH, CCD and ShSlopec of one step: two launches when fused, else
+        the three objects' trigger_code."""
+        if self.fused_chain:
+            self._sh_ccd_slopec()
+        else:
+            self.sh.trigger_code()
+            self.ccd.trigger_code()
+            self.slopec.trigger_code()
+
+    def lenslet_subap_map(self):
+        """Valid sub-aperture index of every lenslet (row-major n x n, -1 when
+        not valid), when every row of the sub-aperture table is one lenslet's
+        npx x npx detector box listed row-major; else None."""
+        n, npx = self.cfg.n_lenses, self.cfg.subap_npx
+        side = n * npx
+        idxs = np.asarray(self.subapdata.idxs)
+        if idxs.ndim != 2 or idxs.shape[1] != npx * npx:
+            return None
+        rr, cc = np.meshgrid(np.arange(npx), np.arange(npx), indexing='ij')
+        box = (rr * side + cc).ravel()
+        r0, c0 = idxs[:, 0] // side, idxs[:, 0] % side
+        if np.any(r0 % npx) or np.any(c0 % npx) or np.any(r0 >= side) or np.any(c0 >= side):
+            return None
+        if not np.array_equal(idxs, idxs[:, :1] + box[np.newaxis, :]):
+            return None
+        lens = (r0 // npx) * n + c0 // npx
+        if len(np.unique(lens)) != len(lens):
+            return None
+        out = np.full(n * n, -1, dtype=np.int32)
+        out[lens] = np.arange(len(lens), dtype=np.int32)
+        return out
+
+    def _can_fuse_chain(self):
+        """True when sb_sh_ccd_slopec computes exactly what SH + CCD + ShSlopec
+        do: plain (not interpolated, not LGS) SH with the FP32 or split-BF16
+        DFTs, a detector of the SH frame size reading out every step without
+        binning, the slope computer reading that detector's pixels, and a
+        sub-aperture table of row-major lenslet boxes."""
+        sh, ccd, sl = self.sh, self.ccd, self.slopec
+        return (not sh.geometry.do_interpolation and sh._kernelobj is None and
+                sh._forward in ('sb_sh_forward', 'sb_sh_forward_split_bf16') and
+                ccd._bin_scratch is None and int(ccd._frames_per_read) == 1 and
+                ccd._in_i.i.data_ptr() == sh._out_i.i.data_ptr() and
+                sl._pix.pixels.data_ptr() == ccd._pixels.pixels.data_ptr() and
+                int(sh._plan.subap_npx) <= 16 and self.lenslet_subap_map() is not None)
+
+    def _setup_chain(self):
+        if not self._can_fuse_chain():
+            raise NotImplementedError('ScaoLoop: the fused SH / CCD / slope chain needs a plain SH, a detector read '
+                                      'every step without binning and lenslet-box sub-apertures')
+        self._lenslet_subap = torch.as_tensor(self.lenslet_subap_map(), device=self.device)
+        nb = _lib.load().sb_sh_ccd_slopec_scratch_bytes(ctypes.byref(self.sh._plan), self.slopec._plan.n_subaps)
+        self._chain_scratch = torch.zeros(nb, dtype=torch.uint8, device=self.device)
+
+    def _sh_ccd_slopec(self):
+        sh, ccd, sl = self.sh, self.ccd, self.slopec
+        ef = sh._in_ef
+        st = sh.stream_handle()
+        mode = 0 if sh._forward == 'sb_sh_forward' else 1
+        _lib.call('sb_sh_ccd_slopec', ctypes.byref(sh._plan), mode, ef.A.data_ptr(), ef.phaseInNm.data_ptr(),
+                  ef.A.data_ptr(), ef.A.numel(), sh._photon_scale, sh._out_i.i.data_ptr(), ctypes.byref(ccd._params),
+                  ccd._integrated_i.i.data_ptr(), ccd._pixels.pixels.data_ptr(), ctypes.byref(sl._plan),
+                  self._lenslet_subap.data_ptr(), sl._target.data_ptr(), sl._flux.data_ptr(),
+                  self._chain_scratch.data_ptr(), self._chain_scratch.numel(), st)
+        sl._apply_products(st)
 
     def _can_fuse_atmo(self):
         """True when the fused atmosphere kernel reads every input in its
@@ -367,8 +444,10 @@ class ScaoLoop:
     @property
     def kernels_per_step(self):
         """Kernels of one captured step: one fewer with the atmosphere and
-        the propagation fused."""
-        return self.KERNELS_PER_STEP - (1 if getattr(self, 'fused_atmo', False) else 0)
+        the propagation fused, three fewer with the SH / CCD / slope chain
+        fused (five launches become two)."""
+        return (self.KERNELS_PER_STEP - (1 if getattr(self, 'fused_atmo', False) else 0) -
+                (3 if getattr(self, 'fused_chain', False) else 0))
 
 
 def valid_subaps(pupil, n_lenses, npx, threshold=0.5):

@@ -1,5 +1,6 @@
 """The headline workloads end to end: the captured, pipelined step graph of
-ScaoLoop (fused atmosphere, the default capture) against the oracle chain
+ScaoLoop (the default capture: fused atmosphere, SH / CCD / slopes in two
+launches) against the oracle chain
 run on the same system, step by step, with no re-synchronisation of the
 two loops.
 
@@ -81,7 +82,7 @@ def _run_against_oracle(cfg, n_steps):
     check(0, loop.slopec.slopes.slopes.cpu().numpy(), loop.integ.out_comm.value.cpu().numpy(),
           loop.dm.layer.phaseInNm.cpu().numpy())
     loop.capture(io=True)
-    assert loop.pipelined and loop.fused_atmo and loop.kernels_per_step == 9
+    assert loop.pipelined and loop.fused_atmo and loop.fused_chain and loop.kernels_per_step == 6
     check(1, loop.slopec.slopes.slopes.cpu().numpy(), loop.integ.out_comm.value.cpu().numpy(),
           loop.dm.layer.phaseInNm.cpu().numpy())
     dm_buf = loop._bufs[0]

@@ -35,6 +35,8 @@ def _loop(mode, n_steps, cfg_kw=None, strided_stop=False):
     else:
         if mode == 'pipelined_default':
             loop.capture()
+        elif mode == 'pipelined_unfused_chain':
+            loop.capture(fuse_chain=False)
         else:
             loop.capture(pipelined=mode.startswith('pipelined'), fuse_atmo=(mode == 'pipelined_fused'))
         done += 1
@@ -46,14 +48,17 @@ def _loop(mode, n_steps, cfg_kw=None, strided_stop=False):
     return loop
 
 
-@pytest.mark.parametrize('mode', ['sequential', 'pipelined', 'pipelined_fused'])
+@pytest.mark.parametrize('mode', ['sequential', 'pipelined', 'pipelined_fused', 'pipelined_unfused_chain'])
 def test_graph_step_matches_object_loop(mode, cuda):
-    """pipelined_fused: AtmoEvolution and AtmoPropagation as one launch."""
+    """pipelined_fused: AtmoEvolution and AtmoPropagation as one launch;
+    every mode but pipelined_unfused_chain runs SH, CCD and ShSlopec as the
+    two launches of sb_sh_ccd_slopec."""
     n = 10
     ref = _loop('eager', n)
     got = _loop(mode, n)
     if mode.startswith('pipelined'):
         assert got.pipelined and got.steps_per_replay == 2
+    assert got.fused_chain == (mode != 'pipelined_unfused_chain')
     for name, a, b in (('slopes', ref.slopec.slopes.slopes, got.slopec.slopes.slopes),
                        ('dm phase', ref.dm.layer.phaseInNm, got.dm.layer.phaseInNm),
                        ('commands', ref.integ.out_comm.value, got.integ.out_comm.value),
@@ -73,22 +78,24 @@ def _assert_same_loop_state(ref, got):
 
 
 def test_default_capture_fuses_the_atmosphere(cuda):
-    """capture() with no arguments picks the fused atmosphere for the SCAO
-    layout: 9 kernels per step, the same bits as the object loop."""
+    """capture() with no arguments picks the fused atmosphere and the fused
+    SH / CCD / slope chain for the SCAO layout: 6 kernels per step, the same
+    bits as the object loop."""
     n = 6
     ref = _loop('eager', n)
     got = _loop('pipelined_default', n)
-    assert got.pipelined and got.fused_atmo and got.kernels_per_step == 9
+    assert got.pipelined and got.fused_atmo and got.fused_chain and got.kernels_per_step == 6
     _assert_same_loop_state(ref, got)
 
 
 def test_default_capture_falls_back_for_a_strided_stop(cuda):
-    """A pupil stop that is not a dense L x L array keeps the two launches
-    (10 kernels per step), with the same bits as the object loop."""
+    """A pupil stop that is not a dense L x L array keeps the two atmosphere
+    launches (7 kernels per step with the fused chain), with the same bits as
+    the object loop."""
     n = 6
     ref = _loop('eager', n, strided_stop=True)
     got = _loop('pipelined_default', n, strided_stop=True)
-    assert got.pipelined and not got.fused_atmo and got.kernels_per_step == 10
+    assert got.pipelined and not got.fused_atmo and got.fused_chain and got.kernels_per_step == 7
     _assert_same_loop_state(ref, got)
     plain = _loop('eager', n)
     assert torch.equal(ref.slopec.slopes.slopes, plain.slopec.slopes.slopes)
