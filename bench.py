@@ -57,6 +57,9 @@ def parse():
     p.add_argument('--profile-batched', action='store_true',
                    help='set up the batched Monte-Carlo graph (split-BF16 SH, autotuned), then run one replay '
                         'between cudaProfilerStart/Stop (for ncu --profile-from-start off) and exit')
+    p.add_argument('--profile-loop', type=int, default=0, metavar='R',
+                   help='set up the ELT step graph, then run R replays between cudaProfilerStart/Stop '
+                        '(for ncu --profile-from-start off) and exit')
     p.add_argument('--batched-only', action='store_true',
                    help='run only the 96-realisation batched Monte-Carlo leg (one GPU)')
     p.add_argument('--adjoint-only', action='store_true',
@@ -73,19 +76,55 @@ def config_dict(cfg, n_gpus):
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled every 200 ms in the background."""
+    """SM clock and clock-event reasons of one GPU, polled every millisecond
+    by a background thread through NVML (read-only queries) while the timed
+    region runs; nvidia-smi at 50 ms when NVML cannot be loaded.  The timed
+    region of a short run lasts a few milliseconds, so the 1 ms poll is what
+    gives it samples of its own."""
+    REASONS = (('hw_slowdown', 'nvmlClocksEventReasonHwSlowdown'),
+               ('hw_thermal_slowdown', 'nvmlClocksEventReasonHwThermalSlowdown'),
+               ('sw_thermal_slowdown', 'nvmlClocksEventReasonSwThermalSlowdown'),
+               ('sw_power_cap', 'nvmlClocksEventReasonSwPowerCap'))
     FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
               'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
               'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
 
     def __init__(self, gpu_index):
-        self.gpu = str(gpu_index)
+        self.gpu = int(gpu_index)
         self.proc = None
+        self.nvml = None
         self.lines = []
+        self.sm = []
+        self.reasons = set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self.thread = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        uuid = str(getattr(torch.cuda.get_device_properties(self.gpu), 'uuid', '') or '')
+        if uuid:
+            try:
+                return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith('GPU-') else 'GPU-' + uuid)
+            except Exception:
+                pass
+        return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(['nvidia-smi', '-i', self.gpu, f'--query-gpu={self.FIELDS}',
+            self.nvml = self._nvml_handle()
+        except Exception:
+            self.nvml = None
+        if self.nvml is not None:
+            nv, h = self.nvml
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.gpu), f'--query-gpu={self.FIELDS}',
                                           '--format=csv,noheader,nounits', '-lms', '50'],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
@@ -93,11 +132,32 @@ class ClockSampler:
         except (OSError, FileNotFoundError):
             self.proc = None
 
+    def _poll(self):
+        nv, h = self.nvml
+        masks = [(name, getattr(nv, attr, 0)) for name, attr in self.REASONS]
+        while not self._stop.is_set():
+            try:
+                self.sm.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                for name, m in masks:
+                    if m and r & m:
+                        self.reasons.add(name)
+            except Exception:
+                break
+            time.sleep(0.001)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def stop(self):
+        if self.nvml is not None:
+            self._stop.set()
+            self.thread.join(timeout=5)
+            if not self.sm:
+                return None
+            return {'sm_mhz': statistics.median(self.sm), 'sm_max_mhz': self.max_mhz,
+                    'reasons': sorted(self.reasons), 'samples': len(self.sm), 'source': 'nvml, 1 ms poll'}
         if self.proc is None:
             return None
         self.proc.terminate()
@@ -106,7 +166,7 @@ class ClockSampler:
         except subprocess.TimeoutExpired:
             self.proc.kill()
         sm, mx, reasons = [], None, set()
-        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        names = [n for n, _ in self.REASONS]
         for l in self.lines:
             f = [x.strip() for x in l.split(',')]
             if len(f) < 9:
@@ -121,7 +181,8 @@ class ClockSampler:
                     reasons.add(n)
         if not sm:
             return None
-        return {'sm_mhz': statistics.median(sm), 'sm_max_mhz': mx, 'reasons': sorted(reasons), 'samples': len(sm)}
+        return {'sm_mhz': statistics.median(sm), 'sm_max_mhz': mx, 'reasons': sorted(reasons), 'samples': len(sm),
+                'source': 'nvidia-smi, 50 ms'}
 
 
 def measured_peak_hbm():
@@ -758,6 +819,29 @@ def run_b200(args):
         dist.destroy_process_group()
 
 
+def profile_loop(dev, replays):
+    """The headline step graph (ELT workload) set up and warmed, then
+    ``replays`` replays (two steps each) between cudaProfilerStart/Stop, for
+    ncu --profile-from-start off."""
+    import torch
+    from specula_b200.scao import ScaoLoop, elt_config
+    loop = ScaoLoop(elt_config(), device_idx=dev.index)
+    loop.start()
+    loop.step_eager()
+    loop.capture()
+    for _ in range(3):
+        loop.replay()
+    torch.cuda.synchronize(dev)
+    torch.cuda.cudart().cudaProfilerStart()
+    for _ in range(replays):
+        loop.replay()
+    torch.cuda.synchronize(dev)
+    torch.cuda.cudart().cudaProfilerStop()
+    _lib_status()
+    print(json.dumps({'profiled_replays': replays, 'steps_per_replay': loop.steps_per_replay,
+                      'kernels_per_step': loop.kernels_per_step}), flush=True)
+
+
 def profile_batched(dev):
     """One replay of the batched graph bracketed for a profiler."""
     import torch
@@ -778,6 +862,12 @@ def profile_batched(dev):
 
 def main():
     args = parse()
+    if args.profile_loop:
+        import torch
+        dev = torch.device('cuda', 0)
+        torch.cuda.set_device(dev)
+        profile_loop(dev, args.profile_loop)
+        return
     if args.profile_batched:
         import torch
         dev = torch.device('cuda', 0)

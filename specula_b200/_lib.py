@@ -143,6 +143,8 @@ SIGNATURES = {
     'sb_sh_slopes_vjp': (C.c_int, [C.POINTER(ShPlan), fp, fp, C.c_int, ip, fp, fp, fp, fp, fp, fp, vp]),
     'sb_intmat_contract': (C.c_int, [fp, fp, C.c_int, C.c_int, C.c_int, C.c_int, ip, ip, fp, C.c_int, C.c_int,
                                      C.c_float, fp, vp]),
+    'sb_intmat_contract_rows': (C.c_int, [fp, fp, C.c_int, C.c_int, C.c_int, C.c_int, ip, ip, ip, C.c_int, fp,
+                                          C.c_int, C.c_int, C.c_float, fp, vp]),
 }
 
 _lib = None

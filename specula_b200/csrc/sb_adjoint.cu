@@ -17,6 +17,7 @@
 // influence-function element is read once.
 #include "sb_common.cuh"
 #include "sb_dft.cuh"
+#include "sb_tma.cuh"
 
 namespace {
 
@@ -404,6 +405,195 @@ extern "C" int sb_sh_slopes_vjp(const sb_sh_plan *pl, const float *A, const floa
                           nullptr, grad_phase, stream);
 }
 
+// ---------------------------------------------------------------------------
+// The same contraction with the influence functions streamed by bulk copies.
+// The mirror's influence-function columns enumerate its pixels row-major, so
+// the np_sub field rows of lenslet row li fall inside one contiguous column
+// range of every mode's row: row_seg[li] = {start, count} (floats, both
+// multiples of 4).  A persistent CTA walks work items (lenslet row, chunk of
+// modes); one producer lane copies each mode's segment into a shared-memory
+// ring (cp.async.bulk, L2 evict-first, one copy per mode and lenslet row) and
+// the consumer warps, one thread per field column as in
+// intmat_contract_kernel, read their np_sub samples from shared memory.  The
+// products, their order and the cut-off are those of intmat_contract_kernel,
+// so the matrices are the same bits.  Every wait is bounded: on timeout the
+// kernel records it in g_contract_status, stops issuing, lets the copies in
+// flight land (bounded) and returns.
+// ---------------------------------------------------------------------------
+constexpr int kCbMaxStages = 8;
+constexpr int kCbMaxConsumers = 992;   // field columns (+ one producer warp <= 1024 threads)
+
+__device__ int g_contract_status = 0;
+
+struct ContractBulkArgs {
+    const float *jac;
+    const float *tot;
+    int n_valid, n, field_ld;
+    const int32_t *slot;
+    const int32_t *pix2col;
+    const int32_t *row_seg;
+    const float *IF;
+    int n_modes, ld_if;
+    float scale;
+    float *im;
+    int stages, stage_floats;
+};
+
+// Columns streamed for lenslet row li: 0 when the row has none, or when its
+// segment is not 16-byte aligned or does not fit the row or a ring stage
+// (recorded in g_contract_status; nothing is copied for it).
+__device__ __forceinline__ int seg_count(const ContractBulkArgs &a, int li) {
+    const int start = a.row_seg[2 * li], cnt = a.row_seg[2 * li + 1];
+    if (cnt <= 0) return 0;
+    if (start < 0 || (start & 3) || (cnt & 3) || cnt > a.stage_floats || (long long)start + cnt > a.ld_if) {
+        atomicExch(&g_contract_status, 3);
+        return 0;
+    }
+    return cnt;
+}
+
+template <int P>
+__global__ void __launch_bounds__(1024, 1) intmat_contract_bulk_kernel(ContractBulkArgs a) {
+    extern __shared__ __align__(128) unsigned char cb_smem[];
+    float *ring = reinterpret_cast<float *>(cb_smem);
+    uint64_t *full = reinterpret_cast<uint64_t *>(cb_smem + (size_t)a.stages * a.stage_floats * 4);
+    uint64_t *empty = full + a.stages;
+    __shared__ double red[33];
+    __shared__ int abort_flag, issued;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int ncons = blockDim.x - 32;           // consumer threads (a multiple of 32)
+    const int nwc = ncons >> 5;
+    const int S = a.stages;
+    if (tid == 0) {
+        for (int k = 0; k < S; ++k) {
+            sb::mbar_init(&full[k], 1);
+            sb::mbar_init(&empty[k], nwc);
+        }
+        sb::mbar_init_fence();
+        abort_flag = 0;
+        issued = 0;
+    }
+    // the CoG cut-off's mean, summed as intmat_contract_kernel sums it (the
+    // producer warp adds zeros)
+    double mean = 0.0;
+    if (a.tot) {
+        double part = 0.0;
+        if (tid < ncons)
+            for (int e = tid; e < a.n_valid; e += ncons) part += (double)a.tot[e];
+        mean = sb::block_sum_all_d(part, red) / a.n_valid;
+    }
+    __syncthreads();
+    const int chunks = (a.n_modes + kContractModes - 1) / kContractModes;
+    const int n_items = chunks * a.n;
+    const size_t ld_im = 2 * (size_t)a.n_valid;
+    if (warp == nwc) {
+        if (lane == 0) {
+            const uint64_t pol = sb::l2_evict_first_policy();
+            int q = 0;
+            bool stop = false;
+            for (int w = blockIdx.x; w < n_items && !stop; w += gridDim.x) {
+                const int li = w % a.n, m0 = (w / a.n) * kContractModes;
+                const int m1 = min(a.n_modes, m0 + kContractModes);
+                const int cnt = seg_count(a, li);
+                if (cnt <= 0) continue;
+                const int start = a.row_seg[2 * li];
+                for (int m = m0; m < m1; ++m, ++q) {
+                    const int st = q % S;
+                    if (q >= S && !sb::mbar_wait(&empty[st], ((q / S) - 1) & 1)) {
+                        atomicExch(&g_contract_status, 1);
+                        abort_flag = 1;
+                        stop = true;
+                        break;
+                    }
+                    if (*(volatile int *)&abort_flag) {
+                        stop = true;
+                        break;
+                    }
+                    sb::mbar_arrive_expect_tx(&full[st], (uint32_t)cnt * 4u);
+                    sb::bulk_load_1d(ring + (size_t)st * a.stage_floats, a.IF + (size_t)m * a.ld_if + start,
+                                     (uint32_t)cnt * 4u, &full[st], pol);
+                }
+            }
+            issued = q;
+        }
+    } else {
+        const int x = tid;
+        const int lj = x / P, c = x - lj * P;
+        int q = 0;
+        for (int w = blockIdx.x; w < n_items; w += gridDim.x) {
+            const int li = w % a.n, m0 = (w / a.n) * kContractModes;
+            const int m1 = min(a.n_modes, m0 + kContractModes);
+            const int cnt = seg_count(a, li);
+            const int start = a.row_seg[2 * li];
+            const int s = (lj < a.n) ? a.slot[li * a.n + lj] : -1;
+            bool act = s >= 0;
+            if (a.tot && act) {
+                const float t = a.tot[s];
+                act = t > 0.f && (double)(1.0f / t) <= 1.0 / (mean * 1e-3);
+            }
+            float jx[P], jy[P];
+            int off[P];
+#pragma unroll
+            for (int rr = 0; rr < P; ++rr) {
+                off[rr] = -1;
+                jx[rr] = jy[rr] = 0.f;
+                if (act) {
+                    const int col = a.pix2col[(size_t)(li * P + rr) * a.field_ld + x];
+                    if (col >= 0 && (col < start || col - start >= cnt)) {
+                        atomicExch(&g_contract_status, 3);      // a column outside its row's segment
+                    } else if (col >= 0) {
+                        off[rr] = col - start;
+                    }
+                    jx[rr] = a.jac[(size_t)s * (P * P) + rr * P + c];
+                    jy[rr] = a.jac[((size_t)a.n_valid + s) * (P * P) + rr * P + c];
+                }
+            }
+            bool failed = false;
+            for (int m = m0; m < m1; ++m) {
+                float vx = 0.f, vy = 0.f;
+                if (cnt > 0) {
+                    const int st = q % S;
+                    if (!sb::mbar_wait(&full[st], (q / S) & 1)) {
+                        atomicExch(&g_contract_status, 2);
+                        abort_flag = 1;
+                        failed = true;
+                        break;
+                    }
+                    if (*(volatile int *)&abort_flag) {
+                        failed = true;
+                        break;
+                    }
+                    const float *seg = ring + (size_t)st * a.stage_floats;
+#pragma unroll
+                    for (int rr = 0; rr < P; ++rr) {
+                        const float f = off[rr] >= 0 ? seg[off[rr]] : 0.f;
+                        vx = fmaf(jx[rr], f, vx);
+                        vy = fmaf(jy[rr], f, vy);
+                    }
+                    __syncwarp();
+                    if (lane == 0) sb::mbar_arrive(&empty[st]);
+                    ++q;
+                }
+#pragma unroll
+                for (int o = P / 2; o > 0; o >>= 1) {
+                    vx += __shfl_down_sync(0xffffffffu, vx, o, P);
+                    vy += __shfl_down_sync(0xffffffffu, vy, o, P);
+                }
+                if (c == 0 && s >= 0) {
+                    a.im[(size_t)m * ld_im + s] = a.scale * vx;
+                    a.im[(size_t)m * ld_im + a.n_valid + s] = a.scale * vy;
+                }
+            }
+            if (failed) break;
+        }
+    }
+    __syncthreads();
+    if (abort_flag && tid == ncons) {
+        // let every issued copy land before the shared memory is released
+        for (int q = 0; q < issued; ++q) sb::mbar_wait(&full[q % S], (q / S) & 1);
+    }
+}
+
 extern "C" int sb_intmat_contract(const float *jac, const float *tot, int n_valid, int np_sub, int n_lenses,
                                   int field_ld, const int32_t *slot, const int32_t *pix2col, const float *ifunc,
                                   int n_modes, int ld_if, float scale, float *intmat, void *stream) {
@@ -437,4 +627,82 @@ extern "C" int sb_intmat_contract(const float *jac, const float *tot, int n_vali
         return sb::fail(SB_EUNSUPPORTED, "sb_intmat_contract: np_sub=%d (4, 8 or 16)", np_sub);
     }
     return sb::check_launch("intmat_contract_kernel");
+}
+
+namespace sb {
+// read and clear the timeout flag of the bulk-copy contraction (0: none, <0: query failed)
+int contract_status_take() {
+    int v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_contract_status, sizeof(int)) != cudaSuccess) return -1;
+    if (v) {
+        const int zero = 0;
+        cudaMemcpyToSymbol(g_contract_status, &zero, sizeof(int));
+    }
+    return v;
+}
+}  // namespace sb
+
+extern "C" int sb_intmat_contract_rows(const float *jac, const float *tot, int n_valid, int np_sub, int n_lenses,
+                                       int field_ld, const int32_t *slot, const int32_t *pix2col,
+                                       const int32_t *row_seg, int seg_max, const float *ifunc, int n_modes,
+                                       int ld_if, float scale, float *intmat, void *stream) {
+    sb::clear_error();
+    if (!jac || !slot || !pix2col || !row_seg || !ifunc || !intmat || n_valid < 1 || n_modes < 0 ||
+        n_lenses < 1 || ld_if < 1 || seg_max < 0)
+        return sb::fail(SB_EINVAL, "sb_intmat_contract_rows: bad args");
+    if (field_ld < n_lenses * np_sub) return sb::fail(SB_EINVAL, "sb_intmat_contract_rows: bad field stride");
+    if (ld_if % 4 || (uintptr_t)ifunc % 16 || seg_max % 4)
+        return sb::fail(SB_EINVAL, "sb_intmat_contract_rows: influence-function rows and segments must be 16-byte "
+                                   "aligned (ld_if %% 4 == 0, 16-byte base, seg_max %% 4 == 0)");
+    const int ncons = (n_lenses * np_sub + 31) / 32 * 32;
+    if (ncons > kCbMaxConsumers)
+        return sb::fail(SB_ESHAPE, "sb_intmat_contract_rows: field of %d columns (at most %d)", n_lenses * np_sub,
+                        kCbMaxConsumers);
+    if (n_modes == 0) return SB_OK;
+    const int stage_floats = seg_max > 0 ? seg_max : 4;
+    int stages = (int)((96 * 1024) / ((size_t)stage_floats * 4));
+    stages = stages > kCbMaxStages ? kCbMaxStages : stages;
+    if (stages < 2)
+        return sb::fail(SB_ESHAPE, "sb_intmat_contract_rows: segments of %d floats exceed the shared-memory ring",
+                        seg_max);
+    const size_t smem = (size_t)stages * stage_floats * 4 + 2 * (size_t)stages * 8;
+    ContractBulkArgs a;
+    a.jac = jac;
+    a.tot = tot;
+    a.n_valid = n_valid;
+    a.n = n_lenses;
+    a.field_ld = field_ld;
+    a.slot = slot;
+    a.pix2col = pix2col;
+    a.row_seg = row_seg;
+    a.IF = ifunc;
+    a.n_modes = n_modes;
+    a.ld_if = ld_if;
+    a.scale = scale;
+    a.im = intmat;
+    a.stages = stages;
+    a.stage_floats = stage_floats;
+    void (*fn)(ContractBulkArgs) = nullptr;
+    switch (np_sub) {
+    case 4: fn = intmat_contract_bulk_kernel<4>; break;
+    case 8: fn = intmat_contract_bulk_kernel<8>; break;
+    default:
+        return sb::fail(SB_EUNSUPPORTED, "sb_intmat_contract_rows: np_sub=%d (4 or 8)", np_sub);
+    }
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess)
+        return sb::fail(SB_ECUDA, "sb_intmat_contract_rows: smem attribute: %s", cudaGetErrorString(e));
+    const int threads = ncons + 32;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
+    if (e != cudaSuccess || per_sm < 1)
+        return sb::fail(SB_ECUDA, "sb_intmat_contract_rows: occupancy query: %s",
+                        e != cudaSuccess ? cudaGetErrorString(e) : "no CTA fits an SM");
+    const int nsm = sb::sm_count();
+    if (nsm < 1) return sb::fail(SB_ECUDA, "sb_intmat_contract_rows: SM count query failed");
+    const int chunks = (n_modes + kContractModes - 1) / kContractModes;
+    int grid = per_sm * nsm;
+    grid = grid > chunks * n_lenses ? chunks * n_lenses : grid;
+    fn<<<grid, threads, smem, sb::as_stream(stream)>>>(a);
+    return sb::check_launch("intmat_contract_bulk_kernel");
 }

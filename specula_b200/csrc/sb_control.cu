@@ -731,7 +731,14 @@ extern "C" int sb_device_status(void) {
         return sb::fail(SB_ECUDA, "sb_device_status: %s", cudaGetErrorString(cudaGetLastError()));
     const int sh = sb::sh_tc_status_take();
     if (sh < 0) return sb::fail(SB_ECUDA, "sb_device_status: %s", cudaGetErrorString(cudaGetLastError()));
-    if (v == 0 && sh == 0) return SB_OK;
+    const int ct = sb::contract_status_take();
+    if (ct < 0) return sb::fail(SB_ECUDA, "sb_device_status: %s", cudaGetErrorString(cudaGetLastError()));
+    if (v == 0 && sh == 0 && ct == 0) return SB_OK;
+    if (v == 0 && sh == 0)
+        return ct == 3 ? sb::fail(SB_EINVAL, "sb_intmat_contract_rows: a row segment does not cover its columns or "
+                                             "is not 16-byte aligned (those rows were not contracted)")
+                       : sb::fail(SB_ETIMEOUT, "an interaction-matrix contraction wait timed out (%s side)",
+                                  ct == 1 ? "producer" : "consumer");
     if (v == 0) return sb::fail(SB_ETIMEOUT, "a tensor-core SH wait timed out (stage %d)", sh);
     const int zero = 0;
     cudaMemcpyToSymbol(g_dm_status, &zero, sizeof(int));

@@ -54,6 +54,31 @@ def pixel_to_column(mask_idx, dm_shape, field_size, top=0, left=0):
     return out
 
 
+def row_segments(pix2col, lenslets, n_lenses, np_sub, field, ld_if):
+    """Per lenslet row the influence-function columns the contraction reads:
+    (start, count) in floats, both multiples of 4, covering every mirror
+    column under a valid sub-aperture of that row (columns enumerate the
+    mirror's pixels row-major, so np_sub consecutive field rows map to one
+    contiguous range).  Returns the (n_lenses, 2) int32 table and the largest
+    count."""
+    p2c = np.asarray(pix2col).reshape(field, field)
+    seg = np.zeros((n_lenses, 2), dtype=np.int32)
+    lens = np.asarray(lenslets, dtype=np.int64)
+    for li in range(n_lenses):
+        cols = [p2c[li * np_sub:(li + 1) * np_sub, lj * np_sub:(lj + 1) * np_sub]
+                for lj in (lens[lens // n_lenses == li] % n_lenses)]
+        if not cols:
+            continue
+        c = np.concatenate([x.ravel() for x in cols])
+        c = c[c >= 0]
+        if c.size == 0:
+            continue
+        start = int(c.min()) & ~3
+        end = min((int(c.max()) + 1 + 3) & ~3, int(ld_if))
+        seg[li] = (start, end - start)
+    return seg, int(seg[:, 1].max()) if n_lenses else 0
+
+
 class ShSlopesAdjoint:
     """Jacobian / VJP of the slopes of a set-up ``SH`` + ``ShSlopec`` pair
     with respect to the SH input phase (nm), and the adjoint interaction
@@ -197,10 +222,40 @@ class ShSlopesAdjoint:
             pix2col = self.pixel_to_column(dm, top, left)
         n_modes = dm._IF.shape[0]
         im = torch.empty((n_modes, 2 * self.n_valid), dtype=torch.float32, device=self.device)
-        _lib.call('sb_intmat_contract', jac.data_ptr(), 0 if tot is None else tot.data_ptr(), self.n_valid,
-                  self.np_sub, self.n_lenses, self.field, self._slot.data_ptr(), pix2col.data_ptr(), dm._IF.data_ptr(),
-                  n_modes, dm._ld, float(2.0 * dm.sign), im.data_ptr(), self._stream())
+        segs = self._segments(pix2col, dm)
+        tot_ptr = 0 if tot is None else tot.data_ptr()
+        if segs is not None:
+            _lib.call('sb_intmat_contract_rows', jac.data_ptr(), tot_ptr, self.n_valid, self.np_sub, self.n_lenses,
+                      self.field, self._slot.data_ptr(), pix2col.data_ptr(), segs[0].data_ptr(), segs[1],
+                      dm._IF.data_ptr(), n_modes, dm._ld, float(2.0 * dm.sign), im.data_ptr(), self._stream())
+        else:
+            _lib.call('sb_intmat_contract', jac.data_ptr(), tot_ptr, self.n_valid, self.np_sub, self.n_lenses,
+                      self.field, self._slot.data_ptr(), pix2col.data_ptr(), dm._IF.data_ptr(), n_modes, dm._ld,
+                      float(2.0 * dm.sign), im.data_ptr(), self._stream())
         return im
+
+    # bulk-copy contraction limits: np_sub 4 or 8, at most 992 field columns,
+    # 16-byte aligned influence-function rows, a row segment within 96 KB / 2
+    BULK_NP_SUB = (4, 8)
+    BULK_MAX_COLUMNS = 992
+    BULK_MAX_SEGMENT = 96 * 1024 // 4 // 2
+
+    def _segments(self, pix2col, dm):
+        """(device table, largest count) of the row segments for the
+        bulk-copy contraction, or None when its limits are not met (then the
+        gather kernel runs); cached per mirror column map."""
+        if (self.np_sub not in self.BULK_NP_SUB or self.field > self.BULK_MAX_COLUMNS or dm._ld % 4 or
+                dm._IF.data_ptr() % 16):
+            return None
+        key = (pix2col.data_ptr(), int(dm._ld))
+        cache = getattr(self, '_seg_cache', None)
+        if cache is None or cache[0] != key:
+            seg, seg_max = row_segments(pix2col.cpu().numpy(), self._lenslet.cpu().numpy(), self.n_lenses,
+                                        self.np_sub, self.field, dm._ld)
+            val = None if seg_max > self.BULK_MAX_SEGMENT else (torch.as_tensor(seg, device=self.device), seg_max)
+            cache = (key, val, pix2col)
+            self._seg_cache = cache
+        return cache[1]
 
     # -- push-pull on the same chain -----------------------------------------
     def pushpull_intmat(self, A, dm, amplitudes, graph=True):
