@@ -438,18 +438,19 @@ int sb_intmat_contract(const float *jac, const float *tot, int n_valid, int np_s
                        const int32_t *slot, const int32_t *pix2col, const float *ifunc, int n_modes,
                        int ld_if, float scale, float *intmat, void *stream);
 
-/* sb_intmat_contract with the influence functions streamed by bulk copies
- * (the same contraction as im_rec_calibrator.py:58-63 in its small-amplitude
- * limit; the same matrix bit for bit).  The mirror's columns enumerate its
- * pixels row-major, so the np_sub field rows of lenslet row li lie in one
- * column range: row_seg[2*li] = first column, row_seg[2*li+1] = number of
- * columns (both multiples of 4, covering every column under a valid
- * sub-aperture of that row; 0 columns for a row without any), seg_max = the
- * largest count.  One mode's segment of one lenslet row is one copy into a
- * shared-memory ring of up to 8 stages (96 KB).  Needs ld_if a multiple of
- * 4, a 16-byte aligned ifunc, np_sub 4 or 8 and at most 992 field columns;
- * a segment that is misaligned or misses a column is skipped and reported
- * by sb_device_status (SB_EINVAL), as are timed-out waits (SB_ETIMEOUT). */
+/* sb_intmat_contract with the influence functions streamed by TMA (the same
+ * contraction as im_rec_calibrator.py:58-63 in its small-amplitude limit; the
+ * same matrix bit for bit).  The mirror's columns enumerate its pixels
+ * row-major, so the np_sub field rows of lenslet row li lie in one column
+ * range: row_seg[2*li] = first column, row_seg[2*li+1] = number of columns
+ * (both multiples of 32, covering every column under a valid sub-aperture of
+ * that row; 0 columns for a row without any), seg_max = the largest count
+ * (<= 8192).  One mode's segment of one lenslet row is one TMA box loaded
+ * into a shared-memory ring of up to 8 stages (96 KB).  Needs ld_if a
+ * multiple of 32, a 16-byte aligned ifunc, np_sub 4 or 8 and at most 992
+ * field columns; a segment that is misaligned or misses a column is skipped
+ * and reported by sb_device_status (SB_EINVAL), as are timed-out waits
+ * (SB_ETIMEOUT). */
 int sb_intmat_contract_rows(const float *jac, const float *tot, int n_valid, int np_sub, int n_lenses,
                             int field_ld, const int32_t *slot, const int32_t *pix2col, const int32_t *row_seg,
                             int seg_max, const float *ifunc, int n_modes, int ld_if, float scale, float *intmat,

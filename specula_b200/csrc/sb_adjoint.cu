@@ -406,26 +406,27 @@ extern "C" int sb_sh_slopes_vjp(const sb_sh_plan *pl, const float *A, const floa
 }
 
 // ---------------------------------------------------------------------------
-// The same contraction with the influence functions streamed by bulk copies.
-// The mirror's influence-function columns enumerate its pixels row-major, so
+// The same contraction with the influence functions streamed by TMA.  The
+// mirror's influence-function columns enumerate its pixels row-major, so
 // the np_sub field rows of lenslet row li fall inside one contiguous column
 // range of every mode's row: row_seg[li] = {start, count} (floats, both
-// multiples of 4).  A persistent CTA walks work items (lenslet row, chunk of
-// modes); one producer lane copies each mode's segment into a shared-memory
-// ring (cp.async.bulk, L2 evict-first, one copy per mode and lenslet row) and
-// the consumer warps, one thread per field column as in
-// intmat_contract_kernel, read their np_sub samples from shared memory.  The
-// products, their order and the cut-off are those of intmat_contract_kernel,
-// so the matrices are the same bits.  Every wait is bounded: on timeout the
-// kernel records it in g_contract_status, stops issuing, lets the copies in
-// flight land (bounded) and returns.
+// multiples of 32).  The matrix is seen as modes x (ld_if / 32) chunks of 32
+// floats (a 3-D tensor map) and one box of seg_max / 32 chunks of one mode
+// is that mode's segment.  A persistent CTA walks work items (lenslet row,
+// chunk of modes); one producer lane loads each mode's box into a
+// shared-memory ring (L2 evict-first) and the consumer warps, one thread per
+// field column as in intmat_contract_kernel, read their np_sub samples from
+// shared memory.  The products, their order and the cut-off are those of
+// intmat_contract_kernel, so the matrices are the same bits.  Every wait is
+// bounded: on timeout the kernel records it in g_contract_status, stops
+// issuing, lets the copies in flight land (bounded) and returns.
 // ---------------------------------------------------------------------------
 constexpr int kCbMaxStages = 8;
 constexpr int kCbMaxConsumers = 992;   // field columns (+ one producer warp <= 1024 threads)
 
 __device__ int g_contract_status = 0;
 
-struct ContractBulkArgs {
+struct ContractTmaArgs {
     const float *jac;
     const float *tot;
     int n_valid, n, field_ld;
@@ -440,12 +441,12 @@ struct ContractBulkArgs {
 };
 
 // Columns streamed for lenslet row li: 0 when the row has none, or when its
-// segment is not 16-byte aligned or does not fit the row or a ring stage
+// segment is not on 32-float boundaries or does not fit the row or a ring stage
 // (recorded in g_contract_status; nothing is copied for it).
-__device__ __forceinline__ int seg_count(const ContractBulkArgs &a, int li) {
+__device__ __forceinline__ int seg_count(const ContractTmaArgs &a, int li) {
     const int start = a.row_seg[2 * li], cnt = a.row_seg[2 * li + 1];
     if (cnt <= 0) return 0;
-    if (start < 0 || (start & 3) || (cnt & 3) || cnt > a.stage_floats || (long long)start + cnt > a.ld_if) {
+    if (start < 0 || (start & 31) || (cnt & 31) || cnt > a.stage_floats || (long long)start + cnt > a.ld_if) {
         atomicExch(&g_contract_status, 3);
         return 0;
     }
@@ -453,10 +454,13 @@ __device__ __forceinline__ int seg_count(const ContractBulkArgs &a, int li) {
 }
 
 template <int P>
-__global__ void __launch_bounds__(1024, 1) intmat_contract_bulk_kernel(ContractBulkArgs a) {
+__global__ void __launch_bounds__(1024, 1) intmat_contract_tma_kernel(const __grid_constant__ CUtensorMap map,
+                                                                      ContractTmaArgs a) {
     extern __shared__ __align__(128) unsigned char cb_smem[];
-    float *ring = reinterpret_cast<float *>(cb_smem);
-    uint64_t *full = reinterpret_cast<uint64_t *>(cb_smem + (size_t)a.stages * a.stage_floats * 4);
+    // TMA destinations on 128-byte boundaries (stages are multiples of 128 bytes)
+    unsigned char *base = cb_smem + ((128 - (sb::smem_u32(cb_smem) & 127)) & 127);
+    float *ring = reinterpret_cast<float *>(base);
+    uint64_t *full = reinterpret_cast<uint64_t *>(base + (size_t)a.stages * a.stage_floats * 4);
     uint64_t *empty = full + a.stages;
     __shared__ double red[33];
     __shared__ int abort_flag, issued;
@@ -509,9 +513,9 @@ __global__ void __launch_bounds__(1024, 1) intmat_contract_bulk_kernel(ContractB
                         stop = true;
                         break;
                     }
-                    sb::mbar_arrive_expect_tx(&full[st], (uint32_t)cnt * 4u);
-                    sb::bulk_load_1d(ring + (size_t)st * a.stage_floats, a.IF + (size_t)m * a.ld_if + start,
-                                     (uint32_t)cnt * 4u, &full[st], pol);
+                    // the box is always stage_floats long (chunks past the row read as zeros)
+                    sb::mbar_arrive_expect_tx(&full[st], (uint32_t)a.stage_floats * 4u);
+                    sb::tma_load_3d(ring + (size_t)st * a.stage_floats, &map, 0, start / 32, m, &full[st], pol);
                 }
             }
             issued = q;
@@ -630,7 +634,7 @@ extern "C" int sb_intmat_contract(const float *jac, const float *tot, int n_vali
 }
 
 namespace sb {
-// read and clear the timeout flag of the bulk-copy contraction (0: none, <0: query failed)
+// read and clear the timeout flag of the TMA contraction (0: none, <0: query failed)
 int contract_status_take() {
     int v = 0;
     if (cudaMemcpyFromSymbol(&v, g_contract_status, sizeof(int)) != cudaSuccess) return -1;
@@ -651,22 +655,25 @@ extern "C" int sb_intmat_contract_rows(const float *jac, const float *tot, int n
         n_lenses < 1 || ld_if < 1 || seg_max < 0)
         return sb::fail(SB_EINVAL, "sb_intmat_contract_rows: bad args");
     if (field_ld < n_lenses * np_sub) return sb::fail(SB_EINVAL, "sb_intmat_contract_rows: bad field stride");
-    if (ld_if % 4 || (uintptr_t)ifunc % 16 || seg_max % 4)
-        return sb::fail(SB_EINVAL, "sb_intmat_contract_rows: influence-function rows and segments must be 16-byte "
-                                   "aligned (ld_if %% 4 == 0, 16-byte base, seg_max %% 4 == 0)");
+    if (ld_if % 32 || (uintptr_t)ifunc % 16 || seg_max % 32 || seg_max > 256 * 32)
+        return sb::fail(SB_EINVAL, "sb_intmat_contract_rows: ld_if and seg_max must be multiples of 32 floats "
+                                   "(seg_max <= 8192), ifunc 16-byte aligned");
     const int ncons = (n_lenses * np_sub + 31) / 32 * 32;
     if (ncons > kCbMaxConsumers)
         return sb::fail(SB_ESHAPE, "sb_intmat_contract_rows: field of %d columns (at most %d)", n_lenses * np_sub,
                         kCbMaxConsumers);
     if (n_modes == 0) return SB_OK;
-    const int stage_floats = seg_max > 0 ? seg_max : 4;
+    const int stage_floats = seg_max > 0 ? seg_max : 32;
     int stages = (int)((96 * 1024) / ((size_t)stage_floats * 4));
     stages = stages > kCbMaxStages ? kCbMaxStages : stages;
     if (stages < 2)
         return sb::fail(SB_ESHAPE, "sb_intmat_contract_rows: segments of %d floats exceed the shared-memory ring",
                         seg_max);
-    const size_t smem = (size_t)stages * stage_floats * 4 + 2 * (size_t)stages * 8;
-    ContractBulkArgs a;
+    CUtensorMap map;
+    int rc = sb::tensor_map_rows32_f32(&map, ifunc, n_modes, ld_if, stage_floats / 32);
+    if (rc) return rc;
+    const size_t smem = 128 + (size_t)stages * stage_floats * 4 + 2 * (size_t)stages * 8;
+    ContractTmaArgs a;
     a.jac = jac;
     a.tot = tot;
     a.n_valid = n_valid;
@@ -682,10 +689,10 @@ extern "C" int sb_intmat_contract_rows(const float *jac, const float *tot, int n
     a.im = intmat;
     a.stages = stages;
     a.stage_floats = stage_floats;
-    void (*fn)(ContractBulkArgs) = nullptr;
+    void (*fn)(const CUtensorMap, ContractTmaArgs) = nullptr;
     switch (np_sub) {
-    case 4: fn = intmat_contract_bulk_kernel<4>; break;
-    case 8: fn = intmat_contract_bulk_kernel<8>; break;
+    case 4: fn = intmat_contract_tma_kernel<4>; break;
+    case 8: fn = intmat_contract_tma_kernel<8>; break;
     default:
         return sb::fail(SB_EUNSUPPORTED, "sb_intmat_contract_rows: np_sub=%d (4 or 8)", np_sub);
     }
@@ -703,6 +710,6 @@ extern "C" int sb_intmat_contract_rows(const float *jac, const float *tot, int n
     const int chunks = (n_modes + kContractModes - 1) / kContractModes;
     int grid = per_sm * nsm;
     grid = grid > chunks * n_lenses ? chunks * n_lenses : grid;
-    fn<<<grid, threads, smem, sb::as_stream(stream)>>>(a);
-    return sb::check_launch("intmat_contract_bulk_kernel");
+    fn<<<grid, threads, smem, sb::as_stream(stream)>>>(map, a);
+    return sb::check_launch("intmat_contract_tma_kernel");
 }

@@ -16,7 +16,7 @@ int fail(int status, const char *fmt, ...);
 void clear_error();
 // read and clear the timeout flag of the tensor-core SH kernels (0: none, <0: query failed)
 int sh_tc_status_take();
-// read and clear the timeout flag of the bulk-copy interaction-matrix contraction
+// read and clear the timeout flag of the TMA interaction-matrix contraction
 int contract_status_take();
 // tile-shape variant registered for (family, key); 0 when none
 int tune_lookup(int family, unsigned long long key);

@@ -74,14 +74,14 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, i
         : "memory");
 }
 
-// 1-D bulk copy (no tensor map) of `bytes` contiguous bytes from this GPU's
-// global memory into this CTA's shared memory, completing on `bar`.  Both
-// addresses 16-byte aligned, `bytes` a multiple of 16.
-__device__ __forceinline__ void bulk_load_1d(void *dst, const void *src, uint32_t bytes, uint64_t *bar,
-                                             uint64_t policy) {
+// 3-D tiled TMA load of the box at element coordinates (x, y, z), completing
+// on `bar`.  x * element size must be a multiple of 16.
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar,
+                                            uint64_t policy) {
     asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;"
-        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+        " [%0], [%1, {%2, %3, %4}], [%5], %6;" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar)), "l"(policy)
         : "memory");
 }
 
@@ -89,6 +89,12 @@ __device__ __forceinline__ void bulk_load_1d(void *dst, const void *src, uint32_
 // `ld` elements) as a 2-D tensor map with box (box_rows x box_cols);
 // out-of-range elements of a box read as zero.  Returns SB_OK or a status.
 int tensor_map_2d_f32(CUtensorMap *map, const float *base, int rows, int cols, int ld, int box_rows, int box_cols);
+
+// Host: a row-major float32 matrix (rows x ld, ld a multiple of 32) seen as
+// rows x (ld / 32) chunks of 32 floats, as a 3-D tensor map whose box is
+// box_chunks consecutive chunks (<= 256) of one row: one box is a contiguous
+// run of 32 * box_chunks floats starting at a 32-float boundary.
+int tensor_map_rows32_f32(CUtensorMap *map, const float *base, int rows, int ld, int box_chunks);
 
 // Streaming multiprocessors of the current device (cached per device).
 int sm_count();

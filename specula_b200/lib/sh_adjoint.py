@@ -56,7 +56,7 @@ def pixel_to_column(mask_idx, dm_shape, field_size, top=0, left=0):
 
 def row_segments(pix2col, lenslets, n_lenses, np_sub, field, ld_if):
     """Per lenslet row the influence-function columns the contraction reads:
-    (start, count) in floats, both multiples of 4, covering every mirror
+    (start, count) in floats, both multiples of 32, covering every mirror
     column under a valid sub-aperture of that row (columns enumerate the
     mirror's pixels row-major, so np_sub consecutive field rows map to one
     contiguous range).  Returns the (n_lenses, 2) int32 table and the largest
@@ -73,8 +73,8 @@ def row_segments(pix2col, lenslets, n_lenses, np_sub, field, ld_if):
         c = c[c >= 0]
         if c.size == 0:
             continue
-        start = int(c.min()) & ~3
-        end = min((int(c.max()) + 1 + 3) & ~3, int(ld_if))
+        start = int(c.min()) & ~31
+        end = min((int(c.max()) + 1 + 31) & ~31, int(ld_if))
         seg[li] = (start, end - start)
     return seg, int(seg[:, 1].max()) if n_lenses else 0
 
@@ -234,17 +234,18 @@ class ShSlopesAdjoint:
                       float(2.0 * dm.sign), im.data_ptr(), self._stream())
         return im
 
-    # bulk-copy contraction limits: np_sub 4 or 8, at most 992 field columns,
-    # 16-byte aligned influence-function rows, a row segment within 96 KB / 2
-    BULK_NP_SUB = (4, 8)
-    BULK_MAX_COLUMNS = 992
-    BULK_MAX_SEGMENT = 96 * 1024 // 4 // 2
+    # TMA contraction limits: np_sub 4 or 8, at most 992 field columns,
+    # influence-function rows of a multiple of 32 floats, a row segment of at
+    # most 8192 floats (256 chunks of 32)
+    TMA_NP_SUB = (4, 8)
+    TMA_MAX_COLUMNS = 992
+    TMA_MAX_SEGMENT = 8192
 
     def _segments(self, pix2col, dm):
-        """(device table, largest count) of the row segments for the
-        bulk-copy contraction, or None when its limits are not met (then the
+        """(device table, largest count) of the row segments for the TMA
+        contraction, or None when its limits are not met (then the
         gather kernel runs); cached per mirror column map."""
-        if (self.np_sub not in self.BULK_NP_SUB or self.field > self.BULK_MAX_COLUMNS or dm._ld % 4 or
+        if (self.np_sub not in self.TMA_NP_SUB or self.field > self.TMA_MAX_COLUMNS or dm._ld % 32 or
                 dm._IF.data_ptr() % 16):
             return None
         key = (pix2col.data_ptr(), int(dm._ld))
@@ -252,7 +253,7 @@ class ShSlopesAdjoint:
         if cache is None or cache[0] != key:
             seg, seg_max = row_segments(pix2col.cpu().numpy(), self._lenslet.cpu().numpy(), self.n_lenses,
                                         self.np_sub, self.field, dm._ld)
-            val = None if seg_max > self.BULK_MAX_SEGMENT else (torch.as_tensor(seg, device=self.device), seg_max)
+            val = None if seg_max > self.TMA_MAX_SEGMENT else (torch.as_tensor(seg, device=self.device), seg_max)
             cache = (key, val, pix2col)
             self._seg_cache = cache
         return cache[1]

@@ -325,41 +325,41 @@ def test_autograd_function_gradient_matches_jacobian(cuda):
     assert torch.equal(s.detach(), sl_fwd)
 
 
-def test_bulk_contraction_equals_gather_contraction(cuda):
-    """sb_intmat_contract_rows (influence functions streamed by bulk copies)
-    gives the matrix of sb_intmat_contract (gathers) bit for bit, on the
+def test_tma_contraction_equals_gather_contraction(cuda):
+    """sb_intmat_contract_rows (influence functions streamed by TMA) gives
+    the matrix of sb_intmat_contract (gathers) bit for bit, on the
     500-Zernike calibration system with the CoG cut-off applied."""
     from specula_b200 import _lib
     from specula_b200.calibration import ShCalibrationSystem
     cal = ShCalibrationSystem()
     adj, dm = cal.adjoint, cal.dm
     assert adj._segments(cal._pix2col, dm) is not None
-    im_bulk = cal.adjoint_intmat()
+    im_tma = cal.adjoint_intmat()
     A = cal.A
     jac = adj._jacobian(A, cal._flat, None)
     tot = adj._tot
-    im_gather = torch.empty_like(im_bulk)
+    im_gather = torch.empty_like(im_tma)
     _lib.call('sb_intmat_contract', jac.data_ptr(), tot.data_ptr(), adj.n_valid, adj.np_sub, adj.n_lenses,
               adj.field, adj._slot.data_ptr(), cal._pix2col.data_ptr(), dm._IF.data_ptr(), dm._IF.shape[0], dm._ld,
               float(2.0 * dm.sign), im_gather.data_ptr(), torch.cuda.current_stream().cuda_stream)
     torch.cuda.synchronize()
     _lib.call('sb_device_status')
-    assert torch.equal(im_bulk, im_gather)
-    assert float(im_bulk.abs().max()) > 0
+    assert torch.equal(im_tma, im_gather)
+    assert float(im_tma.abs().max()) > 0
 
 
-def test_bulk_contraction_reports_a_short_segment(cuda):
+def test_tma_contraction_reports_a_short_segment(cuda):
     """A row segment that misses columns under a valid sub-aperture is not
     read past its end: those entries are skipped and sb_device_status reports
-    SB_EINVAL (the copy itself stays aligned and inside the row)."""
+    SB_EINVAL (the box itself stays aligned and inside the matrix)."""
     from specula_b200 import _lib
     from specula_b200.calibration import ShCalibrationSystem
     cal = ShCalibrationSystem()
     adj, dm = cal.adjoint, cal.dm
     seg, seg_max = adj._segments(cal._pix2col, dm)
     bad = seg.clone()
-    li = int(torch.nonzero(bad[:, 1] > 8)[0])
-    bad[li, 1] = 4                                   # four columns where the row needs more
+    li = int(torch.nonzero(bad[:, 1] > 64)[0])
+    bad[li, 1] = 32                                  # 32 columns where the row needs more
     jac = adj._jacobian(cal.A, cal._flat, None)
     im = torch.zeros((dm._IF.shape[0], 2 * adj.n_valid), device=cal.A.device)
     _lib.call('sb_intmat_contract_rows', jac.data_ptr(), adj._tot.data_ptr(), adj.n_valid, adj.np_sub, adj.n_lenses,
