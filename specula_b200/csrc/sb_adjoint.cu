@@ -422,6 +422,8 @@ extern "C" int sb_sh_slopes_vjp(const sb_sh_plan *pl, const float *A, const floa
 // issuing, lets the copies in flight land (bounded) and returns.
 // ---------------------------------------------------------------------------
 constexpr int kCbMaxStages = 8;
+constexpr int kCbModesPerStage = 2;    // modes per TMA box (kContractModes is a multiple of it)
+static_assert(kContractModes % kCbModesPerStage == 0, "whole stages per chunk of modes");
 constexpr int kCbMaxConsumers = 992;   // field columns (+ one producer warp <= 1024 threads)
 
 __device__ int g_contract_status = 0;
@@ -457,10 +459,12 @@ template <int P>
 __global__ void __launch_bounds__(1024, 1) intmat_contract_tma_kernel(const __grid_constant__ CUtensorMap map,
                                                                       ContractTmaArgs a) {
     extern __shared__ __align__(128) unsigned char cb_smem[];
-    // TMA destinations on 128-byte boundaries (stages are multiples of 128 bytes)
+    // TMA destinations on 128-byte boundaries (segments are multiples of 128 bytes)
     unsigned char *base = cb_smem + ((128 - (sb::smem_u32(cb_smem) & 127)) & 127);
     float *ring = reinterpret_cast<float *>(base);
-    uint64_t *full = reinterpret_cast<uint64_t *>(base + (size_t)a.stages * a.stage_floats * 4);
+    const int seg_floats = a.stage_floats;                 // one mode's segment
+    const int stage = kCbModesPerStage * seg_floats;       // one stage: consecutive modes' segments
+    uint64_t *full = reinterpret_cast<uint64_t *>(base + (size_t)a.stages * stage * 4);
     uint64_t *empty = full + a.stages;
     __shared__ double red[33];
     __shared__ int abort_flag, issued;
@@ -493,7 +497,8 @@ __global__ void __launch_bounds__(1024, 1) intmat_contract_tma_kernel(const __gr
     if (warp == nwc) {
         if (lane == 0) {
             const uint64_t pol = sb::l2_evict_first_policy();
-            int q = 0;
+            int q = 0, st = 0;
+            uint32_t ph = 0;
             bool stop = false;
             for (int w = blockIdx.x; w < n_items && !stop; w += gridDim.x) {
                 const int li = w % a.n, m0 = (w / a.n) * kContractModes;
@@ -501,21 +506,21 @@ __global__ void __launch_bounds__(1024, 1) intmat_contract_tma_kernel(const __gr
                 const int cnt = seg_count(a, li);
                 if (cnt <= 0) continue;
                 const int start = a.row_seg[2 * li];
-                for (int m = m0; m < m1; ++m, ++q) {
-                    const int st = q % S;
-                    if (q >= S && !sb::mbar_wait(&empty[st], ((q / S) - 1) & 1)) {
+                for (int m = m0; m < m1; m += kCbModesPerStage, ++q) {
+                    // reuse a slot once every consumer warp released its previous use
+                    if (q >= S && !sb::mbar_wait(&empty[st], ph ^ 1u)) {
                         atomicExch(&g_contract_status, 1);
                         abort_flag = 1;
                         stop = true;
                         break;
                     }
-                    if (*(volatile int *)&abort_flag) {
-                        stop = true;
-                        break;
+                    // the box is always the whole stage (modes past the matrix read as zeros)
+                    sb::mbar_arrive_expect_tx(&full[st], (uint32_t)stage * 4u);
+                    sb::tma_load_3d(ring + (size_t)st * stage, &map, 0, start / 32, m, &full[st], pol);
+                    if (++st == S) {
+                        st = 0;
+                        ph ^= 1u;
                     }
-                    // the box is always stage_floats long (chunks past the row read as zeros)
-                    sb::mbar_arrive_expect_tx(&full[st], (uint32_t)a.stage_floats * 4u);
-                    sb::tma_load_3d(ring + (size_t)st * a.stage_floats, &map, 0, start / 32, m, &full[st], pol);
                 }
             }
             issued = q;
@@ -523,8 +528,10 @@ __global__ void __launch_bounds__(1024, 1) intmat_contract_tma_kernel(const __gr
     } else {
         const int x = tid;
         const int lj = x / P, c = x - lj * P;
-        int q = 0;
-        for (int w = blockIdx.x; w < n_items; w += gridDim.x) {
+        int st = 0;
+        uint32_t ph = 0;
+        bool failed = false;
+        for (int w = blockIdx.x; w < n_items && !failed; w += gridDim.x) {
             const int li = w % a.n, m0 = (w / a.n) * kContractModes;
             const int m1 = min(a.n_modes, m0 + kContractModes);
             const int cnt = seg_count(a, li);
@@ -535,11 +542,13 @@ __global__ void __launch_bounds__(1024, 1) intmat_contract_tma_kernel(const __gr
                 const float t = a.tot[s];
                 act = t > 0.f && (double)(1.0f / t) <= 1.0 / (mean * 1e-3);
             }
+            // a masked pixel reads offset 0 with zero weights: fmaf(0, f, v) == v for the finite
+            // influence functions, as fmaf(j, 0, v) in intmat_contract_kernel
             float jx[P], jy[P];
             int off[P];
 #pragma unroll
             for (int rr = 0; rr < P; ++rr) {
-                off[rr] = -1;
+                off[rr] = 0;
                 jx[rr] = jy[rr] = 0.f;
                 if (act) {
                     const int col = a.pix2col[(size_t)(li * P + rr) * a.field_ld + x];
@@ -547,54 +556,59 @@ __global__ void __launch_bounds__(1024, 1) intmat_contract_tma_kernel(const __gr
                         atomicExch(&g_contract_status, 3);      // a column outside its row's segment
                     } else if (col >= 0) {
                         off[rr] = col - start;
+                        jx[rr] = a.jac[(size_t)s * (P * P) + rr * P + c];
+                        jy[rr] = a.jac[((size_t)a.n_valid + s) * (P * P) + rr * P + c];
                     }
-                    jx[rr] = a.jac[(size_t)s * (P * P) + rr * P + c];
-                    jy[rr] = a.jac[((size_t)a.n_valid + s) * (P * P) + rr * P + c];
                 }
             }
-            bool failed = false;
-            for (int m = m0; m < m1; ++m) {
-                float vx = 0.f, vy = 0.f;
+            float *im_x = a.im + s;
+            for (int m = m0; m < m1; m += kCbModesPerStage) {
+                float v[kCbModesPerStage][2];
+#pragma unroll
+                for (int k = 0; k < kCbModesPerStage; ++k) v[k][0] = v[k][1] = 0.f;
                 if (cnt > 0) {
-                    const int st = q % S;
-                    if (!sb::mbar_wait(&full[st], (q / S) & 1)) {
+                    if (!sb::mbar_wait_sleep(&full[st], ph)) {
                         atomicExch(&g_contract_status, 2);
                         abort_flag = 1;
                         failed = true;
                         break;
                     }
-                    if (*(volatile int *)&abort_flag) {
-                        failed = true;
-                        break;
-                    }
-                    const float *seg = ring + (size_t)st * a.stage_floats;
+                    const float *seg = ring + (size_t)st * stage;
 #pragma unroll
-                    for (int rr = 0; rr < P; ++rr) {
-                        const float f = off[rr] >= 0 ? seg[off[rr]] : 0.f;
-                        vx = fmaf(jx[rr], f, vx);
-                        vy = fmaf(jy[rr], f, vy);
-                    }
+                    for (int k = 0; k < kCbModesPerStage; ++k)
+#pragma unroll
+                        for (int rr = 0; rr < P; ++rr) {
+                            const float f = seg[k * seg_floats + off[rr]];
+                            v[k][0] = fmaf(jx[rr], f, v[k][0]);
+                            v[k][1] = fmaf(jy[rr], f, v[k][1]);
+                        }
                     __syncwarp();
                     if (lane == 0) sb::mbar_arrive(&empty[st]);
-                    ++q;
+                    if (++st == S) {
+                        st = 0;
+                        ph ^= 1u;
+                    }
                 }
 #pragma unroll
-                for (int o = P / 2; o > 0; o >>= 1) {
-                    vx += __shfl_down_sync(0xffffffffu, vx, o, P);
-                    vy += __shfl_down_sync(0xffffffffu, vy, o, P);
-                }
-                if (c == 0 && s >= 0) {
-                    a.im[(size_t)m * ld_im + s] = a.scale * vx;
-                    a.im[(size_t)m * ld_im + a.n_valid + s] = a.scale * vy;
+                for (int k = 0; k < kCbModesPerStage; ++k) {
+#pragma unroll
+                    for (int o = P / 2; o > 0; o >>= 1) {
+                        v[k][0] += __shfl_down_sync(0xffffffffu, v[k][0], o, P);
+                        v[k][1] += __shfl_down_sync(0xffffffffu, v[k][1], o, P);
+                    }
+                    if (c == 0 && s >= 0 && m + k < m1) {
+                        im_x[(size_t)(m + k) * ld_im] = a.scale * v[k][0];
+                        im_x[(size_t)(m + k) * ld_im + a.n_valid] = a.scale * v[k][1];
+                    }
                 }
             }
-            if (failed) break;
         }
     }
     __syncthreads();
     if (abort_flag && tid == ncons) {
-        // let every issued copy land before the shared memory is released
-        for (int q = 0; q < issued; ++q) sb::mbar_wait(&full[q % S], (q / S) & 1);
+        // let the copies still in flight (at most the last S issued) land
+        // before the shared memory is released
+        for (int q = issued > S ? issued - S : 0; q < issued; ++q) sb::mbar_wait(&full[q % S], (q / S) & 1);
     }
 }
 
@@ -655,24 +669,24 @@ extern "C" int sb_intmat_contract_rows(const float *jac, const float *tot, int n
         n_lenses < 1 || ld_if < 1 || seg_max < 0)
         return sb::fail(SB_EINVAL, "sb_intmat_contract_rows: bad args");
     if (field_ld < n_lenses * np_sub) return sb::fail(SB_EINVAL, "sb_intmat_contract_rows: bad field stride");
-    if (ld_if % 32 || (uintptr_t)ifunc % 16 || seg_max % 32 || seg_max > 256 * 32)
+    if (ld_if % 32 || (uintptr_t)ifunc % 16 || seg_max % 32 || seg_max > 12 * 1024)
         return sb::fail(SB_EINVAL, "sb_intmat_contract_rows: ld_if and seg_max must be multiples of 32 floats "
-                                   "(seg_max <= 8192), ifunc 16-byte aligned");
+                                   "(seg_max <= 12288), ifunc 16-byte aligned");
     const int ncons = (n_lenses * np_sub + 31) / 32 * 32;
     if (ncons > kCbMaxConsumers)
         return sb::fail(SB_ESHAPE, "sb_intmat_contract_rows: field of %d columns (at most %d)", n_lenses * np_sub,
                         kCbMaxConsumers);
     if (n_modes == 0) return SB_OK;
-    const int stage_floats = seg_max > 0 ? seg_max : 32;
-    int stages = (int)((96 * 1024) / ((size_t)stage_floats * 4));
+    const int stage_floats = seg_max > 0 ? seg_max : 32;    // one mode's segment
+    int stages = (int)((96 * 1024) / ((size_t)stage_floats * 4 * kCbModesPerStage));
     stages = stages > kCbMaxStages ? kCbMaxStages : stages;
     if (stages < 2)
         return sb::fail(SB_ESHAPE, "sb_intmat_contract_rows: segments of %d floats exceed the shared-memory ring",
                         seg_max);
     CUtensorMap map;
-    int rc = sb::tensor_map_rows32_f32(&map, ifunc, n_modes, ld_if, stage_floats / 32);
+    int rc = sb::tensor_map_rows32_f32(&map, ifunc, n_modes, ld_if, stage_floats / 32, kCbModesPerStage);
     if (rc) return rc;
-    const size_t smem = 128 + (size_t)stages * stage_floats * 4 + 2 * (size_t)stages * 8;
+    const size_t smem = 128 + (size_t)stages * stage_floats * 4 * kCbModesPerStage + 2 * (size_t)stages * 8;
     ContractTmaArgs a;
     a.jac = jac;
     a.tot = tot;

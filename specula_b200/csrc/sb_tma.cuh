@@ -55,6 +55,29 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
     return true;
 }
 
+// try_wait with a suspend-time hint: the thread may sleep in the barrier
+// (up to `ns` nanoseconds, or until the phase completes) instead of spinning
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t *bar, uint32_t parity, uint32_t ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(ns)
+        : "memory");
+    return ok != 0;
+}
+
+// mbar_wait for many waiting warps: they sleep in the barrier between polls
+// (same bound, false after kMbarWaitCycles)
+__device__ __forceinline__ bool mbar_wait_sleep(uint64_t *bar, uint32_t parity) {
+    const long long t0 = clock64();
+    while (!mbar_try_wait_sleep(bar, parity, 20000u))
+        if (clock64() - t0 > kMbarWaitCycles) return false;
+    return true;
+}
+
 // L2 policy for data read exactly once (lines evicted first, so the working
 // set of concurrently running kernels stays in L2)
 __device__ __forceinline__ uint64_t l2_evict_first_policy() {
@@ -92,9 +115,10 @@ int tensor_map_2d_f32(CUtensorMap *map, const float *base, int rows, int cols, i
 
 // Host: a row-major float32 matrix (rows x ld, ld a multiple of 32) seen as
 // rows x (ld / 32) chunks of 32 floats, as a 3-D tensor map whose box is
-// box_chunks consecutive chunks (<= 256) of one row: one box is a contiguous
-// run of 32 * box_chunks floats starting at a 32-float boundary.
-int tensor_map_rows32_f32(CUtensorMap *map, const float *base, int rows, int ld, int box_chunks);
+// box_chunks consecutive chunks (<= 256) of box_rows consecutive rows: per
+// row a contiguous run of 32 * box_chunks floats starting at a 32-float
+// boundary (rows past the matrix read as zeros).
+int tensor_map_rows32_f32(CUtensorMap *map, const float *base, int rows, int ld, int box_chunks, int box_rows);
 
 // Streaming multiprocessors of the current device (cached per device).
 int sm_count();
