@@ -765,6 +765,7 @@ def run_b200(args):
         dist.all_reduce(t_obj, op=dist.ReduceOp.MAX)
     obj_value = world * obj_steps / float(t_obj.item())
 
+    pieces = step_pieces(loop) if loop.fused_atmo else None
     accuracy = accuracy_vs_fp64(loop, *acc_field) if rank == 0 else None
 
     cpu = None
@@ -810,13 +811,61 @@ def run_b200(args):
                 'step_roofline': {'algorithmic_bytes': step_bytes,
                                   'achieved_gbs': step_bytes / (ms_max / steps / 1e3) / 1e9,
                                   'frac': step_bytes / (ms_max / steps / 1e3) / 1e9 / peak},
-                'accuracy': accuracy, 'clocks': clk, 'cpu_baseline': cpu, 'adjoint_im': adjoint_im, 'loop_gradient': loop_grad,
+                'accuracy': accuracy, 'step_pieces': pieces, 'clocks': clk, 'cpu_baseline': cpu, 'adjoint_im': adjoint_im, 'loop_gradient': loop_grad,
                 'sh_forms': sh_forms, 'batched_mc': batched_mc}
         print(json.dumps(line), flush=True)
     del loop
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def step_pieces(loop, reps=200):
+    """Device time of the captured step and of its pieces, each captured in a
+    graph of its own (CUDA events over ``reps`` replays after warm-up): the
+    chain (atmosphere, SH, detector/CoG, reconstructor) of two steps without
+    the DM projection, the DM projection alone, and the chain's parts."""
+    import torch
+    st = torch.cuda.current_stream(loop.device)
+
+    def timeit(fn):
+        for _ in range(10):
+            fn()
+        torch.cuda.synchronize(loop.device)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize(loop.device)
+        return e0.elapsed_time(e1) / reps * 1e3
+
+    dm_buf, nxt = loop._bufs
+    graphs = []
+
+    def graph_of(fn):
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            fn()
+        graphs.append(g)
+        return g.replay
+
+    def chain_two_steps():
+        for par in (1, 0):
+            loop._atmo_propagate(dm_buf[1 - par])
+            loop._chain()
+            loop._rec_integ(out_next=nxt[1 - par])
+
+    out = {'step_us': timeit(loop.replay) / loop.steps_per_replay,
+           'chain_alone_us_per_step': timeit(graph_of(chain_two_steps)) / 2,
+           'dm_alone_us': timeit(graph_of(lambda: loop.dm.project(nxt[1], dm_buf[1]))),
+           'atmosphere_propagation_us': timeit(graph_of(lambda: loop._atmo_propagate(dm_buf[0]))),
+           'sh_detector_slopes_us': timeit(graph_of(loop._chain)),
+           'reconstructor_integrator_us': timeit(graph_of(lambda: loop._rec_integ(out_next=nxt[0])))}
+    del graphs
+    _lib_status()
+    return out
 
 
 def profile_loop(dev, replays):
