@@ -129,59 +129,75 @@ __device__ __forceinline__ int floor_small(float v) {
     return floor_small(v, fl);
 }
 
-// One 32 x 32 output tile of layer li: thread (tx, ty) produces rows
-// y0 + ty + 8 j (j < 4) of column x0 + tx and hands each value to
-// sink(j, y, x, value).  Every thread of the CTA must call it (it holds two
-// CTA barriers); Q, fp and lyd are the CTA's shared staging.
-template <int CAP, class Sink>
-__device__ __forceinline__ void evolve_tile(const EvolveArgsT<CAP> &a, int li, float (&Q)[kBox][kBox + 1], int *fp,
-                                            LayerDyn &lyd, Sink &&sink) {
+// The pieces of one 32 x 32 output tile of layer li.  tile_footprint (one
+// thread) fixes the layer's per-step parameters and the footprint of the tile
+// in the rot90'd, lerped layer; tile_load issues this thread's share of the
+// footprint reads; tile_stage writes them into the shared staging Q;
+// tile_values (after a barrier) produces rows y0 + ty + 8 j (j < 4) of column
+// x0 + tx and hands each value to sink(j, y, x, value).
+struct TileFootprint {
+    int br0, br1, bc0, bc1, interior;
+};
+
+template <int CAP>
+__device__ __forceinline__ void tile_footprint(const EvolveArgsT<CAP> &a, int li, LayerDyn &lyd, TileFootprint &fp) {
     const sb_atmo_layer &lys = a.layer[li];
+    lyd = a.dyn ? a.dyn[li] : static_dyn(lys);
     const LayerDyn &ly = lyd;
     const int L = a.L;
     const int x0 = blockIdx.x * kTile, y0 = blockIdx.y * kTile;
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-    if (tid == 0) {
-        lyd = a.dyn ? a.dyn[li] : static_dyn(lys);
-        // footprint [br0, br1] x [bc0, bc1] of the tile in the rot90'd layer
-        int br0 = y0, br1 = min(y0 + kTile, L) - 1, bc0 = x0, bc1 = min(x0 + kTile, L) - 1;
-        int interior = 0;
-        if (ly.rotate) {
-            double rmin = 1e300, rmax = -1e300, cmin = 1e300, cmax = -1e300;
-            for (int cy = 0; cy < 2; ++cy)
-                for (int cx = 0; cx < 2; ++cx) {
-                    const double yy = cy ? br1 : br0, xx = cx ? bc1 : bc0;
-                    const double ir = __dadd_rn(__dadd_rn(__dmul_rn(ly.m00, yy), __dmul_rn(ly.m01, xx)), ly.off0);
-                    const double ic = __dadd_rn(__dadd_rn(__dmul_rn(ly.m10, yy), __dmul_rn(ly.m11, xx)), ly.off1);
-                    rmin = fmin(rmin, ir); rmax = fmax(rmax, ir);
-                    cmin = fmin(cmin, ic); cmax = fmax(cmax, ic);
-                }
-            // every sample of the tile at least 0.01 px inside [0, L-1) on
-            // both axes: no edge test, no clamp, all four neighbours on the
-            // grid (the float32 sample positions are within 1e-4 px of these)
-            interior = rmin >= 0.01 && rmax <= L - 1 - 0.01 && cmin >= 0.01 && cmax <= L - 1 - 0.01;
-            br0 = max(0, (int)floor(rmin) - 1);
-            br1 = min(L - 1, (int)floor(rmax) + 2);
-            bc0 = max(0, (int)floor(cmin) - 1);
-            bc1 = min(L - 1, (int)floor(cmax) + 2);
-            // a footprint wider than the staging box means |angle| >= ~6
-            // degrees, which the fractional-degree rotation never produces
-            br1 = min(br1, br0 + kBox - 1);
-            bc1 = min(bc1, bc0 + kBox - 1);
-        }
-        fp[0] = br0; fp[1] = br1; fp[2] = bc0; fp[3] = bc1; fp[4] = interior;
+    int br0 = y0, br1 = min(y0 + kTile, L) - 1, bc0 = x0, bc1 = min(x0 + kTile, L) - 1;
+    int interior = 0;
+    if (ly.rotate) {
+        double rmin = 1e300, rmax = -1e300, cmin = 1e300, cmax = -1e300;
+        for (int cy = 0; cy < 2; ++cy)
+            for (int cx = 0; cx < 2; ++cx) {
+                const double yy = cy ? br1 : br0, xx = cx ? bc1 : bc0;
+                const double ir = __dadd_rn(__dadd_rn(__dmul_rn(ly.m00, yy), __dmul_rn(ly.m01, xx)), ly.off0);
+                const double ic = __dadd_rn(__dadd_rn(__dmul_rn(ly.m10, yy), __dmul_rn(ly.m11, xx)), ly.off1);
+                rmin = fmin(rmin, ir); rmax = fmax(rmax, ir);
+                cmin = fmin(cmin, ic); cmax = fmax(cmax, ic);
+            }
+        // every sample of the tile at least 0.01 px inside [0, L-1) on
+        // both axes: no edge test, no clamp, all four neighbours on the
+        // grid (the float32 sample positions are within 1e-4 px of these)
+        interior = rmin >= 0.01 && rmax <= L - 1 - 0.01 && cmin >= 0.01 && cmax <= L - 1 - 0.01;
+        br0 = max(0, (int)floor(rmin) - 1);
+        br1 = min(L - 1, (int)floor(rmax) + 2);
+        bc0 = max(0, (int)floor(cmin) - 1);
+        bc1 = min(L - 1, (int)floor(cmax) + 2);
+        // a footprint wider than the staging box means |angle| >= ~6
+        // degrees, which the fractional-degree rotation never produces
+        br1 = min(br1, br0 + kBox - 1);
+        bc1 = min(bc1, bc0 + kBox - 1);
     }
+    fp.br0 = br0; fp.br1 = br1; fp.bc0 = bc0; fp.bc1 = bc1; fp.interior = interior;
+}
+
+constexpr int kStagePer = (kBox * kBox + 255) / 256;   // footprint elements per thread
+
+// this thread's footprint reads: the strip's two neighbouring columns of each
+// element (v0, v1), its place in Q (qo, -1: none) and the lerp weights
+struct TileLoads {
+    float v0[kStagePer], v1[kStagePer];
+    int qo[kStagePer];
+    float w0, frac;
+};
+
+template <int CAP>
+__device__ __forceinline__ void tile_load(const EvolveArgsT<CAP> &a, int li, const LayerDyn &ly,
+                                          const TileFootprint &fp, int tid, TileLoads &t) {
+    const sb_atmo_layer &lys = a.layer[li];
+    const int L = a.L;
     // integer position and float32 remainder (atmo_evolution.py:278-279)
     const double np = *a.ptr[li].pos;
     const double q = floor(np);
     const float *row0 = lys.screen + (long long)q;
     const int ld = lys.screen_ld;
-    const float frac = (float)(np - q);
-    const float w0 = __fsub_rn(1.0f, frac);
-    __syncthreads();                      // lyd and fp written by thread 0
+    t.frac = (float)(np - q);
+    t.w0 = __fsub_rn(1.0f, t.frac);
     const int k = ly.rot90;
-    const int br0 = fp[0], br1 = fp[1], bc0 = fp[2], bc1 = fp[3];
-    const bool interior = fp[4] != 0;
+    const int br0 = fp.br0, br1 = fp.br1, bc0 = fp.bc0, bc1 = fp.bc1;
     const int R = br1 - br0 + 1, Cc = bc1 - bc0 + 1;
     // rot90(lerped)[yy][xx] reads screen element base + ra*dR + cb*dC
     // (ra, cb: footprint row / column); thread (tx, ty) of the 32 x 8 block
@@ -198,39 +214,43 @@ __device__ __forceinline__ void evolve_tile(const EvolveArgsT<CAP> &a, int li, f
     const bool odd = k & 1;
     const int n_fast = odd ? R : Cc, n_slow = odd ? Cc : R;
     const int d_fast = odd ? dR : dC, d_slow = odd ? dC : dR;
-    {
-        // Q strides of the fast and slow walk: Q[sl][fa] for even k, Q[fa][sl] for odd k
-        const int qs_fast = odd ? kBox + 1 : 1, qs_slow = odd ? 1 : kBox + 1;
-        float *qbase = &Q[0][0];
-        // the footprint walked as one flat range e = sl * n_fast + fa, every
-        // lane busy and all of a thread's loads issued before its stores;
-        // sl = floor((e + 0.5) / n_fast) in float32 is exact here (e < 1600,
-        // n_fast <= 40: the quotient is >= 0.0125 from an integer, the
-        // float32 error below 5e-6)
-        constexpr int kPer = (kBox * kBox + 255) / 256;
-        const int n_el = n_fast * n_slow;
-        const float inv_nf = 1.0f / (float)n_fast;
-        const float e_half = (float)tid + 0.5f;
-        float v0[kPer], v1[kPer];
-        int qo[kPer];
+    // Q strides of the fast and slow walk: Q[sl][fa] for even k, Q[fa][sl] for odd k
+    const int qs_fast = odd ? kBox + 1 : 1, qs_slow = odd ? 1 : kBox + 1;
+    // the footprint walked as one flat range e = sl * n_fast + fa, every
+    // lane busy; sl = floor((e + 0.5) / n_fast) in float32 is exact here
+    // (e < 1600, n_fast <= 40: the quotient is >= 0.0125 from an integer,
+    // the float32 error below 5e-6)
+    const int n_el = n_fast * n_slow;
+    const float inv_nf = 1.0f / (float)n_fast;
+    const float e_half = (float)tid + 0.5f;
 #pragma unroll
-        for (int j = 0; j < kPer; ++j) {
-            const int e = tid + 256 * j;
-            qo[j] = -1;
-            if (e < n_el) {
-                const int sl = floor_small((e_half + 256.0f * j) * inv_nf);
-                const int fa = e - sl * n_fast;
-                const float *p = row0 + (b0 + sl * d_slow + fa * d_fast);
-                v0[j] = p[0];
-                v1[j] = p[1];
-                qo[j] = sl * qs_slow + fa * qs_fast;
-            }
+    for (int j = 0; j < kStagePer; ++j) {
+        const int e = tid + 256 * j;
+        t.qo[j] = -1;
+        if (e < n_el) {
+            const int sl = floor_small((e_half + 256.0f * j) * inv_nf);
+            const int fa = e - sl * n_fast;
+            const float *p = row0 + (b0 + sl * d_slow + fa * d_fast);
+            t.v0[j] = p[0];
+            t.v1[j] = p[1];
+            t.qo[j] = sl * qs_slow + fa * qs_fast;
         }
-#pragma unroll
-        for (int j = 0; j < kPer; ++j)
-            if (qo[j] >= 0) qbase[qo[j]] = __fadd_rn(__fmul_rn(w0, v0[j]), __fmul_rn(frac, v1[j]));
     }
-    __syncthreads();
+}
+
+__device__ __forceinline__ void tile_stage(float (&Q)[kBox][kBox + 1], const TileLoads &t) {
+    float *qbase = &Q[0][0];
+#pragma unroll
+    for (int j = 0; j < kStagePer; ++j)
+        if (t.qo[j] >= 0) qbase[t.qo[j]] = __fadd_rn(__fmul_rn(t.w0, t.v0[j]), __fmul_rn(t.frac, t.v1[j]));
+}
+
+template <class Sink>
+__device__ __forceinline__ void tile_values(int L, const float (&Q)[kBox][kBox + 1], const LayerDyn &ly,
+                                            const TileFootprint &fp, Sink &&sink) {
+    const int x0 = blockIdx.x * kTile, y0 = blockIdx.y * kTile;
+    const int br0 = fp.br0, bc0 = fp.bc0;
+    const bool interior = fp.interior != 0;
     const int x = x0 + threadIdx.x;
     if (x >= L) return;
     const float scale = ly.scale;
@@ -314,10 +334,25 @@ __device__ __forceinline__ void evolve_tile(const EvolveArgsT<CAP> &a, int li, f
     }
 }
 
+// One whole tile of layer li (every thread of the CTA must call it: it holds
+// two CTA barriers); Q, fp and lyd are the CTA's shared staging.
+template <int CAP, class Sink>
+__device__ __forceinline__ void evolve_tile(const EvolveArgsT<CAP> &a, int li, float (&Q)[kBox][kBox + 1],
+                                            TileFootprint &fp, LayerDyn &lyd, Sink &&sink) {
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    if (tid == 0) tile_footprint(a, li, lyd, fp);
+    __syncthreads();                      // lyd and fp written by thread 0
+    TileLoads t;
+    tile_load(a, li, lyd, fp, tid, t);
+    tile_stage(Q, t);
+    __syncthreads();
+    tile_values(a.L, Q, lyd, fp, sink);
+}
+
 template <int CAP>
 __global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgsT<CAP> a) {
     __shared__ float Q[kBox][kBox + 1];
-    __shared__ int fp[5];                 // footprint br0, br1, bc0, bc1 and the interior flag
+    __shared__ TileFootprint fp;          // footprint of the tile and the interior flag
     __shared__ LayerDyn lyd;              // this layer's per-step parameters
     float *out = a.layer[blockIdx.z].out;
     const int L = a.L;
@@ -329,6 +364,8 @@ __global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgsT<CAP> a) {
 // written as by atmo_evolve_kernel and summed in registers in layer order,
 // then the stop and mirror layers are applied in propagate_batched_kernel's
 // operation order and the field written (the same bits as the two launches).
+constexpr int kFusedMaxLayers = SB_MAX_LAYERS;   // turbulence layers per realisation in the fused kernel
+
 struct FusedPropArgs {
     const float *stop_A, *stop_phase, *dm_A, *dm_phase;
     long long dm_stride, out_stride;
@@ -338,21 +375,32 @@ struct FusedPropArgs {
 
 template <int CAP>
 __global__ void __launch_bounds__(256, 4) atmo_propagate_kernel(EvolveArgsT<CAP> a, FusedPropArgs f) {
-    __shared__ float Q[kBox][kBox + 1];
-    __shared__ int fp[5];
-    __shared__ LayerDyn lyd;
+    // layers are software-pipelined: the footprint reads of layer k+1 are in
+    // flight while layer k's values are computed from the other staging buffer
+    __shared__ float Q[2][kBox][kBox + 1];
+    __shared__ TileFootprint fp[kFusedMaxLayers];
+    __shared__ LayerDyn lyd[kFusedMaxLayers];
     const int L = a.L;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int n = f.n_atm, l0 = blockIdx.z * n;
+    if (tid < n) tile_footprint(a, l0 + tid, lyd[tid], fp[tid]);
     float acc[kTile / kRowStep];
 #pragma unroll
     for (int j = 0; j < kTile / kRowStep; ++j) acc[j] = 0.0f;          // ElectricField.reset()
-    for (int k = 0; k < f.n_atm; ++k) {
-        const int li = blockIdx.z * f.n_atm + k;
-        float *out = a.layer[li].out;
-        evolve_tile(a, li, Q, fp, lyd, [&](int j, int y, int x, float v) {
+    __syncthreads();
+    TileLoads t;
+    tile_load(a, l0, lyd[0], fp[0], tid, t);
+    for (int k = 0; k < n; ++k) {
+        tile_stage(Q[k & 1], t);
+        if (k + 1 < n) tile_load(a, l0 + k + 1, lyd[k + 1], fp[k + 1], tid, t);
+        // staging k complete; the buffer of layer k+1 was last read at layer
+        // k-1, before this barrier's predecessor
+        __syncthreads();
+        float *out = a.layer[l0 + k].out;
+        tile_values(L, Q[k & 1], lyd[k], fp[k], [&](int j, int y, int x, float v) {
             out[(size_t)y * L + x] = v;
             acc[j] = __fadd_rn(acc[j], v);
         });
-        __syncthreads();                  // Q, fp and lyd are restaged for the next layer
     }
     const int x = blockIdx.x * kTile + threadIdx.x;
     if (x >= L) return;
@@ -566,6 +614,8 @@ extern "C" int sb_atmo_propagate_batched(const sb_atmo_layer *layers, const sb_a
         !(constants->pixel_pitch > 0.0) || !(constants->delta_time >= 0.0) || !dm_phase || !A_out || !phase_out ||
         dm_stride < n || out_stride < n)
         return sb::fail(SB_EINVAL, "sb_atmo_propagate_batched: bad args");
+    if (n_atm > kFusedMaxLayers)
+        return sb::fail(SB_ESHAPE, "sb_atmo_propagate_batched: at most %d layers per realisation", kFusedMaxLayers);
     const int n_layers = n_atm * n_batch;
     if (!work || work_bytes < (size_t)n_layers * sizeof(LayerDyn))
         return sb::fail(SB_ESCRATCH, "sb_atmo_propagate_batched: work needs %zu bytes",

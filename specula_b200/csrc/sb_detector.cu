@@ -444,9 +444,17 @@ __global__ void __launch_bounds__(256) slopec_finish_kernel(int n, const float *
 // valid box's pixels row-major (the caller checks it and passes the lenslet
 // -> sub-aperture map).
 // ---------------------------------------------------------------------------
-constexpr int kChainThreads = 256;
-constexpr int kChainLenses = kChainThreads / 32;
+constexpr int kChainSumThreads = 256;    // thread count whose summation orders the sums reproduce
+constexpr int kChainMaxThreads = 512;    // a CTA samples up to this many pixels per pass
+constexpr int kChainLenses = 8;          // lenslets per CTA: one CoG warp each
 constexpr int kChainMaxNpx = 16;
+
+// threads of a CTA: the lenslet tile (npx x 8 npx pixels) in one pass when it
+// fits in 512, never fewer than the 256 whose sums are reproduced
+__host__ __device__ inline int chain_threads(int npx) {
+    const int tile = (npx * kChainLenses * npx + 31) / 32 * 32;
+    return tile < kChainSumThreads ? kChainSumThreads : (tile > kChainMaxThreads ? kChainMaxThreads : tile);
+}
 
 struct ChainArgs {
     sb_ccd_params p;
@@ -465,12 +473,12 @@ struct ChainArgs {
     float *slopes, *flux, *tot, *sxn, *syn;
 };
 
-__global__ void __launch_bounds__(kChainThreads) sh_ccd_slopec_kernel(ChainArgs a) {
+__global__ void __launch_bounds__(kChainMaxThreads) sh_ccd_slopec_kernel(ChainArgs a) {
     __shared__ double dred[33];
     __shared__ float logfact[32];
-    __shared__ int s_idx[kChainThreads];
-    __shared__ float s_mean[kChainThreads];
-    __shared__ int s_small[kChainThreads / 32];
+    __shared__ int s_idx[kChainMaxThreads];
+    __shared__ float s_mean[kChainMaxThreads];
+    __shared__ int s_small[kChainMaxThreads / 32];
     __shared__ float tile[kChainMaxNpx * kChainLenses * kChainMaxNpx];
     __shared__ int s_last;
     const sb_ccd_params &p = a.p;
@@ -481,12 +489,15 @@ __global__ void __launch_bounds__(kChainThreads) sh_ccd_slopec_kernel(ChainArgs 
     const double inv_gain = 1.0 / (double)p.adu_gain;
     const bool gain_pow2 = (__double_as_longlong((double)p.adu_gain) & 0x000FFFFFFFFFFFFFLL) == 0;
 
-    // photon normalisation: the sums of sh_normalize_kernel, in its order
+    const int nthr = blockDim.x, nwarps = nthr >> 5;
+    // photon normalisation: the sums of sh_normalize_kernel (256 threads), in
+    // its order; warps past the eighth add exact zeros
     double si = 0.0, sa = 0.0;
-    for (int e = tid; e < a.nparts; e += kChainThreads) {
-        si += a.part_I[e];
-        sa += a.part_A[e];
-    }
+    if (tid < kChainSumThreads)
+        for (int e = tid; e < a.nparts; e += kChainSumThreads) {
+            si += a.part_I[e];
+            sa += a.part_A[e];
+        }
     si = sb::block_sum_all_d(si, dred);
     sa = sb::block_sum_all_d(sa, dred);
     const float phot = (float)(a.photon_scale * sa);
@@ -495,9 +506,10 @@ __global__ void __launch_bounds__(kChainThreads) sh_ccd_slopec_kernel(ChainArgs 
     const int i = blockIdx.y, j0 = blockIdx.x * kChainLenses;
     const int w = min(kChainLenses, a.n - j0);
     const int npx = a.npx, wc = w * npx, P = npx * wc, tld = kChainLenses * npx;
-    // detector: every pass samples up to 256 pixels of the tile, ordered by
-    // Poisson sampler branch as in ccd_kernel (the draws do not depend on it)
-    for (int base = 0; base < P; base += kChainThreads) {
+    // detector: every pass samples up to blockDim pixels of the tile (one pass
+    // for npx <= 8), ordered by Poisson sampler branch as in ccd_kernel (the
+    // draws do not depend on the order)
+    for (int base = 0; base < P; base += nthr) {
         const int q = base + tid;
         const bool valid = q < P;
         float f = 0.f;
@@ -518,8 +530,7 @@ __global__ void __launch_bounds__(kChainThreads) sh_ccd_slopec_kernel(ChainArgs 
             if (lane == 0) s_small[warp] = __popc(bal);
             __syncthreads();
             int before = 0, total = 0;
-#pragma unroll
-            for (int k = 0; k < kChainThreads / 32; ++k) {
+            for (int k = 0; k < nwarps; ++k) {
                 const int cnt = s_small[k];
                 before += k < warp ? cnt : 0;
                 total += cnt;
@@ -592,7 +603,7 @@ __global__ void __launch_bounds__(kChainThreads) sh_ccd_slopec_kernel(ChainArgs 
     // in warp order, then in float64 over 256 threads (sh_slopec.py:393-400)
     const int nv = a.n_valid, ngroups = (nv + 7) / 8;
     double acc = 0.0;
-    for (int g = tid; g < ngroups; g += kChainThreads) {
+    for (int g = tid; tid < kChainSumThreads && g < ngroups; g += kChainSumThreads) {
         float b = 0.f;
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
@@ -604,7 +615,7 @@ __global__ void __launch_bounds__(kChainThreads) sh_ccd_slopec_kernel(ChainArgs 
     acc = sb::block_sum_all_d(acc, dred);
     const float mean = (float)(acc / nv);
     const float cut = 1.0f / (mean * 1e-3f);
-    for (int s = tid; s < nv; s += kChainThreads) {
+    for (int s = tid; s < nv; s += nthr) {
         const float fac = 1.0f / __ldcg(a.tot + s);
         if (fac > cut) {
             a.slopes[s] = __ldcg(a.sxn + s) * 0.0f;
@@ -822,6 +833,6 @@ extern "C" int sb_sh_ccd_slopec(const sb_sh_plan *sh, int dft_mode, const float 
     a.sxn = a.tot + a.n_valid;
     a.syn = a.sxn + a.n_valid;
     const dim3 grid((n + kChainLenses - 1) / kChainLenses, n);
-    sh_ccd_slopec_kernel<<<grid, kChainThreads, 0, sb::as_stream(stream)>>>(a);
+    sh_ccd_slopec_kernel<<<grid, chain_threads(npx), 0, sb::as_stream(stream)>>>(a);
     return sb::check_launch("sh_ccd_slopec_kernel");
 }
