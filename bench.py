@@ -802,8 +802,9 @@ def run_b200(args):
                 'e2e_object_api': {'value': obj_value, 'unit': UNIT, 'api': 'LoopControl.iter (object by object)',
                                    'steps': obj_steps},
                 'gpu_launches': loop.kernels_per_step * steps,
-                'step_graph': 'pipelined (DM projection concurrent with the SH chain)' if loop.pipelined
-                else 'sequential',
+                'step_graph': ('pipelined (DM projection concurrent with the SH chain' +
+                               (', atmosphere early on a third stream)' if loop.early_atmo else ')'))
+                if loop.pipelined else 'sequential',
                 'roofline': {'bound': 'hbm', 'kernel': 'dm_project_tma_kernel', 'achieved': achieved, 'peak': peak,
                              'peak_kind': peak_kind, 'unit': 'GB/s', 'frac': achieved / peak, 'traffic': DM_TRAFFIC_BYTES,
                              'traffic_over_algorithmic': DM_TRAFFIC_BYTES / dm_bytes,
@@ -851,18 +852,33 @@ def step_pieces(loop, reps=200):
         graphs.append(g)
         return g.replay
 
+    early = getattr(loop, 'early_atmo', False)
+
+    def atmosphere(par):
+        if early:
+            loop._atmo_propagate(None, out=loop._early[par])
+        else:
+            loop._atmo_propagate(dm_buf[1 - par])
+
+    def sh_chain(par):
+        if early:
+            loop._sh_ccd_slopec(mirror=dm_buf[1 - par], partial=loop._early[par])
+        else:
+            loop._chain()
+
     def chain_two_steps():
         for par in (1, 0):
-            loop._atmo_propagate(dm_buf[1 - par])
-            loop._chain()
+            atmosphere(par)
+            sh_chain(par)
             loop._rec_integ(out_next=nxt[1 - par])
 
     out = {'step_us': timeit(loop.replay) / loop.steps_per_replay,
            'chain_alone_us_per_step': timeit(graph_of(chain_two_steps)) / 2,
            'dm_alone_us': timeit(graph_of(lambda: loop.dm.project(nxt[1], dm_buf[1]))),
-           'atmosphere_propagation_us': timeit(graph_of(lambda: loop._atmo_propagate(dm_buf[0]))),
-           'sh_detector_slopes_us': timeit(graph_of(loop._chain)),
-           'reconstructor_integrator_us': timeit(graph_of(lambda: loop._rec_integ(out_next=nxt[0])))}
+           'atmosphere_propagation_us': timeit(graph_of(lambda: atmosphere(0))),
+           'sh_detector_slopes_us': timeit(graph_of(lambda: sh_chain(0))),
+           'reconstructor_integrator_us': timeit(graph_of(lambda: loop._rec_integ(out_next=nxt[0]))),
+           'early_atmosphere': early}
     del graphs
     _lib_status()
     return out

@@ -276,10 +276,20 @@ int sb_slopec_batched(const sb_slopec_plan *plan, const float *pixels, long long
  * lenslet_subap[i * n_lenses + j] is the valid sub-aperture index of lenslet
  * (row i, column j) or -1.  scratch: sb_sh_ccd_slopec_scratch_bytes(sh,
  * n_subaps) bytes, no initialisation needed.
+ * mirror_A / mirror_phase (dft_mode 0 only; NULL: none): the last layer of
+ * the on-axis propagation (atmo_propagation.py:105-144), applied while the
+ * field is read: the SH sees amplitude A * mirror_A and phase phase_nm +
+ * mirror_phase (A, phase_nm then hold the product and sum of the other
+ * layers, in their order), the photon normalisation uses that amplitude
+ * (A_norm must be A, n_norm the whole field), and the field is written to
+ * field_A / field_phase (the AtmoPropagation output) when they are given.
+ * So the turbulence of a step can be computed before the mirror of the
+ * previous step is known.
  */
 size_t sb_sh_ccd_slopec_scratch_bytes(const sb_sh_plan *sh, int n_subaps);
 int sb_sh_ccd_slopec(const sb_sh_plan *sh, int dft_mode, const float *A, const float *phase_nm,
-                     const float *A_norm, int n_norm, float photon_scale, float *intensity,
+                     const float *A_norm, int n_norm, const float *mirror_A, const float *mirror_phase,
+                     float *field_A, float *field_phase, float photon_scale, float *intensity,
                      const sb_ccd_params *ccd, float *integrated, float *pixels,
                      const sb_slopec_plan *slopec, const int32_t *lenslet_subap, float *slopes,
                      float *flux, void *scratch, size_t scratch_bytes, void *stream);
@@ -575,7 +585,11 @@ int sb_propagate_batched(const float *atm, int n_atm, long long atm_layer_stride
  * every layer is still written to its `out`, its values summed in layer
  * order and the field formed as sb_propagate_batched does, with the same
  * bits as the two calls.  n_batch = 1 serves a single system (the pipelined
- * SCAO step graph calls it so). */
+ * SCAO step graph calls it so).  dm_phase NULL: no mirror term (dm_A is not
+ * read); the outputs then hold the product and sum of the turbulence and the
+ * stop, for a consumer that applies the mirror itself (sb_sh_ccd_slopec),
+ * so the turbulence of a step need not wait for the previous mirror;
+ * at most 16 layers per realisation. */
 int sb_atmo_propagate_batched(const sb_atmo_layer *layers, const sb_atmo_layer_inputs *inputs, int n_atm, int n_batch,
                               int L, const sb_atmo_inputs *constants, void *work, size_t work_bytes,
                               const float *stop_A, const float *stop_phase, const float *dm_A, const float *dm_phase,

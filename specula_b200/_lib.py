@@ -91,7 +91,7 @@ SIGNATURES = {
     'sb_slopec_scratch_bytes': (C.c_size_t, [C.POINTER(SlopecPlan)]),
     'sb_slopec': (C.c_int, [C.POINTER(SlopecPlan), fp, fp, fp, vp, C.c_size_t, vp]),
     'sb_sh_ccd_slopec_scratch_bytes': (C.c_size_t, [C.POINTER(ShPlan), C.c_int]),
-    'sb_sh_ccd_slopec': (C.c_int, [C.POINTER(ShPlan), C.c_int, fp, fp, fp, C.c_int, C.c_float, fp,
+    'sb_sh_ccd_slopec': (C.c_int, [C.POINTER(ShPlan), C.c_int, fp, fp, fp, C.c_int, fp, fp, fp, fp, C.c_float, fp,
                                    C.POINTER(CcdParams), fp, fp, C.POINTER(SlopecPlan), ip, fp, fp, vp,
                                    C.c_size_t, vp]),
     'sb_modalrec': (C.c_int, [fp, C.c_int, C.c_int, C.c_int, fp, fp, vp]),

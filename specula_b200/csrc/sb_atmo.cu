@@ -413,8 +413,10 @@ __global__ void __launch_bounds__(256, 4) atmo_propagate_kernel(EvolveArgsT<CAP>
         float amp = 1.0f, ph = acc[j];
         if (f.stop_A) amp = __fmul_rn(amp, f.stop_A[e]);
         if (f.stop_phase) ph = __fadd_rn(ph, f.stop_phase[e]);
-        if (f.dm_A) amp = __fmul_rn(amp, f.dm_A[e]);
-        ph = __fadd_rn(ph, f.dm_phase[b * f.dm_stride + e]);
+        if (f.dm_phase) {                 // NULL: the mirror term is left to the consumer
+            if (f.dm_A) amp = __fmul_rn(amp, f.dm_A[e]);
+            ph = __fadd_rn(ph, f.dm_phase[b * f.dm_stride + e]);
+        }
         f.A[b * f.out_stride + e] = amp;
         f.P[b * f.out_stride + e] = ph;
     }
@@ -611,8 +613,8 @@ extern "C" int sb_atmo_propagate_batched(const sb_atmo_layer *layers, const sb_a
     sb::clear_error();
     const long long n = (long long)L * L;
     if (!layers || !inputs || !constants || n_atm < 1 || n_atm > kBatchLayers || n_batch < 1 || L < 1 ||
-        !(constants->pixel_pitch > 0.0) || !(constants->delta_time >= 0.0) || !dm_phase || !A_out || !phase_out ||
-        dm_stride < n || out_stride < n)
+        !(constants->pixel_pitch > 0.0) || !(constants->delta_time >= 0.0) || !A_out || !phase_out ||
+        (dm_phase && dm_stride < n) || out_stride < n)
         return sb::fail(SB_EINVAL, "sb_atmo_propagate_batched: bad args");
     if (n_atm > kFusedMaxLayers)
         return sb::fail(SB_ESHAPE, "sb_atmo_propagate_batched: at most %d layers per realisation", kFusedMaxLayers);

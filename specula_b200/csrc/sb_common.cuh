@@ -24,9 +24,13 @@ int tune_lookup(int family, unsigned long long key);
 // in `intensity`, the per-CTA partial sums at the start of `scratch` (n_parts
 // sums of the frame, then n_parts sums of A_norm); *n_parts receives the
 // number of CTAs.  mode 0: FP32 DFTs, 1: split-BF16 tensor-core DFTs.
+// mirror_A / mirror_phase (FP32 form): the field is A * mirror_A, phase_nm +
+// mirror_phase, written to field_A / field_phase when those are given.
 int sh_forward_unnormalised(const char *who, const sb_sh_plan *pl, const float *A, const float *phase_nm,
                             const float *A_norm, int n_norm, float *intensity, void *scratch, size_t scratch_bytes,
-                            void *stream, int mode, int *n_parts);
+                            void *stream, int mode, int *n_parts, const float *mirror_A = nullptr,
+                            const float *mirror_phase = nullptr, float *field_A = nullptr,
+                            float *field_phase = nullptr);
 
 // Check the launch that just happened on this thread.
 inline int check_launch(const char *what) {

@@ -778,7 +778,8 @@ extern "C" size_t sb_sh_ccd_slopec_scratch_bytes(const sb_sh_plan *sh, int n_val
 }
 
 extern "C" int sb_sh_ccd_slopec(const sb_sh_plan *sh, int dft_mode, const float *A, const float *phase_nm,
-                                const float *A_norm, int n_norm, float photon_scale, float *intensity,
+                                const float *A_norm, int n_norm, const float *mirror_A, const float *mirror_phase,
+                                float *field_A, float *field_phase, float photon_scale, float *intensity,
                                 const sb_ccd_params *ccd, float *integrated, float *pixels,
                                 const sb_slopec_plan *slopec, const int32_t *lenslet_subap, float *slopes,
                                 float *flux, void *scratch, size_t scratch_bytes, void *stream) {
@@ -807,7 +808,8 @@ extern "C" int sb_sh_ccd_slopec(const sb_sh_plan *sh, int dft_mode, const float 
     int nparts = 0;
     const size_t sh_bytes = sb_sh_scratch_bytes(sh);
     int rc = sb::sh_forward_unnormalised("sb_sh_ccd_slopec", sh, A, phase_nm, A_norm, n_norm, intensity, scratch,
-                                         sh_bytes, stream, dft_mode, &nparts);
+                                         sh_bytes, stream, dft_mode, &nparts, mirror_A, mirror_phase, field_A,
+                                         field_phase);
     if (rc) return rc;
     ChainArgs a;
     a.p = *ccd;

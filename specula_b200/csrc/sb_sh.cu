@@ -37,7 +37,31 @@ struct ShArgs {
     long long sA, sph, sAn, sout;
     int nbp;                       // partial sums per realisation
     int vec;                       // field rows may be read as float4 (16-byte aligned rows and strides)
+    // the mirror term of the on-axis propagation applied while the field is
+    // read (single field, FP32 forms): amplitude A * A2, phase ph + ph2, the
+    // normalising amplitude A_norm * A2; the resulting field is written to
+    // A_out / P_out when they are given.  NULL A2: the field is A, ph.
+    const float *A2, *ph2;
+    float *A_out, *P_out;
 };
+
+// amplitude and phase (nm) of field element g, with the mirror term when present
+__device__ __forceinline__ void field_at(const ShArgs &a, size_t g, float &amp, float &phn) {
+    amp = a.A[g];
+    phn = a.ph[g];
+    if (a.A2) {
+        amp = __fmul_rn(amp, a.A2[g]);      // the order of the on-axis propagation: layers, stop, mirror
+        phn = __fadd_rn(phn, a.ph2[g]);
+        if (a.A_out) {
+            a.A_out[g] = amp;
+            a.P_out[g] = phn;
+        }
+    }
+}
+
+__device__ __forceinline__ float norm_amp(const ShArgs &a, int e) {
+    return a.A2 ? __fmul_rn(a.A_norm[e], a.A2[e]) : a.A_norm[e];
+}
 
 // the realisation's slice of a batched launch
 __device__ __forceinline__ void batch_slice(ShArgs &a) {
@@ -112,8 +136,9 @@ __global__ void __launch_bounds__(256, 4) sh_forward_kernel(ShArgs a) {
         for (int e = lane; e < p * p; e += 32) {
             const int r = e / p, c = e - r * p;
             const size_t g = (row0 + r) * (size_t)a.ld + col0 + c;
-            const float amp = a.A[g];
-            const float phi = a.ph[g] * a.k;
+            float amp, phn;
+            field_at(a, g, amp, phn);
+            const float phi = phn * a.k;
             float sn, co;
             sincosf(phi, &sn, &co);
             const float re = co * amp, im = sn * amp;
@@ -202,7 +227,7 @@ __global__ void __launch_bounds__(256, 4) sh_forward_kernel(ShArgs a) {
     const int lo = bid * chunk;
     const int hi = min(a.n_norm, lo + chunk);
     float sa = 0.f;
-    for (int e = lo + threadIdx.x; e < hi; e += blockDim.x) sa += a.A_norm[e];
+    for (int e = lo + threadIdx.x; e < hi; e += blockDim.x) sa += norm_amp(a, e);
     const float tota = sb::block_sum(sa, red);
     if (threadIdx.x == 0) {
         a.part_I[bid] = tot;
@@ -251,8 +276,9 @@ __global__ void __launch_bounds__(256, 4) sh_forward_fixed_kernel(ShArgs a) {
         for (int e = lane; e < P * P; e += 32) {
             const int r = e / P, c = e % P;
             const size_t g = (row0 + r) * (size_t)a.ld + col0 + c;
-            const float amp = a.A[g];
-            const float phi = a.ph[g] * a.k;
+            float amp, phn;
+            field_at(a, g, amp, phn);
+            const float phi = phn * a.k;
             float sn, co;
             sincosf(phi, &sn, &co);
             const float re = co * amp, im = sn * amp;
@@ -318,7 +344,7 @@ __global__ void __launch_bounds__(256, 4) sh_forward_fixed_kernel(ShArgs a) {
     const int lo = bid * chunk;
     const int hi = min(a.n_norm, lo + chunk);
     float sa = 0.f;
-    for (int e = lo + threadIdx.x; e < hi; e += blockDim.x) sa += a.A_norm[e];
+    for (int e = lo + threadIdx.x; e < hi; e += blockDim.x) sa += norm_amp(a, e);
     const float tota = sb::block_sum(sa, red);
     if (threadIdx.x == 0) {
         a.part_I[bid] = tot;
@@ -787,7 +813,7 @@ __global__ void __launch_bounds__(32 * lgs_warps<N>()) sh_forward_lgs_kernel(ShA
     const int lo = bid * chunk;
     const int hi = min(a.n_norm, lo + chunk);
     float sa = 0.f;
-    for (int e = lo + threadIdx.x; e < hi; e += blockDim.x) sa += a.A_norm[e];
+    for (int e = lo + threadIdx.x; e < hi; e += blockDim.x) sa += norm_amp(a, e);
     const float tota = sb::block_sum(sa, red);
     if (threadIdx.x == 0) {
         a.part_I[bid] = tot;
@@ -929,7 +955,8 @@ namespace {
 int sh_forward_impl(const char *who, const sb_sh_plan *pl, const float *A, long long sA, const float *phase_nm,
                     long long sph, const float *A_norm, long long sAn, int n_norm, float photon_scale,
                     float *intensity, long long sout, int n_batch, void *scratch, size_t scratch_bytes, void *stream,
-                    int mode = 0, bool normalize = true, int *n_parts = nullptr) {
+                    int mode = 0, bool normalize = true, int *n_parts = nullptr, const float *mirror_A = nullptr,
+                    const float *mirror_phase = nullptr, float *field_A = nullptr, float *field_phase = nullptr) {
     if (!pl || !A || !phase_nm || !A_norm || !intensity || !pl->twiddle || !pl->tilt || !pl->fp_mask ||
         !pl->rebin)
         return sb::fail(SB_EINVAL, "%s: null pointer", who);
@@ -946,6 +973,16 @@ int sh_forward_impl(const char *who, const sb_sh_plan *pl, const float *A, long 
     const size_t need = sb_sh_scratch_bytes(pl) * (size_t)n_batch;
     if (!scratch || scratch_bytes < need)
         return sb::fail(SB_ESCRATCH, "%s: scratch needs %zu bytes, got %zu", who, need, scratch_bytes);
+    if (mirror_A || mirror_phase || field_A || field_phase) {
+        if (!mirror_A || !mirror_phase || !field_A != !field_phase)
+            return sb::fail(SB_EINVAL, "%s: the mirror amplitude and phase go together, as do the field outputs", who);
+        if (mode != 0 || n_batch != 1)
+            return sb::fail(SB_EUNSUPPORTED, "%s: the mirror term is applied by the single-field FP32 form only", who);
+        if (field_A && pl->field_ld != pl->n_lenses * pl->np_sub)
+            return sb::fail(SB_EINVAL, "%s: the field outputs need a field of exactly n_lenses x np_sub columns", who);
+        if (A_norm != A || n_norm != pl->field_ld * pl->field_ld)
+            return sb::fail(SB_EINVAL, "%s: with the mirror term the normalising amplitude is the whole field", who);
+    }
     ShTcKernel tk = {nullptr, 0};
     if (mode == 1) {
         tk = tc_kernel(pl->np_sub, pl->cutsize, pl->subap_npx);
@@ -981,6 +1018,10 @@ int sh_forward_impl(const char *who, const sb_sh_plan *pl, const float *A, long 
     a.sAn = sAn;
     a.sout = sout;
     a.nbp = nb;
+    a.A2 = mirror_A;
+    a.ph2 = mirror_phase;
+    a.A_out = field_A;
+    a.P_out = field_phase;
     a.vec = (a.ld % 4 == 0) && (sA % 4 == 0) && (sph % 4 == 0) && ((uintptr_t)A % 16 == 0) &&
             ((uintptr_t)phase_nm % 16 == 0) && (a.p % 4 == 0);
     grid.z = n_batch;
@@ -1019,9 +1060,10 @@ int sh_forward_impl(const char *who, const sb_sh_plan *pl, const float *A, long 
 namespace sb {
 int sh_forward_unnormalised(const char *who, const sb_sh_plan *pl, const float *A, const float *phase_nm,
                             const float *A_norm, int n_norm, float *intensity, void *scratch, size_t scratch_bytes,
-                            void *stream, int mode, int *n_parts) {
+                            void *stream, int mode, int *n_parts, const float *mirror_A, const float *mirror_phase,
+                            float *field_A, float *field_phase) {
     return sh_forward_impl(who, pl, A, 0, phase_nm, 0, A_norm, 0, n_norm, 1.0f, intensity, 0, 1, scratch,
-                           scratch_bytes, stream, mode, false, n_parts);
+                           scratch_bytes, stream, mode, false, n_parts, mirror_A, mirror_phase, field_A, field_phase);
 }
 }  // namespace sb
 

@@ -192,7 +192,7 @@ class ScaoLoop:
         self.wind_speed.value = vec[1:1 + nl]
         self.wind_direction.value = vec[1 + nl:]
 
-    def capture(self, pipelined=True, io=False, fuse_atmo=None, fuse_chain=None):
+    def capture(self, pipelined=True, io=False, fuse_atmo=None, fuse_chain=None, early_atmo=None):
         """Capture whole steps in a CUDA graph.  Call after at least one eager
         step, so the time step used by AtmoEvolution is the loop's (the first
         step has delta_time = 0).
@@ -221,6 +221,16 @@ class ScaoLoop:
         (sb_sh_ccd_slopec: the SH forward, then normalisation, detector and
         CoG on each lenslet's pixels in shared memory) instead of five; the
         same bits.  None: fused whenever the objects allow it.
+
+        ``early_atmo`` (pipelined form with both fusions and the FP32 SH):
+        the mirror term of the propagation moves into the SH's field read
+        (sb_sh_ccd_slopec with the mirror arguments, which also writes the
+        propagated field), so the atmosphere of a step no longer waits for
+        the previous mirror: both steps' atmospheres run on a third stream
+        from the start of the replay, into per-step buffers, and only the
+        SH waits for DM(t-1).  The chain that must end before the next DM
+        projection is then SH, detector/CoG and reconstructor.  The same
+        bits.  None: whenever the objects allow it.
         """
         self.step_eager()
         torch.cuda.synchronize(self.device)
@@ -236,6 +246,12 @@ class ScaoLoop:
         self.fused_chain = bool(fuse_chain)
         if self.fused_chain:
             self._setup_chain()
+        if early_atmo is None:
+            early_atmo = self._can_early_atmo()
+        self.early_atmo = bool(early_atmo and self.pipelined and self.fused_atmo and self.fused_chain)
+        if early_atmo and not self.early_atmo:
+            raise NotImplementedError('ScaoLoop.capture: the early atmosphere needs the pipelined form with the '
+                                      'fused atmosphere and the fused SH / detector / slope chain')
         if io and not self.pipelined:
             raise ValueError('ScaoLoop.capture: io slots need the pipelined form (integer integrator delay >= 1)')
         if not self.pipelined:
@@ -268,43 +284,106 @@ class ScaoLoop:
                 nm = self.integ.out_comm.value.numel()
                 self.io_inputs = self._inputs.repeat(2, 1).contiguous()
                 self.io_outputs = torch.zeros((2, nsl + nm), dtype=torch.float32, device=self.device)
-            with torch.cuda.graph(g, stream=cap):
-                main = torch.cuda.current_stream(self.device)
-                dm_done = None
-                for step, par in enumerate((1, 0)):    # odd step, then even step
-                    # DM(t) needs the integrator output of step t-1
-                    side.wait_stream(main)
-                    with torch.cuda.stream(side):
-                        self.dm.project(nxt[par], dm_buf[par])
-                        ev = torch.cuda.Event()
-                        ev.record(side)
-                    # AtmoEvolution(t) does not depend on the mirror
-                    if io:
-                        self._point_inputs(self.io_inputs[step])
-                    if fuse_atmo:
-                        if dm_done is not None:
-                            main.wait_event(dm_done)
-                        self._atmo_propagate(dm_buf[1 - par])
-                    else:
-                        self.atmo.trigger_code()
-                        # the propagation of step t reads DM(t-1): the previous
-                        # replay (already complete) for the first step of the graph
-                        if dm_done is not None:
-                            main.wait_event(dm_done)
-                        self.prop.trigger_code(phase_override={id(self.dm.layer): dm_buf[1 - par]})
-                    self._chain()
-                    self._rec_integ(out_next=nxt[1 - par])
-                    if io:
-                        self.io_outputs[step, :nsl].copy_(self.slopec.slopes.slopes)
-                        self.io_outputs[step, nsl:].copy_(self.integ.out_comm.value)
-                    dm_done = ev
-                main.wait_stream(side)
+            if self.early_atmo:
+                self._capture_early(g, side, cap, dm_buf, nxt, io)
+            else:
+                self._capture_pipelined(g, side, cap, dm_buf, nxt, io, fuse_atmo)
             if io:
                 self._point_inputs(self._inputs)
             self.steps_per_replay = 2
         torch.cuda.synchronize(self.device)
         self.graph = g
         return g
+
+    def _capture_pipelined(self, g, side, cap, dm_buf, nxt, io, fuse_atmo):
+        """The pipelined two-step graph (see capture())."""
+        if io:
+            nsl = self.slopec.slopes.slopes.numel()
+        with torch.cuda.graph(g, stream=cap):
+            main = torch.cuda.current_stream(self.device)
+            dm_done = None
+            for step, par in enumerate((1, 0)):    # odd step, then even step
+                # DM(t) needs the integrator output of step t-1
+                side.wait_stream(main)
+                with torch.cuda.stream(side):
+                    self.dm.project(nxt[par], dm_buf[par])
+                    ev = torch.cuda.Event()
+                    ev.record(side)
+                # AtmoEvolution(t) does not depend on the mirror
+                if io:
+                    self._point_inputs(self.io_inputs[step])
+                if fuse_atmo:
+                    if dm_done is not None:
+                        main.wait_event(dm_done)
+                    self._atmo_propagate(dm_buf[1 - par])
+                else:
+                    self.atmo.trigger_code()
+                    # the propagation of step t reads DM(t-1): the previous
+                    # replay (already complete) for the first step of the graph
+                    if dm_done is not None:
+                        main.wait_event(dm_done)
+                    self.prop.trigger_code(phase_override={id(self.dm.layer): dm_buf[1 - par]})
+                self._chain()
+                self._rec_integ(out_next=nxt[1 - par])
+                if io:
+                    self.io_outputs[step, :nsl].copy_(self.slopec.slopes.slopes)
+                    self.io_outputs[step, nsl:].copy_(self.integ.out_comm.value)
+                dm_done = ev
+            main.wait_stream(side)
+
+    def _capture_early(self, g, side, cap, dm_buf, nxt, io):
+        """The pipelined two-step graph with the atmosphere of both steps on
+        a stream of its own (see capture(early_atmo=...))."""
+        L = self.cfg.pixel_pupil
+        # per-step product / sum of the turbulence and the stop (the mirror is applied by the SH)
+        self._early = [(torch.empty((L, L), dtype=torch.float32, device=self.device),
+                        torch.empty((L, L), dtype=torch.float32, device=self.device)) for _ in range(2)]
+        atm = torch.cuda.Stream(self.device, priority=0)
+        self._atm = atm
+        if io:
+            nsl = self.slopec.slopes.slopes.numel()
+        with torch.cuda.graph(g, stream=cap):
+            main = torch.cuda.current_stream(self.device)
+            atm.wait_stream(main)
+            atmo_done = []
+            for step, par in enumerate((1, 0)):        # odd step, then even step
+                with torch.cuda.stream(atm):
+                    if io:
+                        self._point_inputs(self.io_inputs[step])
+                    self._atmo_propagate(None, out=self._early[par])
+                    ev = torch.cuda.Event()
+                    ev.record(atm)
+                atmo_done.append(ev)
+            dm_done = None
+            for step, par in enumerate((1, 0)):
+                # DM(t) needs the integrator output of step t-1
+                side.wait_stream(main)
+                with torch.cuda.stream(side):
+                    self.dm.project(nxt[par], dm_buf[par])
+                    ev = torch.cuda.Event()
+                    ev.record(side)
+                main.wait_event(atmo_done[step])
+                # the SH applies DM(t-1): the previous replay (already complete) for the first step
+                if dm_done is not None:
+                    main.wait_event(dm_done)
+                self._sh_ccd_slopec(mirror=dm_buf[1 - par], partial=self._early[par])
+                self._rec_integ(out_next=nxt[1 - par])
+                if io:
+                    self.io_outputs[step, :nsl].copy_(self.slopec.slopes.slopes)
+                    self.io_outputs[step, nsl:].copy_(self.integ.out_comm.value)
+                dm_done = ev
+            main.wait_stream(side)
+            main.wait_stream(atm)
+
+    def _can_early_atmo(self):
+        """True when the mirror term can move into the SH's field read: the
+        fused atmosphere and chain apply, the SH runs its FP32 DFTs on the
+        pupil grid itself (one phase sample per lenslet pixel)."""
+        sh = self.sh
+        g = sh.geometry
+        return (self._can_fuse_atmo() and self._can_fuse_chain() and sh._forward == 'sb_sh_forward' and
+                not g.do_interpolation and int(sh._plan.field_ld) == self.cfg.pixel_pupil and
+                int(sh._plan.n_lenses) * int(sh._plan.np_sub) == self.cfg.pixel_pupil)
 
     def _chain(self):
         """SH, CCD and ShSlopec of one step: two launches when fused, else
@@ -361,13 +440,22 @@ class ScaoLoop:
         nb = _lib.load().sb_sh_ccd_slopec_scratch_bytes(ctypes.byref(self.sh._plan), self.slopec._plan.n_subaps)
         self._chain_scratch = torch.zeros(nb, dtype=torch.uint8, device=self.device)
 
-    def _sh_ccd_slopec(self):
+    def _sh_ccd_slopec(self, mirror=None, partial=None):
+        """The fused chain on the propagated field; with ``mirror`` (a DM
+        phase buffer) and ``partial`` ((A, phase) of turbulence and stop) the
+        SH applies the mirror itself and writes the propagated field."""
         sh, ccd, sl = self.sh, self.ccd, self.slopec
         ef = sh._in_ef
         st = sh.stream_handle()
         mode = 0 if sh._forward == 'sb_sh_forward' else 1
-        _lib.call('sb_sh_ccd_slopec', ctypes.byref(sh._plan), mode, ef.A.data_ptr(), ef.phaseInNm.data_ptr(),
-                  ef.A.data_ptr(), ef.A.numel(), sh._photon_scale, sh._out_i.i.data_ptr(), ctypes.byref(ccd._params),
+        if mirror is None:
+            A, P, mA, mP, fA, fP = ef.A, ef.phaseInNm, None, None, None, None
+        else:
+            A, P = partial
+            mA, mP, fA, fP = self.dm.layer.A.data_ptr(), mirror.data_ptr(), ef.A.data_ptr(), ef.phaseInNm.data_ptr()
+        _lib.call('sb_sh_ccd_slopec', ctypes.byref(sh._plan), mode, A.data_ptr(), P.data_ptr(),
+                  A.data_ptr(), A.numel(), mA, mP, fA, fP, sh._photon_scale, sh._out_i.i.data_ptr(),
+                  ctypes.byref(ccd._params),
                   ccd._integrated_i.i.data_ptr(), ccd._pixels.pixels.data_ptr(), ctypes.byref(sl._plan),
                   self._lenslet_subap.data_ptr(), sl._target.data_ptr(), sl._flux.data_ptr(),
                   self._chain_scratch.data_ptr(), self._chain_scratch.numel(), st)
@@ -390,10 +478,11 @@ class ScaoLoop:
                 len(prop._layers) - 2 == len(self.atmo.layer_list) and
                 all(a is b for a, b in zip(prop._layers[:-2], self.atmo.layer_list)))
 
-    def _atmo_propagate(self, dm_phase):
+    def _atmo_propagate(self, dm_phase, out=None):
         """AtmoEvolution.trigger_code + AtmoPropagation.trigger_code in one
         launch: pupil-sized turbulence layers, then the pupil stop and the
-        mirror (phase read from ``dm_phase``)."""
+        mirror (phase read from ``dm_phase``; None: no mirror term).  The
+        field goes to the propagation output, or to ``out`` = (A, phase)."""
         atmo, prop = self.atmo, self.prop
         nl = atmo.n_phasescreens
         if not self._can_fuse_atmo():
@@ -408,10 +497,11 @@ class ScaoLoop:
         ef = prop.outputs['out_on_axis_source_ef']
         L = self.cfg.pixel_pupil
         stop = self.pupilstop
+        oA, oP = (ef.A, ef.phaseInNm) if out is None else out
         _lib.call('sb_atmo_propagate_batched', atmo._layers, ins, nl, 1, L, ctypes.byref(consts),
                   atmo._work.data_ptr(), atmo._work.numel(), stop.A.data_ptr(), stop.phaseInNm.data_ptr(),
-                  self.dm.layer.A.data_ptr(), dm_phase.data_ptr(), L * L, ef.A.data_ptr(), ef.phaseInNm.data_ptr(),
-                  L * L, atmo.stream_handle())
+                  self.dm.layer.A.data_ptr(), None if dm_phase is None else dm_phase.data_ptr(), L * L,
+                  oA.data_ptr(), oP.data_ptr(), L * L, atmo.stream_handle())
 
     def _rec_integ(self, out_next=None):
         """Modalrec + Integrator of this loop as one launch

@@ -38,7 +38,8 @@ def _loop(mode, n_steps, cfg_kw=None, strided_stop=False):
         elif mode == 'pipelined_unfused_chain':
             loop.capture(fuse_chain=False)
         else:
-            loop.capture(pipelined=mode.startswith('pipelined'), fuse_atmo=(mode == 'pipelined_fused'))
+            loop.capture(pipelined=mode.startswith('pipelined'), fuse_atmo=(mode == 'pipelined_fused'),
+                         early_atmo=False)
         done += 1
         while done < n_steps:
             loop.replay()
@@ -48,23 +49,32 @@ def _loop(mode, n_steps, cfg_kw=None, strided_stop=False):
     return loop
 
 
-@pytest.mark.parametrize('mode', ['sequential', 'pipelined', 'pipelined_fused', 'pipelined_unfused_chain'])
+@pytest.mark.parametrize('mode', ['sequential', 'pipelined', 'pipelined_fused', 'pipelined_unfused_chain',
+                                  'pipelined_default'])
 def test_graph_step_matches_object_loop(mode, cuda):
     """pipelined_fused: AtmoEvolution and AtmoPropagation as one launch;
     every mode but pipelined_unfused_chain runs SH, CCD and ShSlopec as the
-    two launches of sb_sh_ccd_slopec."""
+    two launches of sb_sh_ccd_slopec; pipelined_default (the default capture)
+    also runs the atmosphere early, on a stream of its own, with the mirror
+    applied in the SH's field read."""
     n = 10
     ref = _loop('eager', n)
     got = _loop(mode, n)
     if mode.startswith('pipelined'):
         assert got.pipelined and got.steps_per_replay == 2
     assert got.fused_chain == (mode != 'pipelined_unfused_chain')
+    assert got.early_atmo == (mode == 'pipelined_default')
     for name, a, b in (('slopes', ref.slopec.slopes.slopes, got.slopec.slopes.slopes),
                        ('dm phase', ref.dm.layer.phaseInNm, got.dm.layer.phaseInNm),
                        ('commands', ref.integ.out_comm.value, got.integ.out_comm.value),
                        ('integrator state', ref.integ.state, got.integ.state),
                        ('pixels', ref.ccd.outputs['out_pixels'].pixels, got.ccd.outputs['out_pixels'].pixels),
-                       ('layers', ref.atmo.layer_list[1].phaseInNm, got.atmo.layer_list[1].phaseInNm)):
+                       ('layers', ref.atmo.layer_list[1].phaseInNm, got.atmo.layer_list[1].phaseInNm),
+                       ('field phase', ref.prop.outputs['out_on_axis_source_ef'].phaseInNm,
+                        got.prop.outputs['out_on_axis_source_ef'].phaseInNm),
+                       ('field amplitude', ref.prop.outputs['out_on_axis_source_ef'].A,
+                        got.prop.outputs['out_on_axis_source_ef'].A),
+                       ('intensity', ref.sh.outputs['out_i'].i, got.sh.outputs['out_i'].i)):
         assert torch.equal(a, b), name
     assert float(ref.dm.layer.phaseInNm.abs().max()) > 0
 
@@ -84,7 +94,7 @@ def test_default_capture_fuses_the_atmosphere(cuda):
     n = 6
     ref = _loop('eager', n)
     got = _loop('pipelined_default', n)
-    assert got.pipelined and got.fused_atmo and got.fused_chain and got.kernels_per_step == 6
+    assert got.pipelined and got.fused_atmo and got.fused_chain and got.early_atmo and got.kernels_per_step == 6
     _assert_same_loop_state(ref, got)
 
 
