@@ -247,7 +247,7 @@ class ScaoLoop:
         if self.fused_chain:
             self._setup_chain()
         if early_atmo is None:
-            early_atmo = self._can_early_atmo()
+            early_atmo = self._can_early_atmo() and self.pipelined and self.fused_atmo and self.fused_chain
         self.early_atmo = bool(early_atmo and self.pipelined and self.fused_atmo and self.fused_chain)
         if early_atmo and not self.early_atmo:
             raise NotImplementedError('ScaoLoop.capture: the early atmosphere needs the pipelined form with the '
