@@ -192,7 +192,7 @@ class ScaoLoop:
         self.wind_speed.value = vec[1:1 + nl]
         self.wind_direction.value = vec[1 + nl:]
 
-    def capture(self, pipelined=True, io=False, fuse_atmo=None, fuse_chain=None, early_atmo=None):
+    def capture(self, pipelined=True, io=False, fuse_atmo=None, fuse_chain=None, early_atmo=False):
         """Capture whole steps in a CUDA graph.  Call after at least one eager
         step, so the time step used by AtmoEvolution is the loop's (the first
         step has delta_time = 0).
@@ -230,7 +230,9 @@ class ScaoLoop:
         from the start of the replay, into per-step buffers, and only the
         SH waits for DM(t-1).  The chain that must end before the next DM
         projection is then SH, detector/CoG and reconstructor.  The same
-        bits.  None: whenever the objects allow it.
+        bits.  Off by default: on the ELT step it measured 117.9 us against
+        109.7 us for the fused form, the two atmospheres competing with the
+        replay's first DM projection for HBM and SMs.
         """
         self.step_eager()
         torch.cuda.synchronize(self.device)
@@ -246,8 +248,9 @@ class ScaoLoop:
         self.fused_chain = bool(fuse_chain)
         if self.fused_chain:
             self._setup_chain()
-        if early_atmo is None:
-            early_atmo = self._can_early_atmo() and self.pipelined and self.fused_atmo and self.fused_chain
+        # measured slower on the ELT step (117.9 against 109.7 us: both atmospheres then compete with the
+        # first DM projection of the replay), so it is chosen only when asked for
+        early_atmo = bool(early_atmo)
         self.early_atmo = bool(early_atmo and self.pipelined and self.fused_atmo and self.fused_chain)
         if early_atmo and not self.early_atmo:
             raise NotImplementedError('ScaoLoop.capture: the early atmosphere needs the pipelined form with the '

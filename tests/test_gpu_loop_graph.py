@@ -35,6 +35,8 @@ def _loop(mode, n_steps, cfg_kw=None, strided_stop=False):
     else:
         if mode == 'pipelined_default':
             loop.capture()
+        elif mode == 'pipelined_early':
+            loop.capture(early_atmo=True)
         elif mode == 'pipelined_unfused_chain':
             loop.capture(fuse_chain=False)
         else:
@@ -50,20 +52,20 @@ def _loop(mode, n_steps, cfg_kw=None, strided_stop=False):
 
 
 @pytest.mark.parametrize('mode', ['sequential', 'pipelined', 'pipelined_fused', 'pipelined_unfused_chain',
-                                  'pipelined_default'])
+                                  'pipelined_early'])
 def test_graph_step_matches_object_loop(mode, cuda):
     """pipelined_fused: AtmoEvolution and AtmoPropagation as one launch;
     every mode but pipelined_unfused_chain runs SH, CCD and ShSlopec as the
-    two launches of sb_sh_ccd_slopec; pipelined_default (the default capture)
-    also runs the atmosphere early, on a stream of its own, with the mirror
-    applied in the SH's field read."""
+    two launches of sb_sh_ccd_slopec; pipelined_early also runs the
+    atmosphere early, on a stream of its own, with the mirror applied in the
+    SH's field read."""
     n = 10
     ref = _loop('eager', n)
     got = _loop(mode, n)
     if mode.startswith('pipelined'):
         assert got.pipelined and got.steps_per_replay == 2
     assert got.fused_chain == (mode != 'pipelined_unfused_chain')
-    assert got.early_atmo == (mode == 'pipelined_default')
+    assert got.early_atmo == (mode == 'pipelined_early')
     for name, a, b in (('slopes', ref.slopec.slopes.slopes, got.slopec.slopes.slopes),
                        ('dm phase', ref.dm.layer.phaseInNm, got.dm.layer.phaseInNm),
                        ('commands', ref.integ.out_comm.value, got.integ.out_comm.value),
@@ -94,7 +96,7 @@ def test_default_capture_fuses_the_atmosphere(cuda):
     n = 6
     ref = _loop('eager', n)
     got = _loop('pipelined_default', n)
-    assert got.pipelined and got.fused_atmo and got.fused_chain and got.early_atmo and got.kernels_per_step == 6
+    assert got.pipelined and got.fused_atmo and got.fused_chain and not got.early_atmo and got.kernels_per_step == 6
     _assert_same_loop_state(ref, got)
 
 
