@@ -621,6 +621,25 @@ int sb_psf_field(const float *A, const float *phase_nm, int n_pixels, float phas
 int sb_psf_finish(const void *focal_field, long long n_pixels, float *psf, float *int_psf, void *scratch,
                   size_t scratch_bytes, void *stream);
 
+/* The PSF image on the tensor cores (replaces psf.py:56-96: the zero-padded
+ * field's |fftshift(fft2)|^2 normalised to unit sum, for an m x m field and
+ * the padded size n = round(m nd / 2) * 2).  F = W u W^T with the n x m DFT
+ * matrix W (rows in fftshift order) as two real GEMMs on tcgen05 with
+ * split-BF16 operands (hi*hi + lo*hi + hi*lo, FP32 accumulation in tensor
+ * memory); the normalisation uses Parseval's total n^2 sum |u|^2.
+ *   sb_psf_tc_prepare  builds the DFT operand once (dft: sb_psf_tc_dft_bytes,
+ *                      256-byte aligned)
+ *   sb_psf_tc          one PSF: psf (n x n float32), int_psf += psf when not
+ *                      NULL; scratch: sb_psf_tc_scratch_bytes, 256-byte
+ *                      aligned, zero-filled before the first call
+ * Three launches (field, W u^T, W G); bounded waits, reported by
+ * sb_device_status. */
+size_t sb_psf_tc_dft_bytes(int m, int n);
+int sb_psf_tc_prepare(int m, int n, void *dft, size_t dft_bytes, void *stream);
+size_t sb_psf_tc_scratch_bytes(int m, int n);
+int sb_psf_tc(const float *A, const float *phase_nm, int m, int n, float phase_to_rad, const void *dft, float *psf,
+              float *int_psf, void *scratch, size_t scratch_bytes, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -139,6 +139,10 @@ SIGNATURES = {
     'sb_strehl': (C.c_int, [fp, fp, C.c_int, C.c_float, fp, vp, C.c_int, vp, C.c_size_t, vp]),
     'sb_psf_field': (C.c_int, [fp, fp, C.c_int, C.c_float, vp, vp]),
     'sb_psf_finish': (C.c_int, [vp, C.c_longlong, fp, fp, vp, C.c_size_t, vp]),
+    'sb_psf_tc_dft_bytes': (C.c_size_t, [C.c_int, C.c_int]),
+    'sb_psf_tc_prepare': (C.c_int, [C.c_int, C.c_int, vp, C.c_size_t, vp]),
+    'sb_psf_tc_scratch_bytes': (C.c_size_t, [C.c_int, C.c_int]),
+    'sb_psf_tc': (C.c_int, [fp, fp, C.c_int, C.c_int, C.c_float, vp, fp, fp, vp, C.c_size_t, vp]),
     'sb_sh_slopes_jacobian': (C.c_int, [C.POINTER(ShPlan), fp, fp, C.c_int, ip, fp, fp, fp, fp, fp, fp, vp]),
     'sb_sh_slopes_vjp': (C.c_int, [C.POINTER(ShPlan), fp, fp, C.c_int, ip, fp, fp, fp, fp, fp, fp, vp]),
     'sb_intmat_contract': (C.c_int, [fp, fp, C.c_int, C.c_int, C.c_int, C.c_int, ip, ip, fp, C.c_int, C.c_int,

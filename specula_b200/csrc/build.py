@@ -14,7 +14,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
 ROOT = os.path.dirname(PKG)
 OUT = os.path.join(PKG, 'libspecula_b200.so')
-SOURCES = ['sb_common.cu', 'sb_sh.cu', 'sb_detector.cu', 'sb_control.cu', 'sb_atmo.cu', 'sb_adjoint.cu', 'sb_psf.cu']
+SOURCES = ['sb_common.cu', 'sb_sh.cu', 'sb_detector.cu', 'sb_control.cu', 'sb_atmo.cu', 'sb_adjoint.cu', 'sb_psf.cu',
+           'sb_psf_tc.cu']
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 
 

@@ -18,6 +18,8 @@ void clear_error();
 int sh_tc_status_take();
 // read and clear the timeout flag of the TMA interaction-matrix contraction
 int contract_status_take();
+// read and clear the timeout flag of the tensor-core PSF
+int psf_tc_status_take();
 // tile-shape variant registered for (family, key); 0 when none
 int tune_lookup(int family, unsigned long long key);
 // SH forward without its photon-normalisation launch: the unnormalised frame

@@ -733,7 +733,12 @@ extern "C" int sb_device_status(void) {
     if (sh < 0) return sb::fail(SB_ECUDA, "sb_device_status: %s", cudaGetErrorString(cudaGetLastError()));
     const int ct = sb::contract_status_take();
     if (ct < 0) return sb::fail(SB_ECUDA, "sb_device_status: %s", cudaGetErrorString(cudaGetLastError()));
-    if (v == 0 && sh == 0 && ct == 0) return SB_OK;
+    const int pt = sb::psf_tc_status_take();
+    if (pt < 0) return sb::fail(SB_ECUDA, "sb_device_status: %s", cudaGetErrorString(cudaGetLastError()));
+    if (v == 0 && sh == 0 && ct == 0 && pt == 0) return SB_OK;
+    if (v == 0 && sh == 0 && ct == 0)
+        return sb::fail(SB_ETIMEOUT, "a tensor-core PSF wait timed out (%s)",
+                        pt == 1 ? "copy ring" : (pt == 2 ? "MMA issue" : "epilogue"));
     if (v == 0 && sh == 0)
         return ct == 3 ? sb::fail(SB_EINVAL, "sb_intmat_contract_rows: a row segment does not cover its columns or "
                                              "is not 16-byte aligned (those rows were not contracted)")

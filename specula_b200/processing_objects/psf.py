@@ -10,9 +10,10 @@ the reference, plus the ``int_sr`` / ``int_psf`` values it integrates after
 * PSF image: the reference zero-pads the field to N = round(M nd / 2) * 2,
   FFTs and fftshifts it.  Here the padding never materialises:
   F = W u W^T with the N x M pruned DFT matrix W whose rows are already in
-  fftshift order, as two complex64 GEMMs (cuBLAS through torch.matmul,
-  IEEE float32), between sb_psf_field (u = A e^{i phi}) and sb_psf_finish
-  (|F|^2 / sum, accumulated into the integrated PSF).
+  fftshift order, as two real GEMMs on the tensor cores (sb_psf_tc:
+  tcgen05 with split-BF16 operands and FP32 accumulation), the field built
+  in the first launch, |F|^2 / total (Parseval's total N^2 sum |u|^2) and
+  the integration in the last GEMM's epilogue.
 """
 import numpy as np
 import torch
@@ -27,17 +28,6 @@ from specula_b200.data_objects.electric_field import ElectricField
 def psf_size(dim, nd):
     """Padded PSF size (psf.py:46-52): round(dim * nd / 2) * 2."""
     return int(np.around(dim * nd / 2) * 2)
-
-
-def shifted_dft_matrix(n_out, n_in):
-    """W[p][x] = exp(-2 pi i k_p x / n_out) with k_p = (p - n_out // 2) mod
-    n_out: the rows of the n_out-point DFT restricted to the first n_in
-    inputs, in fftshift order (float64 phases, complex64 result)."""
-    k = (np.arange(n_out) - n_out // 2) % n_out
-    x = np.arange(n_in)
-    # the integer product reduced modulo n_out before the float64 phase
-    ph = (-2.0 * np.pi / n_out) * (np.outer(k, x) % n_out)
-    return (np.cos(ph) + 1j * np.sin(ph)).astype(np.complex64)
 
 
 class PSF(BaseProcessingObj):
@@ -71,12 +61,12 @@ class PSF(BaseProcessingObj):
         dev = self.device
         self.out_size = [n, n]
         self._m, self._n = m, n
-        W = torch.as_tensor(shifted_dft_matrix(n, m), device=dev)
-        self._W = W.contiguous()                    # n x m
-        self._WT = W.t().contiguous()               # m x n
-        self._u = torch.empty((m, m), dtype=torch.complex64, device=dev)
-        self._G = torch.empty((m, n), dtype=torch.complex64, device=dev)
-        self._F = torch.empty((n, n), dtype=torch.complex64, device=dev)
+        lib = _lib.load()
+        # the DFT operand (split-BF16, pre-tiled for the tensor cores), built once on the device
+        self._dft = torch.empty(lib.sb_psf_tc_dft_bytes(m, n), dtype=torch.uint8, device=dev)
+        _lib.call('sb_psf_tc_prepare', m, n, self._dft.data_ptr(), self._dft.numel(),
+                  torch.cuda.current_stream(dev).cuda_stream)
+        self._tc_scratch = torch.zeros(lib.sb_psf_tc_scratch_bytes(m, n), dtype=torch.uint8, device=dev)
         self.psf.value = torch.zeros((n, n), dtype=torch.float32, device=dev)
         self.int_psf.value = torch.zeros((n, n), dtype=torch.float32, device=dev)
         self.sr.value = torch.zeros((), dtype=torch.float32, device=dev)
@@ -100,12 +90,10 @@ class PSF(BaseProcessingObj):
         npx = ef.A.numel()
         _lib.call('sb_strehl', ef.A.data_ptr(), ef.phaseInNm.data_ptr(), npx, self._k, self.sr.value.data_ptr(),
                   self._int_sr.data_ptr(), int(self._integrating), self._scratch.data_ptr(), self._scratch.numel(), st)
-        _lib.call('sb_psf_field', ef.A.data_ptr(), ef.phaseInNm.data_ptr(), npx, self._k, self._u.data_ptr(), st)
-        torch.matmul(self._u, self._WT, out=self._G)      # u W^T  (m x n)
-        torch.matmul(self._W, self._G, out=self._F)       # W u W^T (n x n)
-        _lib.call('sb_psf_finish', self._F.data_ptr(), self._F.numel(), self.psf.value.data_ptr(),
-                  self.int_psf.value.data_ptr() if self._integrating else None, self._scratch.data_ptr(),
-                  self._scratch.numel(), st)
+        _lib.call('sb_psf_tc', ef.A.data_ptr(), ef.phaseInNm.data_ptr(), self._m, self._n, self._k,
+                  self._dft.data_ptr(), self.psf.value.data_ptr(),
+                  self.int_psf.value.data_ptr() if self._integrating else None, self._tc_scratch.data_ptr(),
+                  self._tc_scratch.numel(), st)
         if self._integrating:
             torch.div(self._int_sr[0], self._int_sr[1], out=self.int_sr.value)
 

@@ -1,6 +1,7 @@
-"""GPU parity of the PSF object (sb_strehl, sb_psf_field, two DFT products,
-sb_psf_finish) against the reference PSF object's outputs (golden fixtures)
-and the float64 oracle.
+"""GPU parity of the PSF object (sb_strehl, and sb_psf_tc: the two DFT
+products on the tensor cores with split-BF16 operands) against the reference
+PSF object's outputs (golden fixtures) and the float64 oracle, up to the ELT
+field (640 px, nd 8: a 5120 x 5120 PSF).
 
 Tolerances: PSF images max|d|/max|ref| <= 1e-5; Strehl ratios relative
 1e-5 against the reference's float32 run and 1e-6 against float64.
@@ -69,3 +70,29 @@ def test_psf_and_strehl_against_fp64_at_160px_nd8(cuda):
         assert p.psf.value.shape == (1280, 1280)
         assert rel_max_err(p.psf.value.cpu().numpy(), ref) <= PSF_TOL, step
         assert abs(float(p.sr.value) - sr64) <= SR_TOL_FP64 * sr64, step
+
+
+def test_psf_tensor_cores_at_elt_size_against_fp64(cuda):
+    """640 px pupil, nd 8 (5120 x 5120 PSF, the size where the tensor cores
+    carry 450 GFLOP of split-BF16 products): PSF within 1e-5 of the float64
+    oracle, Strehl within 1e-6, two steps integrated; no device timeout."""
+    from specula_b200 import _lib
+    pix, nd, lam = 640, 8, 1650.0
+    A = make_mask(pix, 0.14, 1.0).astype(np.float32)
+    rng = np.random.default_rng(11)
+    p, ef = _psf(A, lam, nd, 0.0)
+    o64 = opsf.PSFOracle(A.shape, lam, nd=nd, precision=0)
+    acc = None
+    for step in range(2):
+        ph = (rng.standard_normal((pix, pix)) * 120.0).astype(np.float32) * A
+        _step(p, ef, ph, step * 1000000)
+        ref, sr64 = o64.step(A, ph, step * 1e-3)
+        got = p.psf.value.cpu().numpy()
+        assert got.shape == (5120, 5120)
+        e = rel_max_err(got, ref)
+        print(f'640 px nd 8 step {step}: PSF {e:.2e} of the peak, SR {float(p.sr.value):.6f} vs {sr64:.6f}')
+        assert e <= PSF_TOL, step
+        assert abs(float(p.sr.value) - sr64) <= SR_TOL_FP64 * sr64, step
+        acc = ref.astype(np.float64) if acc is None else acc + ref
+    assert rel_max_err(p.int_psf.value.cpu().numpy(), acc) <= PSF_TOL
+    _lib.call('sb_device_status')
