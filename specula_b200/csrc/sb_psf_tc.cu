@@ -24,8 +24,9 @@
 // it to the integrated PSF.  M and N are padded to multiples of 128 with
 // zeros.  One CTA of 128 threads per output tile of 128 rows x 128 complex
 // columns: lane 0 of warp 0 issues the copies into a 4-stage ring, lane 0 of
-// warp 1 the MMAs (tensor memory: 256 FP32 columns), all four warps the
-// epilogue.  Every mbarrier wait is bounded; a timeout is recorded in
+// warp 1 the MMAs (tensor memory: 2 x 256 FP32 columns), all four warps the
+// epilogue; the hi*hi products and the hi*lo + lo*hi corrections accumulate
+// in separate tensor-memory regions.  Every mbarrier wait is bounded; a timeout is recorded in
 // g_psf_tc_status (read by sb_device_status) and leaves the outputs unwritten.
 #include "sb_common.cuh"
 #include "sb_umma.cuh"
@@ -39,7 +40,14 @@ constexpr int kStages = 4;
 constexpr int kATile = kTM * kBK * 2;          // bytes of one A_op tile (bf16)
 constexpr int kBTile = kTN * kBK * 2;
 constexpr int kStageBytes = 2 * kATile + 2 * kBTile;    // hi and lo of both operands
-constexpr uint32_t kTmemCols = 256;
+// two accumulators of 256 FP32 columns: hi*hi in columns 0-255, the hi*lo and
+// lo*hi corrections in 256-511.  The tensor cores add each product into the
+// accumulator with a truncating rounding, whose bias grows with the number of
+// additions; keeping the small corrections apart leaves the large sum a third
+// of the additions (measured at the 640 px / nd 8 PSF: 2.0e-5 of the peak with
+// one accumulator), and the two are added with round-to-nearest at the end.
+constexpr uint32_t kTmemCols = 512;
+constexpr uint32_t kCorrCol = 256;
 constexpr int kThreads = 128;
 constexpr int kFieldThreads = 256;
 constexpr int kFieldMaxBlocks = 592;
@@ -238,9 +246,10 @@ __global__ void __launch_bounds__(kThreads, 1) psf_tc_gemm_kernel(GemmArgs a) {
                 const uint64_t dal = sb::umma_desc_kmajor(st + kATile + ks * (2 * kTM * 16), kTM * 16);
                 const uint64_t dbh = sb::umma_desc_kmajor(st + 2 * kATile + ks * (2 * kTN * 16), kTN * 16);
                 const uint64_t dbl = sb::umma_desc_kmajor(st + 2 * kATile + kBTile + ks * (2 * kTN * 16), kTN * 16);
-                sb::umma_bf16(tmem, dah, dbh, IDESC, (kb | ks) != 0 ? 1u : 0u);
-                sb::umma_bf16(tmem, dal, dbh, IDESC, 1u);
-                sb::umma_bf16(tmem, dah, dbl, IDESC, 1u);
+                const uint32_t acc = (kb | ks) != 0 ? 1u : 0u;
+                sb::umma_bf16(tmem, dah, dbh, IDESC, acc);
+                sb::umma_bf16(tmem + kCorrCol, dal, dbh, IDESC, acc);
+                sb::umma_bf16(tmem + kCorrCol, dah, dbl, IDESC, 1u);
             }
             sb::umma_commit(&empty[s]);
         }
@@ -257,11 +266,20 @@ __global__ void __launch_bounds__(kThreads, 1) psf_tc_gemm_kernel(GemmArgs a) {
         const int row = rb * kTM + warp * 32 + lane;     // q (stage 1) or p (stage 2)
 #pragma unroll 1
         for (int c = 0; c < 8; ++c) {
-            uint32_t re[16], im[16];
+            uint32_t re[16], im[16], rc[16], ic[16];
             sb::tmem_ld16(tl + 16 * c, re);
             sb::tmem_ld16(tl + 128 + 16 * c, im);
+            sb::tmem_ld16(tl + kCorrCol + 16 * c, rc);
+            sb::tmem_ld16(tl + kCorrCol + 128 + 16 * c, ic);
             sb::tmem_wait_ld(re);
             sb::tmem_wait_ld(im);
+            sb::tmem_wait_ld(rc);
+            sb::tmem_wait_ld(ic);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                re[j] = __float_as_uint(__fadd_rn(__uint_as_float(re[j]), __uint_as_float(rc[j])));
+                im[j] = __float_as_uint(__fadd_rn(__uint_as_float(im[j]), __uint_as_float(ic[j])));
+            }
             const int col0 = nb * 128 + 16 * c;          // x (stage 1) or q (stage 2)
             if constexpr (STAGE == 1) {
                 // G(x, q) for x = col0 .. col0 + 15 of row q: stage 2's B_op rows Re q and Im q
