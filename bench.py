@@ -62,6 +62,7 @@ def parse():
                         '(for ncu --profile-from-start off) and exit')
     p.add_argument('--batched-only', action='store_true',
                    help='run only the 96-realisation batched Monte-Carlo leg (one GPU)')
+    p.add_argument('--psf-only', action='store_true', help='run only the PSF leg (one GPU)')
     p.add_argument('--adjoint-only', action='store_true',
                    help='run only the adjoint interaction-matrix leg (one GPU) and print its JSON object')
     return p.parse_args()
@@ -630,6 +631,64 @@ def accuracy_vs_fp64(loop, A, phase):
             'targets': {'intensity': 1e-5, 'slopes': 1e-4}}
 
 
+def bench_psf(dev, reps=20):
+    """The PSF object's image on the ELT field (640 px, nd 8: 5120 x 5120)
+    through sb_psf_tc (split-BF16 tcgen05 GEMMs), CUDA events over `reps`
+    calls after warm-up, beside the same two complex products as complex64
+    GEMMs through the library (torch.matmul) for reference."""
+    import torch
+    from specula_b200.processing_objects.psf import PSF
+    from specula_b200.data_objects.electric_field import ElectricField
+    from specula_b200.lib.make_mask import make_mask
+    pix, nd, lam = 640, 8, 1650.0
+    A = torch.as_tensor(make_mask(pix, 0.14, 1.0).astype(np.float32), device=dev)
+    ef = ElectricField(pix, pix, 39.0 / pix, S0=1.0, target_device_idx=dev.index)
+    ef.A.copy_(A)
+    g = torch.Generator(device=dev).manual_seed(5)
+    ef.phaseInNm.copy_(torch.randn((pix, pix), device=dev, generator=g) * 120.0 * A)
+    p = PSF(wavelengthInNm=lam, nd=nd, target_device_idx=dev.index)
+    p.inputs['in_ef'].set(ef)
+    p.setup()
+    n = p._n
+    st = torch.cuda.current_stream(dev)
+
+    def timeit(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / reps
+
+    tc_ms = timeit(p.trigger_code)
+    _lib_status()
+    # the library form of the same two products (complex64), for comparison
+    k = (np.arange(n) - n // 2) % n
+    W = torch.polar(torch.ones((n, pix), dtype=torch.float64),
+                    torch.as_tensor((-2.0 * np.pi / n) * (np.outer(k, np.arange(pix)) % n))).to(torch.complex64).to(dev)
+    WT = W.t().contiguous()
+    u = torch.polar(A, ef.phaseInNm * p._k).to(torch.complex64)
+    G = torch.empty((pix, n), dtype=torch.complex64, device=dev)
+    F = torch.empty((n, n), dtype=torch.complex64, device=dev)
+
+    def lib_products():
+        torch.matmul(u, WT, out=G)
+        torch.matmul(W, G, out=F)
+    lib_ms = timeit(lib_products)
+    mp, np_ = (pix + 127) // 128 * 128, (n + 127) // 128 * 128
+    bf16_flop = 3 * 2 * (np_ * (2 * mp) * (2 * mp) + np_ * (2 * np_) * (2 * mp))
+    return {'workload': 'psf_640px_nd8_5120x5120', 'psf_ms': tc_ms, 'library_complex64_products_ms': lib_ms,
+            'speedup_vs_library_products': lib_ms / tc_ms,
+            'split_bf16_tflops': bf16_flop / (tc_ms / 1e3) / 1e12,
+            'form': 'Strehl reduction + field + two tcgen05 split-BF16 GEMMs (3 launches); the library figure is '
+                    'the two complex64 products alone'}
+
+
 def _lib_status():
     from specula_b200 import _lib
     _lib.call('sb_device_status')
@@ -784,8 +843,10 @@ def run_b200(args):
                                       cpu_budget_s=0 if args.no_cpu_baseline else 10.0)
 
     sh_forms = None
+    psf = None
     if world == 1 and not args.no_batched:
         sh_forms = bench_sh_forms(dev)
+        psf = bench_psf(dev)
 
     batched_mc = None
     if not args.no_batched:
@@ -813,7 +874,7 @@ def run_b200(args):
                                   'achieved_gbs': step_bytes / (ms_max / steps / 1e3) / 1e9,
                                   'frac': step_bytes / (ms_max / steps / 1e3) / 1e9 / peak},
                 'accuracy': accuracy, 'step_pieces': pieces, 'clocks': clk, 'cpu_baseline': cpu, 'adjoint_im': adjoint_im, 'loop_gradient': loop_grad,
-                'sh_forms': sh_forms, 'batched_mc': batched_mc}
+                'sh_forms': sh_forms, 'psf': psf, 'batched_mc': batched_mc}
         print(json.dumps(line), flush=True)
     del loop
     if world > 1:
@@ -952,6 +1013,12 @@ def main():
         dev = torch.device('cuda', 0)
         torch.cuda.set_device(dev)
         print(json.dumps({'loop_gradient': bench_loop_gradient(dev)}), flush=True)
+        return
+    if args.psf_only:
+        import torch
+        dev = torch.device('cuda', 0)
+        torch.cuda.set_device(dev)
+        print(json.dumps({'psf': bench_psf(dev)}), flush=True)
         return
     if args.adjoint_only:
         import torch
