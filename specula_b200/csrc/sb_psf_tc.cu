@@ -22,11 +22,11 @@
 // stage 2's B_op, stage 2's epilogue writes |F|^2 / total with total =
 // N^2 sum |u|^2 (Parseval: the sum of the padded transform's power) and adds
 // it to the integrated PSF.  M and N are padded to multiples of 128 with
-// zeros.  One CTA of 128 threads per output tile of 128 rows x 128 complex
-// columns: lane 0 of warp 0 issues the copies into a 4-stage ring, lane 0 of
-// warp 1 the MMAs (tensor memory: 2 x 256 FP32 columns), all four warps the
-// epilogue; the hi*hi products and the hi*lo + lo*hi corrections accumulate
-// in separate tensor-memory regions.  Every mbarrier wait is bounded; a timeout is recorded in
+// zeros.  One CTA of 128 threads per output tile of 128 rows x 64 complex
+// columns: lane 0 of warp 0 issues the copies into a 6-stage ring, lane 0 of
+// warp 1 the MMAs (tensor memory: 4 x 128 FP32 columns), all four warps the
+// epilogue; the hi*hi products of each third of K and the hi*lo + lo*hi
+// corrections accumulate in separate tensor-memory regions.  Every mbarrier wait is bounded; a timeout is recorded in
 // g_psf_tc_status (read by sb_device_status) and leaves the outputs unwritten.
 #include "sb_common.cuh"
 #include "sb_umma.cuh"
@@ -34,20 +34,22 @@
 namespace {
 
 constexpr int kTM = 128;                       // A_op rows per tile
-constexpr int kTN = 256;                       // B_op rows per tile: 128 complex columns as Re, Im
+constexpr int kTN = 128;                       // B_op rows per tile: kCC complex columns as Re, Im
+constexpr int kCC = kTN / 2;                   // complex columns per tile
 constexpr int kBK = 32;                        // K per stage: two K=16 MMA steps
-constexpr int kStages = 4;
+constexpr int kStages = 6;
 constexpr int kATile = kTM * kBK * 2;          // bytes of one A_op tile (bf16)
 constexpr int kBTile = kTN * kBK * 2;
 constexpr int kStageBytes = 2 * kATile + 2 * kBTile;    // hi and lo of both operands
-// two accumulators of 256 FP32 columns: hi*hi in columns 0-255, the hi*lo and
-// lo*hi corrections in 256-511.  The tensor cores add each product into the
-// accumulator with a truncating rounding, whose bias grows with the number of
-// additions; keeping the small corrections apart leaves the large sum a third
-// of the additions (measured at the 640 px / nd 8 PSF: 2.0e-5 of the peak with
-// one accumulator), and the two are added with round-to-nearest at the end.
-constexpr uint32_t kTmemCols = 512;
-constexpr uint32_t kCorrCol = 256;
+// four accumulators of kTN FP32 columns: the hi*hi products of the first,
+// second and last third of K in regions 0-2, the hi*lo and lo*hi corrections
+// in region 3.  The tensor cores add each product into the accumulator with a
+// truncating rounding whose bias grows with the number of additions into one
+// accumulator (measured at the 640 px / nd 8 PSF: 2.0e-5 of the peak with one
+// accumulator, 9e-6 with the corrections apart); the regions are added with
+// round-to-nearest in the epilogue.
+constexpr int kRegions = 4;
+constexpr uint32_t kTmemCols = kRegions * kTN;
 constexpr int kThreads = 128;
 constexpr int kFieldThreads = 256;
 constexpr int kFieldMaxBlocks = 592;
@@ -130,8 +132,8 @@ __global__ void __launch_bounds__(kFieldThreads) psf_tc_field_kernel(const float
          g += (long long)gridDim.x * blockDim.x) {
         const int row = (int)(g / gpr);
         const int k0 = (int)(g % gpr) * 8;
-        const int x = (row / kTN) * 128 + (row % kTN) % 128;
-        const bool im_row = (row % kTN) >= 128;
+        const int x = (row / kTN) * kCC + (row % kTN) % kCC;
+        const bool im_row = (row % kTN) >= kCC;
         const bool second = k0 >= mp;
         const int y0 = second ? k0 - mp : k0;
         float v[8];
@@ -240,16 +242,18 @@ __global__ void __launch_bounds__(kThreads, 1) psf_tc_gemm_kernel(GemmArgs a) {
             }
             sb::tc_fence_after_sync();
             const unsigned char *st = ring + (size_t)s * kStageBytes;
+            // region of this K block's hi*hi products: thirds of K
+            const int reg = (kb * 3) / KB, reg_first = (reg * KB + 2) / 3;
+            const uint32_t dm = tmem + (uint32_t)(reg * kTN), dc = tmem + (uint32_t)(3 * kTN);
 #pragma unroll
             for (int ks = 0; ks < 2; ++ks) {
                 const uint64_t dah = sb::umma_desc_kmajor(st + ks * (2 * kTM * 16), kTM * 16);
                 const uint64_t dal = sb::umma_desc_kmajor(st + kATile + ks * (2 * kTM * 16), kTM * 16);
                 const uint64_t dbh = sb::umma_desc_kmajor(st + 2 * kATile + ks * (2 * kTN * 16), kTN * 16);
                 const uint64_t dbl = sb::umma_desc_kmajor(st + 2 * kATile + kBTile + ks * (2 * kTN * 16), kTN * 16);
-                const uint32_t acc = (kb | ks) != 0 ? 1u : 0u;
-                sb::umma_bf16(tmem, dah, dbh, IDESC, acc);
-                sb::umma_bf16(tmem + kCorrCol, dal, dbh, IDESC, acc);
-                sb::umma_bf16(tmem + kCorrCol, dah, dbl, IDESC, 1u);
+                sb::umma_bf16(dm, dah, dbh, IDESC, (kb != reg_first || ks != 0) ? 1u : 0u);
+                sb::umma_bf16(dc, dal, dbh, IDESC, (kb | ks) != 0 ? 1u : 0u);
+                sb::umma_bf16(dc, dah, dbl, IDESC, 1u);
             }
             sb::umma_commit(&empty[s]);
         }
@@ -265,25 +269,30 @@ __global__ void __launch_bounds__(kThreads, 1) psf_tc_gemm_kernel(GemmArgs a) {
         const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);
         const int row = rb * kTM + warp * 32 + lane;     // q (stage 1) or p (stage 2)
 #pragma unroll 1
-        for (int c = 0; c < 8; ++c) {
-            uint32_t re[16], im[16], rc[16], ic[16];
+        for (int c = 0; c < kCC / 16; ++c) {
+            // F = ((M0 + M1) + M2) + C, real parts in a region's first kCC columns, imaginary after
+            uint32_t re[16], im[16];
             sb::tmem_ld16(tl + 16 * c, re);
-            sb::tmem_ld16(tl + 128 + 16 * c, im);
-            sb::tmem_ld16(tl + kCorrCol + 16 * c, rc);
-            sb::tmem_ld16(tl + kCorrCol + 128 + 16 * c, ic);
+            sb::tmem_ld16(tl + kCC + 16 * c, im);
             sb::tmem_wait_ld(re);
             sb::tmem_wait_ld(im);
-            sb::tmem_wait_ld(rc);
-            sb::tmem_wait_ld(ic);
+#pragma unroll 1
+            for (int r = 1; r < kRegions; ++r) {
+                uint32_t rr[16], ri[16];
+                sb::tmem_ld16(tl + r * kTN + 16 * c, rr);
+                sb::tmem_ld16(tl + r * kTN + kCC + 16 * c, ri);
+                sb::tmem_wait_ld(rr);
+                sb::tmem_wait_ld(ri);
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                re[j] = __float_as_uint(__fadd_rn(__uint_as_float(re[j]), __uint_as_float(rc[j])));
-                im[j] = __float_as_uint(__fadd_rn(__uint_as_float(im[j]), __uint_as_float(ic[j])));
+                for (int j = 0; j < 16; ++j) {
+                    re[j] = __float_as_uint(__fadd_rn(__uint_as_float(re[j]), __uint_as_float(rr[j])));
+                    im[j] = __float_as_uint(__fadd_rn(__uint_as_float(im[j]), __uint_as_float(ri[j])));
+                }
             }
-            const int col0 = nb * 128 + 16 * c;          // x (stage 1) or q (stage 2)
+            const int col0 = nb * kCC + 16 * c;          // x (stage 1) or q (stage 2)
             if constexpr (STAGE == 1) {
                 // G(x, q) for x = col0 .. col0 + 15 of row q: stage 2's B_op rows Re q and Im q
-                const int n_re = (row / 128) * kTN + row % 128, n_im = n_re + 128;
+                const int n_re = (row / kCC) * kTN + row % kCC, n_im = n_re + kCC;
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
                     float gr[8], gi[8], ngi[8];
@@ -430,7 +439,7 @@ extern "C" int sb_psf_tc(const float *A, const float *phase_nm, int m, int n, fl
     g.g_hi = b2_hi;
     g.g_lo = b2_lo;
     g.g_kblocks = kblocks;
-    psf_tc_gemm_kernel<1><<<dim3(mp / 128, np_ / kTM), kThreads, kGemmSmem, st>>>(g);
+    psf_tc_gemm_kernel<1><<<dim3(mp / kCC, np_ / kTM), kThreads, kGemmSmem, st>>>(g);
     rc = sb::check_launch("psf_tc_gemm_kernel<1>");
     if (rc) return rc;
     // stage 2: F = W G, |F|^2 / total into the PSF (and the integrated PSF)
@@ -440,6 +449,6 @@ extern "C" int sb_psf_tc(const float *A, const float *phase_nm, int m, int n, fl
     g.psf = psf;
     g.int_psf = int_psf;
     g.total = total;
-    psf_tc_gemm_kernel<2><<<dim3(np_ / 128, np_ / kTM), kThreads, kGemmSmem, st>>>(g);
+    psf_tc_gemm_kernel<2><<<dim3(np_ / kCC, np_ / kTM), kThreads, kGemmSmem, st>>>(g);
     return sb::check_launch("psf_tc_gemm_kernel<2>");
 }
