@@ -209,8 +209,10 @@ __global__ void __launch_bounds__(kThreads, 1) psf_tc_gemm_kernel(GemmArgs a) {
     const uint32_t tmem = *tmem_slot;
     const int KB = a.kblocks;
     if (tid == 0) {
-        // producer: four contiguous copies per stage
-        const uint64_t pol = sb::l2_evict_first_policy();
+        // producer: four contiguous copies per stage; every tile is read by many
+        // CTAs (the DFT operand by all of a stage, B_op by a column of them), so
+        // its lines are kept in L2
+        const uint64_t pol = sb::l2_evict_last_policy();
         const unsigned char *ah = a.a_hi + (size_t)rb * KB * kATile, *al = a.a_lo + (size_t)rb * KB * kATile;
         const unsigned char *bh = a.b_hi + (size_t)nb * KB * kBTile, *bl = a.b_lo + (size_t)nb * KB * kBTile;
         int kb = 0;

@@ -97,6 +97,13 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, i
         : "memory");
 }
 
+// L2 policy for data read by many CTAs (lines kept over streamed data)
+__device__ __forceinline__ uint64_t l2_evict_last_policy() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
 // 1-D bulk copy (no tensor map) of `bytes` contiguous bytes from this GPU's
 // global memory into this CTA's shared memory, completing on `bar`.  Both
 // addresses 16-byte aligned, `bytes` a multiple of 16.
