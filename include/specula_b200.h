@@ -198,6 +198,18 @@ typedef struct sb_ccd_params {
     uint64_t photon_seed;
     uint64_t readout_seed;
     sb_ccd_state *state;    /* device pointer; advanced by the kernel itself  */
+    /* detector-structure options (ccd.py:223-245), in the reference's order
+     * around the photon and read-out noise; all zero / NULL: off */
+    int cic_noise;          /* + Bernoulli(cic_level) electrons before the photon noise */
+    float cic_level;
+    int excess_noise;       /* EMCCD after the photon noise: n -> Gamma(delta n,
+                             * emccd_gain) / delta, then / emccd_gain after ADU */
+    float excess_delta;
+    float emccd_gain;
+    uint64_t excess_seed;
+    const float *pixel_gains;  /* per-pixel gains after the read-out noise */
+    const float *qe_map;       /* per-pixel QE applied with qe (notUniformQe) */
+    int qe_map_normalise;      /* divide by qe_map after the noise */
 } sb_ccd_params;
 
 /* One loop step: integrate; when the frame closes, read it out into
@@ -216,6 +228,15 @@ int sb_ccd_step(const sb_ccd_params *p, const float *intensity, float *integrate
 size_t sb_ccd_binned_scratch_bytes(int rows, int cols, int binning);
 int sb_ccd_step_binned(const sb_ccd_params *p, int rows, int cols, int binning, const float *intensity,
                        float *integrated, float *pixels, void *scratch, size_t scratch_bytes, void *stream);
+
+/* CCD step with charge-transfer inefficiency (ccd.py:223-224): on a
+ * read-out step the frame after QE and background becomes cte0 * frame *
+ * cte1 (row-major side x side matrices, FP32 products) before the noise and
+ * the ADU model of sb_ccd_step; no binning.  scratch:
+ * sb_ccd_cte_scratch_bytes(side) bytes. */
+size_t sb_ccd_cte_scratch_bytes(int side);
+int sb_ccd_step_cte(const sb_ccd_params *p, int side, const float *cte0, const float *cte1, const float *intensity,
+                    float *integrated, float *pixels, void *scratch, size_t scratch_bytes, void *stream);
 
 /* Batched CCD step: n_batch frames of p->n_pixels each, contiguous in
  * intensity / integrated / pixels; frame b draws its noise with

@@ -2,8 +2,10 @@
 
 Restates specula/processing_objects/ccd.py:198-287 (integration, binning,
 QE, background/dark, Poisson photon noise, Gaussian readout noise, ADU
-quantisation).  Excess (EMCCD), CIC and CTE noise are not on the SCAO SH
-step and are not restated.
+quantisation), and the deterministic detector-structure options: the
+charge-transfer matrices (ccd.py:223-224), pixel gains (:239-240) and the
+per-pixel QE map with its normalisation (:242-245, 285-287).  The random
+EMCCD (excess) and CIC draws are checked by their statistics instead.
 
 Binning follows the reference's intended arithmetic (ccd.py:264-280: b x b
 block sums of the full-resolution integrated frame, scaled by
@@ -23,7 +25,7 @@ class CCDOracle:
                  readout_noise=False, background_noise=False, darkcurrent_noise=False,
                  readout_level=0.0, background_level=0.0, darkcurrent_level=0.0,
                  quantum_eff=1.0, photon_seed=1, readout_seed=2, ADU_gain=8, ADU_bias=400,
-                 precision=1):
+                 precision=1, cte_mat=None, pixel_gains=None, qe_map=None, qe_map_normalise=False):
         self.dtype = np.float32 if precision == 1 else np.float64
         self.size = (size[0] // binning, size[1] // binning)
         self.binning = binning
@@ -43,6 +45,10 @@ class CCDOracle:
         self.bias = ADU_bias
         self.photon_rng = np.random.default_rng(photon_seed)
         self.readout_rng = np.random.default_rng(readout_seed)
+        self.cte_mat = None if cte_mat is None else np.asarray(cte_mat, dtype=self.dtype)
+        self.pixel_gains = None if pixel_gains is None else np.asarray(pixel_gains, dtype=self.dtype)
+        self.qe_map = None if qe_map is None else np.asarray(qe_map, dtype=self.dtype)
+        self.qe_map_normalise = qe_map_normalise
 
     def step(self, intensity):
         """One loop step; returns the frame when a read-out happens, else None
@@ -54,6 +60,8 @@ class CCDOracle:
         frame = self._binning()
         if self.qe != 1:
             frame = frame * self.qe
+        if self.qe_map is not None:
+            frame = frame * self.qe_map
         frame = self._noise(frame)
         self.integrated *= 0.0
         return frame
@@ -72,11 +80,17 @@ class CCDOracle:
         # ccd.py:218-262
         if self.background_noise or self.darkcurrent_noise:
             f += (self.background_level + self.darkcurrent_level)
+        if self.cte_mat is not None:
+            f = np.dot(np.dot(self.cte_mat[:, :, 0], f), self.cte_mat[:, :, 1])
         if self.photon_noise:
             f = self.photon_rng.poisson(f)                      # int64 from here on
         if self.readout_noise:
             ron = self.readout_rng.standard_normal(size=f.size)
             f += (ron.reshape(f.shape) * self.readout_level).astype(f.dtype)
+        if self.pixel_gains is not None:
+            f *= self.pixel_gains
+        if self.qe_map is not None and self.qe_map_normalise:
+            f *= 1 / self.qe_map
         if self.photon_noise:
             f = np.round(f * self.gain) + self.bias
             np.maximum(f, 0, out=f)                             # clamp < 0 -> 0, in place

@@ -41,7 +41,10 @@ class CcdParams(C.Structure):
                 ('bg_plus_dark', C.c_float), ('photon_noise', C.c_int), ('readout_noise', C.c_int),
                 ('readout_level', C.c_float), ('adu_gain', C.c_float), ('adu_bias', C.c_float),
                 ('dark_level', C.c_float), ('dark_noise', C.c_int), ('photon_seed', C.c_uint64),
-                ('readout_seed', C.c_uint64), ('state', vp)]
+                ('readout_seed', C.c_uint64), ('state', vp),
+                ('cic_noise', C.c_int), ('cic_level', C.c_float), ('excess_noise', C.c_int),
+                ('excess_delta', C.c_float), ('emccd_gain', C.c_float), ('excess_seed', C.c_uint64),
+                ('pixel_gains', fp), ('qe_map', fp), ('qe_map_normalise', C.c_int)]
 
 
 class SlopecPlan(C.Structure):
@@ -87,6 +90,8 @@ SIGNATURES = {
     'sb_edge_extrapolate': (C.c_int, [fp, ip, ip, C.c_int, fp, vp]),
     'sb_interp2d_field': (C.c_int, [fp, fp, C.c_int, C.c_int, fp, fp, C.c_int, fp, fp, vp]),
     'sb_ccd_step': (C.c_int, [C.POINTER(CcdParams), fp, fp, fp, vp]),
+    'sb_ccd_cte_scratch_bytes': (C.c_size_t, [C.c_int]),
+    'sb_ccd_step_cte': (C.c_int, [C.POINTER(CcdParams), C.c_int, fp, fp, fp, fp, fp, vp, C.c_size_t, vp]),
     'sb_philox_raw': (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, vp, vp]),
     'sb_slopec_scratch_bytes': (C.c_size_t, [C.POINTER(SlopecPlan)]),
     'sb_slopec': (C.c_int, [C.POINTER(SlopecPlan), fp, fp, fp, vp, C.c_size_t, vp]),

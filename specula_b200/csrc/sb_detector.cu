@@ -52,6 +52,8 @@ __device__ __forceinline__ float u01f(uint32_t a) { return ((float)(a >> 8) + 0.
 
 constexpr uint32_t kPhotonTag = 0x50484f54u;   // "PHOT"
 constexpr uint32_t kReadoutTag = 0x52454144u;  // "READ"
+constexpr uint32_t kCicTag = 0x4349434eu;      // "CICN"
+constexpr uint32_t kExcessTag = 0x45584353u;   // "EXCS"
 
 // log(k!) for k < 32 (math.lgamma(k + 1) rounded to float)
 __constant__ float c_logfact[32] = {0.0f, 0.0f, 0.693147181f, 1.79175947f, 3.17805383f, 4.78749174f, 6.57925121f, 8.52516136f, 10.6046029f, 12.8018275f, 15.1044126f, 17.5023078f, 19.9872145f, 22.5521639f, 25.1912212f, 27.8992714f, 30.6718601f, 33.5050735f, 36.3954452f, 39.3398842f, 42.3356165f, 45.3801389f, 48.4711814f, 51.6066756f, 54.7847294f, 58.0036052f, 61.2617018f, 64.5575386f, 67.8897431f, 71.257039f, 74.6582363f, 78.0922236f};
@@ -110,6 +112,47 @@ __device__ float poisson_sample(float lam, uint32_t e, uint64_t frame, uint64_t 
     return floorf(lam + 0.5f);
 }
 
+// Gamma(shape, 1) by Marsaglia and Tsang's squeeze-and-reject method
+// ("A simple method for generating gamma variables", ACM TOMS 26, 2000):
+// d = shape - 1/3, c = 1/sqrt(9 d), v = (1 + c x)^3 for x ~ N(0,1), accepted
+// with u ~ U(0,1) when u < 1 - 0.0331 x^4 or log u < x^2/2 + d (1 - v + log v);
+// shapes below 1 as Gamma(shape + 1) u^(1/shape).  Draws from the excess
+// stream of pixel e in frame f; at most 32 tries (acceptance per try > 0.95).
+__device__ float gamma_sample(float shape, uint32_t e, uint64_t frame, uint64_t seed) {
+    if (!(shape > 0.0f)) return 0.0f;
+    const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32) ^ kExcessTag;
+    const bool boost = shape < 1.0f;
+    const float a = boost ? shape + 1.0f : shape;
+    const float d = a - 1.0f / 3.0f, c = rsqrtf(9.0f * d);
+    float g = d;
+    uint32_t it = 0;
+    for (; it < 32; ++it) {
+        const u4 r = philox4x32_10({e, (uint32_t)frame, (uint32_t)(frame >> 32), 16u + it}, k0, k1);
+        const float x = sqrtf(-2.0f * __logf(u01f(r.x))) * cospif(2.0f * u01f(r.y));
+        float v = fmaf(c, x, 1.0f);
+        if (v <= 0.0f) continue;
+        v = v * v * v;
+        const float u = u01f(r.z);
+        const float x2 = x * x;
+        if (u < 1.0f - 0.0331f * x2 * x2 || __logf(u) < 0.5f * x2 + d * (1.0f - v + __logf(v))) {
+            g = d * v;
+            break;
+        }
+    }
+    if (boost) {
+        const u4 r = philox4x32_10({e, (uint32_t)frame, (uint32_t)(frame >> 32), 15u}, k0, k1);
+        g *= __powf(u01f(r.w), 1.0f / shape);
+    }
+    return g;
+}
+
+// Bernoulli(p) electron of clock-induced charge
+__device__ __forceinline__ float cic_sample(float p, uint32_t e, uint64_t frame, uint64_t seed) {
+    const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32) ^ kCicTag;
+    const u4 r = philox4x32_10({e, (uint32_t)frame, (uint32_t)(frame >> 32), 0u}, k0, k1);
+    return u01f(r.x) < p ? 1.0f : 0.0f;
+}
+
 // N(0,1) by Box-Muller from one Philox block
 __device__ __forceinline__ float std_normal(uint32_t e, uint64_t frame, uint64_t seed) {
     const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32) ^ kReadoutTag;
@@ -140,21 +183,41 @@ __device__ __forceinline__ float ccd_sample(const sb_ccd_params &p, float f, int
         pseed = photon_seeds[b];
         rseed = readout_seeds[b];
     }
+    if (p.cic_noise) f = __fadd_rn(f, cic_sample(p.cic_level, eloc, frame, pseed));       // ccd.py:226-227
+    const bool excess = p.excess_noise != 0;
     if (p.photon_noise) {
         double v = poisson_sample(f, eloc, frame, pseed, logfact);
-        if (p.readout_noise) v += truncf(std_normal(eloc, frame, rseed) * p.readout_level);
-        // ADU: round(x*g)+bias, clamp at 0, -bias, /g, back to the integer
-        // dtype of the Poisson draw (ccd.py:247-258)
+        // EMCCD multiplication (ccd.py:232-233); the frame stays an integer
+        // array (truncating read-out noise and ADU division) only without it
+        if (excess) v = (double)gamma_sample((float)(p.excess_delta * v), eloc, frame, p.excess_seed) *
+                        (double)p.emccd_gain / (double)p.excess_delta;
+        if (p.readout_noise) {
+            const double ron = (double)(std_normal(eloc, frame, rseed) * p.readout_level);
+            v += excess ? ron : trunc(ron);
+        }
+        // float frames only (the host rejects gains on the integer frame)
+        if (p.pixel_gains) v *= (double)p.pixel_gains[eloc];                                  // ccd.py:239-240
+        if (p.qe_map && p.qe_map_normalise) v *= 1.0 / (double)p.qe_map[eloc];                 // ccd.py:242-245
+        // ADU: round(x*g)+bias, clamp at 0, -bias, /g (ccd.py:247-258)
         double x = rint(v * (double)p.adu_gain) + (double)p.adu_bias;
         x = x < 0.0 ? 0.0 : x;
         x -= (double)p.adu_bias;
         // a power-of-two gain (the default 8) divides exactly by its
         // reciprocal; any other gain takes the float64 division
-        x = trunc(gain_pow2 ? x * inv_gain : x / (double)p.adu_gain);
+        x = gain_pow2 ? x * inv_gain : x / (double)p.adu_gain;
+        if (excess)
+            x /= (double)p.emccd_gain;
+        else
+            x = trunc(x);
         if (p.dark_noise) x -= (double)p.dark_level;
         return (float)x;
     }
+    if (excess)
+        f = (float)((double)gamma_sample(__fmul_rn(p.excess_delta, f), eloc, frame, p.excess_seed) *
+                    (double)p.emccd_gain / (double)p.excess_delta);
     if (p.readout_noise) f = __fadd_rn(f, __fmul_rn(std_normal(eloc, frame, rseed), p.readout_level));
+    if (p.pixel_gains) f = __fmul_rn(f, p.pixel_gains[eloc]);
+    if (p.qe_map && p.qe_map_normalise) f = __fmul_rn(f, 1.0f / p.qe_map[eloc]);
     return f;
 }
 
@@ -192,6 +255,7 @@ __global__ void __launch_bounds__(kCcdThreads, 4) ccd_kernel(sb_ccd_params p, co
             } else {
                 f = acc;
                 if (p.qe != 1.0f) f = __fmul_rn(f, p.qe);                  // ccd.py:282-287
+                if (p.qe_map) f = __fmul_rn(f, p.qe_map[photon_seeds ? e % n_per : e]);
                 f = __fadd_rn(f, p.bg_plus_dark);                           // ccd.py:220-221
             }
         }
@@ -323,6 +387,7 @@ __global__ void __launch_bounds__(kCcdThreads) ccd_bin_noise_kernel(sb_ccd_param
         for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_out; e += gridDim.x * blockDim.x) {
             float f = __fmul_rn(__fmul_rn(binned[e], b2), ratio);
             if (p.qe != 1.0f) f = __fmul_rn(f, p.qe);                        // ccd.py:282-287
+            if (p.qe_map) f = __fmul_rn(f, p.qe_map[e]);
             f = __fadd_rn(f, p.bg_plus_dark);                                 // ccd.py:220-221
             pix[e] = ccd_sample(p, f, e, frame, nullptr, nullptr, n_out, logfact, inv_gain, gain_pow2);
         }
@@ -337,6 +402,82 @@ __global__ void __launch_bounds__(kCcdThreads) ccd_bin_noise_kernel(sb_ccd_param
             if (atomicAdd(&p.state->blocks_done, 1u) == gridDim.x - 1) {
                 vs->n_integrated = readout ? 0 : nint;
                 if (readout) vs->frame_index = frame + 1;
+                vs->blocks_done = 0u;
+                __threadfence();
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Charge-transfer inefficiency (ccd.py:223-224): on a read-out step the frame
+// after QE and background goes through M0 * frame * M1 before the noise.
+// Four launches, each gated on the device frame state: the pre-noise frame,
+// the two products (16 x 16 shared-memory tiles, FP32), the noise.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) ccd_cte_frame_kernel(sb_ccd_params p, const float *__restrict__ in,
+                                                            float *__restrict__ integ, float *__restrict__ frame) {
+    volatile sb_ccd_state *vs = p.state;
+    const bool readout = vs->n_integrated + 1 >= p.frames_per_read;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < p.n_pixels; e += gridDim.x * blockDim.x) {
+        const float acc = __fadd_rn(integ[e], __fmul_rn(in[e], p.rate));        // ccd.py:205
+        if (!readout) {
+            integ[e] = acc;
+            continue;
+        }
+        float f = acc;
+        if (p.qe != 1.0f) f = __fmul_rn(f, p.qe);                              // ccd.py:282-287
+        if (p.qe_map) f = __fmul_rn(f, p.qe_map[e]);
+        frame[e] = __fadd_rn(f, p.bg_plus_dark);                                // ccd.py:220-221
+        integ[e] = 0.0f;                                                        // ccd.py:216
+    }
+}
+
+// C (m x n) = A (m x k) * B (k x n), row-major, on read-out steps only
+__global__ void __launch_bounds__(256) ccd_cte_matmul_kernel(sb_ccd_params p, const float *__restrict__ A,
+                                                             const float *__restrict__ B, float *__restrict__ Cm,
+                                                             int m, int n, int k) {
+    __shared__ float As[16][17], Bs[16][17];
+    volatile sb_ccd_state *vs = p.state;
+    if (vs->n_integrated + 1 < p.frames_per_read) return;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int row = blockIdx.y * 16 + ty, col = blockIdx.x * 16 + tx;
+    float acc = 0.f;
+    for (int k0 = 0; k0 < k; k0 += 16) {
+        As[ty][tx] = (row < m && k0 + tx < k) ? A[(size_t)row * k + k0 + tx] : 0.f;
+        Bs[ty][tx] = (k0 + ty < k && col < n) ? B[(size_t)(k0 + ty) * n + col] : 0.f;
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < 16; ++j) acc = fmaf(As[ty][j], Bs[j][tx], acc);
+        __syncthreads();
+    }
+    if (row < m && col < n) Cm[(size_t)row * n + col] = acc;
+}
+
+__global__ void __launch_bounds__(kCcdThreads) ccd_cte_noise_kernel(sb_ccd_params p, const float *__restrict__ frame,
+                                                                    float *__restrict__ pix) {
+    volatile sb_ccd_state *vs = p.state;
+    __shared__ float logfact[32];
+    __shared__ unsigned int warps_done;
+    if (threadIdx.x == 0) warps_done = 0u;
+    if (threadIdx.x < 32) logfact[threadIdx.x] = c_logfact[threadIdx.x];
+    const uint64_t frame_idx = vs->frame_index;
+    const int nint = vs->n_integrated + 1;
+    const bool readout = nint >= p.frames_per_read;
+    const double inv_gain = 1.0 / (double)p.adu_gain;
+    const bool gain_pow2 = (__double_as_longlong((double)p.adu_gain) & 0x000FFFFFFFFFFFFFLL) == 0;
+    __syncthreads();
+    if (readout)
+        for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < p.n_pixels; e += gridDim.x * blockDim.x)
+            pix[e] = ccd_sample(p, frame[e], e, frame_idx, nullptr, nullptr, p.n_pixels, logfact, inv_gain, gain_pow2);
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) {
+        const unsigned int nwarps = (blockDim.x + 31) >> 5;
+        if (atomicAdd(&warps_done, 1u) == nwarps - 1) {
+            __threadfence();
+            if (atomicAdd(&p.state->blocks_done, 1u) == gridDim.x - 1) {
+                vs->n_integrated = readout ? 0 : nint;
+                if (readout) vs->frame_index = frame_idx + 1;
                 vs->blocks_done = 0u;
                 __threadfence();
             }
@@ -520,6 +661,7 @@ __global__ void __launch_bounds__(kChainMaxThreads) sh_ccd_slopec_kernel(ChainAr
             a.I[e] = v;
             f = __fadd_rn(a.integ[e], __fmul_rn(v, p.rate));           // ccd.py:205
             if (p.qe != 1.0f) f = __fmul_rn(f, p.qe);                  // ccd.py:282-287
+            if (p.qe_map) f = __fmul_rn(f, p.qe_map[e]);
             f = __fadd_rn(f, p.bg_plus_dark);                           // ccd.py:220-221
         }
         int qi = valid ? q : -1;
@@ -837,4 +979,40 @@ extern "C" int sb_sh_ccd_slopec(const sb_sh_plan *sh, int dft_mode, const float 
     const dim3 grid((n + kChainLenses - 1) / kChainLenses, n);
     sh_ccd_slopec_kernel<<<grid, chain_threads(npx), 0, sb::as_stream(stream)>>>(a);
     return sb::check_launch("sh_ccd_slopec_kernel");
+}
+
+extern "C" size_t sb_ccd_cte_scratch_bytes(int side) {
+    if (side < 1) return 0;
+    return 2 * (((size_t)side * side * sizeof(float) + 255) & ~(size_t)255);
+}
+
+extern "C" int sb_ccd_step_cte(const sb_ccd_params *p, int side, const float *cte0, const float *cte1,
+                               const float *intensity, float *integrated, float *pixels, void *scratch,
+                               size_t scratch_bytes, void *stream) {
+    sb::clear_error();
+    if (!p || !p->state || !cte0 || !cte1 || !intensity || !integrated || !pixels)
+        return sb::fail(SB_EINVAL, "sb_ccd_step_cte: null pointer");
+    if (side < 1 || p->n_pixels != side * side || p->frames_per_read < 1)
+        return sb::fail(SB_EINVAL, "sb_ccd_step_cte: a square frame of side x side pixels is needed");
+    if (p->photon_noise && !(p->adu_gain > 0.f)) return sb::fail(SB_EINVAL, "sb_ccd_step_cte: ADU gain must be > 0");
+    const size_t need = sb_ccd_cte_scratch_bytes(side);
+    if (!scratch || scratch_bytes < need)
+        return sb::fail(SB_ESCRATCH, "sb_ccd_step_cte: scratch needs %zu bytes", need);
+    float *f0 = static_cast<float *>(scratch);
+    float *f1 = reinterpret_cast<float *>(static_cast<char *>(scratch) + need / 2);
+    cudaStream_t st = sb::as_stream(stream);
+    int nb = (p->n_pixels + 255) / 256;
+    nb = nb > 1184 ? 1184 : nb;
+    ccd_cte_frame_kernel<<<nb, 256, 0, st>>>(*p, intensity, integrated, f0);
+    int rc = sb::check_launch("ccd_cte_frame_kernel");
+    if (rc) return rc;
+    const dim3 g((side + 15) / 16, (side + 15) / 16);
+    ccd_cte_matmul_kernel<<<g, 256, 0, st>>>(*p, cte0, f0, f1, side, side, side);     // M0 * frame
+    rc = sb::check_launch("ccd_cte_matmul_kernel");
+    if (rc) return rc;
+    ccd_cte_matmul_kernel<<<g, 256, 0, st>>>(*p, f1, cte1, f0, side, side, side);     // ... * M1
+    rc = sb::check_launch("ccd_cte_matmul_kernel");
+    if (rc) return rc;
+    ccd_cte_noise_kernel<<<nb, kCcdThreads, 0, st>>>(*p, f0, pixels);
+    return sb::check_launch("ccd_cte_noise_kernel");
 }

@@ -10,8 +10,13 @@ pixel) instead of NumPy's PCG64 / CuPy's XORWOW, so draws are deterministic
 and independent of launch shape; the reference's own CPU and GPU streams
 already differ from each other, so only the distributions are shared.  The
 frame counter lives on the device, so the object can be replayed from a CUDA
-graph.  Not on this path (raise NotImplementedError): excess (EMCCD), CIC and
-CTE noise, pixel gains, start_time > 0, 'auto' noise levels.  Binning (b x b)
+graph.  EMCCD excess noise (a Gamma draw of shape excess_delta * n and scale
+emccd_gain, Marsaglia-Tsang), clock-induced charge (a Bernoulli electron),
+charge-transfer inefficiency (sb_ccd_step_cte: cte0 * frame * cte1 before the
+noise), pixel gains (constructor or setQuadrantGains) and a per-pixel QE map
+(the reference's notUniformQe attributes) follow ccd.py:218-262 in its order.
+Not on this path (raise NotImplementedError): start_time > 0, 'auto' noise
+levels.  Binning (b x b)
 runs as sb_ccd_step_binned: block sums scaled as the reference does
 (ccd.py:262-280), then the same QE / noise / ADU model on the binned pixels.
 """
@@ -64,12 +69,27 @@ class CCD(BaseProcessingObj):
         if self._dt % self.loop_dt != 0:
             raise ValueError(f'integration time dt={dt} must be a multiple of the basic simulation '
                              f'time_step={simul_params.time_step}')
-        for flag, what in ((excess_noise, 'excess (EMCCD) noise'), (cic_noise, 'CIC noise'),
-                           (cte_noise, 'CTE noise'),
-                           (pixelGains is not None, 'pixel gains'), (start_time != 0, 'start_time > 0'),
+        for flag, what in ((start_time != 0, 'start_time > 0'),
                            ('auto' in (readout_level, darkcurrent_level, background_level), "'auto' levels")):
             if flag:
                 raise NotImplementedError(f'CCD: {what} is not on the specula_b200 path')
+        if excess_noise:
+            # the reference sets the EMCCD and ADU gains itself when excess noise is on (ccd.py:100-103)
+            emccd_gain = 400
+            ADU_gain = 1 / 20
+        self._excess_noise = bool(excess_noise)
+        self._excess_seed = int(excess_seed)
+        self._excess_delta = float(excess_delta)
+        self._emccd_gain = float(emccd_gain)
+        self._cic_noise = bool(cic_noise)
+        self._cic_level = float(cic_level)
+        self._cte_noise = bool(cte_noise)
+        self._cte_mat = cte_mat
+        self._pixelGains = pixelGains
+        # per-pixel QE (the reference's notUniformQe attributes, set by the user)
+        self._notUniformQe = False
+        self._notUniformQeMatrix = None
+        self._normNotUniformQe = False
         self._photon_noise = bool(photon_noise)
         self._readout_noise = bool(readout_noise)
         self._darkcurrent_noise = bool(darkcurrent_noise)
@@ -97,6 +117,18 @@ class CCD(BaseProcessingObj):
     def dt(self):
         return self._dt
 
+    def setQuadrantGains(self, quadrantsGains):
+        """Pixel gains constant over the four quadrants of the frame, in the
+        reference's quadrant order (ccd.py:289-296)."""
+        import numpy as np
+        rows, cols = self._pixels.size
+        g = np.zeros((rows, cols), dtype=np.float32)
+        for i in range(2):
+            for j in range(2):
+                g[(rows // self._binning // 2) * i:(rows // self._binning // 2) * (i + 1),
+                  (cols // self._binning // 2) * j:(cols // self._binning // 2) * (j + 1)] = quadrantsGains[j * 2 + i]
+        self._pixelGains = g
+
     @property
     def size(self):
         return self._pixels.size
@@ -123,7 +155,38 @@ class CCD(BaseProcessingObj):
             photon_noise=int(self._photon_noise), readout_noise=int(self._readout_noise),
             readout_level=self._readout_level, adu_gain=float(self._ADU_gain), adu_bias=float(self._ADU_bias),
             dark_level=self._darkcurrent_level, dark_noise=int(self._darkcurrent_noise),
-            photon_seed=self._photon_seed, readout_seed=self._readout_seed, state=self._state.data_ptr())
+            photon_seed=self._photon_seed, readout_seed=self._readout_seed, state=self._state.data_ptr(),
+            cic_noise=int(self._cic_noise), cic_level=self._cic_level, excess_noise=int(self._excess_noise),
+            excess_delta=self._excess_delta, emccd_gain=self._emccd_gain, excess_seed=self._excess_seed)
+        rows, cols = self._pixels.size
+        int_frame = self._photon_noise and not self._excess_noise
+        self._gains_t = None
+        if self._pixelGains is not None:
+            if int_frame:
+                raise ValueError('CCD: pixel gains multiply a float frame; with photon noise and no excess noise '
+                                 "the reference's frame is an integer array (ccd.py:239-240)")
+            self._gains_t = self._device_map(self._pixelGains, rows, cols, 'pixelGains')
+            self._params.pixel_gains = self._gains_t.data_ptr()
+        self._qe_t = None
+        if self._notUniformQe:
+            if self._normNotUniformQe and int_frame:
+                raise ValueError('CCD: the QE-map normalisation multiplies a float frame; with photon noise and no '
+                                 "excess noise the reference's frame is an integer array (ccd.py:242-245)")
+            self._qe_t = self._device_map(self._notUniformQeMatrix, rows, cols, 'notUniformQeMatrix')
+            self._params.qe_map = self._qe_t.data_ptr()
+            self._params.qe_map_normalise = int(bool(self._normNotUniformQe))
+        self._cte = None
+        if self._cte_noise:
+            if self._binning != 1 or rows != cols:
+                raise NotImplementedError('CCD: CTE noise needs a square frame without binning (ccd.py:223-224)')
+            import numpy as np
+            m = np.zeros((rows, cols, 2), dtype=np.float32) if self._cte_mat is None else np.asarray(self._cte_mat)
+            if m.shape != (rows, cols, 2):
+                raise ValueError(f'CCD: cte_mat of shape {m.shape} for a {rows} x {cols} frame')
+            self._cte = (self._tensor(np.ascontiguousarray(m[:, :, 0])).contiguous(),
+                         self._tensor(np.ascontiguousarray(m[:, :, 1])).contiguous())
+            nb = _lib.load().sb_ccd_cte_scratch_bytes(rows)
+            self._cte_scratch = torch.zeros(nb, dtype=torch.uint8, device=self.device)
         self._in_i = in_i
         self._bin_scratch = None
         if self._binning > 1:
@@ -133,7 +196,19 @@ class CCD(BaseProcessingObj):
                 raise ValueError('Warning: binning requested not applied')
             self._bin_scratch = torch.zeros(nb, dtype=torch.uint8, device=self.device)
 
+    def _device_map(self, a, rows, cols, name):
+        t = self._tensor(a).reshape(-1).contiguous()
+        if t.numel() != rows * cols:
+            raise ValueError(f'CCD: {name} must hold {rows} x {cols} values')
+        return t
+
     def trigger_code(self):
+        if self._cte is not None:
+            rows = self._pixels.size[0]
+            _lib.call('sb_ccd_step_cte', _byref(self._params), rows, self._cte[0].data_ptr(), self._cte[1].data_ptr(),
+                      self._in_i.i.data_ptr(), self._integrated_i.i.data_ptr(), self._pixels.pixels.data_ptr(),
+                      self._cte_scratch.data_ptr(), self._cte_scratch.numel(), self.stream_handle())
+            return
         if self._bin_scratch is not None:
             rows, cols = self._integrated_i.size
             _lib.call('sb_ccd_step_binned', _byref(self._params), rows, cols, self._binning, self._in_i.i.data_ptr(),

@@ -430,7 +430,7 @@ class ScaoLoop:
         sh, ccd, sl = self.sh, self.ccd, self.slopec
         return (not sh.geometry.do_interpolation and sh._kernelobj is None and
                 sh._forward in ('sb_sh_forward', 'sb_sh_forward_split_bf16') and
-                ccd._bin_scratch is None and int(ccd._frames_per_read) == 1 and
+                ccd._bin_scratch is None and ccd._cte is None and int(ccd._frames_per_read) == 1 and
                 ccd._in_i.i.data_ptr() == sh._out_i.i.data_ptr() and
                 sl._pix.pixels.data_ptr() == ccd._pixels.pixels.data_ptr() and
                 int(sh._plan.subap_npx) <= 16 and self.lenslet_subap_map() is not None)

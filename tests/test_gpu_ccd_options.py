@@ -1,0 +1,129 @@
+"""Detector-structure options of the CCD object on the device (ccd.py:218-262):
+EMCCD excess noise and clock-induced charge by their statistics (the draws
+come from the device's own counter-based streams), and the deterministic
+options against the oracle's restatement: charge-transfer matrices, pixel
+gains, a per-pixel QE map with and without its normalisation."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip('torch')
+
+from oracle.ccd import CCDOracle  # noqa: E402
+from tests.cases import rel_max_err  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+SIDE = 256
+
+
+def _ccd(side=SIDE, set_attrs=None, **kw):
+    from specula_b200.processing_objects.ccd import CCD
+    from specula_b200.data_objects.intensity import Intensity
+    from specula_b200.data_objects.simul_params import SimulParams
+    sp = SimulParams(pixel_pupil=64, pixel_pitch=0.01, time_step=0.001)
+    c = CCD(sp, size=[side, side], dt=0.001, bandw=1000, target_device_idx=0, **kw)
+    for k, v in (set_attrs or {}).items():
+        setattr(c, k, v)
+    ii = Intensity(side, side, target_device_idx=0)
+    c.inputs['in_i'].set(ii)
+    c.setup()
+    return c, ii
+
+
+def _frames(c, ii, inten, n):
+    out = []
+    for t in range(n):
+        ii.i.copy_(torch.as_tensor(inten))
+        ii.generation_time = t * 1000000
+        c.check_ready(t * 1000000)
+        c.trigger()
+        c.post_trigger()
+        out.append(c.outputs['out_pixels'].pixels.cpu().numpy().astype(np.float64))
+    from specula_b200 import _lib
+    _lib.call('sb_device_status')
+    return np.array(out)
+
+
+@pytest.mark.parametrize('delta', [1.0, 0.5])
+def test_emccd_excess_noise_statistics(cuda, delta):
+    """Photon noise and EMCCD multiplication (gain 400, ADU gain 1/20 as the
+    reference sets them): mean lambda, variance lambda (1 + 1/delta), i.e. the
+    excess factor 2 for delta = 1."""
+    lam = 20.0
+    c, ii = _ccd(photon_noise=True, excess_noise=True, excess_delta=delta)
+    assert c._emccd_gain == 400 and abs(c._ADU_gain - 0.05) < 1e-12
+    f = _frames(c, ii, np.full((SIDE, SIDE), lam, np.float32), 3)        # rate 1: lambda electrons per frame
+    v = f.reshape(-1)
+    n = v.size
+    assert abs(v.mean() - lam) <= 4 * np.sqrt(lam * (1 + 1 / delta) / n) + 0.01
+    ratio = v.var() / lam
+    assert abs(ratio - (1 + 1 / delta)) <= 0.05 * (1 + 1 / delta), ratio
+    assert np.all(f[0] != f[1])                   # each frame draws anew
+
+
+def test_cic_statistics(cuda):
+    """Clock-induced charge: without photon noise every pixel reads lambda or
+    lambda + 1 with P(+1) = cic_level; with photon noise on a dark frame the
+    mean is cic_level."""
+    p = 0.1
+    c, ii = _ccd(cic_noise=True, cic_level=p)
+    f = _frames(c, ii, np.full((SIDE, SIDE), 3.0, np.float32), 2)
+    assert set(np.unique(f)) <= {3.0, 4.0}
+    frac = (f == 4.0).mean()
+    assert abs(frac - p) <= 4 * np.sqrt(p * (1 - p) / f.size)
+    c, ii = _ccd(cic_noise=True, cic_level=p, photon_noise=True)
+    f = _frames(c, ii, np.zeros((SIDE, SIDE), np.float32), 2)
+    assert abs(f.mean() - p) <= 4 * np.sqrt(2 * p / f.size)
+
+
+def test_cte_matches_oracle(cuda):
+    """Charge-transfer matrices (near-identity smearing along rows and
+    columns), background, QE: noise-free frames within 1e-5 of the oracle."""
+    side = 96
+    rng = np.random.default_rng(3)
+    m = np.zeros((side, side, 2), np.float32)
+    for k in range(2):
+        m[:, :, k] = np.eye(side) * 0.98 + np.eye(side, k=1) * 0.015 + rng.random((side, side)) * 1e-4
+    kw = dict(cte_noise=True, cte_mat=m, background_noise=True, background_level=0.5, quantum_eff=0.9)
+    c, ii = _ccd(side, **kw)
+    orc = CCDOracle((side, side), 0.001, 0.001, 1000, background_noise=True, background_level=0.5,
+                    quantum_eff=0.9, cte_mat=m)
+    inten = (rng.random((side, side)) * 0.05).astype(np.float32)
+    got = _frames(c, ii, inten, 1)[0]
+    ref = orc.step(inten)
+    assert rel_max_err(got, ref) <= 1e-5
+    assert rel_max_err(got, (inten * 0.9 + 0.5)) > 1e-3          # the matrices did act
+
+
+@pytest.mark.parametrize('normalise', [False, True])
+def test_pixel_gains_and_qe_map_match_oracle(cuda, normalise):
+    """Pixel gains (set by quadrant) and a per-pixel QE map, with read-out
+    noise: the read-out draws differ from the oracle's, so the frames are
+    compared noise-free and the read-out noise is checked by its variance."""
+    side = 64
+    rng = np.random.default_rng(9)
+    qe = (0.7 + 0.3 * rng.random((side, side))).astype(np.float32)
+    attrs = dict(_notUniformQe=True, _notUniformQeMatrix=qe, _normNotUniformQe=normalise)
+    from specula_b200.processing_objects.ccd import CCD  # noqa: F401
+    c, ii = _ccd(side, set_attrs=attrs)
+    c.setQuadrantGains([1.0, 1.1, 0.9, 1.2])
+    c.setup()
+    gains = c._pixelGains
+    orc = CCDOracle((side, side), 0.001, 0.001, 1000, pixel_gains=gains, qe_map=qe, qe_map_normalise=normalise)
+    inten = (rng.random((side, side)) * 0.05).astype(np.float32)
+    got = _frames(c, ii, inten, 1)[0]
+    ref = orc.step(inten)
+    assert rel_max_err(got, ref) <= 1e-6
+    # read-out noise scaled by the gains (and the map when normalising)
+    c2, ii2 = _ccd(side, set_attrs=attrs, readout_noise=True, readout_level=2.0)
+    c2.setQuadrantGains([1.0, 1.1, 0.9, 1.2])
+    c2.setup()
+    f = _frames(c2, ii2, np.zeros((side, side), np.float32), 8)
+    scale = gains / (qe if normalise else 1.0)
+    z = (f / scale[None]).reshape(-1)
+    assert abs(z.std() - 2.0) <= 0.05 * 2.0
+
+
+def test_pixel_gains_on_an_integer_frame_are_rejected(cuda):
+    with pytest.raises(ValueError, match='integer'):
+        _ccd(64, photon_noise=True, pixelGains=np.ones((64, 64), np.float32))
