@@ -58,7 +58,7 @@ def test_emccd_excess_noise_statistics(cuda, delta):
     assert abs(v.mean() - lam) <= 4 * np.sqrt(lam * (1 + 1 / delta) / n) + 0.01
     ratio = v.var() / lam
     assert abs(ratio - (1 + 1 / delta)) <= 0.05 * (1 + 1 / delta), ratio
-    assert np.all(f[0] != f[1])                   # each frame draws anew
+    assert (f[0] == f[1]).mean() < 0.05           # each frame draws anew (equal values only by chance)
 
 
 def test_cic_statistics(cuda):
