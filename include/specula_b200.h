@@ -265,6 +265,12 @@ typedef struct sb_slopec_plan {
     const float *xw;        /* [npx2] x weights                               */
     const float *yw;        /* [npx2] y weights                               */
     const float *mw;        /* [npx2] mask weights                            */
+    /* options of calc_slopes_nofor (sh_slopec.py:356-420); zero / NULL: off  */
+    int thr_pedestal;       /* pixels below thr set to 0, the others kept     */
+    float thr_ratio;        /* > 0: each sub-aperture's thr = thr_ratio * its
+                             * largest (windowed) pixel                        */
+    const float *window;    /* [npx2][n_subaps] weights after the flux sums   */
+    float mult;             /* != 0: slopes *= mult                           */
 } sb_slopec_plan;
 
 size_t sb_slopec_scratch_bytes(const sb_slopec_plan *plan);

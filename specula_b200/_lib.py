@@ -49,7 +49,8 @@ class CcdParams(C.Structure):
 
 class SlopecPlan(C.Structure):
     _fields_ = [('n_subaps', C.c_int), ('npx2', C.c_int), ('thr', C.c_float),
-                ('idxs', ip), ('xw', fp), ('yw', fp), ('mw', fp)]
+                ('idxs', ip), ('xw', fp), ('yw', fp), ('mw', fp),
+                ('thr_pedestal', C.c_int), ('thr_ratio', C.c_float), ('window', fp), ('mult', C.c_float)]
 
 
 class IirPlan(C.Structure):

@@ -513,12 +513,31 @@ __global__ void __launch_bounds__(256) slopec_sums_kernel(sb_slopec_plan pl, con
     const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const bool valid = s < pl.n_subaps;
     const int32_t *ix = pl.idxs + (size_t)(valid ? s : 0) * pl.npx2;
+    float thr = pl.thr;
+    if (pl.thr_ratio > 0.f) {
+        // thr = thr_ratio * the sub-aperture's largest (windowed) pixel
+        // (sh_slopec.py:215-232); the first pass only reads the pixels
+        float m = -INFINITY;
+        for (int e = lane; valid && e < pl.npx2; e += 32) {
+            float v = pix[ix[e]];
+            if (pl.window) v = __fmul_rn(v, pl.window[(size_t)e * pl.n_subaps + s]);
+            m = fmaxf(m, v);
+        }
+        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+        thr = pl.thr_ratio * m;
+    }
     float f = 0.f, t = 0.f, x = 0.f, y = 0.f;
     for (int e = lane; valid && e < pl.npx2; e += 32) {
-        const float v = pix[ix[e]];
+        float v = pix[ix[e]];
         f += v;
-        float w = v - pl.thr;                 // pixels -= thr; clamp < 0 -> 0
-        w = w < 0.f ? 0.f : w;
+        if (pl.window) v = __fmul_rn(v, pl.window[(size_t)e * pl.n_subaps + s]);    // sh_slopec.py:368-371
+        float w;
+        if (pl.thr_pedestal) {
+            w = v < thr ? 0.f : v;            // pixels below thr -> 0 (sh_slopec.py:381-382)
+        } else {
+            w = v - thr;                      // pixels -= thr; clamp < 0 -> 0
+            w = w < 0.f ? 0.f : w;
+        }
         t = fmaf(w, pl.mw[e], t);
         x = fmaf(w, pl.xw[e], x);
         y = fmaf(w, pl.yw[e], y);
@@ -550,7 +569,7 @@ __global__ void __launch_bounds__(256) slopec_finish_kernel(int n, const float *
                                                             const float *__restrict__ syn,
                                                             const float *__restrict__ part_tot, int nparts,
                                                             float *__restrict__ slopes, int slopes_stride,
-                                                            int work_stride) {
+                                                            int work_stride, float mult) {
     __shared__ double red[33];
     tot += (size_t)blockIdx.y * work_stride;
     sxn += (size_t)blockIdx.y * work_stride;
@@ -565,8 +584,13 @@ __global__ void __launch_bounds__(256) slopec_finish_kernel(int n, const float *
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
         float fac = 1.0f / tot[s];
         fac = fac > cut ? 0.0f : fac;
-        slopes[s] = sxn[s] * fac;
-        slopes[n + s] = syn[s] * fac;
+        float sx = sxn[s] * fac, sy = syn[s] * fac;
+        if (mult != 0.0f) {                   // sh_slopec.py:416-418
+            sx *= mult;
+            sy *= mult;
+        }
+        slopes[s] = sx;
+        slopes[n + s] = sy;
     }
 }
 
@@ -891,7 +915,7 @@ int slopec_impl(const char *who, const sb_slopec_plan *pl, const float *pixels, 
     int nb2 = (n + 255) / 256;
     nb2 = nb2 > 148 ? 148 : nb2;
     slopec_finish_kernel<<<dim3(nb2, n_batch), 256, 0, st>>>(n, tot, sxn, syn, part, nblk, slopes, slopes_stride,
-                                                             work_stride);
+                                                             work_stride, pl->mult);
     return sb::check_launch("slopec_finish_kernel");
 }
 
@@ -944,6 +968,8 @@ extern "C" int sb_sh_ccd_slopec(const sb_sh_plan *sh, int dft_mode, const float 
     if (slopec->npx2 != npx * npx || slopec->n_subaps < 1 || slopec->n_subaps > n * n)
         return sb::fail(SB_EINVAL, "sb_sh_ccd_slopec: slope plan of %d sub-apertures x %d pixels", slopec->n_subaps,
                         slopec->npx2);
+    if (slopec->thr_pedestal || slopec->thr_ratio > 0.f || slopec->window || slopec->mult != 0.f)
+        return sb::fail(SB_EUNSUPPORTED, "sb_sh_ccd_slopec: the slope options beyond thr go through sb_slopec");
     const size_t need = sb_sh_ccd_slopec_scratch_bytes(sh, slopec->n_subaps);
     if (!scratch || need == 0 || scratch_bytes < need)
         return sb::fail(SB_ESCRATCH, "sb_sh_ccd_slopec: scratch needs %zu bytes, got %zu", need, scratch_bytes);

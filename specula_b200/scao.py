@@ -425,14 +425,15 @@ class ScaoLoop:
         """True when sb_sh_ccd_slopec computes exactly what SH + CCD + ShSlopec
         do: plain (not interpolated, not LGS) SH with the FP32 or split-BF16
         DFTs, a detector of the SH frame size reading out every step without
-        binning, the slope computer reading that detector's pixels, and a
-        sub-aperture table of row-major lenslet boxes."""
+        binning, the slope computer reading that detector's pixels with no
+        option beyond thr_value, and a sub-aperture table of row-major lenslet
+        boxes."""
         sh, ccd, sl = self.sh, self.ccd, self.slopec
         return (not sh.geometry.do_interpolation and sh._kernelobj is None and
                 sh._forward in ('sb_sh_forward', 'sb_sh_forward_split_bf16') and
                 ccd._bin_scratch is None and ccd._cte is None and int(ccd._frames_per_read) == 1 and
                 ccd._in_i.i.data_ptr() == sh._out_i.i.data_ptr() and
-                sl._pix.pixels.data_ptr() == ccd._pixels.pixels.data_ptr() and
+                sl._pix.pixels.data_ptr() == ccd._pixels.pixels.data_ptr() and sl.options_plain() and
                 int(sh._plan.subap_npx) <= 16 and self.lenslet_subap_map() is not None)
 
     def _setup_chain(self):

@@ -18,6 +18,7 @@ time; they only read the .npz/.json files written here.
 import json
 import os
 import sys
+import types
 
 import numpy as np
 
@@ -577,6 +578,83 @@ def make_slopec_filter_cases(ref):
     return out
 
 
+def make_slopec_option_cases(ref):
+    """ShSlopec options of calc_slopes_nofor set as attributes after
+    construction, as the reference's own code sets them (sh_slopec.py:48-60):
+    a pedestal threshold, a window matrix, a multiplication factor, quad-cell
+    weights and a windowed mask (weightedPixRad with windowing), on the
+    reference's 8x8 sub-aperture table and random frames.  The relative
+    threshold (thr_ratio_value) and the Gaussian weighted mask stop with an
+    exception in calc_slopes_nofor (sh_slopec.py:376 indexes a scalar, :121
+    calls psf_gaussian with three arguments); their raising is recorded here.
+    The relative threshold does run in the per-sub-aperture loop
+    calc_slopes_for (:150-300, threshold at :231-232): 'ratio_for' holds its
+    slopes, on frames where every sub-aperture is bright so that the two
+    loops' denominators agree."""
+    from specula.processing_objects.sh_slopec import ShSlopec
+    from specula.data_objects.subap_data import SubapData
+    from specula.data_objects.pixels import Pixels
+    out = {}
+    rng = np.random.default_rng(41)
+    idxs = ref['subaps/idxs']
+    dmap = ref['subaps/display_map']
+    n, npx2 = idxs.shape
+    np_sub = int(round(np.sqrt(npx2)))
+    win = (0.5 + rng.random((np_sub, np_sub, n))).astype(np.float32)
+    cases = {
+        'pedestal': dict(thr_value=30.0, attrs=dict(thr_pedestal=True)),
+        'window': dict(thr_value=10.0, attrs=dict(winMatWindowed=win)),
+        'mult': dict(attrs=dict(mult_factor=2.5)),
+        'quadcell': dict(attrs=dict(quadcell_mode=True), weights=True),
+        'windowing': dict(attrs=dict(weightedPixRad=2.0, windowing=True), weights=True),
+        'ratio': dict(attrs=dict(thr_ratio_value=0.002)),
+        'gaussian': dict(attrs=dict(weightedPixRad=1.0), weights=True),
+    }
+    out['slopec_opt/window'] = win
+    frames = [(rng.random((64, 64)) * 100).astype(np.float32) for _ in range(2)]
+    for t, f in enumerate(frames):
+        out['slopec_opt/frame%d' % t] = f
+    for name, c in cases.items():
+        sd = SubapData(idxs=idxs, display_map=dmap, nx=8, ny=8, target_device_idx=-1, precision=1)
+        sc = ShSlopec(sd, thr_value=c.get('thr_value', -1), target_device_idx=-1, precision=1)
+        for k, v in c['attrs'].items():
+            setattr(sc, k, v)
+        try:
+            if c.get('weights'):
+                sc.set_xy_weights()
+            pix = Pixels(64, 64, target_device_idx=-1, precision=1)
+            sc.inputs['in_pixels'].set(pix)
+            sc.setup()
+            for t, f in enumerate(frames):
+                pix.pixels[:] = f
+                pix.generation_time = t + 1
+                sc.check_ready(t + 1)
+                sc.trigger()
+                sc.post_trigger()
+                out['slopec_opt/%s/slopes%d' % (name, t)] = np.array(sc.slopes.slopes, dtype=np.float32)
+            out['slopec_opt/%s/xweights' % name] = np.array(sc.xweights, dtype=np.float64)
+            out['slopec_opt/%s/mask' % name] = np.array(sc.mask_weighted, dtype=np.float64)
+        except Exception as e:            # the reference's failure, by exception type
+            out['slopec_opt/%s/raises' % name] = np.array(type(e).__name__)
+    for ratio in (0.3, 0.6):
+        sd = SubapData(idxs=idxs, display_map=dmap, nx=8, ny=8, target_device_idx=-1, precision=1)
+        sc = ShSlopec(sd, target_device_idx=-1, precision=1)
+        sc.thr_ratio_value = ratio
+        sc.winMatWindowed = win if ratio == 0.6 else None
+        pix = Pixels(64, 64, target_device_idx=-1, precision=1)
+        sc.inputs['in_pixels'].set(pix)
+        sc.setup()
+        for t, f in enumerate(frames):
+            # the loop indexes its frame with the flat sub-aperture indices, as
+            # it does the accumulated frame: hand it the flattened frame there
+            sc.accumulated_pixels = types.SimpleNamespace(pixels=f.ravel().copy())
+            sc.current_time = t + 1
+            sc.calc_slopes_for(accumulated=True)
+            out['slopec_opt/ratio_for%g/slopes%d' % (ratio, t)] = np.array(sc.accumulated_slopes.slopes,
+                                                                          dtype=np.float32)
+    return out
+
+
 def make_polc_cases():
     """Modalrec with POLC (modalrec.py:126-156): pseudo-open-loop slopes
     s + IM c, modes R s - c, without and with a projection matrix, over three
@@ -676,6 +754,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, 'polc_fp32.npz'), **make_polc_cases())
     np.savez_compressed(os.path.join(HERE, 'iir_fp32.npz'), **make_iir_cases())
     np.savez_compressed(os.path.join(HERE, 'slopec_filt_fp32.npz'), **make_slopec_filter_cases(ref))
+    np.savez_compressed(os.path.join(HERE, 'slopec_opt_fp32.npz'), **make_slopec_option_cases(ref))
     print('wrote', sorted(os.listdir(HERE)))
 
 
@@ -700,6 +779,12 @@ if __name__ == '__main__':
         with np.load(os.path.join(HERE, 'ref_fits.npz')) as z:
             ref = {k: z[k] for k in z.files}
         np.savez_compressed(os.path.join(HERE, 'slopec_filt_fp32.npz'), **make_slopec_filter_cases(ref))
+    elif '--slopec-options' in sys.argv:  # only the slope-option fixtures
+        import specula
+        specula.init(-1, precision=1)
+        with np.load(os.path.join(HERE, 'ref_fits.npz')) as z:
+            ref = {k: z[k] for k in z.files}
+        np.savez_compressed(os.path.join(HERE, 'slopec_opt_fp32.npz'), **make_slopec_option_cases(ref))
     elif '--iir' in sys.argv:          # only the general IIR filter fixtures
         import specula
         specula.init(-1, precision=1)

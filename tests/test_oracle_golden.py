@@ -169,3 +169,63 @@ def test_psf_oracle_matches_reference(golden, pix, nd, lam, t0):
         assert abs(sr - float(g[key + '/sr%d' % step])) <= 1e-5 * abs(float(g[key + '/sr%d' % step]))
     np.testing.assert_allclose(o.int_psf, g[key + '/int_psf'], rtol=1e-5, atol=1e-7 * float(o.int_psf.max()))
     assert abs(o.int_sr - float(g[key + '/int_sr'])) <= 1e-5 * abs(float(g[key + '/int_sr']))
+
+
+SLOPEC_OPT_CASES = {
+    'pedestal': dict(thr_value=30.0, thr_pedestal=True),
+    'window': dict(thr_value=10.0, win=True),
+    'mult': dict(mult_factor=2.5),
+    'quadcell': dict(weights=dict(quadcell_mode=True)),
+    'windowing': dict(weights=dict(weighted_pix_rad=2.0, windowing=True)),
+    'ratio_for0.3': dict(thr_ratio_value=0.3),
+    'ratio_for0.6': dict(thr_ratio_value=0.6, win=True),
+}
+
+
+def slopec_option_kwargs(case, opt):
+    """Oracle keyword arguments of one slope-option case of slopec_opt_fp32.npz."""
+    c = dict(SLOPEC_OPT_CASES[case])
+    kw = {k: c[k] for k in ('thr_value', 'thr_pedestal', 'mult_factor', 'thr_ratio_value') if k in c}
+    if c.get('win'):
+        kw['win_mat'] = opt['slopec_opt/window']
+    if 'weights' in c:
+        kw['weights'] = osl.xy_weights(8, **c['weights'])
+    return kw
+
+
+@pytest.fixture(scope='module')
+def slopec_opt():
+    import os
+    with np.load(os.path.join(os.path.dirname(__file__), 'golden', 'slopec_opt_fp32.npz')) as z:
+        return {k: z[k] for k in z.files}
+
+
+@pytest.mark.parametrize('case', list(SLOPEC_OPT_CASES))
+def test_slopec_options_match_reference(golden, slopec_opt, case):
+    """Pedestal threshold, window matrix, multiplication factor, quad-cell
+    weights, a windowed mask (calc_slopes_nofor) and the relative threshold
+    (calc_slopes_for) on the reference's 8x8 sub-aperture table."""
+    idxs = golden['ref_fits']['subaps/idxs']
+    kw = slopec_option_kwargs(case, slopec_opt)
+    for t in range(2):
+        s, _ = osl.sh_slopes(slopec_opt['slopec_opt/frame%d' % t], idxs, **kw)
+        assert rel_max_err(s, slopec_opt['slopec_opt/%s/slopes%d' % (case, t)]) <= 2e-6, (case, t)
+    if 'weights' in SLOPEC_OPT_CASES[case]:
+        xw, _, mw = kw['weights']
+        assert np.array_equal(xw, slopec_opt['slopec_opt/%s/xweights' % case])
+        assert np.array_equal(mw, slopec_opt['slopec_opt/%s/mask' % case])
+
+
+def test_slopec_option_cases_the_reference_raises_on(slopec_opt):
+    """The relative threshold and the Gaussian weighted mask raise in the
+    reference's calc_slopes_nofor / computeXYweights (an index into a scalar,
+    a three-argument call of a two-argument method); the oracle computes the
+    per-sub-aperture form and the Gaussian of psf_gaussian instead (parity for
+    the Gaussian mask is by construction only)."""
+    assert str(slopec_opt['slopec_opt/ratio/raises']) == 'IndexError'
+    assert str(slopec_opt['slopec_opt/gaussian/raises']) == 'TypeError'
+    x, y, m = osl.xy_weights(8, weighted_pix_rad=1.0)
+    v = np.linspace(-1, 1, 8)
+    g = np.exp(-4 * np.log(2) * (v[None, :] ** 2 + v[:, None] ** 2))
+    assert np.allclose(m, g / g.max(), rtol=1e-6)
+    assert m.max() == 1.0 and np.allclose(x, np.meshgrid(v, v)[0] * m)
