@@ -60,6 +60,8 @@ def parse():
     p.add_argument('--profile-loop', type=int, default=0, metavar='R',
                    help='set up the ELT step graph, then run R replays between cudaProfilerStart/Stop '
                         '(for ncu --profile-from-start off) and exit')
+    p.add_argument('--profile-mc', action='store_true',
+                   help='as --profile-batched, for the Monte-Carlo step (sb_mc_step) instead of the group graph')
     p.add_argument('--batched-only', action='store_true',
                    help='run only the 96-realisation batched Monte-Carlo leg (one GPU)')
     p.add_argument('--psf-only', action='store_true', help='run only the PSF leg (one GPU)')
@@ -465,6 +467,14 @@ def bench_batched(dev, steps, cpu_budget_s):
     sys_b.capture()
     tune_s = time.perf_counter() - t_tune
     bf16_ms = timed(sys_b.replay, steps)
+    group_launches = sys_b.launches_per_step
+    # the Monte-Carlo step of the C ABI: one launch per stage over every group
+    mc = {}
+    for dft in ('fp32', 'split_bf16'):
+        sys_b.set_dft(dft)
+        sys_b.capture_mc()
+        mc[dft] = (timed(sys_b.replay, steps), sys_b.launches_per_step)
+    sys_b.release_mc()
     _lib_status()
     by_size = {}
     for (tmpl, reals) in all_groups:
@@ -481,6 +491,13 @@ def bench_batched(dev, steps, cpu_budget_s):
            'batched_split_bf16_ms_per_step': bf16_ms,
            'batched_split_bf16_realisation_steps_per_s': n_real / (bf16_ms / 1e3),
            'speedup_batched_split_bf16_vs_plain': plain_ms / bf16_ms, 'setup_s': setup_s,
+           'group_graph_launches_per_step': group_launches,
+           'mc_step_ms_per_step': mc['fp32'][0], 'mc_step_split_bf16_ms_per_step': mc['split_bf16'][0],
+           'mc_step_launches_per_step': mc['split_bf16'][1],
+           'mc_step_realisation_steps_per_s': n_real / (min(mc['fp32'][0], mc['split_bf16'][0]) / 1e3),
+           'mc_step': 'sb_mc_step: seven launches per step (layer parameters, layers, propagation, SH, '
+                      'normalisation + detector + slopes, reconstructor + integrators, mirror), each over every '
+                      'realisation of every group, captured in one graph',
            'autotune_s': tune_s,
            'autotune': [{k: r[k] for k in ('family', 'shape', 'variant', 'name', 'times_us', 'speedup_vs_variant0',
                                            'cached')} for r in tuner.results],
@@ -968,14 +985,17 @@ def profile_loop(dev, replays):
                       'kernels_per_step': loop.kernels_per_step}), flush=True)
 
 
-def profile_batched(dev):
-    """One replay of the batched graph bracketed for a profiler."""
+def profile_batched(dev, mc=False):
+    """One replay of the batched graph (mc: the Monte-Carlo step) bracketed for a profiler."""
     import torch
     from specula_b200.batched import BatchedScao, mc_groups
     sys_b = BatchedScao(mc_groups(), device_idx=dev.index, dft='split_bf16')
     sys_b.start()
-    sys_b.autotune()
-    sys_b.capture()
+    if mc:
+        sys_b.capture_mc()
+    else:
+        sys_b.autotune()
+        sys_b.capture()
     for _ in range(3):
         sys_b.replay()
     torch.cuda.synchronize(dev)
@@ -994,11 +1014,11 @@ def main():
         torch.cuda.set_device(dev)
         profile_loop(dev, args.profile_loop)
         return
-    if args.profile_batched:
+    if args.profile_batched or args.profile_mc:
         import torch
         dev = torch.device('cuda', 0)
         torch.cuda.set_device(dev)
-        profile_batched(dev)
+        profile_batched(dev, mc=args.profile_mc)
         return
     if args.batched_only:
         import torch

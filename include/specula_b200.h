@@ -667,6 +667,101 @@ size_t sb_psf_tc_scratch_bytes(int m, int n);
 int sb_psf_tc(const float *A, const float *phase_nm, int m, int n, float phase_to_rad, const void *dft, float *psf,
               float *int_psf, void *scratch, size_t scratch_bytes, void *stream);
 
+/* ------------------------------------------------------------------------
+ * Monte-Carlo step over geometry groups — the loop step of many independent
+ * SCAO realisations of uneven pupil / sub-aperture counts (the reference
+ * steps each through its own LoopControl.iter, loop_control.py:83-123).
+ * A group is realisations that share the pupil, sub-aperture grid,
+ * wavelength, reconstructor and mirror, with their own atmospheres and
+ * detector seeds; each stage of the step is ONE launch over every
+ * realisation of every group:
+ *   1 layer positions + per-step parameters    (atmo_evolution.py:258-277)
+ *   2 every turbulence layer                     (atmo_evolution.py:278-294)
+ *   3 on-axis propagation                        (atmo_propagation.py:105-144)
+ *   4 SH forward, unnormalised + partial sums    (sh.py:348-420)
+ *   5 photon normalisation, CCD, CoG slopes, flux cut-off, detector state
+ *                                                (sh.py:422-428, ccd.py:198-287,
+ *                                                 sh_slopec.py:308-438)
+ *   6 reconstructor rows + integrators           (modalrec.py:114-162,
+ *                                                 iir_filter.py:100-211)
+ *   7 mirror projection                          (dm.py:72-86)
+ * Each stage computes what the group-by-group batched calls compute
+ * (sb_atmo_evolve_batched, sb_propagate_batched, sb_sh_forward[_split_bf16]_batched,
+ * sb_ccd_step_batched, sb_slopec_batched, sb_modalrec_batched,
+ * sb_integrator, sb_dm_project_batched with one mode-row group), bit for bit.
+ * Per group: SH geometries with a compile-time kernel, every frame read out
+ * each step (frames_per_read 1, no binning, no charge-transfer matrices),
+ * the slope computer with thr_value only, sub-aperture boxes listed
+ * row-major (lenslet_subap maps lenslet i*n+j to its valid sub-aperture or
+ * -1), at most 1024 modes.  The frames of a group are rows of stacks:
+ * intensity, integrated and pixels share frame_stride; the turbulence
+ * layers' outputs (layers[].out) are rows of atm.
+ *   sb_mc_workspace_bytes  device workspace for the groups (256-byte aligned,
+ *                          zero-filled before sb_mc_create)
+ *   sb_mc_create           validates the groups, copies their tables into the
+ *                          workspace (on stream) and returns a host handle;
+ *                          the host arrays may be freed afterwards
+ *   sb_mc_step             one step: SB_MC_LAUNCHES launches on stream, no
+ *                          allocation, no synchronisation (graph-capturable)
+ *   sb_mc_destroy          frees the handle
+ * ---------------------------------------------------------------------- */
+#define SB_MC_MAX_GROUPS 8
+#define SB_MC_LAUNCHES 7
+
+typedef struct sb_mc_group {
+    int n_batch;                        /* realisations                                */
+    /* atmosphere: n_batch * n_atm layers, realisation-major (host arrays) */
+    int n_atm;
+    int L;                              /* pupil side [px]                             */
+    const sb_atmo_layer *layers;
+    const sb_atmo_layer_inputs *inputs;
+    sb_atmo_inputs constants;           /* its pointers are not read                   */
+    /* propagation: layer k of realisation b is atm + b*atm_real_stride + k*L*L */
+    const float *atm;
+    long long atm_real_stride;
+    const float *stop_A, *stop_phase;   /* pupil stop (shared; NULL: none)             */
+    const float *dm_A;                  /* mirror amplitude (shared; NULL: none)       */
+    float *dm_phase;                    /* per-realisation mirror phase, stride dm_stride */
+    long long dm_stride;
+    float *field_A, *field_phase;       /* per-realisation field, stride field_stride   */
+    long long field_stride;
+    /* SH: dft_mode 0 FP32, 1 split-BF16 */
+    sb_sh_plan sh;
+    int dft_mode;
+    float photon_scale;
+    /* detector and slopes */
+    float *intensity, *integrated, *pixels;
+    long long frame_stride;
+    sb_ccd_params ccd;                  /* shared parameters and frame state           */
+    const uint64_t *photon_seeds;       /* device [n_batch]                            */
+    const uint64_t *readout_seeds;      /* device [n_batch]                            */
+    sb_slopec_plan slopec;
+    const int32_t *lenslet_subap;       /* device [n_lenses^2]                         */
+    float *slopes;                      /* [n_batch][slopes_stride]                    */
+    int slopes_stride;
+    float *flux;                        /* [n_batch][flux_stride]                      */
+    int flux_stride;
+    /* reconstructor and integrators */
+    const float *R;
+    int n_modes, n_slopes, ldr;
+    float *modes;                       /* [n_batch][n_modes]                          */
+    sb_iir_plan iir;                    /* n = n_batch * n_modes, element b*n_modes+m  */
+    float *commands;                    /* [n_batch][n_modes]: the integrators' output */
+    /* mirror: phase[b][mask_idx[p]] = dm_sign * sum_m commands[b][m] IF[m][p] */
+    const float *ifunc;                 /* 16-byte aligned rows                        */
+    int n_valid, ld_if;
+    const int32_t *mask_idx;
+    float dm_sign;
+} sb_mc_group;
+
+typedef struct sb_mc_handle sb_mc_handle;
+
+size_t sb_mc_workspace_bytes(const sb_mc_group *groups, int n_groups);
+int sb_mc_create(const sb_mc_group *groups, int n_groups, void *workspace, size_t workspace_bytes,
+                 sb_mc_handle **handle, void *stream);
+int sb_mc_step(const sb_mc_handle *handle, void *stream);
+void sb_mc_destroy(sb_mc_handle *handle);
+
 #ifdef __cplusplus
 }
 #endif

@@ -81,9 +81,33 @@ class PropLayer(C.Structure):
     _fields_ = [('A', fp), ('phase', fp), ('ld', C.c_int), ('top', C.c_int), ('left', C.c_int)]
 
 
+SB_MC_MAX_GROUPS = 8
+SB_MC_LAUNCHES = 7
+
+
+class McGroup(C.Structure):
+    _fields_ = [('n_batch', C.c_int), ('n_atm', C.c_int), ('L', C.c_int),
+                ('layers', C.POINTER(AtmoLayer)), ('inputs', C.POINTER(AtmoLayerInputs)), ('constants', AtmoInputs),
+                ('atm', fp), ('atm_real_stride', C.c_longlong), ('stop_A', fp), ('stop_phase', fp), ('dm_A', fp),
+                ('dm_phase', fp), ('dm_stride', C.c_longlong), ('field_A', fp), ('field_phase', fp),
+                ('field_stride', C.c_longlong),
+                ('sh', ShPlan), ('dft_mode', C.c_int), ('photon_scale', C.c_float),
+                ('intensity', fp), ('integrated', fp), ('pixels', fp), ('frame_stride', C.c_longlong),
+                ('ccd', CcdParams), ('photon_seeds', vp), ('readout_seeds', vp),
+                ('slopec', SlopecPlan), ('lenslet_subap', ip), ('slopes', fp), ('slopes_stride', C.c_int),
+                ('flux', fp), ('flux_stride', C.c_int),
+                ('R', fp), ('n_modes', C.c_int), ('n_slopes', C.c_int), ('ldr', C.c_int), ('modes', fp),
+                ('iir', IirPlan), ('commands', fp),
+                ('ifunc', fp), ('n_valid', C.c_int), ('ld_if', C.c_int), ('mask_idx', ip), ('dm_sign', C.c_float)]
+
+
 # name -> (restype, argtypes); every function of include/specula_b200.h
 SIGNATURES = {
     'sb_version': (C.c_int, []),
+    'sb_mc_workspace_bytes': (C.c_size_t, [C.POINTER(McGroup), C.c_int]),
+    'sb_mc_create': (C.c_int, [C.POINTER(McGroup), C.c_int, vp, C.c_size_t, C.POINTER(vp), vp]),
+    'sb_mc_step': (C.c_int, [vp, vp]),
+    'sb_mc_destroy': (None, [vp]),
     'sb_last_error': (C.c_char_p, []),
     'sb_sh_scratch_bytes': (C.c_size_t, [C.POINTER(ShPlan)]),
     'sb_sh_forward': (C.c_int, [C.POINTER(ShPlan), fp, fp, fp, C.c_int, C.c_float, fp, vp, C.c_size_t, vp]),

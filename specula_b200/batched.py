@@ -16,6 +16,11 @@ and the mirror (``sb_dm_project_batched``: the influence functions read once
 for up to 16 realisations).  ``capture()`` puts the step of every group into
 one CUDA graph, each group on a stream of its own.
 
+``BatchedScao.capture_mc()`` puts the step of every group into the
+Monte-Carlo step of the C ABI instead (``sb_mc_step``): seven launches per
+step, each stage one launch over every realisation of every group, the same
+bits as the group-by-group graph.
+
 ``BatchedScao.replay_plain()`` runs the same realisations the plain way (each
 ``ScaoLoop``'s own captured step with the FP32 SH, its own reconstructor and
 mirror), for comparison.
@@ -32,6 +37,25 @@ from specula_b200.base_value import BaseValue
 from specula_b200.processing_objects.integrator import Integrator
 from specula_b200.lib.make_mask import make_mask
 from specula_b200.scao import ScaoConfig, ScaoLoop, elt_config, valid_subaps
+
+
+def graph_kernel_count(graph):
+    """Kernel nodes of a captured torch CUDA graph (made with keep_graph=True)."""
+    from cuda.bindings import runtime as rt
+    h = rt.cudaGraph_t(init_value=graph.raw_cuda_graph())
+    err, _, n = rt.cudaGraphGetNodes(h, 0)
+    if err != rt.cudaError_t.cudaSuccess:
+        raise RuntimeError(f'cudaGraphGetNodes: {err}')
+    err, nodes, n = rt.cudaGraphGetNodes(h, n)
+    if err != rt.cudaError_t.cudaSuccess:
+        raise RuntimeError(f'cudaGraphGetNodes: {err}')
+    count = 0
+    for node in nodes[:n]:
+        err, kind = rt.cudaGraphNodeGetType(node)
+        if err != rt.cudaError_t.cudaSuccess:
+            raise RuntimeError(f'cudaGraphNodeGetType: {err}')
+        count += kind == rt.cudaGraphNodeType.cudaGraphNodeTypeKernel
+    return count
 
 
 def seeing_from_r0(r0):
@@ -187,6 +211,46 @@ class _Group:
             self.integ._ost[b * nm:(b + 1) * nm].copy_(lp.integ._ost)
             self.integ.out_comm.value[b * nm:(b + 1) * nm].copy_(lp.integ.out_comm.value)
 
+    def mc_group(self):
+        """This group as an sb_mc_group: the same buffers, plans and seeds the
+        group-by-group launches use (keeps the ctypes arrays it points to)."""
+        lp = self.loops[0]
+        if not lp._can_fuse_chain():
+            raise NotImplementedError('BatchedScao: the Monte-Carlo step needs the fused detector / slope chain '
+                                      '(plain SH, a detector read every step, slopes with thr_value only)')
+        dm = self.dm
+        L2, F2 = self.L * self.L, self.side * self.side
+        self._lenslet_subap = torch.as_tensor(lp.lenslet_subap_map(), device=self.device)
+        m = _lib.McGroup()
+        m.n_batch, m.n_atm, m.L = self.n, self.n_atm, self.L
+        m.layers = ctypes.cast(self.atmo_layers, ctypes.POINTER(_lib.AtmoLayer))
+        m.inputs = ctypes.cast(self.atmo_inputs, ctypes.POINTER(_lib.AtmoLayerInputs))
+        m.constants = lp.atmo.inputs_struct(lp.atmo.delta_time)
+        m.atm, m.atm_real_stride = self.ATM.data_ptr(), self.n_atm * L2
+        m.stop_A, m.stop_phase = self.stop.A.data_ptr(), self.stop.phaseInNm.data_ptr()
+        m.dm_A = lp.dm.layer.A.data_ptr()
+        m.dm_phase, m.dm_stride = self.dm_phase.data_ptr(), L2
+        m.field_A, m.field_phase, m.field_stride = self.EA.data_ptr(), self.EP.data_ptr(), L2
+        m.sh = lp.sh._plan
+        m.dft_mode = 0 if self.sh_forward == SH_FORWARD['fp32'] else 1
+        m.photon_scale = lp.sh._photon_scale
+        m.intensity, m.integrated, m.pixels = self.I.data_ptr(), self.INT.data_ptr(), self.PIX.data_ptr()
+        m.frame_stride = F2
+        m.ccd = lp.ccd._params
+        m.photon_seeds, m.readout_seeds = self.pseeds.data_ptr(), self.rseeds.data_ptr()
+        m.slopec = lp.slopec._plan
+        m.lenslet_subap = self._lenslet_subap.data_ptr()
+        m.slopes, m.slopes_stride = self.S.data_ptr(), self.nsl
+        m.flux, m.flux_stride = self.FLUX.data_ptr(), self.nsl // 2
+        R = lp.rec._R
+        m.R, m.n_modes, m.n_slopes, m.ldr = R.data_ptr(), self.nm, self.nsl, R.stride(0)
+        m.modes = self.M.data_ptr()
+        m.iir = self.integ._plan
+        m.commands = self.integ.out_comm.value.data_ptr()
+        m.ifunc, m.n_valid, m.ld_if = dm._IF.data_ptr(), int(dm._idx.numel()), dm._ld
+        m.mask_idx, m.dm_sign = dm._idx.data_ptr(), float(dm.sign)
+        return m
+
     def group_ops(self):
         """The whole step of every realisation of the group, one launch each:
         atmosphere (every layer), propagation, SH, CCD, slopes, the shared
@@ -235,6 +299,7 @@ class BatchedScao:
         self.groups = [_Group(t, reals, device_idx, dft=dft) for t, reals in groups]
         self.graph = None
         self.plain_graphs = None
+        self._launches = None
 
     def set_dft(self, dft):
         """Switch the groups' SH forward between 'fp32' and 'split_bf16'; the
@@ -301,7 +366,7 @@ class BatchedScao:
         torch.cuda.synchronize(self.device)
         gstreams = [torch.cuda.Stream(self.device) for _ in self.groups]
         cap = torch.cuda.Stream(self.device)
-        g = torch.cuda.CUDAGraph()
+        g = torch.cuda.CUDAGraph(keep_graph=True)
         with torch.cuda.graph(g, stream=cap):
             main = torch.cuda.current_stream(self.device)
             for grp, gs in zip(self.groups, gstreams):
@@ -312,10 +377,63 @@ class BatchedScao:
                 main.wait_stream(gs)
         torch.cuda.synchronize(self.device)
         self.graph = g
+        self._launches = graph_kernel_count(g)
         return g
 
     def replay(self):
         self.graph.replay()
+
+    @property
+    def launches_per_step(self):
+        """Kernel launches of one captured step, counted in the graph."""
+        return self._launches
+
+    def capture_mc(self):
+        """The batched step of every group as one sb_mc_step (seven launches,
+        each over every realisation of every group) captured in a CUDA graph."""
+        lib = _lib.load()
+        self.release_mc()
+        groups = (_lib.McGroup * len(self.groups))(*[g.mc_group() for g in self.groups])
+        nbytes = lib.sb_mc_workspace_bytes(groups, len(self.groups))
+        if nbytes == 0:
+            raise ValueError('BatchedScao: ' + (lib.sb_last_error() or b'').decode())
+        self.mc_workspace = torch.zeros(nbytes, dtype=torch.uint8, device=self.device)
+        handle = ctypes.c_void_p()
+        st = torch.cuda.current_stream(self.device).cuda_stream
+        _lib.call('sb_mc_create', groups, len(self.groups), self.mc_workspace.data_ptr(), nbytes, ctypes.byref(handle),
+                  st)
+        self._mc_groups = groups
+        self.mc_handle = handle
+        _lib.call('sb_mc_step', handle, st)       # one eager step, as capture() takes
+        torch.cuda.synchronize(self.device)
+        cap = torch.cuda.Stream(self.device)
+        g = torch.cuda.CUDAGraph(keep_graph=True)
+        with torch.cuda.graph(g, stream=cap):
+            _lib.call('sb_mc_step', handle, torch.cuda.current_stream(self.device).cuda_stream)
+        torch.cuda.synchronize(self.device)
+        self.graph = g
+        self._launches = graph_kernel_count(g)
+        return g
+
+    def step_mc(self):
+        """One Monte-Carlo step without a graph (after capture_mc)."""
+        _lib.call('sb_mc_step', self.mc_handle, torch.cuda.current_stream(self.device).cuda_stream)
+
+    def release_mc(self):
+        """Free the Monte-Carlo step's handle (the graph that replays it goes too)."""
+        h = getattr(self, 'mc_handle', None)
+        if h is not None and h.value:
+            if self.graph is not None:
+                torch.cuda.synchronize(self.device)
+                self.graph = None
+            _lib.load().sb_mc_destroy(h)
+        self.mc_handle = None
+
+    def __del__(self):
+        try:
+            self.release_mc()
+        except Exception:
+            pass
 
     def capture_plain(self):
         """Every realisation's own sequential step graph (its own

@@ -15,7 +15,7 @@ PKG = os.path.dirname(HERE)
 ROOT = os.path.dirname(PKG)
 OUT = os.path.join(PKG, 'libspecula_b200.so')
 SOURCES = ['sb_common.cu', 'sb_sh.cu', 'sb_detector.cu', 'sb_control.cu', 'sb_atmo.cu', 'sb_adjoint.cu', 'sb_psf.cu',
-           'sb_psf_tc.cu']
+           'sb_psf_tc.cu', 'sb_mc.cu']
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 
 

@@ -10,7 +10,11 @@
 // contraction); the rotation samples are evaluated as small float32 offsets
 // from the output pixel, with SciPy's exact float64 expression deciding the
 // edge test wherever it is within 1e-4 px.
+#include <new>
+#include <vector>
+
 #include "sb_common.cuh"
+#include "sb_mc.cuh"
 
 namespace {
 
@@ -139,13 +143,26 @@ struct TileFootprint {
     int br0, br1, bc0, bc1, interior;
 };
 
+// the layer a tile is cut from: its record, position, per-step parameters
+// (NULL: the record's static ones), side and the tile's origin
+struct TileSrc {
+    const sb_atmo_layer *layer;
+    const double *pos;
+    const LayerDyn *dyn;
+    int L, x0, y0;
+};
+
 template <int CAP>
-__device__ __forceinline__ void tile_footprint(const EvolveArgsT<CAP> &a, int li, LayerDyn &lyd, TileFootprint &fp) {
-    const sb_atmo_layer &lys = a.layer[li];
-    lyd = a.dyn ? a.dyn[li] : static_dyn(lys);
+__device__ __forceinline__ TileSrc tile_src(const EvolveArgsT<CAP> &a, int li) {
+    return {&a.layer[li], a.ptr[li].pos, a.dyn ? a.dyn + li : nullptr, a.L, (int)blockIdx.x * kTile,
+            (int)blockIdx.y * kTile};
+}
+
+__device__ __forceinline__ void tile_footprint(const TileSrc &src, LayerDyn &lyd, TileFootprint &fp) {
+    lyd = src.dyn ? *src.dyn : static_dyn(*src.layer);
     const LayerDyn &ly = lyd;
-    const int L = a.L;
-    const int x0 = blockIdx.x * kTile, y0 = blockIdx.y * kTile;
+    const int L = src.L;
+    const int x0 = src.x0, y0 = src.y0;
     int br0 = y0, br1 = min(y0 + kTile, L) - 1, bc0 = x0, bc1 = min(x0 + kTile, L) - 1;
     int interior = 0;
     if (ly.rotate) {
@@ -184,13 +201,12 @@ struct TileLoads {
     float w0, frac;
 };
 
-template <int CAP>
-__device__ __forceinline__ void tile_load(const EvolveArgsT<CAP> &a, int li, const LayerDyn &ly,
-                                          const TileFootprint &fp, int tid, TileLoads &t) {
-    const sb_atmo_layer &lys = a.layer[li];
-    const int L = a.L;
+__device__ __forceinline__ void tile_load(const TileSrc &src, const LayerDyn &ly, const TileFootprint &fp, int tid,
+                                          TileLoads &t) {
+    const sb_atmo_layer &lys = *src.layer;
+    const int L = src.L;
     // integer position and float32 remainder (atmo_evolution.py:278-279)
-    const double np = *a.ptr[li].pos;
+    const double np = *src.pos;
     const double q = floor(np);
     const float *row0 = lys.screen + (long long)q;
     const int ld = lys.screen_ld;
@@ -246,9 +262,8 @@ __device__ __forceinline__ void tile_stage(float (&Q)[kBox][kBox + 1], const Til
 }
 
 template <class Sink>
-__device__ __forceinline__ void tile_values(int L, const float (&Q)[kBox][kBox + 1], const LayerDyn &ly,
-                                            const TileFootprint &fp, Sink &&sink) {
-    const int x0 = blockIdx.x * kTile, y0 = blockIdx.y * kTile;
+__device__ __forceinline__ void tile_values(int L, int x0, int y0, const float (&Q)[kBox][kBox + 1],
+                                            const LayerDyn &ly, const TileFootprint &fp, Sink &&sink) {
     const int br0 = fp.br0, bc0 = fp.bc0;
     const bool interior = fp.interior != 0;
     const int x = x0 + threadIdx.x;
@@ -334,19 +349,19 @@ __device__ __forceinline__ void tile_values(int L, const float (&Q)[kBox][kBox +
     }
 }
 
-// One whole tile of layer li (every thread of the CTA must call it: it holds
-// two CTA barriers); Q, fp and lyd are the CTA's shared staging.
-template <int CAP, class Sink>
-__device__ __forceinline__ void evolve_tile(const EvolveArgsT<CAP> &a, int li, float (&Q)[kBox][kBox + 1],
-                                            TileFootprint &fp, LayerDyn &lyd, Sink &&sink) {
+// One whole tile (every thread of the CTA must call it: it holds two CTA
+// barriers); Q, fp and lyd are the CTA's shared staging.
+template <class Sink>
+__device__ __forceinline__ void evolve_tile(const TileSrc &src, float (&Q)[kBox][kBox + 1], TileFootprint &fp,
+                                            LayerDyn &lyd, Sink &&sink) {
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-    if (tid == 0) tile_footprint(a, li, lyd, fp);
+    if (tid == 0) tile_footprint(src, lyd, fp);
     __syncthreads();                      // lyd and fp written by thread 0
     TileLoads t;
-    tile_load(a, li, lyd, fp, tid, t);
+    tile_load(src, lyd, fp, tid, t);
     tile_stage(Q, t);
     __syncthreads();
-    tile_values(a.L, Q, lyd, fp, sink);
+    tile_values(src.L, src.x0, src.y0, Q, lyd, fp, sink);
 }
 
 template <int CAP>
@@ -356,7 +371,7 @@ __global__ void __launch_bounds__(256) atmo_evolve_kernel(EvolveArgsT<CAP> a) {
     __shared__ LayerDyn lyd;              // this layer's per-step parameters
     float *out = a.layer[blockIdx.z].out;
     const int L = a.L;
-    evolve_tile(a, blockIdx.z, Q, fp, lyd, [&](int, int y, int x, float v) { out[(size_t)y * L + x] = v; });
+    evolve_tile(tile_src(a, blockIdx.z), Q, fp, lyd, [&](int, int y, int x, float v) { out[(size_t)y * L + x] = v; });
 }
 
 // The on-axis propagation of pupil-sized layers fused in: blockIdx.z is a
@@ -383,21 +398,22 @@ __global__ void __launch_bounds__(256, 4) atmo_propagate_kernel(EvolveArgsT<CAP>
     const int L = a.L;
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
     const int n = f.n_atm, l0 = blockIdx.z * n;
-    if (tid < n) tile_footprint(a, l0 + tid, lyd[tid], fp[tid]);
+    if (tid < n) tile_footprint(tile_src(a, l0 + tid), lyd[tid], fp[tid]);
     float acc[kTile / kRowStep];
 #pragma unroll
     for (int j = 0; j < kTile / kRowStep; ++j) acc[j] = 0.0f;          // ElectricField.reset()
     __syncthreads();
     TileLoads t;
-    tile_load(a, l0, lyd[0], fp[0], tid, t);
+    tile_load(tile_src(a, l0), lyd[0], fp[0], tid, t);
     for (int k = 0; k < n; ++k) {
         tile_stage(Q[k & 1], t);
-        if (k + 1 < n) tile_load(a, l0 + k + 1, lyd[k + 1], fp[k + 1], tid, t);
+        if (k + 1 < n) tile_load(tile_src(a, l0 + k + 1), lyd[k + 1], fp[k + 1], tid, t);
         // staging k complete; the buffer of layer k+1 was last read at layer
         // k-1, before this barrier's predecessor
         __syncthreads();
         float *out = a.layer[l0 + k].out;
-        tile_values(L, Q[k & 1], lyd[k], fp[k], [&](int j, int y, int x, float v) {
+        tile_values(L, (int)blockIdx.x * kTile, (int)blockIdx.y * kTile, Q[k & 1], lyd[k], fp[k],
+                    [&](int j, int y, int x, float v) {
             out[(size_t)y * L + x] = v;
             acc[j] = __fadd_rn(acc[j], v);
         });
@@ -447,27 +463,33 @@ __global__ void __launch_bounds__(256) propagate_kernel(PropArgs a, float *__res
 
 namespace {
 
+// the checks every layer passes before a launch reads it
+int check_layer(const char *who, int k, const sb_atmo_layer &l, const LayerPtrs &ptr, int L, bool inputs) {
+    // the window [pos, pos + L] must stay inside the strip for every
+    // position the cycling rule allows: pos + L < screen_cols
+    if (!l.screen || !l.out || l.screen_cols < L + 1 || l.screen_ld < l.screen_cols || !ptr.pos ||
+        (!inputs && (l.rot90 < 0 || l.rot90 > 3 || !(l.delta >= 0.0))))
+        return sb::fail(SB_EINVAL, "%s: layer %d: bad screen window", who, k);
+    if (inputs && (!ptr.seeing || !ptr.wind_speed || !ptr.wind_direction))
+        return sb::fail(SB_EINVAL, "%s: layer %d: null input pointer", who, k);
+    // element offsets inside the strip window are 32-bit
+    if ((long long)L * l.screen_ld + l.screen_cols >= (1LL << 31))
+        return sb::fail(SB_ESHAPE, "%s: layer %d: strip too large", who, k);
+    // the fractional-degree rotation is below 1 degree: the staged
+    // footprint of a tile is sized for that
+    if (!inputs && l.rotate && !(fabs(l.m01) < 0.0175 && fabs(l.m10) < 0.0175 && l.m00 > 0.9998 && l.m11 > 0.9998))
+        return sb::fail(SB_EINVAL, "%s: layer %d: rotation must be below one degree", who, k);
+    return SB_OK;
+}
+
 template <int CAP>
 int launch_evolve_t(const char *who, const sb_atmo_layer *layers, const LayerPtrs *ptrs, int n_layers, int L,
                     const sb_atmo_inputs *in, LayerDyn *dyn, void *stream, const FusedPropArgs *fuse = nullptr) {
     EvolveArgsT<CAP> a;
     for (int k = 0; k < n_layers; ++k) {
-        const sb_atmo_layer &l = layers[k];
-        // the window [pos, pos + L] must stay inside the strip for every
-        // position the cycling rule allows: pos + L < screen_cols
-        if (!l.screen || !l.out || l.screen_cols < L + 1 || l.screen_ld < l.screen_cols || !ptrs[k].pos ||
-            (!in && (l.rot90 < 0 || l.rot90 > 3 || !(l.delta >= 0.0))))
-            return sb::fail(SB_EINVAL, "%s: layer %d: bad screen window", who, k);
-        if (in && (!ptrs[k].seeing || !ptrs[k].wind_speed || !ptrs[k].wind_direction))
-            return sb::fail(SB_EINVAL, "%s: layer %d: null input pointer", who, k);
-        // element offsets inside the strip window are 32-bit
-        if ((long long)L * l.screen_ld + l.screen_cols >= (1LL << 31))
-            return sb::fail(SB_ESHAPE, "%s: layer %d: strip too large", who, k);
-        // the fractional-degree rotation is below 1 degree: the staged
-        // footprint of a tile is sized for that
-        if (!in && l.rotate && !(fabs(l.m01) < 0.0175 && fabs(l.m10) < 0.0175 && l.m00 > 0.9998 && l.m11 > 0.9998))
-            return sb::fail(SB_EINVAL, "%s: layer %d: rotation must be below one degree", who, k);
-        a.layer[k] = l;
+        const int rc = check_layer(who, k, layers[k], ptrs[k], L, in != nullptr);
+        if (rc) return rc;
+        a.layer[k] = layers[k];
         a.ptr[k] = ptrs[k];
     }
     a.n = n_layers;
@@ -503,6 +525,25 @@ int launch_evolve(const char *who, const sb_atmo_layer *layers, int n_layers, in
     return launch_evolve_t<SB_MAX_LAYERS>(who, layers, ptrs, n_layers, L, in, dyn, stream);
 }
 
+// One realisation's field, elements e0, e0 + step, ... (the order of the sums
+// does not depend on the split)
+__device__ __forceinline__ void propagate_field(const float *__restrict__ at, int n_atm, long long atm_layer_stride,
+                                                const float *__restrict__ stop_A,
+                                                const float *__restrict__ stop_phase,
+                                                const float *__restrict__ dm_A, const float *__restrict__ dp, int n,
+                                                float *__restrict__ Ao, float *__restrict__ Po, int e0, int step) {
+    for (int e = e0; e < n; e += step) {
+        float amp = 1.0f, ph = 0.0f;
+        for (int k = 0; k < n_atm; ++k) ph = __fadd_rn(ph, at[k * atm_layer_stride + e]);
+        if (stop_A) amp = __fmul_rn(amp, stop_A[e]);
+        if (stop_phase) ph = __fadd_rn(ph, stop_phase[e]);
+        if (dm_A) amp = __fmul_rn(amp, dm_A[e]);
+        ph = __fadd_rn(ph, dp[e]);
+        Ao[e] = amp;
+        Po[e] = ph;
+    }
+}
+
 // Batched on-axis propagation of realisations with the same layer structure:
 // n_atm unit-amplitude turbulence layers (rows of a stack), one shared
 // amplitude/phase layer (the pupil stop) and a mirror layer with a shared
@@ -518,20 +559,9 @@ __global__ void __launch_bounds__(256) propagate_batched_kernel(const float *__r
                                                                 long long dm_stride, int n, float *__restrict__ A,
                                                                 float *__restrict__ P, long long out_stride) {
     const long long b = blockIdx.y;
-    const float *at = atm + b * atm_real_stride;
-    const float *dp = dm_phase + b * dm_stride;
-    float *Ao = A + b * out_stride;
-    float *Po = P + b * out_stride;
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
-        float amp = 1.0f, ph = 0.0f;
-        for (int k = 0; k < n_atm; ++k) ph = __fadd_rn(ph, at[k * atm_layer_stride + e]);
-        if (stop_A) amp = __fmul_rn(amp, stop_A[e]);
-        if (stop_phase) ph = __fadd_rn(ph, stop_phase[e]);
-        if (dm_A) amp = __fmul_rn(amp, dm_A[e]);
-        ph = __fadd_rn(ph, dp[e]);
-        Ao[e] = amp;
-        Po[e] = ph;
-    }
+    propagate_field(atm + b * atm_real_stride, n_atm, atm_layer_stride, stop_A, stop_phase, dm_A,
+                    dm_phase + b * dm_stride, n, A + b * out_stride, P + b * out_stride,
+                    blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 }  // namespace
@@ -651,6 +681,204 @@ extern "C" int sb_atmo_propagate_batched(const sb_atmo_layer *layers, const sb_a
     }
     return SB_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Monte-Carlo step, stages 1-3: every turbulence layer of every realisation of
+// every group.  The layer records live in the workspace; a CTA finds its
+// group from the block prefix in the kernel arguments, then its layer and
+// tile, and runs the same tile code as atmo_evolve_kernel.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct McAtmoLayer {
+    sb_atmo_layer layer;
+    LayerPtrs ptr;
+};
+
+struct McAtmoGroup {
+    sb_atmo_inputs in;               // constants (pointers unused)
+    int layer0, n_layers, L, tiles;  // first layer in the table, count, side, tiles per side
+};
+
+struct McAtmoArgs {
+    const McAtmoLayer *layers;
+    LayerDyn *dyn;
+    int n_groups, n_layers;
+    McAtmoGroup g[sb::kMcMaxGroups];
+    int blk0[sb::kMcMaxGroups + 1];  // evolve CTAs before each group
+};
+
+struct McPropGroup {
+    const float *atm;
+    long long atm_real_stride, atm_layer_stride;
+    const float *stop_A, *stop_phase, *dm_A, *dm_phase;
+    long long dm_stride;
+    float *A, *P;
+    long long out_stride;
+    int n_atm, n;
+};
+
+struct McPropArgs {
+    int n_groups;
+    McPropGroup g[sb::kMcMaxGroups];
+    int real0[sb::kMcMaxGroups + 1];  // realisations before each group
+};
+
+struct McAtmoBlob {
+    McAtmoArgs atmo;
+    McPropArgs prop;
+    int evolve_blocks, prop_blocks, n_real;
+};
+
+__global__ void __launch_bounds__(256) mc_atmo_advance_kernel(McAtmoArgs a) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.n_layers) return;
+    int g = 0;
+    while (g + 1 < a.n_groups && k >= a.g[g + 1].layer0) ++g;
+    const McAtmoLayer &ly = a.layers[k];
+    const int L = a.g[g].L;
+    // as atmo_advance_kernel with device inputs
+    const LayerDyn d = layer_dyn(a.g[g].in, ly.ptr, L);
+    a.dyn[k] = d;
+    double *pos = ly.ptr.pos;
+    double np = __dadd_rn(*pos, d.delta);
+    if (__dadd_rn(np, (double)L) >= (double)ly.layer.screen_cols) np = 0.0;
+    *pos = np;
+}
+
+__global__ void __launch_bounds__(256) mc_atmo_evolve_kernel(McAtmoArgs a) {
+    __shared__ float Q[kBox][kBox + 1];
+    __shared__ TileFootprint fp;
+    __shared__ LayerDyn lyd;
+    const int blk = blockIdx.x;
+    int g = 0;
+    while (g + 1 < a.n_groups && blk >= a.blk0[g + 1]) ++g;
+    const int tiles = a.g[g].tiles, L = a.g[g].L;
+    const int t2 = tiles * tiles, local = blk - a.blk0[g];
+    const int kl = local / t2, tt = local - kl * t2;
+    const int ty = tt / tiles, tx = tt - ty * tiles;
+    const int li = a.g[g].layer0 + kl;
+    const McAtmoLayer &ly = a.layers[li];
+    const TileSrc src{&ly.layer, ly.ptr.pos, a.dyn + li, L, tx * kTile, ty * kTile};
+    float *out = ly.layer.out;
+    evolve_tile(src, Q, fp, lyd, [&](int, int y, int x, float v) { out[(size_t)y * L + x] = v; });
+}
+
+__global__ void __launch_bounds__(256) mc_propagate_kernel(McPropArgs a) {
+    const int r = blockIdx.y;
+    int g = 0;
+    while (g + 1 < a.n_groups && r >= a.real0[g + 1]) ++g;
+    const McPropGroup &G = a.g[g];
+    const long long b = r - a.real0[g];
+    propagate_field(G.atm ? G.atm + b * G.atm_real_stride : nullptr, G.n_atm, G.atm_layer_stride, G.stop_A,
+                    G.stop_phase, G.dm_A, G.dm_phase + b * G.dm_stride, G.n, G.A + b * G.out_stride,
+                    G.P + b * G.out_stride, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
+}  // namespace
+
+namespace sb {
+
+size_t mc_atmo_workspace(const sb_mc_group *gs, int n) {
+    size_t nl = 0;
+    for (int g = 0; g < n; ++g) nl += (size_t)gs[g].n_batch * gs[g].n_atm;
+    return mc_align(nl * sizeof(McAtmoLayer)) + mc_align(nl * sizeof(LayerDyn));
+}
+
+int mc_atmo_prepare(const sb_mc_group *gs, int n, void *ws, McBlob &blob, cudaStream_t st) {
+    static_assert(sizeof(McAtmoBlob) <= sizeof(McBlob), "atmosphere stage arguments exceed the blob");
+    static_assert(sizeof(McAtmoArgs) <= 4096 && sizeof(McPropArgs) <= 4096, "kernel arguments above 4 KB");
+    const char *who = "sb_mc_create";
+    McAtmoBlob *B = new (blob.b) McAtmoBlob();
+    size_t nl = 0;
+    for (int g = 0; g < n; ++g) nl += (size_t)gs[g].n_batch * gs[g].n_atm;
+    std::vector<McAtmoLayer> tab(nl);
+    McAtmoArgs &a = B->atmo;
+    McPropArgs &p = B->prop;
+    a.layers = static_cast<const McAtmoLayer *>(ws);
+    a.dyn = reinterpret_cast<LayerDyn *>(static_cast<unsigned char *>(ws) + mc_align(nl * sizeof(McAtmoLayer)));
+    a.n_groups = p.n_groups = n;
+    a.n_layers = (int)nl;
+    int k = 0, blocks = 0, real = 0, max_n = 1;
+    for (int g = 0; g < n; ++g) {
+        const sb_mc_group &G = gs[g];
+        const int L = G.L, cnt = G.n_batch * G.n_atm;
+        const sb_atmo_inputs &in = G.constants;
+        if (!(in.pixel_pitch > 0.0) || !(in.delta_time >= 0.0) || L < 1 || G.n_atm < 0 || (cnt && (!G.layers || !G.inputs)))
+            return fail(SB_EINVAL, "%s: group %d: bad atmosphere", who, g);
+        const int tiles = (L + kTile - 1) / kTile;
+        a.g[g].in = in;
+        a.g[g].layer0 = k;
+        a.g[g].n_layers = cnt;
+        a.g[g].L = L;
+        a.g[g].tiles = tiles;
+        a.blk0[g] = blocks;
+        for (int j = 0; j < cnt; ++j, ++k) {
+            const sb_atmo_layer_inputs &li = G.inputs[j];
+            tab[k].layer = G.layers[j];
+            tab[k].ptr.seeing = li.seeing;
+            tab[k].ptr.wind_speed = li.wind_speed;
+            tab[k].ptr.wind_direction = li.wind_direction;
+            tab[k].ptr.pos = li.position;
+            const int rc = check_layer(who, j, tab[k].layer, tab[k].ptr, L, true);
+            if (rc) return rc;
+            // the layers are the rows of atm, as the propagation reads them
+            const float *want = G.atm + (j / G.n_atm) * G.atm_real_stride + (long long)(j % G.n_atm) * L * L;
+            if (tab[k].layer.out != want)
+                return fail(SB_EINVAL, "%s: group %d: layer %d does not write its row of atm", who, g, j);
+        }
+        blocks += cnt * tiles * tiles;
+        McPropGroup &q = p.g[g];
+        const long long nn = (long long)L * L;
+        if (!G.dm_phase || !G.field_A || !G.field_phase || G.dm_stride < nn || G.field_stride < nn ||
+            (G.n_atm > 0 && (!G.atm || G.atm_real_stride < G.n_atm * nn)))
+            return fail(SB_EINVAL, "%s: group %d: bad propagation buffers", who, g);
+        q.atm = G.atm;
+        q.atm_real_stride = G.atm_real_stride;
+        q.atm_layer_stride = nn;
+        q.stop_A = G.stop_A;
+        q.stop_phase = G.stop_phase;
+        q.dm_A = G.dm_A;
+        q.dm_phase = G.dm_phase;
+        q.dm_stride = G.dm_stride;
+        q.A = G.field_A;
+        q.P = G.field_phase;
+        q.out_stride = G.field_stride;
+        q.n_atm = G.n_atm;
+        q.n = (int)nn;
+        p.real0[g] = real;
+        real += G.n_batch;
+        max_n = nn > max_n ? (int)nn : max_n;
+    }
+    a.blk0[n] = blocks;
+    p.real0[n] = real;
+    B->evolve_blocks = blocks;
+    B->n_real = real;
+    const int nblk = (max_n + 255) / 256;
+    B->prop_blocks = nblk > 296 ? 296 : nblk;
+    if (real > 65535) return fail(SB_ESHAPE, "%s: at most 65535 realisations", who);
+    if (nl) {
+        const cudaError_t e = cudaMemcpyAsync(ws, tab.data(), nl * sizeof(McAtmoLayer), cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return fail(SB_ECUDA, "%s: layer table copy: %s", who, cudaGetErrorString(e));
+    }
+    return SB_OK;
+}
+
+int mc_atmo_launch(const McBlob &blob, cudaStream_t st) {
+    const McAtmoBlob *B = reinterpret_cast<const McAtmoBlob *>(blob.b);
+    if (B->atmo.n_layers > 0) {
+        mc_atmo_advance_kernel<<<(B->atmo.n_layers + 255) / 256, 256, 0, st>>>(B->atmo);
+        int rc = check_launch("mc_atmo_advance_kernel");
+        if (rc) return rc;
+        mc_atmo_evolve_kernel<<<B->evolve_blocks, dim3(32, kRowStep), 0, st>>>(B->atmo);
+        rc = check_launch("mc_atmo_evolve_kernel");
+        if (rc) return rc;
+    }
+    mc_propagate_kernel<<<dim3(B->prop_blocks, B->n_real), 256, 0, st>>>(B->prop);
+    return check_launch("mc_propagate_kernel");
+}
+
+}  // namespace sb
 
 namespace {
 struct PropSampArgs {

@@ -7,7 +7,11 @@
 // DM projection streams the influence functions through shared memory with
 // 2-D TMA loads.  Sums run in a fixed order, so results are bit-reproducible
 // run to run.
+#include <new>
+#include <vector>
+
 #include "sb_common.cuh"
+#include "sb_mc.cuh"
 #include "sb_tma.cuh"
 
 namespace {
@@ -541,12 +545,11 @@ size_t dm_c4_smem_bytes(int nmodes, int nb_max) {
     return 1024 + (size_t)kDbStages * kDmRows * kDmCols * 4 + 2 * kDbStages * 8 + (size_t)nst * rows * nb_max * 4;
 }
 
+// the tiles bid, bid + nblk, ... of the columns
 template <int NB, int NBX>
-__global__ void __launch_bounds__(32 * (2 * NBX + 1), 1)
-    dm_project_batched_c4_kernel(const __grid_constant__ CUtensorMap map, int nmodes, int nvalid,
-                                 const float *__restrict__ cmd, int ldc, int nb, float sign,
-                                 const int32_t *__restrict__ idx, float *__restrict__ phase,
-                                 long long phase_stride) {
+__device__ __forceinline__ void dm_c4_body(const CUtensorMap &map, int nmodes, int nvalid, const float *__restrict__ cmd,
+                                           int ldc, int nb, float sign, const int32_t *__restrict__ idx,
+                                           float *__restrict__ phase, long long phase_stride, int bid, int nblk) {
     static_assert(NB % 4 == 0 && (NBX == 1 || NBX == 2 || NBX == 4), "NB multiple of 4, 1/2/4 boxes per stage");
     constexpr int NCW = 2 * NBX;                  // consumer warps: 128 columns each
     constexpr int ROWS = kDmRows / NBX;           // mode rows per stage
@@ -576,7 +579,6 @@ __global__ void __launch_bounds__(32 * (2 * NBX + 1), 1)
     }
     __syncthreads();
     const int ntiles = (nvalid + TW - 1) / TW;
-    const int bid = blockIdx.x, nblk = gridDim.x;
     const int my_tiles = bid < ntiles ? (ntiles - 1 - bid) / nblk + 1 : 0;
     const int total = my_tiles * nst;
     if (warp == NCW) {
@@ -661,6 +663,16 @@ __global__ void __launch_bounds__(32 * (2 * NBX + 1), 1)
     }
 }
 
+template <int NB, int NBX>
+__global__ void __launch_bounds__(32 * (2 * NBX + 1), 1)
+    dm_project_batched_c4_kernel(const __grid_constant__ CUtensorMap map, int nmodes, int nvalid,
+                                 const float *__restrict__ cmd, int ldc, int nb, float sign,
+                                 const int32_t *__restrict__ idx, float *__restrict__ phase,
+                                 long long phase_stride) {
+    dm_c4_body<NB, NBX>(map, nmodes, nvalid, cmd, ldc, nb, sign, idx, phase, phase_stride, blockIdx.x, gridDim.x);
+}
+
+
 // modes_b[m] = sum_j R[m][j] s_b[j] for b < NB.  A CTA of 256 threads takes
 // RB reconstructor rows; each thread walks the slope index in pairs (8-byte
 // loads when the strides allow), loads the NB slope pairs once and uses them
@@ -668,12 +680,12 @@ __global__ void __launch_bounds__(32 * (2 * NBX + 1), 1)
 // HBM once.  Per (row, vector): warp sums, then a fixed-order sum over the
 // 8 warps (deterministic).  RB (1, 2, 4) is the SB_TUNE_MODALREC_BATCHED
 // variant.
-template <int NB, int RB>
-__global__ void __launch_bounds__(256) gemv_rows_batched_kernel(const float *__restrict__ R, int nrows, int ncols,
-                                                                int ldr, const float *__restrict__ S, int lds,
-                                                                int nb, float *__restrict__ M, int ldm, int vec2) {
+// rows m0 .. m0 + RB - 1; epi(m, b, t) receives each finished sum
+template <int NB, int RB, class Epi>
+__device__ __forceinline__ void gemv_rows_batched_body(const float *__restrict__ R, int nrows, int ncols, int ldr,
+                                                       const float *__restrict__ S, int lds, int nb, int vec2, int m0,
+                                                       Epi &&epi) {
     __shared__ float red[RB * NB][9];
-    const int m0 = blockIdx.x * RB;
     float acc[RB][NB];
 #pragma unroll
     for (int r = 0; r < RB; ++r)
@@ -718,12 +730,254 @@ __global__ void __launch_bounds__(256) gemv_rows_batched_kernel(const float *__r
         if (m0 + r < nrows && b < nb) {
             float t = 0.f;
             for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[e][w];
-            M[(size_t)b * ldm + m0 + r] = t;
+            epi(m0 + r, b, t);
         }
     }
 }
 
+template <int NB, int RB>
+__global__ void __launch_bounds__(256) gemv_rows_batched_kernel(const float *__restrict__ R, int nrows, int ncols,
+                                                                int ldr, const float *__restrict__ S, int lds,
+                                                                int nb, float *__restrict__ M, int ldm, int vec2) {
+    gemv_rows_batched_body<NB, RB>(R, nrows, ncols, ldr, S, lds, nb, vec2, blockIdx.x * RB,
+                                   [&](int m, int b, float t) { M[(size_t)b * ldm + m] = t; });
+}
+
 }  // namespace
+
+// ---------------------------------------------------------------------------
+// Monte-Carlo step, stages 6-7.  Realisations go in chunks of up to 16
+// (a job): the reconstructor launch gives every job ceil(n_modes / 2) CTAs of
+// gemv_rows_batched_body followed by the group's integrator update of each
+// finished mode; the mirror launch shares the SMs among the jobs so that the
+// busiest CTA streams the fewest influence-function rows, each CTA running
+// the register-blocked TMA projection (4 boxes per stage) over its job's
+// tiles.  The sums are those of sb_modalrec_batched, sb_integrator and
+// sb_dm_project_batched with one mode-row group.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kMcRecRows = 2;          // reconstructor rows per CTA
+constexpr int kMcChunk = 16;           // realisations per job
+constexpr int kMcDmNbx = 4;            // boxes per mirror stage
+
+struct McRecJob {
+    const float *R, *S;
+    float *M;
+    int nrows, ncols, ldr, lds, ldm, nb, vec2, g, e0;
+};
+
+struct McRecArgs {
+    const McRecJob *jobs;
+    const int2 *blk;                   // per CTA: job, row block
+    sb_iir_plan iir[sb::kMcMaxGroups];
+    float *out[sb::kMcMaxGroups];
+};
+
+struct McDmJob {
+    const float *cmd;
+    const int32_t *idx;
+    float *phase;
+    long long phase_stride;
+    int ldc, nb, nmodes, nvalid, g, cta0, ncta;
+    float sign;
+};
+
+struct McDmArgs {
+    CUtensorMap map[sb::kMcMaxGroups];
+    const McDmJob *jobs;
+    const int *cta_job;
+};
+
+struct McRecBlob {
+    McRecArgs args;
+    int blocks;
+};
+
+struct McDmBlob {
+    McDmArgs args;
+    int blocks;
+    size_t smem;
+};
+
+template <int NB>
+__device__ __forceinline__ void mc_rec_job(const McRecJob &J, int m0, const sb_iir_plan &p, float *out) {
+    gemv_rows_batched_body<NB, kMcRecRows>(J.R, J.nrows, J.ncols, J.ldr, J.S, J.lds, J.nb, J.vec2, m0,
+                                           [&](int m, int b, float t) {
+                                               J.M[(size_t)b * J.ldm + m] = t;
+                                               iir_update(p, J.e0 + b * J.nrows + m, t, out);
+                                           });
+}
+
+__global__ void __launch_bounds__(256) mc_rec_kernel(McRecArgs m) {
+    const int2 jb = m.blk[blockIdx.x];
+    const McRecJob &J = m.jobs[jb.x];
+    const int m0 = jb.y * kMcRecRows;
+    const sb_iir_plan &p = m.iir[J.g];
+    float *out = m.out[J.g];
+    if (J.nb <= 4) mc_rec_job<4>(J, m0, p, out);
+    else if (J.nb <= 8) mc_rec_job<8>(J, m0, p, out);
+    else mc_rec_job<16>(J, m0, p, out);
+}
+
+__global__ void __launch_bounds__(32 * (2 * kMcDmNbx + 1), 1) mc_dm_kernel(const __grid_constant__ McDmArgs m) {
+    const McDmJob &J = m.jobs[m.cta_job[blockIdx.x]];
+    const int bid = blockIdx.x - J.cta0;
+    if (J.nb <= 8)
+        dm_c4_body<8, kMcDmNbx>(m.map[J.g], J.nmodes, J.nvalid, J.cmd, J.ldc, J.nb, J.sign, J.idx, J.phase,
+                                J.phase_stride, bid, J.ncta);
+    else
+        dm_c4_body<16, kMcDmNbx>(m.map[J.g], J.nmodes, J.nvalid, J.cmd, J.ldc, J.nb, J.sign, J.idx, J.phase,
+                                 J.phase_stride, bid, J.ncta);
+}
+
+int mc_jobs(const sb_mc_group *gs, int n) {
+    int j = 0;
+    for (int g = 0; g < n; ++g) j += (gs[g].n_batch + kMcChunk - 1) / kMcChunk;
+    return j;
+}
+
+int mc_rec_blocks(const sb_mc_group *gs, int n) {
+    int b = 0;
+    for (int g = 0; g < n; ++g)
+        b += ((gs[g].n_batch + kMcChunk - 1) / kMcChunk) * ((gs[g].n_modes + kMcRecRows - 1) / kMcRecRows);
+    return b;
+}
+
+}  // namespace
+
+namespace sb {
+
+size_t mc_control_workspace(const sb_mc_group *gs, int n) {
+    const size_t nj = mc_jobs(gs, n);
+    return mc_align(nj * sizeof(McRecJob)) + mc_align((size_t)mc_rec_blocks(gs, n) * sizeof(int2)) +
+           mc_align(nj * sizeof(McDmJob)) + mc_align((size_t)sm_count() * sizeof(int));
+}
+
+int mc_control_prepare(const sb_mc_group *gs, int n, void *ws, McBlob &rec, McBlob &dm, cudaStream_t st) {
+    static_assert(sizeof(McRecBlob) <= sizeof(McBlob) && sizeof(McDmBlob) <= sizeof(McBlob),
+                  "control stage arguments exceed the blob");
+    static_assert(sizeof(McRecArgs) <= 4096 && sizeof(McDmArgs) <= 4096, "kernel arguments above 4 KB");
+    const char *who = "sb_mc_create";
+    McRecBlob *RB = new (rec.b) McRecBlob();
+    McDmBlob *DB = new (dm.b) McDmBlob();
+    const int nj = mc_jobs(gs, n), nblk_rec = mc_rec_blocks(gs, n), nsm = sm_count();
+    if (nj > nsm) return fail(SB_ESHAPE, "%s: %d realisation chunks for %d SMs", who, nj, nsm);
+    std::vector<McRecJob> rj(nj);
+    std::vector<int2> rb(nblk_rec);
+    std::vector<McDmJob> dj(nj);
+    std::vector<int> tiles(nj), ncta(nj, 1);
+    unsigned char *w = static_cast<unsigned char *>(ws);
+    McRecJob *d_rj = reinterpret_cast<McRecJob *>(w);
+    w += mc_align(nj * sizeof(McRecJob));
+    int2 *d_rb = reinterpret_cast<int2 *>(w);
+    w += mc_align((size_t)nblk_rec * sizeof(int2));
+    McDmJob *d_dj = reinterpret_cast<McDmJob *>(w);
+    w += mc_align(nj * sizeof(McDmJob));
+    int *d_cta = reinterpret_cast<int *>(w);
+    constexpr int TW = kDmCols * kMcDmNbx;
+    int j = 0, blk = 0;
+    size_t smem = 0;
+    for (int g = 0; g < n; ++g) {
+        const sb_mc_group &G = gs[g];
+        const int nm = G.n_modes;
+        if (!G.R || !G.modes || !G.commands || !G.ifunc || !G.mask_idx || nm < 1 || G.n_slopes < 1 ||
+            G.ldr < G.n_slopes || G.n_slopes > G.slopes_stride || G.iir.n != G.n_batch * nm)
+            return fail(SB_EINVAL, "%s: group %d: bad reconstructor / integrator", who, g);
+        if (nm > kDbMaxModes) return fail(SB_ESHAPE, "%s: group %d: at most %d modes", who, g, kDbMaxModes);
+        if (G.n_valid < 1 || G.ld_if < G.n_valid || G.ld_if % 4 || (uintptr_t)G.ifunc % 16)
+            return fail(SB_EINVAL, "%s: group %d: influence functions need 16-byte aligned rows", who, g);
+        RB->args.iir[g] = G.iir;
+        RB->args.out[g] = G.commands;
+        int rc = tensor_map_2d_f32(&DB->args.map[g], G.ifunc, nm, G.ld_if, G.ld_if, kDmRows / kMcDmNbx, kDmCols);
+        if (rc) return rc;
+        const int vec2 = (G.ldr % 2 == 0) && (G.slopes_stride % 2 == 0) && ((uintptr_t)G.R % 8 == 0) &&
+                         ((uintptr_t)G.slopes % 8 == 0);
+        for (int b0 = 0; b0 < G.n_batch; b0 += kMcChunk, ++j) {
+            const int nb = G.n_batch - b0 < kMcChunk ? G.n_batch - b0 : kMcChunk;
+            McRecJob &r = rj[j];
+            r.R = G.R;
+            r.S = G.slopes + (size_t)b0 * G.slopes_stride;
+            r.M = G.modes + (size_t)b0 * nm;
+            r.nrows = nm;
+            r.ncols = G.n_slopes;
+            r.ldr = G.ldr;
+            r.lds = G.slopes_stride;
+            r.ldm = nm;
+            r.nb = nb;
+            r.vec2 = vec2;
+            r.g = g;
+            r.e0 = b0 * nm;
+            for (int k = 0; k < (nm + kMcRecRows - 1) / kMcRecRows; ++k) rb[blk++] = make_int2(j, k);
+            McDmJob &d = dj[j];
+            d.cmd = G.commands + (size_t)b0 * nm;
+            d.idx = G.mask_idx;
+            d.phase = G.dm_phase + (size_t)b0 * G.dm_stride;
+            d.phase_stride = G.dm_stride;
+            d.ldc = nm;
+            d.nb = nb;
+            d.nmodes = nm;
+            d.nvalid = G.n_valid;
+            d.g = g;
+            d.sign = G.dm_sign;
+            tiles[j] = (G.n_valid + TW - 1) / TW;
+            const size_t sm = nb <= 8 ? dm_c4_smem_bytes<kMcDmNbx>(nm, 8) : dm_c4_smem_bytes<kMcDmNbx>(nm, 16);
+            smem = sm > smem ? sm : smem;
+        }
+    }
+    // SMs to jobs: each added CTA goes to the job whose busiest CTA streams
+    // the most influence-function rows (tiles per CTA x modes)
+    for (int left = nsm - nj; left > 0; --left) {
+        int best = -1;
+        long long worst = 0;
+        for (int k = 0; k < nj; ++k) {
+            if (ncta[k] >= tiles[k]) continue;
+            const long long c = (long long)((tiles[k] + ncta[k] - 1) / ncta[k]) * dj[k].nmodes;
+            if (c > worst) {
+                worst = c;
+                best = k;
+            }
+        }
+        if (best < 0) break;
+        ++ncta[best];
+    }
+    std::vector<int> cta_job;
+    for (int k = 0; k < nj; ++k) {
+        dj[k].cta0 = (int)cta_job.size();
+        dj[k].ncta = ncta[k];
+        for (int c = 0; c < ncta[k]; ++c) cta_job.push_back(k);
+    }
+    RB->args.jobs = d_rj;
+    RB->args.blk = d_rb;
+    RB->blocks = nblk_rec;
+    DB->args.jobs = d_dj;
+    DB->args.cta_job = d_cta;
+    DB->blocks = (int)cta_job.size();
+    DB->smem = smem;
+    cudaError_t e = cudaMemcpyAsync(d_rj, rj.data(), nj * sizeof(McRecJob), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_rb, rb.data(), nblk_rec * sizeof(int2), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_dj, dj.data(), nj * sizeof(McDmJob), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_cta, cta_job.data(), cta_job.size() * sizeof(int), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(mc_dm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return fail(SB_ECUDA, "%s: control tables: %s", who, cudaGetErrorString(e));
+    return SB_OK;
+}
+
+int mc_rec_launch(const McBlob &blob, cudaStream_t st) {
+    const McRecBlob *B = reinterpret_cast<const McRecBlob *>(blob.b);
+    mc_rec_kernel<<<B->blocks, 256, 0, st>>>(B->args);
+    return check_launch("mc_rec_kernel");
+}
+
+int mc_dm_launch(const McBlob &blob, cudaStream_t st) {
+    const McDmBlob *B = reinterpret_cast<const McDmBlob *>(blob.b);
+    mc_dm_kernel<<<B->blocks, 32 * (2 * kMcDmNbx + 1), B->smem, st>>>(B->args);
+    return check_launch("mc_dm_kernel");
+}
+
+}  // namespace sb
 
 extern "C" int sb_device_status(void) {
     int v = 0;

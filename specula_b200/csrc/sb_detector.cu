@@ -13,7 +13,10 @@
 // its pixels through the index table and reduces flux, denominator and the
 // two weighted sums; a second kernel applies the 1e-3*mean cut-off that
 // needs the mean over all sub-apertures, in a fixed order.
+#include <new>
+
 #include "sb_common.cuh"
+#include "sb_mc.cuh"
 
 namespace {
 
@@ -638,15 +641,36 @@ struct ChainArgs {
     float *slopes, *flux, *tot, *sxn, *syn;
 };
 
-__global__ void __launch_bounds__(kChainMaxThreads) sh_ccd_slopec_kernel(ChainArgs a) {
+// element offsets of a CTA's realisation in the buffers of ChainArgs
+struct ChainOff {
+    long long frame;
+    size_t part, slopes, flux, work;
+};
+
+// where a CTA's realisation keeps its seeds and completion counters
+struct ChainSlot {
+    const uint64_t *photon_seed, *readout_seed;  // NULL: the parameters' seeds
+    unsigned int *real_done;    // NULL: the frame state's counter serves the whole launch
+    unsigned int real_ctas;     // CTAs of the realisation
+    unsigned int group_ctas;    // CTAs sharing the frame state
+};
+
+// the chain for lenslet block (bx, by) of one realisation; any CTA size from
+// 256 to 512 threads gives the same bits
+__device__ __forceinline__ void chain_body(const ChainArgs &a, const ChainOff &o, int bx, int by,
+                                           const ChainSlot &slot) {
     __shared__ double dred[33];
     __shared__ float logfact[32];
     __shared__ int s_idx[kChainMaxThreads];
     __shared__ float s_mean[kChainMaxThreads];
     __shared__ int s_small[kChainMaxThreads / 32];
     __shared__ float tile[kChainMaxNpx * kChainLenses * kChainMaxNpx];
-    __shared__ int s_last;
+    __shared__ int s_last, s_group_last;
     const sb_ccd_params &p = a.p;
+    const float *part_I = a.part_I + o.part, *part_A = a.part_A + o.part;
+    float *I = a.I + o.frame, *integ = a.integ + o.frame, *pix = a.pix + o.frame;
+    float *slopes = a.slopes + o.slopes, *flux = a.flux + o.flux;
+    float *tot = a.tot + o.work, *sxn = a.sxn + o.work, *syn = a.syn + o.work;
     volatile sb_ccd_state *vs = p.state;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid < 32) logfact[tid] = c_logfact[tid];
@@ -660,15 +684,15 @@ __global__ void __launch_bounds__(kChainMaxThreads) sh_ccd_slopec_kernel(ChainAr
     double si = 0.0, sa = 0.0;
     if (tid < kChainSumThreads)
         for (int e = tid; e < a.nparts; e += kChainSumThreads) {
-            si += a.part_I[e];
-            sa += a.part_A[e];
+            si += part_I[e];
+            sa += part_A[e];
         }
     si = sb::block_sum_all_d(si, dred);
     sa = sb::block_sum_all_d(sa, dred);
     const float phot = (float)(a.photon_scale * sa);
     const float scale = phot / (float)si;
 
-    const int i = blockIdx.y, j0 = blockIdx.x * kChainLenses;
+    const int i = by, j0 = bx * kChainLenses;
     const int w = min(kChainLenses, a.n - j0);
     const int npx = a.npx, wc = w * npx, P = npx * wc, tld = kChainLenses * npx;
     // detector: every pass samples up to blockDim pixels of the tile (one pass
@@ -681,9 +705,9 @@ __global__ void __launch_bounds__(kChainMaxThreads) sh_ccd_slopec_kernel(ChainAr
         if (valid) {
             const int r = q / wc, c = q - r * wc;
             const int e = (i * npx + r) * a.side + j0 * npx + c;
-            const float v = a.I[e] * scale;
-            a.I[e] = v;
-            f = __fadd_rn(a.integ[e], __fmul_rn(v, p.rate));           // ccd.py:205
+            const float v = I[e] * scale;
+            I[e] = v;
+            f = __fadd_rn(integ[e], __fmul_rn(v, p.rate));           // ccd.py:205
             if (p.qe != 1.0f) f = __fmul_rn(f, p.qe);                  // ccd.py:282-287
             if (p.qe_map) f = __fmul_rn(f, p.qe_map[e]);
             f = __fadd_rn(f, p.bg_plus_dark);                           // ccd.py:220-221
@@ -713,9 +737,10 @@ __global__ void __launch_bounds__(kChainMaxThreads) sh_ccd_slopec_kernel(ChainAr
         if (qi >= 0) {
             const int r = qi / wc, c = qi - r * wc;
             const int e = (i * npx + r) * a.side + j0 * npx + c;
-            const float v = ccd_sample(p, fi, e, frame, nullptr, nullptr, p.n_pixels, logfact, inv_gain, gain_pow2);
-            a.pix[e] = v;
-            a.integ[e] = 0.0f;                                          // ccd.py:216
+            const float v = ccd_sample(p, fi, e, frame, slot.photon_seed, slot.readout_seed, p.n_pixels, logfact,
+                                       inv_gain, gain_pow2);
+            pix[e] = v;
+            integ[e] = 0.0f;                                          // ccd.py:216
             tile[r * tld + c] = v;
         }
     }
@@ -741,29 +766,41 @@ __global__ void __launch_bounds__(kChainMaxThreads) sh_ccd_slopec_kernel(ChainAr
             x = sb::warp_sum(x);
             y = sb::warp_sum(y);
             if (lane == 0) {
-                a.flux[s] = fl;
-                a.tot[s] = t;
-                a.sxn[s] = x;
-                a.syn[s] = y;
+                flux[s] = fl;
+                tot[s] = t;
+                sxn[s] = x;
+                syn[s] = y;
                 const float fac = 1.0f / t;
-                a.slopes[s] = x * fac;
-                a.slopes[a.n_valid + s] = y * fac;
+                slopes[s] = x * fac;
+                slopes[a.n_valid + s] = y * fac;
             }
         }
     }
 
-    // the last CTA to finish: frame state, then the flux cut-off
+    // the last CTA sharing the frame state advances it; the last CTA of the
+    // realisation applies the flux cut-off
     __threadfence();
     __syncthreads();
-    if (tid == 0) s_last = atomicAdd(&p.state->blocks_done, 1u) == gridDim.x * gridDim.y - 1u;
+    if (tid == 0) {
+        if (!slot.real_done) {
+            s_last = s_group_last = atomicAdd(&p.state->blocks_done, 1u) == slot.group_ctas - 1u;
+        } else {
+            s_last = atomicAdd(slot.real_done, 1u) == slot.real_ctas - 1u;
+            s_group_last = atomicAdd(&p.state->blocks_done, 1u) == slot.group_ctas - 1u;
+        }
+    }
     __syncthreads();
+    if (s_group_last) {
+        __threadfence();
+        if (tid == 0) {
+            vs->n_integrated = 0;
+            vs->frame_index = frame + 1;
+            vs->blocks_done = 0u;
+        }
+    }
     if (!s_last) return;
     __threadfence();
-    if (tid == 0) {
-        vs->n_integrated = 0;
-        vs->frame_index = frame + 1;
-        vs->blocks_done = 0u;
-    }
+    if (slot.real_done && tid == 0) *slot.real_done = 0u;
     // mean of the denominators as slopec_finish_kernel forms it: partials of 8
     // consecutive sub-apertures (slopec_sums_kernel's CTAs), summed in float
     // in warp order, then in float64 over 256 threads (sh_slopec.py:393-400)
@@ -774,7 +811,7 @@ __global__ void __launch_bounds__(kChainMaxThreads) sh_ccd_slopec_kernel(ChainAr
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
             const int s = 8 * g + k;
-            b += s < nv ? __ldcg(a.tot + s) : 0.f;
+            b += s < nv ? __ldcg(tot + s) : 0.f;
         }
         acc += b;
     }
@@ -782,12 +819,17 @@ __global__ void __launch_bounds__(kChainMaxThreads) sh_ccd_slopec_kernel(ChainAr
     const float mean = (float)(acc / nv);
     const float cut = 1.0f / (mean * 1e-3f);
     for (int s = tid; s < nv; s += nthr) {
-        const float fac = 1.0f / __ldcg(a.tot + s);
+        const float fac = 1.0f / __ldcg(tot + s);
         if (fac > cut) {
-            a.slopes[s] = __ldcg(a.sxn + s) * 0.0f;
-            a.slopes[nv + s] = __ldcg(a.syn + s) * 0.0f;
+            slopes[s] = __ldcg(sxn + s) * 0.0f;
+            slopes[nv + s] = __ldcg(syn + s) * 0.0f;
         }
     }
+}
+
+__global__ void __launch_bounds__(kChainMaxThreads) sh_ccd_slopec_kernel(ChainArgs a) {
+    const unsigned int ctas = gridDim.x * gridDim.y;
+    chain_body(a, ChainOff{0, 0, 0, 0, 0}, blockIdx.x, blockIdx.y, ChainSlot{nullptr, nullptr, nullptr, ctas, ctas});
 }
 
 }  // namespace
@@ -1006,6 +1048,151 @@ extern "C" int sb_sh_ccd_slopec(const sb_sh_plan *sh, int dft_mode, const float 
     sh_ccd_slopec_kernel<<<grid, chain_threads(npx), 0, sb::as_stream(stream)>>>(a);
     return sb::check_launch("sh_ccd_slopec_kernel");
 }
+
+// ---------------------------------------------------------------------------
+// Monte-Carlo step, stage 5: the chain of every realisation of every group in
+// one launch.  A CTA finds its group, realisation and lenslet block from the
+// flat block index; realisation b draws with its own seeds, keeps its own
+// completion counter (the flux cut-off), and the group's CTAs share the
+// group's frame state, as sb_ccd_step_batched does.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct McChainGroup {
+    ChainArgs a;                     // realisation 0
+    long long frame_stride;
+    const uint64_t *photon_seeds, *readout_seeds;
+    unsigned int *done;              // [n_batch] realisation counters
+    int gx, gy, slopes_stride, flux_stride;
+};
+
+struct McChainArgs {
+    int n_groups;
+    McChainGroup g[sb::kMcMaxGroups];
+    int blk0[sb::kMcMaxGroups + 1];
+};
+
+struct McChainBlob {
+    McChainArgs args;
+    int blocks, threads;
+};
+
+__global__ void __launch_bounds__(kChainMaxThreads, 2) mc_chain_kernel(McChainArgs m) {
+    // the group's arguments staged in shared memory: read there on use, not
+    // held in registers
+    __shared__ __align__(16) McChainGroup G;
+    static_assert(sizeof(McChainGroup) % 4 == 0, "staged as words");
+    const int bi = blockIdx.x;
+    int g = 0;
+    while (g + 1 < m.n_groups && bi >= m.blk0[g + 1]) ++g;
+    {
+        const uint32_t *src = reinterpret_cast<const uint32_t *>(&m.g[g]);
+        uint32_t *dst = reinterpret_cast<uint32_t *>(&G);
+        for (int k = threadIdx.x; k < (int)(sizeof(McChainGroup) / 4); k += blockDim.x) dst[k] = src[k];
+    }
+    __syncthreads();
+    const int per = G.gx * G.gy, local = bi - m.blk0[g];
+    const int b = local / per, rem = local - b * per;
+    const ChainOff off{(long long)b * G.frame_stride, (size_t)b * G.a.nparts, (size_t)b * G.slopes_stride,
+                       (size_t)b * G.flux_stride, (size_t)b * 3 * G.a.n_valid};
+    const ChainSlot slot{G.photon_seeds + b, G.readout_seeds + b, G.done + b, (unsigned int)per,
+                         (unsigned int)(m.blk0[g + 1] - m.blk0[g])};
+    chain_body(G.a, off, rem % G.gx, rem / G.gx, slot);
+}
+
+}  // namespace
+
+namespace sb {
+
+size_t mc_chain_workspace(const sb_mc_group *gs, int n) {
+    size_t b = 0;
+    for (int g = 0; g < n; ++g)
+        b += mc_align((size_t)gs[g].n_batch * 3 * gs[g].slopec.n_subaps * sizeof(float)) +
+             mc_align((size_t)gs[g].n_batch * sizeof(unsigned int));
+    return b;
+}
+
+int mc_chain_prepare(const sb_mc_group *gs, int n, const McShParts &parts, void *ws, McBlob &blob) {
+    static_assert(sizeof(McChainBlob) <= sizeof(McBlob), "detector stage arguments exceed the blob");
+    static_assert(sizeof(McChainArgs) <= 4096, "kernel arguments above 4 KB");
+    const char *who = "sb_mc_create";
+    McChainBlob *B = new (blob.b) McChainBlob();
+    B->args.n_groups = n;
+    unsigned char *w = static_cast<unsigned char *>(ws);
+    int blocks = 0, threads = kChainSumThreads;
+    for (int g = 0; g < n; ++g) {
+        const sb_mc_group &G = gs[g];
+        const sb_ccd_params &c = G.ccd;
+        const sb_slopec_plan &sl = G.slopec;
+        const int nl = G.sh.n_lenses, npx = G.sh.subap_npx, side = nl * npx;
+        if (!c.state || !G.integrated || !G.pixels || !G.photon_seeds || !G.readout_seeds || !sl.xw || !sl.yw ||
+            !sl.mw || !G.lenslet_subap || !G.slopes || !G.flux)
+            return fail(SB_EINVAL, "%s: group %d: null detector / slope pointer", who, g);
+        if (npx < 1 || npx > kChainMaxNpx)
+            return fail(SB_ESHAPE, "%s: group %d: %d pixels per sub-aperture (1..%d)", who, g, npx, kChainMaxNpx);
+        if (c.frames_per_read != 1 || c.n_pixels != side * side)
+            return fail(SB_EUNSUPPORTED, "%s: group %d: the detector must read a %d x %d frame every step", who, g,
+                        side, side);
+        if (c.photon_noise && !(c.adu_gain > 0.f)) return fail(SB_EINVAL, "%s: group %d: ADU gain <= 0", who, g);
+        if (sl.npx2 != npx * npx || sl.n_subaps < 1 || sl.n_subaps > nl * nl)
+            return fail(SB_EINVAL, "%s: group %d: slope plan of %d sub-apertures x %d pixels", who, g, sl.n_subaps,
+                        sl.npx2);
+        if (sl.thr_pedestal || sl.thr_ratio > 0.f || sl.window || sl.mult != 0.f)
+            return fail(SB_EUNSUPPORTED, "%s: group %d: slope options beyond thr are not in the step", who, g);
+        if (G.slopes_stride < 2 * sl.n_subaps || G.flux_stride < sl.n_subaps)
+            return fail(SB_EINVAL, "%s: group %d: slope / flux strides below one realisation", who, g);
+        McChainGroup &q = B->args.g[g];
+        ChainArgs &a = q.a;
+        a.p = c;
+        a.part_I = parts.part_I[g];
+        a.part_A = parts.part_A[g];
+        a.nparts = parts.nparts[g];
+        a.photon_scale = G.photon_scale;
+        a.I = G.intensity;
+        a.integ = G.integrated;
+        a.pix = G.pixels;
+        a.n = nl;
+        a.npx = npx;
+        a.side = side;
+        a.lenslet_subap = G.lenslet_subap;
+        a.n_valid = sl.n_subaps;
+        a.thr = sl.thr;
+        a.xw = sl.xw;
+        a.yw = sl.yw;
+        a.mw = sl.mw;
+        a.slopes = G.slopes;
+        a.flux = G.flux;
+        a.tot = reinterpret_cast<float *>(w);
+        a.sxn = a.tot + a.n_valid;
+        a.syn = a.sxn + a.n_valid;
+        w += mc_align((size_t)G.n_batch * 3 * sl.n_subaps * sizeof(float));
+        q.done = reinterpret_cast<unsigned int *>(w);
+        w += mc_align((size_t)G.n_batch * sizeof(unsigned int));
+        q.frame_stride = G.frame_stride;
+        q.photon_seeds = G.photon_seeds;
+        q.readout_seeds = G.readout_seeds;
+        q.gx = (nl + kChainLenses - 1) / kChainLenses;
+        q.gy = nl;
+        q.slopes_stride = G.slopes_stride;
+        q.flux_stride = G.flux_stride;
+        B->args.blk0[g] = blocks;
+        blocks += q.gx * q.gy * G.n_batch;
+        const int t = chain_threads(npx);
+        threads = t > threads ? t : threads;
+    }
+    B->args.blk0[n] = blocks;
+    B->blocks = blocks;
+    B->threads = threads;
+    return SB_OK;
+}
+
+int mc_chain_launch(const McBlob &blob, cudaStream_t st) {
+    const McChainBlob *B = reinterpret_cast<const McChainBlob *>(blob.b);
+    mc_chain_kernel<<<B->blocks, B->threads, 0, st>>>(B->args);
+    return check_launch("mc_chain_kernel");
+}
+
+}  // namespace sb
 
 extern "C" size_t sb_ccd_cte_scratch_bytes(int side) {
     if (side < 1) return 0;

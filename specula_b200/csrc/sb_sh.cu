@@ -12,8 +12,11 @@
 // the samples that reach the detector.  Row/column sums of D and of the
 // input amplitude go to per-CTA partials; a second kernel turns them into
 // the photon normalisation of sh.py:425-427 in a fixed (deterministic) order.
+#include <new>
+
 #include "sb_common.cuh"
 #include "sb_dft.cuh"
+#include "sb_mc.cuh"
 #include "sb_umma.cuh"
 
 namespace {
@@ -63,9 +66,8 @@ __device__ __forceinline__ float norm_amp(const ShArgs &a, int e) {
     return a.A2 ? __fmul_rn(a.A_norm[e], a.A2[e]) : a.A_norm[e];
 }
 
-// the realisation's slice of a batched launch
-__device__ __forceinline__ void batch_slice(ShArgs &a) {
-    const long long z = blockIdx.z;
+// realisation z's slice of a batched launch
+__device__ __forceinline__ void slice_to(ShArgs &a, long long z) {
     a.A += z * a.sA;
     a.ph += z * a.sph;
     a.A_norm += z * a.sAn;
@@ -73,6 +75,8 @@ __device__ __forceinline__ void batch_slice(ShArgs &a) {
     a.part_I += z * a.nbp;
     a.part_A += z * a.nbp;
 }
+
+__device__ __forceinline__ void batch_slice(ShArgs &a) { slice_to(a, blockIdx.z); }
 
 struct ShSmem {
     int tw, tilt, mask, rebin, per_warp_E, per_warp_G, per_warp_I, per_warp_H, tables, per_warp;
@@ -242,18 +246,34 @@ __global__ void __launch_bounds__(256, 4) sh_forward_kernel(ShArgs a) {
 // (operands loaded once per k and reused RB*CB times), loops unrolled.
 // ---------------------------------------------------------------------------
 
+// this CTA's place in the grid of one realisation (a launch over several
+// groups maps its flat index to it)
+struct ShBlk {
+    int x, y, gx, gy;
+};
+
+__device__ __forceinline__ ShBlk grid_blk() {
+    return {(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x, (int)gridDim.y};
+}
+
+// the compile-time kernel's shared memory (per-warp buffers for 8 warps)
 template <int P, int CS, int NPX>
-__global__ void __launch_bounds__(256, 4) sh_forward_fixed_kernel(ShArgs a) {
-    batch_slice(a);
+struct FixedSmem {
+    float2 twT[P * CS];          // twT[c][b] = W[b][c]
+    float2 tilt[P * P];
+    float mask[CS * CS];
+    float R[NPX * CS];
+    float2 Es[8][P * (P + 1)];
+    float2 Gs[8][P * CS > (CS * NPX + 1) / 2 ? P * CS : (CS * NPX + 1) / 2];
+    float Is[8][CS * CS];
+    float red[33];
+};
+
+template <int P, int CS, int NPX>
+__device__ __forceinline__ void sh_fixed_body(const ShArgs &a, const ShBlk &blk, FixedSmem<P, CS, NPX> &S) {
     constexpr int PE = P + 1;
-    __shared__ float2 twT[P * CS];          // twT[c][b] = W[b][c]
-    __shared__ float2 tilt[P * P];
-    __shared__ float mask[CS * CS];
-    __shared__ float R[NPX * CS];
-    __shared__ float2 Es[8][P * PE];
-    __shared__ float2 Gs[8][P * CS > (CS * NPX + 1) / 2 ? P * CS : (CS * NPX + 1) / 2];
-    __shared__ float Is[8][CS * CS];
-    __shared__ float red[33];
+    float2 *twT = S.twT, *tilt = S.tilt;
+    float *mask = S.mask, *R = S.R, *red = S.red;
     for (int e = threadIdx.x; e < CS * P; e += blockDim.x) {
         const int b = e / P, c = e - b * P;
         twT[c * CS + b] = a.tw[e];
@@ -264,11 +284,11 @@ __global__ void __launch_bounds__(256, 4) sh_forward_fixed_kernel(ShArgs a) {
     __syncthreads();
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int i = blockIdx.y;
-    const int j = blockIdx.x * a.spc + warp;
-    float2 *E = Es[warp];
-    float2 *G = Gs[warp];
-    float *I = Is[warp];
+    const int i = blk.y;
+    const int j = blk.x * a.spc + warp;
+    float2 *E = S.Es[warp];
+    float2 *G = S.Gs[warp];
+    float *I = S.Is[warp];
     float local = 0.f;
     if (j < a.n) {
         const size_t row0 = (size_t)i * P, col0 = (size_t)j * P;
@@ -337,9 +357,9 @@ __global__ void __launch_bounds__(256, 4) sh_forward_fixed_kernel(ShArgs a) {
             }
         }
     }
-    const int bid = blockIdx.y * gridDim.x + blockIdx.x;
+    const int bid = blk.y * blk.gx + blk.x;
     const float tot = sb::block_sum(local, red);
-    const int nblk = gridDim.x * gridDim.y;
+    const int nblk = blk.gx * blk.gy;
     const int chunk = (a.n_norm + nblk - 1) / nblk;
     const int lo = bid * chunk;
     const int hi = min(a.n_norm, lo + chunk);
@@ -350,6 +370,13 @@ __global__ void __launch_bounds__(256, 4) sh_forward_fixed_kernel(ShArgs a) {
         a.part_I[bid] = tot;
         a.part_A[bid] = tota;
     }
+}
+
+template <int P, int CS, int NPX>
+__global__ void __launch_bounds__(256, 4) sh_forward_fixed_kernel(ShArgs a) {
+    batch_slice(a);
+    __shared__ FixedSmem<P, CS, NPX> S;
+    sh_fixed_body<P, CS, NPX>(a, grid_blk(), S);
 }
 
 // ---------------------------------------------------------------------------
@@ -395,7 +422,7 @@ __host__ __device__ constexpr size_t tc_smem_bytes() {
 static_assert(tc_smem_bytes<8, 8, 8>() * 8 > 228 * 1024, "more than 8 CTAs per SM would exceed tensor memory");
 
 template <int P, int CS, int NPX>
-__global__ void __launch_bounds__(kTcThreads) sh_forward_tc_kernel(ShArgs a) {
+__device__ __forceinline__ void sh_tc_body(const ShArgs &a, const ShBlk &blk) {
     static_assert(P == 8, "one 16-byte K segment per field row");
     static_assert(CS <= 16, "one 16-row stage-2 block per sub-aperture");
     static_assert(kTcSub * CS * CS <= kTcSub * TcShape<CS>::GS * 2, "intensity buffer aliases the G buffer");
@@ -403,7 +430,6 @@ __global__ void __launch_bounds__(kTcThreads) sh_forward_tc_kernel(ShArgs a) {
     constexpr int GS = TcShape<CS>::GS;
     constexpr uint32_t IDESC = sb::umma_idesc_bf16_f32(128, NB);
     constexpr uint32_t LBO_A = 128 * 16, LBO_B = NB * 16;
-    batch_slice(a);
     extern __shared__ __align__(128) unsigned char tc_smem[];
     unsigned char *A1h = tc_smem, *A1l = tc_smem + kTcOperandBytes;
     unsigned char *A2h = tc_smem + 2 * kTcOperandBytes;   // two tiles
@@ -421,9 +447,9 @@ __global__ void __launch_bounds__(kTcThreads) sh_forward_tc_kernel(ShArgs a) {
     const int t = threadIdx.x, warp = t >> 5;
     // issue the global loads first: this thread's field row and its share of
     // the normalising amplitude; the table set-up below overlaps them
-    const int i = blockIdx.y;
+    const int i = blk.y;
     const int s = t >> 3, r = t & 7;
-    const int j = blockIdx.x * kTcSub + s;
+    const int j = blk.x * kTcSub + s;
     float amp[8], phv[8];
     if (j < a.n) {
         const size_t g = (size_t)(i * P + r) * a.ld + (size_t)j * P;
@@ -447,10 +473,10 @@ __global__ void __launch_bounds__(kTcThreads) sh_forward_tc_kernel(ShArgs a) {
 #pragma unroll
         for (int c = 0; c < 8; ++c) amp[c] = phv[c] = 0.f;
     }
-    const int bid = blockIdx.y * gridDim.x + blockIdx.x;
+    const int bid = blk.y * blk.gx + blk.x;
     float sa = 0.f;
     {
-        const int nblk = gridDim.x * gridDim.y;
+        const int nblk = blk.gx * blk.gy;
         const int chunk = (a.n_norm + nblk - 1) / nblk;
         const int lo = bid * chunk;
         const int hi = min(a.n_norm, lo + chunk);
@@ -622,7 +648,7 @@ __global__ void __launch_bounds__(kTcThreads) sh_forward_tc_kernel(ShArgs a) {
             for (int e = t; e < NPX * kTcSub * NPX; e += kTcThreads) {
                 const int pp = e / (kTcSub * NPX), rem = e - pp * (kTcSub * NPX);
                 const int s2 = rem / NPX, q = rem - s2 * NPX;
-                const int j2 = blockIdx.x * kTcSub + s2;
+                const int j2 = blk.x * kTcSub + s2;
                 if (j2 >= a.n) continue;
                 const float *I = Ib + s2 * CS * CS;
                 float acc = 0.f;
@@ -665,6 +691,12 @@ __global__ void __launch_bounds__(kTcThreads) sh_forward_tc_kernel(ShArgs a) {
         sb::tc_fence_after_sync();
         sb::tmem_dealloc(tmem, kTcTmemCols);
     }
+}
+
+template <int P, int CS, int NPX>
+__global__ void __launch_bounds__(kTcThreads) sh_forward_tc_kernel(ShArgs a) {
+    batch_slice(a);
+    sh_tc_body<P, CS, NPX>(a, grid_blk());
 }
 
 // ---------------------------------------------------------------------------
@@ -1171,6 +1203,216 @@ extern "C" int sb_sh_forward_split_bf16_batched(const sb_sh_plan *pl, const floa
                            A_norm_stride, n_norm, photon_scale, intensity, intensity_stride, n_batch, scratch,
                            scratch_bytes, stream, 1);
 }
+
+// ---------------------------------------------------------------------------
+// Monte-Carlo step, stage 4: the SH forward of every realisation of every
+// group in one launch, unnormalised, with the per-CTA partial sums that
+// sb_sh_forward_batched leaves.  A CTA finds its group, realisation and
+// lenslet block from the flat block index and runs that geometry's
+// compile-time body (FP32, 8 sub-apertures per CTA) or tensor-core body
+// (split-BF16); every group of a plan uses the same DFT form.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct McShGroup {
+    ShArgs a;          // the group's arguments for realisation 0
+    int kind, gx, gy;  // geometry index, CTAs per realisation along x / y
+};
+
+struct McShArgs {
+    int n_groups;
+    McShGroup g[sb::kMcMaxGroups];
+    int blk0[sb::kMcMaxGroups + 1];
+};
+
+struct McShBlob {
+    McShArgs args;
+    int mode, blocks;
+    size_t smem;
+};
+
+// geometries (np_sub, cutsize, subap_npx) of the launch over groups; the
+// split-BF16 form has the first five
+constexpr int kMcShKinds = 6, kMcTcKinds = 5;
+constexpr int kMcShGeom[kMcShKinds][3] = {{8, 12, 6}, {8, 14, 8}, {8, 16, 8}, {8, 8, 8}, {8, 12, 8}, {16, 16, 8}};
+
+int mc_sh_kind(int mode, const sb_sh_plan &pl) {
+    const int nk = mode == 1 ? kMcTcKinds : kMcShKinds;
+    for (int k = 0; k < nk; ++k)
+        if (pl.np_sub == kMcShGeom[k][0] && pl.cutsize == kMcShGeom[k][1] && pl.subap_npx == kMcShGeom[k][2])
+            return k;
+    return -1;
+}
+
+size_t mc_fixed_smem(int kind) {
+    switch (kind) {
+        case 0: return sizeof(FixedSmem<8, 12, 6>);
+        case 1: return sizeof(FixedSmem<8, 14, 8>);
+        case 2: return sizeof(FixedSmem<8, 16, 8>);
+        case 3: return sizeof(FixedSmem<8, 8, 8>);
+        case 4: return sizeof(FixedSmem<8, 12, 8>);
+        default: return sizeof(FixedSmem<16, 16, 8>);
+    }
+}
+
+size_t mc_tc_smem(int kind) {
+    switch (kind) {
+        case 0: return tc_smem_bytes<8, 12, 6>();
+        case 1: return tc_smem_bytes<8, 14, 8>();
+        case 2: return tc_smem_bytes<8, 16, 8>();
+        case 3: return tc_smem_bytes<8, 8, 8>();
+        default: return tc_smem_bytes<8, 12, 8>();
+    }
+}
+
+__device__ __forceinline__ int mc_sh_locate(const McShArgs &m, ShArgs &a, ShBlk &blk) {
+    const int bi = blockIdx.x;
+    int g = 0;
+    while (g + 1 < m.n_groups && bi >= m.blk0[g + 1]) ++g;
+    const McShGroup &G = m.g[g];
+    const int per = G.gx * G.gy, local = bi - m.blk0[g];
+    const int b = local / per, rem = local - b * per;
+    a = G.a;
+    slice_to(a, b);
+    blk = {rem % G.gx, rem / G.gx, G.gx, G.gy};
+    return G.kind;
+}
+
+__global__ void __launch_bounds__(256, 4) mc_sh_fixed_kernel(McShArgs m) {
+    extern __shared__ __align__(16) unsigned char mc_sh_smem[];
+    ShArgs a;
+    ShBlk blk;
+    switch (mc_sh_locate(m, a, blk)) {
+        case 0: sh_fixed_body<8, 12, 6>(a, blk, *reinterpret_cast<FixedSmem<8, 12, 6> *>(mc_sh_smem)); break;
+        case 1: sh_fixed_body<8, 14, 8>(a, blk, *reinterpret_cast<FixedSmem<8, 14, 8> *>(mc_sh_smem)); break;
+        case 2: sh_fixed_body<8, 16, 8>(a, blk, *reinterpret_cast<FixedSmem<8, 16, 8> *>(mc_sh_smem)); break;
+        case 3: sh_fixed_body<8, 8, 8>(a, blk, *reinterpret_cast<FixedSmem<8, 8, 8> *>(mc_sh_smem)); break;
+        case 4: sh_fixed_body<8, 12, 8>(a, blk, *reinterpret_cast<FixedSmem<8, 12, 8> *>(mc_sh_smem)); break;
+        default: sh_fixed_body<16, 16, 8>(a, blk, *reinterpret_cast<FixedSmem<16, 16, 8> *>(mc_sh_smem)); break;
+    }
+}
+
+__global__ void __launch_bounds__(kTcThreads) mc_sh_tc_kernel(McShArgs m) {
+    ShArgs a;
+    ShBlk blk;
+    switch (mc_sh_locate(m, a, blk)) {
+        case 0: sh_tc_body<8, 12, 6>(a, blk); break;
+        case 1: sh_tc_body<8, 14, 8>(a, blk); break;
+        case 2: sh_tc_body<8, 16, 8>(a, blk); break;
+        case 3: sh_tc_body<8, 8, 8>(a, blk); break;
+        default: sh_tc_body<8, 12, 8>(a, blk); break;
+    }
+}
+
+// CTAs per realisation of a group
+void mc_sh_grid(int mode, const sb_sh_plan &pl, int *gx, int *gy) {
+    const int per = mode == 1 ? kTcSub : 8;
+    *gx = (pl.n_lenses + per - 1) / per;
+    *gy = pl.n_lenses;
+}
+
+}  // namespace
+
+namespace sb {
+
+size_t mc_sh_workspace(const sb_mc_group *gs, int n) {
+    size_t b = 0;
+    for (int g = 0; g < n; ++g) {
+        int gx, gy;
+        mc_sh_grid(gs[g].dft_mode, gs[g].sh, &gx, &gy);
+        b += mc_align(2 * (size_t)gx * gy * gs[g].n_batch * sizeof(float));
+    }
+    return b;
+}
+
+int mc_sh_prepare(const sb_mc_group *gs, int n, void *ws, McBlob &blob, McShParts &parts) {
+    static_assert(sizeof(McShBlob) <= sizeof(McBlob), "SH stage arguments exceed the blob");
+    static_assert(sizeof(McShArgs) <= 4096, "kernel arguments above 4 KB");
+    const char *who = "sb_mc_create";
+    McShBlob *B = new (blob.b) McShBlob();
+    const int mode = gs[0].dft_mode;
+    if (mode != 0 && mode != 1) return fail(SB_EINVAL, "%s: dft_mode must be 0 or 1", who);
+    B->mode = mode;
+    B->args.n_groups = n;
+    unsigned char *w = static_cast<unsigned char *>(ws);
+    int blocks = 0;
+    size_t smem = 0;
+    for (int g = 0; g < n; ++g) {
+        const sb_mc_group &G = gs[g];
+        const sb_sh_plan &pl = G.sh;
+        if (G.dft_mode != mode) return fail(SB_EINVAL, "%s: every group must use the same dft_mode", who);
+        if (!pl.twiddle || !pl.tilt || !pl.fp_mask || !pl.rebin || !G.intensity || !G.field_A || !G.field_phase)
+            return fail(SB_EINVAL, "%s: group %d: null SH pointer", who, g);
+        if (pl.n_lenses < 1 || pl.field_ld != G.L || pl.n_lenses * pl.np_sub > G.L)
+            return fail(SB_EINVAL, "%s: group %d: SH field of %d columns on a %d pupil", who, g, pl.field_ld, G.L);
+        const int kind = mc_sh_kind(mode, pl);
+        if (kind < 0)
+            return fail(SB_EUNSUPPORTED, "%s: group %d: no %s kernel for (np=%d, cut=%d, npx=%d)", who, g,
+                        mode ? "split-BF16" : "compile-time", pl.np_sub, pl.cutsize, pl.subap_npx);
+        const long long side = (long long)pl.n_lenses * pl.subap_npx;
+        if (G.frame_stride < side * side) return fail(SB_EINVAL, "%s: group %d: frame stride below a frame", who, g);
+        int gx, gy;
+        mc_sh_grid(mode, pl, &gx, &gy);
+        const int nb = gx * gy;
+        McShGroup &q = B->args.g[g];
+        ShArgs &a = q.a;
+        a = ShArgs{};
+        a.n = pl.n_lenses;
+        a.p = pl.np_sub;
+        a.cs = pl.cutsize;
+        a.npx = pl.subap_npx;
+        a.ld = pl.field_ld;
+        a.spc = 8;
+        a.k = pl.phase_to_rad;
+        a.tw = reinterpret_cast<const float2 *>(pl.twiddle);
+        a.tilt = reinterpret_cast<const float2 *>(pl.tilt);
+        a.mask = pl.fp_mask;
+        a.rebin = pl.rebin;
+        a.A = G.field_A;
+        a.ph = G.field_phase;
+        a.A_norm = G.field_A;                   // the normalising amplitude is the whole field
+        a.n_norm = G.L * G.L;
+        a.out = G.intensity;
+        float *part = reinterpret_cast<float *>(w);
+        a.part_I = part;
+        a.part_A = part + (size_t)nb * G.n_batch;
+        a.sA = a.sph = a.sAn = G.field_stride;
+        a.sout = G.frame_stride;
+        a.nbp = nb;
+        a.vec = (a.ld % 4 == 0) && (a.sA % 4 == 0) && ((uintptr_t)a.A % 16 == 0) && ((uintptr_t)a.ph % 16 == 0) &&
+                (a.p % 4 == 0);
+        q.kind = kind;
+        q.gx = gx;
+        q.gy = gy;
+        parts.part_I[g] = a.part_I;
+        parts.part_A[g] = a.part_A;
+        parts.nparts[g] = nb;
+        B->args.blk0[g] = blocks;
+        blocks += nb * G.n_batch;
+        const size_t sm = mode == 1 ? mc_tc_smem(kind) : mc_fixed_smem(kind);
+        smem = sm > smem ? sm : smem;
+        w += mc_align(2 * (size_t)nb * G.n_batch * sizeof(float));
+    }
+    B->args.blk0[n] = blocks;
+    B->blocks = blocks;
+    B->smem = smem;
+    const cudaError_t e = cudaFuncSetAttribute(mode == 1 ? (const void *)mc_sh_tc_kernel : (const void *)mc_sh_fixed_kernel,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return fail(SB_ECUDA, "%s: SH shared memory: %s", who, cudaGetErrorString(e));
+    return SB_OK;
+}
+
+int mc_sh_launch(const McBlob &blob, cudaStream_t st) {
+    const McShBlob *B = reinterpret_cast<const McShBlob *>(blob.b);
+    if (B->mode == 1) {
+        mc_sh_tc_kernel<<<B->blocks, kTcThreads, B->smem, st>>>(B->args);
+        return check_launch("mc_sh_tc_kernel");
+    }
+    mc_sh_fixed_kernel<<<B->blocks, 256, B->smem, st>>>(B->args);
+    return check_launch("mc_sh_fixed_kernel");
+}
+
+}  // namespace sb
 
 namespace sb {
 // read and clear the tensor-core SH timeout flag (0: none)

@@ -87,7 +87,8 @@ def test_fused_atmosphere_and_batched_mirror_validation_without_device(lib):
 STRUCTS = {'sb_sh_plan': _lib.ShPlan, 'sb_ccd_params': _lib.CcdParams, 'sb_slopec_plan': _lib.SlopecPlan,
            'sb_iir_plan': _lib.IirPlan, 'sb_atmo_layer': _lib.AtmoLayer, 'sb_prop_layer': _lib.PropLayer,
            'sb_atmo_inputs': _lib.AtmoInputs, 'sb_atmo_layer_inputs': _lib.AtmoLayerInputs,
-           'sb_sh_lgs_tables': _lib.ShLgsTables, 'sb_prop_sampling': _lib.PropSampling}
+           'sb_sh_lgs_tables': _lib.ShLgsTables, 'sb_prop_sampling': _lib.PropSampling,
+           'sb_mc_group': _lib.McGroup}
 
 
 def test_struct_layouts_match_header(tmp_path):
@@ -129,3 +130,17 @@ def test_static_scratch_limit_without_device(lib):
     buf = C.c_void_p(16)                     # never dereferenced: the size check fails first
     rc = lib.sb_sh_forward_static(C.byref(plan), buf, buf, buf, 16, C.c_float(1.0), buf, None)
     assert rc == -4 and b'static array' in lib.sb_last_error()
+
+
+def test_monte_carlo_step_validation_without_device(lib):
+    """sb_mc_* reject an empty or oversized group list, a null handle and a
+    missing workspace before any device work."""
+    groups = (_lib.McGroup * 9)()
+    assert lib.sb_mc_workspace_bytes(groups, 0) == 0
+    assert lib.sb_mc_workspace_bytes(groups, 9) == 0 and b'groups' in lib.sb_last_error()
+    groups[0].n_batch = 0
+    assert lib.sb_mc_workspace_bytes(groups, 1) == 0 and b'no realisations' in lib.sb_last_error()
+    assert lib.sb_mc_step(None, None) == -1
+    h = C.c_void_p()
+    assert lib.sb_mc_create(groups, 1, None, 0, C.byref(h), None) == -1
+    lib.sb_mc_destroy(None)

@@ -1,0 +1,69 @@
+"""Monte-Carlo step over geometry groups (sb_mc_step): seven launches per step,
+each over every realisation of every group, against the group-by-group
+graph of the same realisations (BatchedScao.capture), bit for bit, with the
+FP32 and the split-BF16 SH.  The mix is the Monte-Carlo benchmark's three
+geometries (20x20 / 160 px, 40x40 / 320 px, 74x74 / 592 px) at two
+wavelengths, nine realisations in six groups."""
+import pytest
+
+torch = pytest.importorskip('torch')
+
+pytestmark = pytest.mark.gpu
+
+N_REAL = (4, 3, 2)
+STEPS = 3
+
+
+def _state(sys_b):
+    out = []
+    for g in sys_b.groups:
+        st = {k: getattr(g, k).clone() for k in ('ATM', 'EA', 'EP', 'I', 'INT', 'PIX', 'S', 'FLUX', 'M', 'dm_phase')}
+        st['commands'] = g.integ.out_comm.value.clone()
+        st['integ_state'] = g.integ.state.clone()
+        st['positions'] = torch.cat([lp.atmo._positions.clone() for lp in g.loops])
+        st['ccd_state'] = g.loops[0].ccd._state.clone()
+        out.append(st)
+    return out
+
+
+def _run(dft, mc):
+    from specula_b200.batched import BatchedScao, mc_groups
+    sys_b = BatchedScao(mc_groups(n_real=N_REAL), device_idx=0, dft=dft)
+    sys_b.start()
+    if mc:
+        sys_b.capture_mc()
+    else:
+        sys_b.capture()
+    for _ in range(STEPS):
+        sys_b.replay()
+    torch.cuda.synchronize()
+    from specula_b200 import _lib
+    _lib.call('sb_device_status')
+    return sys_b, _state(sys_b)
+
+
+@pytest.mark.parametrize('dft', ['fp32', 'split_bf16'])
+def test_mc_step_equals_group_graph(cuda, dft):
+    ref_sys, ref = _run(dft, mc=False)
+    mc_sys, got = _run(dft, mc=True)
+    assert len(mc_sys.groups) == 6
+    assert mc_sys.launches_per_step == 7
+    assert ref_sys.launches_per_step > 7
+    for gi, (a, b) in enumerate(zip(ref, got)):
+        for k in a:
+            assert torch.equal(a[k], b[k]), (dft, gi, k, float((a[k].double() - b[k].double()).abs().max()))
+    # the loop moved: slopes and mirror non-trivial
+    assert all(float(st['S'].abs().max()) > 0 for st in got)
+    assert all(float(st['dm_phase'].abs().max()) > 0 for st in got)
+    mc_sys.release_mc()
+
+
+def test_mc_step_rejects_unfusable_groups(cuda):
+    """A slope option the fused detector / slope stage does not implement
+    keeps the Monte-Carlo step from being built."""
+    from specula_b200.batched import BatchedScao, mc_groups
+    sys_b = BatchedScao(mc_groups(n_real=(2, 0, 0)), device_idx=0)
+    sys_b.start()
+    sys_b.groups[0].loops[0].slopec.thr_pedestal = True
+    with pytest.raises(NotImplementedError, match='fused detector'):
+        sys_b.capture_mc()
