@@ -470,10 +470,11 @@ def bench_batched(dev, steps, cpu_budget_s):
     group_launches = sys_b.launches_per_step
     # the Monte-Carlo step of the C ABI: one launch per stage over every group
     mc = {}
-    for dft in ('fp32', 'split_bf16'):
+    for dft, pipe in (('fp32', False), ('split_bf16', False), ('split_bf16', True)):
         sys_b.set_dft(dft)
-        sys_b.capture_mc()
-        mc[dft] = (timed(sys_b.replay, steps), sys_b.launches_per_step)
+        sys_b.capture_mc(pipelined=pipe)
+        spr = sys_b.steps_per_replay
+        mc[(dft, pipe)] = (timed(sys_b.replay, max(1, steps // spr)) / spr, sys_b.launches_per_step)
     sys_b.release_mc()
     _lib_status()
     by_size = {}
@@ -492,9 +493,11 @@ def bench_batched(dev, steps, cpu_budget_s):
            'batched_split_bf16_realisation_steps_per_s': n_real / (bf16_ms / 1e3),
            'speedup_batched_split_bf16_vs_plain': plain_ms / bf16_ms, 'setup_s': setup_s,
            'group_graph_launches_per_step': group_launches,
-           'mc_step_ms_per_step': mc['fp32'][0], 'mc_step_split_bf16_ms_per_step': mc['split_bf16'][0],
-           'mc_step_launches_per_step': mc['split_bf16'][1],
-           'mc_step_realisation_steps_per_s': n_real / (min(mc['fp32'][0], mc['split_bf16'][0]) / 1e3),
+           'mc_step_ms_per_step': mc[('fp32', False)][0],
+           'mc_step_split_bf16_ms_per_step': mc[('split_bf16', False)][0],
+           'mc_step_pipelined_split_bf16_ms_per_step': mc[('split_bf16', True)][0],
+           'mc_step_launches_per_step': mc[('split_bf16', True)][1],
+           'mc_step_realisation_steps_per_s': n_real / (min(v[0] for v in mc.values()) / 1e3),
            'mc_step': 'sb_mc_step: seven launches per step (layer parameters, layers, propagation, SH, '
                       'normalisation + detector + slopes, reconstructor + integrators, mirror), each over every '
                       'realisation of every group, captured in one graph',
@@ -986,13 +989,14 @@ def profile_loop(dev, replays):
 
 
 def profile_batched(dev, mc=False):
-    """One replay of the batched graph (mc: the Monte-Carlo step) bracketed for a profiler."""
+    """One replay of the batched graph (mc: the pipelined Monte-Carlo step,
+    two steps) bracketed for a profiler."""
     import torch
     from specula_b200.batched import BatchedScao, mc_groups
     sys_b = BatchedScao(mc_groups(), device_idx=dev.index, dft='split_bf16')
     sys_b.start()
     if mc:
-        sys_b.capture_mc()
+        sys_b.capture_mc(pipelined=True)
     else:
         sys_b.autotune()
         sys_b.capture()

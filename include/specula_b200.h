@@ -752,6 +752,11 @@ typedef struct sb_mc_group {
     int n_valid, ld_if;
     const int32_t *mask_idx;
     float dm_sign;
+    /* pipelined stages (NULL: sb_mc_stage takes parity -1 only): a second
+     * mirror-phase buffer (stride dm_stride) and the integrators' next
+     * output, which iir.out_next must point to */
+    float *dm_phase_alt;
+    float *commands_next;
 } sb_mc_group;
 
 typedef struct sb_mc_handle sb_mc_handle;
@@ -761,6 +766,26 @@ int sb_mc_create(const sb_mc_group *groups, int n_groups, void *workspace, size_
                  sb_mc_handle **handle, void *stream);
 int sb_mc_step(const sb_mc_handle *handle, void *stream);
 void sb_mc_destroy(sb_mc_handle *handle);
+
+/* One stage of the step on a stream of the caller's choice, so that the
+ * mirror projection of step t can overlap the other stages of step t (the
+ * integrators' output for step t is known after step t-1, for integer
+ * delays >= 1).  parity -1: the stages of sb_mc_step (propagation reads
+ * dm_phase, the mirror writes it from commands).  parity p = t % 2, with
+ * dm_phase_alt and commands_next set: SB_MC_PROP reads buffer p ^ 1 and
+ * SB_MC_DM writes buffer p (0: dm_phase, 1: dm_phase_alt) from
+ * commands_next.  Step t then runs, with DM(t) on a second stream:
+ *   second stream: wait for REC(t-1); DM(t)
+ *   first stream:  ATMO, PROP, SH, CHAIN; wait for DM(t); REC
+ * after one sb_mc_step (which fills commands_next and dm_phase) as step
+ * t = 0, i.e. parities 1, 0, 1, ...  The results equal sb_mc_step's. */
+#define SB_MC_ATMO 0    /* layer parameters + layers (two launches) */
+#define SB_MC_PROP 1
+#define SB_MC_SH 2
+#define SB_MC_CHAIN 3
+#define SB_MC_REC 4
+#define SB_MC_DM 5
+int sb_mc_stage(const sb_mc_handle *handle, int stage, int parity, void *stream);
 
 #ifdef __cplusplus
 }

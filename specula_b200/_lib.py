@@ -98,7 +98,11 @@ class McGroup(C.Structure):
                 ('flux', fp), ('flux_stride', C.c_int),
                 ('R', fp), ('n_modes', C.c_int), ('n_slopes', C.c_int), ('ldr', C.c_int), ('modes', fp),
                 ('iir', IirPlan), ('commands', fp),
-                ('ifunc', fp), ('n_valid', C.c_int), ('ld_if', C.c_int), ('mask_idx', ip), ('dm_sign', C.c_float)]
+                ('ifunc', fp), ('n_valid', C.c_int), ('ld_if', C.c_int), ('mask_idx', ip), ('dm_sign', C.c_float),
+                ('dm_phase_alt', fp), ('commands_next', fp)]
+
+
+SB_MC_ATMO, SB_MC_PROP, SB_MC_SH, SB_MC_CHAIN, SB_MC_REC, SB_MC_DM = range(6)
 
 
 # name -> (restype, argtypes); every function of include/specula_b200.h
@@ -108,6 +112,7 @@ SIGNATURES = {
     'sb_mc_create': (C.c_int, [C.POINTER(McGroup), C.c_int, vp, C.c_size_t, C.POINTER(vp), vp]),
     'sb_mc_step': (C.c_int, [vp, vp]),
     'sb_mc_destroy': (None, [vp]),
+    'sb_mc_stage': (C.c_int, [vp, C.c_int, C.c_int, vp]),
     'sb_last_error': (C.c_char_p, []),
     'sb_sh_scratch_bytes': (C.c_size_t, [C.POINTER(ShPlan)]),
     'sb_sh_forward': (C.c_int, [C.POINTER(ShPlan), fp, fp, fp, C.c_int, C.c_float, fp, vp, C.c_size_t, vp]),

@@ -211,9 +211,11 @@ class _Group:
             self.integ._ost[b * nm:(b + 1) * nm].copy_(lp.integ._ost)
             self.integ.out_comm.value[b * nm:(b + 1) * nm].copy_(lp.integ.out_comm.value)
 
-    def mc_group(self):
+    def mc_group(self, pipelined=False):
         """This group as an sb_mc_group: the same buffers, plans and seeds the
-        group-by-group launches use (keeps the ctypes arrays it points to)."""
+        group-by-group launches use (keeps the ctypes arrays it points to).
+        pipelined: with a second mirror-phase buffer and the integrators'
+        next output, for sb_mc_stage's overlapped mirror."""
         lp = self.loops[0]
         if not lp._can_fuse_chain():
             raise NotImplementedError('BatchedScao: the Monte-Carlo step needs the fused detector / slope chain '
@@ -247,6 +249,12 @@ class _Group:
         m.modes = self.M.data_ptr()
         m.iir = self.integ._plan
         m.commands = self.integ.out_comm.value.data_ptr()
+        if pipelined:
+            self.dm_phase_alt = torch.zeros_like(self.dm_phase)
+            self.commands_next = torch.zeros_like(self.integ.out_comm.value)
+            m.dm_phase_alt = self.dm_phase_alt.data_ptr()
+            m.commands_next = self.commands_next.data_ptr()
+            m.iir.out_next = m.commands_next         # on the group's copy of the plan only
         m.ifunc, m.n_valid, m.ld_if = dm._IF.data_ptr(), int(dm._idx.numel()), dm._ld
         m.mask_idx, m.dm_sign = dm._idx.data_ptr(), float(dm.sign)
         return m
@@ -300,6 +308,7 @@ class BatchedScao:
         self.graph = None
         self.plain_graphs = None
         self._launches = None
+        self.steps_per_replay = 1
 
     def set_dft(self, dft):
         """Switch the groups' SH forward between 'fp32' and 'split_bf16'; the
@@ -378,6 +387,7 @@ class BatchedScao:
         torch.cuda.synchronize(self.device)
         self.graph = g
         self._launches = graph_kernel_count(g)
+        self.steps_per_replay = 1
         return g
 
     def replay(self):
@@ -388,12 +398,15 @@ class BatchedScao:
         """Kernel launches of one captured step, counted in the graph."""
         return self._launches
 
-    def capture_mc(self):
+    def capture_mc(self, pipelined=False):
         """The batched step of every group as one sb_mc_step (seven launches,
-        each over every realisation of every group) captured in a CUDA graph."""
+        each over every realisation of every group) captured in a CUDA graph.
+        pipelined: two steps per replay, each step's mirror projection on a
+        second (high-priority) stream overlapping the step's atmosphere, SH
+        and detector stages (sb_mc_stage); the same results."""
         lib = _lib.load()
         self.release_mc()
-        groups = (_lib.McGroup * len(self.groups))(*[g.mc_group() for g in self.groups])
+        groups = (_lib.McGroup * len(self.groups))(*[g.mc_group(pipelined) for g in self.groups])
         nbytes = lib.sb_mc_workspace_bytes(groups, len(self.groups))
         if nbytes == 0:
             raise ValueError('BatchedScao: ' + (lib.sb_last_error() or b'').decode())
@@ -404,15 +417,35 @@ class BatchedScao:
                   st)
         self._mc_groups = groups
         self.mc_handle = handle
-        _lib.call('sb_mc_step', handle, st)       # one eager step, as capture() takes
+        # one eager step, as capture() takes; with pipelining it also fills
+        # the integrators' next output and the mirror phase of step t = 0
+        _lib.call('sb_mc_step', handle, st)
         torch.cuda.synchronize(self.device)
         cap = torch.cuda.Stream(self.device)
         g = torch.cuda.CUDAGraph(keep_graph=True)
-        with torch.cuda.graph(g, stream=cap):
-            _lib.call('sb_mc_step', handle, torch.cuda.current_stream(self.device).cuda_stream)
+        if not pipelined:
+            with torch.cuda.graph(g, stream=cap):
+                _lib.call('sb_mc_step', handle, torch.cuda.current_stream(self.device).cuda_stream)
+            self.steps_per_replay = 1
+        else:
+            side = torch.cuda.Stream(self.device, priority=-1)
+
+            def stage(k, p, stream):
+                _lib.call('sb_mc_stage', handle, k, p, stream.cuda_stream)
+
+            with torch.cuda.graph(g, stream=cap):
+                main = torch.cuda.current_stream(self.device)
+                for p in (1, 0):
+                    side.wait_stream(main)            # the commands of step t: after REC(t-1)
+                    stage(_lib.SB_MC_DM, p, side)
+                    for k in (_lib.SB_MC_ATMO, _lib.SB_MC_PROP, _lib.SB_MC_SH, _lib.SB_MC_CHAIN):
+                        stage(k, p, main)
+                    main.wait_stream(side)            # REC(t) rewrites the next commands
+                    stage(_lib.SB_MC_REC, p, main)
+            self.steps_per_replay = 2
         torch.cuda.synchronize(self.device)
         self.graph = g
-        self._launches = graph_kernel_count(g)
+        self._launches = graph_kernel_count(g) // self.steps_per_replay
         return g
 
     def step_mc(self):

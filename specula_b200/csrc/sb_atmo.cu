@@ -711,7 +711,8 @@ struct McAtmoArgs {
 struct McPropGroup {
     const float *atm;
     long long atm_real_stride, atm_layer_stride;
-    const float *stop_A, *stop_phase, *dm_A, *dm_phase;
+    const float *stop_A, *stop_phase, *dm_A;
+    const float *dm_phase[2];        // the mirror-phase buffers (the second may be NULL)
     long long dm_stride;
     float *A, *P;
     long long out_stride;
@@ -719,7 +720,7 @@ struct McPropGroup {
 };
 
 struct McPropArgs {
-    int n_groups;
+    int n_groups, sel;               // sel: the mirror-phase buffer read
     McPropGroup g[sb::kMcMaxGroups];
     int real0[sb::kMcMaxGroups + 1];  // realisations before each group
 };
@@ -771,7 +772,7 @@ __global__ void __launch_bounds__(256) mc_propagate_kernel(McPropArgs a) {
     const McPropGroup &G = a.g[g];
     const long long b = r - a.real0[g];
     propagate_field(G.atm ? G.atm + b * G.atm_real_stride : nullptr, G.n_atm, G.atm_layer_stride, G.stop_A,
-                    G.stop_phase, G.dm_A, G.dm_phase + b * G.dm_stride, G.n, G.A + b * G.out_stride,
+                    G.stop_phase, G.dm_A, G.dm_phase[a.sel] + b * G.dm_stride, G.n, G.A + b * G.out_stride,
                     G.P + b * G.out_stride, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
@@ -839,7 +840,8 @@ int mc_atmo_prepare(const sb_mc_group *gs, int n, void *ws, McBlob &blob, cudaSt
         q.stop_A = G.stop_A;
         q.stop_phase = G.stop_phase;
         q.dm_A = G.dm_A;
-        q.dm_phase = G.dm_phase;
+        q.dm_phase[0] = G.dm_phase;
+        q.dm_phase[1] = G.dm_phase_alt;
         q.dm_stride = G.dm_stride;
         q.A = G.field_A;
         q.P = G.field_phase;
@@ -864,18 +866,29 @@ int mc_atmo_prepare(const sb_mc_group *gs, int n, void *ws, McBlob &blob, cudaSt
     return SB_OK;
 }
 
-int mc_atmo_launch(const McBlob &blob, cudaStream_t st) {
+int mc_atmo_layers_launch(const McBlob &blob, cudaStream_t st) {
     const McAtmoBlob *B = reinterpret_cast<const McAtmoBlob *>(blob.b);
-    if (B->atmo.n_layers > 0) {
-        mc_atmo_advance_kernel<<<(B->atmo.n_layers + 255) / 256, 256, 0, st>>>(B->atmo);
-        int rc = check_launch("mc_atmo_advance_kernel");
-        if (rc) return rc;
-        mc_atmo_evolve_kernel<<<B->evolve_blocks, dim3(32, kRowStep), 0, st>>>(B->atmo);
-        rc = check_launch("mc_atmo_evolve_kernel");
-        if (rc) return rc;
-    }
-    mc_propagate_kernel<<<dim3(B->prop_blocks, B->n_real), 256, 0, st>>>(B->prop);
+    if (B->atmo.n_layers == 0) return SB_OK;
+    mc_atmo_advance_kernel<<<(B->atmo.n_layers + 255) / 256, 256, 0, st>>>(B->atmo);
+    int rc = check_launch("mc_atmo_advance_kernel");
+    if (rc) return rc;
+    mc_atmo_evolve_kernel<<<B->evolve_blocks, dim3(32, kRowStep), 0, st>>>(B->atmo);
+    return check_launch("mc_atmo_evolve_kernel");
+}
+
+int mc_prop_launch(const McBlob &blob, int sel, cudaStream_t st) {
+    const McAtmoBlob *B = reinterpret_cast<const McAtmoBlob *>(blob.b);
+    McPropArgs p = B->prop;
+    p.sel = sel;
+    for (int g = 0; g < p.n_groups; ++g)
+        if (!p.g[g].dm_phase[sel]) return fail(SB_EINVAL, "sb_mc_stage: group %d has no second mirror buffer", g);
+    mc_propagate_kernel<<<dim3(B->prop_blocks, B->n_real), 256, 0, st>>>(p);
     return check_launch("mc_propagate_kernel");
+}
+
+int mc_atmo_launch(const McBlob &blob, cudaStream_t st) {
+    const int rc = mc_atmo_layers_launch(blob, st);
+    return rc ? rc : mc_prop_launch(blob, 0, st);
 }
 
 }  // namespace sb

@@ -775,9 +775,9 @@ struct McRecArgs {
 };
 
 struct McDmJob {
-    const float *cmd;
+    const float *cmd[2];               // commands, commands_next
     const int32_t *idx;
-    float *phase;
+    float *phase[2];                   // dm_phase, dm_phase_alt
     long long phase_stride;
     int ldc, nb, nmodes, nvalid, g, cta0, ncta;
     float sign;
@@ -787,6 +787,7 @@ struct McDmArgs {
     CUtensorMap map[sb::kMcMaxGroups];
     const McDmJob *jobs;
     const int *cta_job;
+    int cmd, sel;                      // command and phase buffers of this launch
 };
 
 struct McRecBlob {
@@ -796,7 +797,7 @@ struct McRecBlob {
 
 struct McDmBlob {
     McDmArgs args;
-    int blocks;
+    int blocks, pipelined;
     size_t smem;
 };
 
@@ -824,11 +825,11 @@ __global__ void __launch_bounds__(32 * (2 * kMcDmNbx + 1), 1) mc_dm_kernel(const
     const McDmJob &J = m.jobs[m.cta_job[blockIdx.x]];
     const int bid = blockIdx.x - J.cta0;
     if (J.nb <= 8)
-        dm_c4_body<8, kMcDmNbx>(m.map[J.g], J.nmodes, J.nvalid, J.cmd, J.ldc, J.nb, J.sign, J.idx, J.phase,
-                                J.phase_stride, bid, J.ncta);
+        dm_c4_body<8, kMcDmNbx>(m.map[J.g], J.nmodes, J.nvalid, J.cmd[m.cmd], J.ldc, J.nb, J.sign, J.idx,
+                                J.phase[m.sel], J.phase_stride, bid, J.ncta);
     else
-        dm_c4_body<16, kMcDmNbx>(m.map[J.g], J.nmodes, J.nvalid, J.cmd, J.ldc, J.nb, J.sign, J.idx, J.phase,
-                                 J.phase_stride, bid, J.ncta);
+        dm_c4_body<16, kMcDmNbx>(m.map[J.g], J.nmodes, J.nvalid, J.cmd[m.cmd], J.ldc, J.nb, J.sign, J.idx,
+                                 J.phase[m.sel], J.phase_stride, bid, J.ncta);
 }
 
 int mc_jobs(const sb_mc_group *gs, int n) {
@@ -885,6 +886,10 @@ int mc_control_prepare(const sb_mc_group *gs, int n, void *ws, McBlob &rec, McBl
             G.ldr < G.n_slopes || G.n_slopes > G.slopes_stride || G.iir.n != G.n_batch * nm)
             return fail(SB_EINVAL, "%s: group %d: bad reconstructor / integrator", who, g);
         if (nm > kDbMaxModes) return fail(SB_ESHAPE, "%s: group %d: at most %d modes", who, g, kDbMaxModes);
+        if (G.commands_next && G.iir.out_next != G.commands_next)
+            return fail(SB_EINVAL, "%s: group %d: iir.out_next must be commands_next", who, g);
+        if (!G.commands_next != !G.dm_phase_alt)
+            return fail(SB_EINVAL, "%s: group %d: dm_phase_alt and commands_next go together", who, g);
         if (G.n_valid < 1 || G.ld_if < G.n_valid || G.ld_if % 4 || (uintptr_t)G.ifunc % 16)
             return fail(SB_EINVAL, "%s: group %d: influence functions need 16-byte aligned rows", who, g);
         RB->args.iir[g] = G.iir;
@@ -910,9 +915,11 @@ int mc_control_prepare(const sb_mc_group *gs, int n, void *ws, McBlob &rec, McBl
             r.e0 = b0 * nm;
             for (int k = 0; k < (nm + kMcRecRows - 1) / kMcRecRows; ++k) rb[blk++] = make_int2(j, k);
             McDmJob &d = dj[j];
-            d.cmd = G.commands + (size_t)b0 * nm;
+            d.cmd[0] = G.commands + (size_t)b0 * nm;
+            d.cmd[1] = G.commands_next ? G.commands_next + (size_t)b0 * nm : nullptr;
             d.idx = G.mask_idx;
-            d.phase = G.dm_phase + (size_t)b0 * G.dm_stride;
+            d.phase[0] = G.dm_phase + (size_t)b0 * G.dm_stride;
+            d.phase[1] = G.dm_phase_alt ? G.dm_phase_alt + (size_t)b0 * G.dm_stride : nullptr;
             d.phase_stride = G.dm_stride;
             d.ldc = nm;
             d.nb = nb;
@@ -925,14 +932,17 @@ int mc_control_prepare(const sb_mc_group *gs, int n, void *ws, McBlob &rec, McBl
             smem = sm > smem ? sm : smem;
         }
     }
-    // SMs to jobs: each added CTA goes to the job whose busiest CTA streams
-    // the most influence-function rows (tiles per CTA x modes)
+    // SMs to jobs: each added CTA goes to the job whose busiest CTA has the
+    // most work: tiles per CTA x modes, x 7/4 for 16 realisations per pass
+    // (twice the FMAs per influence-function value: a CTA streams ~1.75x
+    // slower than with 8)
     for (int left = nsm - nj; left > 0; --left) {
         int best = -1;
         long long worst = 0;
         for (int k = 0; k < nj; ++k) {
             if (ncta[k] >= tiles[k]) continue;
-            const long long c = (long long)((tiles[k] + ncta[k] - 1) / ncta[k]) * dj[k].nmodes;
+            const long long c =
+                (long long)((tiles[k] + ncta[k] - 1) / ncta[k]) * dj[k].nmodes * (dj[k].nb > 8 ? 7 : 4);
             if (c > worst) {
                 worst = c;
                 best = k;
@@ -953,6 +963,8 @@ int mc_control_prepare(const sb_mc_group *gs, int n, void *ws, McBlob &rec, McBl
     DB->args.jobs = d_dj;
     DB->args.cta_job = d_cta;
     DB->blocks = (int)cta_job.size();
+    DB->pipelined = 1;
+    for (int g = 0; g < n; ++g) DB->pipelined &= gs[g].commands_next != nullptr;
     DB->smem = smem;
     cudaError_t e = cudaMemcpyAsync(d_rj, rj.data(), nj * sizeof(McRecJob), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_rb, rb.data(), nblk_rec * sizeof(int2), cudaMemcpyHostToDevice, st);
@@ -971,9 +983,14 @@ int mc_rec_launch(const McBlob &blob, cudaStream_t st) {
     return check_launch("mc_rec_kernel");
 }
 
-int mc_dm_launch(const McBlob &blob, cudaStream_t st) {
+int mc_dm_launch(const McBlob &blob, int cmd, int sel, cudaStream_t st) {
     const McDmBlob *B = reinterpret_cast<const McDmBlob *>(blob.b);
-    mc_dm_kernel<<<B->blocks, 32 * (2 * kMcDmNbx + 1), B->smem, st>>>(B->args);
+    if ((cmd || sel) && !B->pipelined)
+        return fail(SB_EINVAL, "sb_mc_stage: the groups have no commands_next / dm_phase_alt");
+    McDmArgs a = B->args;
+    a.cmd = cmd;
+    a.sel = sel;
+    mc_dm_kernel<<<B->blocks, 32 * (2 * kMcDmNbx + 1), B->smem, st>>>(a);
     return check_launch("mc_dm_kernel");
 }
 

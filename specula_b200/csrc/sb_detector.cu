@@ -657,7 +657,8 @@ struct ChainSlot {
 
 // the chain for lenslet block (bx, by) of one realisation; any CTA size from
 // 256 to 512 threads gives the same bits
-__device__ __forceinline__ void chain_body(const ChainArgs &a, const ChainOff &o, int bx, int by,
+template <bool ROWS>
+__device__ __forceinline__ void chain_body(const ChainArgs &a, const ChainOff &o, int bx0, int nbx, int by,
                                            const ChainSlot &slot) {
     __shared__ double dred[33];
     __shared__ float logfact[32];
@@ -692,7 +693,11 @@ __device__ __forceinline__ void chain_body(const ChainArgs &a, const ChainOff &o
     const float phot = (float)(a.photon_scale * sa);
     const float scale = phot / (float)si;
 
-    const int i = by, j0 = bx * kChainLenses;
+    const int i = by;
+    // lenslet blocks bx0 .. bx0 + nbx - 1 of row i, one after the other
+    const int nb = ROWS ? nbx : 1;
+    for (int bx = bx0; bx < bx0 + nb; ++bx) {
+    const int j0 = bx * kChainLenses;
     const int w = min(kChainLenses, a.n - j0);
     const int npx = a.npx, wc = w * npx, P = npx * wc, tld = kChainLenses * npx;
     // detector: every pass samples up to blockDim pixels of the tile (one pass
@@ -726,9 +731,9 @@ __device__ __forceinline__ void chain_body(const ChainArgs &a, const ChainOff &o
                 total += cnt;
             }
             const int rank = __popc(bal & ((1u << lane) - 1u));
-            const int slot = small ? before + rank : total + (warp * 32 - before) + (lane - rank);
-            s_idx[slot] = qi;
-            s_mean[slot] = f;
+            const int pos = small ? before + rank : total + (warp * 32 - before) + (lane - rank);
+            s_idx[pos] = qi;
+            s_mean[pos] = f;
             __syncthreads();
             qi = s_idx[tid];
             fi = s_mean[tid];
@@ -775,6 +780,8 @@ __device__ __forceinline__ void chain_body(const ChainArgs &a, const ChainOff &o
                 slopes[a.n_valid + s] = y * fac;
             }
         }
+    }
+    __syncthreads();                      // the next block refills the tile
     }
 
     // the last CTA sharing the frame state advances it; the last CTA of the
@@ -829,7 +836,8 @@ __device__ __forceinline__ void chain_body(const ChainArgs &a, const ChainOff &o
 
 __global__ void __launch_bounds__(kChainMaxThreads) sh_ccd_slopec_kernel(ChainArgs a) {
     const unsigned int ctas = gridDim.x * gridDim.y;
-    chain_body(a, ChainOff{0, 0, 0, 0, 0}, blockIdx.x, blockIdx.y, ChainSlot{nullptr, nullptr, nullptr, ctas, ctas});
+    chain_body<false>(a, ChainOff{0, 0, 0, 0, 0}, blockIdx.x, 1, blockIdx.y,
+               ChainSlot{nullptr, nullptr, nullptr, ctas, ctas});
 }
 
 }  // namespace
@@ -1064,6 +1072,7 @@ struct McChainGroup {
     const uint64_t *photon_seeds, *readout_seeds;
     unsigned int *done;              // [n_batch] realisation counters
     int gx, gy, slopes_stride, flux_stride;
+    int tpc, row_blocks;             // lenslet blocks per CTA, blocks per lenslet row
 };
 
 struct McChainArgs {
@@ -1077,7 +1086,7 @@ struct McChainBlob {
     int blocks, threads;
 };
 
-__global__ void __launch_bounds__(kChainMaxThreads, 2) mc_chain_kernel(McChainArgs m) {
+__global__ void __launch_bounds__(kChainSumThreads, 4) mc_chain_kernel(McChainArgs m) {
     // the group's arguments staged in shared memory: read there on use, not
     // held in registers
     __shared__ __align__(16) McChainGroup G;
@@ -1097,7 +1106,8 @@ __global__ void __launch_bounds__(kChainMaxThreads, 2) mc_chain_kernel(McChainAr
                        (size_t)b * G.flux_stride, (size_t)b * 3 * G.a.n_valid};
     const ChainSlot slot{G.photon_seeds + b, G.readout_seeds + b, G.done + b, (unsigned int)per,
                          (unsigned int)(m.blk0[g + 1] - m.blk0[g])};
-    chain_body(G.a, off, rem % G.gx, rem / G.gx, slot);
+    const int bx0 = (rem % G.gx) * G.tpc;
+    chain_body<true>(G.a, off, bx0, min(G.tpc, G.row_blocks - bx0), rem / G.gx, slot);
 }
 
 }  // namespace
@@ -1119,6 +1129,8 @@ int mc_chain_prepare(const sb_mc_group *gs, int n, const McShParts &parts, void 
     McChainBlob *B = new (blob.b) McChainBlob();
     B->args.n_groups = n;
     unsigned char *w = static_cast<unsigned char *>(ws);
+    // 256 threads: several passes over a block's pixels when npx > 8 (the
+    // sums do not depend on the CTA size)
     int blocks = 0, threads = kChainSumThreads;
     for (int g = 0; g < n; ++g) {
         const sb_mc_group &G = gs[g];
@@ -1171,14 +1183,16 @@ int mc_chain_prepare(const sb_mc_group *gs, int n, const McShParts &parts, void 
         q.frame_stride = G.frame_stride;
         q.photon_seeds = G.photon_seeds;
         q.readout_seeds = G.readout_seeds;
-        q.gx = (nl + kChainLenses - 1) / kChainLenses;
+        // whole lenslet rows per CTA: the per-CTA work (normalisation sums,
+        // completion counters) is paid once per row
+        q.row_blocks = (nl + kChainLenses - 1) / kChainLenses;
+        q.tpc = q.row_blocks;
+        q.gx = 1;
         q.gy = nl;
         q.slopes_stride = G.slopes_stride;
         q.flux_stride = G.flux_stride;
         B->args.blk0[g] = blocks;
         blocks += q.gx * q.gy * G.n_batch;
-        const int t = chain_threads(npx);
-        threads = t > threads ? t : threads;
     }
     B->args.blk0[n] = blocks;
     B->blocks = blocks;

@@ -78,8 +78,24 @@ extern "C" int sb_mc_step(const sb_mc_handle *h, void *stream) {
     if (!rc) rc = sb::mc_sh_launch(h->sh, st);
     if (!rc) rc = sb::mc_chain_launch(h->chain, st);
     if (!rc) rc = sb::mc_rec_launch(h->rec, st);
-    if (!rc) rc = sb::mc_dm_launch(h->dm, st);
+    if (!rc) rc = sb::mc_dm_launch(h->dm, 0, 0, st);
     return rc;
+}
+
+extern "C" int sb_mc_stage(const sb_mc_handle *h, int stage, int parity, void *stream) {
+    sb::clear_error();
+    if (!h) return sb::fail(SB_EINVAL, "sb_mc_stage: null handle");
+    if (parity < -1 || parity > 1) return sb::fail(SB_EINVAL, "sb_mc_stage: parity must be -1, 0 or 1");
+    cudaStream_t st = sb::as_stream(stream);
+    switch (stage) {
+        case SB_MC_ATMO: return sb::mc_atmo_layers_launch(h->atmo, st);
+        case SB_MC_PROP: return sb::mc_prop_launch(h->atmo, parity < 0 ? 0 : parity ^ 1, st);
+        case SB_MC_SH: return sb::mc_sh_launch(h->sh, st);
+        case SB_MC_CHAIN: return sb::mc_chain_launch(h->chain, st);
+        case SB_MC_REC: return sb::mc_rec_launch(h->rec, st);
+        case SB_MC_DM: return parity < 0 ? sb::mc_dm_launch(h->dm, 0, 0, st) : sb::mc_dm_launch(h->dm, 1, parity, st);
+        default: return sb::fail(SB_EINVAL, "sb_mc_stage: no stage %d", stage);
+    }
 }
 
 extern "C" void sb_mc_destroy(sb_mc_handle *h) { delete h; }

@@ -28,7 +28,10 @@ inline size_t mc_align(size_t b) { return (b + 255) & ~(size_t)255; }
 // stages 1-3: layer parameters, layers, propagation (three launches)
 size_t mc_atmo_workspace(const sb_mc_group *g, int n);
 int mc_atmo_prepare(const sb_mc_group *g, int n, void *ws, McBlob &blob, cudaStream_t st);
-int mc_atmo_launch(const McBlob &blob, cudaStream_t st);
+int mc_atmo_launch(const McBlob &blob, cudaStream_t st);          // advance + layers + propagation
+int mc_atmo_layers_launch(const McBlob &blob, cudaStream_t st);   // advance + layers
+// propagation reading mirror-phase buffer sel (0: dm_phase, 1: dm_phase_alt)
+int mc_prop_launch(const McBlob &blob, int sel, cudaStream_t st);
 
 // stage 4: SH forward (one launch)
 size_t mc_sh_workspace(const sb_mc_group *g, int n);
@@ -44,6 +47,7 @@ int mc_chain_launch(const McBlob &blob, cudaStream_t st);
 size_t mc_control_workspace(const sb_mc_group *g, int n);
 int mc_control_prepare(const sb_mc_group *g, int n, void *ws, McBlob &rec, McBlob &dm, cudaStream_t st);
 int mc_rec_launch(const McBlob &blob, cudaStream_t st);
-int mc_dm_launch(const McBlob &blob, cudaStream_t st);
+// mirror from commands (cmd 0) or commands_next (1) into buffer sel
+int mc_dm_launch(const McBlob &blob, int cmd, int sel, cudaStream_t st);
 
 }  // namespace sb

@@ -26,15 +26,16 @@ def _state(sys_b):
     return out
 
 
-def _run(dft, mc):
+def _run(dft, mc, pipelined=False, steps=STEPS):
     from specula_b200.batched import BatchedScao, mc_groups
     sys_b = BatchedScao(mc_groups(n_real=N_REAL), device_idx=0, dft=dft)
     sys_b.start()
     if mc:
-        sys_b.capture_mc()
+        sys_b.capture_mc(pipelined=pipelined)
     else:
         sys_b.capture()
-    for _ in range(STEPS):
+    assert steps % sys_b.steps_per_replay == 0
+    for _ in range(steps // sys_b.steps_per_replay):
         sys_b.replay()
     torch.cuda.synchronize()
     from specula_b200 import _lib
@@ -55,6 +56,18 @@ def test_mc_step_equals_group_graph(cuda, dft):
     # the loop moved: slopes and mirror non-trivial
     assert all(float(st['S'].abs().max()) > 0 for st in got)
     assert all(float(st['dm_phase'].abs().max()) > 0 for st in got)
+    mc_sys.release_mc()
+
+
+def test_pipelined_mc_step_equals_group_graph(cuda):
+    """The mirror projection of each step on a second stream (two steps per
+    replay, sb_mc_stage): the same bits after four steps."""
+    ref_sys, ref = _run('split_bf16', mc=False, steps=4)
+    mc_sys, got = _run('split_bf16', mc=True, pipelined=True, steps=4)
+    assert mc_sys.steps_per_replay == 2 and mc_sys.launches_per_step == 7
+    for gi, (a, b) in enumerate(zip(ref, got)):
+        for k in a:
+            assert torch.equal(a[k], b[k]), (gi, k, float((a[k].double() - b[k].double()).abs().max()))
     mc_sys.release_mc()
 
 
