@@ -498,9 +498,10 @@ def bench_batched(dev, steps, cpu_budget_s):
            'mc_step_pipelined_split_bf16_ms_per_step': mc[('split_bf16', True)][0],
            'mc_step_launches_per_step': mc[('split_bf16', True)][1],
            'mc_step_realisation_steps_per_s': n_real / (min(v[0] for v in mc.values()) / 1e3),
-           'mc_step': 'sb_mc_step: seven launches per step (layer parameters, layers, propagation, SH, '
+           'mc_step': 'sb_mc_step: six launches per step (layer parameters, layers + on-axis field, SH, '
                       'normalisation + detector + slopes, reconstructor + integrators, mirror), each over every '
-                      'realisation of every group, captured in one graph',
+                      'realisation of every group, captured in one graph; pipelined: the mirror of each step on a '
+                      'second stream beside its other stages',
            'autotune_s': tune_s,
            'autotune': [{k: r[k] for k in ('family', 'shape', 'variant', 'name', 'times_us', 'speedup_vs_variant0',
                                            'cached')} for r in tuner.results],

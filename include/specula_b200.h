@@ -676,15 +676,17 @@ int sb_psf_tc(const float *A, const float *phase_nm, int m, int n, float phase_t
  * detector seeds; each stage of the step is ONE launch over every
  * realisation of every group:
  *   1 layer positions + per-step parameters    (atmo_evolution.py:258-277)
- *   2 every turbulence layer                     (atmo_evolution.py:278-294)
- *   3 on-axis propagation                        (atmo_propagation.py:105-144)
- *   4 SH forward, unnormalised + partial sums    (sh.py:348-420)
- *   5 photon normalisation, CCD, CoG slopes, flux cut-off, detector state
+ *   2 every turbulence layer and the on-axis field
+ *                                                (atmo_evolution.py:278-294,
+ *                                                 atmo_propagation.py:105-144)
+ *   3 SH forward, unnormalised + partial sums    (sh.py:348-420)
+ *   4 photon normalisation, CCD, CoG slopes, flux cut-off, detector state
  *                                                (sh.py:422-428, ccd.py:198-287,
  *                                                 sh_slopec.py:308-438)
- *   6 reconstructor rows + integrators           (modalrec.py:114-162,
+ *   5 reconstructor rows + integrators           (modalrec.py:114-162,
  *                                                 iir_filter.py:100-211)
- *   7 mirror projection                          (dm.py:72-86)
+ *   6 mirror projection                          (dm.py:72-86)
+ * (stage 2 is two launches when a group has more than 16 layers)
  * Each stage computes what the group-by-group batched calls compute
  * (sb_atmo_evolve_batched, sb_propagate_batched, sb_sh_forward[_split_bf16]_batched,
  * sb_ccd_step_batched, sb_slopec_batched, sb_modalrec_batched,
@@ -706,7 +708,7 @@ int sb_psf_tc(const float *A, const float *phase_nm, int m, int n, float phase_t
  *   sb_mc_destroy          frees the handle
  * ---------------------------------------------------------------------- */
 #define SB_MC_MAX_GROUPS 8
-#define SB_MC_LAUNCHES 7
+#define SB_MC_LAUNCHES 6
 
 typedef struct sb_mc_group {
     int n_batch;                        /* realisations                                */
@@ -770,21 +772,20 @@ void sb_mc_destroy(sb_mc_handle *handle);
 /* One stage of the step on a stream of the caller's choice, so that the
  * mirror projection of step t can overlap the other stages of step t (the
  * integrators' output for step t is known after step t-1, for integer
- * delays >= 1).  parity -1: the stages of sb_mc_step (propagation reads
+ * delays >= 1).  parity -1: the stages of sb_mc_step (the field takes
  * dm_phase, the mirror writes it from commands).  parity p = t % 2, with
- * dm_phase_alt and commands_next set: SB_MC_PROP reads buffer p ^ 1 and
- * SB_MC_DM writes buffer p (0: dm_phase, 1: dm_phase_alt) from
+ * dm_phase_alt and commands_next set: SB_MC_ATMO's field takes buffer p ^ 1
+ * and SB_MC_DM writes buffer p (0: dm_phase, 1: dm_phase_alt) from
  * commands_next.  Step t then runs, with DM(t) on a second stream:
  *   second stream: wait for REC(t-1); DM(t)
- *   first stream:  ATMO, PROP, SH, CHAIN; wait for DM(t); REC
+ *   first stream:  ATMO, SH, CHAIN; wait for DM(t); REC
  * after one sb_mc_step (which fills commands_next and dm_phase) as step
  * t = 0, i.e. parities 1, 0, 1, ...  The results equal sb_mc_step's. */
-#define SB_MC_ATMO 0    /* layer parameters + layers (two launches) */
-#define SB_MC_PROP 1
-#define SB_MC_SH 2
-#define SB_MC_CHAIN 3
-#define SB_MC_REC 4
-#define SB_MC_DM 5
+#define SB_MC_ATMO 0    /* stages 1-2 (two launches) */
+#define SB_MC_SH 1
+#define SB_MC_CHAIN 2
+#define SB_MC_REC 3
+#define SB_MC_DM 4
 int sb_mc_stage(const sb_mc_handle *handle, int stage, int parity, void *stream);
 
 #ifdef __cplusplus

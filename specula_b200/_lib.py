@@ -82,7 +82,7 @@ class PropLayer(C.Structure):
 
 
 SB_MC_MAX_GROUPS = 8
-SB_MC_LAUNCHES = 7
+SB_MC_LAUNCHES = 6
 
 
 class McGroup(C.Structure):
@@ -102,7 +102,7 @@ class McGroup(C.Structure):
                 ('dm_phase_alt', fp), ('commands_next', fp)]
 
 
-SB_MC_ATMO, SB_MC_PROP, SB_MC_SH, SB_MC_CHAIN, SB_MC_REC, SB_MC_DM = range(6)
+SB_MC_ATMO, SB_MC_SH, SB_MC_CHAIN, SB_MC_REC, SB_MC_DM = range(5)
 
 
 # name -> (restype, argtypes); every function of include/specula_b200.h

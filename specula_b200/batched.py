@@ -17,7 +17,7 @@ for up to 16 realisations).  ``capture()`` puts the step of every group into
 one CUDA graph, each group on a stream of its own.
 
 ``BatchedScao.capture_mc()`` puts the step of every group into the
-Monte-Carlo step of the C ABI instead (``sb_mc_step``): seven launches per
+Monte-Carlo step of the C ABI instead (``sb_mc_step``): six launches per
 step, each stage one launch over every realisation of every group, the same
 bits as the group-by-group graph.
 
@@ -399,7 +399,7 @@ class BatchedScao:
         return self._launches
 
     def capture_mc(self, pipelined=False):
-        """The batched step of every group as one sb_mc_step (seven launches,
+        """The batched step of every group as one sb_mc_step (six launches,
         each over every realisation of every group) captured in a CUDA graph.
         pipelined: two steps per replay, each step's mirror projection on a
         second (high-priority) stream overlapping the step's atmosphere, SH
@@ -438,7 +438,7 @@ class BatchedScao:
                 for p in (1, 0):
                     side.wait_stream(main)            # the commands of step t: after REC(t-1)
                     stage(_lib.SB_MC_DM, p, side)
-                    for k in (_lib.SB_MC_ATMO, _lib.SB_MC_PROP, _lib.SB_MC_SH, _lib.SB_MC_CHAIN):
+                    for k in (_lib.SB_MC_ATMO, _lib.SB_MC_SH, _lib.SB_MC_CHAIN):
                         stage(k, p, main)
                     main.wait_stream(side)            # REC(t) rewrites the next commands
                     stage(_lib.SB_MC_REC, p, main)

@@ -705,7 +705,8 @@ struct McAtmoArgs {
     LayerDyn *dyn;
     int n_groups, n_layers;
     McAtmoGroup g[sb::kMcMaxGroups];
-    int blk0[sb::kMcMaxGroups + 1];  // evolve CTAs before each group
+    int blk0[sb::kMcMaxGroups + 1];   // evolve CTAs before each group
+    int fblk0[sb::kMcMaxGroups + 1];  // fused evolve + propagation CTAs before each group
 };
 
 struct McPropGroup {
@@ -728,7 +729,7 @@ struct McPropArgs {
 struct McAtmoBlob {
     McAtmoArgs atmo;
     McPropArgs prop;
-    int evolve_blocks, prop_blocks, n_real;
+    int evolve_blocks, prop_blocks, n_real, fused_blocks, fused;
 };
 
 __global__ void __launch_bounds__(256) mc_atmo_advance_kernel(McAtmoArgs a) {
@@ -763,6 +764,67 @@ __global__ void __launch_bounds__(256) mc_atmo_evolve_kernel(McAtmoArgs a) {
     const TileSrc src{&ly.layer, ly.ptr.pos, a.dyn + li, L, tx * kTile, ty * kTile};
     float *out = ly.layer.out;
     evolve_tile(src, Q, fp, lyd, [&](int, int y, int x, float v) { out[(size_t)y * L + x] = v; });
+}
+
+// Layers and field in one launch: a CTA is one 32 x 32 tile of one
+// realisation; its layers are evaluated in turn, software-pipelined and
+// written as in atmo_propagate_kernel, and summed in registers in layer
+// order, then the stop and mirror terms are applied in propagate_field's
+// order (the same bits as mc_atmo_evolve_kernel + mc_propagate_kernel).
+__global__ void __launch_bounds__(256, 3) mc_atmo_propagate_kernel(McAtmoArgs a, McPropArgs f) {
+    __shared__ float Q[2][kBox][kBox + 1];
+    __shared__ TileFootprint fp[kFusedMaxLayers];
+    __shared__ LayerDyn lyd[kFusedMaxLayers];
+    const int blk = blockIdx.x;
+    int g = 0;
+    while (g + 1 < a.n_groups && blk >= a.fblk0[g + 1]) ++g;
+    const int tiles = a.g[g].tiles, L = a.g[g].L;
+    const int t2 = tiles * tiles, local = blk - a.fblk0[g];
+    const int b = local / t2, tt = local - b * t2;
+    const int ty = tt / tiles, tx = tt - ty * tiles;
+    const int x0 = tx * kTile, y0 = ty * kTile;
+    const McPropGroup &G = f.g[g];
+    const int n = G.n_atm, l0 = a.g[g].layer0 + b * n;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    auto src = [&](int li) {
+        const McAtmoLayer &ly = a.layers[li];
+        return TileSrc{&ly.layer, ly.ptr.pos, a.dyn + li, L, x0, y0};
+    };
+    if (tid < n) tile_footprint(src(l0 + tid), lyd[tid], fp[tid]);
+    float acc[kTile / kRowStep];
+#pragma unroll
+    for (int j = 0; j < kTile / kRowStep; ++j) acc[j] = 0.0f;
+    __syncthreads();
+    if (n > 0) {
+        TileLoads t;
+        tile_load(src(l0), lyd[0], fp[0], tid, t);
+        for (int k = 0; k < n; ++k) {
+            tile_stage(Q[k & 1], t);
+            if (k + 1 < n) tile_load(src(l0 + k + 1), lyd[k + 1], fp[k + 1], tid, t);
+            __syncthreads();
+            float *out = a.layers[l0 + k].layer.out;
+            tile_values(L, x0, y0, Q[k & 1], lyd[k], fp[k], [&](int j, int y, int x, float v) {
+                out[(size_t)y * L + x] = v;
+                acc[j] = __fadd_rn(acc[j], v);
+            });
+        }
+    }
+    const int x = x0 + threadIdx.x;
+    if (x >= L) return;
+    const float *dp = G.dm_phase[f.sel] + b * G.dm_stride;
+#pragma unroll
+    for (int j = 0; j < kTile / kRowStep; ++j) {
+        const int y = y0 + (int)threadIdx.y + kRowStep * j;
+        if (y >= L) break;
+        const long long e = (long long)y * L + x;
+        float amp = 1.0f, ph = acc[j];
+        if (G.stop_A) amp = __fmul_rn(amp, G.stop_A[e]);
+        if (G.stop_phase) ph = __fadd_rn(ph, G.stop_phase[e]);
+        if (G.dm_A) amp = __fmul_rn(amp, G.dm_A[e]);
+        ph = __fadd_rn(ph, dp[e]);
+        G.A[b * G.out_stride + e] = amp;
+        G.P[b * G.out_stride + e] = ph;
+    }
 }
 
 __global__ void __launch_bounds__(256) mc_propagate_kernel(McPropArgs a) {
@@ -800,7 +862,7 @@ int mc_atmo_prepare(const sb_mc_group *gs, int n, void *ws, McBlob &blob, cudaSt
     a.dyn = reinterpret_cast<LayerDyn *>(static_cast<unsigned char *>(ws) + mc_align(nl * sizeof(McAtmoLayer)));
     a.n_groups = p.n_groups = n;
     a.n_layers = (int)nl;
-    int k = 0, blocks = 0, real = 0, max_n = 1;
+    int k = 0, blocks = 0, real = 0, max_n = 1, fblocks = 0, fused = 1;
     for (int g = 0; g < n; ++g) {
         const sb_mc_group &G = gs[g];
         const int L = G.L, cnt = G.n_batch * G.n_atm;
@@ -814,6 +876,9 @@ int mc_atmo_prepare(const sb_mc_group *gs, int n, void *ws, McBlob &blob, cudaSt
         a.g[g].L = L;
         a.g[g].tiles = tiles;
         a.blk0[g] = blocks;
+        a.fblk0[g] = fblocks;
+        fblocks += G.n_batch * tiles * tiles;
+        fused &= G.n_atm <= kFusedMaxLayers;
         for (int j = 0; j < cnt; ++j, ++k) {
             const sb_atmo_layer_inputs &li = G.inputs[j];
             tab[k].layer = G.layers[j];
@@ -853,7 +918,10 @@ int mc_atmo_prepare(const sb_mc_group *gs, int n, void *ws, McBlob &blob, cudaSt
         max_n = nn > max_n ? (int)nn : max_n;
     }
     a.blk0[n] = blocks;
+    a.fblk0[n] = fblocks;
     p.real0[n] = real;
+    B->fused_blocks = fblocks;
+    B->fused = fused;
     B->evolve_blocks = blocks;
     B->n_real = real;
     const int nblk = (max_n + 255) / 256;
@@ -866,29 +934,29 @@ int mc_atmo_prepare(const sb_mc_group *gs, int n, void *ws, McBlob &blob, cudaSt
     return SB_OK;
 }
 
-int mc_atmo_layers_launch(const McBlob &blob, cudaStream_t st) {
-    const McAtmoBlob *B = reinterpret_cast<const McAtmoBlob *>(blob.b);
-    if (B->atmo.n_layers == 0) return SB_OK;
-    mc_atmo_advance_kernel<<<(B->atmo.n_layers + 255) / 256, 256, 0, st>>>(B->atmo);
-    int rc = check_launch("mc_atmo_advance_kernel");
-    if (rc) return rc;
-    mc_atmo_evolve_kernel<<<B->evolve_blocks, dim3(32, kRowStep), 0, st>>>(B->atmo);
-    return check_launch("mc_atmo_evolve_kernel");
-}
-
-int mc_prop_launch(const McBlob &blob, int sel, cudaStream_t st) {
+int mc_atmo_launch(const McBlob &blob, int sel, cudaStream_t st) {
     const McAtmoBlob *B = reinterpret_cast<const McAtmoBlob *>(blob.b);
     McPropArgs p = B->prop;
     p.sel = sel;
     for (int g = 0; g < p.n_groups; ++g)
         if (!p.g[g].dm_phase[sel]) return fail(SB_EINVAL, "sb_mc_stage: group %d has no second mirror buffer", g);
+    if (B->atmo.n_layers > 0) {
+        mc_atmo_advance_kernel<<<(B->atmo.n_layers + 255) / 256, 256, 0, st>>>(B->atmo);
+        const int rc = check_launch("mc_atmo_advance_kernel");
+        if (rc) return rc;
+    }
+    if (B->fused) {
+        mc_atmo_propagate_kernel<<<B->fused_blocks, dim3(32, kRowStep), 0, st>>>(B->atmo, p);
+        return check_launch("mc_atmo_propagate_kernel");
+    }
+    // a group with more layers than the fused kernel stages: layers, then the field
+    if (B->atmo.n_layers > 0) {
+        mc_atmo_evolve_kernel<<<B->evolve_blocks, dim3(32, kRowStep), 0, st>>>(B->atmo);
+        const int rc = check_launch("mc_atmo_evolve_kernel");
+        if (rc) return rc;
+    }
     mc_propagate_kernel<<<dim3(B->prop_blocks, B->n_real), 256, 0, st>>>(p);
     return check_launch("mc_propagate_kernel");
-}
-
-int mc_atmo_launch(const McBlob &blob, cudaStream_t st) {
-    const int rc = mc_atmo_layers_launch(blob, st);
-    return rc ? rc : mc_prop_launch(blob, 0, st);
 }
 
 }  // namespace sb

@@ -538,15 +538,15 @@ __global__ void __launch_bounds__(32 * (kDbWarps * RS + 1), 1)
 // is 256*NBX columns with 2*NBX consumer warps, and every column still sums
 // its modes in order from 0: the phases are bit-identical to the scalar
 // form with one mode-row group.
-template <int NBX>
+template <int NBX, int ST = kDbStages>
 size_t dm_c4_smem_bytes(int nmodes, int nb_max) {
     constexpr int rows = kDmRows / NBX;
     const int nst = (nmodes + rows - 1) / rows;
-    return 1024 + (size_t)kDbStages * kDmRows * kDmCols * 4 + 2 * kDbStages * 8 + (size_t)nst * rows * nb_max * 4;
+    return 1024 + (size_t)ST * kDmRows * kDmCols * 4 + 2 * ST * 8 + (size_t)nst * rows * nb_max * 4;
 }
 
-// the tiles bid, bid + nblk, ... of the columns
-template <int NB, int NBX>
+// the tiles bid, bid + nblk, ... of the columns; ST stages in the ring
+template <int NB, int NBX, int ST = kDbStages>
 __device__ __forceinline__ void dm_c4_body(const CUtensorMap &map, int nmodes, int nvalid, const float *__restrict__ cmd,
                                            int ldc, int nb, float sign, const int32_t *__restrict__ idx,
                                            float *__restrict__ phase, long long phase_stride, int bid, int nblk) {
@@ -558,14 +558,14 @@ __device__ __forceinline__ void dm_c4_body(const CUtensorMap &map, int nmodes, i
     extern __shared__ unsigned char smem_raw[];
     unsigned char *base = smem_raw + ((1024 - (sb::smem_u32(smem_raw) & 1023)) & 1023);
     float *ring = reinterpret_cast<float *>(base);
-    uint64_t *full = reinterpret_cast<uint64_t *>(base + (size_t)kDbStages * kDmRows * kDmCols * 4);
-    uint64_t *empty = full + kDbStages;
-    float *c = reinterpret_cast<float *>(empty + kDbStages);       // [mode][NB]
+    uint64_t *full = reinterpret_cast<uint64_t *>(base + (size_t)ST * kDmRows * kDmCols * 4);
+    uint64_t *empty = full + ST;
+    float *c = reinterpret_cast<float *>(empty + ST);       // [mode][NB]
     __shared__ int abort_flag, issued;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nst = (nmodes + ROWS - 1) / ROWS;
     if (tid == 0) {
-        for (int s = 0; s < kDbStages; ++s) {
+        for (int s = 0; s < ST; ++s) {
             sb::mbar_init(&full[s], 1);
             sb::mbar_init(&empty[s], NCW);
         }
@@ -586,8 +586,8 @@ __device__ __forceinline__ void dm_c4_body(const CUtensorMap &map, int nmodes, i
             const uint64_t pol = sb::l2_evict_first_policy();
             int q = 0;
             for (; q < total; ++q) {
-                const int slot = q % kDbStages;
-                if (q >= kDbStages && !sb::mbar_wait(&empty[slot], ((q / kDbStages) - 1) & 1)) {
+                const int slot = q % ST;
+                if (q >= ST && !sb::mbar_wait(&empty[slot], ((q / ST) - 1) & 1)) {
                     atomicExch(&g_dm_status, 5);
                     abort_flag = 1;
                     break;
@@ -611,9 +611,9 @@ __device__ __forceinline__ void dm_c4_body(const CUtensorMap &map, int nmodes, i
 #pragma unroll
             for (int b = 0; b < NB; ++b) acc[j][b] = 0.f;
         for (int q = 0; q < total; ++q) {
-            const int slot = q % kDbStages;
+            const int slot = q % ST;
             // warp-uniform decisions: the lanes meet in __syncwarp below
-            if (!__all_sync(0xffffffffu, sb::mbar_wait(&full[slot], (q / kDbStages) & 1))) {
+            if (!__all_sync(0xffffffffu, sb::mbar_wait(&full[slot], (q / ST) & 1))) {
                 if (lane == 0) atomicExch(&g_dm_status, 6);
                 abort_flag = 1;
                 break;
@@ -659,7 +659,7 @@ __device__ __forceinline__ void dm_c4_body(const CUtensorMap &map, int nmodes, i
     }
     __syncthreads();
     if (abort_flag && tid == 0) {
-        for (int q = 0; q < issued; ++q) sb::mbar_wait(&full[q % kDbStages], (q / kDbStages) & 1);
+        for (int q = 0; q < issued; ++q) sb::mbar_wait(&full[q % ST], (q / ST) & 1);
     }
 }
 
@@ -760,6 +760,9 @@ namespace {
 constexpr int kMcRecRows = 2;          // reconstructor rows per CTA
 constexpr int kMcChunk = 16;           // realisations per job
 constexpr int kMcDmNbx = 4;            // boxes per mirror stage
+// ring stages of the mirror launch: three (about 130 KB of shared memory)
+// leave room on each SM for CTAs of the stages it overlaps
+constexpr int kMcDmStages = 3;
 
 struct McRecJob {
     const float *R, *S;
@@ -825,11 +828,11 @@ __global__ void __launch_bounds__(32 * (2 * kMcDmNbx + 1), 1) mc_dm_kernel(const
     const McDmJob &J = m.jobs[m.cta_job[blockIdx.x]];
     const int bid = blockIdx.x - J.cta0;
     if (J.nb <= 8)
-        dm_c4_body<8, kMcDmNbx>(m.map[J.g], J.nmodes, J.nvalid, J.cmd[m.cmd], J.ldc, J.nb, J.sign, J.idx,
-                                J.phase[m.sel], J.phase_stride, bid, J.ncta);
+        dm_c4_body<8, kMcDmNbx, kMcDmStages>(m.map[J.g], J.nmodes, J.nvalid, J.cmd[m.cmd], J.ldc, J.nb, J.sign,
+                                             J.idx, J.phase[m.sel], J.phase_stride, bid, J.ncta);
     else
-        dm_c4_body<16, kMcDmNbx>(m.map[J.g], J.nmodes, J.nvalid, J.cmd[m.cmd], J.ldc, J.nb, J.sign, J.idx,
-                                 J.phase[m.sel], J.phase_stride, bid, J.ncta);
+        dm_c4_body<16, kMcDmNbx, kMcDmStages>(m.map[J.g], J.nmodes, J.nvalid, J.cmd[m.cmd], J.ldc, J.nb, J.sign,
+                                              J.idx, J.phase[m.sel], J.phase_stride, bid, J.ncta);
 }
 
 int mc_jobs(const sb_mc_group *gs, int n) {
@@ -928,7 +931,8 @@ int mc_control_prepare(const sb_mc_group *gs, int n, void *ws, McBlob &rec, McBl
             d.g = g;
             d.sign = G.dm_sign;
             tiles[j] = (G.n_valid + TW - 1) / TW;
-            const size_t sm = nb <= 8 ? dm_c4_smem_bytes<kMcDmNbx>(nm, 8) : dm_c4_smem_bytes<kMcDmNbx>(nm, 16);
+            const size_t sm = nb <= 8 ? dm_c4_smem_bytes<kMcDmNbx, kMcDmStages>(nm, 8)
+                                      : dm_c4_smem_bytes<kMcDmNbx, kMcDmStages>(nm, 16);
             smem = sm > smem ? sm : smem;
         }
     }

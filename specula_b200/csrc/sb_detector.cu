@@ -616,6 +616,7 @@ constexpr int kChainSumThreads = 256;    // thread count whose summation orders 
 constexpr int kChainMaxThreads = 512;    // a CTA samples up to this many pixels per pass
 constexpr int kChainLenses = 8;          // lenslets per CTA: one CoG warp each
 constexpr int kChainMaxNpx = 16;
+constexpr int kChainTile = 4096;         // pixels of a CTA's lenslets (npx x width*npx)
 
 // threads of a CTA: the lenslet tile (npx x 8 npx pixels) in one pass when it
 // fits in 512, never fewer than the 256 whose sums are reproduced
@@ -657,15 +658,16 @@ struct ChainSlot {
 
 // the chain for lenslet block (bx, by) of one realisation; any CTA size from
 // 256 to 512 threads gives the same bits
-template <bool ROWS>
-__device__ __forceinline__ void chain_body(const ChainArgs &a, const ChainOff &o, int bx0, int nbx, int by,
+// the chain for lenslets j0 .. j0 + width - 1 of lenslet row by (their
+// npx x width*npx pixels staged in shared memory, at most kChainTile)
+__device__ __forceinline__ void chain_body(const ChainArgs &a, const ChainOff &o, int j0, int width, int by,
                                            const ChainSlot &slot) {
     __shared__ double dred[33];
     __shared__ float logfact[32];
     __shared__ int s_idx[kChainMaxThreads];
     __shared__ float s_mean[kChainMaxThreads];
     __shared__ int s_small[kChainMaxThreads / 32];
-    __shared__ float tile[kChainMaxNpx * kChainLenses * kChainMaxNpx];
+    __shared__ float tile[kChainTile];
     __shared__ int s_last, s_group_last;
     const sb_ccd_params &p = a.p;
     const float *part_I = a.part_I + o.part, *part_A = a.part_A + o.part;
@@ -694,12 +696,8 @@ __device__ __forceinline__ void chain_body(const ChainArgs &a, const ChainOff &o
     const float scale = phot / (float)si;
 
     const int i = by;
-    // lenslet blocks bx0 .. bx0 + nbx - 1 of row i, one after the other
-    const int nb = ROWS ? nbx : 1;
-    for (int bx = bx0; bx < bx0 + nb; ++bx) {
-    const int j0 = bx * kChainLenses;
-    const int w = min(kChainLenses, a.n - j0);
-    const int npx = a.npx, wc = w * npx, P = npx * wc, tld = kChainLenses * npx;
+    const int w = min(width, a.n - j0);
+    const int npx = a.npx, wc = w * npx, P = npx * wc, tld = wc;
     // detector: every pass samples up to blockDim pixels of the tile (one pass
     // for npx <= 8), ordered by Poisson sampler branch as in ccd_kernel (the
     // draws do not depend on the order)
@@ -752,13 +750,13 @@ __device__ __forceinline__ void chain_body(const ChainArgs &a, const ChainOff &o
     __syncthreads();
 
     // CoG sums, one warp per lenslet, in slopec_sums_kernel's lane order
-    if (warp < w) {
-        const int s = a.lenslet_subap[i * a.n + j0 + warp];
+    for (int k = warp; k < w; k += nwarps) {
+        const int s = a.lenslet_subap[i * a.n + j0 + k];
         if (s >= 0) {
             float fl = 0.f, t = 0.f, x = 0.f, y = 0.f;
             for (int e = lane; e < npx * npx; e += 32) {
                 const int r = e / npx, c = e - r * npx;
-                const float v = tile[r * tld + warp * npx + c];
+                const float v = tile[r * tld + k * npx + c];
                 fl += v;
                 float wv = v - a.thr;                 // pixels -= thr; clamp < 0 -> 0
                 wv = wv < 0.f ? 0.f : wv;
@@ -780,8 +778,6 @@ __device__ __forceinline__ void chain_body(const ChainArgs &a, const ChainOff &o
                 slopes[a.n_valid + s] = y * fac;
             }
         }
-    }
-    __syncthreads();                      // the next block refills the tile
     }
 
     // the last CTA sharing the frame state advances it; the last CTA of the
@@ -836,7 +832,7 @@ __device__ __forceinline__ void chain_body(const ChainArgs &a, const ChainOff &o
 
 __global__ void __launch_bounds__(kChainMaxThreads) sh_ccd_slopec_kernel(ChainArgs a) {
     const unsigned int ctas = gridDim.x * gridDim.y;
-    chain_body<false>(a, ChainOff{0, 0, 0, 0, 0}, blockIdx.x, 1, blockIdx.y,
+    chain_body(a, ChainOff{0, 0, 0, 0, 0}, blockIdx.x * kChainLenses, kChainLenses, blockIdx.y,
                ChainSlot{nullptr, nullptr, nullptr, ctas, ctas});
 }
 
@@ -1072,7 +1068,7 @@ struct McChainGroup {
     const uint64_t *photon_seeds, *readout_seeds;
     unsigned int *done;              // [n_batch] realisation counters
     int gx, gy, slopes_stride, flux_stride;
-    int tpc, row_blocks;             // lenslet blocks per CTA, blocks per lenslet row
+    int lpc;                         // lenslets per CTA (a lenslet row, or as much of it as the tile holds)
 };
 
 struct McChainArgs {
@@ -1106,8 +1102,7 @@ __global__ void __launch_bounds__(kChainSumThreads, 4) mc_chain_kernel(McChainAr
                        (size_t)b * G.flux_stride, (size_t)b * 3 * G.a.n_valid};
     const ChainSlot slot{G.photon_seeds + b, G.readout_seeds + b, G.done + b, (unsigned int)per,
                          (unsigned int)(m.blk0[g + 1] - m.blk0[g])};
-    const int bx0 = (rem % G.gx) * G.tpc;
-    chain_body<true>(G.a, off, bx0, min(G.tpc, G.row_blocks - bx0), rem / G.gx, slot);
+    chain_body(G.a, off, (rem % G.gx) * G.lpc, G.lpc, rem / G.gx, slot);
 }
 
 }  // namespace
@@ -1183,11 +1178,11 @@ int mc_chain_prepare(const sb_mc_group *gs, int n, const McShParts &parts, void 
         q.frame_stride = G.frame_stride;
         q.photon_seeds = G.photon_seeds;
         q.readout_seeds = G.readout_seeds;
-        // whole lenslet rows per CTA: the per-CTA work (normalisation sums,
-        // completion counters) is paid once per row
-        q.row_blocks = (nl + kChainLenses - 1) / kChainLenses;
-        q.tpc = q.row_blocks;
-        q.gx = 1;
+        // whole lenslet rows per CTA where the tile holds them: the per-CTA
+        // work (normalisation sums, completion counters) is paid once per
+        // row and the pixel passes run over the row
+        q.lpc = kChainTile / (npx * npx) < nl ? kChainTile / (npx * npx) : nl;
+        q.gx = (nl + q.lpc - 1) / q.lpc;
         q.gy = nl;
         q.slopes_stride = G.slopes_stride;
         q.flux_stride = G.flux_stride;

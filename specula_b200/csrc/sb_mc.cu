@@ -1,7 +1,7 @@
 // Monte-Carlo step over geometry groups: the plan and the C ABI.  The stages
 // live beside the kernels they reuse (sb_atmo.cu, sb_sh.cu, sb_detector.cu,
 // sb_control.cu); this file carves the workspace, has each stage build its
-// arguments once, and issues the seven launches of a step.
+// arguments once, and issues the six launches of a step.
 #include <new>
 
 #include "sb_mc.cuh"
@@ -74,7 +74,7 @@ extern "C" int sb_mc_step(const sb_mc_handle *h, void *stream) {
     sb::clear_error();
     if (!h) return sb::fail(SB_EINVAL, "sb_mc_step: null handle");
     cudaStream_t st = sb::as_stream(stream);
-    int rc = sb::mc_atmo_launch(h->atmo, st);
+    int rc = sb::mc_atmo_launch(h->atmo, 0, st);
     if (!rc) rc = sb::mc_sh_launch(h->sh, st);
     if (!rc) rc = sb::mc_chain_launch(h->chain, st);
     if (!rc) rc = sb::mc_rec_launch(h->rec, st);
@@ -88,8 +88,7 @@ extern "C" int sb_mc_stage(const sb_mc_handle *h, int stage, int parity, void *s
     if (parity < -1 || parity > 1) return sb::fail(SB_EINVAL, "sb_mc_stage: parity must be -1, 0 or 1");
     cudaStream_t st = sb::as_stream(stream);
     switch (stage) {
-        case SB_MC_ATMO: return sb::mc_atmo_layers_launch(h->atmo, st);
-        case SB_MC_PROP: return sb::mc_prop_launch(h->atmo, parity < 0 ? 0 : parity ^ 1, st);
+        case SB_MC_ATMO: return sb::mc_atmo_launch(h->atmo, parity < 0 ? 0 : parity ^ 1, st);
         case SB_MC_SH: return sb::mc_sh_launch(h->sh, st);
         case SB_MC_CHAIN: return sb::mc_chain_launch(h->chain, st);
         case SB_MC_REC: return sb::mc_rec_launch(h->rec, st);

@@ -25,25 +25,24 @@ struct McShParts {
 
 inline size_t mc_align(size_t b) { return (b + 255) & ~(size_t)255; }
 
-// stages 1-3: layer parameters, layers, propagation (three launches)
+// stages 1-2: layer parameters, then layers and the on-axis field in one
+// launch (a group of more than 16 layers: layers and field separately); the
+// field takes mirror-phase buffer sel (0: dm_phase, 1: dm_phase_alt)
 size_t mc_atmo_workspace(const sb_mc_group *g, int n);
 int mc_atmo_prepare(const sb_mc_group *g, int n, void *ws, McBlob &blob, cudaStream_t st);
-int mc_atmo_launch(const McBlob &blob, cudaStream_t st);          // advance + layers + propagation
-int mc_atmo_layers_launch(const McBlob &blob, cudaStream_t st);   // advance + layers
-// propagation reading mirror-phase buffer sel (0: dm_phase, 1: dm_phase_alt)
-int mc_prop_launch(const McBlob &blob, int sel, cudaStream_t st);
+int mc_atmo_launch(const McBlob &blob, int sel, cudaStream_t st);
 
-// stage 4: SH forward (one launch)
+// stage 3: SH forward (one launch)
 size_t mc_sh_workspace(const sb_mc_group *g, int n);
 int mc_sh_prepare(const sb_mc_group *g, int n, void *ws, McBlob &blob, McShParts &parts);
 int mc_sh_launch(const McBlob &blob, cudaStream_t st);
 
-// stage 5: normalisation, detector, slopes (one launch)
+// stage 4: normalisation, detector, slopes (one launch)
 size_t mc_chain_workspace(const sb_mc_group *g, int n);
 int mc_chain_prepare(const sb_mc_group *g, int n, const McShParts &parts, void *ws, McBlob &blob);
 int mc_chain_launch(const McBlob &blob, cudaStream_t st);
 
-// stages 6-7: reconstructor + integrators, mirror (two launches)
+// stages 5-6: reconstructor + integrators, mirror (two launches)
 size_t mc_control_workspace(const sb_mc_group *g, int n);
 int mc_control_prepare(const sb_mc_group *g, int n, void *ws, McBlob &rec, McBlob &dm, cudaStream_t st);
 int mc_rec_launch(const McBlob &blob, cudaStream_t st);

@@ -1,4 +1,4 @@
-"""Monte-Carlo step over geometry groups (sb_mc_step): seven launches per step,
+"""Monte-Carlo step over geometry groups (sb_mc_step): six launches per step,
 each over every realisation of every group, against the group-by-group
 graph of the same realisations (BatchedScao.capture), bit for bit, with the
 FP32 and the split-BF16 SH.  The mix is the Monte-Carlo benchmark's three
@@ -48,8 +48,8 @@ def test_mc_step_equals_group_graph(cuda, dft):
     ref_sys, ref = _run(dft, mc=False)
     mc_sys, got = _run(dft, mc=True)
     assert len(mc_sys.groups) == 6
-    assert mc_sys.launches_per_step == 7
-    assert ref_sys.launches_per_step > 7
+    assert mc_sys.launches_per_step == 6
+    assert ref_sys.launches_per_step > 8
     for gi, (a, b) in enumerate(zip(ref, got)):
         for k in a:
             assert torch.equal(a[k], b[k]), (dft, gi, k, float((a[k].double() - b[k].double()).abs().max()))
@@ -64,7 +64,7 @@ def test_pipelined_mc_step_equals_group_graph(cuda):
     replay, sb_mc_stage): the same bits after four steps."""
     ref_sys, ref = _run('split_bf16', mc=False, steps=4)
     mc_sys, got = _run('split_bf16', mc=True, pipelined=True, steps=4)
-    assert mc_sys.steps_per_replay == 2 and mc_sys.launches_per_step == 7
+    assert mc_sys.steps_per_replay == 2 and mc_sys.launches_per_step == 6
     for gi, (a, b) in enumerate(zip(ref, got)):
         for k in a:
             assert torch.equal(a[k], b[k]), (gi, k, float((a[k].double() - b[k].double()).abs().max()))
