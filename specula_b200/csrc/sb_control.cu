@@ -804,24 +804,35 @@ struct McDmBlob {
     size_t smem;
 };
 
+// realisations b0 .. b0 + nb - 1 of job J (nb <= NB)
 template <int NB>
-__device__ __forceinline__ void mc_rec_job(const McRecJob &J, int m0, const sb_iir_plan &p, float *out) {
-    gemv_rows_batched_body<NB, kMcRecRows>(J.R, J.nrows, J.ncols, J.ldr, J.S, J.lds, J.nb, J.vec2, m0,
-                                           [&](int m, int b, float t) {
-                                               J.M[(size_t)b * J.ldm + m] = t;
-                                               iir_update(p, J.e0 + b * J.nrows + m, t, out);
+__device__ __forceinline__ void mc_rec_job(const McRecJob &J, int b0, int nb, int m0, const sb_iir_plan &p,
+                                           float *out) {
+    gemv_rows_batched_body<NB, kMcRecRows>(J.R, J.nrows, J.ncols, J.ldr, J.S + (size_t)b0 * J.lds, J.lds, nb,
+                                           J.vec2, m0, [&](int m, int b, float t) {
+                                               J.M[(size_t)(b0 + b) * J.ldm + m] = t;
+                                               iir_update(p, J.e0 + (b0 + b) * J.nrows + m, t, out);
                                            });
 }
 
+// a job of more than 8 realisations in two passes of 8 over the reconstructor
+// rows (the sums of each (row, realisation) do not depend on the pass)
 __global__ void __launch_bounds__(256) mc_rec_kernel(McRecArgs m) {
     const int2 jb = m.blk[blockIdx.x];
     const McRecJob &J = m.jobs[jb.x];
     const int m0 = jb.y * kMcRecRows;
     const sb_iir_plan &p = m.iir[J.g];
     float *out = m.out[J.g];
-    if (J.nb <= 4) mc_rec_job<4>(J, m0, p, out);
-    else if (J.nb <= 8) mc_rec_job<8>(J, m0, p, out);
-    else mc_rec_job<16>(J, m0, p, out);
+    const int nb = J.nb;
+    if (nb <= 4) {
+        mc_rec_job<4>(J, 0, nb, m0, p, out);
+        return;
+    }
+    mc_rec_job<8>(J, 0, nb < 8 ? nb : 8, m0, p, out);
+    if (nb > 8) {
+        __syncthreads();                  // the reduction buffer is reused
+        mc_rec_job<8>(J, 8, nb - 8, m0, p, out);
+    }
 }
 
 __global__ void __launch_bounds__(32 * (2 * kMcDmNbx + 1), 1) mc_dm_kernel(const __grid_constant__ McDmArgs m) {
