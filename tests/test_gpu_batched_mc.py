@@ -80,3 +80,31 @@ def test_mc_step_rejects_unfusable_groups(cuda):
     sys_b.groups[0].loops[0].slopec.thr_pedestal = True
     with pytest.raises(NotImplementedError, match='fused detector'):
         sys_b.capture_mc()
+
+
+def test_single_system_step_through_the_c_abi(cuda):
+    """One group of one realisation: sb_mc_step is the whole loop step of one
+    SCAO system behind the C ABI (six launches).  Noise-free, against the
+    system's own sequential step graph (its single-vector reconstructor and
+    mirror kernels sum in another order): slopes and mirror phase within 1e-4
+    of their largest values over six steps."""
+    from specula_b200.batched import BatchedScao
+    from specula_b200.scao import ScaoConfig
+    from tests.cases import rel_max_err
+    cfg = ScaoConfig(photon_noise=False, readout_noise=0.0)
+    a = BatchedScao([(cfg, [cfg])], device_idx=0)
+    a.start()
+    a.capture_plain()
+    b = BatchedScao([(cfg, [cfg])], device_idx=0)
+    b.start()
+    b.capture_mc()
+    assert b.launches_per_step == 6
+    for _ in range(6):
+        a.replay_plain()
+        b.replay()
+        torch.cuda.synchronize()
+        ga, gb = a.groups[0], b.groups[0]
+        assert rel_max_err(gb.S.cpu().numpy(), ga.S.cpu().numpy()) <= 1e-4
+        assert rel_max_err(gb.dm_phase.cpu().numpy(), ga.dm_phase.cpu().numpy()) <= 1e-4
+    assert float(gb.S.abs().max()) > 0
+    b.release_mc()
