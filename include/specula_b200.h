@@ -443,6 +443,10 @@ int sb_device_status(void);
  *               sub-aperture with flux (then apply the cut-off from
  *               tot_out, as sb_intmat_contract does)
  * Threshold 0 only (the thresholded CoG is not differentiable).
+ * Geometries (np_sub, cutsize, subap_npx): (8, 12, 6), (8, 14, 8),
+ * (8, 16, 8), (8, 8, 8) and (16, 16, 8), the 2x-resampled 8-pixel lenslets
+ * of fov_ovs != 1 geometries (A and phase_nm are then the SH's resampled
+ * field; the host carries the resampling's transpose).
  * ---------------------------------------------------------------------- */
 
 /* jac[axis][s][r * np_sub + c] = d slope(axis, s) / d phase_nm at pixel

@@ -254,6 +254,7 @@ AdjKernel adjoint_kernel(int p, int cs, int npx) {
     if (p == 8 && cs == 14 && npx == 8) return adj_entry<8, 14, 8>();
     if (p == 8 && cs == 16 && npx == 8) return adj_entry<8, 16, 8>();
     if (p == 8 && cs == 8 && npx == 8) return adj_entry<8, 8, 8>();
+    if (p == 16 && cs == 16 && npx == 8) return adj_entry<16, 16, 8>();   // 2x-resampled 8-px lenslets
     return {nullptr, 0};
 }
 

@@ -21,6 +21,7 @@ on the same CUDA chain (one mode's influence function projected per step,
 SH forward, CoG), captured in one CUDA graph: the measured alternative.
 """
 import ctypes
+import warnings
 
 import numpy as np
 import torch
@@ -79,17 +80,66 @@ def row_segments(pix2col, lenslets, n_lenses, np_sub, field, ld_if):
     return seg, int(seg[:, 1].max()) if n_lenses else 0
 
 
+def resample_matrix(ext1, ext2, yy, xx, in_shape):
+    """The SH's field resampling as a sparse float64 matrix (see
+    _resample_matrix), built with torch's sparse index checks on."""
+    with torch.sparse.check_sparse_tensor_invariants(enable=True):
+        return _resample_matrix(ext1, ext2, yy, xx, in_shape)
+
+
+def _resample_matrix(ext1, ext2, yy, xx, in_shape):
+    """The SH's field resampling as a sparse float64 matrix (out pixels x in
+    pixels): edge extrapolation of the input phase (extrapolate_edge_pixel.py:
+    ext[k] = ph[k], ph[s1], or 2 ph[s1] - ph[s2]) followed by the bilinear
+    interpolation at (yy, xx) on the input grid (interp2d.py:95-122, the
+    weights of sb_interp2d_field).  Both steps are linear in the phase, so
+    the resampled phase of any phase map is this matrix times it."""
+    rows, cols = in_shape
+    n_in = rows * cols
+    s1 = torch.as_tensor(ext1, dtype=torch.int64).reshape(-1)
+    s2 = torch.as_tensor(ext2, dtype=torch.int64).reshape(-1)
+    k = torch.arange(n_in, dtype=torch.int64)
+    own = s1 < 0
+    one = (~own) & (s2 < 0)
+    two = (~own) & (s2 >= 0)
+    er = torch.cat([k[own], k[one], k[two], k[two]])
+    ec = torch.cat([k[own], s1[one], s1[two], s2[two]])
+    ev = torch.cat([torch.ones(int(own.sum()), dtype=torch.float64), torch.ones(int(one.sum()), dtype=torch.float64),
+                    torch.full((int(two.sum()),), 2.0, dtype=torch.float64),
+                    torch.full((int(two.sum()),), -1.0, dtype=torch.float64)])
+    E = torch.sparse_coo_tensor(torch.stack([er, ec]), ev, (n_in, n_in), check_invariants=True).coalesce()
+    y = torch.as_tensor(yy, dtype=torch.float64).reshape(-1)
+    x = torch.as_tensor(xx, dtype=torch.float64).reshape(-1)
+    y0 = torch.clamp(torch.floor(y), 0, rows - 2)
+    x0 = torch.clamp(torch.floor(x), 0, cols - 2)
+    fy, fx = y - y0, x - x0
+    i00 = (y0 * cols + x0).long()
+    n_out = y.numel()
+    o = torch.arange(n_out, dtype=torch.int64)
+    ir = torch.cat([o, o, o, o])
+    ic = torch.cat([i00, i00 + 1, i00 + cols, i00 + cols + 1])
+    iv = torch.cat([(1 - fy) * (1 - fx), (1 - fy) * fx, fy * (1 - fx), fy * fx])
+    Ip = torch.sparse_coo_tensor(torch.stack([ir, ic]), iv, (n_out, n_in), check_invariants=True).coalesce()
+    with warnings.catch_warnings():
+        warnings.filterwarnings('ignore', message='Sparse CSR tensor support is in beta')
+        return torch.sparse.mm(Ip, E).coalesce()
+
+
 class ShSlopesAdjoint:
     """Jacobian / VJP of the slopes of a set-up ``SH`` + ``ShSlopec`` pair
     with respect to the SH input phase (nm), and the adjoint interaction
-    matrix.  Noise-free detector, CoG threshold 0, no field interpolation
-    (fov_ovs_coeff giving one phase sample per lenslet pixel)."""
+    matrix.  Noise-free detector, CoG threshold 0.
+
+    Geometries that resample the field (fov_ovs != 1, sh.py:353-357,447-460):
+    ``slopes``, ``vjp`` and ``intmat`` take the SH's input field (its grid)
+    and run the SH's edge extrapolation and interpolation first; ``vjp``
+    returns the gradient on the input grid through the transpose of that
+    linear map, ``intmat`` contracts with the influence functions resampled
+    by it; ``jacobian`` stays with respect to the resampled phase samples."""
 
     def __init__(self, sh, slopec):
         g = sh.geometry
-        if g.do_interpolation:
-            raise NotImplementedError('ShSlopesAdjoint: geometries that resample the field (fov_ovs != 1) '
-                                      'are not supported')
+        self.interp = bool(g.do_interpolation)
         if slopec.thr_value > 0:
             raise ValueError('ShSlopesAdjoint: the thresholded CoG is not differentiable (thr_value must be <= 0)')
         self.sh = sh
@@ -112,6 +162,14 @@ class ShSlopesAdjoint:
         self._flux = torch.empty(self.n_valid, dtype=torch.float32, device=self.device)
         nb = _lib.load().sb_slopec_scratch_bytes(ctypes.byref(self._slopec_plan()))
         self._sc_scratch = torch.empty(max(nb, 1), dtype=torch.uint8, device=self.device)
+        if self.interp:
+            self.in_shape = tuple(sh._in_ef.phaseInNm.shape)
+            self._pext = torch.empty(self.in_shape, dtype=torch.float32, device=self.device)
+            self._Ai = torch.empty((self.field, self.field), dtype=torch.float32, device=self.device)
+            self._Pi = torch.empty((self.field, self.field), dtype=torch.float32, device=self.device)
+            self._M = None
+        else:
+            self.in_shape = (self.field, self.field)
 
     # -- plumbing ---------------------------------------------------------
     def _slopec_plan(self):
@@ -125,9 +183,32 @@ class ShSlopesAdjoint:
 
     def _field(self, t, name):
         t = torch.as_tensor(t, dtype=torch.float32, device=self.device)
-        if t.shape != (self.field, self.field) or not t.is_contiguous():
-            raise ValueError(f'ShSlopesAdjoint: {name} must be a contiguous {self.field}x{self.field} array')
+        if tuple(t.shape) != self.in_shape or not t.is_contiguous():
+            raise ValueError(f'ShSlopesAdjoint: {name} must be a contiguous {self.in_shape[0]}x{self.in_shape[1]} '
+                             'array')
         return t
+
+    def resampled(self, A, phase, st=None):
+        """The field the SH kernels see: (A, phase) itself, or with
+        resampling the SH's extrapolated and interpolated field (the calls of
+        SH.trigger_code; internal buffers)."""
+        if not self.interp:
+            return A, phase
+        sh = self.sh
+        st = self._stream() if st is None else st
+        _lib.call('sb_edge_extrapolate', phase.data_ptr(), sh._ext1.data_ptr(), sh._ext2.data_ptr(), phase.numel(),
+                  self._pext.data_ptr(), st)
+        _lib.call('sb_interp2d_field', A.data_ptr(), self._pext.data_ptr(), self.in_shape[0], self.in_shape[1],
+                  sh._yy.data_ptr(), sh._xx.data_ptr(), sh._yy.numel(), self._Ai.data_ptr(), self._Pi.data_ptr(), st)
+        return self._Ai, self._Pi
+
+    def resample_matrix(self):
+        """The resampling as a sparse float64 matrix on the device (built once)."""
+        if self._M is None:
+            sh = self.sh
+            self._M = resample_matrix(sh._ext1.cpu(), sh._ext2.cpu(), sh._yy.cpu(), sh._xx.cpu(),
+                                      self.in_shape).to(self.device)
+        return self._M
 
     def _weights(self):
         sc = self.slopec
@@ -142,7 +223,8 @@ class ShSlopesAdjoint:
         phase = self._field(phase, 'phase')
         st = self._stream()
         sh = self.sh
-        _lib.call('sb_sh_forward', ctypes.byref(sh._plan), A.data_ptr(), phase.data_ptr(), A.data_ptr(), A.numel(),
+        Af, Pf = self.resampled(A, phase)
+        _lib.call('sb_sh_forward', ctypes.byref(sh._plan), Af.data_ptr(), Pf.data_ptr(), A.data_ptr(), A.numel(),
                   1.0, self._frame.data_ptr(), sh._scratch.data_ptr(), sh._scratch.numel(), st)
         _lib.call('sb_slopec', ctypes.byref(self._slopec_plan()), self._frame.data_ptr(), self._slopes.data_ptr(),
                   self._flux.data_ptr(), self._sc_scratch.data_ptr(), self._sc_scratch.numel(), st)
@@ -172,9 +254,11 @@ class ShSlopesAdjoint:
     def jacobian(self, A, phase, active=None):
         """(2, n_valid, np_sub^2): d slope / d phase_nm per valid sub-aperture
         (zero for sub-apertures the CoG cuts off at (A, phase), or outside
-        ``active`` when given)."""
+        ``active`` when given); with resampling, with respect to the resampled
+        phase samples."""
         A = self._field(A, 'A')
         phase = self._field(phase, 'phase')
+        A, phase = self.resampled(A, phase)
         if active is not None:
             return self._jacobian(A, phase, torch.as_tensor(active, dtype=torch.float32,
                                                             device=self.device).contiguous())
@@ -191,12 +275,17 @@ class ShSlopesAdjoint:
             raise ValueError(f'ShSlopesAdjoint.vjp: seed has {seed.numel()} entries, expected {2 * self.n_valid}')
         if active is None:
             active = self.active(A, phase)
+        Af, Pf = self.resampled(A, phase)
         grad = torch.zeros((self.field, self.field), dtype=torch.float32, device=self.device)
         xw, yw, mw = self._weights()
-        _lib.call('sb_sh_slopes_vjp', ctypes.byref(self.sh._plan), A.data_ptr(), phase.data_ptr(), self.n_valid,
+        _lib.call('sb_sh_slopes_vjp', ctypes.byref(self.sh._plan), Af.data_ptr(), Pf.data_ptr(), self.n_valid,
                   self._lenslet.data_ptr(), xw, yw, mw, active.data_ptr(), seed.data_ptr(), grad.data_ptr(),
                   self._stream())
-        return grad
+        if not self.interp:
+            return grad
+        # back through the resampling: its transpose, in float64
+        g = torch.sparse.mm(self.resample_matrix().t(), grad.reshape(-1, 1).double())
+        return g.reshape(self.in_shape).float()
 
     def pixel_to_column(self, dm, top=0, left=0):
         shape = tuple(dm.layer.phaseInNm.shape)
@@ -214,25 +303,57 @@ class ShSlopesAdjoint:
             A = self._field(A, 'A')
             phase = self._field(phase, 'phase')
             if active is None:
-                jac = self._jacobian(A, phase, None)
+                jac = self._jacobian(*self.resampled(A, phase), None)
                 tot = self._tot
             else:
                 jac = self.jacobian(A, phase, active)
-        if pix2col is None:
-            pix2col = self.pixel_to_column(dm, top, left)
         n_modes = dm._IF.shape[0]
+        if self.interp:
+            IF, ld, pix2col = self.resampled_ifunc(dm, top, left)
+        else:
+            IF, ld = dm._IF, dm._ld
+            if pix2col is None:
+                pix2col = self.pixel_to_column(dm, top, left)
         im = torch.empty((n_modes, 2 * self.n_valid), dtype=torch.float32, device=self.device)
-        segs = self._segments(pix2col, dm)
+        segs = self._segments(pix2col, IF, ld)
         tot_ptr = 0 if tot is None else tot.data_ptr()
         if segs is not None:
             _lib.call('sb_intmat_contract_rows', jac.data_ptr(), tot_ptr, self.n_valid, self.np_sub, self.n_lenses,
                       self.field, self._slot.data_ptr(), pix2col.data_ptr(), segs[0].data_ptr(), segs[1],
-                      dm._IF.data_ptr(), n_modes, dm._ld, float(2.0 * dm.sign), im.data_ptr(), self._stream())
+                      IF.data_ptr(), n_modes, ld, float(2.0 * dm.sign), im.data_ptr(), self._stream())
         else:
             _lib.call('sb_intmat_contract', jac.data_ptr(), tot_ptr, self.n_valid, self.np_sub, self.n_lenses,
-                      self.field, self._slot.data_ptr(), pix2col.data_ptr(), dm._IF.data_ptr(), n_modes, dm._ld,
+                      self.field, self._slot.data_ptr(), pix2col.data_ptr(), IF.data_ptr(), n_modes, ld,
                       float(2.0 * dm.sign), im.data_ptr(), self._stream())
         return im
+
+    def resampled_ifunc(self, dm, top=0, left=0):
+        """The mirror's influence functions on the SH's resampled grid (one row
+        per mode, a column per field pixel, rows padded to 32 floats) with the
+        identity column map; cached per mirror and crop."""
+        key = (id(dm), dm._IF.data_ptr(), top, left)
+        cache = getattr(self, '_if_cache', None)
+        if cache is not None and cache[0] == key:
+            return cache[1]
+        n_modes = dm._IF.shape[0]
+        rows, cols = self.in_shape
+        p2c = pixel_to_column(dm._ifunc.idx_inf_func, tuple(dm.layer.phaseInNm.shape), rows, top, left)
+        if rows != cols:
+            raise ValueError('ShSlopesAdjoint: square SH input fields only')
+        p2c = torch.as_tensor(p2c, device=self.device).long()
+        keep = p2c >= 0
+        M = self.resample_matrix()
+        n_out = self.field * self.field
+        ld = (n_out + 31) // 32 * 32
+        IF = torch.zeros((n_modes, ld), dtype=torch.float32, device=self.device)
+        for m0 in range(0, n_modes, 64):
+            m1 = min(n_modes, m0 + 64)
+            src = torch.zeros((rows * cols, m1 - m0), dtype=torch.float64, device=self.device)
+            src[keep] = dm._IF[m0:m1, p2c[keep]].t().double()
+            IF[m0:m1, :n_out] = torch.sparse.mm(M, src).t().float()
+        out = (IF, ld, torch.arange(n_out, dtype=torch.int32, device=self.device))
+        self._if_cache = (key, out)
+        return out
 
     # TMA contraction limits: np_sub 4 or 8, at most 992 field columns,
     # influence-function rows of a multiple of 32 floats, a row segment of at
@@ -241,18 +362,18 @@ class ShSlopesAdjoint:
     TMA_MAX_COLUMNS = 992
     TMA_MAX_SEGMENT = 8192
 
-    def _segments(self, pix2col, dm):
+    def _segments(self, pix2col, IF, ld):
         """(device table, largest count) of the row segments for the TMA
         contraction, or None when its limits are not met (then the
         gather kernel runs); cached per mirror column map."""
-        if (self.np_sub not in self.TMA_NP_SUB or self.field > self.TMA_MAX_COLUMNS or dm._ld % 32 or
-                dm._IF.data_ptr() % 16):
+        if (self.np_sub not in self.TMA_NP_SUB or self.field > self.TMA_MAX_COLUMNS or ld % 32 or
+                IF.data_ptr() % 16):
             return None
-        key = (pix2col.data_ptr(), int(dm._ld))
+        key = (pix2col.data_ptr(), int(ld))
         cache = getattr(self, '_seg_cache', None)
         if cache is None or cache[0] != key:
             seg, seg_max = row_segments(pix2col.cpu().numpy(), self._lenslet.cpu().numpy(), self.n_lenses,
-                                        self.np_sub, self.field, dm._ld)
+                                        self.np_sub, self.field, ld)
             val = None if seg_max > self.TMA_MAX_SEGMENT else (torch.as_tensor(seg, device=self.device), seg_max)
             cache = (key, val, pix2col)
             self._seg_cache = cache
@@ -272,8 +393,8 @@ class ShSlopesAdjoint:
             amps = amps.repeat(n_modes)
         pm = torch.stack([amps, -amps], 1).reshape(-1).float().to(self.device)
         shape = tuple(dm.layer.phaseInNm.shape)
-        if shape != (self.field, self.field):
-            raise ValueError('pushpull_intmat: the mirror grid must be the SH field grid')
+        if shape != self.in_shape:
+            raise ValueError('pushpull_intmat: the mirror grid must be the SH input grid')
         phase = torch.zeros(shape, dtype=torch.float32, device=self.device)
         S = torch.empty((2 * n_modes, 2 * self.n_valid), dtype=torch.float32, device=self.device)
         sh = self.sh
@@ -288,7 +409,8 @@ class ShSlopesAdjoint:
                     j = 2 * k + h
                     _lib.call('sb_dm_project', row, 1, int(mask_idx.numel()), dm._ld, pm.data_ptr() + 4 * j, 1,
                               float(dm.sign), mask_idx.data_ptr(), phase.data_ptr(), st)
-                    _lib.call('sb_sh_forward', plan_sh, A.data_ptr(), phase.data_ptr(), A.data_ptr(), A.numel(),
+                    Af, Pf = self.resampled(A, phase, st)
+                    _lib.call('sb_sh_forward', plan_sh, Af.data_ptr(), Pf.data_ptr(), A.data_ptr(), A.numel(),
                               1.0, self._frame.data_ptr(), sh._scratch.data_ptr(), sh._scratch.numel(), st)
                     _lib.call('sb_slopec', ctypes.byref(plan_sc), self._frame.data_ptr(),
                               S[j].data_ptr(), self._flux.data_ptr(), self._sc_scratch.data_ptr(),

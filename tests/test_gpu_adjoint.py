@@ -55,14 +55,14 @@ def _setup(case):
     sh.inputs['in_ef'].set(ef)
     sh.setup()
     geom = osh.sh_geometry(lam, fov, pxs, n, npx, pix, pitch, fov_ovs_coeff=coeff)
-    flat = osh.SHOracle(geom, lam, precision=1).forward(A, np.zeros_like(A), S0, pitch)
+    flat = osh.SHOracle(geom, lam, ef_A_for_tables=A, precision=1).forward(A, np.zeros_like(A), S0, pitch)
     idxs, dmap = osl.detect_subaps(flat, n, 0.5)
     px = Pixels(n * npx, n * npx, target_device_idx=0)
     sl = ShSlopec(SubapData(idxs=idxs, display_map=dmap, nx=n, ny=n, target_device_idx=0), target_device_idx=0)
     sl.inputs['in_pixels'].set(px)
     sl.setup()
     adj = ShSlopesAdjoint(sh, sl)
-    oracle64 = osh.SHOracle(geom, lam, precision=0)
+    oracle64 = osh.SHOracle(geom, lam, ef_A_for_tables=A, precision=0)
 
     def slopes64(phase):
         img = oracle64.forward(A.astype(np.float64), phase, S0, pitch)
@@ -155,6 +155,63 @@ def test_adjoint_intmat_matches_fp64_pushpull(case, cuda):
     ref = octl.pushpull_intmat(slopes_fn, IF.shape[0], [amp] * IF.shape[0])
     assert im.shape == ref.shape
     assert rel_max_err(im, ref) <= ADJ_TOL
+
+
+INTERP_CASES = [c for c in SH_CASES if c[0] == 'c1_interp']    # the SH resamples its field (fov_ovs != 1)
+
+
+@pytest.mark.parametrize('case', INTERP_CASES, ids=[c[0] for c in INTERP_CASES])
+def test_adjoint_intmat_with_resampling_matches_fp64_pushpull(case, cuda):
+    """The adjoint interaction matrix through the SH's edge extrapolation and
+    interpolation (sh.py:353-357,447-460): the influence functions resampled
+    by the same linear map, against the float64 oracle's push-pull."""
+    c = _setup(case)
+    adj, A, pix = c['adj'], c['A'], c['pix']
+    assert adj.interp and adj.field != pix
+    dm, IF, mask = _dm(c, 10, seed=5)
+    flat = torch.zeros((pix, pix), dtype=torch.float32, device='cuda')
+    im = adj.intmat(torch.as_tensor(A), flat, dm).cpu().numpy()
+    amp = 1e-2
+
+    def slopes_fn(k, a):
+        cmd = np.zeros(IF.shape[0])
+        cmd[k] = a
+        return c['slopes64'](octl.dm_phase(IF.astype(np.float64), mask, cmd, sign=dm.sign, precision=0))
+
+    ref = octl.pushpull_intmat(slopes_fn, IF.shape[0], [amp] * IF.shape[0])
+    assert rel_max_err(im, ref) <= ADJ_TOL
+    # the push-pull on the GPU chain, resampling included, agrees too
+    pp, _ = adj.pushpull_intmat(torch.as_tensor(A), dm, 1.0, graph=False)
+    assert rel_max_err(pp.cpu().numpy(), ref) <= 1e-3
+
+
+@pytest.mark.parametrize('case', INTERP_CASES, ids=[c[0] for c in INTERP_CASES])
+def test_jacobian_and_vjp_with_resampling_match_fp64_finite_differences(case, cuda):
+    """The Jacobian (on the resampled samples) through the resampling matrix
+    against central differences of the float64 oracle along random
+    directions of the input phase (<= 1e-4), and the VJP on the input grid
+    consistent with it (<= 1e-5)."""
+    c = _setup(case)
+    adj, A, lam, pix = c['adj'], c['A'], c['lam'], c['pix']
+    rng = np.random.default_rng(11)
+    nm_per_rad = lam / (2 * math.pi)
+    phase0 = (smooth_field(pix, rng, 0.6) * nm_per_rad * A).astype(np.float32)
+    jac = adj.jacobian(torch.as_tensor(A), torch.as_tensor(phase0))
+    M = adj.resample_matrix()
+    lens = adj._lenslet.cpu().numpy()
+    seed = rng.standard_normal(2 * adj.n_valid).astype(np.float32)
+    grad = adj.vjp(torch.as_tensor(A), torch.as_tensor(phase0), torch.as_tensor(seed)).cpu().numpy()
+    eps = 1e-3
+    for probe in range(3):
+        delta = smooth_field(pix, np.random.default_rng(200 + probe), 1.0) * nm_per_rad
+        d_res = torch.sparse.mm(M, torch.as_tensor(delta.reshape(-1, 1), device='cuda')).cpu().numpy()
+        ad = _dir_derivative(jac, lens, c['n'], adj.np_sub, d_res.reshape(adj.field, adj.field))
+        p64 = phase0.astype(np.float64)
+        fd = (c['slopes64'](p64 + eps * delta) - c['slopes64'](p64 - eps * delta)) / (2 * eps)
+        assert rel_max_err(ad, fd) <= ADJ_TOL, probe
+        lhs = float((grad.astype(np.float64) * delta).sum())
+        rhs = float(seed.astype(np.float64) @ ad)
+        assert abs(lhs - rhs) <= VJP_TOL * float(np.abs(seed).astype(np.float64) @ np.abs(ad)), probe
 
 
 def test_intmat_contract_matches_host_contraction(cuda):
@@ -333,7 +390,7 @@ def test_tma_contraction_equals_gather_contraction(cuda):
     from specula_b200.calibration import ShCalibrationSystem
     cal = ShCalibrationSystem()
     adj, dm = cal.adjoint, cal.dm
-    assert adj._segments(cal._pix2col, dm) is not None
+    assert adj._segments(cal._pix2col, dm._IF, dm._ld) is not None
     im_tma = cal.adjoint_intmat()
     A = cal.A
     jac = adj._jacobian(A, cal._flat, None)
@@ -356,7 +413,7 @@ def test_tma_contraction_reports_a_short_segment(cuda):
     from specula_b200.calibration import ShCalibrationSystem
     cal = ShCalibrationSystem()
     adj, dm = cal.adjoint, cal.dm
-    seg, seg_max = adj._segments(cal._pix2col, dm)
+    seg, seg_max = adj._segments(cal._pix2col, dm._IF, dm._ld)
     bad = seg.clone()
     li = int(torch.nonzero(bad[:, 1] > 64)[0])
     bad[li, 1] = 32                                  # 32 columns where the row needs more
