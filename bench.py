@@ -33,10 +33,13 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = 'SH loop steps/s at 80x80 subaps'
-# dram__bytes_read.sum + dram__bytes_write.sum of one dm_project_tma_kernel
-# launch of this workload (ncu --set full capture of
-# `bench.py --steps 20 --warmup 3 --no-cpu-baseline --no-adjoint`)
-DM_TRAFFIC_BYTES = 636_357_120
+# Stored, not measured by this run: dram__bytes_read.sum (632 241 664) +
+# dram__bytes_write.sum (3 805 440) of one dm_project_tma_kernel launch of
+# this workload, captured 2026-12-04 with
+#   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none \
+#       --profile-from-start off -k regex:dm_project_tma -c 1 python bench.py --profile-loop 1
+# (one pass; the step graph's mirror launch)
+DM_TRAFFIC_BYTES = 636_047_104
 UNIT = 'steps/s'
 WORKLOAD = 'elt_80x80_fft16_7layers_500modes'
 
@@ -889,6 +892,7 @@ def run_b200(args):
                 if loop.pipelined else 'sequential',
                 'roofline': {'bound': 'hbm', 'kernel': 'dm_project_tma_kernel', 'achieved': achieved, 'peak': peak,
                              'peak_kind': peak_kind, 'unit': 'GB/s', 'frac': achieved / peak, 'traffic': DM_TRAFFIC_BYTES,
+                             'traffic_source': 'stored ncu capture of this kernel and workload (bench.py comment)',
                              'traffic_over_algorithmic': DM_TRAFFIC_BYTES / dm_bytes,
                              'algorithmic_bytes_per_launch': dm_bytes, 'avg_launch_us': dm_ms * 1e3},
                 'step_roofline': {'algorithmic_bytes': step_bytes,

@@ -4,9 +4,11 @@ against central finite differences of the loop metric along random gain and
 reconstructor directions, and the functional forward loop against the
 object-by-object loop (noise-free detector).
 
-Tolerances: gradient . direction vs finite differences <= 2e-2 relative (the
-loop runs in float32 and the differences are taken over T steps); slopes of
-the two forward loops <= 1e-4 (max|d|/max).
+Tolerances: gradient . direction vs central differences <= 1e-3 relative
+(steps 2e-2 on unit gain directions, 0.25 on the reconstructor direction;
+measured errors on these seeded directions 2e-5 .. 5e-5 and 3e-5: the
+differences' truncation and the float32 loss set the floor); slopes of the
+two forward loops <= 1e-4 (max|d|/max).
 """
 import numpy as np
 import pytest
@@ -17,7 +19,7 @@ from tests.cases import rel_max_err  # noqa: E402
 
 pytestmark = pytest.mark.gpu
 
-FD_TOL = 2e-2
+FD_TOL = 1e-3
 
 
 def _cfg():
@@ -62,7 +64,7 @@ def test_gradient_matches_finite_differences(cuda):
         assert abs(ad - fd) <= FD_TOL * abs(fd), (k, ad, fd)
     D = torch.as_tensor(rng.standard_normal(tuple(R.shape)), dtype=torch.float32, device='cuda')
     D *= 0.05 * float(R.norm()) / float(D.norm())
-    eps = 0.5
+    eps = 0.25
     fd = (lg.loss(g, R + eps * D) - lg.loss(g, R - eps * D)) / (2 * eps)
     ad = float((dR.double() * D.double()).sum())
     assert abs(ad - fd) <= FD_TOL * abs(fd), (ad, fd)
