@@ -321,6 +321,38 @@ int sb_sh_ccd_slopec(const sb_sh_plan *sh, int dft_mode, const float *A, const f
                      const sb_slopec_plan *slopec, const int32_t *lenslet_subap, float *slopes,
                      float *flux, void *scratch, size_t scratch_bytes, void *stream);
 
+/* One SCAO system split over GPUs by bands of lenslet rows (the reference
+ * steps the whole pupil in one process; a band is rows row0 .. row0+n_rows-1
+ * of the lenslet grid).  Per step on every GPU:
+ *   sb_sh_forward_rows   the band's SH frame rows, unnormalised, and the
+ *                        per-CTA partial sums in the WHOLE grid's layout
+ *                        (2 x sb_sh_rows_parts floats at the start of
+ *                        scratch: frame sums, then A_norm sums), written for
+ *                        the band's CTAs only
+ *   [sum the bands' partial arrays: zero outside each band, so the sum is
+ *    the array of one whole-grid launch, bit for bit]
+ *   sb_ccd_slopec_rows   photon normalisation from the summed partials, CCD and
+ *                        CoG of the band: its pixels, and tot / sxn / syn
+ *                        (work: 3 x n_valid floats) / flux / slopes of its
+ *                        valid sub-apertures at their places
+ *   [sum the bands' slope, flux and work vectors]
+ *   sb_slopec_cutoff     the flux cut-off on the summed vectors
+ * then the reconstructor on the whole slope vector and the mirror on the
+ * band's influence-function columns (sb_dm_project on a column range).
+ * The results are those of sb_sh_ccd_slopec on the whole system, bit for
+ * bit (the CCD draws use the whole frame's pixel indices).  Compile-time SH
+ * geometries; the detector read out every step without binning. */
+int sb_sh_rows_parts(const sb_sh_plan *plan, int dft_mode);
+int sb_sh_forward_rows(const sb_sh_plan *plan, int dft_mode, int row0, int n_rows, const float *A,
+                       const float *phase_nm, const float *A_norm, int n_norm, float *intensity, void *scratch,
+                       size_t scratch_bytes, void *stream);
+int sb_ccd_slopec_rows(const sb_sh_plan *sh, const float *parts, int nparts, float photon_scale, int row0,
+                       int n_rows, float *intensity, const sb_ccd_params *ccd, float *integrated, float *pixels,
+                       const sb_slopec_plan *slopec, const int32_t *lenslet_subap, float *slopes, float *flux,
+                       float *work, void *stream);
+int sb_slopec_cutoff(const float *tot, const float *sxn, const float *syn, int n_valid, float *slopes,
+                     void *stream);
+
 /* ------------------------------------------------------------------------
  * Modalrec — replaces specula/processing_objects/modalrec.py:159
  * (modes = R @ slopes), R row-major (n_modes x n_slopes).

@@ -113,6 +113,12 @@ SIGNATURES = {
     'sb_mc_step': (C.c_int, [vp, vp]),
     'sb_mc_destroy': (None, [vp]),
     'sb_mc_stage': (C.c_int, [vp, C.c_int, C.c_int, vp]),
+    'sb_sh_rows_parts': (C.c_int, [C.POINTER(ShPlan), C.c_int]),
+    'sb_sh_forward_rows': (C.c_int, [C.POINTER(ShPlan), C.c_int, C.c_int, C.c_int, fp, fp, fp, C.c_int, fp, vp,
+                                     C.c_size_t, vp]),
+    'sb_ccd_slopec_rows': (C.c_int, [C.POINTER(ShPlan), fp, C.c_int, C.c_float, C.c_int, C.c_int, fp,
+                                     C.POINTER(CcdParams), fp, fp, C.POINTER(SlopecPlan), ip, fp, fp, fp, vp]),
+    'sb_slopec_cutoff': (C.c_int, [fp, fp, fp, C.c_int, fp, vp]),
     'sb_last_error': (C.c_char_p, []),
     'sb_sh_scratch_bytes': (C.c_size_t, [C.POINTER(ShPlan)]),
     'sb_sh_forward': (C.c_int, [C.POINTER(ShPlan), fp, fp, fp, C.c_int, C.c_float, fp, vp, C.c_size_t, vp]),

@@ -654,7 +654,39 @@ struct ChainSlot {
     unsigned int *real_done;    // NULL: the frame state's counter serves the whole launch
     unsigned int real_ctas;     // CTAs of the realisation
     unsigned int group_ctas;    // CTAs sharing the frame state
+    int cutoff;                 // 0: leave the flux cut-off to sb_slopec_cutoff (a band of rows)
 };
+
+// the 1e-3 * mean flux cut-off of sh_slopec.py:393-404 over every valid
+// sub-aperture, by one CTA of at least kChainSumThreads threads: the mean of
+// the denominators as slopec_finish_kernel forms it (partials of 8
+// consecutive sub-apertures summed in float in warp order, then in float64
+// over 256 threads), then the slopes of the sub-apertures below it zeroed
+__device__ __forceinline__ void chain_cutoff(const float *tot, const float *sxn, const float *syn, float *slopes,
+                                             int nv, double *dred) {
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int ngroups = (nv + 7) / 8;
+    double acc = 0.0;
+    for (int g = tid; tid < kChainSumThreads && g < ngroups; g += kChainSumThreads) {
+        float b = 0.f;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int s = 8 * g + k;
+            b += s < nv ? __ldcg(tot + s) : 0.f;
+        }
+        acc += b;
+    }
+    acc = sb::block_sum_all_d(acc, dred);
+    const float mean = (float)(acc / nv);
+    const float cut = 1.0f / (mean * 1e-3f);
+    for (int s = tid; s < nv; s += nthr) {
+        const float fac = 1.0f / __ldcg(tot + s);
+        if (fac > cut) {
+            slopes[s] = __ldcg(sxn + s) * 0.0f;
+            slopes[nv + s] = __ldcg(syn + s) * 0.0f;
+        }
+    }
+}
 
 // the chain for lenslet block (bx, by) of one realisation; any CTA size from
 // 256 to 512 threads gives the same bits
@@ -801,39 +833,30 @@ __device__ __forceinline__ void chain_body(const ChainArgs &a, const ChainOff &o
             vs->blocks_done = 0u;
         }
     }
-    if (!s_last) return;
+    if (!s_last || !slot.cutoff) return;
     __threadfence();
     if (slot.real_done && tid == 0) *slot.real_done = 0u;
-    // mean of the denominators as slopec_finish_kernel forms it: partials of 8
-    // consecutive sub-apertures (slopec_sums_kernel's CTAs), summed in float
-    // in warp order, then in float64 over 256 threads (sh_slopec.py:393-400)
-    const int nv = a.n_valid, ngroups = (nv + 7) / 8;
-    double acc = 0.0;
-    for (int g = tid; tid < kChainSumThreads && g < ngroups; g += kChainSumThreads) {
-        float b = 0.f;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const int s = 8 * g + k;
-            b += s < nv ? __ldcg(tot + s) : 0.f;
-        }
-        acc += b;
-    }
-    acc = sb::block_sum_all_d(acc, dred);
-    const float mean = (float)(acc / nv);
-    const float cut = 1.0f / (mean * 1e-3f);
-    for (int s = tid; s < nv; s += nthr) {
-        const float fac = 1.0f / __ldcg(tot + s);
-        if (fac > cut) {
-            slopes[s] = __ldcg(sxn + s) * 0.0f;
-            slopes[nv + s] = __ldcg(syn + s) * 0.0f;
-        }
-    }
+    chain_cutoff(tot, sxn, syn, slopes, a.n_valid, dred);
+}
+
+// lenslet rows row0 .. row0 + gridDim.y - 1 of a system split by rows; the
+// cut-off waits for every band (sb_slopec_cutoff)
+__global__ void __launch_bounds__(kChainMaxThreads) ccd_slopec_rows_kernel(ChainArgs a, int row0) {
+    const unsigned int ctas = gridDim.x * gridDim.y;
+    chain_body(a, ChainOff{0, 0, 0, 0, 0}, blockIdx.x * kChainLenses, kChainLenses, blockIdx.y + row0,
+               ChainSlot{nullptr, nullptr, nullptr, ctas, ctas, 0});
+}
+
+__global__ void __launch_bounds__(kChainSumThreads) slopec_cutoff_kernel(const float *tot, const float *sxn,
+                                                                        const float *syn, float *slopes, int nv) {
+    __shared__ double dred[33];
+    chain_cutoff(tot, sxn, syn, slopes, nv, dred);
 }
 
 __global__ void __launch_bounds__(kChainMaxThreads) sh_ccd_slopec_kernel(ChainArgs a) {
     const unsigned int ctas = gridDim.x * gridDim.y;
     chain_body(a, ChainOff{0, 0, 0, 0, 0}, blockIdx.x * kChainLenses, kChainLenses, blockIdx.y,
-               ChainSlot{nullptr, nullptr, nullptr, ctas, ctas});
+               ChainSlot{nullptr, nullptr, nullptr, ctas, ctas, 1});
 }
 
 }  // namespace
@@ -1101,7 +1124,7 @@ __global__ void __launch_bounds__(kChainSumThreads, 4) mc_chain_kernel(McChainAr
     const ChainOff off{(long long)b * G.frame_stride, (size_t)b * G.a.nparts, (size_t)b * G.slopes_stride,
                        (size_t)b * G.flux_stride, (size_t)b * 3 * G.a.n_valid};
     const ChainSlot slot{G.photon_seeds + b, G.readout_seeds + b, G.done + b, (unsigned int)per,
-                         (unsigned int)(m.blk0[g + 1] - m.blk0[g])};
+                         (unsigned int)(m.blk0[g + 1] - m.blk0[g]), 1};
     chain_body(G.a, off, (rem % G.gx) * G.lpc, G.lpc, rem / G.gx, slot);
 }
 
@@ -1202,6 +1225,64 @@ int mc_chain_launch(const McBlob &blob, cudaStream_t st) {
 }
 
 }  // namespace sb
+
+extern "C" int sb_ccd_slopec_rows(const sb_sh_plan *sh, const float *parts, int nparts, float photon_scale, int row0,
+                                  int n_rows, float *intensity, const sb_ccd_params *ccd, float *integrated,
+                                  float *pixels, const sb_slopec_plan *slopec, const int32_t *lenslet_subap,
+                                  float *slopes, float *flux, float *work, void *stream) {
+    sb::clear_error();
+    const char *who = "sb_ccd_slopec_rows";
+    if (!sh || !parts || !intensity || !ccd || !ccd->state || !integrated || !pixels || !slopec || !slopec->xw ||
+        !slopec->yw || !slopec->mw || !lenslet_subap || !slopes || !flux || !work)
+        return sb::fail(SB_EINVAL, "%s: null pointer", who);
+    const int n = sh->n_lenses, npx = sh->subap_npx, side = n * npx;
+    if (n < 1 || npx < 1 || npx > kChainMaxNpx || nparts < 1)
+        return sb::fail(SB_ESHAPE, "%s: %d detector pixels per sub-aperture (1..%d supported)", who, npx, kChainMaxNpx);
+    if (row0 < 0 || n_rows < 1 || row0 + n_rows > n)
+        return sb::fail(SB_EINVAL, "%s: lenslet rows %d..%d of %d", who, row0, row0 + n_rows - 1, n);
+    if (ccd->frames_per_read != 1 || ccd->n_pixels != side * side)
+        return sb::fail(SB_EUNSUPPORTED, "%s: the detector must read a %d x %d frame every step", who, side, side);
+    if (ccd->photon_noise && !(ccd->adu_gain > 0.f)) return sb::fail(SB_EINVAL, "%s: ADU gain must be > 0", who);
+    if (slopec->npx2 != npx * npx || slopec->n_subaps < 1 || slopec->n_subaps > n * n)
+        return sb::fail(SB_EINVAL, "%s: slope plan of %d sub-apertures x %d pixels", who, slopec->n_subaps,
+                        slopec->npx2);
+    if (slopec->thr_pedestal || slopec->thr_ratio > 0.f || slopec->window || slopec->mult != 0.f)
+        return sb::fail(SB_EUNSUPPORTED, "%s: the slope options beyond thr go through sb_slopec", who);
+    ChainArgs a;
+    a.p = *ccd;
+    a.part_I = parts;
+    a.part_A = parts + nparts;
+    a.nparts = nparts;
+    a.photon_scale = photon_scale;
+    a.I = intensity;
+    a.integ = integrated;
+    a.pix = pixels;
+    a.n = n;
+    a.npx = npx;
+    a.side = side;
+    a.lenslet_subap = lenslet_subap;
+    a.n_valid = slopec->n_subaps;
+    a.thr = slopec->thr;
+    a.xw = slopec->xw;
+    a.yw = slopec->yw;
+    a.mw = slopec->mw;
+    a.slopes = slopes;
+    a.flux = flux;
+    a.tot = work;
+    a.sxn = work + a.n_valid;
+    a.syn = a.sxn + a.n_valid;
+    const dim3 grid((n + kChainLenses - 1) / kChainLenses, n_rows);
+    ccd_slopec_rows_kernel<<<grid, chain_threads(npx), 0, sb::as_stream(stream)>>>(a, row0);
+    return sb::check_launch("ccd_slopec_rows_kernel");
+}
+
+extern "C" int sb_slopec_cutoff(const float *tot, const float *sxn, const float *syn, int n_valid, float *slopes,
+                                void *stream) {
+    sb::clear_error();
+    if (!tot || !sxn || !syn || !slopes || n_valid < 1) return sb::fail(SB_EINVAL, "sb_slopec_cutoff: bad args");
+    slopec_cutoff_kernel<<<1, kChainSumThreads, 0, sb::as_stream(stream)>>>(tot, sxn, syn, slopes, n_valid);
+    return sb::check_launch("slopec_cutoff_kernel");
+}
 
 extern "C" size_t sb_ccd_cte_scratch_bytes(int side) {
     if (side < 1) return 0;

@@ -46,6 +46,10 @@ struct ShArgs {
     // A_out / P_out when they are given.  NULL A2: the field is A, ph.
     const float *A2, *ph2;
     float *A_out, *P_out;
+    // a band of lenslet rows (sb_sh_forward_rows): grid row y is lenslet row
+    // row0 + y, and the partial sums are indexed as in the whole grid of
+    // grid_rows rows (0: the launch grid itself)
+    int row0, grid_rows;
 };
 
 // amplitude and phase (nm) of field element g, with the mirror term when present
@@ -252,8 +256,8 @@ struct ShBlk {
     int x, y, gx, gy;
 };
 
-__device__ __forceinline__ ShBlk grid_blk() {
-    return {(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x, (int)gridDim.y};
+__device__ __forceinline__ ShBlk grid_blk(const ShArgs &a) {
+    return {(int)blockIdx.x, (int)blockIdx.y + a.row0, (int)gridDim.x, a.grid_rows ? a.grid_rows : (int)gridDim.y};
 }
 
 // the compile-time kernel's shared memory (per-warp buffers for 8 warps)
@@ -376,7 +380,7 @@ template <int P, int CS, int NPX>
 __global__ void __launch_bounds__(256, 4) sh_forward_fixed_kernel(ShArgs a) {
     batch_slice(a);
     __shared__ FixedSmem<P, CS, NPX> S;
-    sh_fixed_body<P, CS, NPX>(a, grid_blk(), S);
+    sh_fixed_body<P, CS, NPX>(a, grid_blk(a), S);
 }
 
 // ---------------------------------------------------------------------------
@@ -696,7 +700,7 @@ __device__ __forceinline__ void sh_tc_body(const ShArgs &a, const ShBlk &blk) {
 template <int P, int CS, int NPX>
 __global__ void __launch_bounds__(kTcThreads) sh_forward_tc_kernel(ShArgs a) {
     batch_slice(a);
-    sh_tc_body<P, CS, NPX>(a, grid_blk());
+    sh_tc_body<P, CS, NPX>(a, grid_blk(a));
 }
 
 // ---------------------------------------------------------------------------
@@ -988,7 +992,8 @@ int sh_forward_impl(const char *who, const sb_sh_plan *pl, const float *A, long 
                     long long sph, const float *A_norm, long long sAn, int n_norm, float photon_scale,
                     float *intensity, long long sout, int n_batch, void *scratch, size_t scratch_bytes, void *stream,
                     int mode = 0, bool normalize = true, int *n_parts = nullptr, const float *mirror_A = nullptr,
-                    const float *mirror_phase = nullptr, float *field_A = nullptr, float *field_phase = nullptr) {
+                    const float *mirror_phase = nullptr, float *field_A = nullptr, float *field_phase = nullptr,
+                    int row0 = 0, int n_rows = -1) {
     if (!pl || !A || !phase_nm || !A_norm || !intensity || !pl->twiddle || !pl->tilt || !pl->fp_mask ||
         !pl->rebin)
         return sb::fail(SB_EINVAL, "%s: null pointer", who);
@@ -1024,8 +1029,21 @@ int sh_forward_impl(const char *who, const sb_sh_plan *pl, const float *A, long 
         // 16 sub-apertures per CTA (never more CTAs than the FP32 grid, so the scratch size holds)
         grid = dim3((pl->n_lenses + kTcSub - 1) / kTcSub, pl->n_lenses, 1);
     }
-    const int nb = grid.x * grid.y;
+    const int nb = grid.x * grid.y;     // the whole grid's CTAs: the partial-sum layout
+    if (n_rows >= 0) {
+        // a band of lenslet rows: compile-time kernels, unnormalised, one field
+        if (row0 < 0 || n_rows < 1 || row0 + n_rows > pl->n_lenses || normalize || n_batch != 1 || mirror_A)
+            return sb::fail(SB_EINVAL, "%s: lenslet rows %d..%d of %d", who, row0, row0 + n_rows - 1, pl->n_lenses);
+        if (!tk.fn && !(spc <= 8 && fixed_kernel(pl->np_sub, pl->cutsize, pl->subap_npx)))
+            return sb::fail(SB_EUNSUPPORTED, "%s: no compile-time kernel for (np=%d, cut=%d, npx=%d)", who,
+                            pl->np_sub, pl->cutsize, pl->subap_npx);
+        grid.y = n_rows;
+    }
     ShArgs a = {};
+    if (n_rows >= 0) {
+        a.row0 = row0;
+        a.grid_rows = pl->n_lenses;
+    }
     a.n = pl->n_lenses;
     a.p = pl->np_sub;
     a.cs = pl->cutsize;
@@ -1088,6 +1106,27 @@ int sh_forward_impl(const char *who, const sb_sh_plan *pl, const float *A, long 
 }
 
 }  // namespace
+
+extern "C" int sb_sh_rows_parts(const sb_sh_plan *pl, int dft_mode) {
+    if (!pl || pl->n_lenses < 1) return 0;
+    int spc;
+    dim3 grid;
+    size_t smem;
+    if (dft_mode == 1) return ((pl->n_lenses + kTcSub - 1) / kTcSub) * pl->n_lenses;
+    const int variant = sb::tune_lookup(SB_TUNE_SH_FP32, sb_tune_key(pl->n_lenses, pl->cutsize, 1));
+    if (sh_grid(pl, &spc, &grid, &smem, 8 >> variant)) return 0;
+    return (int)(grid.x * grid.y);
+}
+
+extern "C" int sb_sh_forward_rows(const sb_sh_plan *pl, int dft_mode, int row0, int n_rows, const float *A,
+                                  const float *phase_nm, const float *A_norm, int n_norm, float *intensity,
+                                  void *scratch, size_t scratch_bytes, void *stream) {
+    sb::clear_error();
+    if (dft_mode != 0 && dft_mode != 1) return sb::fail(SB_EINVAL, "sb_sh_forward_rows: dft_mode must be 0 or 1");
+    return sh_forward_impl("sb_sh_forward_rows", pl, A, 0, phase_nm, 0, A_norm, 0, n_norm, 1.0f, intensity, 0, 1,
+                           scratch, scratch_bytes, stream, dft_mode, false, nullptr, nullptr, nullptr, nullptr,
+                           nullptr, row0, n_rows < 0 ? 0 : n_rows);
+}
 
 namespace sb {
 int sh_forward_unnormalised(const char *who, const sb_sh_plan *pl, const float *A, const float *phase_nm,

@@ -76,8 +76,10 @@ class DM(BaseProcessingObj):
     def trigger_code(self):
         self.project(self.local_inputs['in_command'].value, self.layer.phaseInNm)
 
-    def project(self, c, out_phase):
-        """phase[mask] = (sign * m2c @ c) @ IF into ``out_phase`` (pix x pix)."""
+    def project(self, c, out_phase, columns=None):
+        """phase[mask] = (sign * m2c @ c) @ IF into ``out_phase`` (pix x pix).
+        ``columns`` = (c0, c1): only influence-function columns c0 .. c1 - 1
+        (c0 a multiple of 4), i.e. only those mask pixels."""
         if not isinstance(c, torch.Tensor) or c.device != self.device or c.dtype != torch.float32:
             c = torch.as_tensor(c, dtype=torch.float32, device=self.device)
         if self.nmodes is not None:
@@ -91,8 +93,12 @@ class DM(BaseProcessingObj):
             c = self._cmd
         if out_phase.shape != self.layer.phaseInNm.shape or not out_phase.is_contiguous():
             raise ValueError('DM.project: output must be a contiguous array shaped like the layer')
-        _lib.call('sb_dm_project', self._IF.data_ptr(), self._IF.shape[0], int(self._idx.numel()), self._ld,
-                  c.data_ptr(), int(c.numel()), float(self.sign), self._idx.data_ptr(), out_phase.data_ptr(), st)
+        c0, c1 = (0, int(self._idx.numel())) if columns is None else columns
+        if c0 % 4 or not 0 <= c0 <= c1 <= self._idx.numel():
+            raise ValueError(f'DM.project: columns {columns} outside 0..{self._idx.numel()} or unaligned')
+        _lib.call('sb_dm_project', self._IF.data_ptr() + 4 * c0, self._IF.shape[0], c1 - c0, self._ld,
+                  c.data_ptr(), int(c.numel()), float(self.sign), self._idx.data_ptr() + 4 * c0,
+                  out_phase.data_ptr(), st)
 
     def post_trigger(self):
         self.layer.generation_time = self.current_time
