@@ -495,14 +495,19 @@ __global__ void __launch_bounds__(1024, 1) intmat_contract_tma_kernel(const __gr
     const int chunks = (a.n_modes + kContractModes - 1) / kContractModes;
     const int n_items = chunks * a.n;
     const size_t ld_im = 2 * (size_t)a.n_valid;
+    // items (lenslet row, 16 modes) in row-major order, a contiguous range per
+    // CTA: a CTA meets few lenslet rows, so its consumers load each row's
+    // Jacobian and column offsets once for all its mode chunks
+    const int w_begin = (int)((long long)blockIdx.x * n_items / gridDim.x);
+    const int w_end = (int)((long long)(blockIdx.x + 1) * n_items / gridDim.x);
     if (warp == nwc) {
         if (lane == 0) {
             const uint64_t pol = sb::l2_evict_first_policy();
             int q = 0, st = 0;
             uint32_t ph = 0;
             bool stop = false;
-            for (int w = blockIdx.x; w < n_items && !stop; w += gridDim.x) {
-                const int li = w % a.n, m0 = (w / a.n) * kContractModes;
+            for (int w = w_begin; w < w_end && !stop; ++w) {
+                const int li = w / chunks, m0 = (w % chunks) * kContractModes;
                 const int m1 = min(a.n_modes, m0 + kContractModes);
                 const int cnt = seg_count(a, li);
                 if (cnt <= 0) continue;
@@ -532,33 +537,37 @@ __global__ void __launch_bounds__(1024, 1) intmat_contract_tma_kernel(const __gr
         int st = 0;
         uint32_t ph = 0;
         bool failed = false;
-        for (int w = blockIdx.x; w < n_items && !failed; w += gridDim.x) {
-            const int li = w % a.n, m0 = (w / a.n) * kContractModes;
+        int cur = -1, cnt = 0, s = -1;
+        // a masked pixel reads offset 0 with zero weights: fmaf(0, f, v) == v for the finite
+        // influence functions, as fmaf(j, 0, v) in intmat_contract_kernel
+        float jx[P], jy[P];
+        int off[P];
+        for (int w = w_begin; w < w_end && !failed; ++w) {
+            const int li = w / chunks, m0 = (w % chunks) * kContractModes;
             const int m1 = min(a.n_modes, m0 + kContractModes);
-            const int cnt = seg_count(a, li);
-            const int start = a.row_seg[2 * li];
-            const int s = (lj < a.n) ? a.slot[li * a.n + lj] : -1;
-            bool act = s >= 0;
-            if (a.tot && act) {
-                const float t = a.tot[s];
-                act = t > 0.f && (double)(1.0f / t) <= 1.0 / (mean * 1e-3);
-            }
-            // a masked pixel reads offset 0 with zero weights: fmaf(0, f, v) == v for the finite
-            // influence functions, as fmaf(j, 0, v) in intmat_contract_kernel
-            float jx[P], jy[P];
-            int off[P];
+            if (li != cur) {
+                cur = li;
+                cnt = seg_count(a, li);
+                const int start = a.row_seg[2 * li];
+                s = (lj < a.n) ? a.slot[li * a.n + lj] : -1;
+                bool act = s >= 0;
+                if (a.tot && act) {
+                    const float t = a.tot[s];
+                    act = t > 0.f && (double)(1.0f / t) <= 1.0 / (mean * 1e-3);
+                }
 #pragma unroll
-            for (int rr = 0; rr < P; ++rr) {
-                off[rr] = 0;
-                jx[rr] = jy[rr] = 0.f;
-                if (act) {
-                    const int col = a.pix2col[(size_t)(li * P + rr) * a.field_ld + x];
-                    if (col >= 0 && (col < start || col - start >= cnt)) {
-                        atomicExch(&g_contract_status, 3);      // a column outside its row's segment
-                    } else if (col >= 0) {
-                        off[rr] = col - start;
-                        jx[rr] = a.jac[(size_t)s * (P * P) + rr * P + c];
-                        jy[rr] = a.jac[((size_t)a.n_valid + s) * (P * P) + rr * P + c];
+                for (int rr = 0; rr < P; ++rr) {
+                    off[rr] = 0;
+                    jx[rr] = jy[rr] = 0.f;
+                    if (act) {
+                        const int col = a.pix2col[(size_t)(li * P + rr) * a.field_ld + x];
+                        if (col >= 0 && (col < start || col - start >= cnt)) {
+                            atomicExch(&g_contract_status, 3);      // a column outside its row's segment
+                        } else if (col >= 0) {
+                            off[rr] = col - start;
+                            jx[rr] = a.jac[(size_t)s * (P * P) + rr * P + c];
+                            jy[rr] = a.jac[((size_t)a.n_valid + s) * (P * P) + rr * P + c];
+                        }
                     }
                 }
             }
