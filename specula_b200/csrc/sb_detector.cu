@@ -692,13 +692,15 @@ __device__ __forceinline__ void chain_cutoff(const float *tot, const float *sxn,
 // 256 to 512 threads gives the same bits
 // the chain for lenslets j0 .. j0 + width - 1 of lenslet row by (their
 // npx x width*npx pixels staged in shared memory, at most kChainTile)
+template <int IPT>
 __device__ __forceinline__ void chain_body(const ChainArgs &a, const ChainOff &o, int j0, int width, int by,
                                            const ChainSlot &slot) {
+    static_assert(IPT >= 1 && IPT * kChainSumThreads <= kChainMaxThreads * 2, "pixels per pass");
     __shared__ double dred[33];
     __shared__ float logfact[32];
-    __shared__ int s_idx[kChainMaxThreads];
-    __shared__ float s_mean[kChainMaxThreads];
-    __shared__ int s_small[kChainMaxThreads / 32];
+    __shared__ int s_idx[IPT * kChainMaxThreads];
+    __shared__ float s_mean[IPT * kChainMaxThreads];
+    __shared__ int s_small[IPT * kChainMaxThreads / 32];
     __shared__ float tile[kChainTile];
     __shared__ int s_last, s_group_last;
     const sb_ccd_params &p = a.p;
@@ -730,49 +732,66 @@ __device__ __forceinline__ void chain_body(const ChainArgs &a, const ChainOff &o
     const int i = by;
     const int w = min(width, a.n - j0);
     const int npx = a.npx, wc = w * npx, P = npx * wc, tld = wc;
-    // detector: every pass samples up to blockDim pixels of the tile (one pass
-    // for npx <= 8), ordered by Poisson sampler branch as in ccd_kernel (the
-    // draws do not depend on the order)
-    for (int base = 0; base < P; base += nthr) {
-        const int q = base + tid;
-        const bool valid = q < P;
-        float f = 0.f;
-        if (valid) {
-            const int r = q / wc, c = q - r * wc;
-            const int e = (i * npx + r) * a.side + j0 * npx + c;
-            const float v = I[e] * scale;
-            I[e] = v;
-            f = __fadd_rn(integ[e], __fmul_rn(v, p.rate));           // ccd.py:205
-            if (p.qe != 1.0f) f = __fmul_rn(f, p.qe);                  // ccd.py:282-287
-            if (p.qe_map) f = __fmul_rn(f, p.qe_map[e]);
-            f = __fadd_rn(f, p.bg_plus_dark);                           // ccd.py:220-221
-        }
-        int qi = valid ? q : -1;
-        float fi = f;
-        if (p.photon_noise) {
-            const bool small = valid && f < 10.0f;
-            const unsigned int bal = __ballot_sync(0xffffffffu, small);
-            if (lane == 0) s_small[warp] = __popc(bal);
-            __syncthreads();
-            int before = 0, total = 0;
-            for (int k = 0; k < nwarps; ++k) {
-                const int cnt = s_small[k];
-                before += k < warp ? cnt : 0;
-                total += cnt;
+    // detector: every pass samples up to IPT * blockDim pixels of the tile
+    // (IPT per thread), ordered by Poisson sampler branch as in ccd_kernel
+    // (the draws do not depend on the order); item j of thread t is pass
+    // entry j * blockDim + t, in virtual warp j * nwarps + warp
+    for (int base = 0; base < P; base += IPT * nthr) {
+        int qi[IPT];
+        float fi[IPT];
+#pragma unroll
+        for (int j = 0; j < IPT; ++j) {
+            const int q = base + j * nthr + tid;
+            const bool valid = q < P;
+            float f = 0.f;
+            if (valid) {
+                const int r = q / wc, c = q - r * wc;
+                const int e = (i * npx + r) * a.side + j0 * npx + c;
+                const float v = I[e] * scale;
+                I[e] = v;
+                f = __fadd_rn(integ[e], __fmul_rn(v, p.rate));           // ccd.py:205
+                if (p.qe != 1.0f) f = __fmul_rn(f, p.qe);                  // ccd.py:282-287
+                if (p.qe_map) f = __fmul_rn(f, p.qe_map[e]);
+                f = __fadd_rn(f, p.bg_plus_dark);                           // ccd.py:220-221
             }
-            const int rank = __popc(bal & ((1u << lane) - 1u));
-            const int pos = small ? before + rank : total + (warp * 32 - before) + (lane - rank);
-            s_idx[pos] = qi;
-            s_mean[pos] = f;
+            qi[j] = valid ? q : -1;
+            fi[j] = f;
+        }
+        if (p.photon_noise) {
+            unsigned int bal[IPT];
+#pragma unroll
+            for (int j = 0; j < IPT; ++j) {
+                bal[j] = __ballot_sync(0xffffffffu, qi[j] >= 0 && fi[j] < 10.0f);
+                if (lane == 0) s_small[j * nwarps + warp] = __popc(bal[j]);
+            }
             __syncthreads();
-            qi = s_idx[tid];
-            fi = s_mean[tid];
+            int total = 0;
+            for (int k = 0; k < IPT * nwarps; ++k) total += s_small[k];
+#pragma unroll
+            for (int j = 0; j < IPT; ++j) {
+                const int vw = j * nwarps + warp;
+                int before = 0;
+                for (int k = 0; k < vw; ++k) before += s_small[k];
+                const bool small = (bal[j] >> lane) & 1u;
+                const int rank = __popc(bal[j] & ((1u << lane) - 1u));
+                const int pos = small ? before + rank : total + (vw * 32 - before) + (lane - rank);
+                s_idx[pos] = qi[j];
+                s_mean[pos] = fi[j];
+            }
+            __syncthreads();
+#pragma unroll
+            for (int j = 0; j < IPT; ++j) {
+                qi[j] = s_idx[j * nthr + tid];
+                fi[j] = s_mean[j * nthr + tid];
+            }
             __syncthreads();
         }
-        if (qi >= 0) {
-            const int r = qi / wc, c = qi - r * wc;
+#pragma unroll
+        for (int j = 0; j < IPT; ++j) {
+            if (qi[j] < 0) continue;
+            const int r = qi[j] / wc, c = qi[j] - r * wc;
             const int e = (i * npx + r) * a.side + j0 * npx + c;
-            const float v = ccd_sample(p, fi, e, frame, slot.photon_seed, slot.readout_seed, p.n_pixels, logfact,
+            const float v = ccd_sample(p, fi[j], e, frame, slot.photon_seed, slot.readout_seed, p.n_pixels, logfact,
                                        inv_gain, gain_pow2);
             pix[e] = v;
             integ[e] = 0.0f;                                          // ccd.py:216
@@ -843,7 +862,7 @@ __device__ __forceinline__ void chain_body(const ChainArgs &a, const ChainOff &o
 // cut-off waits for every band (sb_slopec_cutoff)
 __global__ void __launch_bounds__(kChainMaxThreads) ccd_slopec_rows_kernel(ChainArgs a, int row0) {
     const unsigned int ctas = gridDim.x * gridDim.y;
-    chain_body(a, ChainOff{0, 0, 0, 0, 0}, blockIdx.x * kChainLenses, kChainLenses, blockIdx.y + row0,
+    chain_body<1>(a, ChainOff{0, 0, 0, 0, 0}, blockIdx.x * kChainLenses, kChainLenses, blockIdx.y + row0,
                ChainSlot{nullptr, nullptr, nullptr, ctas, ctas, 0});
 }
 
@@ -855,7 +874,7 @@ __global__ void __launch_bounds__(kChainSumThreads) slopec_cutoff_kernel(const f
 
 __global__ void __launch_bounds__(kChainMaxThreads) sh_ccd_slopec_kernel(ChainArgs a) {
     const unsigned int ctas = gridDim.x * gridDim.y;
-    chain_body(a, ChainOff{0, 0, 0, 0, 0}, blockIdx.x * kChainLenses, kChainLenses, blockIdx.y,
+    chain_body<1>(a, ChainOff{0, 0, 0, 0, 0}, blockIdx.x * kChainLenses, kChainLenses, blockIdx.y,
                ChainSlot{nullptr, nullptr, nullptr, ctas, ctas, 1});
 }
 
@@ -1085,6 +1104,8 @@ extern "C" int sb_sh_ccd_slopec(const sb_sh_plan *sh, int dft_mode, const float 
 // ---------------------------------------------------------------------------
 namespace {
 
+constexpr int kMcChainIpt = 1;          // pixels per thread and pass in the Monte-Carlo detector stage (2 measured slower)
+
 struct McChainGroup {
     ChainArgs a;                     // realisation 0
     long long frame_stride;
@@ -1125,7 +1146,7 @@ __global__ void __launch_bounds__(kChainSumThreads, 4) mc_chain_kernel(McChainAr
                        (size_t)b * G.flux_stride, (size_t)b * 3 * G.a.n_valid};
     const ChainSlot slot{G.photon_seeds + b, G.readout_seeds + b, G.done + b, (unsigned int)per,
                          (unsigned int)(m.blk0[g + 1] - m.blk0[g]), 1};
-    chain_body(G.a, off, (rem % G.gx) * G.lpc, G.lpc, rem / G.gx, slot);
+    chain_body<kMcChainIpt>(G.a, off, (rem % G.gx) * G.lpc, G.lpc, rem / G.gx, slot);
 }
 
 }  // namespace
