@@ -286,6 +286,18 @@ def convert_ref_fits():
     return out
 
 
+def convert_interp_fits():
+    """The reference's Interp2D fixtures (test/data/input_phase.fits ->
+    ref_phase.fits, checked by test_interp2d.py:19-43 at rtol 4e-2), with the
+    sampling of that test: make_xy(480, 479.84003 / 2) shifted by the half
+    layer (240.5, 240.5) and the position (0.0930127, 0)."""
+    d = os.path.join(REF, 'test', 'data')
+    return {'interp/input_phase': np.asarray(fits_min.read_hdus(os.path.join(d, 'input_phase.fits'))[0][1],
+                                             dtype=np.float32),
+            'interp/ref_phase': np.asarray(fits_min.read_hdus(os.path.join(d, 'ref_phase.fits'))[0][1],
+                                           dtype=np.float32)}
+
+
 def make_zernike_cases():
     """IFunc(type_str='zernike') tables (compute_zern_ifunc.py:6-29)."""
     from specula.lib.compute_zern_ifunc import compute_zern_ifunc
@@ -738,6 +750,7 @@ def main():
     specula.init(-1, precision=1)
     ref = convert_ref_fits()
     np.savez_compressed(os.path.join(HERE, 'ref_fits.npz'), **ref)
+    np.savez_compressed(os.path.join(HERE, 'interp_fits.npz'), **convert_interp_fits())
     sh32, geoms = make_sh_cases(precision=1)
     np.savez_compressed(os.path.join(HERE, 'sh_fp32.npz'), **sh32)
     with open(os.path.join(HERE, 'sh_geometry.json'), 'w') as f:
@@ -785,6 +798,8 @@ if __name__ == '__main__':
         with np.load(os.path.join(HERE, 'ref_fits.npz')) as z:
             ref = {k: z[k] for k in z.files}
         np.savez_compressed(os.path.join(HERE, 'slopec_opt_fp32.npz'), **make_slopec_option_cases(ref))
+    elif '--interp-fits' in sys.argv:  # only the Interp2D FITS fixtures
+        np.savez_compressed(os.path.join(HERE, 'interp_fits.npz'), **convert_interp_fits())
     elif '--iir' in sys.argv:          # only the general IIR filter fixtures
         import specula
         specula.init(-1, precision=1)

@@ -229,3 +229,25 @@ def test_slopec_option_cases_the_reference_raises_on(slopec_opt):
     g = np.exp(-4 * np.log(2) * (v[None, :] ** 2 + v[:, None] ** 2))
     assert np.allclose(m, g / g.max(), rtol=1e-6)
     assert m.max() == 1.0 and np.allclose(x, np.meshgrid(v, v)[0] * m)
+
+
+def _interp_fits_case():
+    import os
+    from specula_b200.lib.make_mask import make_xy
+    from specula_b200.lib.interp2d import interp_coords_xy
+    with np.load(os.path.join(os.path.dirname(__file__), 'golden', 'interp_fits.npz')) as z:
+        phase, ref = z['interp/input_phase'], z['interp/ref_phase']
+    # the sampling of the reference's test_interp2d.py:25-33
+    xx, yy = make_xy(480, 479.84003 / 2.0)
+    yy, xx = interp_coords_xy(phase.shape, yy + 240.5 + 0.0, xx + 240.5 + 0.0930127)
+    return phase, ref, yy, xx
+
+
+def test_interp2d_matches_reference_fits():
+    """The reference's Interp2D fixture (test_interp2d.py:19-43, 482^2 ->
+    480^2 with a sub-pixel shift) at the reference test's tolerance (rtol
+    4e-2, its one known outlier pixel excepted)."""
+    phase, ref, yy, xx = _interp_fits_case()
+    got = osh.interp2d(phase, yy, xx, ref.shape)
+    got[394, 365] = ref[394, 365]
+    np.testing.assert_allclose(got, ref, rtol=4e-2)
