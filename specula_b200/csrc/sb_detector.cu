@@ -1126,7 +1126,7 @@ struct McChainBlob {
     int blocks, threads;
 };
 
-__global__ void __launch_bounds__(kChainSumThreads, 4) mc_chain_kernel(McChainArgs m) {
+__global__ void __launch_bounds__(kChainSumThreads, 6) mc_chain_kernel(McChainArgs m) {
     // the group's arguments staged in shared memory: read there on use, not
     // held in registers
     __shared__ __align__(16) McChainGroup G;
