@@ -412,26 +412,24 @@ __device__ int g_sh_tc_status = 0;      // nonzero: a bounded wait on the tensor
 template <int CS>
 struct TcShape {
     static constexpr int NB = 2 * CS <= 16 ? 16 : 32;   // MMA N
-    static constexpr int GS = CS * 8 + 8;                // float2 per sub-aperture in the G buffer (bank offset)
 };
 
-// Dynamic shared memory per CTA: operands, G / |F|^2 buffer and tables
-// (35-46 KB), so at most 6 CTAs, 384 tensor-memory columns, share an SM and
-// the allocation never waits.
+// Dynamic shared memory per CTA: the operands (whose space holds |F|^2 once
+// both products are done) and the tables, 26-29 KB: at most 8 CTAs, 512
+// tensor-memory columns, share an SM, so the allocation never waits.
 template <int P, int CS, int NPX>
 __host__ __device__ constexpr size_t tc_smem_bytes() {
-    return 6 * (size_t)kTcOperandBytes + 2 * (size_t)TcShape<CS>::NB * 32 + (size_t)kTcSub * TcShape<CS>::GS * 8 +
-           (size_t)P * P * 8 + (size_t)CS * CS * 4 + (size_t)NPX * CS * 4 + 8 + 16;
+    return 6 * (size_t)kTcOperandBytes + 2 * (size_t)TcShape<CS>::NB * 32 + (size_t)P * P * 8 +
+           (size_t)CS * CS * 4 + (size_t)NPX * CS * 4 + 8 + 16;
 }
-static_assert(tc_smem_bytes<8, 8, 8>() * 8 > 228 * 1024, "more than 8 CTAs per SM would exceed tensor memory");
+static_assert(tc_smem_bytes<8, 8, 8>() * 9 > 228 * 1024, "more than 8 CTAs per SM would exceed tensor memory");
 
 template <int P, int CS, int NPX>
 __device__ __forceinline__ void sh_tc_body(const ShArgs &a, const ShBlk &blk) {
     static_assert(P == 8, "one 16-byte K segment per field row");
     static_assert(CS <= 16, "one 16-row stage-2 block per sub-aperture");
-    static_assert(kTcSub * CS * CS <= kTcSub * TcShape<CS>::GS * 2, "intensity buffer aliases the G buffer");
+    static_assert(kTcSub * CS * CS * 4 <= 6 * kTcOperandBytes, "the intensity buffer reuses the operand space");
     constexpr int NB = TcShape<CS>::NB;
-    constexpr int GS = TcShape<CS>::GS;
     constexpr uint32_t IDESC = sb::umma_idesc_bf16_f32(128, NB);
     constexpr uint32_t LBO_A = 128 * 16, LBO_B = NB * 16;
     extern __shared__ __align__(128) unsigned char tc_smem[];
@@ -439,9 +437,8 @@ __device__ __forceinline__ void sh_tc_body(const ShArgs &a, const ShBlk &blk) {
     unsigned char *A2h = tc_smem + 2 * kTcOperandBytes;   // two tiles
     unsigned char *A2l = tc_smem + 4 * kTcOperandBytes;   // two tiles
     unsigned char *Bh = tc_smem + 6 * kTcOperandBytes, *Bl = Bh + NB * 32;
-    float2 *Gb = reinterpret_cast<float2 *>(Bl + NB * 32);
-    float *Ib = reinterpret_cast<float *>(Gb);        // |F|^2 after G is consumed
-    float2 *tilt = Gb + kTcSub * GS;
+    float *Ib = reinterpret_cast<float *>(tc_smem);   // |F|^2, once both products are done
+    float2 *tilt = reinterpret_cast<float2 *>(Bl + NB * 32);
     float *mask = reinterpret_cast<float *>(tilt + P * P);
     float *R = mask + CS * CS;
     uint64_t *bar = reinterpret_cast<uint64_t *>((reinterpret_cast<uintptr_t>(R + NPX * CS) + 7) & ~(uintptr_t)7);
@@ -577,37 +574,32 @@ __device__ __forceinline__ void sh_tc_body(const ShArgs &a, const ShBlk &blk) {
         if constexpr (NB == 32) sb::tmem_ld16(tmem + lane_base + 16, v[1]);
         sb::tmem_wait_ld(v[0]);
         if constexpr (NB == 32) sb::tmem_wait_ld(v[1]);
+        // stage-2 operand rows (s, b) hold column b of G_s: K element r is
+        // this thread's G[r][b], split straight from tensor memory (the
+        // split of each value as split_bf16x8 forms it); the lanes of rows
+        // r and r + 1 pair their 16-bit halves so the even lane stores a word
 #pragma unroll
         for (int b = 0; b < CS; ++b) {
             const int nr = b, ni = CS + b;
-            Gb[s * GS + b * 8 + r] = make_float2(__uint_as_float(v[nr >> 4][nr & 15]),
-                                                 __uint_as_float(v[ni >> 4][ni & 15]));
-        }
-        sb::tc_fence_before_sync();
-        __syncthreads();
-        // stage-2 operand rows (s2, b): column b of G_s2, split
-        for (int e = t; e < kTcSub * CS; e += kTcThreads) {
-            const int s2 = e / CS, b = e - s2 * CS;
-            const float4 *g = reinterpret_cast<const float4 *>(Gb + s2 * GS + b * 8);
-            float gr[8], gi[8];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const float4 x = g[q];
-                gr[2 * q] = x.x;
-                gi[2 * q] = x.y;
-                gr[2 * q + 1] = x.z;
-                gi[2 * q + 1] = x.w;
+            const float gre = __uint_as_float(v[nr >> 4][nr & 15]);
+            const float gim = __uint_as_float(v[ni >> 4][ni & 15]);
+            const __nv_bfloat16 hr = __float2bfloat16_rn(gre), hi = __float2bfloat16_rn(gim);
+            const __nv_bfloat16 lr = __float2bfloat16_rn(gre - __bfloat162float(hr));
+            const __nv_bfloat16 li = __float2bfloat16_rn(gim - __bfloat162float(hi));
+            const uint32_t own_r = (uint32_t)__bfloat16_as_ushort(hr) | ((uint32_t)__bfloat16_as_ushort(lr) << 16);
+            const uint32_t own_i = (uint32_t)__bfloat16_as_ushort(hi) | ((uint32_t)__bfloat16_as_ushort(li) << 16);
+            const uint32_t nb_r = __shfl_xor_sync(0xffffffffu, own_r, 1);
+            const uint32_t nb_i = __shfl_xor_sync(0xffffffffu, own_i, 1);
+            if ((r & 1) == 0) {
+                const int off = (s >> 3) * kTcOperandBytes + ((s & 7) * 16 + b) * 16 + r * 2;
+                *reinterpret_cast<uint32_t *>(A2h + off) = (own_r & 0xffffu) | (nb_r << 16);
+                *reinterpret_cast<uint32_t *>(A2l + off) = (own_r >> 16) | (nb_r & 0xffff0000u);
+                *reinterpret_cast<uint32_t *>(A2h + off + LBO_A) = (own_i & 0xffffu) | (nb_i << 16);
+                *reinterpret_cast<uint32_t *>(A2l + off + LBO_A) = (own_i >> 16) | (nb_i & 0xffff0000u);
             }
-            const int off = (s2 >> 3) * kTcOperandBytes + ((s2 & 7) * 16 + b) * 16;
-            uint4 h, l;
-            sb::split_bf16x8(gr, h, l);
-            *reinterpret_cast<uint4 *>(A2h + off) = h;
-            *reinterpret_cast<uint4 *>(A2l + off) = l;
-            sb::split_bf16x8(gi, h, l);
-            *reinterpret_cast<uint4 *>(A2h + off + LBO_A) = h;
-            *reinterpret_cast<uint4 *>(A2l + off + LBO_A) = l;
         }
         sb::fence_proxy_async_smem();
+        sb::tc_fence_before_sync();
         __syncthreads();
         sb::tc_fence_after_sync();
         // stage 2: F^T = G^T W^T per sub-aperture, tile k into columns 32k..32k+31
