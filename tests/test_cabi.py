@@ -144,3 +144,25 @@ def test_monte_carlo_step_validation_without_device(lib):
     h = C.c_void_p()
     assert lib.sb_mc_create(groups, 1, None, 0, C.byref(h), None) == -1
     lib.sb_mc_destroy(None)
+
+
+def test_row_band_and_stage_validation_without_device(lib):
+    """The row-band entry points and sb_mc_stage reject bad bands, null
+    pointers and unknown stages before any device work."""
+    plan = _lib.ShPlan()
+    plan.n_lenses, plan.np_sub, plan.cutsize, plan.subap_npx, plan.field_ld = 20, 8, 14, 8, 160
+    buf = C.c_void_p(16)                       # never dereferenced: validation fails first
+    rc = lib.sb_sh_forward_rows(C.byref(plan), 2, 0, 4, buf, buf, buf, 16, buf, buf, 1 << 20, None)
+    assert rc == -1 and b'dft_mode' in lib.sb_last_error()
+    ccd = _lib.CcdParams()
+    sl = _lib.SlopecPlan()
+    rc = lib.sb_ccd_slopec_rows(C.byref(plan), None, 10, C.c_float(1.0), 0, 4, buf, C.byref(ccd), buf, buf,
+                                C.byref(sl), buf, buf, buf, buf, None)
+    assert rc == -1 and b'null' in lib.sb_last_error()
+    ccd.state = buf
+    sl.xw = sl.yw = sl.mw = buf
+    rc = lib.sb_ccd_slopec_rows(C.byref(plan), buf, 10, C.c_float(1.0), 18, 4, buf, C.byref(ccd), buf, buf,
+                                C.byref(sl), buf, buf, buf, buf, None)
+    assert rc == -1 and b'lenslet rows 18..21 of 20' in lib.sb_last_error()
+    assert lib.sb_slopec_cutoff(buf, buf, buf, 0, buf, None) == -1
+    assert lib.sb_mc_stage(None, 0, -1, None) == -1
