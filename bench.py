@@ -801,33 +801,48 @@ def run_b200(args):
     # two-step graph (ScaoLoop.capture(io=True) / replay), each step's seeing
     # and wind values copied host->device from pinned memory before the
     # replay and each step's slopes + DM commands read back device->host
-    # after it, then a synchronise
+    # after it.  Two forms: the host waits for each replay's results before
+    # launching the next (synchronous), or reads them one replay behind into
+    # two alternating pinned buffers, so the device never waits for the host
+    # (overlapped; the reported e2e)
     nl = len(cfg.heights)
     loop.capture(io=True)
     h_in = torch.empty(tuple(loop.io_inputs.shape), dtype=torch.float64).pin_memory()
     h_in.copy_(loop.io_inputs.cpu())
-    h_out = torch.empty(tuple(loop.io_outputs.shape), dtype=torch.float32).pin_memory()
+    h_out = [torch.empty(tuple(loop.io_outputs.shape), dtype=torch.float32).pin_memory() for _ in range(2)]
     e2e_reps = max(10, min(args.steps, 2000)) // loop.steps_per_replay
+    cur = torch.cuda.current_stream(dev)
+    done = [torch.cuda.Event(), torch.cuda.Event()]
 
-    def e2e_round():
+    def e2e_round(k, overlapped):
         loop.io_inputs.copy_(h_in, non_blocking=True)
         loop.replay()
-        h_out.copy_(loop.io_outputs, non_blocking=True)
-        torch.cuda.synchronize(dev)
+        h_out[k % 2].copy_(loop.io_outputs, non_blocking=True)
+        done[k % 2].record(cur)
+        if not overlapped:
+            done[k % 2].synchronize()
+        elif k >= 1:
+            done[(k - 1) % 2].synchronize()     # the previous replay's results are on the host
 
-    for _ in range(3):
-        e2e_round()
-    if world > 1:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(e2e_reps):
-        e2e_round()
-    e2e_dt = time.perf_counter() - t0
-    e2e = torch.tensor([e2e_dt], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(e2e, op=dist.ReduceOp.MAX)
+    def e2e_run(overlapped):
+        for k in range(3):
+            e2e_round(k, overlapped)
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for k in range(e2e_reps):
+            e2e_round(k, overlapped)
+        done[(e2e_reps - 1) % 2].synchronize()
+        dt = time.perf_counter() - t0
+        t = torch.tensor([dt], device=dev, dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return world * e2e_reps * loop.steps_per_replay / float(t.item())
+
+    e2e_sync_value = e2e_run(False)
+    e2e_value = e2e_run(True)
     e2e_steps = e2e_reps * loop.steps_per_replay
-    e2e_value = world * e2e_steps / float(e2e.item())
 
     # the same through the object API (LoopControl.iter: every object's
     # check_ready / trigger / post_trigger in Python, one step at a time)
@@ -839,8 +854,8 @@ def run_b200(args):
     for _ in range(obj_steps):
         loop._inputs.copy_(h_in[0], non_blocking=True)
         loop.step_eager()
-        h_out[0, :nsl].copy_(loop.slopec.slopes.slopes, non_blocking=True)
-        h_out[0, nsl:].copy_(loop.integ.out_comm.value, non_blocking=True)
+        h_out[0][0, :nsl].copy_(loop.slopec.slopes.slopes, non_blocking=True)
+        h_out[0][0, nsl:].copy_(loop.integ.out_comm.value, non_blocking=True)
         torch.cuda.synchronize(dev)
     obj_dt = time.perf_counter() - t0
     t_obj = torch.tensor([obj_dt], device=dev, dtype=torch.float64)
@@ -882,8 +897,14 @@ def run_b200(args):
                 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
                 'config': config_dict(cfg, world),
                 'e2e': {'value': e2e_value, 'unit': UNIT, 'h2d_bytes_per_step': int(loop.n_inputs * 8),
-                        'd2h_bytes_per_step': int((nsl + nm) * 4), 'api': 'ScaoLoop.replay (captured 2-step graph)',
+                        'd2h_bytes_per_step': int((nsl + nm) * 4),
+                        'api': 'ScaoLoop.replay (captured 2-step graph); every step inputs host->device and results '
+                               'device->host, the host reading each replay\'s results one replay behind (two '
+                               'alternating pinned buffers)',
                         'steps': e2e_steps},
+                'e2e_synchronous': {'value': e2e_sync_value, 'unit': UNIT,
+                                    'api': 'the same, the host waiting for each replay\'s results before the next',
+                                    'steps': e2e_steps},
                 'e2e_object_api': {'value': obj_value, 'unit': UNIT, 'api': 'LoopControl.iter (object by object)',
                                    'steps': obj_steps},
                 'gpu_launches': loop.kernels_per_step * steps,
