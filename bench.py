@@ -806,23 +806,43 @@ def run_b200(args):
     # two alternating pinned buffers, so the device never waits for the host
     # (overlapped; the reported e2e)
     nl = len(cfg.heights)
-    loop.capture(io=True)
+    loop.capture(io=True, io_slots=2)
     h_in = torch.empty(tuple(loop.io_inputs.shape), dtype=torch.float64).pin_memory()
     h_in.copy_(loop.io_inputs.cpu())
     h_out = [torch.empty(tuple(loop.io_outputs.shape), dtype=torch.float32).pin_memory() for _ in range(2)]
     e2e_reps = max(10, min(args.steps, 2000)) // loop.steps_per_replay
     cur = torch.cuda.current_stream(dev)
+    s_in, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
     done = [torch.cuda.Event(), torch.cuda.Event()]
+    ran = [torch.cuda.Event(), torch.cuda.Event()]
+    fed = [torch.cuda.Event(), torch.cuda.Event()]
 
     def e2e_round(k, overlapped):
-        loop.io_inputs.copy_(h_in, non_blocking=True)
-        loop.replay()
-        h_out[k % 2].copy_(loop.io_outputs, non_blocking=True)
-        done[k % 2].record(cur)
         if not overlapped:
-            done[k % 2].synchronize()
-        elif k >= 1:
-            done[(k - 1) % 2].synchronize()     # the previous replay's results are on the host
+            loop.io_inputs.copy_(h_in, non_blocking=True)
+            loop.replay()
+            h_out[0].copy_(loop.io_outputs, non_blocking=True)
+            done[0].record(cur)
+            done[0].synchronize()
+            return
+        # slot k % 2: its inputs go in on one copy stream once the replay that
+        # last read them (k - 2) is done, its results come out on another
+        # while the next replay runs; the host takes replay k-1's results
+        j = k % 2
+        if k >= 2:
+            s_in.wait_event(ran[j])
+        with torch.cuda.stream(s_in):
+            loop.io_inputs_slots[j].copy_(h_in, non_blocking=True)
+            fed[j].record(s_in)
+        cur.wait_event(fed[j])
+        loop.replay(j)
+        ran[j].record(cur)
+        s_out.wait_event(ran[j])
+        with torch.cuda.stream(s_out):
+            h_out[j].copy_(loop.io_outputs_slots[j], non_blocking=True)
+            done[j].record(s_out)
+        if k >= 1:
+            done[1 - j].synchronize()           # the previous replay's results are on the host
 
     def e2e_run(overlapped):
         for k in range(3):
@@ -833,7 +853,7 @@ def run_b200(args):
         t0 = time.perf_counter()
         for k in range(e2e_reps):
             e2e_round(k, overlapped)
-        done[(e2e_reps - 1) % 2].synchronize()
+        done[(e2e_reps - 1) % 2 if overlapped else 0].synchronize()
         dt = time.perf_counter() - t0
         t = torch.tensor([dt], device=dev, dtype=torch.float64)
         if world > 1:
@@ -898,9 +918,9 @@ def run_b200(args):
                 'config': config_dict(cfg, world),
                 'e2e': {'value': e2e_value, 'unit': UNIT, 'h2d_bytes_per_step': int(loop.n_inputs * 8),
                         'd2h_bytes_per_step': int((nsl + nm) * 4),
-                        'api': 'ScaoLoop.replay (captured 2-step graph); every step inputs host->device and results '
-                               'device->host, the host reading each replay\'s results one replay behind (two '
-                               'alternating pinned buffers)',
+                        'api': 'ScaoLoop.replay (captured 2-step graphs of two input / output slots); every step '
+                               'inputs host->device and results device->host on copy streams beside the replays, '
+                               'the host reading each replay\'s results one replay behind',
                         'steps': e2e_steps},
                 'e2e_synchronous': {'value': e2e_sync_value, 'unit': UNIT,
                                     'api': 'the same, the host waiting for each replay\'s results before the next',

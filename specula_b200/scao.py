@@ -192,7 +192,7 @@ class ScaoLoop:
         self.wind_speed.value = vec[1:1 + nl]
         self.wind_direction.value = vec[1 + nl:]
 
-    def capture(self, pipelined=True, io=False, fuse_atmo=None, fuse_chain=None, early_atmo=False):
+    def capture(self, pipelined=True, io=False, fuse_atmo=None, fuse_chain=None, early_atmo=False, io_slots=1):
         """Capture whole steps in a CUDA graph.  Call after at least one eager
         step, so the time step used by AtmoEvolution is the loop's (the first
         step has delta_time = 0).
@@ -221,6 +221,12 @@ class ScaoLoop:
         (sb_sh_ccd_slopec: the SH forward, then normalisation, detector and
         CoG on each lenslet's pixels in shared memory) instead of five; the
         same bits.  None: fused whenever the objects allow it.
+
+        ``io_slots`` (with ``io``): that many graphs of the same two steps,
+        each with its own input / output slots (``io_inputs_slots[k]``,
+        ``io_outputs_slots[k]``, run by ``replay(k)``), so a caller can copy
+        the next replay's inputs and the last replay's results while a
+        replay runs; ``io_inputs`` / ``io_outputs`` are slot 0's.
 
         ``early_atmo`` (pipelined form with both fusions and the FP32 SH):
         the mirror term of the propagation moves into the SH's field read
@@ -282,16 +288,25 @@ class ScaoLoop:
             self._side = side
             self._cap = cap
             self._bufs = (dm_buf, nxt)
+            n_slots = max(1, int(io_slots)) if io else 1
             if io:
                 nsl = self.slopec.slopes.slopes.numel()
                 nm = self.integ.out_comm.value.numel()
-                self.io_inputs = self._inputs.repeat(2, 1).contiguous()
-                self.io_outputs = torch.zeros((2, nsl + nm), dtype=torch.float32, device=self.device)
-            if self.early_atmo:
-                self._capture_early(g, side, cap, dm_buf, nxt, io)
-            else:
-                self._capture_pipelined(g, side, cap, dm_buf, nxt, io, fuse_atmo)
+                self.io_inputs_slots = [self._inputs.repeat(2, 1).contiguous() for _ in range(n_slots)]
+                self.io_outputs_slots = [torch.zeros((2, nsl + nm), dtype=torch.float32, device=self.device)
+                                         for _ in range(n_slots)]
+            self.graphs = []
+            for k in range(n_slots):
+                gk = g if k == 0 else torch.cuda.CUDAGraph()
+                if io:
+                    self.io_inputs, self.io_outputs = self.io_inputs_slots[k], self.io_outputs_slots[k]
+                if self.early_atmo:
+                    self._capture_early(gk, side, cap, dm_buf, nxt, io)
+                else:
+                    self._capture_pipelined(gk, side, cap, dm_buf, nxt, io, fuse_atmo)
+                self.graphs.append(gk)
             if io:
+                self.io_inputs, self.io_outputs = self.io_inputs_slots[0], self.io_outputs_slots[0]
                 self._point_inputs(self._inputs)
             self.steps_per_replay = 2
         torch.cuda.synchronize(self.device)
@@ -526,9 +541,10 @@ class ScaoLoop:
         finally:
             integ._plan.out_next = None
 
-    def replay(self):
-        """Run the captured graph: ``steps_per_replay`` loop steps."""
-        self.graph.replay()
+    def replay(self, slot=0):
+        """Run the captured graph (of input / output slot ``slot``):
+        ``steps_per_replay`` loop steps."""
+        (self.graph if slot == 0 else self.graphs[slot]).replay()
 
     # kernels launched by one captured step (for the launch count): atmo
     # advance + evolve, propagate, SH forward + normalise, CCD, slopes (2),

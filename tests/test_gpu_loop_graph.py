@@ -118,7 +118,8 @@ def test_fractional_delay_falls_back_to_sequential_graph(cuda):
     assert not loop.pipelined and loop.steps_per_replay == 1
 
 
-def test_io_graph_follows_per_step_inputs(cuda):
+@pytest.mark.parametrize('slots', [1, 2])
+def test_io_graph_follows_per_step_inputs(cuda, slots):
     """capture(io=True): every replayed step reads its own seeing / wind row
     from io_inputs and leaves its slopes and commands in io_outputs; the
     results equal the object-by-object loop fed the same per-step inputs."""
@@ -143,7 +144,7 @@ def test_io_graph_follows_per_step_inputs(cuda):
     got._inputs.copy_(torch.tensor(inputs(0), dtype=torch.float64))
     got.step_eager()
     got._inputs.copy_(torch.tensor(inputs(1), dtype=torch.float64))
-    got.capture(io=True)
+    got.capture(io=True, io_slots=slots)
     assert tuple(got.io_inputs.shape) == (2, n_in)
     nsl = got.slopec.slopes.slopes.numel()
     for t in range(2, 8):
@@ -152,10 +153,12 @@ def test_io_graph_follows_per_step_inputs(cuda):
         outs_ref.append(torch.cat([ref.slopec.slopes.slopes, ref.integ.out_comm.value]).clone())
     outs_got = []
     for r in range(3):
+        # with two slots the replays alternate between the slots' graphs
+        j = r % slots
         for s in range(2):
-            got.io_inputs[s].copy_(torch.tensor(inputs(2 + 2 * r + s), dtype=torch.float64))
-        got.replay()
-        outs_got.extend([got.io_outputs[0].clone(), got.io_outputs[1].clone()])
+            got.io_inputs_slots[j][s].copy_(torch.tensor(inputs(2 + 2 * r + s), dtype=torch.float64))
+        got.replay(j)
+        outs_got.extend([got.io_outputs_slots[j][0].clone(), got.io_outputs_slots[j][1].clone()])
     torch.cuda.synchronize()
     for t, (a, b) in enumerate(zip(outs_ref, outs_got)):
         assert torch.equal(a[:nsl], b[:nsl]), ('slopes', t)
