@@ -770,7 +770,7 @@ typedef struct sb_mc_group {
     /* detector and slopes */
     float *intensity, *integrated, *pixels;
     long long frame_stride;
-    sb_ccd_params ccd;                  /* shared parameters and frame state           */
+    sb_ccd_params ccd;                  /* shared parameters and frame state (one per group) */
     const uint64_t *photon_seeds;       /* device [n_batch]                            */
     const uint64_t *readout_seeds;      /* device [n_batch]                            */
     sb_slopec_plan slopec;

@@ -1185,6 +1185,10 @@ int mc_chain_prepare(const sb_mc_group *gs, int n, const McShParts &parts, void 
             return fail(SB_EUNSUPPORTED, "%s: group %d: the detector must read a %d x %d frame every step", who, g,
                         side, side);
         if (c.photon_noise && !(c.adu_gain > 0.f)) return fail(SB_EINVAL, "%s: group %d: ADU gain <= 0", who, g);
+        // the group's CTAs count down on its own frame state
+        for (int h = 0; h < g; ++h)
+            if (gs[h].ccd.state == c.state)
+                return fail(SB_EINVAL, "%s: groups %d and %d share a detector frame state", who, h, g);
         if (sl.npx2 != npx * npx || sl.n_subaps < 1 || sl.n_subaps > nl * nl)
             return fail(SB_EINVAL, "%s: group %d: slope plan of %d sub-apertures x %d pixels", who, g, sl.n_subaps,
                         sl.npx2);
