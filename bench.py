@@ -287,6 +287,9 @@ def bench_adjoint_im(dev, reps, cpu_budget_s):
             # dirty lines are written back before the timed call
             flush.fill_(1.0)
             clean.sum()
+            # keep the device busy (~0.5 ms) while the host prepares the timed
+            # call, so the start event does not count host-side launch work
+            torch.cuda._sleep(1_000_000)
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(st)

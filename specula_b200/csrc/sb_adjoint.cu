@@ -411,21 +411,27 @@ extern "C" int sb_sh_slopes_vjp(const sb_sh_plan *pl, const float *A, const floa
 // mirror's influence-function columns enumerate its pixels row-major, so
 // the np_sub field rows of lenslet row li fall inside one contiguous column
 // range of every mode's row: row_seg[li] = {start, count} (floats, both
-// multiples of 32).  The matrix is seen as modes x (ld_if / 32) chunks of 32
-// floats (a 3-D tensor map) and one box of seg_max / 32 chunks of one mode
-// is that mode's segment.  A persistent CTA walks work items (lenslet row,
-// chunk of modes); one producer lane loads each mode's box into a
-// shared-memory ring (L2 evict-first) and the consumer warps, one thread per
-// field column as in intmat_contract_kernel, read their np_sub samples from
-// shared memory.  The products, their order and the cut-off are those of
-// intmat_contract_kernel, so the matrices are the same bits.  Every wait is
-// bounded: on timeout the kernel records it in g_contract_status, stops
-// issuing, lets the copies in flight land (bounded) and returns.
+// multiples of 32).  A work unit is (lenslet row, kCbUnitModes consecutive
+// modes): one ring stage, filled by ceil(count / 256) 2-D TMA boxes of 256
+// columns x kCbUnitModes modes, so a thread's sample of mode k sits k * 1 KB
+// past its sample of mode 0.  A persistent CTA walks a contiguous range of units in
+// row-major order; one producer lane loads each unit's box into the ring (L2
+// evict-first) and the consumer warps, one thread per field column as in
+// intmat_contract_kernel, read their np_sub samples per mode from shared
+// memory.  Each column's products are summed over its np_sub rows in the
+// order of intmat_contract_kernel; the np_sub columns of a lenslet are then
+// summed by a transposed butterfly (group_sum_transposed) that adds the same
+// pairs as that kernel's shuffle tree, so the matrices are the same bits.
+// Every wait is bounded: on timeout the kernel records it in
+// g_contract_status, stops issuing, lets the copies in flight land
+// (bounded) and returns.
 // ---------------------------------------------------------------------------
 constexpr int kCbMaxStages = 8;
-constexpr int kCbModesPerStage = 2;    // modes per TMA box (kContractModes is a multiple of it)
-static_assert(kContractModes % kCbModesPerStage == 0, "whole stages per chunk of modes");
+constexpr int kCbUnitModes = 4;        // modes per TMA box and work unit
 constexpr int kCbMaxConsumers = 992;   // field columns (+ one producer warp <= 1024 threads)
+constexpr int kCbRingBytes = 100 * 1024;
+constexpr int kCbBoxCols = 256;        // columns per TMA box (the largest box extent)
+constexpr int kCbMaxSegment = 7168;    // two stages of kCbUnitModes modes: 224 KB
 
 __device__ int g_contract_status = 0;
 
@@ -440,7 +446,7 @@ struct ContractTmaArgs {
     int n_modes, ld_if;
     float scale;
     float *im;
-    int stages, stage_floats;
+    int stages, stage_floats;          // ring stages; floats per mode in a stage (multiple of kCbBoxCols)
 };
 
 // Columns streamed for lenslet row li: 0 when the row has none, or when its
@@ -456,19 +462,121 @@ __device__ __forceinline__ int seg_count(const ContractTmaArgs &a, int li) {
     return cnt;
 }
 
+// Sums v[0..NV) of the P lanes of each aligned lane group (P a power of two
+// dividing 32) with NV / 2 + NV / 4 + ... shuffles instead of NV * log2(P):
+// at the level of lane distance o every lane keeps half of its values (the
+// upper half when lane bit o is set), adds its partner's copy of that half
+// and passes the other half on.  On return lane c of a group holds, in
+// v[0..NV / P), the sums of values c * NV / P .. c * NV / P + NV / P - 1.
+// Each sum adds the same pairs as v += shfl_down(v, o, P) for o = P/2 .. 1
+// (addition commutes exactly), so it has the same bits as that tree's lane 0.
+template <int P, int NV>
+__device__ __forceinline__ void group_sum_transposed(float (&v)[NV], int c) {
+    static_assert(NV % P == 0, "whole values per lane");
+#pragma unroll
+    for (int o = P / 2, h = NV / 2; o >= 1; o >>= 1, h >>= 1) {
+        const bool upper = (c & o) != 0;
+#pragma unroll
+        for (int i = 0; i < h; ++i) {
+            const float send = upper ? v[i] : v[i + h];
+            const float keep = upper ? v[i + h] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+    }
+}
+
+// Weight of each unit of a lenslet row with cnt columns: its TMA boxes + 1
+// (a unit's fixed cost).
+__device__ __forceinline__ int cb_unit_weight(const ContractTmaArgs &a, int cnt) {
+    cnt = cnt < 0 ? 0 : cnt > a.stage_floats ? a.stage_floats : cnt;
+    return (cnt + kCbBoxCols - 1) / kCbBoxCols + 1;
+}
+
+constexpr int kCbMaxRows = (kCbMaxConsumers + 3) / 4;      // lenslet rows (np_sub >= 4)
+constexpr int kCbRowBlocks = (kCbMaxRows + 31) / 32;
+
+// The range [r[0], r[1]) of units of work part `part` of `parts`, in
+// row-major order.  Unit (li, j) starts at weight W(li) + j * w(li), W(li) the
+// weight of the rows before li; part b takes the units starting in
+// [T * b / parts, T * (b + 1) / parts), T the total, so the ranges tile the
+// units and carry about equal numbers of boxes.  Run by the 32 lanes of one
+// warp (every row's count loaded in one round); lane 0 writes r.
+__device__ void cb_unit_range(const ContractTmaArgs &a, int per_row, int part, int parts, int lane, int *r) {
+    int w[kCbRowBlocks];
+#pragma unroll
+    for (int k = 0; k < kCbRowBlocks; ++k) {
+        const int li = 32 * k + lane;
+        w[k] = li < a.n ? cb_unit_weight(a, a.row_seg[2 * li + 1]) : 0;
+    }
+    long long T = 0;
+#pragma unroll
+    for (int k = 0; k < kCbRowBlocks; ++k) {
+        long long t = (long long)per_row * w[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+        T += t;
+    }
+    const long long lo = T * part / parts, hi = T * (part + 1) / parts;
+    const int n_units = per_row * a.n;
+    int u0 = n_units, u1 = n_units;
+    bool f0 = false, f1 = false;
+    long long W = 0;
+#pragma unroll
+    for (int k = 0; k < kCbRowBlocks; ++k) {
+        const int li = 32 * k + lane;
+        const bool row = li < a.n;
+        const long long rw = (long long)per_row * w[k];
+        long long incl = rw;     // inclusive scan of the row weights over the lanes
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const long long wr = W + incl - rw;
+        // the row's first unit starting at or after weight t (per_row: none)
+        const auto first = [&](long long t) -> int {
+            if (!row) return per_row;
+            if (t <= wr) return 0;
+            const long long j = (t - wr + w[k] - 1) / w[k];
+            return j < per_row ? (int)j : per_row;
+        };
+        const int j0 = first(lo), j1 = first(hi);
+        const unsigned m0 = __ballot_sync(0xffffffffu, j0 < per_row);
+        const unsigned m1 = __ballot_sync(0xffffffffu, j1 < per_row);
+        if (!f0 && m0) {
+            const int L = __ffs(m0) - 1;
+            u0 = (32 * k + L) * per_row + __shfl_sync(0xffffffffu, j0, L);
+            f0 = true;
+        }
+        if (!f1 && m1) {
+            const int L = __ffs(m1) - 1;
+            u1 = (32 * k + L) * per_row + __shfl_sync(0xffffffffu, j1, L);
+            f1 = true;
+        }
+        W += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    if (lane == 0) {
+        r[0] = u0;
+        r[1] = u1;
+    }
+}
+
 template <int P>
 __global__ void __launch_bounds__(1024, 1) intmat_contract_tma_kernel(const __grid_constant__ CUtensorMap map,
                                                                       ContractTmaArgs a) {
+    constexpr int MU = kCbUnitModes;
+    constexpr int NV = 2 * MU;                  // (mode, axis) sums per unit
+    constexpr int R = NV / P > 0 ? NV / P : 1;  // of them left on each lane
+    static_assert(NV % P == 0, "a lenslet's lanes share the unit's sums");
     extern __shared__ __align__(128) unsigned char cb_smem[];
     // TMA destinations on 128-byte boundaries (segments are multiples of 128 bytes)
     unsigned char *base = cb_smem + ((128 - (sb::smem_u32(cb_smem) & 127)) & 127);
     float *ring = reinterpret_cast<float *>(base);
-    const int seg_floats = a.stage_floats;                 // one mode's segment
-    const int stage = kCbModesPerStage * seg_floats;       // one stage: consecutive modes' segments
+    const int stage = MU * a.stage_floats;      // floats per ring stage
     uint64_t *full = reinterpret_cast<uint64_t *>(base + (size_t)a.stages * stage * 4);
     uint64_t *empty = full + a.stages;
     __shared__ double red[33];
-    __shared__ int abort_flag, issued;
+    __shared__ int abort_flag, issued, unit_range[2];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int ncons = blockDim.x - 32;           // consumer threads (a multiple of 32)
     const int nwc = ncons >> 5;
@@ -482,134 +590,151 @@ __global__ void __launch_bounds__(1024, 1) intmat_contract_tma_kernel(const __gr
         abort_flag = 0;
         issued = 0;
     }
-    // the CoG cut-off's mean, summed as intmat_contract_kernel sums it (the
-    // producer warp adds zeros)
-    double mean = 0.0;
-    if (a.tot) {
-        double part = 0.0;
-        if (tid < ncons)
-            for (int e = tid; e < a.n_valid; e += ncons) part += (double)a.tot[e];
-        mean = sb::block_sum_all_d(part, red) / a.n_valid;
-    }
     __syncthreads();
-    const int chunks = (a.n_modes + kContractModes - 1) / kContractModes;
-    const int n_items = chunks * a.n;
+    const int per_row = (a.n_modes + MU - 1) / MU;
     const size_t ld_im = 2 * (size_t)a.n_valid;
-    // items (lenslet row, 16 modes) in row-major order, a contiguous range per
-    // CTA: a CTA meets few lenslet rows, so its consumers load each row's
-    // Jacobian and column offsets once for all its mode chunks
-    const int w_begin = (int)((long long)blockIdx.x * n_items / gridDim.x);
-    const int w_end = (int)((long long)(blockIdx.x + 1) * n_items / gridDim.x);
     if (warp == nwc) {
+        // the CTA's contiguous range of units (lenslet row, MU modes) in row-major
+        // order, balanced by the boxes they load; published to the consumers
+        // through named barrier 1 (arrive here, sync there)
+        cb_unit_range(a, per_row, blockIdx.x, gridDim.x, lane, unit_range);
+        asm volatile("bar.arrive 1, %0;" ::"r"(blockDim.x) : "memory");
         if (lane == 0) {
+            const int u_begin = unit_range[0], u_end = unit_range[1];
             const uint64_t pol = sb::l2_evict_first_policy();
-            int q = 0, st = 0;
+            int q = 0, st = 0, cur = -1, cnt = 0, start = 0;
             uint32_t ph = 0;
-            bool stop = false;
-            for (int w = w_begin; w < w_end && !stop; ++w) {
-                const int li = w / chunks, m0 = (w % chunks) * kContractModes;
-                const int m1 = min(a.n_modes, m0 + kContractModes);
-                const int cnt = seg_count(a, li);
+            for (int u = u_begin; u < u_end; ++u) {
+                const int li = u / per_row, m0 = (u - li * per_row) * MU;
+                if (li != cur) {
+                    cur = li;
+                    cnt = seg_count(a, li);
+                    start = a.row_seg[2 * li];
+                }
                 if (cnt <= 0) continue;
-                const int start = a.row_seg[2 * li];
-                for (int m = m0; m < m1; m += kCbModesPerStage, ++q) {
-                    // reuse a slot once every consumer warp released its previous use
-                    if (q >= S && !sb::mbar_wait(&empty[st], ph ^ 1u)) {
-                        atomicExch(&g_contract_status, 1);
-                        abort_flag = 1;
-                        stop = true;
-                        break;
-                    }
-                    // the box is always the whole stage (modes past the matrix read as zeros)
-                    sb::mbar_arrive_expect_tx(&full[st], (uint32_t)stage * 4u);
-                    sb::tma_load_3d(ring + (size_t)st * stage, &map, 0, start / 32, m, &full[st], pol);
-                    if (++st == S) {
-                        st = 0;
-                        ph ^= 1u;
-                    }
+                // reuse a slot once every consumer warp released its previous use
+                if (q >= S && !sb::mbar_wait(&empty[st], ph ^ 1u)) {
+                    atomicExch(&g_contract_status, 1);
+                    abort_flag = 1;
+                    break;
+                }
+                // whole boxes: columns and modes past the matrix read as zeros
+                const int nb = (cnt + kCbBoxCols - 1) / kCbBoxCols;
+                sb::mbar_arrive_expect_tx(&full[st], (uint32_t)(nb * kCbBoxCols * MU * 4));
+                for (int b = 0; b < nb; ++b)
+                    sb::tma_load_2d(ring + (size_t)st * stage + b * (kCbBoxCols * MU), &map, start + b * kCbBoxCols,
+                                    m0, &full[st], pol);
+                ++q;
+                if (++st == S) {
+                    st = 0;
+                    ph ^= 1u;
                 }
             }
             issued = q;
         }
     } else {
+        // the CoG cut-off's mean over the consumer threads (named barrier 2),
+        // while the producer already streams
+        double mean = 0.0;
+        if (a.tot) {
+            double part = 0.0;
+            for (int e = tid; e < a.n_valid; e += ncons) part += (double)a.tot[e];
+            part = sb::warp_sum_d(part);
+            if (lane == 0) red[warp] = part;
+            asm volatile("bar.sync 2, %0;" ::"r"(ncons) : "memory");
+            if (warp == 0) {
+                double r = lane < nwc ? red[lane] : 0.0;
+                r = sb::warp_sum_d(r);
+                if (lane == 0) red[32] = r;
+            }
+            asm volatile("bar.sync 2, %0;" ::"r"(ncons) : "memory");
+            mean = red[32] / a.n_valid;
+        }
+        asm volatile("bar.sync 1, %0;" ::"r"(blockDim.x) : "memory");
+        const int u_begin = unit_range[0], u_end = unit_range[1];
         const int x = tid;
         const int lj = x / P, c = x - lj * P;
         int st = 0;
         uint32_t ph = 0;
-        bool failed = false;
         int cur = -1, cnt = 0, s = -1;
         // a masked pixel reads offset 0 with zero weights: fmaf(0, f, v) == v for the finite
         // influence functions, as fmaf(j, 0, v) in intmat_contract_kernel
         float jx[P], jy[P];
-        int off[P];
-        for (int w = w_begin; w < w_end && !failed; ++w) {
-            const int li = w / chunks, m0 = (w % chunks) * kContractModes;
-            const int m1 = min(a.n_modes, m0 + kContractModes);
+        int off[P];      // offset of the sample of mode 0 in a stage
+        for (int u = u_begin; u < u_end; ++u) {
+            const int li = u / per_row, m0 = (u - li * per_row) * MU;
             if (li != cur) {
+                // a new lenslet row: slot and column map, then flux and Jacobian
+                // (two dependent rounds of loads)
                 cur = li;
                 cnt = seg_count(a, li);
                 const int start = a.row_seg[2 * li];
                 s = (lj < a.n) ? a.slot[li * a.n + lj] : -1;
-                bool act = s >= 0;
-                if (a.tot && act) {
-                    const float t = a.tot[s];
-                    act = t > 0.f && (double)(1.0f / t) <= 1.0 / (mean * 1e-3);
+                int col[P];
+#pragma unroll
+                for (int rr = 0; rr < P; ++rr)
+                    col[rr] = (lj < a.n) ? a.pix2col[(size_t)(li * P + rr) * a.field_ld + x] : -1;
+                float t = 1.f;
+#pragma unroll
+                for (int rr = 0; rr < P; ++rr) jx[rr] = jy[rr] = 0.f;
+                if (s >= 0) {
+                    if (a.tot) t = a.tot[s];
+#pragma unroll
+                    for (int rr = 0; rr < P; ++rr) {
+                        jx[rr] = a.jac[(size_t)s * (P * P) + rr * P + c];
+                        jy[rr] = a.jac[((size_t)a.n_valid + s) * (P * P) + rr * P + c];
+                    }
                 }
+                const bool act = s >= 0 && (!a.tot || (t > 0.f && (double)(1.0f / t) <= 1.0 / (mean * 1e-3)));
 #pragma unroll
                 for (int rr = 0; rr < P; ++rr) {
                     off[rr] = 0;
-                    jx[rr] = jy[rr] = 0.f;
-                    if (act) {
-                        const int col = a.pix2col[(size_t)(li * P + rr) * a.field_ld + x];
-                        if (col >= 0 && (col < start || col - start >= cnt)) {
-                            atomicExch(&g_contract_status, 3);      // a column outside its row's segment
-                        } else if (col >= 0) {
-                            off[rr] = col - start;
-                            jx[rr] = a.jac[(size_t)s * (P * P) + rr * P + c];
-                            jy[rr] = a.jac[((size_t)a.n_valid + s) * (P * P) + rr * P + c];
-                        }
+                    const int cl = act ? col[rr] : -1;
+                    if (cl >= 0 && (cl < start || cl - start >= cnt))
+                        atomicExch(&g_contract_status, 3);      // a column outside its row's segment
+                    if (cl >= 0 && cl >= start && cl - start < cnt) {
+                        const int o = cl - start;
+                        off[rr] = (o / kCbBoxCols) * (kCbBoxCols * MU) + o % kCbBoxCols;
+                    } else {
+                        jx[rr] = jy[rr] = 0.f;
                     }
                 }
             }
-            float *im_x = a.im + s;
-            for (int m = m0; m < m1; m += kCbModesPerStage) {
-                float v[kCbModesPerStage][2];
+            float v[NV];
 #pragma unroll
-                for (int k = 0; k < kCbModesPerStage; ++k) v[k][0] = v[k][1] = 0.f;
-                if (cnt > 0) {
-                    if (!sb::mbar_wait_sleep(&full[st], ph)) {
-                        atomicExch(&g_contract_status, 2);
-                        abort_flag = 1;
-                        failed = true;
-                        break;
-                    }
-                    const float *seg = ring + (size_t)st * stage;
+            for (int i = 0; i < NV; ++i) v[i] = 0.f;
+            if (cnt > 0) {
+                const bool ok = sb::mbar_wait_sleep(&full[st], ph);
+                if (__any_sync(0xffffffffu, !ok)) {
+                    if (lane == 0) atomicExch(&g_contract_status, 2);
+                    abort_flag = 1;
+                    break;
+                }
+                const float *seg = ring + (size_t)st * stage;
 #pragma unroll
-                    for (int k = 0; k < kCbModesPerStage; ++k)
+                for (int rr = 0; rr < P; ++rr) {
+                    const float *p = seg + off[rr];
 #pragma unroll
-                        for (int rr = 0; rr < P; ++rr) {
-                            const float f = seg[k * seg_floats + off[rr]];
-                            v[k][0] = fmaf(jx[rr], f, v[k][0]);
-                            v[k][1] = fmaf(jy[rr], f, v[k][1]);
-                        }
-                    __syncwarp();
-                    if (lane == 0) sb::mbar_arrive(&empty[st]);
-                    if (++st == S) {
-                        st = 0;
-                        ph ^= 1u;
+                    for (int k = 0; k < MU; ++k) {
+                        const float f = p[kCbBoxCols * k];
+                        v[2 * k] = fmaf(jx[rr], f, v[2 * k]);
+                        v[2 * k + 1] = fmaf(jy[rr], f, v[2 * k + 1]);
                     }
                 }
+                __syncwarp();
+                if (lane == 0) sb::mbar_arrive(&empty[st]);
+                if (++st == S) {
+                    st = 0;
+                    ph ^= 1u;
+                }
+            }
+            group_sum_transposed<P, NV>(v, c);
+            if (s >= 0) {
 #pragma unroll
-                for (int k = 0; k < kCbModesPerStage; ++k) {
-#pragma unroll
-                    for (int o = P / 2; o > 0; o >>= 1) {
-                        v[k][0] += __shfl_down_sync(0xffffffffu, v[k][0], o, P);
-                        v[k][1] += __shfl_down_sync(0xffffffffu, v[k][1], o, P);
-                    }
-                    if (c == 0 && s >= 0 && m + k < m1) {
-                        im_x[(size_t)(m + k) * ld_im] = a.scale * v[k][0];
-                        im_x[(size_t)(m + k) * ld_im + a.n_valid] = a.scale * v[k][1];
-                    }
+                for (int r = 0; r < R; ++r) {
+                    const int i = c * R + r;          // (mode, axis) of this sum
+                    const int m = m0 + (i >> 1);
+                    if (m < a.n_modes) a.im[(size_t)m * ld_im + (i & 1) * a.n_valid + s] = a.scale * v[r];
                 }
             }
         }
@@ -679,24 +804,22 @@ extern "C" int sb_intmat_contract_rows(const float *jac, const float *tot, int n
         n_lenses < 1 || ld_if < 1 || seg_max < 0)
         return sb::fail(SB_EINVAL, "sb_intmat_contract_rows: bad args");
     if (field_ld < n_lenses * np_sub) return sb::fail(SB_EINVAL, "sb_intmat_contract_rows: bad field stride");
-    if (ld_if % 32 || (uintptr_t)ifunc % 16 || seg_max % 32 || seg_max > 12 * 1024)
+    if (ld_if % 32 || (uintptr_t)ifunc % 16 || seg_max % 32 || seg_max > kCbMaxSegment)
         return sb::fail(SB_EINVAL, "sb_intmat_contract_rows: ld_if and seg_max must be multiples of 32 floats "
-                                   "(seg_max <= 12288), ifunc 16-byte aligned");
+                                   "(seg_max <= %d), ifunc 16-byte aligned", kCbMaxSegment);
     const int ncons = (n_lenses * np_sub + 31) / 32 * 32;
     if (ncons > kCbMaxConsumers)
         return sb::fail(SB_ESHAPE, "sb_intmat_contract_rows: field of %d columns (at most %d)", n_lenses * np_sub,
                         kCbMaxConsumers);
     if (n_modes == 0) return SB_OK;
-    const int stage_floats = seg_max > 0 ? seg_max : 32;    // one mode's segment
-    int stages = (int)((96 * 1024) / ((size_t)stage_floats * 4 * kCbModesPerStage));
-    stages = stages > kCbMaxStages ? kCbMaxStages : stages;
-    if (stages < 2)
-        return sb::fail(SB_ESHAPE, "sb_intmat_contract_rows: segments of %d floats exceed the shared-memory ring",
-                        seg_max);
+    const int stage_floats = seg_max > 0 ? (seg_max + kCbBoxCols - 1) / kCbBoxCols * kCbBoxCols : kCbBoxCols;
+    // a ring of kCbRingBytes (two CTAs per SM), else two stages in one CTA's shared memory
+    int stages = (int)(kCbRingBytes / ((size_t)stage_floats * 4 * kCbUnitModes));
+    stages = stages > kCbMaxStages ? kCbMaxStages : stages < 2 ? 2 : stages;
     CUtensorMap map;
-    int rc = sb::tensor_map_rows32_f32(&map, ifunc, n_modes, ld_if, stage_floats / 32, kCbModesPerStage);
+    int rc = sb::tensor_map_2d_f32(&map, ifunc, n_modes, ld_if, ld_if, kCbUnitModes, kCbBoxCols);
     if (rc) return rc;
-    const size_t smem = 128 + (size_t)stages * stage_floats * 4 * kCbModesPerStage + 2 * (size_t)stages * 8;
+    const size_t smem = 128 + (size_t)stages * stage_floats * 4 * kCbUnitModes + 2 * (size_t)stages * 8;
     ContractTmaArgs a;
     a.jac = jac;
     a.tot = tot;
@@ -731,9 +854,9 @@ extern "C" int sb_intmat_contract_rows(const float *jac, const float *tot, int n
                         e != cudaSuccess ? cudaGetErrorString(e) : "no CTA fits an SM");
     const int nsm = sb::sm_count();
     if (nsm < 1) return sb::fail(SB_ECUDA, "sb_intmat_contract_rows: SM count query failed");
-    const int chunks = (n_modes + kContractModes - 1) / kContractModes;
+    const int units = (n_modes + kCbUnitModes - 1) / kCbUnitModes * n_lenses;
     int grid = per_sm * nsm;
-    grid = grid > chunks * n_lenses ? chunks * n_lenses : grid;
+    grid = grid > units ? units : grid;
     fn<<<grid, threads, smem, sb::as_stream(stream)>>>(map, a);
     return sb::check_launch("intmat_contract_tma_kernel");
 }

@@ -55,30 +55,6 @@ int tensor_map_2d_f32(CUtensorMap *map, const float *base, int rows, int cols, i
     return SB_OK;
 }
 
-int tensor_map_rows32_f32(CUtensorMap *map, const float *base, int rows, int ld, int box_chunks, int box_rows) {
-    static EncodeTiledFn enc = nullptr;
-    if (!enc) {
-        cudaDriverEntryPointQueryResult qr;
-        void *fn = nullptr;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &qr) != cudaSuccess ||
-            qr != cudaDriverEntryPointSuccess || !fn)
-            return fail(SB_ECUDA, "cuTensorMapEncodeTiled is not available from the driver");
-        enc = reinterpret_cast<EncodeTiledFn>(fn);
-    }
-    if ((reinterpret_cast<uintptr_t>(base) & 15) || ld % 32 || box_chunks < 1 || box_chunks > 256 || box_rows < 1 ||
-        box_rows > 256)
-        return fail(SB_EINVAL, "tensor map: 16-byte base, row stride a multiple of 32 floats, 1..256 chunks and rows");
-    cuuint64_t dims[3] = {32, (cuuint64_t)(ld / 32), (cuuint64_t)rows};
-    cuuint64_t strides[2] = {128, (cuuint64_t)ld * 4};
-    cuuint32_t box[3] = {32, (cuuint32_t)box_chunks, (cuuint32_t)box_rows};
-    cuuint32_t estr[3] = {1, 1, 1};
-    const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(base), dims, strides, box,
-                           estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return fail(SB_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
-    return SB_OK;
-}
-
 int sm_count() {
     static int cache[64] = {0};
     int dev = 0;

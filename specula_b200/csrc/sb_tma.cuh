@@ -131,12 +131,6 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, i
 // out-of-range elements of a box read as zero.  Returns SB_OK or a status.
 int tensor_map_2d_f32(CUtensorMap *map, const float *base, int rows, int cols, int ld, int box_rows, int box_cols);
 
-// Host: a row-major float32 matrix (rows x ld, ld a multiple of 32) seen as
-// rows x (ld / 32) chunks of 32 floats, as a 3-D tensor map whose box is
-// box_chunks consecutive chunks (<= 256) of box_rows consecutive rows: per
-// row a contiguous run of 32 * box_chunks floats starting at a 32-float
-// boundary (rows past the matrix read as zeros).
-int tensor_map_rows32_f32(CUtensorMap *map, const float *base, int rows, int ld, int box_chunks, int box_rows);
 
 // Streaming multiprocessors of the current device (cached per device).
 int sm_count();

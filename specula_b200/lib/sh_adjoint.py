@@ -357,10 +357,10 @@ class ShSlopesAdjoint:
 
     # TMA contraction limits: np_sub 4 or 8, at most 992 field columns,
     # influence-function rows of a multiple of 32 floats, a row segment of at
-    # most 8192 floats (256 chunks of 32)
+    # most 7168 floats (two ring stages of four modes in one CTA's shared memory)
     TMA_NP_SUB = (4, 8)
     TMA_MAX_COLUMNS = 992
-    TMA_MAX_SEGMENT = 8192
+    TMA_MAX_SEGMENT = 7168
 
     def _segments(self, pix2col, IF, ld):
         """(device table, largest count) of the row segments for the TMA
