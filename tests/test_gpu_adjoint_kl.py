@@ -97,6 +97,32 @@ def test_kl_adjoint_intmat_matches_fp64_pushpull(kl_system):
         assert rel_max_err(im[k], ref) <= ADJ_TOL, k
 
 
+def test_kl_adjoint_full_intmat_matches_fp64_pushpull(kl_system):
+    """Every row of the 500 x 2 n_valid matrix against the float64 oracle's
+    push-pull at 1e-2 nm RMS (im_rec_calibrator.py:58-63: row k is
+    s(+a)/a + s(-a)/(-a)), 1000 oracle forwards.  Mode k's phase is
+    sign * a * IF[k] on the pupil, which is what dm.py:72-86 gives for a
+    one-hot command."""
+    cal, slopes64 = kl_system
+    im = cal.adjoint_intmat().cpu().numpy().astype(np.float64)
+    IF = cal.dm._ifunc.influence_function.cpu().numpy().astype(np.float64)
+    idx = np.where(cal.pupil > 0)
+    amp = 1e-2
+
+    def s64(k, a):
+        ph = np.zeros(cal.pupil.shape)
+        ph[idx] = cal.dm.sign * a * IF[k]
+        return slopes64(ph)
+
+    ref = octl.pushpull_intmat(s64, IF.shape[0], np.full(IF.shape[0], amp))
+    assert ref.shape == im.shape
+    per_mode = np.array([rel_max_err(im[k], ref[k]) for k in range(im.shape[0])])
+    print(f'full adjoint IM vs float64 push-pull: whole matrix {rel_max_err(im, ref):.2e}, '
+          f'per mode max {per_mode.max():.2e} (mode {int(per_mode.argmax())}), median {np.median(per_mode):.2e}')
+    assert rel_max_err(im, ref) <= ADJ_TOL
+    assert per_mode.max() <= ADJ_TOL, int(per_mode.argmax())
+
+
 @pytest.mark.parametrize('operating_point', [None, 0, 1, 2, 3])
 def test_jacobian_on_kolmogorov_probes(kl_system, operating_point):
     """Flat calibration point (None) along all 32 probes; probe k as the
