@@ -309,6 +309,12 @@ def bench_adjoint_im(dev, reps, cpu_budget_s):
     active = adj.active(cal.A, cal._flat)
     jac_ms, jac = timed(lambda: adj.jacobian(cal.A, cal._flat, active), reps)
     con_ms, _ = timed(lambda: adj.intmat(cal.A, cal._flat, cal.dm, jac=jac, pix2col=cal._pix2col), reps)
+    # set-up of the contraction's lenslet-major copy of the influence functions
+    # (once per mirror and column map; cached by the adjoint)
+    def relayout():
+        adj._ifl_cache = None
+        return adj.lenslet_ifunc(cal.dm._IF, cal.dm._ld, cal._pix2col)
+    layout_ms, _ = timed(relayout, 3)
     n_in = cal.pixels_under_valid_subaps()
     con_bytes = cal.contract_bytes(cal.n_modes, n_in, cal.n_valid, adj.np_sub ** 2)
     peak, peak_kind = measured_peak_hbm()
@@ -323,6 +329,7 @@ def bench_adjoint_im(dev, reps, cpu_budget_s):
                             'CUDA graph',
            'rel_diff_vs_gpu_pushpull': err,
            'jacobian_kernel_us': jac_ms * 1e3, 'contract_kernel_us': con_ms * 1e3,
+           'contract_form': adj.contraction, 'contract_layout_us': layout_ms * 1e3,
            'contract_roofline': {'bound': 'hbm', 'achieved': con_gbs, 'peak': peak, 'peak_kind': peak_kind,
                                  'unit': 'GB/s', 'frac': con_gbs / peak, 'algorithmic_bytes': con_bytes},
            'l2': 'flushed before every timed call (256 MB written, then 256 MB read)'}

@@ -518,8 +518,9 @@ int sb_intmat_contract(const float *jac, const float *tot, int n_valid, int np_s
  * range: row_seg[2*li] = first column, row_seg[2*li+1] = number of columns
  * (both multiples of 32, covering every column under a valid sub-aperture of
  * that row; 0 columns for a row without any), seg_max = the largest count
- * (<= 8192).  One mode's segment of one lenslet row is one TMA box loaded
- * into a shared-memory ring of up to 8 stages (96 KB).  Needs ld_if a
+ * (<= 7168).  A work unit (lenslet row, 4 modes) is one stage of a
+ * shared-memory ring (about 100 KB per CTA), loaded as 256-column x 4-mode
+ * 2-D TMA boxes.  Needs ld_if a
  * multiple of 32, a 16-byte aligned ifunc, np_sub 4 or 8 and at most 992
  * field columns; a segment that is misaligned or misses a column is skipped
  * and reported by sb_device_status (SB_EINVAL), as are timed-out waits
@@ -528,6 +529,25 @@ int sb_intmat_contract_rows(const float *jac, const float *tot, int n_valid, int
                             int field_ld, const int32_t *slot, const int32_t *pix2col, const int32_t *row_seg,
                             int seg_max, const float *ifunc, int n_modes, int ld_if, float scale, float *intmat,
                             void *stream);
+
+/* The same contraction (im_rec_calibrator.py:58-63 in its small-amplitude
+ * limit) in two steps, for a mirror whose interaction matrix is computed
+ * more than once (at several operating points, or each calibration).
+ * sb_intmat_lenslet_ifunc copies, once per mirror and column map, the
+ * influence-function samples under the valid sub-apertures into a
+ * lenslet-major array: ifl[m][s][c][r] = ifunc[m * ld_if + col] with col =
+ * pix2col[(li * np_sub + r) * field_ld + lj * np_sub + c], 0 where col < 0,
+ * lenslet[s] = li * n_lenses + lj the lenslet of valid sub-aperture s
+ * (n_modes * n_valid * np_sub^2 floats, 16-byte aligned).
+ * sb_intmat_contract_lenslets then reads that array once per matrix (one
+ * contiguous np_sub^2 run per mode and sub-aperture) with jac, tot and
+ * scale as in sb_intmat_contract, and writes the same matrix bit for bit
+ * (the same products, summed in the same order).  np_sub 4 or 8. */
+int sb_intmat_lenslet_ifunc(const float *ifunc, int n_modes, int ld_if, const int32_t *lenslet, int n_valid,
+                            int np_sub, int n_lenses, int field_ld, const int32_t *pix2col, float *ifl,
+                            void *stream);
+int sb_intmat_contract_lenslets(const float *jac, const float *tot, int n_valid, int np_sub, const float *ifl,
+                                int n_modes, float scale, float *intmat, void *stream);
 
 /* ------------------------------------------------------------------------
  * AtmoEvolution — replaces specula/processing_objects/atmo_evolution.py:

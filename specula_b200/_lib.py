@@ -190,6 +190,9 @@ SIGNATURES = {
                                      C.c_float, fp, vp]),
     'sb_intmat_contract_rows': (C.c_int, [fp, fp, C.c_int, C.c_int, C.c_int, C.c_int, ip, ip, ip, C.c_int, fp,
                                           C.c_int, C.c_int, C.c_float, fp, vp]),
+    'sb_intmat_lenslet_ifunc': (C.c_int, [fp, C.c_int, C.c_int, ip, C.c_int, C.c_int, C.c_int, C.c_int, ip, fp,
+                                          vp]),
+    'sb_intmat_contract_lenslets': (C.c_int, [fp, fp, C.c_int, C.c_int, fp, C.c_int, C.c_float, fp, vp]),
 }
 
 _lib = None

@@ -860,3 +860,184 @@ extern "C" int sb_intmat_contract_rows(const float *jac, const float *tot, int n
     fn<<<grid, threads, smem, sb::as_stream(stream)>>>(map, a);
     return sb::check_launch("intmat_contract_tma_kernel");
 }
+
+// ---------------------------------------------------------------------------
+// The contraction on a lenslet-major copy of the influence functions.  At
+// set-up (once per mirror and column map) sb_intmat_lenslet_ifunc gathers
+// the samples under each valid sub-aperture into
+//   ifl[m][s][c][r] = IF[m][pix2col[(li * P + r) * field_ld + lj * P + c]]
+// (0 where pix2col < 0; (li, lj) the lenslet of valid sub-aperture s), so a
+// sub-aperture's P x P samples of one mode are one contiguous run and field
+// column c's P rows are P consecutive floats.  sb_intmat_contract_lenslets
+// then streams that copy once: thread (s, c) reads its P rows as float4
+// loads, sums jac * sample over them in row order and the P columns of the
+// sub-aperture by group_sum_transposed: the pairs and order of
+// intmat_contract_kernel, so the same matrix bit for bit.  No shared-memory
+// ring, no producer: CTAs of 256 threads (256 / P sub-apertures) over a
+// chunk of modes each, loads marked streaming (read once).
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kClThreads = 256;
+constexpr int kClModes = 4;           // modes summed per pass (2 * 4 sums per lenslet)
+
+template <int P>
+__global__ void intmat_lenslet_layout_kernel(const float *__restrict__ IF, int n_modes, int ld_if,
+                                             const int32_t *__restrict__ lenslet, int n_valid, int n, int field_ld,
+                                             const int32_t *__restrict__ pix2col, float *__restrict__ ifl) {
+    const long long per_mode = (long long)n_valid * P * P;
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= per_mode) return;
+    const int s = (int)(e / (P * P)), q = (int)(e - (long long)s * P * P);
+    const int c = q / P, r = q - c * P;
+    const int L = lenslet[s];
+    const int li = L / n, lj = L - li * n;
+    const int col = pix2col[(size_t)(li * P + r) * field_ld + lj * P + c];
+    for (int m = blockIdx.y; m < n_modes; m += gridDim.y)
+        ifl[(size_t)m * per_mode + e] = col >= 0 ? IF[(size_t)m * ld_if + col] : 0.f;
+}
+
+template <int P>
+__global__ void __launch_bounds__(kClThreads, 3) intmat_contract_lenslet_kernel(
+    const float *__restrict__ jac, const float *__restrict__ tot, int n_valid, const float *__restrict__ ifl,
+    int n_modes, int modes_per_cta, float scale, float *__restrict__ im) {
+    constexpr int NV = 2 * kClModes;
+    constexpr int R = NV / P > 0 ? NV / P : 1;
+    static_assert(NV % P == 0 && P % 4 == 0, "whole sums per lane, float4 rows");
+    __shared__ double red[33];
+    const int t = blockIdx.x * kClThreads + threadIdx.x;
+    const int s = t / P, c = t - s * P;
+    const bool in = s < n_valid;
+    bool act = in;
+    if (tot) {
+        // the CoG cut-off of sh_slopec.py:400, as intmat_contract_kernel applies it
+        double part = 0.0;
+        for (int e = threadIdx.x; e < n_valid; e += kClThreads) part += (double)tot[e];
+        const double mean = sb::block_sum_all_d(part, red) / n_valid;
+        if (act) {
+            const float tt = tot[s];
+            act = tt > 0.f && (double)(1.0f / tt) <= 1.0 / (mean * 1e-3);
+        }
+    }
+    float jx[P], jy[P];
+#pragma unroll
+    for (int r = 0; r < P; ++r) {
+        jx[r] = act ? jac[(size_t)s * (P * P) + r * P + c] : 0.f;
+        jy[r] = act ? jac[((size_t)n_valid + s) * (P * P) + r * P + c] : 0.f;
+    }
+    const size_t per_mode = (size_t)n_valid * P * P;
+    const float *mine = ifl + (in ? (size_t)s * (P * P) + c * P : 0);
+    const int m0 = blockIdx.y * modes_per_cta;
+    const int m1 = min(n_modes, m0 + modes_per_cta);
+    const size_t ld_im = 2 * (size_t)n_valid;
+    for (int m = m0; m < m1; m += kClModes) {
+        float4 f[kClModes][P / 4];
+#pragma unroll
+        for (int k = 0; k < kClModes; ++k) {
+            const bool ok = in && m + k < m1;
+            const float4 *p = reinterpret_cast<const float4 *>(mine + (size_t)(ok ? m + k : 0) * per_mode);
+#pragma unroll
+            for (int b = 0; b < P / 4; ++b) f[k][b] = ok ? __ldcs(p + b) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        float v[NV];
+#pragma unroll
+        for (int k = 0; k < kClModes; ++k) {
+            float vx = 0.f, vy = 0.f;
+#pragma unroll
+            for (int b = 0; b < P / 4; ++b) {
+                vx = fmaf(jx[4 * b + 0], f[k][b].x, vx);
+                vy = fmaf(jy[4 * b + 0], f[k][b].x, vy);
+                vx = fmaf(jx[4 * b + 1], f[k][b].y, vx);
+                vy = fmaf(jy[4 * b + 1], f[k][b].y, vy);
+                vx = fmaf(jx[4 * b + 2], f[k][b].z, vx);
+                vy = fmaf(jy[4 * b + 2], f[k][b].z, vy);
+                vx = fmaf(jx[4 * b + 3], f[k][b].w, vx);
+                vy = fmaf(jy[4 * b + 3], f[k][b].w, vy);
+            }
+            v[2 * k] = vx;
+            v[2 * k + 1] = vy;
+        }
+        group_sum_transposed<P, NV>(v, c);
+        if (in) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int i = c * R + r;          // (mode, axis) of this sum
+                const int mm = m + (i >> 1);
+                if (mm < m1) im[(size_t)mm * ld_im + (i & 1) * n_valid + s] = scale * v[r];
+            }
+        }
+    }
+}
+
+// modes per CTA: about four waves of the resident CTAs, whole passes of kClModes
+int lenslet_modes_per_cta(int n_valid, int np_sub, int n_modes) {
+    const int bx = (int)(((long long)n_valid * np_sub + kClThreads - 1) / kClThreads);
+    const int nsm = sb::sm_count();
+    const long long target = 4LL * 3 * (nsm > 0 ? nsm : 148);
+    long long chunks = (target + bx - 1) / bx;
+    const long long passes = (n_modes + kClModes - 1) / kClModes;
+    chunks = chunks < 1 ? 1 : chunks > passes ? passes : chunks;
+    const long long per = (passes + chunks - 1) / chunks;
+    return (int)(per * kClModes);
+}
+
+}  // namespace
+
+extern "C" int sb_intmat_lenslet_ifunc(const float *ifunc, int n_modes, int ld_if, const int32_t *lenslet,
+                                       int n_valid, int np_sub, int n_lenses, int field_ld, const int32_t *pix2col,
+                                       float *ifl, void *stream) {
+    sb::clear_error();
+    if (!ifunc || !lenslet || !pix2col || !ifl || n_modes < 0 || n_valid < 1 || n_lenses < 1 || ld_if < 1)
+        return sb::fail(SB_EINVAL, "sb_intmat_lenslet_ifunc: bad args");
+    if (np_sub != 4 && np_sub != 8)
+        return sb::fail(SB_EUNSUPPORTED, "sb_intmat_lenslet_ifunc: np_sub=%d (4 or 8)", np_sub);
+    if (field_ld < n_lenses * np_sub) return sb::fail(SB_EINVAL, "sb_intmat_lenslet_ifunc: bad field stride");
+    if ((uintptr_t)ifl % 16) return sb::fail(SB_EINVAL, "sb_intmat_lenslet_ifunc: ifl must be 16-byte aligned");
+    if (n_modes == 0) return SB_OK;
+    const long long per_mode = (long long)n_valid * np_sub * np_sub;
+    const unsigned bx = (unsigned)((per_mode + 255) / 256);
+    const dim3 grid(bx, (unsigned)(n_modes < 64 ? n_modes : 64));
+    cudaStream_t st = sb::as_stream(stream);
+    switch (np_sub) {
+    case 4:
+        intmat_lenslet_layout_kernel<4><<<grid, 256, 0, st>>>(ifunc, n_modes, ld_if, lenslet, n_valid, n_lenses,
+                                                             field_ld, pix2col, ifl);
+        break;
+    case 8:
+        intmat_lenslet_layout_kernel<8><<<grid, 256, 0, st>>>(ifunc, n_modes, ld_if, lenslet, n_valid, n_lenses,
+                                                             field_ld, pix2col, ifl);
+        break;
+    default:
+        return sb::fail(SB_EUNSUPPORTED, "sb_intmat_lenslet_ifunc: np_sub=%d (4 or 8)", np_sub);
+    }
+    return sb::check_launch("intmat_lenslet_layout_kernel");
+}
+
+extern "C" int sb_intmat_contract_lenslets(const float *jac, const float *tot, int n_valid, int np_sub,
+                                           const float *ifl, int n_modes, float scale, float *intmat,
+                                           void *stream) {
+    sb::clear_error();
+    if (!jac || !ifl || !intmat || n_valid < 1 || n_modes < 0)
+        return sb::fail(SB_EINVAL, "sb_intmat_contract_lenslets: bad args");
+    if (np_sub != 4 && np_sub != 8)
+        return sb::fail(SB_EUNSUPPORTED, "sb_intmat_contract_lenslets: np_sub=%d (4 or 8)", np_sub);
+    if ((uintptr_t)ifl % 16) return sb::fail(SB_EINVAL, "sb_intmat_contract_lenslets: ifl must be 16-byte aligned");
+    if (n_modes == 0) return SB_OK;
+    const int per = lenslet_modes_per_cta(n_valid, np_sub, n_modes);
+    const dim3 grid((unsigned)(((long long)n_valid * np_sub + kClThreads - 1) / kClThreads),
+                    (unsigned)((n_modes + per - 1) / per));
+    cudaStream_t st = sb::as_stream(stream);
+    switch (np_sub) {
+    case 4:
+        intmat_contract_lenslet_kernel<4><<<grid, kClThreads, 0, st>>>(jac, tot, n_valid, ifl, n_modes, per, scale,
+                                                                      intmat);
+        break;
+    case 8:
+        intmat_contract_lenslet_kernel<8><<<grid, kClThreads, 0, st>>>(jac, tot, n_valid, ifl, n_modes, per, scale,
+                                                                      intmat);
+        break;
+    default:
+        return sb::fail(SB_EUNSUPPORTED, "sb_intmat_contract_lenslets: np_sub=%d (4 or 8)", np_sub);
+    }
+    return sb::check_launch("intmat_contract_lenslet_kernel");
+}

@@ -315,8 +315,13 @@ class ShSlopesAdjoint:
             if pix2col is None:
                 pix2col = self.pixel_to_column(dm, top, left)
         im = torch.empty((n_modes, 2 * self.n_valid), dtype=torch.float32, device=self.device)
-        segs = self._segments(pix2col, IF, ld)
         tot_ptr = 0 if tot is None else tot.data_ptr()
+        ifl = self.lenslet_ifunc(IF, ld, pix2col) if self.contraction == 'lenslet' else None
+        if ifl is not None:
+            _lib.call('sb_intmat_contract_lenslets', jac.data_ptr(), tot_ptr, self.n_valid, self.np_sub,
+                      ifl.data_ptr(), n_modes, float(2.0 * dm.sign), im.data_ptr(), self._stream())
+            return im
+        segs = self._segments(pix2col, IF, ld) if self.contraction in ('lenslet', 'rows') else None
         if segs is not None:
             _lib.call('sb_intmat_contract_rows', jac.data_ptr(), tot_ptr, self.n_valid, self.np_sub, self.n_lenses,
                       self.field, self._slot.data_ptr(), pix2col.data_ptr(), segs[0].data_ptr(), segs[1],
@@ -358,6 +363,40 @@ class ShSlopesAdjoint:
     # TMA contraction limits: np_sub 4 or 8, at most 992 field columns,
     # influence-function rows of a multiple of 32 floats, a row segment of at
     # most 7168 floats (two ring stages of four modes in one CTA's shared memory)
+    # contraction form of ``intmat``: 'lenslet' (the influence functions
+    # copied once per mirror into a lenslet-major layout, then streamed),
+    # 'rows' (streamed by TMA from the mirror's own layout) or 'gather'; the
+    # first two fall back to the next when their limits are not met, and all
+    # three give the same matrix bit for bit
+    contraction = 'lenslet'
+    LENSLET_NP_SUB = (4, 8)
+    LENSLET_MAX_BYTES = 16 << 30
+
+    def lenslet_ifunc(self, IF, ld, pix2col):
+        """The influence functions under the valid sub-apertures in the
+        lenslet-major layout of sb_intmat_contract_lenslets (n_modes x n_valid
+        x np_sub x np_sub floats, built by sb_intmat_lenslet_ifunc), or None
+        when np_sub or its size is outside the limits; cached per mirror and
+        column map."""
+        n_modes = IF.shape[0]
+        nbytes = 4 * n_modes * self.n_valid * self.np_sub ** 2
+        if self.np_sub not in self.LENSLET_NP_SUB or nbytes > self.LENSLET_MAX_BYTES:
+            return None
+        key = (IF.data_ptr(), n_modes, int(ld), pix2col.data_ptr())
+        cache = getattr(self, '_ifl_cache', None)
+        if cache is None or cache[0] != key:
+            self._ifl_cache = None
+            ifl = torch.empty((n_modes, self.n_valid, self.np_sub, self.np_sub), dtype=torch.float32,
+                              device=self.device)
+            lens = self._lenslet.to(torch.int32)
+            p2c = pix2col.to(torch.int32)
+            _lib.call('sb_intmat_lenslet_ifunc', IF.data_ptr(), n_modes, int(ld), lens.data_ptr(), self.n_valid,
+                      self.np_sub, self.n_lenses, self.field, p2c.data_ptr(), ifl.data_ptr(), self._stream())
+            # the tables stay referenced until the copy has run
+            cache = (key, ifl, IF, pix2col, lens, p2c)
+            self._ifl_cache = cache
+        return cache[1]
+
     TMA_NP_SUB = (4, 8)
     TMA_MAX_COLUMNS = 992
     TMA_MAX_SEGMENT = 7168

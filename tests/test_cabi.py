@@ -166,3 +166,21 @@ def test_row_band_and_stage_validation_without_device(lib):
     assert rc == -1 and b'lenslet rows 18..21 of 20' in lib.sb_last_error()
     assert lib.sb_slopec_cutoff(buf, buf, buf, 0, buf, None) == -1
     assert lib.sb_mc_stage(None, 0, -1, None) == -1
+
+
+def test_lenslet_contraction_validation_without_device(lib):
+    """sb_intmat_lenslet_ifunc and sb_intmat_contract_lenslets reject null
+    pointers, unsupported lenslet sizes and a misaligned layout before any
+    device work."""
+    buf = C.c_void_p(256)                      # never dereferenced: validation fails first
+    assert lib.sb_intmat_lenslet_ifunc(None, 10, 64, buf, 4, 8, 4, 32, buf, buf, None) == -1
+    assert b'bad args' in lib.sb_last_error()
+    rc = lib.sb_intmat_lenslet_ifunc(buf, 10, 64, buf, 4, 16, 4, 64, buf, buf, None)
+    assert rc != 0 and b'np_sub=16' in lib.sb_last_error()
+    rc = lib.sb_intmat_lenslet_ifunc(buf, 10, 64, buf, 4, 8, 4, 16, buf, buf, None)
+    assert rc == -1 and b'field stride' in lib.sb_last_error()
+    assert lib.sb_intmat_contract_lenslets(buf, None, 0, 8, buf, 10, C.c_float(1.0), buf, None) == -1
+    rc = lib.sb_intmat_contract_lenslets(buf, None, 4, 16, buf, 10, C.c_float(1.0), buf, None)
+    assert rc != 0 and b'np_sub=16' in lib.sb_last_error()
+    rc = lib.sb_intmat_contract_lenslets(buf, None, 4, 8, C.c_void_p(260), 10, C.c_float(1.0), buf, None)
+    assert rc == -1 and b'16-byte aligned' in lib.sb_last_error()
