@@ -377,7 +377,8 @@ class ShSlopesAdjoint:
         lenslet-major layout of sb_intmat_contract_lenslets (n_modes x n_valid
         x np_sub x np_sub floats, built by sb_intmat_lenslet_ifunc), or None
         when np_sub or its size is outside the limits; cached per mirror and
-        column map."""
+        column map (an influence-function tensor changed in place needs
+        ``self._ifl_cache = None`` before the next matrix)."""
         n_modes = IF.shape[0]
         nbytes = 4 * n_modes * self.n_valid * self.np_sub ** 2
         if self.np_sub not in self.LENSLET_NP_SUB or nbytes > self.LENSLET_MAX_BYTES:
