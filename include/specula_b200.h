@@ -437,7 +437,10 @@ int sb_modalrec_batched(const float *R, int n_modes, int n_slopes, int ldr, cons
  *                       per thread) with 8 (6-8) or 16 (9-11) realisations per pass in 1024-, 512- or
  *                       256-column tiles
  *   SB_TUNE_SH_FP32     sb_sh_forward / sb_sh_forward_batched; key sb_tune_key(n_lenses, cutsize, n_batch);
- *                       sub-apertures per CTA (8, 4, 2)
+ *                       sub-apertures per CTA (8, 4, 2) with each CTA's field tile staged in shared
+ *                       memory by 2-D TMA loads where the launch allows it (variants 0-2: a single
+ *                       field without the mirror term, 16-byte aligned rows), or read directly
+ *                       (variants 3-5, and every other launch); same frames for the same CTA size
  *   SB_TUNE_MODALREC_BATCHED  sb_modalrec_batched; key sb_tune_key(n_modes, n_slopes, n_batch);
  *                       reconstructor rows per CTA (2, 1, 4)
  * ------------------------------------------------------------------------ */

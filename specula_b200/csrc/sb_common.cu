@@ -89,8 +89,10 @@ const char *const kDmBatchedVariants[] = {
     "16 realisations per pass, 4 columns per thread, 1024-column tiles",
     "16 realisations per pass, 4 columns per thread, 512-column tiles",
     "16 realisations per pass, 4 columns per thread, 256-column tiles"};
-const char *const kShFp32Variants[] = {"8 sub-apertures per CTA", "4 sub-apertures per CTA",
-                                       "2 sub-apertures per CTA"};
+const char *const kShFp32Variants[] = {"8 sub-apertures per CTA, field tile by TMA",
+                                       "4 sub-apertures per CTA, field tile by TMA",
+                                       "2 sub-apertures per CTA, field tile by TMA", "8 sub-apertures per CTA",
+                                       "4 sub-apertures per CTA", "2 sub-apertures per CTA"};
 const char *const kModalrecVariants[] = {"2 reconstructor rows per CTA", "1 reconstructor row per CTA",
                                          "4 reconstructor rows per CTA"};
 }  // namespace

@@ -1030,7 +1030,9 @@ extern "C" int sb_device_status(void) {
                                              "is not 16-byte aligned (those rows were not contracted)")
                        : sb::fail(SB_ETIMEOUT, "an interaction-matrix contraction wait timed out (%s side)",
                                   ct == 1 ? "producer" : "consumer");
-    if (v == 0) return sb::fail(SB_ETIMEOUT, "a tensor-core SH wait timed out (stage %d)", sh);
+    if (v == 0)
+        return sh == 9 ? sb::fail(SB_ETIMEOUT, "an SH field-tile (TMA) wait timed out")
+                       : sb::fail(SB_ETIMEOUT, "a tensor-core SH wait timed out (stage %d)", sh);
     const int zero = 0;
     cudaMemcpyToSymbol(g_dm_status, &zero, sizeof(int));
     return sb::fail(SB_ETIMEOUT, "a DM projection wait timed out (%s side)", v == 1 ? "producer" : "consumer");

@@ -261,6 +261,9 @@ __device__ __forceinline__ ShBlk grid_blk(const ShArgs &a) {
 }
 
 // the compile-time kernel's shared memory (per-warp buffers for 8 warps)
+// nonzero: a bounded wait of an SH kernel timed out (tensor-core stages, or 9: a field tile)
+__device__ int g_sh_tc_status = 0;
+
 template <int P, int CS, int NPX>
 struct FixedSmem {
     float2 twT[P * CS];          // twT[c][b] = W[b][c]
@@ -274,7 +277,9 @@ struct FixedSmem {
 };
 
 template <int P, int CS, int NPX>
-__device__ __forceinline__ void sh_fixed_body(const ShArgs &a, const ShBlk &blk, FixedSmem<P, CS, NPX> &S) {
+__device__ __forceinline__ void sh_fixed_body(const ShArgs &a, const ShBlk &blk, FixedSmem<P, CS, NPX> &S,
+                                              const float *tileA = nullptr, const float *tileP = nullptr,
+                                              uint64_t *tile_bar = nullptr) {
     constexpr int PE = P + 1;
     float2 *twT = S.twT, *tilt = S.tilt;
     float *mask = S.mask, *R = S.R, *red = S.red;
@@ -286,6 +291,14 @@ __device__ __forceinline__ void sh_fixed_body(const ShArgs &a, const ShBlk &blk,
     for (int e = threadIdx.x; e < CS * CS; e += blockDim.x) mask[e] = a.mask[e];
     for (int e = threadIdx.x; e < NPX * CS; e += blockDim.x) R[e] = a.rebin[e];
     __syncthreads();
+    if (tile_bar && !sb::mbar_wait(tile_bar, 0)) {
+        // the field tile did not land in time: record it (stage 9 of the SH
+        // status), give the copies one more bounded wait and read the field
+        // from global memory
+        atomicExch(&g_sh_tc_status, 9);
+        sb::mbar_wait(tile_bar, 0);
+        tileA = nullptr;
+    }
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int i = blk.y;
@@ -299,9 +312,16 @@ __device__ __forceinline__ void sh_fixed_body(const ShArgs &a, const ShBlk &blk,
 #pragma unroll
         for (int e = lane; e < P * P; e += 32) {
             const int r = e / P, c = e % P;
-            const size_t g = (row0 + r) * (size_t)a.ld + col0 + c;
             float amp, phn;
-            field_at(a, g, amp, phn);
+            if (tileA) {
+                // the CTA's field tile: P rows x spc * P columns, this warp's P columns
+                const int o = r * (a.spc * P) + warp * P + c;
+                amp = tileA[o];
+                phn = tileP[o];
+            } else {
+                const size_t g = (row0 + r) * (size_t)a.ld + col0 + c;
+                field_at(a, g, amp, phn);
+            }
             const float phi = phn * a.k;
             float sn, co;
             sincosf(phi, &sn, &co);
@@ -383,6 +403,31 @@ __global__ void __launch_bounds__(256, 4) sh_forward_fixed_kernel(ShArgs a) {
     sh_fixed_body<P, CS, NPX>(a, grid_blk(a), S);
 }
 
+// The same kernel with the CTA's field tile (its lenslet row's P field rows
+// under its spc sub-apertures, amplitude and phase) staged in shared memory
+// by two 2-D TMA loads issued at entry, so the tile is in flight while the
+// CTA loads its DFT tables.  Single field without the mirror term; the same
+// arithmetic on the same values as the plain kernel (bit-identical frames).
+// Columns past the field read as zero and feed no sub-aperture.
+template <int P, int CS, int NPX>
+__global__ void __launch_bounds__(256, 4) sh_forward_fixed_tma_kernel(ShArgs a, const __grid_constant__ CUtensorMap mapA,
+                                                                      const __grid_constant__ CUtensorMap mapP) {
+    __shared__ FixedSmem<P, CS, NPX> S;
+    __shared__ __align__(128) float tileA[8 * P * P];
+    __shared__ __align__(128) float tileP[8 * P * P];
+    __shared__ __align__(8) uint64_t bar;
+    const ShBlk blk = grid_blk(a);
+    if (threadIdx.x == 0) {
+        sb::mbar_init(&bar, 1);
+        sb::mbar_init_fence();
+        sb::mbar_arrive_expect_tx(&bar, (uint32_t)(2 * a.spc * P * P * sizeof(float)));
+        const uint64_t pol = sb::l2_evict_first_policy();
+        sb::tma_load_2d(tileA, &mapA, blk.x * a.spc * P, blk.y * P, &bar, pol);
+        sb::tma_load_2d(tileP, &mapP, blk.x * a.spc * P, blk.y * P, &bar, pol);
+    }
+    sh_fixed_body<P, CS, NPX>(a, blk, S, tileA, tileP, &bar);
+}
+
 // ---------------------------------------------------------------------------
 // Split-BF16 tensor-core form (tcgen05).  One CTA of 128 threads takes 16
 // consecutive sub-apertures of a lenslet row and runs both DFT products as
@@ -407,7 +452,6 @@ constexpr int kTcThreads = 128;         // one thread per MMA row
 constexpr uint32_t kTcTmemCols = 64;    // stage 1 in columns 0-31, then stage 2 tiles in 0-31 and 32-63
 constexpr int kTcOperandBytes = 128 * 32;   // one 128-row x 16 bf16 operand
 
-__device__ int g_sh_tc_status = 0;      // nonzero: a bounded wait on the tensor cores timed out
 
 template <int CS>
 struct TcShape {
@@ -888,6 +932,16 @@ ShTcKernel tc_kernel(int p, int cs, int npx) {
 }
 
 // geometries with a compile-time kernel: (np_sub, cutsize, subap_npx)
+typedef void (*ShTmaKernel)(ShArgs, const CUtensorMap, const CUtensorMap);
+
+ShTmaKernel fixed_tma_kernel(int p, int cs, int npx) {
+    if (p == 8 && cs == 12 && npx == 6) return sh_forward_fixed_tma_kernel<8, 12, 6>;
+    if (p == 8 && cs == 14 && npx == 8) return sh_forward_fixed_tma_kernel<8, 14, 8>;
+    if (p == 8 && cs == 16 && npx == 8) return sh_forward_fixed_tma_kernel<8, 16, 8>;
+    if (p == 8 && cs == 8 && npx == 8) return sh_forward_fixed_tma_kernel<8, 8, 8>;
+    return nullptr;     // np_sub 16: the two tiles would not fit the static shared memory
+}
+
 ShKernel fixed_kernel(int p, int cs, int npx) {
     if (p == 8 && cs == 12 && npx == 6) return sh_forward_fixed_kernel<8, 12, 6>;
     if (p == 8 && cs == 14 && npx == 8) return sh_forward_fixed_kernel<8, 14, 8>;
@@ -996,7 +1050,7 @@ int sh_forward_impl(const char *who, const sb_sh_plan *pl, const float *A, long 
     dim3 grid;
     size_t smem;
     const int variant = mode == 0 ? sb::tune_lookup(SB_TUNE_SH_FP32, sb_tune_key(pl->n_lenses, pl->cutsize, n_batch)) : 0;
-    if (sh_grid(pl, &spc, &grid, &smem, 8 >> variant))
+    if (sh_grid(pl, &spc, &grid, &smem, 8 >> (variant % 3)))
         return sb::fail(SB_ESHAPE, "%s: sub-aperture (np=%d, cut=%d, npx=%d) does not fit in shared memory", who,
                         pl->np_sub, pl->cutsize, pl->subap_npx);
     const size_t need = sb_sh_scratch_bytes(pl) * (size_t)n_batch;
@@ -1077,7 +1131,23 @@ int sh_forward_impl(const char *who, const sb_sh_plan *pl, const float *A, long 
         }
         tk.fn<<<grid, kTcThreads, tk.smem, st>>>(a);
     } else if (fk) {
-        fk<<<grid, 32 * spc, 0, st>>>(a);
+        // variants 0-2: the field tile staged by TMA where the launch allows it
+        // (single field, no mirror term, 16-byte aligned rows); variants 3-5
+        // and every other launch read the field directly (the same frames)
+        ShTmaKernel fkt = variant < 3 && n_batch == 1 && !mirror_A && a.ld % 4 == 0 && (uintptr_t)A % 16 == 0 &&
+                                  (uintptr_t)phase_nm % 16 == 0
+                              ? fixed_tma_kernel(a.p, a.cs, a.npx)
+                              : nullptr;
+        if (fkt) {
+            const int field = pl->n_lenses * pl->np_sub;
+            CUtensorMap mapA, mapP;
+            int rc = sb::tensor_map_2d_f32(&mapA, A, field, field, a.ld, a.p, spc * a.p);
+            if (!rc) rc = sb::tensor_map_2d_f32(&mapP, phase_nm, field, field, a.ld, a.p, spc * a.p);
+            if (rc) return rc;
+            fkt<<<grid, 32 * spc, 0, st>>>(a, mapA, mapP);
+        } else {
+            fk<<<grid, 32 * spc, 0, st>>>(a);
+        }
     } else {
         if (smem > 48 * 1024) {
             cudaError_t e = cudaFuncSetAttribute(sh_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1106,7 +1176,7 @@ extern "C" int sb_sh_rows_parts(const sb_sh_plan *pl, int dft_mode) {
     size_t smem;
     if (dft_mode == 1) return ((pl->n_lenses + kTcSub - 1) / kTcSub) * pl->n_lenses;
     const int variant = sb::tune_lookup(SB_TUNE_SH_FP32, sb_tune_key(pl->n_lenses, pl->cutsize, 1));
-    if (sh_grid(pl, &spc, &grid, &smem, 8 >> variant)) return 0;
+    if (sh_grid(pl, &spc, &grid, &smem, 8 >> (variant % 3))) return 0;
     return (int)(grid.x * grid.y);
 }
 

@@ -8,7 +8,9 @@ from specula_b200 import _lib
 def test_families_and_names():
     lib = _lib.load()
     assert lib.sb_tune_variants(_lib.SB_TUNE_DM_BATCHED) == 12
-    assert lib.sb_tune_variants(_lib.SB_TUNE_SH_FP32) == 3
+    assert lib.sb_tune_variants(_lib.SB_TUNE_SH_FP32) == 6
+    assert b'by TMA' in lib.sb_tune_variant_name(_lib.SB_TUNE_SH_FP32, 0)
+    assert b'TMA' not in lib.sb_tune_variant_name(_lib.SB_TUNE_SH_FP32, 3)
     assert lib.sb_tune_variants(_lib.SB_TUNE_MODALREC_BATCHED) == 3
     assert b'rows per CTA' in lib.sb_tune_variant_name(_lib.SB_TUNE_MODALREC_BATCHED, 2)
     assert lib.sb_tune_variants(99) == 0
