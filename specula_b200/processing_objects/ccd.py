@@ -15,8 +15,12 @@ emccd_gain, Marsaglia-Tsang), clock-induced charge (a Bernoulli electron),
 charge-transfer inefficiency (sb_ccd_step_cte: cte0 * frame * cte1 before the
 noise), pixel gains (constructor or setQuadrantGains) and a per-pixel QE map
 (the reference's notUniformQe attributes) follow ccd.py:218-262 in its order.
-Not on this path (raise NotImplementedError): start_time > 0, 'auto' noise
-levels.  Binning (b x b)
+start_time > 0 (ccd.py:199-207): nothing is integrated or read out before
+start_time, and frames close every dt from there; the gate is evaluated on
+the host at each trigger (a graph captured before start_time would replay
+the capture-time decision), and start_time must be a multiple of the time
+step.  Not on this path (raises NotImplementedError): 'auto' noise levels (a
+table of vendor detector figures).  Binning (b x b)
 runs as sb_ccd_step_binned: block sums scaled as the reference does
 (ccd.py:262-280), then the same QE / noise / ADU model on the binned pixels.
 """
@@ -69,10 +73,14 @@ class CCD(BaseProcessingObj):
         if self._dt % self.loop_dt != 0:
             raise ValueError(f'integration time dt={dt} must be a multiple of the basic simulation '
                              f'time_step={simul_params.time_step}')
-        for flag, what in ((start_time != 0, 'start_time > 0'),
-                           ('auto' in (readout_level, darkcurrent_level, background_level), "'auto' levels")):
-            if flag:
-                raise NotImplementedError(f'CCD: {what} is not on the specula_b200 path')
+        if 'auto' in (readout_level, darkcurrent_level, background_level):
+            raise NotImplementedError("CCD: 'auto' levels are not on the specula_b200 path")
+        self._start_time = self.seconds_to_t(start_time)
+        if self._start_time < 0:
+            raise ValueError(f'start_time is {start_time} and must not be negative')
+        if self._start_time % self.loop_dt != 0:
+            raise NotImplementedError(f'CCD: start_time={start_time} must be a multiple of the time step '
+                                      f'{simul_params.time_step} on the specula_b200 path')
         if excess_noise:
             # the reference sets the EMCCD and ADU gains itself when excess noise is on (ccd.py:100-103)
             emccd_gain = 400
@@ -202,7 +210,13 @@ class CCD(BaseProcessingObj):
             raise ValueError(f'CCD: {name} must hold {rows} x {cols} values')
         return t
 
+    def _before_start(self):
+        # ccd.py:199: no integration (and no frame) before start_time
+        return self._start_time > 0 and self.current_time < self._start_time
+
     def trigger_code(self):
+        if self._before_start():
+            return
         if self._cte is not None:
             rows = self._pixels.size[0]
             _lib.call('sb_ccd_step_cte', _byref(self._params), rows, self._cte[0].data_ptr(), self._cte[1].data_ptr(),
@@ -219,6 +233,8 @@ class CCD(BaseProcessingObj):
                   self._pixels.pixels.data_ptr(), self.stream_handle())
 
     def post_trigger(self):
+        if self._before_start():
+            return
         # host mirror of the device frame counter, for the time stamps
         self._n_integrated += 1
         if self._n_integrated >= self._frames_per_read:

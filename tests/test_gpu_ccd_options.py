@@ -127,3 +127,61 @@ def test_pixel_gains_and_qe_map_match_oracle(cuda, normalise):
 def test_pixel_gains_on_an_integer_frame_are_rejected(cuda):
     with pytest.raises(ValueError, match='integer'):
         _ccd(64, photon_noise=True, pixelGains=np.ones((64, 64), np.float32))
+
+
+@pytest.mark.parametrize('start_steps, frame_steps', [(3, 2), (4, 1), (5, 3)])
+def test_start_time_gates_integration_and_frames(cuda, start_steps, frame_steps):
+    """start_time (ccd.py:199-207): nothing integrates before it, and a frame
+    closes at step t when (t + 1 - D - S) % D == 0 (S the start and D the
+    frame length in steps).  Each frame then equals that of a detector
+    started at step 0 and fed the same intensities from step S on."""
+    from specula_b200.processing_objects.ccd import CCD
+    from specula_b200.data_objects.intensity import Intensity
+    from specula_b200.data_objects.simul_params import SimulParams
+    sp = SimulParams(pixel_pupil=64, pixel_pitch=0.01, time_step=0.001)
+    side, n = 32, 14
+    rng = np.random.default_rng(start_steps)
+    inten = [rng.uniform(0.0, 50.0, (side, side)).astype(np.float32) for _ in range(n)]
+
+    def run(start, feed_from):
+        c = CCD(sp, size=[side, side], dt=0.001 * frame_steps, bandw=1000, target_device_idx=0,
+                start_time=0.001 * start)
+        ii = Intensity(side, side, target_device_idx=0)
+        c.inputs['in_i'].set(ii)
+        c.setup()
+        frames, stamps = [], []
+        for t in range(n - feed_from):
+            ii.i.copy_(torch.as_tensor(inten[t + feed_from]))
+            ii.generation_time = t * 1000000
+            c.check_ready(t * 1000000)
+            c.trigger()
+            c.post_trigger()
+            frames.append(c.outputs['out_pixels'].pixels.cpu().numpy().copy())
+            stamps.append(c.outputs['out_pixels'].generation_time)
+        return frames, stamps
+
+    frames, stamps = run(start_steps, 0)
+    ref_frames, _ = run(0, start_steps)
+    S, D = start_steps, frame_steps
+    closes = [t for t in range(n) if t >= S and (t + 1 - D - S) % D == 0]
+    assert closes, 'no frame in the test window'
+    for t in range(n):
+        done = [c for c in closes if c <= t]
+        assert stamps[t] == (done[-1] * 1000000 if done else stamps[0]), t
+        if not done:
+            assert float(np.abs(frames[t]).max()) == 0.0, t
+    for c in closes:
+        assert np.array_equal(frames[c], ref_frames[c - S]), c
+        assert float(frames[c].max()) > 0
+    from specula_b200 import _lib
+    _lib.call('sb_device_status')
+
+
+def test_start_time_off_the_step_grid_is_rejected():
+    from specula_b200.processing_objects.ccd import CCD
+    from specula_b200.data_objects.simul_params import SimulParams
+    sp = SimulParams(pixel_pupil=64, pixel_pitch=0.01, time_step=0.001)
+    with pytest.raises(NotImplementedError, match='multiple of the time step'):
+        CCD(sp, size=[16, 16], dt=0.002, bandw=1000, start_time=0.0015)
+    with pytest.raises(NotImplementedError, match="'auto'"):
+        CCD(sp, size=[16, 16], dt=0.002, bandw=1000, readout_level='auto', darkcurrent_level=1, background_level=1)
