@@ -1,6 +1,7 @@
 """Oracle: CCD detector (test infrastructure only).
 
-Restates specula/processing_objects/ccd.py:198-287 (integration, binning,
+Restates specula/processing_objects/ccd.py:198-287 (the start_time gate,
+integration, binning,
 QE, background/dark, Poisson photon noise, Gaussian readout noise, ADU
 quantisation), and the deterministic detector-structure options: the
 charge-transfer matrices (ccd.py:223-224), pixel gains (:239-240) and the
@@ -57,6 +58,23 @@ class CCDOracle:
         self.count += 1
         if self.count % self.frames_per_read:
             return None
+        return self._read()
+
+    def step_at(self, intensity, t, start=0):
+        """The loop step at time t with the start_time gate and read-out rule
+        of ccd.py:199-207 (times in loop steps, start a multiple of them):
+        nothing before ``start``; the frame closes when
+        (t + 1 - D - start) is a multiple of D, D = frames_per_read.  Returns
+        the frame when one closes, else None."""
+        if start > 0 and t < start:
+            return None
+        self.integrated += intensity * self.dt_ratio
+        D = self.frames_per_read
+        if (t + 1 - D - start) % D:
+            return None
+        return self._read()
+
+    def _read(self):
         frame = self._binning()
         if self.qe != 1:
             frame = frame * self.qe

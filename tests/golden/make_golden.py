@@ -724,6 +724,44 @@ PS_NAME_CASES = [
 ]
 
 
+def make_ccd_start_cases():
+    """The reference CCD with start_time > 0 (ccd.py:199-207): seeded
+    intensities per step, frame length 2 and 3 steps, noise-free and with
+    photon + read-out noise (its own NumPy generators); per step the output
+    frame and its generation time."""
+    import specula  # noqa: F401
+    from specula.processing_objects.ccd import CCD
+    from specula.data_objects.intensity import Intensity
+    from specula.data_objects.simul_params import SimulParams
+    out = {}
+    rng = np.random.default_rng(11)
+    sp = SimulParams(pixel_pupil=64, pixel_pitch=0.01, time_step=0.001)
+    n = 12
+    inten = (rng.random((n, 24, 24)) * 0.3).astype(np.float32)
+    out['intensity'] = inten
+    for tag, kw in (('clean_s3_d2', dict(start_time=0.003, dt=0.002)),
+                    ('clean_s4_d3', dict(start_time=0.004, dt=0.003)),
+                    ('noisy_s3_d2', dict(start_time=0.003, dt=0.002, photon_noise=True, readout_noise=True,
+                                         readout_level=3.0))):
+        c = CCD(sp, size=[24, 24], bandw=300, quantum_eff=0.5, target_device_idx=-1, **kw)
+        ii = Intensity(24, 24, target_device_idx=-1)
+        c.inputs['in_i'].set(ii)
+        c.setup()
+        frames, stamps = [], []
+        for t in range(n):
+            ii.i[:] = inten[t]
+            tt = t * 1000000
+            ii.generation_time = tt
+            c.check_ready(tt)
+            c.trigger()
+            c.post_trigger()
+            frames.append(np.array(c.outputs['out_pixels'].pixels, dtype=np.float64))
+            stamps.append(c.outputs['out_pixels'].generation_time)
+        out[tag + '/frames'] = np.array(frames)
+        out[tag + '/stamps'] = np.array(stamps, dtype=np.int64)
+    return out
+
+
 def make_phasescreen_names():
     """File names the reference's phasescreen cache writes
     (lib/phasescreen_manager.py), captured through the harness fits stand-in."""
@@ -768,6 +806,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, 'iir_fp32.npz'), **make_iir_cases())
     np.savez_compressed(os.path.join(HERE, 'slopec_filt_fp32.npz'), **make_slopec_filter_cases(ref))
     np.savez_compressed(os.path.join(HERE, 'slopec_opt_fp32.npz'), **make_slopec_option_cases(ref))
+    np.savez_compressed(os.path.join(HERE, 'ccd_start_fp32.npz'), **make_ccd_start_cases())
     print('wrote', sorted(os.listdir(HERE)))
 
 
@@ -825,6 +864,10 @@ if __name__ == '__main__':
         specula.init(-1, precision=1)
         with open(os.path.join(HERE, 'phasescreen_names.json'), 'w') as f:
             json.dump(make_phasescreen_names(), f, indent=1)
+    elif '--ccd-start' in sys.argv:    # only the CCD start_time fixtures
+        import specula
+        specula.init(-1, precision=1)
+        np.savez_compressed(os.path.join(HERE, 'ccd_start_fp32.npz'), **make_ccd_start_cases())
     elif '--zernike' in sys.argv:      # only the Zernike influence-function tables
         import specula
         specula.init(-1, precision=1)

@@ -1,6 +1,8 @@
 """The oracle is pinned against the reference: golden vectors produced by
 running SPECULA itself (tests/golden/make_golden.py) and the reference's own
 committed FITS fixtures (test/data/*.fits, converted to ref_fits.npz)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -77,6 +79,29 @@ def test_ccd_matches_reference(golden, tag, kw):
         if last is not None:
             # the reference keeps its last frame between read-outs
             np.testing.assert_allclose(np.asarray(last, dtype=np.float64), ref[t], rtol=1e-6, atol=1e-6)
+
+
+@pytest.mark.parametrize('tag,start,kw', [('clean_s3_d2', 3, dict(dt_s=0.002)),
+                                          ('clean_s4_d3', 4, dict(dt_s=0.003)),
+                                          ('noisy_s3_d2', 3, dict(dt_s=0.002, photon_noise=True,
+                                                                  readout_noise=True, readout_level=3.0))])
+def test_ccd_start_time_matches_reference(tag, start, kw):
+    """The oracle's start_time gate and read-out rule (ccd.py:199-207)
+    against the reference CCD run with start_time > 0
+    (tests/golden/ccd_start_fp32.npz): the frame held at every step and the
+    steps at which frames close."""
+    with np.load(os.path.join(os.path.dirname(__file__), 'golden', 'ccd_start_fp32.npz')) as z:
+        g = {k: z[k] for k in z.files}
+    o = occd.CCDOracle((24, 24), loop_dt_s=0.001, bandw=300, quantum_eff=0.5, **kw)
+    frames, stamps = g[tag + '/frames'], g[tag + '/stamps']
+    held, when = np.zeros((24, 24)), -1
+    for t in range(len(frames)):
+        f = o.step_at(g['intensity'][t], t, start)
+        if f is not None:
+            held, when = np.asarray(f, dtype=np.float64), t * 1000000
+        assert stamps[t] == when, t
+        np.testing.assert_allclose(held, frames[t], rtol=1e-6, atol=1e-6)
+    assert when > 0
 
 
 def test_integrator_matches_reference(golden):
