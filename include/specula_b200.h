@@ -545,7 +545,10 @@ int sb_intmat_contract_rows(const float *jac, const float *tot, int n_valid, int
  * sb_intmat_contract_lenslets then reads that array once per matrix (one
  * contiguous np_sub^2 run per mode and sub-aperture) with jac, tot and
  * scale as in sb_intmat_contract, and writes the same matrix bit for bit
- * (the same products, summed in the same order).  np_sub 4 or 8. */
+ * (the same products, summed in the same order).  The mean flux of the CoG
+ * cut-off is summed over another thread grouping, so a sub-aperture whose
+ * flux lies within a rounding of the cut-off could be decided the other
+ * way.  np_sub 4 or 8. */
 int sb_intmat_lenslet_ifunc(const float *ifunc, int n_modes, int ld_if, const int32_t *lenslet, int n_valid,
                             int np_sub, int n_lenses, int field_ld, const int32_t *pix2col, float *ifl,
                             void *stream);
