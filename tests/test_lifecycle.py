@@ -86,3 +86,29 @@ def test_any_fresh_input_makes_the_object_due():
     c.trigger()
     assert not c.check_ready(5)
     assert c.runs == 2
+
+
+def test_lenslet_grid_and_calibrator_boxes():
+    """Lenslet.get(i, j) = [x, y, side] on the make_xy grid (x along j), and
+    the calibrator's per-lenslet pixel boxes, as the oracle's sub-aperture
+    detection builds them (sh_subap_calibrator.py:47-60)."""
+    import numpy as np
+    from specula_b200.data_objects.lenslet import Lenslet
+    from specula_b200.processing_objects.sh_subap_calibrator import lenslet_boxes
+    for n, side in ((1, 8), (4, 24), (8, 64), (12, 72), (20, 160), (40, 240)):
+        lens = Lenslet(n)
+        assert (lens.dimx, lens.dimy) == (n, n)
+        centres = (np.arange(n) - (n - 1) / 2.0) / (n / 2.0)
+        for i in range(n):
+            for j in range(n):
+                x, y, size = lens.get(i, j)
+                assert abs(x - centres[j]) < 1e-12 and abs(y - centres[i]) < 1e-12 and size == 2.0 / n
+        boxes, np_sub = lenslet_boxes(n, side)
+        assert np_sub == round(side / 2.0 * 2.0 / n)
+        want = []
+        for i in range(n):
+            for j in range(n):
+                xc, yc = side / 2.0 * (1 + centres[j]), side / 2.0 * (1 + centres[i])
+                want.append((int(np.round(xc - np_sub / 2)), int(np.round(xc + np_sub / 2)),
+                             int(np.round(yc - np_sub / 2)), int(np.round(yc + np_sub / 2))))
+        assert boxes == want
